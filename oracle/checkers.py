@@ -1,0 +1,225 @@
+"""ctypes front end for the CPU checkers (TEST INFRASTRUCTURE, not the product).
+
+Two interchangeable backends with one interface:
+  * ``kind="oracle"``: liboracle.so, the plain-C restatement of the reference step
+  * ``kind="ref"``:    _ref/libavbd_ref.so, the reference solver compiled from its own
+                      sources with a thin driver (built only where the reference exists;
+                      the prebuilt library travels with the repository)
+
+Only the tests, the smoke check and the benchmark's CPU-baseline leg use this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libavbd_ref.so")
+
+_libs: dict[str, ctypes.CDLL] = {}
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_float), ("gravity", ctypes.c_float), ("iterations", ctypes.c_int),
+                ("alpha", ctypes.c_float), ("betaLin", ctypes.c_float), ("betaAng", ctypes.c_float),
+                ("gamma", ctypes.c_float), ("broadphase", ctypes.c_int), ("orderMode", ctypes.c_int)]
+
+
+def build_oracle() -> str:
+    """Compile liboracle.so if missing or stale (gcc only; works on any box)."""
+    src = os.path.join(HERE, "avbd_oracle.c")
+    if not os.path.exists(ORACLE_LIB) or os.path.getmtime(ORACLE_LIB) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+    return ORACLE_LIB
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def _lib(kind: str) -> ctypes.CDLL:
+    if kind in _libs:
+        return _libs[kind]
+    if kind == "oracle":
+        lib = ctypes.CDLL(build_oracle())
+        p = "oracle_"
+    elif kind == "ref":
+        if not ref_available():
+            raise FileNotFoundError(f"{REF_LIB} not built (needs the reference sources: make -C oracle ref)")
+        lib = ctypes.CDLL(REF_LIB)
+        p = "ref_"
+    else:
+        raise ValueError(kind)
+    vp, ip, fp = ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p
+    getattr(lib, p + "create").restype = vp
+    getattr(lib, p + "create").argtypes = [ctypes.POINTER(_Params), ip] + [fp] * 6 + [ip] + [fp] * 6
+    for name in ("destroy",):
+        getattr(lib, p + name).argtypes = [vp]
+        getattr(lib, p + name).restype = None
+    for name in ("prepare", "iterate", "finish", "num_bodies", "num_manifolds", "num_joints"):
+        getattr(lib, p + name).argtypes = [vp]
+        getattr(lib, p + name).restype = ip
+    getattr(lib, p + "step").argtypes = [vp, ip]
+    getattr(lib, p + "step").restype = ip
+    getattr(lib, p + "set_params").argtypes = [vp, ctypes.POINTER(_Params)]
+    getattr(lib, p + "set_params").restype = None
+    getattr(lib, p + "get_bodies").argtypes = [vp] + [fp] * 5
+    getattr(lib, p + "get_bodies").restype = None
+    getattr(lib, p + "get_body_props").argtypes = [vp] + [fp] * 5
+    getattr(lib, p + "get_body_props").restype = None
+    getattr(lib, p + "get_manifolds").argtypes = [vp] + [fp] * 8
+    getattr(lib, p + "get_manifolds").restype = None
+    getattr(lib, p + "get_joints").argtypes = [vp] + [fp] * 3
+    getattr(lib, p + "get_joints").restype = None
+    getattr(lib, p + "get_counters").argtypes = [vp, fp]
+    getattr(lib, p + "get_counters").restype = None
+    getattr(lib, p + "collide_boxes").argtypes = [fp] * 10
+    getattr(lib, p + "collide_boxes").restype = ip
+    if kind == "oracle":
+        lib.oracle_get_colours.argtypes = [vp, fp, fp]
+        lib.oracle_get_colours.restype = None
+        lib.oracle_get_solve_order.argtypes = [vp, fp]
+        lib.oracle_get_solve_order.restype = ip
+        lib.oracle_get_body_aux.argtypes = [vp] + [fp] * 4
+        lib.oracle_get_body_aux.restype = None
+        lib.oracle_set_bodies.argtypes = [vp] + [fp] * 5
+        lib.oracle_set_bodies.restype = None
+        lib.oracle_colour_priority.argtypes = [ctypes.c_uint32]
+        lib.oracle_colour_priority.restype = ctypes.c_uint32
+    else:
+        lib.ref_iterate_ordered.argtypes = [vp, fp, ip]
+        lib.ref_iterate_ordered.restype = ip
+    _libs[kind] = lib
+    return lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def make_params(params, order_mode: int = 0) -> _Params:
+    return _Params(params.dt, params.gravity, params.iterations, params.alpha, params.betaLin, params.betaAng,
+                   params.gamma, params.broadphase, order_mode)
+
+
+class World:
+    """A scene stepped by the oracle or the reference; all queries are in list order."""
+
+    def __init__(self, scene, kind: str = "oracle", order_mode: int = 0):
+        self.kind = kind
+        self.lib = _lib(kind)
+        self.p = "oracle_" if kind == "oracle" else "ref_"
+        self._keep = [np.ascontiguousarray(x) for x in (
+            scene.size, scene.density, scene.friction, scene.pos, scene.vel, scene.quat,
+            scene.ftype, scene.fa, scene.fb, scene.frA, scene.frB, scene.fparam)]
+        k = self._keep
+        self.params = make_params(scene.params, order_mode)
+        self.h = self._f("create")(ctypes.byref(self.params), scene.n_bodies, *[_ptr(x) for x in k[:6]],
+                                   scene.n_forces, *[_ptr(x) for x in k[6:]])
+        self.n = scene.n_bodies
+
+    def _f(self, name):
+        return getattr(self.lib, self.p + name)
+
+    def close(self):
+        if self.h:
+            self._f("destroy")(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n: int = 1):
+        self._f("step")(self.h, n)
+
+    def prepare(self):
+        self._f("prepare")(self.h)
+
+    def iterate(self):
+        self._f("iterate")(self.h)
+
+    def iterate_ordered(self, order: np.ndarray):
+        order = np.ascontiguousarray(order, dtype=np.int32)
+        self.lib.ref_iterate_ordered(self.h, _ptr(order), int(order.size))
+
+    def finish(self):
+        self._f("finish")(self.h)
+
+    def bodies(self) -> dict:
+        n = self.n
+        out = {k: np.zeros((n, d), np.float32) for k, d in
+               (("pos", 3), ("quat", 4), ("vel", 3), ("angvel", 3), ("prevvel", 3))}
+        self._f("get_bodies")(self.h, *[_ptr(out[k]) for k in ("pos", "quat", "vel", "angvel", "prevvel")])
+        return out
+
+    def body_props(self) -> dict:
+        n = self.n
+        out = {"mass": np.zeros(n, np.float32), "moment": np.zeros((n, 3), np.float32),
+               "radius": np.zeros(n, np.float32), "size": np.zeros((n, 3), np.float32),
+               "friction": np.zeros(n, np.float32)}
+        self._f("get_body_props")(self.h, *[_ptr(out[k]) for k in ("mass", "moment", "radius", "size", "friction")])
+        return out
+
+    def manifolds(self) -> dict:
+        m = self._f("num_manifolds")(self.h)
+        out = {"ab": np.zeros((m, 2), np.int32), "seq": np.zeros(m, np.int64), "n": np.zeros(m, np.int32),
+               "basis": np.zeros((m, 9), np.float32), "friction": np.zeros(m, np.float32),
+               "keys": np.zeros((m, 8), np.int32), "contact": np.zeros((m, 8, 15), np.float32),
+               "stick": np.zeros((m, 8), np.int32)}
+        self._f("get_manifolds")(self.h, *[_ptr(out[k]) for k in
+                                           ("ab", "seq", "n", "basis", "friction", "keys", "contact", "stick")])
+        return out
+
+    def joints(self) -> dict:
+        m = self._f("num_joints")(self.h)
+        out = {"ab": np.zeros((m, 2), np.int32), "state": np.zeros((m, 18), np.float32),
+               "broken": np.zeros(m, np.int32)}
+        self._f("get_joints")(self.h, _ptr(out["ab"]), _ptr(out["state"]), _ptr(out["broken"]))
+        return out
+
+    def counters(self) -> np.ndarray:
+        c = np.zeros(9, np.int64)
+        self._f("get_counters")(self.h, _ptr(c))
+        return c
+
+    # oracle-only
+    def colours(self):
+        c = np.zeros(self.n, np.int32)
+        nc = np.zeros(1, np.int32)
+        self.lib.oracle_get_colours(self.h, _ptr(c), _ptr(nc))
+        return c, int(nc[0])
+
+    def solve_order(self) -> np.ndarray:
+        o = np.zeros(max(self.n, 1), np.int32)
+        k = self.lib.oracle_get_solve_order(self.h, _ptr(o))
+        return o[:k].copy()
+
+    def body_aux(self) -> dict:
+        n = self.n
+        out = {"init_lin": np.zeros((n, 3), np.float32), "init_ang": np.zeros((n, 4), np.float32),
+               "inert_lin": np.zeros((n, 3), np.float32), "inert_ang": np.zeros((n, 4), np.float32)}
+        self.lib.oracle_get_body_aux(self.h, *[_ptr(out[k]) for k in ("init_lin", "init_ang", "inert_lin", "inert_ang")])
+        return out
+
+
+def collide_boxes(kind: str, pA, qA, sA, pB, qB, sB):
+    lib = _lib(kind)
+    f = getattr(lib, ("oracle_" if kind == "oracle" else "ref_") + "collide_boxes")
+    args = [np.ascontiguousarray(np.asarray(x, np.float32)) for x in (pA, qA, sA, pB, qB, sB)]
+    keys = np.zeros(8, np.int32)
+    rA = np.zeros((8, 3), np.float32)
+    rB = np.zeros((8, 3), np.float32)
+    basis = np.zeros(9, np.float32)
+    n = f(*[_ptr(a) for a in args], _ptr(keys), _ptr(rA), _ptr(rB), _ptr(basis))
+    return n, keys, rA, rB, basis
+
+
+def colour_priority(b: int) -> int:
+    return int(_lib("oracle").oracle_colour_priority(b))

@@ -1,0 +1,1388 @@
+// Host side of the B200 AVBD step: context, device memory, launch orchestration and
+// the C ABI declared in include/avbd_cuda.h.
+//
+// One avbd_step() runs what Solver::stepCpuReference does (solver.cpp:1036-1041) as a
+// sequence of kernels on the context stream:
+//   broadphase (grid or all pairs) -> new manifolds in the reference's creation order
+//   -> manifold/joint initialisation -> compaction -> per-body force lists (CSR, newest
+//   first) -> body warm start -> Jones-Plassmann colouring -> iterations x (per-colour
+//   primal, dual) -> velocities.
+// The host reads a handful of counts per step (new pairs, surviving forces, colouring
+// progress, colour ranges) to size launches and buffers.
+#include "../../include/avbd_cuda.h"
+#include "avbd_kernels.cuh"
+
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace avbd;
+
+namespace
+{
+
+template <class T>
+struct DArr
+{
+    T *p = nullptr;
+    size_t cap = 0;
+};
+
+struct ManBuf
+{
+    DArr<int2> ab;
+    DArr<unsigned long long> seq;
+    DArr<int> n;
+    DArr<float4> basis;
+    DArr<float4> contact;
+};
+
+constexpr int PRIMAL_BLOCK = 128;
+constexpr int PRIMAL_GROUP = 8;
+constexpr unsigned CELL_TABLE = CELL_TABLE_SIZE;
+
+} // namespace
+
+struct AvbdContext
+{
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool ownStream = false;
+    std::string err;
+    int errCode = 0;
+    AvbdParams params{};
+    bool loaded = false;
+
+    int n = 0;
+    DArr<float4> pos, quat, initLin, initAng, inertLin, inertAng, vel, angvel, prevVel, massMoment, sizeRad;
+    DArr<float> friction;
+
+    std::vector<int> hBinned, hLarge;
+    float binnedRadius = 0.0f;
+    DArr<int> binned, large;
+    DArr<float4> largeLo, largeHi, largeSphere;
+    DArr<int> llCount, llOffset;
+    DArr<unsigned> bounds;
+    DArr<GridParams> grid;
+    DArr<unsigned> cellStart;
+    DArr<unsigned long long> bpKeys, bpKeysAlt;
+    DArr<int> pairCount, pairOffset;
+
+    ManBuf man[2];
+    int cur = 0;
+    int nMan = 0;
+    DArr<unsigned char> keep;
+    DArr<int> keepIdx;
+
+    int nJoint = 0, nSpring = 0, nIgnore = 0;
+    DArr<int2> jointAB[2];
+    DArr<unsigned long long> jointSeq[2];
+    DArr<float4> joint[2];
+    int jcur = 0;
+    DArr<int2> springAB, ignoreAB;
+    DArr<unsigned long long> springSeq, ignoreSeq;
+    DArr<float4> spring;
+
+    DArr<int> adjStart;
+    DArr<unsigned> adj, incVals, incValsAlt;
+    DArr<unsigned long long> incKeys, incKeysAlt;
+
+    DArr<int> colourState, colour, solveList, colourStart, remaining;
+    DArr<unsigned long long> colKeys, colKeysAlt;
+    std::vector<int> hColourStart;
+    int nColours = 0, nSolve = 0;
+
+    DArr<char> cubTemp;
+    DArr<StepCounters> counters;
+    StepCounters *hCounters = nullptr;
+    long long *hScalars = nullptr; // pinned scratch for small readbacks
+
+    long long nextSeq = 0;
+    AvbdStats stats{};
+    cudaEvent_t evStart = nullptr, evStop = nullptr;
+
+    // profiling: events around each phase, summed per phase after the step
+    bool profiling = false;
+    std::vector<cudaEvent_t> evPool;
+    size_t evUsed = 0;
+    std::vector<std::pair<int, std::pair<size_t, size_t>>> marks;
+    double phaseMs[AVBD_PHASE_COUNT] = {0};
+    long long phaseLaunches[AVBD_PHASE_COUNT] = {0};
+    long long launches = 0;
+    long long stepsProfiled = 0;
+};
+
+namespace
+{
+
+int fail(AvbdContext *ctx, int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (ctx)
+    {
+        ctx->err = buf;
+        ctx->errCode = code;
+    }
+    return code;
+}
+
+#define CU(call)                                                                                                   \
+    do                                                                                                             \
+    {                                                                                                              \
+        cudaError_t e_ = (call);                                                                                   \
+        if (e_ != cudaSuccess)                                                                                     \
+            return fail(ctx, AVBD_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__,      \
+                        __LINE__);                                                                                 \
+    } while (0)
+
+#define CHECK(expr)                                                                                                \
+    do                                                                                                             \
+    {                                                                                                              \
+        int r_ = (expr);                                                                                           \
+        if (r_ != AVBD_OK)                                                                                         \
+            return r_;                                                                                             \
+    } while (0)
+
+#define LAUNCHED()                                                                                                 \
+    do                                                                                                             \
+    {                                                                                                              \
+        ctx->launches++;                                                                                           \
+        cudaError_t e_ = cudaGetLastError();                                                                       \
+        if (e_ != cudaSuccess)                                                                                     \
+            return fail(ctx, AVBD_ERR_CUDA, "kernel launch failed: %s (%s:%d)", cudaGetErrorString(e_), __FILE__,  \
+                        __LINE__);                                                                                 \
+    } while (0)
+
+template <class T>
+int reserve(AvbdContext *ctx, DArr<T> &a, size_t count, bool preserve, size_t used = 0)
+{
+    if (count <= a.cap && a.p)
+        return AVBD_OK;
+    size_t cap = std::max(count, a.cap + a.cap / 2);
+    cap = std::max<size_t>(cap, 16);
+    T *p = nullptr;
+    CU(cudaMalloc((void **)&p, cap * sizeof(T)));
+    if (a.p)
+    {
+        if (preserve && used)
+            CU(cudaMemcpyAsync(p, a.p, std::min(used, a.cap) * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+        CU(cudaFree(a.p));
+    }
+    a.p = p;
+    a.cap = cap;
+    return AVBD_OK;
+}
+
+template <class T>
+void release(DArr<T> &a)
+{
+    if (a.p)
+        cudaFree(a.p);
+    a.p = nullptr;
+    a.cap = 0;
+}
+
+int grid_for(long long n, int block) { return (int)std::max<long long>(1, (n + block - 1) / block); }
+
+int ensure_temp(AvbdContext *ctx, size_t bytes) { return reserve(ctx, ctx->cubTemp, bytes, false); }
+
+// Phase timing with CUDA events on the context stream (enabled by avbd_set_profiling).
+int prof_event(AvbdContext *ctx, size_t &idx)
+{
+    if (ctx->evUsed == ctx->evPool.size())
+    {
+        cudaEvent_t e;
+        CU(cudaEventCreate(&e));
+        ctx->evPool.push_back(e);
+    }
+    idx = ctx->evUsed++;
+    CU(cudaEventRecord(ctx->evPool[idx], ctx->stream));
+    return AVBD_OK;
+}
+
+struct PhaseScope
+{
+    AvbdContext *ctx;
+    int phase;
+    size_t begin = 0;
+    bool on;
+    PhaseScope(AvbdContext *c, int p) : ctx(c), phase(p), on(c->profiling)
+    {
+        if (on && prof_event(ctx, begin) != AVBD_OK)
+            on = false;
+    }
+    ~PhaseScope()
+    {
+        size_t end;
+        if (on && prof_event(ctx, end) == AVBD_OK)
+            ctx->marks.push_back({phase, {begin, end}});
+    }
+};
+
+int prof_collect(AvbdContext *ctx)
+{
+    if (!ctx->profiling)
+        return AVBD_OK;
+    CU(cudaStreamSynchronize(ctx->stream));
+    for (auto &m : ctx->marks)
+    {
+        float ms = 0.0f;
+        CU(cudaEventElapsedTime(&ms, ctx->evPool[m.second.first], ctx->evPool[m.second.second]));
+        ctx->phaseMs[m.first] += ms;
+        ctx->phaseLaunches[m.first]++;
+    }
+    ctx->marks.clear();
+    ctx->evUsed = 0;
+    ctx->stepsProfiled++;
+    return AVBD_OK;
+}
+
+int reserve_manifolds(AvbdContext *ctx, ManBuf &b, size_t count, size_t used)
+{
+    CHECK(reserve(ctx, b.ab, count, true, used));
+    CHECK(reserve(ctx, b.seq, count, true, used));
+    CHECK(reserve(ctx, b.n, count, true, used));
+    CHECK(reserve(ctx, b.basis, 3 * count, true, 3 * used));
+    CHECK(reserve(ctx, b.contact, 32 * count, true, 32 * used));
+    return AVBD_OK;
+}
+
+DevBodies dev_bodies(AvbdContext *ctx)
+{
+    DevBodies B;
+    B.n = ctx->n;
+    B.pos = ctx->pos.p;
+    B.quat = ctx->quat.p;
+    B.initLin = ctx->initLin.p;
+    B.initAng = ctx->initAng.p;
+    B.inertLin = ctx->inertLin.p;
+    B.inertAng = ctx->inertAng.p;
+    B.vel = ctx->vel.p;
+    B.angvel = ctx->angvel.p;
+    B.prevVel = ctx->prevVel.p;
+    B.massMoment = ctx->massMoment.p;
+    B.sizeRad = ctx->sizeRad.p;
+    B.friction = ctx->friction.p;
+    return B;
+}
+
+DevManifolds dev_man(ManBuf &b)
+{
+    DevManifolds M;
+    M.ab = b.ab.p;
+    M.seq = b.seq.p;
+    M.n = b.n.p;
+    M.basis = b.basis.p;
+    M.contact = b.contact.p;
+    return M;
+}
+
+DevForces dev_forces(AvbdContext *ctx)
+{
+    DevForces F;
+    F.nMan = ctx->nMan;
+    F.man = dev_man(ctx->man[ctx->cur]);
+    F.nJoint = ctx->nJoint;
+    F.jointAB = ctx->jointAB[ctx->jcur].p;
+    F.jointSeq = ctx->jointSeq[ctx->jcur].p;
+    F.joint = ctx->joint[ctx->jcur].p;
+    F.nSpring = ctx->nSpring;
+    F.springAB = ctx->springAB.p;
+    F.springSeq = ctx->springSeq.p;
+    F.spring = ctx->spring.p;
+    F.nIgnore = ctx->nIgnore;
+    F.ignoreAB = ctx->ignoreAB.p;
+    F.ignoreSeq = ctx->ignoreSeq.p;
+    F.adjStart = ctx->adjStart.p;
+    F.adj = ctx->adj.p;
+    return F;
+}
+
+Params dev_params(const AvbdParams &p)
+{
+    Params P;
+    P.dt = p.dt;
+    P.gravity = p.gravity;
+    P.iterations = p.iterations;
+    P.alpha = p.alpha;
+    P.betaLin = p.betaLin;
+    P.betaAng = p.betaAng;
+    P.gamma = p.gamma;
+    return P;
+}
+
+// Exclusive scan of n ints into out; total (out[n-1] + in[n-1]) lands in hScalars[slot].
+int scan_counts(AvbdContext *ctx, const int *in, int *out, int n, int slot)
+{
+    size_t bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, ctx->stream);
+    CHECK(ensure_temp(ctx, bytes));
+    CU(cub::DeviceScan::ExclusiveSum(ctx->cubTemp.p, bytes, in, out, n, ctx->stream));
+    return AVBD_OK;
+}
+
+__global__ void k_total(const int *scan, const int *in, int n, long long *out)
+{
+    *out = (long long)scan[n - 1] + (long long)in[n - 1];
+}
+__global__ void k_u8_to_int(const unsigned char *in, int *out, int n)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n)
+        out[k] = in[k];
+}
+
+// Per-body force lists (CSR) sorted newest first.
+int build_adjacency(AvbdContext *ctx)
+{
+    int n = ctx->n;
+    CHECK(reserve(ctx, ctx->adjStart, (size_t)n + 1, false));
+    long long T = 2ll * (ctx->nMan + ctx->nJoint + ctx->nSpring + ctx->nIgnore);
+    if (T == 0)
+    {
+        CU(cudaMemsetAsync(ctx->adjStart.p, 0, sizeof(int) * ((size_t)n + 1), ctx->stream));
+        return AVBD_OK;
+    }
+    if (T > (long long)ADJ_INDEX_MASK)
+        return fail(ctx, AVBD_ERR_CAPACITY, "too many force incidences (%lld)", T);
+    CHECK(reserve(ctx, ctx->incKeys, T, false));
+    CHECK(reserve(ctx, ctx->incKeysAlt, T, false));
+    CHECK(reserve(ctx, ctx->incVals, T, false));
+    CHECK(reserve(ctx, ctx->incValsAlt, T, false));
+    CHECK(reserve(ctx, ctx->adj, T, false));
+    DevForces F = dev_forces(ctx);
+    k_incidences<<<grid_for(T, 256), 256, 0, ctx->stream>>>(F, ctx->incKeys.p, ctx->incVals.p);
+    LAUNCHED();
+    cub::DoubleBuffer<unsigned long long> dk(ctx->incKeys.p, ctx->incKeysAlt.p);
+    cub::DoubleBuffer<unsigned> dv(ctx->incVals.p, ctx->incValsAlt.p);
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, dk, dv, (int)T, 0, 64, ctx->stream);
+    CHECK(ensure_temp(ctx, bytes));
+    CU(cub::DeviceRadixSort::SortPairs(ctx->cubTemp.p, bytes, dk, dv, (int)T, 0, 64, ctx->stream));
+    ctx->launches++;
+    k_segment_starts<<<grid_for(T, 256), 256, 0, ctx->stream>>>(dk.Current(), (int)T, KEY_BODY_SHIFT, n,
+                                                                  ctx->adjStart.p);
+    LAUNCHED();
+    k_copy_adj<<<grid_for(T, 256), 256, 0, ctx->stream>>>(dv.Current(), ctx->adj.p, (int)T);
+    LAUNCHED();
+    return AVBD_OK;
+}
+
+// Broadphase: appends new manifolds after the existing ones.
+int broadphase(AvbdContext *ctx)
+{
+    int n = ctx->n;
+    if (n < 2)
+        return AVBD_OK;
+    DevBodies B = dev_bodies(ctx);
+    float dt = ctx->params.dt;
+    StepCounters *cnt = ctx->counters.p;
+    int M0 = ctx->nMan;
+    long long P1 = 0, P2 = 0;
+    const int mode = ctx->params.broadphase;
+    if (mode == AVBD_BROADPHASE_ALL_PAIRS)
+    {
+        CHECK(reserve(ctx, ctx->pairCount, n, false));
+        CHECK(reserve(ctx, ctx->pairOffset, n, false));
+        DevForces F = dev_forces(ctx);
+        k_bp_all_pairs<false><<<grid_for(n, 128), 128, 0, ctx->stream>>>(B, F, n, ctx->pairCount.p, nullptr, 0, 0,
+                                                                          cnt);
+        LAUNCHED();
+        CHECK(scan_counts(ctx, ctx->pairCount.p, ctx->pairOffset.p, n, 0));
+        k_total<<<1, 1, 0, ctx->stream>>>(ctx->pairOffset.p, ctx->pairCount.p, n, ctx->hScalars);
+        LAUNCHED();
+        CU(cudaStreamSynchronize(ctx->stream));
+        P1 = ctx->hScalars[0];
+        if (P1 > 0)
+        {
+            CHECK(reserve_manifolds(ctx, ctx->man[ctx->cur], (size_t)(M0 + P1), (size_t)M0));
+            DevForces F2 = dev_forces(ctx);
+            k_bp_all_pairs<true><<<grid_for(n, 128), 128, 0, ctx->stream>>>(B, F2, n, nullptr, ctx->pairOffset.p, M0,
+                                                                             (unsigned long long)ctx->nextSeq, cnt);
+            LAUNCHED();
+        }
+    }
+    else
+    {
+        if (mode != AVBD_BROADPHASE_GRID)
+            return fail(ctx, AVBD_ERR_ARGUMENT, "broadphase mode %d is not implemented on the GPU", mode);
+        int nB = (int)ctx->hBinned.size(), nL = (int)ctx->hLarge.size();
+        int nChunks = (nL + LL_CHUNK - 1) / LL_CHUNK;
+        long long nLL = (long long)nL * nChunks;
+        if (nL)
+        {
+            k_bp_large<<<grid_for(nL, 64), 64, 0, ctx->stream>>>(B, ctx->large.p, nL, dt, ctx->largeLo.p,
+                                                                  ctx->largeHi.p, ctx->largeSphere.p);
+            LAUNCHED();
+        }
+        cub::DoubleBuffer<unsigned long long> dk(ctx->bpKeys.p, ctx->bpKeysAlt.p);
+        ctx->hScalars[0] = 0;
+        ctx->hScalars[1] = 0;
+        DevForces F = dev_forces(ctx);
+        if (nB)
+        {
+            k_bp_bounds_init<<<1, 32, 0, ctx->stream>>>(ctx->bounds.p);
+            LAUNCHED();
+            k_bp_bounds<<<std::min(grid_for(nB, 256), 148 * 4), 256, 0, ctx->stream>>>(B, ctx->binned.p, nB,
+                                                                                          ctx->bounds.p);
+            LAUNCHED();
+            k_bp_params<<<1, 1, 0, ctx->stream>>>(ctx->bounds.p, ctx->binnedRadius, ctx->grid.p, cnt);
+            LAUNCHED();
+            k_bp_keys<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(B, ctx->binned.p, nB, ctx->grid.p,
+                                                                    ctx->bpKeys.p);
+            LAUNCHED();
+            size_t bytes = 0;
+            cub::DeviceRadixSort::SortKeys(nullptr, bytes, dk, nB, 0, 64, ctx->stream);
+            CHECK(ensure_temp(ctx, bytes));
+            CU(cub::DeviceRadixSort::SortKeys(ctx->cubTemp.p, bytes, dk, nB, 0, 64, ctx->stream));
+            ctx->launches++;
+            k_bp_cell_start<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(dk.Current(), nB, ctx->cellStart.p, 1);
+            LAUNCHED();
+            k_bp_pairs<false><<<grid_for(nB, 128), 128, 0, ctx->stream>>>(
+                B, F, dk.Current(), nB, ctx->cellStart.p, ctx->grid.p, ctx->large.p, nL, ctx->largeLo.p,
+                ctx->largeHi.p, dt, ctx->pairCount.p, nullptr, 0, 0, cnt);
+            LAUNCHED();
+            CHECK(scan_counts(ctx, ctx->pairCount.p, ctx->pairOffset.p, nB, 0));
+            ctx->launches++;
+            k_total<<<1, 1, 0, ctx->stream>>>(ctx->pairOffset.p, ctx->pairCount.p, nB, ctx->hScalars);
+            LAUNCHED();
+        }
+        if (nL > 1)
+        {
+            CHECK(reserve(ctx, ctx->llCount, (size_t)nLL, false));
+            CHECK(reserve(ctx, ctx->llOffset, (size_t)nLL, false));
+            k_bp_large_large<false><<<grid_for(nLL, 128), 128, 0, ctx->stream>>>(
+                F, ctx->large.p, ctx->largeSphere.p, nL, nChunks, ctx->llCount.p, nullptr, 0, 0, cnt);
+            LAUNCHED();
+            CHECK(scan_counts(ctx, ctx->llCount.p, ctx->llOffset.p, (int)nLL, 0));
+            ctx->launches++;
+            k_total<<<1, 1, 0, ctx->stream>>>(ctx->llOffset.p, ctx->llCount.p, (int)nLL, ctx->hScalars + 1);
+            LAUNCHED();
+        }
+        CU(cudaMemcpyAsync(ctx->hCounters, cnt, sizeof(StepCounters), cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+        if (ctx->hCounters->error)
+            return fail(ctx, AVBD_ERR_CAPACITY, "broadphase grid exceeds the cell cap");
+        P1 = ctx->hScalars[0];
+        P2 = ctx->hScalars[1];
+        if (P1 + P2 > 0)
+            CHECK(reserve_manifolds(ctx, ctx->man[ctx->cur], (size_t)(M0 + P1 + P2), (size_t)M0));
+        F = dev_forces(ctx);
+        if (P1 > 0)
+        {
+            k_bp_pairs<true><<<grid_for(nB, 128), 128, 0, ctx->stream>>>(
+                B, F, dk.Current(), nB, ctx->cellStart.p, ctx->grid.p, ctx->large.p, nL, ctx->largeLo.p,
+                ctx->largeHi.p, dt, nullptr, ctx->pairOffset.p, M0, (unsigned long long)ctx->nextSeq, cnt);
+            LAUNCHED();
+        }
+        if (P2 > 0)
+        {
+            k_bp_large_large<true><<<grid_for(nLL, 128), 128, 0, ctx->stream>>>(
+                F, ctx->large.p, ctx->largeSphere.p, nL, nChunks, nullptr, ctx->llOffset.p, (int)(M0 + P1),
+                (unsigned long long)(ctx->nextSeq + P1), cnt);
+            LAUNCHED();
+        }
+        if (nB)
+        {
+            k_bp_cell_start<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(dk.Current(), nB, ctx->cellStart.p, 0);
+            LAUNCHED();
+        }
+    }
+    ctx->stats.manifolds_created = P1 + P2;
+    ctx->nMan = (int)(M0 + P1 + P2);
+    ctx->nextSeq += P1 + P2;
+    return AVBD_OK;
+}
+
+int init_forces(AvbdContext *ctx)
+{
+    DevBodies B = dev_bodies(ctx);
+    Params P = dev_params(ctx->params);
+    int M = ctx->nMan, J = ctx->nJoint;
+    int need = std::max(M, J);
+    CHECK(reserve(ctx, ctx->keep, (size_t)std::max(need, 1), false));
+    CHECK(reserve(ctx, ctx->keepIdx, (size_t)std::max(need, 1) * 2, false));
+    long long newM = 0, newJ = J;
+    int *idx = ctx->keepIdx.p;
+    int *cnt32 = ctx->keepIdx.p + std::max(need, 1);
+    if (M)
+    {
+        DevManifolds Md = dev_man(ctx->man[ctx->cur]);
+        k_manifold_init<<<grid_for(M, 128), 128, 0, ctx->stream>>>(B, Md, M, P, ctx->keep.p);
+        LAUNCHED();
+        k_u8_to_int<<<grid_for(M, 256), 256, 0, ctx->stream>>>(ctx->keep.p, cnt32, M);
+        LAUNCHED();
+        CHECK(scan_counts(ctx, cnt32, idx, M, 0));
+        ctx->launches++;
+        k_total<<<1, 1, 0, ctx->stream>>>(idx, cnt32, M, ctx->hScalars);
+        LAUNCHED();
+        CU(cudaStreamSynchronize(ctx->stream));
+        newM = ctx->hScalars[0];
+        ManBuf &dst = ctx->man[ctx->cur ^ 1];
+        CHECK(reserve_manifolds(ctx, dst, (size_t)std::max<long long>(newM, 1), 0));
+        k_manifold_compact<<<grid_for(M, 128), 128, 0, ctx->stream>>>(Md, dev_man(dst), M, ctx->keep.p, idx);
+        LAUNCHED();
+        ctx->cur ^= 1;
+        ctx->nMan = (int)newM;
+    }
+    if (J)
+    {
+        DevForces F = dev_forces(ctx);
+        k_joint_init<<<grid_for(J, 128), 128, 0, ctx->stream>>>(B, F, P, ctx->keep.p);
+        LAUNCHED();
+        k_u8_to_int<<<grid_for(J, 256), 256, 0, ctx->stream>>>(ctx->keep.p, cnt32, J);
+        LAUNCHED();
+        CHECK(scan_counts(ctx, cnt32, idx, J, 0));
+        ctx->launches++;
+        k_total<<<1, 1, 0, ctx->stream>>>(idx, cnt32, J, ctx->hScalars + 1);
+        LAUNCHED();
+        CU(cudaStreamSynchronize(ctx->stream));
+        newJ = ctx->hScalars[1];
+        if (newJ != J)
+        {
+            int o = ctx->jcur ^ 1;
+            CHECK(reserve(ctx, ctx->jointAB[o], (size_t)std::max<long long>(newJ, 1), false));
+            CHECK(reserve(ctx, ctx->jointSeq[o], (size_t)std::max<long long>(newJ, 1), false));
+            CHECK(reserve(ctx, ctx->joint[o], 8 * (size_t)std::max<long long>(newJ, 1), false));
+            k_joint_compact<<<grid_for(J, 128), 128, 0, ctx->stream>>>(
+                J, ctx->keep.p, idx, ctx->jointAB[ctx->jcur].p, ctx->jointSeq[ctx->jcur].p, ctx->joint[ctx->jcur].p,
+                ctx->jointAB[o].p, ctx->jointSeq[o].p, ctx->joint[o].p);
+            LAUNCHED();
+            ctx->jcur = o;
+            ctx->nJoint = (int)newJ;
+        }
+    }
+    return AVBD_OK;
+}
+
+int colour_bodies(AvbdContext *ctx)
+{
+    int n = ctx->n;
+    DevBodies B = dev_bodies(ctx);
+    CHECK(reserve(ctx, ctx->colourState, n, false));
+    CHECK(reserve(ctx, ctx->colour, n, false));
+    CHECK(reserve(ctx, ctx->solveList, n, false));
+    CHECK(reserve(ctx, ctx->colKeys, n, false));
+    CHECK(reserve(ctx, ctx->colKeysAlt, n, false));
+    CHECK(reserve(ctx, ctx->remaining, 2, false));
+    CU(cudaMemsetAsync(ctx->remaining.p, 0, sizeof(int) * 2, ctx->stream));
+    k_colour_init<<<grid_for(n, 256), 256, 0, ctx->stream>>>(B, ctx->adjStart.p, ctx->colourState.p,
+                                                               ctx->remaining.p);
+    LAUNCHED();
+    CU(cudaMemcpyAsync(ctx->remaining.p + 1, ctx->remaining.p, sizeof(int), cudaMemcpyDeviceToDevice, ctx->stream));
+    DevForces F = dev_forces(ctx);
+    int rounds = 0;
+    int *hRem = (int *)(ctx->hScalars + 2);
+    const int batch = 4;
+    for (;;)
+    {
+        for (int k = 0; k < batch; ++k)
+        {
+            k_colour_round<<<grid_for(n, 256), 256, 0, ctx->stream>>>(F, n, rounds, ctx->colourState.p,
+                                                                        ctx->remaining.p, ctx->counters.p);
+            LAUNCHED();
+            rounds++;
+        }
+        CU(cudaMemcpyAsync(hRem, ctx->remaining.p, sizeof(int) * 2, cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+        if (hRem[0] == 0)
+            break;
+        if (rounds > 60000)
+            return fail(ctx, AVBD_ERR_STATE, "colouring did not converge");
+    }
+    int nVert = hRem[1];
+    CU(cudaMemcpyAsync(ctx->hCounters, ctx->counters.p, sizeof(StepCounters), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    if (ctx->hCounters->error == DERR_TOO_MANY_COLOURS)
+        return fail(ctx, AVBD_ERR_CAPACITY, "constraint graph needs more than 256 colours");
+    int C = nVert > 0 ? ctx->hCounters->maxColour + 1 : 0;
+    ctx->nColours = C;
+    ctx->nSolve = nVert;
+    ctx->stats.colour_rounds = rounds;
+    k_colour_keys<<<grid_for(n, 256), 256, 0, ctx->stream>>>(ctx->colourState.p, n, ctx->colour.p, ctx->colKeys.p);
+    LAUNCHED();
+    ctx->hColourStart.assign((size_t)C + 1, 0);
+    if (nVert > 0)
+    {
+        cub::DoubleBuffer<unsigned long long> dk(ctx->colKeys.p, ctx->colKeysAlt.p);
+        size_t bytes = 0;
+        cub::DeviceRadixSort::SortKeys(nullptr, bytes, dk, n, 0, 64, ctx->stream);
+        CHECK(ensure_temp(ctx, bytes));
+        CU(cub::DeviceRadixSort::SortKeys(ctx->cubTemp.p, bytes, dk, n, 0, 64, ctx->stream));
+        ctx->launches++;
+        k_solve_list<<<grid_for(nVert, 256), 256, 0, ctx->stream>>>(dk.Current(), nVert, ctx->solveList.p);
+        LAUNCHED();
+        CHECK(reserve(ctx, ctx->colourStart, (size_t)C + 1, false));
+        k_segment_starts<<<grid_for(nVert, 256), 256, 0, ctx->stream>>>(dk.Current(), nVert, 32, C,
+                                                                          ctx->colourStart.p);
+        LAUNCHED();
+        CU(cudaMemcpyAsync(ctx->hColourStart.data(), ctx->colourStart.p, sizeof(int) * ((size_t)C + 1),
+                           cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+    }
+    return AVBD_OK;
+}
+
+int iterate(AvbdContext *ctx)
+{
+    DevBodies B = dev_bodies(ctx);
+    DevForces F = dev_forces(ctx);
+    Params P = dev_params(ctx->params);
+    constexpr int GPB = PRIMAL_BLOCK / PRIMAL_GROUP;
+    for (int it = 0; it < ctx->params.iterations; ++it)
+    {
+        for (int c = 0; c < ctx->nColours; ++c)
+        {
+            int first = ctx->hColourStart[c];
+            int count = ctx->hColourStart[c + 1] - first;
+            if (count <= 0)
+                continue;
+            PhaseScope ps(ctx, AVBD_PHASE_PRIMAL);
+            k_primal<PRIMAL_GROUP, PRIMAL_BLOCK><<<grid_for(count, GPB), PRIMAL_BLOCK, 0, ctx->stream>>>(
+                B, F, P, ctx->solveList.p, first, count);
+            LAUNCHED();
+        }
+        PhaseScope ps(ctx, AVBD_PHASE_DUAL);
+        if (ctx->nMan)
+        {
+            k_dual_contacts<<<grid_for(8ll * ctx->nMan, 256), 256, 0, ctx->stream>>>(B, F.man, ctx->nMan, P);
+            LAUNCHED();
+        }
+        if (ctx->nJoint)
+        {
+            k_dual_joints<<<grid_for(ctx->nJoint, 128), 128, 0, ctx->stream>>>(B, F, P);
+            LAUNCHED();
+        }
+    }
+    return AVBD_OK;
+}
+
+int step_once(AvbdContext *ctx)
+{
+    CU(cudaMemsetAsync(ctx->counters.p, 0, sizeof(StepCounters), ctx->stream));
+    {
+        PhaseScope ps(ctx, AVBD_PHASE_BROADPHASE);
+        CHECK(broadphase(ctx));
+    }
+    {
+        PhaseScope ps(ctx, AVBD_PHASE_FORCE_INIT);
+        CHECK(init_forces(ctx));
+    }
+    {
+        PhaseScope ps(ctx, AVBD_PHASE_ADJACENCY);
+        CHECK(build_adjacency(ctx));
+    }
+    DevBodies B = dev_bodies(ctx);
+    Params P = dev_params(ctx->params);
+    if (ctx->n)
+    {
+        PhaseScope ps(ctx, AVBD_PHASE_BODY_INIT);
+        k_warm_start<<<grid_for(ctx->n, 256), 256, 0, ctx->stream>>>(B, ctx->adjStart.p, P);
+        LAUNCHED();
+    }
+    {
+        PhaseScope ps(ctx, AVBD_PHASE_COLOURING);
+        CHECK(colour_bodies(ctx));
+    }
+    CHECK(iterate(ctx));
+    if (ctx->n)
+    {
+        PhaseScope ps(ctx, AVBD_PHASE_VELOCITY);
+        k_finish<<<grid_for(ctx->n, 256), 256, 0, ctx->stream>>>(B, P);
+        LAUNCHED();
+    }
+    ctx->stats.body_count = ctx->n;
+    ctx->stats.manifold_count = ctx->nMan;
+    ctx->stats.joint_count = ctx->nJoint;
+    ctx->stats.spring_count = ctx->nSpring;
+    ctx->stats.solved_bodies = ctx->nSolve;
+    ctx->stats.colours = ctx->nColours;
+    ctx->stats.pair_checks = (int64_t)ctx->hCounters->pairChecks;
+    ctx->stats.sphere_hits = (int64_t)ctx->hCounters->sphereHits;
+    ctx->stats.constrained_hits = (int64_t)ctx->hCounters->constrainedHits;
+    CHECK(prof_collect(ctx));
+    return AVBD_OK;
+}
+
+void pack3(std::vector<float4> &out, const float *src, int n, float w = 0.0f)
+{
+    out.resize(n);
+    for (int i = 0; i < n; ++i)
+        out[i] = make_float4(src ? src[3 * i] : 0.0f, src ? src[3 * i + 1] : 0.0f, src ? src[3 * i + 2] : 0.0f, w);
+}
+
+template <class T>
+int upload(AvbdContext *ctx, DArr<T> &a, const T *src, size_t count)
+{
+    CHECK(reserve(ctx, a, std::max<size_t>(count, 1), false));
+    if (count)
+        CU(cudaMemcpyAsync(a.p, src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+    return AVBD_OK;
+}
+
+int upload_bodies(AvbdContext *ctx, const AvbdBodies *b, bool props)
+{
+    int n = b->count;
+    std::vector<float4> tmp;
+    pack3(tmp, b->position3, n);
+    CHECK(upload(ctx, ctx->pos, tmp.data(), n));
+    tmp.resize(n);
+    for (int i = 0; i < n; ++i)
+        tmp[i] = b->orientation4 ? make_float4(b->orientation4[4 * i], b->orientation4[4 * i + 1],
+                                               b->orientation4[4 * i + 2], b->orientation4[4 * i + 3])
+                                 : make_float4(0, 0, 0, 1);
+    CHECK(upload(ctx, ctx->quat, tmp.data(), n));
+    pack3(tmp, b->velocity3, n);
+    CHECK(upload(ctx, ctx->vel, tmp.data(), n));
+    pack3(tmp, b->angular3, n);
+    CHECK(upload(ctx, ctx->angvel, tmp.data(), n));
+    pack3(tmp, b->prev_velocity3 ? b->prev_velocity3 : b->velocity3, n);
+    CHECK(upload(ctx, ctx->prevVel, tmp.data(), n));
+    if (props)
+    {
+        tmp.resize(n);
+        for (int i = 0; i < n; ++i)
+            tmp[i] = make_float4(b->mass[i], b->moment3[3 * i], b->moment3[3 * i + 1], b->moment3[3 * i + 2]);
+        CHECK(upload(ctx, ctx->massMoment, tmp.data(), n));
+        for (int i = 0; i < n; ++i)
+            tmp[i] = make_float4(b->size3[3 * i], b->size3[3 * i + 1], b->size3[3 * i + 2], b->radius[i]);
+        CHECK(upload(ctx, ctx->sizeRad, tmp.data(), n));
+        CHECK(upload(ctx, ctx->friction, b->friction, n));
+        for (DArr<float4> *a : {&ctx->initLin, &ctx->initAng, &ctx->inertLin, &ctx->inertAng})
+        {
+            CHECK(reserve(ctx, *a, std::max(n, 1), false));
+            CU(cudaMemsetAsync(a->p, 0, sizeof(float4) * std::max(n, 1), ctx->stream));
+        }
+    }
+    return AVBD_OK;
+}
+
+// Grid classification: bodies above the 95th-percentile bounding radius are "large"
+// (solver.cpp:297-329). Radii never change, so this is fixed per world.
+int classify_bodies(AvbdContext *ctx, const float *radius, int n)
+{
+    ctx->hBinned.clear();
+    ctx->hLarge.clear();
+    if (n >= 2)
+    {
+        std::vector<float> r(radius, radius + n);
+        size_t pct = std::min<size_t>((size_t)n - 1, (size_t)n * 95 / 100);
+        std::nth_element(r.begin(), r.begin() + pct, r.end());
+        ctx->binnedRadius = r[pct] > 1e-3f ? r[pct] : 1e-3f;
+        for (int i = 0; i < n; ++i)
+            (radius[i] > ctx->binnedRadius ? ctx->hLarge : ctx->hBinned).push_back(i);
+    }
+    int nB = (int)ctx->hBinned.size(), nL = (int)ctx->hLarge.size();
+    CHECK(upload(ctx, ctx->binned, ctx->hBinned.data(), nB));
+    CHECK(upload(ctx, ctx->large, ctx->hLarge.data(), nL));
+    CHECK(reserve(ctx, ctx->largeLo, std::max(nL, 1), false));
+    CHECK(reserve(ctx, ctx->largeHi, std::max(nL, 1), false));
+    CHECK(reserve(ctx, ctx->largeSphere, std::max(nL, 1), false));
+    CHECK(reserve(ctx, ctx->bpKeys, std::max(nB, 1), false));
+    CHECK(reserve(ctx, ctx->bpKeysAlt, std::max(nB, 1), false));
+    CHECK(reserve(ctx, ctx->pairCount, std::max(n, 1), false));
+    CHECK(reserve(ctx, ctx->pairOffset, std::max(n, 1), false));
+    return AVBD_OK;
+}
+
+} // namespace
+
+extern "C"
+{
+
+const char *avbd_backend_name(void) { return "CUDA AVBD (sm_100a)"; }
+
+int avbd_create(AvbdContext **out, int32_t device_ordinal, void *cuda_stream)
+{
+    if (!out)
+        return AVBD_ERR_ARGUMENT;
+    *out = nullptr;
+    AvbdContext *ctx = new AvbdContext();
+    ctx->device = device_ordinal;
+    cudaError_t e = cudaSetDevice(device_ordinal);
+    if (e != cudaSuccess)
+    {
+        delete ctx;
+        return AVBD_ERR_CUDA;
+    }
+    if (cuda_stream)
+        ctx->stream = (cudaStream_t)cuda_stream;
+    else
+    {
+        if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
+        {
+            delete ctx;
+            return AVBD_ERR_CUDA;
+        }
+        ctx->ownStream = true;
+    }
+    if (cudaMallocHost((void **)&ctx->hCounters, sizeof(StepCounters)) != cudaSuccess ||
+        cudaMallocHost((void **)&ctx->hScalars, sizeof(long long) * 16) != cudaSuccess ||
+        cudaEventCreate(&ctx->evStart) != cudaSuccess || cudaEventCreate(&ctx->evStop) != cudaSuccess)
+    {
+        avbd_destroy(ctx);
+        return AVBD_ERR_CUDA;
+    }
+    memset(ctx->hCounters, 0, sizeof(StepCounters));
+    if (reserve(ctx, ctx->counters, 1, false) || reserve(ctx, ctx->bounds, 8, false) ||
+        reserve(ctx, ctx->grid, 1, false) || reserve(ctx, ctx->cellStart, CELL_TABLE, false))
+    {
+        avbd_destroy(ctx);
+        return AVBD_ERR_CUDA;
+    }
+    cudaMemsetAsync(ctx->cellStart.p, 0xFF, sizeof(unsigned) * CELL_TABLE, ctx->stream);
+    ctx->params.dt = 1.0f / 60.0f;
+    ctx->params.gravity = -10.0f;
+    ctx->params.iterations = 10;
+    ctx->params.alpha = 0.99f;
+    ctx->params.betaLin = 10000.0f;
+    ctx->params.betaAng = 100.0f;
+    ctx->params.gamma = 0.999f;
+    ctx->params.broadphase = AVBD_BROADPHASE_GRID;
+    *out = ctx;
+    return AVBD_OK;
+}
+
+void avbd_destroy(AvbdContext *ctx)
+{
+    if (!ctx)
+        return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream)
+        cudaStreamSynchronize(ctx->stream);
+    for (DArr<float4> *a : {&ctx->pos, &ctx->quat, &ctx->initLin, &ctx->initAng, &ctx->inertLin, &ctx->inertAng,
+                            &ctx->vel, &ctx->angvel, &ctx->prevVel, &ctx->massMoment, &ctx->sizeRad, &ctx->largeLo,
+                            &ctx->largeHi, &ctx->largeSphere, &ctx->spring, &ctx->joint[0], &ctx->joint[1]})
+        release(*a);
+    release(ctx->friction);
+    release(ctx->binned);
+    release(ctx->large);
+    release(ctx->bounds);
+    release(ctx->grid);
+    release(ctx->cellStart);
+    release(ctx->bpKeys);
+    release(ctx->bpKeysAlt);
+    release(ctx->pairCount);
+    release(ctx->pairOffset);
+    release(ctx->llCount);
+    release(ctx->llOffset);
+    for (cudaEvent_t e : ctx->evPool)
+        cudaEventDestroy(e);
+    for (ManBuf &m : ctx->man)
+    {
+        release(m.ab);
+        release(m.seq);
+        release(m.n);
+        release(m.basis);
+        release(m.contact);
+    }
+    release(ctx->keep);
+    release(ctx->keepIdx);
+    for (int k = 0; k < 2; ++k)
+    {
+        release(ctx->jointAB[k]);
+        release(ctx->jointSeq[k]);
+    }
+    release(ctx->springAB);
+    release(ctx->springSeq);
+    release(ctx->ignoreAB);
+    release(ctx->ignoreSeq);
+    release(ctx->adjStart);
+    release(ctx->adj);
+    release(ctx->incVals);
+    release(ctx->incValsAlt);
+    release(ctx->incKeys);
+    release(ctx->incKeysAlt);
+    release(ctx->colourState);
+    release(ctx->colour);
+    release(ctx->solveList);
+    release(ctx->colourStart);
+    release(ctx->remaining);
+    release(ctx->colKeys);
+    release(ctx->colKeysAlt);
+    release(ctx->cubTemp);
+    release(ctx->counters);
+    if (ctx->hCounters)
+        cudaFreeHost(ctx->hCounters);
+    if (ctx->hScalars)
+        cudaFreeHost(ctx->hScalars);
+    if (ctx->evStart)
+        cudaEventDestroy(ctx->evStart);
+    if (ctx->evStop)
+        cudaEventDestroy(ctx->evStop);
+    if (ctx->ownStream && ctx->stream)
+        cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char *avbd_last_error(const AvbdContext *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+void avbd_clear_error(AvbdContext *ctx)
+{
+    if (ctx)
+    {
+        ctx->err.clear();
+        ctx->errCode = 0;
+    }
+}
+
+int avbd_set_params(AvbdContext *ctx, const AvbdParams *params)
+{
+    if (!ctx || !params)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
+    if (!(params->dt > 0.0f) || params->iterations < 0)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "invalid dt or iteration count");
+    if (params->broadphase != AVBD_BROADPHASE_GRID && params->broadphase != AVBD_BROADPHASE_ALL_PAIRS)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "broadphase mode %d is not available on the GPU", params->broadphase);
+    ctx->params = *params;
+    return AVBD_OK;
+}
+
+int avbd_load_world(AvbdContext *ctx, const AvbdBodies *bodies, const AvbdJoints *joints, const AvbdSprings *springs,
+                    const AvbdIgnores *ignores, const AvbdManifolds *manifolds, int64_t next_seq)
+{
+    if (!ctx || !bodies)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
+    if (ctx->errCode)
+        return AVBD_ERR_LATCHED;
+    int n = bodies->count;
+    if (n < 0 || n >= (int)KEY_NO_BODY)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "body count %d out of range", n);
+    if (n > 0 && (!bodies->position3 || !bodies->size3 || !bodies->mass || !bodies->moment3 ||
+                  !bodies->friction || !bodies->radius || !bodies->velocity3))
+        return fail(ctx, AVBD_ERR_ARGUMENT, "missing body arrays");
+    CU(cudaSetDevice(ctx->device));
+    ctx->n = n;
+    CHECK(upload_bodies(ctx, bodies, true));
+    CHECK(classify_bodies(ctx, bodies->radius, n));
+
+    auto check_ab = [&](const int32_t *ab, int count, bool allowWorldA) -> bool {
+        for (int i = 0; i < count; ++i)
+        {
+            int a = ab[2 * i], b = ab[2 * i + 1];
+            if (b < 0 || b >= n || a >= n || (a < 0 && !(allowWorldA && a == -1)) || a == b)
+                return false;
+        }
+        return true;
+    };
+    auto seqs = [&](const int64_t *s, int count, std::vector<unsigned long long> &out) {
+        out.resize(count);
+        for (int i = 0; i < count; ++i)
+            out[i] = (unsigned long long)s[i];
+    };
+    std::vector<unsigned long long> sq;
+    // joints
+    int J = joints ? joints->count : 0;
+    if (J && (!joints->body_ab2 || !joints->seq || !joints->state28 || !check_ab(joints->body_ab2, J, true)))
+        return fail(ctx, AVBD_ERR_ARGUMENT, "invalid joint arrays");
+    {
+        std::vector<float4> d((size_t)8 * J);
+        for (int j = 0; j < J; ++j)
+        {
+            const float *s = joints->state28 + 28 * (size_t)j;
+            float broken = joints->broken && joints->broken[j] ? 1.0f : 0.0f;
+            d[8 * j + 0] = make_float4(s[0], s[1], s[2], s[24]);
+            d[8 * j + 1] = make_float4(s[3], s[4], s[5], s[25]);
+            d[8 * j + 2] = make_float4(s[6], s[7], s[8], s[26]);
+            d[8 * j + 3] = make_float4(s[9], s[10], s[11], s[27]);
+            d[8 * j + 4] = make_float4(s[12], s[13], s[14], broken);
+            d[8 * j + 5] = make_float4(s[15], s[16], s[17], 0.0f);
+            d[8 * j + 6] = make_float4(s[18], s[19], s[20], 0.0f);
+            d[8 * j + 7] = make_float4(s[21], s[22], s[23], 0.0f);
+        }
+        ctx->jcur = 0;
+        CHECK(upload(ctx, ctx->joint[0], d.data(), d.size()));
+        CHECK(upload(ctx, ctx->jointAB[0], (const int2 *)(J ? joints->body_ab2 : nullptr), J));
+        if (J)
+            seqs(joints->seq, J, sq);
+        CHECK(upload(ctx, ctx->jointSeq[0], sq.data(), J));
+        ctx->nJoint = J;
+    }
+    int S = springs ? springs->count : 0;
+    if (S && (!springs->body_ab2 || !springs->seq || !springs->state8 || !check_ab(springs->body_ab2, S, false)))
+        return fail(ctx, AVBD_ERR_ARGUMENT, "invalid spring arrays");
+    {
+        std::vector<float4> d((size_t)2 * S);
+        for (int s = 0; s < S; ++s)
+        {
+            const float *v = springs->state8 + 8 * (size_t)s;
+            d[2 * s] = make_float4(v[0], v[1], v[2], v[6]);
+            d[2 * s + 1] = make_float4(v[3], v[4], v[5], v[7]);
+        }
+        CHECK(upload(ctx, ctx->spring, d.data(), d.size()));
+        CHECK(upload(ctx, ctx->springAB, (const int2 *)(S ? springs->body_ab2 : nullptr), S));
+        if (S)
+            seqs(springs->seq, S, sq);
+        CHECK(upload(ctx, ctx->springSeq, sq.data(), S));
+        ctx->nSpring = S;
+    }
+    int I = ignores ? ignores->count : 0;
+    if (I && (!ignores->body_ab2 || !ignores->seq || !check_ab(ignores->body_ab2, I, false)))
+        return fail(ctx, AVBD_ERR_ARGUMENT, "invalid ignore-collision arrays");
+    CHECK(upload(ctx, ctx->ignoreAB, (const int2 *)(I ? ignores->body_ab2 : nullptr), I));
+    if (I)
+        seqs(ignores->seq, I, sq);
+    CHECK(upload(ctx, ctx->ignoreSeq, sq.data(), I));
+    ctx->nIgnore = I;
+
+    int M = manifolds ? manifolds->count : 0;
+    if (M && (!manifolds->body_ab2 || !manifolds->seq || !manifolds->num_contacts ||
+              !check_ab(manifolds->body_ab2, M, false)))
+        return fail(ctx, AVBD_ERR_ARGUMENT, "invalid manifold arrays");
+    ctx->cur = 0;
+    CHECK(reserve_manifolds(ctx, ctx->man[0], (size_t)std::max(M, 1), 0));
+    if (M)
+    {
+        std::vector<float4> basis((size_t)3 * M), contact((size_t)32 * M);
+        std::vector<int> nc(M);
+        for (int m = 0; m < M; ++m)
+        {
+            nc[m] = std::min(std::max(manifolds->num_contacts[m], 0), 8);
+            const float *bs = manifolds->basis9 ? manifolds->basis9 + 9 * (size_t)m : nullptr;
+            float fr = manifolds->friction ? manifolds->friction[m] : 0.0f;
+            for (int r = 0; r < 3; ++r)
+                basis[3 * m + r] = bs ? make_float4(bs[3 * r], bs[3 * r + 1], bs[3 * r + 2], r == 0 ? fr : 0.0f)
+                                      : make_float4(0, 0, 0, 0);
+            for (int k = 0; k < 8; ++k)
+            {
+                const float *c = manifolds->contact15x8 ? manifolds->contact15x8 + ((size_t)8 * m + k) * 15 : nullptr;
+                float v[15] = {0};
+                if (c)
+                    memcpy(v, c, sizeof(v));
+                unsigned key = manifolds->keys8 ? (unsigned)manifolds->keys8[8 * m + k] & 0x7FFFFFFFu : 0u;
+                unsigned stick = manifolds->stick8 && manifolds->stick8[8 * m + k] ? 0x80000000u : 0u;
+                float4 *o = &contact[(size_t)32 * m + 4 * k];
+                o[0] = make_float4(v[0], v[1], v[2], v[3]);
+                o[1] = make_float4(v[4], v[5], v[6], v[7]);
+                o[2] = make_float4(v[8], v[9], v[10], v[11]);
+                unsigned bits = key | stick;
+                float w;
+                memcpy(&w, &bits, 4);
+                o[3] = make_float4(v[12], v[13], v[14], w);
+            }
+        }
+        CU(cudaMemcpyAsync(ctx->man[0].ab.p, manifolds->body_ab2, sizeof(int2) * M, cudaMemcpyHostToDevice,
+                           ctx->stream));
+        seqs(manifolds->seq, M, sq);
+        CU(cudaMemcpyAsync(ctx->man[0].seq.p, sq.data(), sizeof(unsigned long long) * M, cudaMemcpyHostToDevice,
+                           ctx->stream));
+        CU(cudaMemcpyAsync(ctx->man[0].n.p, nc.data(), sizeof(int) * M, cudaMemcpyHostToDevice, ctx->stream));
+        CU(cudaMemcpyAsync(ctx->man[0].basis.p, basis.data(), sizeof(float4) * 3 * M, cudaMemcpyHostToDevice,
+                           ctx->stream));
+        CU(cudaMemcpyAsync(ctx->man[0].contact.p, contact.data(), sizeof(float4) * 32 * M, cudaMemcpyHostToDevice,
+                           ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+    }
+    ctx->nMan = M;
+    ctx->nextSeq = next_seq;
+    CHECK(build_adjacency(ctx));
+    CU(cudaStreamSynchronize(ctx->stream));
+    ctx->nColours = 0;
+    ctx->nSolve = 0;
+    ctx->loaded = true;
+    return AVBD_OK;
+}
+
+int avbd_write_bodies(AvbdContext *ctx, const AvbdBodies *bodies)
+{
+    if (!ctx || !bodies)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
+    if (!ctx->loaded || bodies->count != ctx->n)
+        return fail(ctx, AVBD_ERR_STATE, "body count does not match the loaded world");
+    CU(cudaSetDevice(ctx->device));
+    CHECK(upload_bodies(ctx, bodies, false));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return AVBD_OK;
+}
+
+int avbd_step(AvbdContext *ctx, int32_t nsteps)
+{
+    if (!ctx)
+        return AVBD_ERR_ARGUMENT;
+    if (ctx->errCode)
+        return AVBD_ERR_LATCHED;
+    if (!ctx->loaded)
+        return fail(ctx, AVBD_ERR_STATE, "no world loaded");
+    CU(cudaSetDevice(ctx->device));
+    for (int s = 0; s < nsteps; ++s)
+        CHECK(step_once(ctx));
+    return AVBD_OK;
+}
+
+int avbd_synchronize(AvbdContext *ctx)
+{
+    if (!ctx)
+        return AVBD_ERR_ARGUMENT;
+    CU(cudaStreamSynchronize(ctx->stream));
+    return AVBD_OK;
+}
+
+int avbd_read_bodies(AvbdContext *ctx, const AvbdBodyState *out)
+{
+    if (!ctx || !out)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
+    int n = ctx->n;
+    std::vector<float4> tmp(n);
+    struct Field
+    {
+        DArr<float4> *src;
+        float *dst;
+        int width;
+    } fields[] = {{&ctx->pos, out->position3, 3},
+                  {&ctx->quat, out->orientation4, 4},
+                  {&ctx->vel, out->velocity3, 3},
+                  {&ctx->angvel, out->angular3, 3},
+                  {&ctx->prevVel, out->prev_velocity3, 3},
+                  {&ctx->initLin, out->initial_position3, 3},
+                  {&ctx->initAng, out->initial_orientation4, 4},
+                  {&ctx->inertLin, out->inertial_position3, 3},
+                  {&ctx->inertAng, out->inertial_orientation4, 4}};
+    for (const Field &f : fields)
+    {
+        if (!f.dst || !n)
+            continue;
+        CU(cudaMemcpyAsync(tmp.data(), f.src->p, sizeof(float4) * n, cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+        for (int i = 0; i < n; ++i)
+        {
+            f.dst[f.width * i] = tmp[i].x;
+            f.dst[f.width * i + 1] = tmp[i].y;
+            f.dst[f.width * i + 2] = tmp[i].z;
+            if (f.width == 4)
+                f.dst[4 * i + 3] = tmp[i].w;
+        }
+    }
+    return AVBD_OK;
+}
+
+int avbd_num_manifolds(AvbdContext *ctx, int32_t *count)
+{
+    if (!ctx || !count)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
+    *count = ctx->nMan;
+    return AVBD_OK;
+}
+
+int avbd_read_manifolds(AvbdContext *ctx, const AvbdManifoldsOut *out)
+{
+    if (!ctx || !out)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
+    int M = ctx->nMan;
+    if (!M)
+        return AVBD_OK;
+    ManBuf &b = ctx->man[ctx->cur];
+    std::vector<int2> ab(M);
+    std::vector<unsigned long long> seq(M);
+    std::vector<int> nc(M);
+    std::vector<float4> basis((size_t)3 * M), contact((size_t)32 * M);
+    CU(cudaMemcpyAsync(ab.data(), b.ab.p, sizeof(int2) * M, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaMemcpyAsync(seq.data(), b.seq.p, sizeof(unsigned long long) * M, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaMemcpyAsync(nc.data(), b.n.p, sizeof(int) * M, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaMemcpyAsync(basis.data(), b.basis.p, sizeof(float4) * 3 * M, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaMemcpyAsync(contact.data(), b.contact.p, sizeof(float4) * 32 * M, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    for (int m = 0; m < M; ++m)
+    {
+        if (out->body_ab2)
+        {
+            out->body_ab2[2 * m] = ab[m].x;
+            out->body_ab2[2 * m + 1] = ab[m].y;
+        }
+        if (out->seq)
+            out->seq[m] = (int64_t)seq[m];
+        if (out->num_contacts)
+            out->num_contacts[m] = nc[m];
+        if (out->basis9)
+            for (int r = 0; r < 3; ++r)
+            {
+                out->basis9[9 * m + 3 * r] = basis[3 * m + r].x;
+                out->basis9[9 * m + 3 * r + 1] = basis[3 * m + r].y;
+                out->basis9[9 * m + 3 * r + 2] = basis[3 * m + r].z;
+            }
+        if (out->friction)
+            out->friction[m] = basis[3 * m].w;
+        for (int k = 0; k < 8; ++k)
+        {
+            bool live = k < nc[m];
+            const float4 *c = &contact[(size_t)32 * m + 4 * k];
+            unsigned bits;
+            memcpy(&bits, &c[3].w, 4);
+            if (out->keys8)
+                out->keys8[8 * m + k] = live ? (int)(bits & 0x7FFFFFFFu) : 0;
+            if (out->stick8)
+                out->stick8[8 * m + k] = live ? (int)(bits >> 31) : 0;
+            if (out->contact15x8)
+            {
+                float *o = out->contact15x8 + ((size_t)8 * m + k) * 15;
+                float v[16] = {c[0].x, c[0].y, c[0].z, c[0].w, c[1].x, c[1].y, c[1].z, c[1].w,
+                               c[2].x, c[2].y, c[2].z, c[2].w, c[3].x, c[3].y, c[3].z, 0.0f};
+                for (int q = 0; q < 15; ++q)
+                    o[q] = live ? v[q] : 0.0f;
+            }
+        }
+    }
+    return AVBD_OK;
+}
+
+int avbd_num_joints(AvbdContext *ctx, int32_t *count)
+{
+    if (!ctx || !count)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
+    *count = ctx->nJoint;
+    return AVBD_OK;
+}
+
+int avbd_read_joints(AvbdContext *ctx, const AvbdJointsOut *out)
+{
+    if (!ctx || !out)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
+    int J = ctx->nJoint;
+    if (!J)
+        return AVBD_OK;
+    std::vector<int2> ab(J);
+    std::vector<unsigned long long> seq(J);
+    std::vector<float4> d((size_t)8 * J);
+    CU(cudaMemcpyAsync(ab.data(), ctx->jointAB[ctx->jcur].p, sizeof(int2) * J, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaMemcpyAsync(seq.data(), ctx->jointSeq[ctx->jcur].p, sizeof(unsigned long long) * J,
+                       cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaMemcpyAsync(d.data(), ctx->joint[ctx->jcur].p, sizeof(float4) * 8 * J, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    for (int j = 0; j < J; ++j)
+    {
+        if (out->body_ab2)
+        {
+            out->body_ab2[2 * j] = ab[j].x;
+            out->body_ab2[2 * j + 1] = ab[j].y;
+        }
+        if (out->seq)
+            out->seq[j] = (int64_t)seq[j];
+        if (out->state28)
+        {
+            float *s = out->state28 + 28 * (size_t)j;
+            for (int k = 0; k < 8; ++k)
+            {
+                s[3 * k] = d[8 * j + k].x;
+                s[3 * k + 1] = d[8 * j + k].y;
+                s[3 * k + 2] = d[8 * j + k].z;
+            }
+            s[24] = d[8 * j + 0].w;
+            s[25] = d[8 * j + 1].w;
+            s[26] = d[8 * j + 2].w;
+            s[27] = d[8 * j + 3].w;
+        }
+        if (out->broken)
+            out->broken[j] = d[8 * j + 4].w != 0.0f ? 1 : 0;
+    }
+    return AVBD_OK;
+}
+
+int avbd_next_seq(AvbdContext *ctx, int64_t *next_seq)
+{
+    if (!ctx || !next_seq)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
+    *next_seq = ctx->nextSeq;
+    return AVBD_OK;
+}
+
+int avbd_read_colours(AvbdContext *ctx, int32_t *colour, int32_t *num_colours)
+{
+    if (!ctx)
+        return AVBD_ERR_ARGUMENT;
+    if (num_colours)
+        *num_colours = ctx->nColours;
+    if (colour && ctx->n)
+    {
+        if (!ctx->colour.p)
+        {
+            for (int i = 0; i < ctx->n; ++i)
+                colour[i] = -1;
+            return AVBD_OK;
+        }
+        CU(cudaMemcpyAsync(colour, ctx->colour.p, sizeof(int) * ctx->n, cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+    }
+    return AVBD_OK;
+}
+
+int avbd_read_solve_order(AvbdContext *ctx, int32_t *order, int32_t *count)
+{
+    if (!ctx)
+        return AVBD_ERR_ARGUMENT;
+    if (count)
+        *count = ctx->nSolve;
+    if (order && ctx->nSolve)
+    {
+        CU(cudaMemcpyAsync(order, ctx->solveList.p, sizeof(int) * ctx->nSolve, cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+    }
+    return AVBD_OK;
+}
+
+int avbd_get_stats(AvbdContext *ctx, AvbdStats *stats)
+{
+    if (!ctx || !stats)
+        return AVBD_ERR_ARGUMENT;
+    *stats = ctx->stats;
+    return AVBD_OK;
+}
+
+int avbd_device_pose(AvbdContext *ctx, void **position4, void **orientation4)
+{
+    if (!ctx)
+        return AVBD_ERR_ARGUMENT;
+    if (position4)
+        *position4 = ctx->pos.p;
+    if (orientation4)
+        *orientation4 = ctx->quat.p;
+    return AVBD_OK;
+}
+
+int avbd_set_profiling(AvbdContext *ctx, int32_t enable)
+{
+    if (!ctx)
+        return AVBD_ERR_ARGUMENT;
+    ctx->profiling = enable != 0;
+    return AVBD_OK;
+}
+
+int avbd_read_profile(AvbdContext *ctx, AvbdProfile *out)
+{
+    if (!ctx || !out)
+        return AVBD_ERR_ARGUMENT;
+    out->steps = ctx->stepsProfiled;
+    for (int k = 0; k < AVBD_PHASE_COUNT; ++k)
+    {
+        out->phase_ms[k] = ctx->phaseMs[k];
+        out->phase_spans[k] = ctx->phaseLaunches[k];
+    }
+    out->launches = ctx->launches;
+    return AVBD_OK;
+}
+
+int avbd_reset_profile(AvbdContext *ctx)
+{
+    if (!ctx)
+        return AVBD_ERR_ARGUMENT;
+    for (int k = 0; k < AVBD_PHASE_COUNT; ++k)
+    {
+        ctx->phaseMs[k] = 0.0;
+        ctx->phaseLaunches[k] = 0;
+    }
+    ctx->launches = 0;
+    ctx->stepsProfiled = 0;
+    return AVBD_OK;
+}
+
+} // extern "C"

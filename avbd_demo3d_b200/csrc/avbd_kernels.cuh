@@ -1,0 +1,1726 @@
+// Device kernels of the AVBD step for sm_100a.
+//
+// Data layout (HBM, structure of arrays, one float4 per 3-vector so every load is a
+// single 128-bit transaction):
+//   bodies     pos/quat/initLin/initAng/inertLin/inertAng/vel/angvel/prevVel float4[n],
+//              massMoment float4 (mass, moment xyz), sizeRad float4 (size xyz, radius), friction float
+//   manifolds  ab int2, seq u64, n int, basis float4[3] (row0.w = friction),
+//              contact float4[8][4]: (rA.xyz, rB.x) (rB.yz, C0.xy) (C0.z, penalty.xyz)
+//                                     (lambda.xyz, key | stick << 31)
+//   joints     ab int2, seq u64, float4[8]: (rA, stiffLin) (rB, stiffAng) (C0Lin, fracture)
+//              (C0Ang, torqueArm) (penLin, broken) (penAng) (lamLin) (lamAng)
+//   springs    ab int2, seq u64, float4[2]: (rA, rest) (rB, stiffness)
+//   adjacency  CSR over bodies: entry = type << 30 | isA << 29 | index, newest force first
+//
+// Reference behaviour each kernel reproduces is cited at the kernel.
+#pragma once
+
+#include "avbd_math.cuh"
+
+namespace avbd
+{
+
+constexpr float PENALTY_MIN = 1.0f;
+constexpr float PENALTY_MAX = 10000000000.0f;
+constexpr float COLLISION_MARGIN = 0.01f;
+constexpr float STICK_THRESH = 0.00001f;
+
+constexpr unsigned ADJ_MANIFOLD = 0u, ADJ_JOINT = 1u, ADJ_SPRING = 2u, ADJ_IGNORE = 3u;
+constexpr unsigned ADJ_INDEX_MASK = (1u << 29) - 1u;
+constexpr unsigned ADJ_NONE = 0xFFFFFFFFu;
+
+struct Params
+{
+    float dt, gravity;
+    int iterations;
+    float alpha, betaLin, betaAng, gamma;
+};
+
+struct DevBodies
+{
+    int n;
+    float4 *pos, *quat, *initLin, *initAng, *inertLin, *inertAng, *vel, *angvel, *prevVel;
+    float4 *massMoment, *sizeRad;
+    float *friction;
+};
+
+struct DevManifolds
+{
+    int2 *ab;
+    unsigned long long *seq;
+    int *n;
+    float4 *basis;   // 3 per manifold
+    float4 *contact; // 32 per manifold
+};
+
+struct DevForces
+{
+    int nMan;
+    DevManifolds man;
+    int nJoint;
+    int2 *jointAB;
+    unsigned long long *jointSeq;
+    float4 *joint; // 8 per joint
+    int nSpring;
+    int2 *springAB;
+    unsigned long long *springSeq;
+    float4 *spring; // 2 per spring
+    int nIgnore;
+    int2 *ignoreAB;
+    unsigned long long *ignoreSeq;
+    int *adjStart; // n + 1
+    unsigned *adj;
+};
+
+// Capacity of the cell-start table; the reference caps the grid at 2^22 cells.
+constexpr unsigned CELL_TABLE_SIZE = 1u << 22;
+
+struct GridParams
+{
+    float bminx, bminy, bminz;
+    float cellSize;
+    int nx, ny, nz;
+    unsigned long long numCells;
+};
+
+// Device-side counters of one step.
+struct StepCounters
+{
+    unsigned long long pairChecks;
+    unsigned long long sphereHits;
+    unsigned long long constrainedHits;
+    int largePairs;
+    int colouredThisRound;
+    int maxColour;
+    int error;
+};
+
+enum DeviceError
+{
+    DERR_NONE = 0,
+    DERR_TOO_MANY_COLOURS = 1,
+    DERR_TOO_MANY_CELLS = 2
+};
+
+AVBD_DEV unsigned adj_type(unsigned e) { return e >> 30; }
+AVBD_DEV unsigned adj_isA(unsigned e) { return (e >> 29) & 1u; }
+AVBD_DEV unsigned adj_index(unsigned e) { return e & ADJ_INDEX_MASK; }
+AVBD_DEV unsigned make_adj(unsigned type, unsigned isA, unsigned index) { return (type << 30) | (isA << 29) | index; }
+
+AVBD_DEV int2 force_bodies(const DevForces &F, unsigned e)
+{
+    unsigned i = adj_index(e);
+    switch (adj_type(e))
+    {
+    case ADJ_MANIFOLD:
+        return F.man.ab[i];
+    case ADJ_JOINT:
+        return F.jointAB[i];
+    case ADJ_SPRING:
+        return F.springAB[i];
+    default:
+        return F.ignoreAB[i];
+    }
+}
+
+// Rigid::constrainedTo, walking the shorter force list (solver.cpp:197-205, rigid.cpp:105-116)
+AVBD_DEV bool constrained(const DevForces &F, int a, int b)
+{
+    int da = F.adjStart[a + 1] - F.adjStart[a];
+    int db = F.adjStart[b + 1] - F.adjStart[b];
+    int self = da <= db ? a : b;
+    int other = self == a ? b : a;
+    for (int k = F.adjStart[self]; k < F.adjStart[self + 1]; ++k)
+    {
+        int2 ab = force_bodies(F, F.adj[k]);
+        if ((ab.x == self && ab.y == other) || (ab.x == other && ab.y == self))
+            return true;
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// Broadphase: the reference's uniform grid (solver.cpp:284-486), run on the GPU.
+// Pairs come out in the reference's creation order: sorted entry i, then the rest of
+// its own cell, the 13 forward cells, the large bodies; large-large pairs last.
+// ---------------------------------------------------------------------------
+
+AVBD_DEV unsigned float_order(float f)
+{
+    unsigned u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+AVBD_DEV float float_unorder(unsigned u) { return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u); }
+
+__global__ void k_bp_bounds_init(unsigned *bounds)
+{
+    if (threadIdx.x < 3)
+        bounds[threadIdx.x] = 0xFFFFFFFFu; // min slots
+    else if (threadIdx.x < 6)
+        bounds[threadIdx.x] = 0u; // max slots
+}
+
+__global__ void k_bp_bounds(DevBodies B, const int *binned, int nBinned, unsigned *bounds)
+{
+    unsigned lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, hi[3] = {0u, 0u, 0u};
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nBinned; k += gridDim.x * blockDim.x)
+    {
+        float4 p = B.pos[binned[k]];
+        unsigned v[3] = {float_order(p.x), float_order(p.y), float_order(p.z)};
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+        {
+            lo[d] = min(lo[d], v[d]);
+            hi[d] = max(hi[d], v[d]);
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+    {
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            lo[d] = min(lo[d], __shfl_xor_sync(0xFFFFFFFFu, lo[d], o));
+            hi[d] = max(hi[d], __shfl_xor_sync(0xFFFFFFFFu, hi[d], o));
+        }
+    }
+    if ((threadIdx.x & 31) == 0)
+    {
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+        {
+            atomicMin(&bounds[d], lo[d]);
+            atomicMax(&bounds[3 + d], hi[d]);
+        }
+    }
+}
+
+// World AABB plus travel slack of the few bodies too large for the grid (solver.cpp:311-327)
+__global__ void k_bp_large(DevBodies B, const int *large, int nLarge, float dt, float4 *lo, float4 *hi,
+                           float4 *sphere)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nLarge)
+        return;
+    int b = large[k];
+    float3 p = xyz(B.pos[b]);
+    float4 q = B.quat[b];
+    float4 sr = B.sizeRad[b];
+    float slack = len(xyz(B.vel[b])) * dt;
+    float3 e = mul(xyz(sr), 0.5f);
+    float3 cx = rotate(q, f3(1, 0, 0));
+    float3 cy = rotate(q, f3(0, 1, 0));
+    float3 cz = rotate(q, f3(0, 0, 1));
+    float3 h = f3(fabsf(cx.x) * e.x + fabsf(cy.x) * e.y + fabsf(cz.x) * e.z,
+                  fabsf(cx.y) * e.x + fabsf(cy.y) * e.y + fabsf(cz.y) * e.z,
+                  fabsf(cx.z) * e.x + fabsf(cy.z) * e.y + fabsf(cz.z) * e.z);
+    lo[k] = f4(sub(p, h), slack);
+    hi[k] = f4(add(p, h), slack);
+    sphere[k] = f4(p, sr.w);
+}
+
+// Cell size and grid dimensions with the reference's cell-count cap (solver.cpp:338-357)
+__global__ void k_bp_params(const unsigned *bounds, float binnedRadius, GridParams *gp, StepCounters *cnt)
+{
+    float bminx = float_unorder(bounds[0]), bminy = float_unorder(bounds[1]), bminz = float_unorder(bounds[2]);
+    float bmaxx = float_unorder(bounds[3]), bmaxy = float_unorder(bounds[4]), bmaxz = float_unorder(bounds[5]);
+    float cellSize = binnedRadius * 2.0f;
+    const unsigned long long maxCells = 1ull << 22;
+    float3 extent = f3(bmaxx - bminx, bmaxy - bminy, bmaxz - bminz);
+    int nx = (int)(extent.x / cellSize) + 1;
+    int ny = (int)(extent.y / cellSize) + 1;
+    int nz = (int)(extent.z / cellSize) + 1;
+    unsigned long long numCells = (unsigned long long)nx * (unsigned long long)ny * (unsigned long long)nz;
+    int guard = 0;
+    while (numCells > maxCells && guard++ < 64)
+    {
+        cellSize *= rmax(cbrtf((float)numCells / (float)maxCells), 1.1f);
+        nx = (int)(extent.x / cellSize) + 1;
+        ny = (int)(extent.y / cellSize) + 1;
+        nz = (int)(extent.z / cellSize) + 1;
+        numCells = (unsigned long long)nx * (unsigned long long)ny * (unsigned long long)nz;
+    }
+    if (numCells > maxCells)
+        cnt->error = DERR_TOO_MANY_CELLS;
+    gp->bminx = bminx;
+    gp->bminy = bminy;
+    gp->bminz = bminz;
+    gp->cellSize = cellSize;
+    gp->nx = nx;
+    gp->ny = ny;
+    gp->nz = nz;
+    gp->numCells = numCells;
+}
+
+__global__ void k_bp_keys(DevBodies B, const int *binned, int nBinned, const GridParams *gp,
+                          unsigned long long *keys)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nBinned)
+        return;
+    int b = binned[k];
+    float4 c = B.pos[b];
+    GridParams g = *gp;
+    int ix = (int)rclamp((c.x - g.bminx) / g.cellSize, 0.0f, (float)(g.nx - 1));
+    int iy = (int)rclamp((c.y - g.bminy) / g.cellSize, 0.0f, (float)(g.ny - 1));
+    int iz = (int)rclamp((c.z - g.bminz) / g.cellSize, 0.0f, (float)(g.nz - 1));
+    unsigned key = (unsigned)(ix + g.nx * (iy + g.ny * iz));
+    if (g.numCells > CELL_TABLE_SIZE || key >= CELL_TABLE_SIZE)
+        key = 0; // only reachable with non-finite positions; the step reports DERR_TOO_MANY_CELLS
+    keys[k] = ((unsigned long long)key << 32) | (unsigned)b;
+}
+
+__global__ void k_bp_cell_start(const unsigned long long *keys, int nBinned, unsigned *cellStart, int set)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nBinned)
+        return;
+    unsigned key = (unsigned)(keys[k] >> 32);
+    if (key < CELL_TABLE_SIZE && (k == 0 || (unsigned)(keys[k - 1] >> 32) != key))
+        cellStart[key] = set ? (unsigned)k : 0xFFFFFFFFu;
+}
+
+__constant__ int c_forward[13][3] = {{1, 0, 0},   {-1, 1, 0}, {0, 1, 0},  {1, 1, 0}, {-1, -1, 1},
+                                     {0, -1, 1},  {1, -1, 1}, {-1, 0, 1}, {0, 0, 1}, {1, 0, 1},
+                                     {-1, 1, 1},  {0, 1, 1},  {1, 1, 1}};
+
+constexpr int LARGE_TILE = 256;
+constexpr int LL_CHUNK = 128;
+
+// Warp-aggregated add of per-thread statistics (one atomic per warp).
+AVBD_DEV void warp_add(unsigned long long *dst, unsigned v)
+{
+    unsigned s = __reduce_add_sync(0xFFFFFFFFu, v);
+    if ((threadIdx.x & 31) == 0 && s)
+        atomicAdd(dst, (unsigned long long)s);
+}
+
+// One thread per sorted grid entry i (solver.cpp:405-465). EMIT == false counts new
+// (unconstrained) hits, EMIT == true writes them as fresh manifolds at base + offset[i]
+// in hit order. The large bodies are streamed through shared memory in tiles; each
+// thread still visits them in list order.
+template <bool EMIT>
+__global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, const unsigned long long *keys,
+                                                  int nBinned, const unsigned *cellStart, const GridParams *gp,
+                                                  const int *large, int nLarge, const float4 *largeLo,
+                                                  const float4 *largeHi, float dt, int *counts, const int *offsets,
+                                                  int base, unsigned long long seqBase, StepCounters *cnt)
+{
+    __shared__ float4 sLo[LARGE_TILE], sHi[LARGE_TILE];
+    __shared__ int sId[LARGE_TILE];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = i < nBinned;
+    GridParams g = *gp;
+    unsigned akey = 0;
+    int a = 0;
+    float3 ac = f3(0, 0, 0);
+    float ar = 0.0f, aslack = 0.0f;
+    if (active)
+    {
+        unsigned long long ki = keys[i];
+        akey = (unsigned)(ki >> 32);
+        a = (int)(unsigned)ki;
+        ac = xyz(B.pos[a]);
+        ar = B.sizeRad[a].w;
+        aslack = len(xyz(B.vel[a])) * dt;
+    }
+    int found = 0;
+    int out = (EMIT && active) ? base + offsets[i] : 0;
+    unsigned checks = 0, hits = 0, cons = 0;
+
+    auto hit = [&](int bIdx) {
+        hits++;
+        if (constrained(F, a, bIdx))
+        {
+            cons++;
+            return;
+        }
+        if (EMIT)
+        {
+            int m = out + found;
+            F.man.ab[m] = make_int2(a, bIdx);
+            F.man.seq[m] = seqBase + (unsigned long long)(m - base);
+            F.man.n[m] = 0;
+        }
+        found++;
+    };
+    auto test = [&](int j) {
+        checks++;
+        int bIdx = (int)(unsigned)keys[j];
+        float3 dp = sub(ac, xyz(B.pos[bIdx]));
+        float r = ar + B.sizeRad[bIdx].w;
+        if (!(dot(dp, dp) > r * r))
+            hit(bIdx);
+    };
+
+    if (active)
+    {
+        for (int j = i + 1; j < nBinned && (unsigned)(keys[j] >> 32) == akey; ++j)
+            test(j);
+        int ix = (int)(akey % (unsigned)g.nx);
+        unsigned t = akey / (unsigned)g.nx;
+        int iy = (int)(t % (unsigned)g.ny);
+        int iz = (int)(t / (unsigned)g.ny);
+        for (int d = 0; d < 13; ++d)
+        {
+            int cx = ix + c_forward[d][0], cy = iy + c_forward[d][1], cz = iz + c_forward[d][2];
+            if (cx < 0 || cx >= g.nx || cy < 0 || cy >= g.ny || cz < 0 || cz >= g.nz)
+                continue;
+            unsigned nkey = (unsigned)(cx + g.nx * (cy + g.ny * cz));
+            if (nkey >= CELL_TABLE_SIZE)
+                continue;
+            unsigned s = cellStart[nkey];
+            if (s == 0xFFFFFFFFu)
+                continue;
+            for (int j = (int)s; j < nBinned && (unsigned)(keys[j] >> 32) == nkey; ++j)
+                test(j);
+        }
+    }
+    const float margin4 = 4.0f * COLLISION_MARGIN;
+    for (int t0 = 0; t0 < nLarge; t0 += LARGE_TILE)
+    {
+        int tn = min(LARGE_TILE, nLarge - t0);
+        __syncthreads();
+        for (int k = threadIdx.x; k < tn; k += blockDim.x)
+        {
+            sLo[k] = largeLo[t0 + k];
+            sHi[k] = largeHi[t0 + k];
+            sId[k] = large[t0 + k];
+        }
+        __syncthreads();
+        if (!active)
+            continue;
+        for (int l = 0; l < tn; ++l)
+        {
+            checks++;
+            float4 lo = sLo[l], hi = sHi[l];
+            float3 q = f3(rclamp(ac.x, lo.x, hi.x), rclamp(ac.y, lo.y, hi.y), rclamp(ac.z, lo.z, hi.z));
+            float3 dp = sub(ac, q);
+            float reach = ar + aslack + lo.w + margin4;
+            if (dot(dp, dp) > reach * reach)
+                continue;
+            hit(sId[l]);
+        }
+    }
+    if (!EMIT)
+    {
+        if (active)
+            counts[i] = found;
+        warp_add(&cnt->pairChecks, checks);
+        warp_add(&cnt->sphereHits, hits);
+        warp_add(&cnt->constrainedHits, cons);
+    }
+}
+
+// Large-vs-large pairs (solver.cpp:476-479), which the reference tests serially after
+// all grid pairs. Work item w = (i, chunk) covers j in one LL_CHUNK-wide slice of (i, n);
+// items in (i, chunk) order reproduce the serial i < j order.
+template <bool EMIT>
+__global__ void k_bp_large_large(DevForces F, const int *large, const float4 *largeSphere, int nLarge, int nChunks,
+                                 int *counts, const int *offsets, int base, unsigned long long seqBase,
+                                 StepCounters *cnt)
+{
+    const long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = w < (long long)nLarge * nChunks;
+    unsigned checks = 0, hits = 0, cons = 0;
+    if (active)
+    {
+        int i = (int)(w / nChunks), c = (int)(w % nChunks);
+        int jBeg = max(i + 1, c * LL_CHUNK), jEnd = min(nLarge, (c + 1) * LL_CHUNK);
+        float4 si = largeSphere[i];
+        int a = large[i];
+        int found = 0;
+        int out = EMIT ? base + offsets[w] : 0;
+        for (int j = jBeg; j < jEnd; ++j)
+        {
+            checks++;
+            float4 sj = largeSphere[j];
+            float3 dp = sub(xyz(si), xyz(sj));
+            float r = si.w + sj.w;
+            if (!(dot(dp, dp) <= r * r))
+                continue;
+            hits++;
+            int b = large[j];
+            if (constrained(F, a, b))
+            {
+                cons++;
+                continue;
+            }
+            if (EMIT)
+            {
+                int m = out + found;
+                F.man.ab[m] = make_int2(a, b);
+                F.man.seq[m] = seqBase + (unsigned long long)(m - base);
+                F.man.n[m] = 0;
+            }
+            found++;
+        }
+        if (!EMIT)
+            counts[w] = found;
+    }
+    if (!EMIT)
+    {
+        warp_add(&cnt->pairChecks, checks);
+        warp_add(&cnt->sphereHits, hits);
+        warp_add(&cnt->constrainedHits, cons);
+    }
+}
+
+// All-pairs broadphase (solver.cpp:176-185): thread per body a, pairs (a, b > a) in order.
+template <bool EMIT>
+__global__ void k_bp_all_pairs(DevBodies B, DevForces F, int n, int *counts, const int *offsets, int base,
+                               unsigned long long seqBase, StepCounters *cnt)
+{
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n)
+        return;
+    float3 pa = xyz(B.pos[a]);
+    float ra = B.sizeRad[a].w;
+    int found = 0;
+    int out = EMIT ? base + offsets[a] : 0;
+    unsigned long long hits = 0, cons = 0;
+    for (int b = a + 1; b < n; ++b)
+    {
+        float3 dp = sub(pa, xyz(B.pos[b]));
+        float r = ra + B.sizeRad[b].w;
+        if (!(dot(dp, dp) <= r * r))
+            continue;
+        hits++;
+        if (constrained(F, a, b))
+        {
+            cons++;
+            continue;
+        }
+        if (EMIT)
+        {
+            int m = out + found;
+            F.man.ab[m] = make_int2(a, b);
+            F.man.seq[m] = seqBase + (unsigned long long)(m - base);
+            F.man.n[m] = 0;
+        }
+        found++;
+    }
+    if (!EMIT)
+    {
+        counts[a] = found;
+        atomicAdd(&cnt->pairChecks, (unsigned long long)(n - 1 - a));
+        atomicAdd(&cnt->sphereHits, hits);
+        atomicAdd(&cnt->constrainedHits, cons);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Box-box narrowphase (collide.cpp:60-433, 898-955)
+// ---------------------------------------------------------------------------
+
+struct Obb
+{
+    float3 c;
+    float4 q;
+    float3 h;
+    float3 ax[3];
+};
+
+struct NewContact
+{
+    int key;
+    float3 rA, rB;
+};
+
+AVBD_DEV Obb make_obb(float3 p, float4 q, float3 size)
+{
+    Obb o;
+    o.c = p;
+    o.q = q;
+    o.h = mul(size, 0.5f);
+    o.ax[0] = rotate(q, f3(1.0f, 0.0f, 0.0f));
+    o.ax[1] = rotate(q, f3(0.0f, 1.0f, 0.0f));
+    o.ax[2] = rotate(q, f3(0.0f, 0.0f, 1.0f));
+    return o;
+}
+
+AVBD_DEV float absdot(float3 a, float3 b) { return fabsf(dot(a, b)); }
+
+AVBD_DEV float3 support_point(const Obb &o, float3 d)
+{
+    float sx = dot(d, o.ax[0]) >= 0.0f ? 1.0f : -1.0f;
+    float sy = dot(d, o.ax[1]) >= 0.0f ? 1.0f : -1.0f;
+    float sz = dot(d, o.ax[2]) >= 0.0f ? 1.0f : -1.0f;
+    return add(add(add(o.c, mul(o.ax[0], o.h.x * sx)), mul(o.ax[1], o.h.y * sy)), mul(o.ax[2], o.h.z * sz));
+}
+
+AVBD_DEV void face_axes(const Obb &o, int ax, float3 &u, float3 &v, float &eu, float &ev)
+{
+    if (ax == 0)
+    {
+        u = o.ax[1];
+        v = o.ax[2];
+        eu = o.h.y;
+        ev = o.h.z;
+    }
+    else if (ax == 1)
+    {
+        u = o.ax[0];
+        v = o.ax[2];
+        eu = o.h.x;
+        ev = o.h.z;
+    }
+    else
+    {
+        u = o.ax[0];
+        v = o.ax[1];
+        eu = o.h.x;
+        ev = o.h.y;
+    }
+}
+
+// Sutherland-Hodgman step against one side plane (collide.cpp:159-195)
+AVBD_DEV int clip_plane(const float3 *in, int cnt, float3 pn, float off, float3 *out)
+{
+    if (cnt <= 0)
+        return 0;
+    int k = 0;
+    float3 a = in[cnt - 1];
+    float da = dot(pn, a) - off;
+    for (int i = 0; i < cnt; ++i)
+    {
+        float3 b = in[i];
+        float db = dot(pn, b) - off;
+        bool ain = da <= 1.0e-5f;
+        bool bin = db <= 1.0e-5f;
+        if (ain != bin)
+        {
+            float t = 0.0f;
+            float denom = da - db;
+            if (fabsf(denom) > 1.0e-6f)
+                t = rclamp(da / denom, 0.0f, 1.0f);
+            if (k < 16)
+                out[k++] = add(a, mul(sub(b, a), t));
+        }
+        if (bin && k < 16)
+            out[k++] = b;
+        a = b;
+        da = db;
+    }
+    return k;
+}
+
+// addContact (collide.cpp:197-222): merge by midpoint distance, store body-local offsets
+AVBD_DEV void add_contact(float3 pA, float4 qA, float3 pB, float4 qB, NewContact *cs, int &count, float3 *mids,
+                          float3 xA, float3 xB, int key)
+{
+    float3 mid = mul(add(xA, xB), 0.5f);
+    for (int i = 0; i < count; ++i)
+        if (lensq(sub(mid, mids[i])) < 1.0e-6f)
+            return;
+    if (count >= 8)
+        return;
+    cs[count].key = key;
+    cs[count].rA = rotate(qconj(qA), sub(xA, pA));
+    cs[count].rB = rotate(qconj(qB), sub(xB, pB));
+    mids[count] = mid;
+    count++;
+}
+
+struct SatBest
+{
+    int type, ia, ib;
+    float sep;
+    float3 n;
+    bool valid;
+};
+
+AVBD_DEV bool test_axis(const Obb &A, const Obb &B, float3 delta, float3 axis, int type, int ia, int ib, SatBest &best)
+{
+    float lenSq = lensq(axis);
+    if (lenSq < 1.0e-6f)
+        return true;
+    float invLen = 1.0f / sqrtf(lenSq);
+    float3 n = mul(axis, invLen);
+    if (dot(n, delta) < 0.0f)
+        n = neg(n);
+    float distance = fabsf(dot(delta, n));
+    float rA = A.h.x * absdot(n, A.ax[0]) + A.h.y * absdot(n, A.ax[1]) + A.h.z * absdot(n, A.ax[2]);
+    float rB = B.h.x * absdot(n, B.ax[0]) + B.h.y * absdot(n, B.ax[1]) + B.h.z * absdot(n, B.ax[2]);
+    float sep = distance - (rA + rB);
+    if (sep > 0.0f)
+        return false;
+    if (!best.valid || sep > best.sep)
+    {
+        best.valid = true;
+        best.type = type;
+        best.ia = ia;
+        best.ib = ib;
+        best.sep = sep;
+        best.n = n;
+    }
+    return true;
+}
+
+AVBD_DEV void support_edge(const Obb &o, int ax, float3 d, float3 &ea, float3 &eb)
+{
+    int a1 = (ax + 1) % 3, a2 = (ax + 2) % 3;
+    float s1 = dot(d, o.ax[a1]) >= 0.0f ? 1.0f : -1.0f;
+    float s2 = dot(d, o.ax[a2]) >= 0.0f ? 1.0f : -1.0f;
+    float3 ec = add(add(o.c, mul(o.ax[a1], comp(o.h, a1) * s1)), mul(o.ax[a2], comp(o.h, a2) * s2));
+    ea = sub(ec, mul(o.ax[ax], comp(o.h, ax)));
+    eb = add(ec, mul(o.ax[ax], comp(o.h, ax)));
+}
+
+AVBD_DEV void closest_segments(float3 p0, float3 p1, float3 q0, float3 q1, float3 &c0, float3 &c1)
+{
+    float3 d1 = sub(p1, p0), d2 = sub(q1, q0), r = sub(p0, q0);
+    float a = dot(d1, d1), e = dot(d2, d2), f = dot(d2, r);
+    float s = 0.0f, t = 0.0f;
+    if (a <= 1.0e-6f && e <= 1.0e-6f)
+    {
+        c0 = p0;
+        c1 = q0;
+        return;
+    }
+    if (a <= 1.0e-6f)
+        t = rclamp(f / e, 0.0f, 1.0f);
+    else
+    {
+        float c = dot(d1, r);
+        if (e <= 1.0e-6f)
+            s = rclamp(-c / a, 0.0f, 1.0f);
+        else
+        {
+            float b = dot(d1, d2);
+            float denom = a * e - b * b;
+            if (fabsf(denom) > 1.0e-6f)
+                s = rclamp((b * f - c * e) / denom, 0.0f, 1.0f);
+            t = (b * s + f) / e;
+            if (t < 0.0f)
+            {
+                t = 0.0f;
+                s = rclamp(-c / a, 0.0f, 1.0f);
+            }
+            else if (t > 1.0f)
+            {
+                t = 1.0f;
+                s = rclamp((b - c) / a, 0.0f, 1.0f);
+            }
+        }
+    }
+    c0 = add(p0, mul(d1, s));
+    c1 = add(q0, mul(d2, t));
+}
+
+// Reference face clipped against the incident face (collide.cpp:337-405)
+AVBD_DEV int face_manifold(const Obb &A, const Obb &B, bool refIsA, int refAxis, float3 nAB, NewContact *cs)
+{
+    const Obb &R = refIsA ? A : B;
+    const Obb &I = refIsA ? B : A;
+    float3 outward = refIsA ? nAB : neg(nAB);
+    float sgn = dot(outward, R.ax[refAxis]) >= 0.0f ? 1.0f : -1.0f;
+    float3 rn = mul(R.ax[refAxis], sgn);
+    float3 rc = add(R.c, mul(rn, comp(R.h, refAxis)));
+    float3 ru, rv;
+    float reu, rev;
+    face_axes(R, refAxis, ru, rv, reu, rev);
+
+    int incAxis = 0;
+    float best = -3.402823466e+38f;
+    for (int i = 0; i < 3; ++i)
+    {
+        float d = absdot(I.ax[i], rn);
+        if (d > best)
+        {
+            best = d;
+            incAxis = i;
+        }
+    }
+    float3 c0[16], c1[16];
+    {
+        float s = dot(I.ax[incAxis], rn) > 0.0f ? -1.0f : 1.0f;
+        float3 fn = mul(I.ax[incAxis], s);
+        float3 fc = add(I.c, mul(fn, comp(I.h, incAxis)));
+        float3 u, v;
+        float eu, ev;
+        face_axes(I, incAxis, u, v, eu, ev);
+        c0[0] = add(add(fc, mul(u, eu)), mul(v, ev));
+        c0[1] = add(sub(fc, mul(u, eu)), mul(v, ev));
+        c0[2] = sub(sub(fc, mul(u, eu)), mul(v, ev));
+        c0[3] = sub(add(fc, mul(u, eu)), mul(v, ev));
+    }
+    int cnt = 4;
+    float3 n0 = ru;
+    cnt = clip_plane(c0, cnt, n0, dot(n0, rc) + reu, c1);
+    if (!cnt)
+        return 0;
+    float3 n1 = neg(ru);
+    cnt = clip_plane(c1, cnt, n1, dot(n1, rc) + reu, c0);
+    if (!cnt)
+        return 0;
+    float3 n2 = rv;
+    cnt = clip_plane(c0, cnt, n2, dot(n2, rc) + rev, c1);
+    if (!cnt)
+        return 0;
+    float3 n3 = neg(rv);
+    cnt = clip_plane(c1, cnt, n3, dot(n3, rc) + rev, c0);
+    if (!cnt)
+        return 0;
+
+    int count = 0;
+    float3 mids[8];
+    int prefix = (refIsA ? 0 : 1) << 24;
+    prefix |= (refAxis & 0xFF) << 16;
+    prefix |= (incAxis & 0xFF) << 8;
+    for (int i = 0; i < cnt && count < 8; ++i)
+    {
+        float3 p = c0[i];
+        float dist = dot(sub(p, rc), rn);
+        if (dist > 1.0e-5f)
+            continue;
+        float3 pr = sub(p, mul(rn, dist));
+        add_contact(A.c, A.q, B.c, B.q, cs, count, mids, refIsA ? pr : p, refIsA ? p : pr, prefix | (i & 0xFF));
+    }
+    if (!count)
+        add_contact(A.c, A.q, B.c, B.q, cs, count, mids, support_point(A, nAB), support_point(B, neg(nAB)), prefix);
+    return count;
+}
+
+// Edge-edge contact (collide.cpp:407-433)
+AVBD_DEV int edge_contact(const Obb &A, const Obb &B, int axA, int axB, float3 nAB, NewContact *cs)
+{
+    float3 a0, a1, b0, b1, xA, xB;
+    support_edge(A, axA, nAB, a0, a1);
+    support_edge(B, axB, neg(nAB), b0, b1);
+    closest_segments(a0, a1, b0, b1, xA, xB);
+    int count = 0;
+    float3 mids[8];
+    int key = (2 << 24) | ((axA & 0xFF) << 8) | (axB & 0xFF);
+    add_contact(A.c, A.q, B.c, B.q, cs, count, mids, xA, xB, key);
+    if (!count)
+        add_contact(A.c, A.q, B.c, B.q, cs, count, mids, support_point(A, nAB), support_point(B, neg(nAB)), key);
+    return count;
+}
+
+// collideBoxes (collide.cpp:898-955): 15-axis SAT with early out, edge preference, clipping
+AVBD_DEV int collide_boxes(float3 pA, float4 qA, float3 sA, float3 pB, float4 qB, float3 sB, NewContact *cs,
+                           M3 &basis)
+{
+    Obb A = make_obb(pA, qA, sA), B = make_obb(pB, qB, sB);
+    float3 delta = sub(B.c, A.c);
+    SatBest face, edge;
+    face.valid = false;
+    face.sep = -3.402823466e+38f;
+    face.type = face.ia = face.ib = 0;
+    face.n = f3(0, 0, 0);
+    edge = face;
+    for (int i = 0; i < 3; ++i)
+        if (!test_axis(A, B, delta, A.ax[i], 0, i, -1, face))
+            return 0;
+    for (int i = 0; i < 3; ++i)
+        if (!test_axis(A, B, delta, B.ax[i], 1, -1, i, face))
+            return 0;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            if (!test_axis(A, B, delta, cross(A.ax[i], B.ax[j]), 2, i, j, edge))
+                return 0;
+    if (!face.valid)
+        return 0;
+    SatBest best = face;
+    if (edge.valid && 0.95f * edge.sep > face.sep + 0.01f)
+        best = edge;
+    basis = orthonormal(neg(best.n));
+    if (best.type == 2)
+        return edge_contact(A, B, best.ia, best.ib, best.n, cs);
+    if (best.type == 0)
+        return face_manifold(A, B, true, best.ia, best.n, cs);
+    return face_manifold(A, B, false, best.ib, best.n, cs);
+}
+
+// ---------------------------------------------------------------------------
+// Force initialisation
+// ---------------------------------------------------------------------------
+
+struct ContactRec
+{
+    float3 rA, rB, C0, pen, lam;
+    int key;
+    bool stick;
+};
+
+AVBD_DEV ContactRec load_contact(const float4 *c)
+{
+    float4 k0 = c[0], k1 = c[1], k2 = c[2], k3 = c[3];
+    ContactRec r;
+    r.rA = f3(k0.x, k0.y, k0.z);
+    r.rB = f3(k0.w, k1.x, k1.y);
+    r.C0 = f3(k1.z, k1.w, k2.x);
+    r.pen = f3(k2.y, k2.z, k2.w);
+    r.lam = f3(k3.x, k3.y, k3.z);
+    unsigned bits = __float_as_uint(k3.w);
+    r.key = (int)(bits & 0x7FFFFFFFu);
+    r.stick = (bits >> 31) != 0;
+    return r;
+}
+
+AVBD_DEV void store_contact(float4 *c, const ContactRec &r)
+{
+    c[0] = make_float4(r.rA.x, r.rA.y, r.rA.z, r.rB.x);
+    c[1] = make_float4(r.rB.y, r.rB.z, r.C0.x, r.C0.y);
+    c[2] = make_float4(r.C0.z, r.pen.x, r.pen.y, r.pen.z);
+    c[3] = make_float4(r.lam.x, r.lam.y, r.lam.z, __uint_as_float((unsigned)r.key | (r.stick ? 0x80000000u : 0u)));
+}
+
+AVBD_DEV M3 load_basis(const float4 *b) { return rows(xyz(b[0]), xyz(b[1]), xyz(b[2])); }
+
+// Manifold::initialize for boxes (manifold.cpp:100-174): collide at q-, keep warm-start data
+// of contacts whose feature key persists, C0, lambda/penalty decay.
+__global__ void k_manifold_init(DevBodies B, DevManifolds M, int count, Params P, unsigned char *keep)
+{
+    int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= count)
+        return;
+    int2 ab = M.ab[m];
+    float3 pA = xyz(B.pos[ab.x]), pB = xyz(B.pos[ab.y]);
+    float4 qA = B.quat[ab.x], qB = B.quat[ab.y];
+    float3 sA = xyz(B.sizeRad[ab.x]), sB = xyz(B.sizeRad[ab.y]);
+    float friction = sqrtf(B.friction[ab.x] * B.friction[ab.y]);
+    NewContact nc[8];
+    for (int i = 0; i < 8; ++i)
+    {
+        nc[i].key = 0;
+        nc[i].rA = f3(0, 0, 0);
+        nc[i].rB = f3(0, 0, 0);
+    }
+    M3 basis = load_basis(M.basis + 3 * m);
+    int nn = collide_boxes(pA, qA, sA, pB, qB, sB, nc, basis);
+    int nOld = M.n[m];
+    float4 *cbase = M.contact + (size_t)m * 32;
+    ContactRec merged[8];
+    for (int i = 0; i < nn; ++i)
+    {
+        ContactRec r;
+        r.key = nc[i].key;
+        r.rA = nc[i].rA;
+        r.rB = nc[i].rB;
+        r.C0 = f3(0, 0, 0);
+        r.pen = f3(0, 0, 0);
+        r.lam = f3(0, 0, 0);
+        r.stick = false;
+        for (int j = 0; j < nOld; ++j)
+        {
+            ContactRec o = load_contact(cbase + 4 * j);
+            if (o.key == nc[i].key)
+            {
+                r = o;
+                if (!o.stick)
+                {
+                    r.rA = nc[i].rA;
+                    r.rB = nc[i].rB;
+                }
+                break;
+            }
+        }
+        merged[i] = r;
+    }
+    for (int i = 0; i < nn; ++i)
+    {
+        ContactRec &c = merged[i];
+        float3 xA = add(pA, rotate(qA, c.rA));
+        float3 xB = add(pB, rotate(qB, c.rB));
+        c.C0 = add(mv(basis, sub(xA, xB)), f3(COLLISION_MARGIN, 0, 0));
+        c.lam = mul(mul(c.lam, P.alpha), P.gamma);
+        c.pen = clampv(mul(c.pen, P.gamma), PENALTY_MIN, PENALTY_MAX);
+        store_contact(cbase + 4 * i, c);
+    }
+    M.n[m] = nn;
+    M.basis[3 * m + 0] = f4(basis.r0, friction);
+    M.basis[3 * m + 1] = f4(basis.r1, 0.0f);
+    M.basis[3 * m + 2] = f4(basis.r2, 0.0f);
+    keep[m] = nn > 0 ? 1 : 0;
+}
+
+// Joint::initialize (joint.cpp:35-54)
+__global__ void k_joint_init(DevBodies B, DevForces F, Params P, unsigned char *keep)
+{
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= F.nJoint)
+        return;
+    float4 *d = F.joint + 8 * (size_t)j;
+    int2 ab = F.jointAB[j];
+    float4 d0 = d[0], d1 = d[1], d3 = d[3], d4 = d[4], d5 = d[5], d6 = d[6], d7 = d[7];
+    float3 rA = xyz(d0), rB = xyz(d1);
+    float stiffLin = d0.w, stiffAng = d1.w, torqueArm = d3.w;
+    float3 pB = xyz(B.pos[ab.y]);
+    float4 qB = B.quat[ab.y];
+    float3 pa = ab.x >= 0 ? xform(xyz(B.pos[ab.x]), B.quat[ab.x], rA) : rA;
+    float3 C0Lin = sub(pa, xform(pB, qB, rB));
+    float4 qa = ab.x >= 0 ? B.quat[ab.x] : make_float4(0, 0, 0, 1);
+    float3 C0Ang = mul(qdiff(qa, qB), torqueArm);
+    float3 lamLin = mul(mul(xyz(d6), P.alpha), P.gamma);
+    float3 lamAng = mul(mul(xyz(d7), P.alpha), P.gamma);
+    float3 penLin = clampv(mul(xyz(d4), P.gamma), PENALTY_MIN, PENALTY_MAX);
+    float3 penAng = clampv(mul(xyz(d5), P.gamma), PENALTY_MIN, PENALTY_MAX);
+    penLin = minv(penLin, stiffLin);
+    penAng = minv(penAng, stiffAng);
+    d[2] = f4(C0Lin, d[2].w);
+    d[3] = f4(C0Ang, torqueArm);
+    d[4] = f4(penLin, d4.w);
+    d[5] = f4(penAng, 0.0f);
+    d[6] = f4(lamLin, 0.0f);
+    d[7] = f4(lamAng, 0.0f);
+    keep[j] = d4.w != 0.0f ? 0 : 1;
+}
+
+// Stable compaction of manifolds into the other buffer.
+__global__ void k_manifold_compact(DevManifolds src, DevManifolds dst, int count, const unsigned char *keep,
+                                   const int *newIndex)
+{
+    int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= count || !keep[m])
+        return;
+    int d = newIndex[m];
+    dst.ab[d] = src.ab[m];
+    dst.seq[d] = src.seq[m];
+    int n = src.n[m];
+    dst.n[d] = n;
+    dst.basis[3 * d + 0] = src.basis[3 * m + 0];
+    dst.basis[3 * d + 1] = src.basis[3 * m + 1];
+    dst.basis[3 * d + 2] = src.basis[3 * m + 2];
+    const float4 *s = src.contact + (size_t)m * 32;
+    float4 *t = dst.contact + (size_t)d * 32;
+    for (int k = 0; k < 4 * n; ++k)
+        t[k] = s[k];
+}
+
+__global__ void k_joint_compact(int count, const unsigned char *keep, const int *newIndex, const int2 *abS,
+                                const unsigned long long *seqS, const float4 *dS, int2 *abD,
+                                unsigned long long *seqD, float4 *dD)
+{
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= count || !keep[j])
+        return;
+    int d = newIndex[j];
+    abD[d] = abS[j];
+    seqD[d] = seqS[j];
+    for (int k = 0; k < 8; ++k)
+        dD[8 * (size_t)d + k] = dS[8 * (size_t)j + k];
+}
+
+// ---------------------------------------------------------------------------
+// Adjacency (per-body force lists, newest first)
+// ---------------------------------------------------------------------------
+
+constexpr int KEY_BODY_SHIFT = 40;
+constexpr unsigned long long KEY_SEQ_MASK = (1ull << KEY_BODY_SHIFT) - 1ull;
+constexpr unsigned long long KEY_NO_BODY = 0xFFFFFFull;
+
+AVBD_DEV unsigned long long incidence_key(int body, unsigned long long seq)
+{
+    unsigned long long b = body >= 0 ? (unsigned long long)body : KEY_NO_BODY;
+    return (b << KEY_BODY_SHIFT) | (KEY_SEQ_MASK - (seq & KEY_SEQ_MASK));
+}
+
+// Two incidences per force: manifolds [0, 2M), joints [2M, 2M+2J), springs, ignores.
+__global__ void k_incidences(DevForces F, unsigned long long *keys, unsigned *vals)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int total = 2 * (F.nMan + F.nJoint + F.nSpring + F.nIgnore);
+    if (t >= total)
+        return;
+    int f = t >> 1;
+    unsigned isA = (t & 1) ? 0u : 1u;
+    int2 ab;
+    unsigned long long seq;
+    unsigned type;
+    if (f < F.nMan)
+    {
+        ab = F.man.ab[f];
+        seq = F.man.seq[f];
+        type = ADJ_MANIFOLD;
+    }
+    else if ((f -= F.nMan) < F.nJoint)
+    {
+        ab = F.jointAB[f];
+        seq = F.jointSeq[f];
+        type = ADJ_JOINT;
+    }
+    else if ((f -= F.nJoint) < F.nSpring)
+    {
+        ab = F.springAB[f];
+        seq = F.springSeq[f];
+        type = ADJ_SPRING;
+    }
+    else
+    {
+        f -= F.nSpring;
+        ab = F.ignoreAB[f];
+        seq = F.ignoreSeq[f];
+        type = ADJ_IGNORE;
+    }
+    keys[t] = incidence_key(isA ? ab.x : ab.y, seq);
+    vals[t] = make_adj(type, isA, (unsigned)f);
+}
+
+// Segment starts of a sorted key array whose top bits are the segment id (0..n-1, or
+// larger for "no segment"); start[s] for s in [0, n] with gaps filled.
+__global__ void k_segment_starts(const unsigned long long *keys, int total, int shift, int n, int *start)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= total)
+        return;
+    long long cur = (long long)(keys[k] >> shift);
+    if (cur > n)
+        cur = n;
+    long long prev = -1;
+    if (k > 0)
+    {
+        prev = (long long)(keys[k - 1] >> shift);
+        if (prev > n)
+            prev = n;
+    }
+    for (long long s = prev + 1; s <= cur; ++s)
+        start[s] = k;
+    if (k == total - 1)
+        for (long long s = cur + 1; s <= n; ++s)
+            start[s] = total;
+}
+
+__global__ void k_copy_adj(const unsigned *vals, unsigned *adj, int total)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < total)
+        adj[k] = vals[k];
+}
+
+// ---------------------------------------------------------------------------
+// Body warm start (solver.cpp:1134-1169)
+// ---------------------------------------------------------------------------
+
+__global__ void k_warm_start(DevBodies B, const int *adjStart, Params P)
+{
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B.n)
+        return;
+    float dt = P.dt, g = P.gravity;
+    float3 pos = xyz(B.pos[b]);
+    float4 q = B.quat[b];
+    float3 vel = xyz(B.vel[b]);
+    float3 w = xyz(B.angvel[b]);
+    float3 pv = xyz(B.prevVel[b]);
+    float mass = B.massMoment[b].x;
+    float3 inertLin = add(pos, mul(vel, dt));
+    if (mass > 0)
+        inertLin = add(inertLin, mul(f3(0, 0, g), dt * dt));
+    float4 inertAng = qstep(q, mul(w, dt));
+    float3 accel = divs(sub(vel, pv), dt);
+    float accelExt = accel.z * rsign(g);
+    float accelWeight = rclamp(accelExt / fabsf(g), 0.0f, 1.0f);
+    if (!isfinite(accelWeight))
+        accelWeight = 0.0f;
+    B.initLin[b] = f4(pos, 0.0f);
+    B.initAng[b] = q;
+    if (mass > 0)
+    {
+        pos = add(add(pos, mul(vel, dt)), mul(f3(0, 0, g), accelWeight * dt * dt));
+        q = qstep(q, mul(w, dt));
+    }
+    if (mass > 0 && adjStart[b + 1] == adjStart[b])
+    {
+        pos = inertLin;
+        q = inertAng;
+    }
+    B.pos[b] = f4(pos, 0.0f);
+    B.quat[b] = q;
+    B.inertLin[b] = f4(inertLin, 0.0f);
+    B.inertAng[b] = inertAng;
+}
+
+// finishStep velocities (solver.cpp:1275-1287); rolling friction is sphere-only
+__global__ void k_finish(DevBodies B, Params P)
+{
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B.n)
+        return;
+    float4 v = B.vel[b];
+    B.prevVel[b] = v;
+    if (B.massMoment[b].x > 0)
+    {
+        B.vel[b] = f4(divs(sub(xyz(B.pos[b]), xyz(B.initLin[b])), P.dt), 0.0f);
+        B.angvel[b] = f4(divs(qdiff(B.quat[b], B.initAng[b]), P.dt), 0.0f);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Jones-Plassmann colouring of the dynamic-body constraint graph. In round r an
+// uncoloured vertex whose (priority, index) beats every uncoloured neighbour takes the
+// smallest colour unused by neighbours coloured in earlier rounds. The result depends
+// only on the graph, so the CPU oracle reproduces it exactly.
+// state: -2 not a vertex, -1 uncoloured, else round << 16 | colour
+// ---------------------------------------------------------------------------
+
+AVBD_DEV unsigned colour_priority(unsigned b)
+{
+    unsigned h = b * 0x9E3779B1u + 0x7F4A7C15u;
+    h ^= h >> 16;
+    h *= 0x85EBCA6Bu;
+    h ^= h >> 13;
+    h *= 0xC2B2AE35u;
+    h ^= h >> 16;
+    return h;
+}
+
+__global__ void k_colour_init(DevBodies B, const int *adjStart, int *state, int *remaining)
+{
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B.n)
+        return;
+    bool vertex = B.massMoment[b].x > 0 && adjStart[b + 1] > adjStart[b];
+    state[b] = vertex ? -1 : -2;
+    if (vertex)
+        atomicAdd(remaining, 1);
+}
+
+__global__ void k_colour_round(DevForces F, int n, int round, int *state, int *remaining, StepCounters *cnt)
+{
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n || state[v] != -1)
+        return;
+    unsigned pv = colour_priority((unsigned)v);
+    unsigned long long used[4] = {0ull, 0ull, 0ull, 0ull};
+    for (int k = F.adjStart[v]; k < F.adjStart[v + 1]; ++k)
+    {
+        unsigned e = F.adj[k];
+        if (adj_type(e) == ADJ_IGNORE)
+            continue;
+        int2 ab = force_bodies(F, e);
+        int u = ab.x == v ? ab.y : ab.x;
+        if (u < 0)
+            continue;
+        int s = state[u];
+        if (s == -2)
+            continue;
+        if (s == -1 || (s >> 16) == round)
+        {
+            unsigned pu = colour_priority((unsigned)u);
+            if (!(pv > pu || (pv == pu && v > u)))
+                return;
+        }
+        else
+        {
+            int c = s & 0xFFFF;
+            if (c < 256)
+                used[c >> 6] |= 1ull << (c & 63);
+        }
+    }
+    int c = 0;
+    while (c < 256 && ((used[c >> 6] >> (c & 63)) & 1ull))
+        c++;
+    if (c >= 256)
+    {
+        cnt->error = DERR_TOO_MANY_COLOURS;
+        c = 255;
+    }
+    state[v] = (round << 16) | c;
+    atomicSub(remaining, 1);
+    atomicMax(&cnt->maxColour, c);
+}
+
+__global__ void k_colour_keys(const int *state, int n, int *colour, unsigned long long *keys)
+{
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n)
+        return;
+    int s = state[b];
+    int c = s >= 0 ? (s & 0xFFFF) : -1;
+    colour[b] = c;
+    keys[b] = c >= 0 ? (((unsigned long long)c << 32) | (unsigned)b) : 0xFFFFFFFFFFFFFFFFull;
+}
+
+__global__ void k_solve_list(const unsigned long long *keys, int count, int *list)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < count)
+        list[k] = (int)(unsigned)keys[k];
+}
+
+// ---------------------------------------------------------------------------
+// Primal: one group of G lanes per body of the current colour (solver.cpp:1177-1242).
+// Each lane evaluates one constraint row (a manifold contact, a joint part or a spring)
+// into its 27-entry contribution; lanes that own an entry then add the rows in the
+// body's force order (newest force first, contacts in manifold order), so every sum has
+// the reference's order and the result is bit-identical. One lane factors the 6x6 LDL.
+// ---------------------------------------------------------------------------
+
+constexpr unsigned KIND_NONE = 0u;
+constexpr unsigned KIND_FULL = (1u << 27) - 1u;
+constexpr unsigned KIND_LHSANG = 0x3Fu << 6;
+constexpr unsigned KIND_ANG = (0x3Fu << 6) | (0x7u << 24);
+
+struct Pose
+{
+    float3 p, ip;
+    float4 q, iq;
+};
+
+AVBD_DEV Pose load_pose(const DevBodies &B, int b)
+{
+    Pose s;
+    s.p = xyz(B.pos[b]);
+    s.q = B.quat[b];
+    s.ip = xyz(B.initLin[b]);
+    s.iq = B.initAng[b];
+    return s;
+}
+
+AVBD_DEV float mm_entry(const M3 &a, const M3 &b, int i, int j) { return dot(row(a, i), col(b, j)); }
+
+AVBD_DEV void store_terms(float *t, const M3 &LL, const M3 &LA, const M3 &LC, float3 RL, float3 RA)
+{
+    t[E_LL00] = LL.r0.x;
+    t[E_LL10] = LL.r1.x;
+    t[E_LL11] = LL.r1.y;
+    t[E_LL20] = LL.r2.x;
+    t[E_LL21] = LL.r2.y;
+    t[E_LL22] = LL.r2.z;
+    t[E_LA00] = LA.r0.x;
+    t[E_LA10] = LA.r1.x;
+    t[E_LA11] = LA.r1.y;
+    t[E_LA20] = LA.r2.x;
+    t[E_LA21] = LA.r2.y;
+    t[E_LA22] = LA.r2.z;
+    t[E_LC00] = LC.r0.x;
+    t[E_LC01] = LC.r0.y;
+    t[E_LC02] = LC.r0.z;
+    t[E_LC10] = LC.r1.x;
+    t[E_LC11] = LC.r1.y;
+    t[E_LC12] = LC.r1.z;
+    t[E_LC20] = LC.r2.x;
+    t[E_LC21] = LC.r2.y;
+    t[E_LC22] = LC.r2.z;
+    t[E_RL0] = RL.x;
+    t[E_RL1] = RL.y;
+    t[E_RL2] = RL.z;
+    t[E_RA0] = RA.x;
+    t[E_RA1] = RA.y;
+    t[E_RA2] = RA.z;
+}
+
+// Contact row: C, F with normal clamp and friction cone (manifold.cpp:183-212)
+struct ContactEval
+{
+    M3 jALin, jBLin, jAAng, jBAng;
+    float3 C, F;
+    float fs, bounds;
+};
+
+AVBD_DEV ContactEval eval_contact(const Pose &A, const Pose &Bp, const M3 &basis, float friction,
+                                  const ContactRec &c, float alpha)
+{
+    ContactEval e;
+    float3 dqALin = sub(A.p, A.ip);
+    float3 dqAAng = qdiff(A.q, A.iq);
+    float3 dqBLin = sub(Bp.p, Bp.ip);
+    float3 dqBAng = qdiff(Bp.q, Bp.iq);
+    float3 rAW = rotate(A.q, c.rA);
+    float3 rBW = rotate(Bp.q, c.rB);
+    e.jALin = basis;
+    e.jBLin = mneg(basis);
+    e.jAAng = rows(cross(rAW, e.jALin.r0), cross(rAW, e.jALin.r1), cross(rAW, e.jALin.r2));
+    e.jBAng = rows(cross(rBW, e.jBLin.r0), cross(rBW, e.jBLin.r1), cross(rBW, e.jBLin.r2));
+    M3 K = diag(c.pen.x, c.pen.y, c.pen.z);
+    e.C = add(add(add(add(mul(c.C0, 1.0f - alpha), mv(e.jALin, dqALin)), mv(e.jBLin, dqBLin)), mv(e.jAAng, dqAAng)),
+              mv(e.jBAng, dqBAng));
+    float3 F = add(mv(K, e.C), c.lam);
+    F.x = rmin(F.x, 0.0f);
+    e.bounds = fabsf(F.x) * friction;
+    e.fs = sqrtf(F.y * F.y + F.z * F.z);
+    if (e.fs > e.bounds && e.fs > 0)
+    {
+        F.y *= e.bounds / e.fs;
+        F.z *= e.bounds / e.fs;
+    }
+    e.F = F;
+    return e;
+}
+
+AVBD_DEV unsigned contact_term(const DevBodies &B, const DevForces &F, unsigned m, int ci, bool isA, float alpha,
+                               float *t)
+{
+    int2 ab = F.man.ab[m];
+    Pose A = load_pose(B, ab.x), Bp = load_pose(B, ab.y);
+    const float4 *bs = F.man.basis + 3 * (size_t)m;
+    float4 b0 = bs[0];
+    M3 basis = rows(xyz(b0), xyz(bs[1]), xyz(bs[2]));
+    ContactRec c = load_contact(F.man.contact + (size_t)m * 32 + 4 * ci);
+    ContactEval e = eval_contact(A, Bp, basis, b0.w, c, alpha);
+    M3 K = diag(c.pen.x, c.pen.y, c.pen.z);
+    const M3 &jLin = isA ? e.jALin : e.jBLin;
+    const M3 &jAng = isA ? e.jAAng : e.jBAng;
+    M3 jLinT = trans(jLin), jAngT = trans(jAng);
+    M3 jAngTk = mm(jAngT, K);
+    store_terms(t, mm(mm(jLinT, K), jLin), mm(jAngTk, jAng), mm(jAngTk, jLin), mv(jLinT, e.F), mv(jAngT, e.F));
+    return KIND_FULL;
+}
+
+AVBD_DEV M3 gs_ball_socket(int k, float3 v)
+{
+    float vk = comp(v, k);
+    float3 r0 = f3(-vk, 0, 0), r1 = f3(0, -vk, 0), r2 = f3(0, 0, -vk);
+    if (k == 0)
+    {
+        r0.x += v.x;
+        r1.x += v.y;
+        r2.x += v.z;
+    }
+    else if (k == 1)
+    {
+        r0.y += v.x;
+        r1.y += v.y;
+        r2.y += v.z;
+    }
+    else
+    {
+        r0.z += v.x;
+        r1.z += v.y;
+        r2.z += v.z;
+    }
+    return rows(r0, r1, r2);
+}
+
+// Joint rows (joint.cpp:56-123): part 0 = linear stamp, 1 = diagonalised geometric
+// stiffness added to lhsAng, 2 = angular stamp.
+AVBD_DEV unsigned joint_term(const DevBodies &B, const DevForces &F, unsigned j, int part, bool isA, float alpha,
+                             float *t)
+{
+    const float4 *d = F.joint + 8 * (size_t)j;
+    int2 ab = F.jointAB[j];
+    float4 d0 = d[0], d1 = d[1];
+    float3 pB = xyz(B.pos[ab.y]);
+    float4 qB = B.quat[ab.y];
+    const M3 I = rows(f3(1, 0, 0), f3(0, 1, 0), f3(0, 0, 1));
+    const M3 NI = rows(f3(-1, 0, 0), f3(0, -1, 0), f3(0, 0, -1));
+    if (part < 2)
+    {
+        float3 rA = xyz(d0), rB = xyz(d1);
+        float3 penLin = xyz(d[4]);
+        float3 rAW = ab.x >= 0 ? rotate(B.quat[ab.x], rA) : f3(0, 0, 0);
+        float3 rBW = rotate(qB, rB);
+        M3 K = diag(penLin.x, penLin.y, penLin.z);
+        float3 C = sub(ab.x >= 0 ? add(xyz(B.pos[ab.x]), rAW) : rA, add(pB, rBW));
+        if (isinf(d0.w))
+            C = sub(C, mul(xyz(d[2]), alpha));
+        float3 Fv = add(mv(K, C), xyz(d[6]));
+        if (part == 0)
+        {
+            M3 jLin = isA ? I : NI;
+            M3 jAng = isA ? skew(neg(rAW)) : skew(rBW);
+            M3 jLinT = trans(jLin), jAngT = trans(jAng);
+            M3 jAngTk = mm(jAngT, K);
+            store_terms(t, mm(mm(jLinT, K), jLin), mm(jAngTk, jAng), mm(jAngTk, jLin), mv(jLinT, Fv), mv(jAngT, Fv));
+            return KIND_FULL;
+        }
+        float3 r = isA ? rAW : neg(rBW);
+        M3 H = madd(madd(mscale(gs_ball_socket(0, r), Fv.x), mscale(gs_ball_socket(1, r), Fv.y)),
+                    mscale(gs_ball_socket(2, r), Fv.z));
+        M3 D = diagonalize(H);
+        t[E_LA00] = D.r0.x;
+        t[E_LA10] = D.r1.x;
+        t[E_LA11] = D.r1.y;
+        t[E_LA20] = D.r2.x;
+        t[E_LA21] = D.r2.y;
+        t[E_LA22] = D.r2.z;
+        return KIND_LHSANG;
+    }
+    float3 penAng = xyz(d[5]);
+    float torqueArm = d[3].w;
+    M3 K = diag(penAng.x, penAng.y, penAng.z);
+    float4 qa = ab.x >= 0 ? B.quat[ab.x] : make_float4(0, 0, 0, 1);
+    float3 C = mul(qdiff(qa, qB), torqueArm);
+    if (isinf(d1.w))
+        C = sub(C, mul(xyz(d[3]), alpha));
+    float3 Fv = add(mv(K, C), xyz(d[7]));
+    M3 jAng = mscale(isA ? I : NI, torqueArm);
+    M3 LA = mm(mm(trans(jAng), K), jAng);
+    float3 RA = mv(trans(jAng), Fv);
+    t[E_LA00] = LA.r0.x;
+    t[E_LA10] = LA.r1.x;
+    t[E_LA11] = LA.r1.y;
+    t[E_LA20] = LA.r2.x;
+    t[E_LA21] = LA.r2.y;
+    t[E_LA22] = LA.r2.z;
+    t[E_RA0] = RA.x;
+    t[E_RA1] = RA.y;
+    t[E_RA2] = RA.z;
+    return KIND_ANG;
+}
+
+// Spring row (spring.cpp:27-69)
+AVBD_DEV unsigned spring_term(const DevBodies &B, const DevForces &F, unsigned s, bool isA, float *t)
+{
+    const float4 *d = F.spring + 2 * (size_t)s;
+    int2 ab = F.springAB[s];
+    float4 d0 = d[0], d1 = d[1];
+    float3 rA = xyz(d0), rB = xyz(d1);
+    float rest = d0.w, stiffness = d1.w;
+    float4 qA = B.quat[ab.x], qB = B.quat[ab.y];
+    float3 pA = xform(xyz(B.pos[ab.x]), qA, rA);
+    float3 pB = xform(xyz(B.pos[ab.y]), qB, rB);
+    float3 dd = sub(pA, pB);
+    float dLen = len(dd);
+    if (dLen <= 1.0e-6f)
+        return KIND_NONE;
+    float3 n = divs(dd, dLen);
+    float C = dLen - rest;
+    float f = stiffness * C;
+    float3 jLin, jAng;
+    if (isA)
+    {
+        float3 rW = rotate(qA, rA);
+        jLin = n;
+        jAng = cross(rW, n);
+    }
+    else
+    {
+        float3 rW = rotate(qB, rB);
+        jLin = neg(n);
+        jAng = neg(cross(rW, n));
+    }
+    store_terms(t, mscale(outer(jLin, jLin), stiffness), mscale(outer(jAng, jAng), stiffness),
+                mscale(outer(jAng, jLin), stiffness), mul(jLin, f), mul(jAng, f));
+    return KIND_FULL;
+}
+
+AVBD_DEV int rows_of(const DevForces &F, unsigned e)
+{
+    if (e == ADJ_NONE)
+        return 0;
+    unsigned i = adj_index(e);
+    switch (adj_type(e))
+    {
+    case ADJ_MANIFOLD:
+        return F.man.n[i];
+    case ADJ_JOINT:
+    {
+        const float4 *d = F.joint + 8 * (size_t)i;
+        int r = lensq(xyz(d[4])) > 0 ? 2 : 0;
+        return r + (lensq(xyz(d[5])) > 0 ? 1 : 0);
+    }
+    case ADJ_SPRING:
+        return 1;
+    default:
+        return 0;
+    }
+}
+
+AVBD_DEV unsigned row_term(const DevBodies &B, const DevForces &F, unsigned e, int sub, float alpha, float *t)
+{
+    unsigned i = adj_index(e);
+    bool isA = adj_isA(e) != 0;
+    switch (adj_type(e))
+    {
+    case ADJ_MANIFOLD:
+        return contact_term(B, F, i, sub, isA, alpha, t);
+    case ADJ_JOINT:
+    {
+        const float4 *d = F.joint + 8 * (size_t)i;
+        bool lin = lensq(xyz(d[4])) > 0;
+        int part = lin ? sub : 2;
+        return joint_term(B, F, i, part, isA, alpha, t);
+    }
+    case ADJ_SPRING:
+        return spring_term(B, F, i, isA, t);
+    default:
+        return KIND_NONE;
+    }
+}
+
+// Initial system M/dt^2 (solver.cpp:1189-1198) as 27 entries
+AVBD_DEV void initial_system(const DevBodies &B, int b, float dt, float *t)
+{
+    float4 mm4 = B.massMoment[b];
+    M3 MLin = diag(mm4.x, mm4.x, mm4.x);
+    M3 MAng = diag(mm4.y, mm4.z, mm4.w);
+    float dt2 = dt * dt;
+    M3 lhsLin = mdivs(MLin, dt2);
+    M3 lhsAng = mdivs(MAng, dt2);
+    M3 lhsCross = diag(0, 0, 0);
+    float3 rhsLin = mv(mdivs(MLin, dt2), sub(xyz(B.pos[b]), xyz(B.inertLin[b])));
+    float3 rhsAng = mv(mdivs(MAng, dt2), qdiff(B.quat[b], B.inertAng[b]));
+    store_terms(t, lhsLin, lhsAng, lhsCross, rhsLin, rhsAng);
+}
+
+template <int G, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_primal(DevBodies B, DevForces F, Params P, const int *list, int first,
+                                                  int count)
+{
+    static_assert(BLOCK % G == 0 && 32 % G == 0, "group size");
+    constexpr int GPB = BLOCK / G;
+    constexpr int OWN = (E_COUNT + G - 1) / G;
+    __shared__ float sTerm[GPB][G][E_COUNT];
+    __shared__ unsigned sKind[GPB][G];
+    __shared__ unsigned sEnt[GPB][G];
+    __shared__ int sOff[GPB][G];
+
+    const int g = threadIdx.x / G;
+    const int lane = threadIdx.x % G;
+    const int gid = blockIdx.x * GPB + g;
+    if (gid >= count)
+        return;
+    const unsigned gmask = (G == 32) ? 0xFFFFFFFFu : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
+    const int b = list[first + gid];
+
+    if (lane == 0)
+        initial_system(B, b, P.dt, sTerm[g][0]);
+    __syncwarp(gmask);
+    float acc[OWN];
+#pragma unroll
+    for (int k = 0; k < OWN; ++k)
+    {
+        int e = lane + k * G;
+        acc[k] = e < E_COUNT ? sTerm[g][0][e] : 0.0f;
+    }
+    __syncwarp(gmask);
+
+    const int start = F.adjStart[b], end = F.adjStart[b + 1];
+    for (int base = start; base < end; base += G)
+    {
+        int k = base + lane;
+        unsigned ent = k < end ? F.adj[k] : ADJ_NONE;
+        int nr = rows_of(F, ent);
+        int incl = nr;
+#pragma unroll
+        for (int o = 1; o < G; o <<= 1)
+        {
+            int v = __shfl_up_sync(gmask, incl, o, G);
+            if (lane >= o)
+                incl += v;
+        }
+        int total = __shfl_sync(gmask, incl, G - 1, G);
+        sEnt[g][lane] = ent;
+        sOff[g][lane] = incl - nr;
+        __syncwarp(gmask);
+        for (int rb = 0; rb < total; rb += G)
+        {
+            int r = rb + lane;
+            if (r < total)
+            {
+                int j = G - 1;
+                while (sOff[g][j] > r)
+                    --j;
+                sKind[g][lane] = row_term(B, F, sEnt[g][j], r - sOff[g][j], P.alpha, sTerm[g][lane]);
+            }
+            __syncwarp(gmask);
+            int nrows = min(G, total - rb);
+            for (int rr = 0; rr < nrows; ++rr)
+            {
+                unsigned kind = sKind[g][rr];
+#pragma unroll
+                for (int kk = 0; kk < OWN; ++kk)
+                {
+                    int e = lane + kk * G;
+                    if (e < E_COUNT && ((kind >> e) & 1u))
+                        acc[kk] = acc[kk] + sTerm[g][rr][e];
+                }
+            }
+            __syncwarp(gmask);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < OWN; ++k)
+    {
+        int e = lane + k * G;
+        if (e < E_COUNT)
+            sTerm[g][0][e] = acc[k];
+    }
+    __syncwarp(gmask);
+    if (lane == 0)
+    {
+        float3 dxl, dxa;
+        ldl_solve27(sTerm[g][0], dxl, dxa);
+        B.pos[b] = f4(add(xyz(B.pos[b]), dxl), 0.0f);
+        B.quat[b] = qstep(B.quat[b], dxa);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Dual (solver.cpp:1244-1271)
+// ---------------------------------------------------------------------------
+
+// Manifold::updateDual per contact slot (manifold.cpp:231-280)
+__global__ void k_dual_contacts(DevBodies B, DevManifolds M, int nMan, Params P)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int m = t >> 3, ci = t & 7;
+    if (m >= nMan || ci >= M.n[m])
+        return;
+    int2 ab = M.ab[m];
+    Pose A = load_pose(B, ab.x), Bp = load_pose(B, ab.y);
+    const float4 *bs = M.basis + 3 * (size_t)m;
+    float4 b0 = bs[0];
+    M3 basis = rows(xyz(b0), xyz(bs[1]), xyz(bs[2]));
+    float4 *cp = M.contact + (size_t)m * 32 + 4 * ci;
+    ContactRec c = load_contact(cp);
+    ContactEval e = eval_contact(A, Bp, basis, b0.w, c, P.alpha);
+    c.lam = e.F;
+    if (e.F.x < 0)
+        c.pen.x = rmin(c.pen.x + P.betaLin * fabsf(e.C.x), PENALTY_MAX);
+    if (e.fs <= e.bounds)
+    {
+        c.pen.y = rmin(c.pen.y + P.betaLin * fabsf(e.C.y), PENALTY_MAX);
+        c.pen.z = rmin(c.pen.z + P.betaLin * fabsf(e.C.z), PENALTY_MAX);
+        c.stick = sqrtf(e.C.y * e.C.y + e.C.z * e.C.z) < STICK_THRESH;
+    }
+    cp[2] = make_float4(c.C0.z, c.pen.x, c.pen.y, c.pen.z);
+    cp[3] = make_float4(c.lam.x, c.lam.y, c.lam.z, __uint_as_float((unsigned)c.key | (c.stick ? 0x80000000u : 0u)));
+}
+
+// Joint::updateDual with fracture (joint.cpp:125-182)
+__global__ void k_dual_joints(DevBodies B, DevForces F, Params P)
+{
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= F.nJoint)
+        return;
+    float4 *d = F.joint + 8 * (size_t)j;
+    int2 ab = F.jointAB[j];
+    float4 d0 = d[0], d1 = d[1];
+    float3 penLin = xyz(d[4]), penAng = xyz(d[5]);
+    float3 lamLin = xyz(d[6]), lamAng = xyz(d[7]);
+    float brokenFlag = d[4].w;
+    float3 pB = xyz(B.pos[ab.y]);
+    float4 qB = B.quat[ab.y];
+    if (lensq(penLin) > 0)
+    {
+        M3 K = diag(penLin.x, penLin.y, penLin.z);
+        float3 pa = ab.x >= 0 ? xform(xyz(B.pos[ab.x]), B.quat[ab.x], xyz(d0)) : xyz(d0);
+        float3 C = sub(pa, xform(pB, qB, xyz(d1)));
+        if (isinf(d0.w))
+        {
+            C = sub(C, mul(xyz(d[2]), P.alpha));
+            lamLin = add(mv(K, C), lamLin);
+        }
+        penLin = minv(add(penLin, mul(absv(C), P.betaLin)), rmin(d0.w, PENALTY_MAX));
+    }
+    if (lensq(penAng) > 0)
+    {
+        M3 K = diag(penAng.x, penAng.y, penAng.z);
+        float4 qa = ab.x >= 0 ? B.quat[ab.x] : make_float4(0, 0, 0, 1);
+        float3 C = mul(qdiff(qa, qB), d[3].w);
+        if (isinf(d1.w))
+        {
+            C = sub(C, mul(xyz(d[3]), P.alpha));
+            lamAng = add(mv(K, C), lamAng);
+        }
+        penAng = minv(add(penAng, mul(absv(C), P.betaAng)), rmin(d1.w, PENALTY_MAX));
+    }
+    float fracture = d[2].w;
+    if (lensq(lamAng) > fracture * fracture)
+    {
+        penLin = f3(0, 0, 0);
+        penAng = f3(0, 0, 0);
+        lamLin = f3(0, 0, 0);
+        lamAng = f3(0, 0, 0);
+        brokenFlag = 1.0f;
+    }
+    d[4] = f4(penLin, brokenFlag);
+    d[5] = f4(penAng, 0.0f);
+    d[6] = f4(lamLin, 0.0f);
+    d[7] = f4(lamAng, 0.0f);
+}
+
+} // namespace avbd

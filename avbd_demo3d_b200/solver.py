@@ -1,0 +1,423 @@
+"""Host side of the CUDA AVBD step, mirroring the reference's interfaces.
+
+``World`` owns one device context (include/avbd_cuda.h) holding a scene; it is what the
+benchmark and the parity tests drive. ``Solver``, ``Rigid``, ``Joint``, ``Spring``,
+``IgnoreCollision`` and ``CudaAvbdBackend`` mirror the reference's C++ classes
+(source/solver.h:197-417) with the same constructor arguments and parameter names, so a
+scene is built the way source/scenes.h builds it and ``solver.step()`` runs the GPU step.
+
+Derived quantities (mass, moment, bounding radius, joint torque arm, spring rest
+length) are computed in float32 with the reference's operation order
+(rigid.cpp:34-40, joint.cpp:33, spring.cpp:18-24), so the device starts from the same
+bits the reference would hold.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib
+from . import scenes as _scenes
+
+F32 = np.float32
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _c(a, dtype, shape=None):
+    a = np.ascontiguousarray(np.asarray(a, dtype=dtype))
+    return a if shape is None else a.reshape(shape)
+
+
+# ---------------------------------------------------------------------------
+# float32 arithmetic in the reference's order
+# ---------------------------------------------------------------------------
+
+
+def _cross32(a, b):
+    return np.stack([a[..., 1] * b[..., 2] - a[..., 2] * b[..., 1],
+                     a[..., 2] * b[..., 0] - a[..., 0] * b[..., 2],
+                     a[..., 0] * b[..., 1] - a[..., 1] * b[..., 0]], axis=-1)
+
+
+def rotate32(q: np.ndarray, v: np.ndarray) -> np.ndarray:
+    """rotate(q, v) = v + t*w + cross(u, t), t = 2 cross(u, v)   (maths.h:441-446)"""
+    q = np.asarray(q, F32)
+    v = np.asarray(v, F32)
+    u = q[..., :3]
+    t = _cross32(u, v) * F32(2.0)
+    return (v + t * q[..., 3:4]) + _cross32(u, t)
+
+
+def _dot32(a, b):
+    return (a[..., 0] * b[..., 0] + a[..., 1] * b[..., 1]) + a[..., 2] * b[..., 2]
+
+
+def box_properties(size: np.ndarray, density: np.ndarray):
+    """Mass, moment and bounding radius of boxes (rigid.cpp:34-40)."""
+    s = np.asarray(size, F32).reshape(-1, 3)
+    d = np.asarray(density, F32).reshape(-1)
+    mass = ((s[:, 0] * s[:, 1]) * s[:, 2]) * d
+    twelve = F32(12.0)
+    moment = np.stack([(s[:, 1] * s[:, 1] + s[:, 2] * s[:, 2]) / twelve * mass,
+                       (s[:, 0] * s[:, 0] + s[:, 2] * s[:, 2]) / twelve * mass,
+                       (s[:, 0] * s[:, 0] + s[:, 1] * s[:, 1]) / twelve * mass], axis=1)
+    h = s * F32(0.5)
+    radius = np.sqrt(_dot32(h, h))
+    return mass.astype(F32), moment.astype(F32), radius.astype(F32)
+
+
+# ---------------------------------------------------------------------------
+# Device world
+# ---------------------------------------------------------------------------
+
+
+class World:
+    """A scene resident on one GPU. Body arrays are in list order (index 0 = newest body,
+    the head of the reference's Solver::bodies)."""
+
+    def __init__(self, scene: _scenes.Scene, device: int = 0, stream: int | None = None):
+        self.lib = _lib.load()
+        self.h = ctypes.c_void_p()
+        rc = self.lib.avbd_create(ctypes.byref(self.h), device, stream)
+        if rc != _lib.AVBD_OK:
+            raise _lib.AvbdError(f"avbd_create failed ({rc}); is a CUDA device present?")
+        self.scene = scene
+        self.n = scene.n_bodies
+        self.set_params(scene.params)
+        self._load(scene)
+
+    # -- helpers
+    def _check(self, rc: int, what: str):
+        if rc != _lib.AVBD_OK:
+            msg = self.lib.avbd_last_error(self.h).decode(errors="replace")
+            raise _lib.AvbdError(f"{what} failed ({_lib.ERRORS.get(rc, rc)}): {msg}")
+
+    def close(self):
+        if self.h:
+            self.lib.avbd_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, p):
+        self.params = _lib.AvbdParams(p.dt, p.gravity, p.iterations, p.alpha, p.betaLin, p.betaAng, p.gamma,
+                                      p.broadphase)
+        self._check(self.lib.avbd_set_params(self.h, ctypes.byref(self.params)), "avbd_set_params")
+
+    @staticmethod
+    def list_order(a):
+        """Creation order -> list order (the reference prepends every new body)."""
+        return np.ascontiguousarray(a[::-1])
+
+    def _load(self, sc: _scenes.Scene):
+        n = sc.n_bodies
+        mass, moment, radius = box_properties(sc.size, sc.density)
+        L = self.list_order
+        self._body_arrays = dict(
+            position3=L(sc.pos), orientation4=L(sc.quat), velocity3=L(sc.vel), angular3=np.zeros((n, 3), F32),
+            prev_velocity3=L(sc.vel), size3=L(sc.size), mass=L(mass), moment3=L(moment), friction=L(sc.friction),
+            radius=L(radius))
+        self.props = {"mass": self._body_arrays["mass"], "moment": self._body_arrays["moment3"],
+                      "radius": self._body_arrays["radius"], "size": self._body_arrays["size3"],
+                      "friction": self._body_arrays["friction"]}
+        bodies = _lib.AvbdBodies(n, *[_ptr(self._body_arrays[k]) for k in (
+            "position3", "orientation4", "velocity3", "angular3", "prev_velocity3", "size3", "mass", "moment3",
+            "friction", "radius")])
+        # forces: creation index -> list index, sequence numbers in creation order
+        to_list = lambda c: np.where(c >= 0, n - 1 - c, -1).astype(np.int32)
+        seq = np.arange(sc.n_forces, dtype=np.int64)
+        fa, fb = to_list(sc.fa), to_list(sc.fb)
+        jm = sc.ftype == _scenes.FORCE_JOINT
+        sm = sc.ftype == _scenes.FORCE_SPRING
+        im = sc.ftype == _scenes.FORCE_IGNORE
+        lp = self._body_arrays["position3"]
+        lq = self._body_arrays["orientation4"]
+        lsize = self._body_arrays["size3"]
+        # joints (joint.cpp:25-33): torqueArm = lengthSq(sizeA + sizeB)
+        J = int(jm.sum())
+        j_ab = _c(np.stack([fa[jm], fb[jm]], axis=1), np.int32, (J, 2))
+        j_state = np.zeros((J, 28), F32)
+        if J:
+            sa = np.where((fa[jm] >= 0)[:, None], lsize[np.maximum(fa[jm], 0)], F32(0.0)).astype(F32)
+            ssum = sa + lsize[fb[jm]]
+            j_state[:, 0:3] = sc.frA[jm]
+            j_state[:, 3:6] = sc.frB[jm]
+            j_state[:, 24] = sc.fparam[jm][:, 0]
+            j_state[:, 25] = sc.fparam[jm][:, 1]
+            j_state[:, 26] = sc.fparam[jm][:, 2]
+            j_state[:, 27] = _dot32(ssum, ssum)
+        # springs (spring.cpp:14-25): rest < 0 -> initial distance of the anchor points
+        S = int(sm.sum())
+        s_ab = _c(np.stack([fa[sm], fb[sm]], axis=1), np.int32, (S, 2))
+        s_state = np.zeros((S, 8), F32)
+        if S:
+            a, b = fa[sm], fb[sm]
+            rA, rB = sc.frA[sm], sc.frB[sm]
+            pA = rotate32(lq[a], rA) + lp[a]
+            pB = rotate32(lq[b], rB) + lp[b]
+            d = pA - pB
+            dist = np.sqrt(_dot32(d, d))
+            rest = sc.fparam[sm][:, 1].copy()
+            rest = np.where(rest < 0, dist, rest).astype(F32)
+            s_state[:, 0:3] = rA
+            s_state[:, 3:6] = rB
+            s_state[:, 6] = rest
+            s_state[:, 7] = sc.fparam[sm][:, 0]
+        I = int(im.sum())
+        i_ab = _c(np.stack([fa[im], fb[im]], axis=1), np.int32, (I, 2))
+        self._force_arrays = dict(j_ab=j_ab, j_seq=_c(seq[jm], np.int64), j_state=j_state,
+                                  j_broken=np.zeros(J, np.int32), s_ab=s_ab, s_seq=_c(seq[sm], np.int64),
+                                  s_state=s_state, i_ab=i_ab, i_seq=_c(seq[im], np.int64))
+        fa_ = self._force_arrays
+        joints = _lib.AvbdJoints(J, _ptr(fa_["j_ab"]), _ptr(fa_["j_seq"]), _ptr(fa_["j_state"]), _ptr(fa_["j_broken"]))
+        springs = _lib.AvbdSprings(S, _ptr(fa_["s_ab"]), _ptr(fa_["s_seq"]), _ptr(fa_["s_state"]))
+        ignores = _lib.AvbdIgnores(I, _ptr(fa_["i_ab"]), _ptr(fa_["i_seq"]))
+        manifolds = _lib.AvbdManifolds(0)
+        self._check(self.lib.avbd_load_world(self.h, ctypes.byref(bodies), ctypes.byref(joints), ctypes.byref(springs),
+                                             ctypes.byref(ignores), ctypes.byref(manifolds), sc.n_forces),
+                    "avbd_load_world")
+
+    # -- stepping
+    def step(self, n: int = 1, sync: bool = True):
+        self._check(self.lib.avbd_step(self.h, n), "avbd_step")
+        if sync:
+            self.synchronize()
+
+    def synchronize(self):
+        self._check(self.lib.avbd_synchronize(self.h), "avbd_synchronize")
+
+    # -- readback
+    def bodies(self, aux: bool = False) -> dict:
+        n = self.n
+        out = {"pos": np.zeros((n, 3), F32), "quat": np.zeros((n, 4), F32), "vel": np.zeros((n, 3), F32),
+               "angvel": np.zeros((n, 3), F32), "prevvel": np.zeros((n, 3), F32)}
+        if aux:
+            out.update(init_lin=np.zeros((n, 3), F32), init_ang=np.zeros((n, 4), F32),
+                       inert_lin=np.zeros((n, 3), F32), inert_ang=np.zeros((n, 4), F32))
+        st = _lib.AvbdBodyState(*[_ptr(out.get(k)) for k in (
+            "pos", "quat", "vel", "angvel", "prevvel", "init_lin", "init_ang", "inert_lin", "inert_ang")])
+        self._check(self.lib.avbd_read_bodies(self.h, ctypes.byref(st)), "avbd_read_bodies")
+        return out
+
+    def write_bodies(self, pos=None, quat=None, vel=None, angvel=None, prevvel=None):
+        """Overwrite body state (list order) between steps."""
+        cur = self.bodies()
+        arr = dict(position3=_c(cur["pos"] if pos is None else pos, F32),
+                   orientation4=_c(cur["quat"] if quat is None else quat, F32),
+                   velocity3=_c(cur["vel"] if vel is None else vel, F32),
+                   angular3=_c(cur["angvel"] if angvel is None else angvel, F32),
+                   prev_velocity3=_c(cur["prevvel"] if prevvel is None else prevvel, F32))
+        b = _lib.AvbdBodies(self.n, _ptr(arr["position3"]), _ptr(arr["orientation4"]), _ptr(arr["velocity3"]),
+                            _ptr(arr["angular3"]), _ptr(arr["prev_velocity3"]), None, None, None, None, None)
+        self._check(self.lib.avbd_write_bodies(self.h, ctypes.byref(b)), "avbd_write_bodies")
+
+    def manifolds(self) -> dict:
+        m = ctypes.c_int32()
+        self._check(self.lib.avbd_num_manifolds(self.h, ctypes.byref(m)), "avbd_num_manifolds")
+        m = m.value
+        out = {"ab": np.zeros((m, 2), np.int32), "seq": np.zeros(m, np.int64), "n": np.zeros(m, np.int32),
+               "basis": np.zeros((m, 9), F32), "friction": np.zeros(m, F32), "keys": np.zeros((m, 8), np.int32),
+               "contact": np.zeros((m, 8, 15), F32), "stick": np.zeros((m, 8), np.int32)}
+        o = _lib.AvbdManifoldsOut(*[_ptr(out[k]) for k in ("ab", "seq", "n", "basis", "friction", "keys", "contact",
+                                                            "stick")])
+        self._check(self.lib.avbd_read_manifolds(self.h, ctypes.byref(o)), "avbd_read_manifolds")
+        return out
+
+    def joints(self) -> dict:
+        m = ctypes.c_int32()
+        self._check(self.lib.avbd_num_joints(self.h, ctypes.byref(m)), "avbd_num_joints")
+        m = m.value
+        out = {"ab": np.zeros((m, 2), np.int32), "seq": np.zeros(m, np.int64), "state28": np.zeros((m, 28), F32),
+               "broken": np.zeros(m, np.int32)}
+        o = _lib.AvbdJointsOut(_ptr(out["ab"]), _ptr(out["seq"]), _ptr(out["state28"]), _ptr(out["broken"]))
+        self._check(self.lib.avbd_read_joints(self.h, ctypes.byref(o)), "avbd_read_joints")
+        # same 18-float view as the checkers: C0Lin C0Ang penLin penAng lamLin lamAng
+        out["state"] = np.ascontiguousarray(out["state28"][:, 6:24])
+        return out
+
+    def colours(self):
+        c = np.zeros(max(self.n, 1), np.int32)
+        nc = ctypes.c_int32()
+        self._check(self.lib.avbd_read_colours(self.h, c.ctypes.data_as(_lib.c_int_p), ctypes.byref(nc)),
+                    "avbd_read_colours")
+        return c[:self.n], nc.value
+
+    def solve_order(self) -> np.ndarray:
+        o = np.zeros(max(self.n, 1), np.int32)
+        k = ctypes.c_int32()
+        self._check(self.lib.avbd_read_solve_order(self.h, o.ctypes.data_as(_lib.c_int_p), ctypes.byref(k)),
+                    "avbd_read_solve_order")
+        return o[:k.value].copy()
+
+    def set_profiling(self, on: bool = True):
+        self._check(self.lib.avbd_set_profiling(self.h, 1 if on else 0), "avbd_set_profiling")
+
+    def reset_profile(self):
+        self._check(self.lib.avbd_reset_profile(self.h), "avbd_reset_profile")
+
+    def profile(self) -> dict:
+        p = _lib.AvbdProfile()
+        self._check(self.lib.avbd_read_profile(self.h, ctypes.byref(p)), "avbd_read_profile")
+        out = {"steps": p.steps, "launches": p.launches}
+        for k, name in enumerate(_lib.PHASES):
+            out[name + "_ms"] = p.phase_ms[k]
+            out[name + "_spans"] = p.phase_spans[k]
+        return out
+
+    def stats(self) -> dict:
+        s = _lib.AvbdStats()
+        self._check(self.lib.avbd_get_stats(self.h, ctypes.byref(s)), "avbd_get_stats")
+        return {k: getattr(s, k) for k, _ in s._fields_}
+
+
+# ---------------------------------------------------------------------------
+# Mirror of the reference's object interface (solver.h)
+# ---------------------------------------------------------------------------
+
+
+class Rigid:
+    """``Rigid(solver, size, density, friction, position, velocity)`` (solver.h:221). After a
+    step its state reads from the device world."""
+
+    def __init__(self, solver: "Solver", size, density, friction, position, velocity=(0, 0, 0)):
+        self.solver = solver
+        self.creation = solver._builder.body(size, density, friction, position, velocity)
+        solver._topology_changed()
+
+    @property
+    def index(self) -> int:
+        """Position in the solver's body list (0 = newest)."""
+        return self.solver._n_bodies() - 1 - self.creation
+
+    def _state(self, key):
+        st = self.solver._state()
+        if st is None:
+            b = self.solver._builder.b
+            return {"pos": b["pos"], "quat": b["quat"], "vel": b["vel"]}[key][self.creation]
+        return st[key][self.index]
+
+    @property
+    def positionLin(self):
+        return self._state("pos")
+
+    @property
+    def positionAng(self):
+        return self._state("quat")
+
+    @positionAng.setter
+    def positionAng(self, q):
+        if self.solver._world is not None:
+            raise RuntimeError("orientation edits after the first step go through World.write_bodies")
+        self.solver._builder.b["quat"][self.creation] = np.asarray(q, F32).reshape(4)
+
+    @property
+    def velocityLin(self):
+        return self._state("vel")
+
+
+class Joint:
+    """``Joint(solver, bodyA, bodyB, rA, rB, stiffnessLin=INFINITY, stiffnessAng=0, fracture=INFINITY)``
+    (solver.h:252-267); bodyA None anchors bodyB to the world point rA."""
+
+    def __init__(self, solver, bodyA, bodyB, rA, rB, stiffnessLin=math.inf, stiffnessAng=0.0, fracture=math.inf):
+        solver._builder.joint(None if bodyA is None else bodyA.creation, bodyB.creation, rA, rB, stiffnessLin,
+                              stiffnessAng, fracture)
+        solver._topology_changed()
+
+
+class Spring:
+    """``Spring(solver, bodyA, bodyB, rA, rB, stiffness, rest=-1)`` (solver.h:270-281)."""
+
+    def __init__(self, solver, bodyA, bodyB, rA, rB, stiffness, rest=-1.0):
+        solver._builder.spring(bodyA.creation, bodyB.creation, rA, rB, stiffness, rest)
+        solver._topology_changed()
+
+
+class IgnoreCollision:
+    """``IgnoreCollision(solver, bodyA, bodyB)`` (solver.h:284-291)."""
+
+    def __init__(self, solver, bodyA, bodyB):
+        solver._builder.ignore_collision(bodyA.creation, bodyB.creation)
+        solver._topology_changed()
+
+
+class CudaAvbdBackend:
+    """The ``PhysicsBackend`` (solver.h:410-417) that runs ``Solver::step`` on the GPU."""
+
+    def __init__(self, device: int = 0):
+        self.device = device
+
+    def name(self) -> str:
+        return _lib.load().avbd_backend_name().decode()
+
+    def step(self, solver: "Solver"):
+        if solver._world is None:
+            solver._world = World(solver._scene(), self.device)
+        else:
+            solver._world.set_params(solver._params())
+        solver._world.step(1)
+        solver._cached = None
+
+
+class Solver:
+    """``Solver`` (solver.h:346-408): parameters, scene construction, ``step()``."""
+
+    def __init__(self, device: int = 0):
+        self.physicsBackend = CudaAvbdBackend(device)
+        self.broadphaseMode = _scenes.BROADPHASE_GRID
+        self.clear()
+        self.defaultParams()
+
+    def defaultParams(self):
+        """solver.cpp:909-932"""
+        self.dt = float(F32(1.0) / F32(60.0))
+        self.gravity = -10.0
+        self.iterations = 10
+        self.betaLin = 10000.0
+        self.betaAng = 100.0
+        self.alpha = 0.99
+        self.gamma = 0.999
+
+    def clear(self):
+        self._builder = _scenes.SceneBuilder("solver", _scenes.Params())
+        self._world = None
+        self._cached = None
+
+    def _params(self):
+        return _scenes.Params(self.dt, self.gravity, self.iterations, self.alpha, self.betaLin, self.betaAng,
+                              self.gamma, self.broadphaseMode)
+
+    def _scene(self):
+        self._builder.params = self._params()
+        return self._builder.build()
+
+    def _topology_changed(self):
+        if self._world is not None:
+            raise RuntimeError("adding bodies or forces after the first step needs a reload: call clear()")
+
+    def _n_bodies(self):
+        return len(self._builder.b["size"])
+
+    def _state(self):
+        if self._world is None:
+            return None
+        if self._cached is None:
+            self._cached = self._world.bodies()
+        return self._cached
+
+    def step(self):
+        """Solver::step -> physicsBackend->step(*this) (solver.cpp:934-937)."""
+        self.physicsBackend.step(self)
+
+    @property
+    def world(self) -> World | None:
+        return self._world

@@ -1,0 +1,261 @@
+/*
+ * avbd_cuda.h -- C ABI of the B200 (sm_100a) AVBD step.
+ *
+ * The library replaces what runs under the reference's physics-backend seam:
+ *   struct PhysicsBackend { virtual const char *name() const; virtual void step(Solver &); }
+ *   (ts-jls/avbd-demo3d source/solver.h:410-417), installed as Solver::physicsBackend
+ *   (solver.h:360) and called from Solver::step (solver.cpp:934-937).
+ * One avbd_step() call performs what Solver::stepCpuReference does
+ * (solver.cpp:1036-1041): broadphase, manifold creation and narrowphase, force
+ * initialisation and warm start, body warm start, the primal/dual iterations and
+ * the velocity update. Everything runs on the GPU; there is no CPU fallback.
+ *
+ * Conventions
+ *  - Body index = position in the reference's Solver::bodies list (0 = list head =
+ *    newest body). Forces carry a creation sequence number: a larger number is a
+ *    newer force (the reference keeps per-body force lists newest first,
+ *    force.cpp:25-36, and sums constraint rows in that order).
+ *  - All functions return 0 on success or a negative AVBD_ERR_* code; the text of
+ *    the last error is available from avbd_last_error(). Failures latch: after an
+ *    error the context refuses to step until avbd_clear_error().
+ *  - A context is single-threaded and bound to one device and one CUDA stream.
+ *  - Floats are FP32 throughout, with the reference's operation order, so results
+ *    are bit-identical to the reference CPU solver run in the same body order.
+ */
+#ifndef AVBD_CUDA_H
+#define AVBD_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AVBD_OK 0
+#define AVBD_ERR_ARGUMENT -1
+#define AVBD_ERR_CUDA -2
+#define AVBD_ERR_CAPACITY -3
+#define AVBD_ERR_STATE -4
+#define AVBD_ERR_LATCHED -5
+
+#define AVBD_BROADPHASE_ALL_PAIRS 0
+#define AVBD_BROADPHASE_GRID 1
+#define AVBD_BROADPHASE_SAP 2
+
+#define AVBD_FORCE_MANIFOLD 0
+#define AVBD_FORCE_JOINT 1
+#define AVBD_FORCE_SPRING 2
+#define AVBD_FORCE_IGNORE 3
+
+typedef struct AvbdContext AvbdContext;
+
+/* Solver parameters: Solver::dt, gravity, iterations, alpha, betaLin, betaAng, gamma,
+ * broadphaseMode (solver.h:348-366). */
+typedef struct AvbdParams
+{
+    float dt;
+    float gravity;
+    int32_t iterations;
+    float alpha;
+    float betaLin;
+    float betaAng;
+    float gamma;
+    int32_t broadphase;
+} AvbdParams;
+
+/* Rigid state and properties (Rigid, solver.h:197-228), arrays of n entries in list order.
+ * position3/velocity3/angular3/prev_velocity3/size3/moment3 hold 3 floats per body,
+ * orientation4 holds x, y, z, w. Boxes only (RigidShape::type == RIGID_SHAPE_BOX). */
+typedef struct AvbdBodies
+{
+    int32_t count;
+    const float *position3;
+    const float *orientation4;
+    const float *velocity3;
+    const float *angular3;
+    const float *prev_velocity3;
+    const float *size3;
+    const float *mass;
+    const float *moment3;
+    const float *friction;
+    const float *radius;
+} AvbdBodies;
+
+/* Body state written back after a step. Any pointer may be NULL to skip that field. */
+typedef struct AvbdBodyState
+{
+    float *position3;
+    float *orientation4;
+    float *velocity3;
+    float *angular3;
+    float *prev_velocity3;
+    float *initial_position3;
+    float *initial_orientation4;
+    float *inertial_position3;
+    float *inertial_orientation4;
+} AvbdBodyState;
+
+/* Joints (Joint, solver.h:252-267). body_a may be -1 (anchored to world point rA).
+ * state28 per joint: rA[3] rB[3] C0Lin[3] C0Ang[3] penaltyLin[3] penaltyAng[3]
+ * lambdaLin[3] lambdaAng[3] stiffnessLin stiffnessAng fracture torqueArm. */
+typedef struct AvbdJoints
+{
+    int32_t count;
+    const int32_t *body_ab2;
+    const int64_t *seq;
+    const float *state28;
+    const int32_t *broken;
+} AvbdJoints;
+
+/* Springs (Spring, solver.h:270-281). state8: rA[3] rB[3] rest stiffness. */
+typedef struct AvbdSprings
+{
+    int32_t count;
+    const int32_t *body_ab2;
+    const int64_t *seq;
+    const float *state8;
+} AvbdSprings;
+
+/* IgnoreCollision pairs (solver.h:284-291). */
+typedef struct AvbdIgnores
+{
+    int32_t count;
+    const int32_t *body_ab2;
+    const int64_t *seq;
+} AvbdIgnores;
+
+/* Manifolds (Manifold, solver.h:294-334). Per manifold: bodies, sequence number, contact
+ * count, basis (3 rows of 3), friction; per contact slot (8 per manifold): feature key,
+ * contact15 = rA[3] rB[3] C0[3] penalty[3] lambda[3], stick flag. */
+typedef struct AvbdManifolds
+{
+    int32_t count;
+    const int32_t *body_ab2;
+    const int64_t *seq;
+    const int32_t *num_contacts;
+    const float *basis9;
+    const float *friction;
+    const int32_t *keys8;
+    const float *contact15x8;
+    const int32_t *stick8;
+} AvbdManifolds;
+
+/* Writable views for readback (same layouts). */
+typedef struct AvbdManifoldsOut
+{
+    int32_t *body_ab2;
+    int64_t *seq;
+    int32_t *num_contacts;
+    float *basis9;
+    float *friction;
+    int32_t *keys8;
+    float *contact15x8;
+    int32_t *stick8;
+} AvbdManifoldsOut;
+
+typedef struct AvbdJointsOut
+{
+    int32_t *body_ab2;
+    int64_t *seq;
+    float *state28;
+    int32_t *broken;
+} AvbdJointsOut;
+
+/* Per-step counters, in the spirit of SolverStats (solver.h:121-188). */
+typedef struct AvbdStats
+{
+    int64_t body_count;
+    int64_t pair_checks;
+    int64_t sphere_hits;
+    int64_t constrained_hits;
+    int64_t manifolds_created;
+    int64_t manifold_count;
+    int64_t contact_count;
+    int64_t joint_count;
+    int64_t spring_count;
+    int64_t solved_bodies;
+    int64_t colours;
+    int64_t colour_rounds;
+    int64_t primal_rows;
+    float step_ms;
+} AvbdStats;
+
+/* Context lifetime. Replaces constructing a backend for Solver::physicsBackend
+ * (makeCpuReferencePhysicsBackend, solver.cpp:676-680). stream may be NULL (the
+ * context creates its own). */
+int avbd_create(AvbdContext **out, int32_t device_ordinal, void *cuda_stream);
+void avbd_destroy(AvbdContext *ctx);
+const char *avbd_last_error(const AvbdContext *ctx);
+void avbd_clear_error(AvbdContext *ctx);
+/* PhysicsBackend::name() (solver.h:413). */
+const char *avbd_backend_name(void);
+
+/* Solver parameters (Solver::dt .. broadphaseMode, solver.h:348-366). */
+int avbd_set_params(AvbdContext *ctx, const AvbdParams *params);
+
+/* Full world upload: replaces the device world (scene load, topology edits between
+ * steps such as the drag joint of simulation_host.cpp:242-274). next_seq is the
+ * sequence number the next created manifold receives (greater than every seq given). */
+int avbd_load_world(AvbdContext *ctx, const AvbdBodies *bodies, const AvbdJoints *joints,
+                    const AvbdSprings *springs, const AvbdIgnores *ignores, const AvbdManifolds *manifolds,
+                    int64_t next_seq);
+
+/* Overwrite body state only (positions/orientations/velocities edited between steps,
+ * e.g. scenes.h:45). Same layout and order as avbd_load_world's bodies. */
+int avbd_write_bodies(AvbdContext *ctx, const AvbdBodies *bodies);
+
+/* Solver::step() for nsteps steps (solver.cpp:934-937 via stepCpuReference 1036-1041).
+ * Asynchronous on the context stream; returns after launch except where the step
+ * needs a device count (buffer growth). */
+int avbd_step(AvbdContext *ctx, int32_t nsteps);
+/* Wait for the context stream. */
+int avbd_synchronize(AvbdContext *ctx);
+
+/* Post-step readback (the contract of readbackAndApply, avbd_gpu_solver.cpp:1970-2022). */
+int avbd_read_bodies(AvbdContext *ctx, const AvbdBodyState *out);
+int avbd_num_manifolds(AvbdContext *ctx, int32_t *count);
+int avbd_read_manifolds(AvbdContext *ctx, const AvbdManifoldsOut *out);
+int avbd_num_joints(AvbdContext *ctx, int32_t *count);
+int avbd_read_joints(AvbdContext *ctx, const AvbdJointsOut *out);
+int avbd_next_seq(AvbdContext *ctx, int64_t *next_seq);
+
+/* Parity dumps: colour per body of the last step (-1 = not solved) and colour count;
+ * the primal sweep order (bodies grouped by colour). */
+int avbd_read_colours(AvbdContext *ctx, int32_t *colour, int32_t *num_colours);
+int avbd_read_solve_order(AvbdContext *ctx, int32_t *order, int32_t *count);
+int avbd_get_stats(AvbdContext *ctx, AvbdStats *stats);
+
+/* Device pointers of the resident body pose arrays (float4 xyz_ / xyzw per body) for
+ * callers that keep data on the GPU. */
+int avbd_device_pose(AvbdContext *ctx, void **position4, void **orientation4);
+
+/* Per-phase GPU time, the counterpart of SolverStats' phase timers (broadphaseMs,
+ * forceInitMs, bodyInitMs, primalSolveMs, dualUpdateMs, velocityUpdateMs; solver.h:121-188),
+ * measured with CUDA events on the context stream. Profiling adds one stream sync per step. */
+#define AVBD_PHASE_BROADPHASE 0
+#define AVBD_PHASE_FORCE_INIT 1
+#define AVBD_PHASE_ADJACENCY 2
+#define AVBD_PHASE_BODY_INIT 3
+#define AVBD_PHASE_COLOURING 4
+#define AVBD_PHASE_PRIMAL 5
+#define AVBD_PHASE_DUAL 6
+#define AVBD_PHASE_VELOCITY 7
+#define AVBD_PHASE_COUNT 8
+
+typedef struct AvbdProfile
+{
+    int64_t steps;                         /* steps profiled since the last reset */
+    double phase_ms[AVBD_PHASE_COUNT];     /* summed GPU time per phase */
+    int64_t phase_spans[AVBD_PHASE_COUNT]; /* timed spans per phase (primal: one per launch) */
+    int64_t launches;                      /* kernel launch calls issued (a library sort/scan call counts once) */
+} AvbdProfile;
+
+int avbd_set_profiling(AvbdContext *ctx, int32_t enable);
+int avbd_read_profile(AvbdContext *ctx, AvbdProfile *out);
+int avbd_reset_profile(AvbdContext *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -102,6 +102,9 @@ struct AvbdContext
     DArr<StepCounters> counters;
     StepCounters *hCounters = nullptr;
     long long *hScalars = nullptr; // pinned scratch for small readbacks
+    float4 *hStage = nullptr;      // pinned staging for body state transfers
+    size_t hStageCap = 0;
+    cudaEvent_t stageDone = nullptr; // staging copies issued before this event are complete
 
     long long nextSeq = 0;
     AvbdStats stats{};
@@ -232,7 +235,7 @@ struct PhaseScope
 
 int prof_collect(AvbdContext *ctx)
 {
-    if (!ctx->profiling)
+    if (ctx->marks.empty())
         return AVBD_OK;
     CU(cudaStreamSynchronize(ctx->stream));
     for (auto &m : ctx->marks)
@@ -244,7 +247,6 @@ int prof_collect(AvbdContext *ctx)
     }
     ctx->marks.clear();
     ctx->evUsed = 0;
-    ctx->stepsProfiled++;
     return AVBD_OK;
 }
 
@@ -711,15 +713,67 @@ int step_once(AvbdContext *ctx)
     ctx->stats.pair_checks = (int64_t)ctx->hCounters->pairChecks;
     ctx->stats.sphere_hits = (int64_t)ctx->hCounters->sphereHits;
     ctx->stats.constrained_hits = (int64_t)ctx->hCounters->constrainedHits;
-    CHECK(prof_collect(ctx));
+    if (ctx->profiling)
+        ctx->stepsProfiled++;
     return AVBD_OK;
 }
 
-void pack3(std::vector<float4> &out, const float *src, int n, float w = 0.0f)
+int stage_reserve(AvbdContext *ctx, size_t count)
 {
-    out.resize(n);
-    for (int i = 0; i < n; ++i)
-        out[i] = make_float4(src ? src[3 * i] : 0.0f, src ? src[3 * i + 1] : 0.0f, src ? src[3 * i + 2] : 0.0f, w);
+    if (!ctx->stageDone)
+        CU(cudaEventCreateWithFlags(&ctx->stageDone, cudaEventDisableTiming));
+    CU(cudaEventSynchronize(ctx->stageDone)); // earlier copies out of the staging buffer are done
+    if (count <= ctx->hStageCap)
+        return AVBD_OK;
+    if (ctx->hStage)
+    {
+        CU(cudaStreamSynchronize(ctx->stream));
+        CU(cudaFreeHost(ctx->hStage));
+        ctx->hStage = nullptr;
+        ctx->hStageCap = 0;
+    }
+    CU(cudaMallocHost((void **)&ctx->hStage, count * sizeof(float4)));
+    ctx->hStageCap = count;
+    return AVBD_OK;
+}
+
+// Body state from caller arrays (3 or 4 floats per body) into pinned staging, then one
+// asynchronous copy per field.
+int write_state(AvbdContext *ctx, const AvbdBodies *b)
+{
+    int n = b->count;
+    CHECK(stage_reserve(ctx, (size_t)5 * n));
+    struct F
+    {
+        const float *src;
+        int width;
+        DArr<float4> *dst;
+        float w;
+    } fields[] = {{b->position3, 3, &ctx->pos, 0.0f},
+                  {b->orientation4, 4, &ctx->quat, 1.0f},
+                  {b->velocity3, 3, &ctx->vel, 0.0f},
+                  {b->angular3, 3, &ctx->angvel, 0.0f},
+                  {b->prev_velocity3 ? b->prev_velocity3 : b->velocity3, 3, &ctx->prevVel, 0.0f}};
+    for (int f = 0; f < 5; ++f)
+    {
+        float4 *st = ctx->hStage + (size_t)f * n;
+        const float *src = fields[f].src;
+        int wdt = fields[f].width;
+        for (int i = 0; i < n; ++i)
+        {
+            if (!src)
+                st[i] = wdt == 4 ? make_float4(0, 0, 0, 1) : make_float4(0, 0, 0, 0);
+            else if (wdt == 4)
+                st[i] = make_float4(src[4 * i], src[4 * i + 1], src[4 * i + 2], src[4 * i + 3]);
+            else
+                st[i] = make_float4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.0f);
+        }
+        CHECK(reserve(ctx, *fields[f].dst, std::max(n, 1), false));
+        if (n)
+            CU(cudaMemcpyAsync(fields[f].dst->p, st, sizeof(float4) * n, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    CU(cudaEventRecord(ctx->stageDone, ctx->stream));
+    return AVBD_OK;
 }
 
 template <class T>
@@ -734,24 +788,10 @@ int upload(AvbdContext *ctx, DArr<T> &a, const T *src, size_t count)
 int upload_bodies(AvbdContext *ctx, const AvbdBodies *b, bool props)
 {
     int n = b->count;
-    std::vector<float4> tmp;
-    pack3(tmp, b->position3, n);
-    CHECK(upload(ctx, ctx->pos, tmp.data(), n));
-    tmp.resize(n);
-    for (int i = 0; i < n; ++i)
-        tmp[i] = b->orientation4 ? make_float4(b->orientation4[4 * i], b->orientation4[4 * i + 1],
-                                               b->orientation4[4 * i + 2], b->orientation4[4 * i + 3])
-                                 : make_float4(0, 0, 0, 1);
-    CHECK(upload(ctx, ctx->quat, tmp.data(), n));
-    pack3(tmp, b->velocity3, n);
-    CHECK(upload(ctx, ctx->vel, tmp.data(), n));
-    pack3(tmp, b->angular3, n);
-    CHECK(upload(ctx, ctx->angvel, tmp.data(), n));
-    pack3(tmp, b->prev_velocity3 ? b->prev_velocity3 : b->velocity3, n);
-    CHECK(upload(ctx, ctx->prevVel, tmp.data(), n));
+    CHECK(write_state(ctx, b));
     if (props)
     {
-        tmp.resize(n);
+        std::vector<float4> tmp(n);
         for (int i = 0; i < n; ++i)
             tmp[i] = make_float4(b->mass[i], b->moment3[3 * i], b->moment3[3 * i + 1], b->moment3[3 * i + 2]);
         CHECK(upload(ctx, ctx->massMoment, tmp.data(), n));
@@ -764,6 +804,7 @@ int upload_bodies(AvbdContext *ctx, const AvbdBodies *b, bool props)
             CHECK(reserve(ctx, *a, std::max(n, 1), false));
             CU(cudaMemsetAsync(a->p, 0, sizeof(float4) * std::max(n, 1), ctx->stream));
         }
+        CU(cudaStreamSynchronize(ctx->stream));
     }
     return AVBD_OK;
 }
@@ -917,6 +958,10 @@ void avbd_destroy(AvbdContext *ctx)
         cudaFreeHost(ctx->hCounters);
     if (ctx->hScalars)
         cudaFreeHost(ctx->hScalars);
+    if (ctx->hStage)
+        cudaFreeHost(ctx->hStage);
+    if (ctx->stageDone)
+        cudaEventDestroy(ctx->stageDone);
     if (ctx->evStart)
         cudaEventDestroy(ctx->evStart);
     if (ctx->evStop)
@@ -1102,7 +1147,6 @@ int avbd_write_bodies(AvbdContext *ctx, const AvbdBodies *bodies)
         return fail(ctx, AVBD_ERR_STATE, "body count does not match the loaded world");
     CU(cudaSetDevice(ctx->device));
     CHECK(upload_bodies(ctx, bodies, false));
-    CU(cudaStreamSynchronize(ctx->stream));
     return AVBD_OK;
 }
 
@@ -1133,7 +1177,6 @@ int avbd_read_bodies(AvbdContext *ctx, const AvbdBodyState *out)
     if (!ctx || !out)
         return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
     int n = ctx->n;
-    std::vector<float4> tmp(n);
     struct Field
     {
         DArr<float4> *src;
@@ -1148,20 +1191,29 @@ int avbd_read_bodies(AvbdContext *ctx, const AvbdBodyState *out)
                   {&ctx->initAng, out->initial_orientation4, 4},
                   {&ctx->inertLin, out->inertial_position3, 3},
                   {&ctx->inertAng, out->inertial_orientation4, 4}};
-    for (const Field &f : fields)
+    if (!n)
+        return AVBD_OK;
+    CHECK(stage_reserve(ctx, (size_t)9 * n));
+    for (int f = 0; f < 9; ++f)
+        if (fields[f].dst)
+            CU(cudaMemcpyAsync(ctx->hStage + (size_t)f * n, fields[f].src->p, sizeof(float4) * n,
+                               cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    for (int f = 0; f < 9; ++f)
     {
-        if (!f.dst || !n)
+        float *d = fields[f].dst;
+        if (!d)
             continue;
-        CU(cudaMemcpyAsync(tmp.data(), f.src->p, sizeof(float4) * n, cudaMemcpyDeviceToHost, ctx->stream));
-        CU(cudaStreamSynchronize(ctx->stream));
-        for (int i = 0; i < n; ++i)
-        {
-            f.dst[f.width * i] = tmp[i].x;
-            f.dst[f.width * i + 1] = tmp[i].y;
-            f.dst[f.width * i + 2] = tmp[i].z;
-            if (f.width == 4)
-                f.dst[4 * i + 3] = tmp[i].w;
-        }
+        const float4 *st = ctx->hStage + (size_t)f * n;
+        if (fields[f].width == 4)
+            memcpy(d, st, sizeof(float4) * n);
+        else
+            for (int i = 0; i < n; ++i)
+            {
+                d[3 * i] = st[i].x;
+                d[3 * i + 1] = st[i].y;
+                d[3 * i + 2] = st[i].z;
+            }
     }
     return AVBD_OK;
 }
@@ -1361,6 +1413,7 @@ int avbd_read_profile(AvbdContext *ctx, AvbdProfile *out)
 {
     if (!ctx || !out)
         return AVBD_ERR_ARGUMENT;
+    CHECK(prof_collect(ctx));
     out->steps = ctx->stepsProfiled;
     for (int k = 0; k < AVBD_PHASE_COUNT; ++k)
     {
@@ -1375,6 +1428,7 @@ int avbd_reset_profile(AvbdContext *ctx)
 {
     if (!ctx)
         return AVBD_ERR_ARGUMENT;
+    CHECK(prof_collect(ctx));
     for (int k = 0; k < AVBD_PHASE_COUNT; ++k)
     {
         ctx->phaseMs[k] = 0.0;

@@ -133,6 +133,8 @@ class World:
             "position3", "orientation4", "velocity3", "angular3", "prev_velocity3", "size3", "mass", "moment3",
             "friction", "radius")])
         # forces: creation index -> list index, sequence numbers in creation order
+        if sc.n_forces and (sc.fb.min() < 0 or sc.fb.max() >= n or sc.fa.max() >= n or sc.fa.min() < -1):
+            raise _lib.AvbdError("avbd_load_world failed (argument): force body index out of range")
         to_list = lambda c: np.where(c >= 0, n - 1 - c, -1).astype(np.int32)
         seq = np.arange(sc.n_forces, dtype=np.int64)
         fa, fb = to_list(sc.fa), to_list(sc.fb)

@@ -1,0 +1,301 @@
+"""Benchmark: body-steps/s of the AVBD step on the 65,536-box stack grid.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
+
+A step is one Solver::step of the whole scene (broadphase, narrowphase, warm start,
+10 coloured primal/dual iterations, velocities), device-resident. Each rank runs an
+independent replica of the scene (the single-world step does not shard: "replicas
+only"); value = bodies x steps summed over ranks / slowest rank's time.
+
+--impl reference times the reference's own CPU solver (built from its sources into
+oracle/_ref; the C oracle port stands in if that library is absent) on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "body-steps/s at 65k boxes"
+UNIT = "body-steps/s"
+GRID = (64, 64, 16)
+SEED = 1
+WORKLOAD = "stack grid 64x64x16 = 65,536 boxes + ground (seed 1); dt 1/60, 10 iterations, alpha 0.99, " \
+           "gamma 0.99, betaLin 1e5, g -9.81"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic_per_launch():
+    """dram bytes per primal launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "primal_stacks65k_ncu.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.device), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.rows = []
+        if self.proc is None:
+            return
+        time.sleep(0.25)
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 8:
+                self.rows.append(parts)
+
+    def summary(self):
+        if not getattr(self, "rows", None):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[4 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def algorithmic_primal_bytes(world) -> tuple[int, dict]:
+    """Bytes one primal iteration must move (per-colour launches summed): 128 per solved body
+    (100 B state read + 28 B pose write), 164 per contact row incidence on a dynamic body
+    (108 B row + 56 B partner pose/initial), 176 per joint and 96 per spring incidence."""
+    m = world.manifolds()
+    mass = world.props["mass"]
+    dyn = mass > 0
+    ab = m["ab"]
+    n_rows = m["n"].astype(np.int64)
+    ic = int((n_rows * dyn[ab[:, 0]]).sum() + (n_rows * dyn[ab[:, 1]]).sum())
+    j = world.joints()
+    ij = int(sum(dyn[a] for a in j["ab"][:, 0] if a >= 0) + dyn[j["ab"][:, 1]].sum()) if len(j["ab"]) else 0
+    sab = world._force_arrays["s_ab"]
+    isp = int(dyn[sab[:, 0]].sum() + dyn[sab[:, 1]].sum()) if len(sab) else 0
+    solved = int(world.stats()["solved_bodies"])
+    per_iter = 128 * solved + 164 * ic + 176 * ij + 96 * isp
+    return per_iter, {"solved_bodies": solved, "contact_incidences": ic, "joint_incidences": ij,
+                      "spring_incidences": isp, "contacts": int(n_rows.sum()), "manifolds": int(len(n_rows))}
+
+
+def run_cuda(args):
+    import torch
+    import torch.distributed as dist
+
+    from avbd_demo3d_b200 import World, scenes
+
+    rank, world_size, local = dist_env()
+    torch.cuda.set_device(local)
+    if world_size > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    scene = scenes.stack_grid(*GRID, seed=SEED)
+    stream = torch.cuda.Stream(device=local)
+    w = World(scene, device=local, stream=stream.cuda_stream)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
+    w.step(args.warmup)
+
+    # ---- timed region: device-resident step, L2 flushed before every step
+    w.set_profiling(True)
+    w.reset_profile()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if world_size > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(k))
+                starts[k].record(stream)
+            w.step(1, sync=False)
+            with torch.cuda.stream(stream):
+                ends[k].record(stream)
+        torch.cuda.synchronize()
+    if world_size > 1:
+        dist.barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = float(sum(step_ms))
+    prof = w.profile()
+    w.set_profiling(False)
+    t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
+    if world_size > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    bodies = scene.n_bodies - 1  # the static ground is not counted
+    value = world_size * bodies * args.steps / (max_ms / 1e3)
+
+    # ---- roofline of the dominant kernel (the coloured primal sweep)
+    per_iter, counts = algorithmic_primal_bytes(w)
+    iters = scene.params.iterations
+    primal_ms = prof["primal_ms"]
+    primal_launches = max(1, prof["primal_spans"])
+    achieved = per_iter * iters * prof["steps"] / (primal_ms / 1e3) / 1e9 if primal_ms > 0 else None
+    peak, peak_kind = measured_peak()
+    traffic = ncu_traffic_per_launch()
+    roofline = {"kernel": "k_primal (coloured primal sweep)", "bound": "hbm", "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                "algorithmic_bytes_per_launch": per_iter * iters * prof["steps"] / primal_launches,
+                "avg_launch_us": primal_ms * 1e3 / primal_launches, "launches": primal_launches, **counts}
+    phases = {k[:-3]: round(v / max(1, prof["steps"]), 4) for k, v in prof.items() if k.endswith("_ms")}
+
+    # ---- end to end through the C ABI with host buffers (H2D state, step, D2H state)
+    st = w.bodies()
+    host = {k: np.ascontiguousarray(v) for k, v in st.items()}
+    h2d = sum(host[k].nbytes for k in ("pos", "quat", "vel", "angvel", "prevvel"))
+    e2e_steps = max(3, args.steps)
+    torch.cuda.synchronize()
+    if world_size > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        w.write_bodies(pos=host["pos"], quat=host["quat"], vel=host["vel"], angvel=host["angvel"],
+                       prevvel=host["prevvel"])
+        w.step(1, sync=False)
+        host = w.bodies()
+    e2e_s = time.perf_counter() - t0
+    d2h = sum(host[k].nbytes for k in ("pos", "quat", "vel", "angvel", "prevvel"))
+    t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+    if world_size > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e = {"value": world_size * bodies * e2e_steps / float(t.item()), "unit": UNIT, "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h, "steps": e2e_steps,
+           "path": "avbd_write_bodies (pinned staging H2D) + avbd_step + avbd_read_bodies (D2H), host timer"}
+
+    cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(scene)
+    w.close()
+    if world_size > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "bodies_per_gpu": bodies, "parallelism": f"replicas x{world_size}",
+                           "l2": "flushed before every timed step (256 MiB device write)",
+                           "timing": "CUDA events on the solver stream, summed per step, max over ranks"},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(),
+                "gpu_launches": prof["launches"], "phases_ms_per_step": phases,
+                "step_ms_min_max": [min(step_ms), max(step_ms)]}
+        print(json.dumps(line), flush=True)
+
+
+def reference_world(scene):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import checkers
+
+    kind = "ref" if checkers.ref_available() else "oracle"
+    return checkers.World(scene, kind), ("reference" if kind == "ref" else "port")
+
+
+def cpu_cores(kind: str) -> int:
+    n = os.cpu_count() or 1
+    # the reference's WorkerPool runs min(hw - 1, 7) workers plus the calling thread
+    return min(n, 8) if kind == "reference" else 1
+
+
+def cpu_baseline(scene, warm: int = 1, timed: int = 5):
+    w, kind = reference_world(scene)
+    w.step(warm)
+    t0 = time.perf_counter()
+    w.step(timed)
+    dt = time.perf_counter() - t0
+    bodies = scene.n_bodies - 1
+    return {"value": bodies * timed / dt, "unit": UNIT, "cores": cpu_cores(kind), "kind": kind,
+            "sample": f"the same 65,536-box scene, steps {warm + 1}-{warm + timed} after {warm} untimed step(s), "
+                      f"Solver::step with the CPU reference backend; {dt / timed * 1e3:.0f} ms/step"}
+
+
+def run_reference(args):
+    rank, world_size, _ = dist_env()
+    if rank != 0:
+        return
+    from avbd_demo3d_b200 import scenes
+
+    scene = scenes.stack_grid(*GRID, seed=SEED)
+    w, kind = reference_world(scene)
+    warm = min(args.warmup, 2)
+    timed = max(1, min(args.steps, 8))
+    w.step(warm)
+    t0 = time.perf_counter()
+    w.step(timed)
+    dt = time.perf_counter() - t0
+    bodies = scene.n_bodies - 1
+    value = bodies * timed / dt
+    cores = cpu_cores(kind)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world_size,
+            "steps": timed, "warmup": warm, "ms_per_step": dt / timed * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "bodies_per_gpu": bodies, "parallelism": "cpu"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                             "sample": f"{timed} steps of the 65,536-box scene after {warm} untimed "
+                                       f"(bounded sample of --steps {args.steps})"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("cuda", "reference"), default="cuda")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_cuda(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -29,3 +29,7 @@ def gpu():
     from avbd_demo3d_b200 import build
     build.build()
     return 0
+
+GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+if GOLDEN_DIR not in sys.path:
+    sys.path.insert(0, GOLDEN_DIR)

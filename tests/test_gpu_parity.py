@@ -1,0 +1,132 @@
+"""CUDA step against the CPU oracle (itself bit-exact with the reference): body state,
+manifolds (pairs, feature keys, contact rows), joints and colouring are compared bit for
+bit after every step, with the oracle sweeping bodies in the GPU's colour order."""
+import os
+
+import numpy as np
+import pytest
+
+import checkers
+from avbd_demo3d_b200 import World, scenes
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def bits(a):
+    return np.ascontiguousarray(a).view(np.uint32)
+
+
+def assert_same_state(g, o, where):
+    bg, bo = g.bodies(), o.bodies()
+    for k in ("pos", "quat", "vel", "angvel", "prevvel"):
+        if not np.array_equal(bits(bg[k]), bits(bo[k])):
+            d = np.abs(bg[k] - bo[k]).max()
+            raise AssertionError(f"{where}: body {k} differs (max |d| {d:.3e})")
+    cg, ng = g.colours()
+    co, no = o.colours()
+    assert ng == no and np.array_equal(cg, co), f"{where}: colouring differs"
+    mg, mo = g.manifolds(), o.manifolds()
+    assert np.array_equal(mg["ab"], mo["ab"]), f"{where}: manifold pairs differ"
+    assert np.array_equal(mg["n"], mo["n"]) and np.array_equal(mg["keys"], mo["keys"]), f"{where}: feature keys differ"
+    assert np.array_equal(mg["seq"], mo["seq"]), f"{where}: manifold creation order differs"
+    assert np.array_equal(bits(mg["contact"]), bits(mo["contact"])), f"{where}: contact rows differ"
+    assert np.array_equal(mg["stick"], mo["stick"]), f"{where}: stick flags differ"
+    jg, jo = g.joints(), o.joints()
+    assert np.array_equal(jg["ab"], jo["ab"]) and np.array_equal(bits(jg["state"]), bits(jo["state"])), where
+    assert np.array_equal(jg["broken"], jo["broken"]), where
+
+
+def lockstep(scene, steps, every=1):
+    g = World(scene)
+    o = checkers.World(scene, "oracle", order_mode=1)
+    for s in range(1, steps + 1):
+        g.step(1)
+        o.step(1)
+        if s % every == 0 or s == steps:
+            assert_same_state(g, o, f"{scene.name} step {s}")
+    st = g.stats()
+    g.close()
+    return st
+
+
+SMALL = {
+    "pyramid20": lambda: scenes.pyramid(20),
+    "rope": lambda: scenes.rope(20),
+    "springs": lambda: scenes.spring_chain(8),
+    "bridge": lambda: scenes.bridge(),
+    "breakable": lambda: scenes.breakable(),
+    "boxbox": lambda: scenes.box_box_probe(),
+    "rotboxbox": lambda: scenes.rotated_box_box_probe(),
+    "cluster": lambda: scenes.box_cluster_probe(),
+    "stacks": lambda: scenes.stack_grid(6, 6, 8, seed=3),
+    "mixed": lambda: scenes.mixed_drop(3000, 20, 12, 0.05, extent=(30, 30, 20), seed=5),
+}
+
+
+@pytest.mark.parametrize("name", sorted(SMALL))
+def test_small_scenes_bit_exact_60_steps(gpu, name):
+    lockstep(SMALL[name](), 60)
+
+
+def test_pyramid_600_steps_matches_reference_fixture_pins(gpu):
+    """The 210-box benchmark pyramid for the full 600 steps, checked every 20 steps."""
+    lockstep(scenes.pyramid(20), 600, every=20)
+
+
+def test_all_pairs_broadphase(gpu):
+    sc = scenes.stack_grid(5, 5, 6, seed=25)
+    sc.params.broadphase = scenes.BROADPHASE_ALL_PAIRS
+    lockstep(sc, 40)
+
+
+def test_stacks_4096_bit_exact(gpu):
+    st = lockstep(scenes.stack_grid(16, 16, 16, seed=1), 60, every=10)
+    assert st["manifold_count"] >= 4096 and st["colours"] >= 2
+
+
+def test_mixed_joints_springs_fracture(gpu):
+    sc = scenes.mixed_drop(6000, 40, 16, 0.1, extent=(40, 40, 30), seed=31)
+    lockstep(sc, 120, every=10)
+
+
+@pytest.mark.slow
+def test_benchmark_scene_65536_boxes_first_steps(gpu):
+    """Full-size benchmark scene: the first steps bit-exact (the oracle is serial, so only a few)."""
+    lockstep(scenes.stack_grid(64, 64, 16, seed=1), 3)
+
+
+def test_colour_order_fixture_from_reference(gpu):
+    """GPU state after 60 steps equals the reference run with its body list relinked
+    into colour order (golden fixture made from the reference itself)."""
+    import make_golden
+
+    g = np.load(os.path.join(GOLDEN, "scenes60_ref.npz"))
+    for name, sc in make_golden.golden_scenes().items():
+        w = World(sc)
+        w.step(60)
+        b, m = w.bodies(), w.manifolds()
+        p = f"{name}_colour_"
+        for k in ("pos", "quat", "vel", "angvel"):
+            assert np.array_equal(bits(b[k]), bits(g[p + k])), (name, k)
+        assert np.array_equal(m["keys"], g[p + "man_keys"]), name
+        assert np.array_equal(bits(m["contact"]), bits(g[p + "man_contact"])), name
+        w.close()
+
+
+def test_list_order_drift_within_reference_gates(gpu):
+    """Against the reference's own list-order solve (what the CPU backend runs), the GPU's
+    colour-order sweep stays inside the reference's GPU-vs-CPU compare gates
+    (max position error < 0.05, viewer/package.json:24) over 120 frames."""
+    if not checkers.ref_available():
+        pytest.skip("reference library not built")
+    for sc in (scenes.pyramid(20), scenes.rope(20), scenes.stack_grid(6, 6, 8, seed=3)):
+        g = World(sc)
+        r = checkers.World(sc, "ref")
+        worst = 0.0
+        for _ in range(120):
+            g.step(1)
+            r.step(1)
+            worst = max(worst, float(np.abs(g.bodies()["pos"] - r.bodies()["pos"]).max()))
+        assert worst < 0.05, (sc.name, worst)
+        g.close()

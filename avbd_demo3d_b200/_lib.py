@@ -67,7 +67,7 @@ class AvbdStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_int64) for k in (
         "body_count", "pair_checks", "sphere_hits", "constrained_hits", "manifolds_created", "manifold_count",
         "contact_count", "joint_count", "spring_count", "solved_bodies", "colours", "colour_rounds",
-        "primal_rows")] + [("step_ms", ctypes.c_float)]
+        "primal_rows", "grid_rescaled")] + [("step_ms", ctypes.c_float)]
 
 
 PHASES = ("broadphase", "force_init", "adjacency", "body_init", "colouring", "primal", "dual", "velocity")
@@ -104,6 +104,10 @@ SIGNATURES = {
     "avbd_device_pose": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
                                         ctypes.POINTER(ctypes.c_void_p)]),
     "avbd_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    "avbd_set_colouring": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    "avbd_num_primal_variants": (ctypes.c_int, [c_int_p, c_int_p, c_int_p]),
+    "avbd_set_primal_variant": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    "avbd_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, c_int_p, c_float_p]),
     "avbd_read_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AvbdProfile)]),
     "avbd_reset_profile": (ctypes.c_int, [ctypes.c_void_p]),
 }

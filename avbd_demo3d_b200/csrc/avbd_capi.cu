@@ -44,8 +44,23 @@ struct ManBuf
 };
 
 constexpr int PRIMAL_BLOCK = 128;
-constexpr int PRIMAL_GROUP = 8;
 constexpr unsigned CELL_TABLE = CELL_TABLE_SIZE;
+
+// Primal kernel variants: lanes per body (G) and the occupancy target given to the
+// compiler (resident blocks per SM; 1 = no register cap).
+struct PrimalVariant
+{
+    int group, minBlocks;
+    void (*kernel)(DevBodies, DevForces, Params, const int *, int, int);
+};
+
+const PrimalVariant kPrimalVariants[] = {
+    {8, 1, k_primal<8, PRIMAL_BLOCK, 1>},   {8, 6, k_primal<8, PRIMAL_BLOCK, 6>},
+    {8, 8, k_primal<8, PRIMAL_BLOCK, 8>},   {4, 1, k_primal<4, PRIMAL_BLOCK, 1>},
+    {4, 6, k_primal<4, PRIMAL_BLOCK, 6>},   {16, 1, k_primal<16, PRIMAL_BLOCK, 1>},
+    {16, 6, k_primal<16, PRIMAL_BLOCK, 6>}, {32, 1, k_primal<32, PRIMAL_BLOCK, 1>},
+};
+constexpr int kNumPrimalVariants = (int)(sizeof(kPrimalVariants) / sizeof(kPrimalVariants[0]));
 
 } // namespace
 
@@ -67,7 +82,10 @@ struct AvbdContext
     float binnedRadius = 0.0f;
     DArr<int> binned, large;
     DArr<float4> largeLo, largeHi, largeSphere;
-    DArr<int> llCount, llOffset;
+    DArr<int> llCount, llOffset, largeGlobalStart;
+    DArr<unsigned long long> largeKeys, largeKeysAlt;
+    DArr<unsigned> largeCellStart;
+    const unsigned long long *largeSorted = nullptr;
     DArr<unsigned> bounds;
     DArr<GridParams> grid;
     DArr<unsigned> cellStart;
@@ -93,8 +111,13 @@ struct AvbdContext
     DArr<unsigned> adj, incVals, incValsAlt;
     DArr<unsigned long long> incKeys, incKeysAlt;
 
-    DArr<int> colourState, colour, solveList, colourStart, remaining;
-    DArr<unsigned long long> colKeys, colKeysAlt;
+    DArr<int> colourState, colour, solveList, colourStart;
+    DArr<unsigned> colKeys, colKeysAlt;
+    DArr<ColourControl> colourCtl;
+    int colourBlocks = 148;   // co-resident blocks for the cooperative colouring launch
+    int colourMode = 0;       // 0 greedy (list-index priority), 1 hashed priority
+    int *hColourSummary = nullptr; // pinned: vertices, rounds, max colour, error
+    int *hColourStarts = nullptr;  // pinned: 257 colour range starts
     std::vector<int> hColourStart;
     int nColours = 0, nSolve = 0;
 
@@ -102,6 +125,7 @@ struct AvbdContext
     DArr<StepCounters> counters;
     StepCounters *hCounters = nullptr;
     long long *hScalars = nullptr; // pinned scratch for small readbacks
+    GridParams *hGrid = nullptr;   // pinned copy of the grid parameters
     float4 *hStage = nullptr;      // pinned staging for body state transfers
     size_t hStageCap = 0;
     cudaEvent_t stageDone = nullptr; // staging copies issued before this event are complete
@@ -111,6 +135,7 @@ struct AvbdContext
     cudaEvent_t evStart = nullptr, evStop = nullptr;
 
     // profiling: events around each phase, summed per phase after the step
+    int primalVariant = 4; // G = 4 lanes per body, 6 resident blocks per SM (autotuned on stacks)
     bool profiling = false;
     std::vector<cudaEvent_t> evPool;
     size_t evUsed = 0;
@@ -338,6 +363,35 @@ __global__ void k_total(const int *scan, const int *in, int n, long long *out)
 {
     *out = (long long)scan[n - 1] + (long long)in[n - 1];
 }
+__global__ void k_fill_int(int *p, int v) { *p = v; }
+
+// Colouring summary into pinned host memory: vertices, rounds, max colour, error.
+__global__ void k_colour_count(const ColourControl *ctl, int *unused, int *summary)
+{
+    summary[0] = ctl->vertices;
+    summary[1] = ctl->rounds;
+    summary[2] = ctl->maxColour;
+    summary[3] = ctl->error;
+}
+
+__global__ void k_solve_list_all(const unsigned *keys, int n, int *list, int *colourStart, const ColourControl *ctl)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    int count = ctl->vertices;
+    int nColours = count > 0 ? ctl->maxColour + 1 : 0;
+    if (k >= count)
+        return;
+    unsigned key = keys[k];
+    list[k] = (int)(key & 0xFFFFFFu);
+    int c = (int)(key >> 24);
+    int prev = k > 0 ? (int)(keys[k - 1] >> 24) : -1;
+    for (int x = prev + 1; x <= c; ++x)
+        colourStart[x] = k;
+    if (k == count - 1)
+        for (int x = c + 1; x <= nColours; ++x)
+            colourStart[x] = count;
+}
+
 __global__ void k_u8_to_int(const unsigned char *in, int *out, int n)
 {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -377,6 +431,68 @@ int build_adjacency(AvbdContext *ctx)
                                                                   ctx->adjStart.p);
     LAUNCHED();
     k_copy_adj<<<grid_for(T, 256), 256, 0, ctx->stream>>>(dv.Current(), ctx->adj.p, (int)T);
+    LAUNCHED();
+    return AVBD_OK;
+}
+
+// The reference's cell-count cap (solver.cpp:341-357) with the host C library's cbrtf, the
+// function the reference itself calls, so the rescaled grid matches bit for bit.
+void host_grid_cap(GridParams &g)
+{
+    const unsigned long long maxCells = 1ull << 22;
+    float cellSize = g.cellSize0;
+    int nx, ny, nz;
+    auto dims = [&](float cs) -> unsigned long long {
+        nx = (int)(g.extx / cs) + 1;
+        ny = (int)(g.exty / cs) + 1;
+        nz = (int)(g.extz / cs) + 1;
+        return (unsigned long long)nx * (unsigned long long)ny * (unsigned long long)nz;
+    };
+    unsigned long long numCells = dims(cellSize);
+    while (numCells > maxCells)
+    {
+        float f = cbrtf((float)numCells / (float)maxCells);
+        cellSize *= f > 1.1f ? f : 1.1f;
+        numCells = dims(cellSize);
+    }
+    g.cellSize = cellSize;
+    g.nx = nx;
+    g.ny = ny;
+    g.nz = nz;
+    g.numCells = numCells;
+    g.capped = 0;
+}
+
+// Large bodies binned into the grid cells their inflated AABB touches (sorted (cell, index)
+// keys, a cell-start table, and the global run for bodies spanning too many cells).
+int large_cell_lists(AvbdContext *ctx, int nL)
+{
+    int total = nL * LARGE_MAX_CELLS;
+    CU(cudaMemsetAsync(ctx->largeGlobalStart.p, 0, sizeof(int), ctx->stream));
+    if (!nL)
+    {
+        ctx->largeSorted = ctx->largeKeys.p;
+        return AVBD_OK;
+    }
+    k_bp_large_cells<<<grid_for(nL, 128), 128, 0, ctx->stream>>>(ctx->largeLo.p, ctx->largeHi.p, nL, ctx->grid.p,
+                                                                   ctx->bounds.p, ctx->binnedRadius,
+                                                                   ctx->largeKeys.p);
+    LAUNCHED();
+    cub::DoubleBuffer<unsigned long long> lk(ctx->largeKeys.p, ctx->largeKeysAlt.p);
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortKeys(nullptr, bytes, lk, total, 0, 64, ctx->stream);
+    CHECK(ensure_temp(ctx, bytes));
+    CU(cub::DeviceRadixSort::SortKeys(ctx->cubTemp.p, bytes, lk, total, 0, 64, ctx->stream));
+    ctx->launches++;
+    ctx->largeSorted = lk.Current();
+    // sentinel after the sorted keys, and the global-run start defaults to it
+    CU(cudaMemsetAsync(lk.Current() + total, 0xFF, sizeof(unsigned long long), ctx->stream));
+    k_fill_int<<<1, 1, 0, ctx->stream>>>(ctx->largeGlobalStart.p, total);
+    LAUNCHED();
+    k_bp_large_global_start<<<grid_for(total, 256), 256, 0, ctx->stream>>>(lk.Current(), total, nL,
+                                                                             ctx->largeGlobalStart.p);
+    LAUNCHED();
+    k_bp_cell_start<<<grid_for(total, 256), 256, 0, ctx->stream>>>(lk.Current(), total, ctx->largeCellStart.p, 1);
     LAUNCHED();
     return AVBD_OK;
 }
@@ -432,18 +548,11 @@ int broadphase(AvbdContext *ctx)
         ctx->hScalars[0] = 0;
         ctx->hScalars[1] = 0;
         DevForces F = dev_forces(ctx);
-        if (nB)
-        {
-            k_bp_bounds_init<<<1, 32, 0, ctx->stream>>>(ctx->bounds.p);
+        // keys -> sorted entries -> cell tables -> large-body lists -> counted new pairs
+        auto counting_pass = [&]() -> int {
+            k_bp_keys<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(B, ctx->binned.p, nB, ctx->grid.p, ctx->bpKeys.p);
             LAUNCHED();
-            k_bp_bounds<<<std::min(grid_for(nB, 256), 148 * 4), 256, 0, ctx->stream>>>(B, ctx->binned.p, nB,
-                                                                                          ctx->bounds.p);
-            LAUNCHED();
-            k_bp_params<<<1, 1, 0, ctx->stream>>>(ctx->bounds.p, ctx->binnedRadius, ctx->grid.p, cnt);
-            LAUNCHED();
-            k_bp_keys<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(B, ctx->binned.p, nB, ctx->grid.p,
-                                                                    ctx->bpKeys.p);
-            LAUNCHED();
+            dk = cub::DoubleBuffer<unsigned long long>(ctx->bpKeys.p, ctx->bpKeysAlt.p);
             size_t bytes = 0;
             cub::DeviceRadixSort::SortKeys(nullptr, bytes, dk, nB, 0, 64, ctx->stream);
             CHECK(ensure_temp(ctx, bytes));
@@ -451,29 +560,73 @@ int broadphase(AvbdContext *ctx)
             ctx->launches++;
             k_bp_cell_start<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(dk.Current(), nB, ctx->cellStart.p, 1);
             LAUNCHED();
+            CHECK(large_cell_lists(ctx, nL));
             k_bp_pairs<false><<<grid_for(nB, 128), 128, 0, ctx->stream>>>(
                 B, F, dk.Current(), nB, ctx->cellStart.p, ctx->grid.p, ctx->large.p, nL, ctx->largeLo.p,
-                ctx->largeHi.p, dt, ctx->pairCount.p, nullptr, 0, 0, cnt);
+                ctx->largeHi.p, ctx->largeSorted, ctx->largeCellStart.p, ctx->largeGlobalStart.p, dt,
+                ctx->pairCount.p, nullptr, 0, 0, cnt);
             LAUNCHED();
             CHECK(scan_counts(ctx, ctx->pairCount.p, ctx->pairOffset.p, nB, 0));
             ctx->launches++;
             k_total<<<1, 1, 0, ctx->stream>>>(ctx->pairOffset.p, ctx->pairCount.p, nB, ctx->hScalars);
             LAUNCHED();
-        }
-        if (nL > 1)
+            return AVBD_OK;
+        };
+        auto large_large_count = [&]() -> int {
+            if (nL > 1)
+            {
+                CHECK(reserve(ctx, ctx->llCount, (size_t)nLL, false));
+                CHECK(reserve(ctx, ctx->llOffset, (size_t)nLL, false));
+                k_bp_large_large<false><<<grid_for(nLL, 128), 128, 0, ctx->stream>>>(
+                    F, ctx->large.p, ctx->largeSphere.p, nL, nChunks, ctx->llCount.p, nullptr, 0, 0, cnt);
+                LAUNCHED();
+                CHECK(scan_counts(ctx, ctx->llCount.p, ctx->llOffset.p, (int)nLL, 0));
+                ctx->launches++;
+                k_total<<<1, 1, 0, ctx->stream>>>(ctx->llOffset.p, ctx->llCount.p, (int)nLL, ctx->hScalars + 1);
+                LAUNCHED();
+            }
+            return AVBD_OK;
+        };
+        auto reset_tables = [&]() -> int {
+            k_bp_cell_start<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(dk.Current(), nB, ctx->cellStart.p, 0);
+            LAUNCHED();
+            if (nL)
+            {
+                int total = nL * LARGE_MAX_CELLS;
+                k_bp_cell_start<<<grid_for(total, 256), 256, 0, ctx->stream>>>(ctx->largeSorted, total,
+                                                                                 ctx->largeCellStart.p, 0);
+                LAUNCHED();
+            }
+            return AVBD_OK;
+        };
+        if (nB)
         {
-            CHECK(reserve(ctx, ctx->llCount, (size_t)nLL, false));
-            CHECK(reserve(ctx, ctx->llOffset, (size_t)nLL, false));
-            k_bp_large_large<false><<<grid_for(nLL, 128), 128, 0, ctx->stream>>>(
-                F, ctx->large.p, ctx->largeSphere.p, nL, nChunks, ctx->llCount.p, nullptr, 0, 0, cnt);
+            k_bp_bounds_init<<<1, 32, 0, ctx->stream>>>(ctx->bounds.p);
             LAUNCHED();
-            CHECK(scan_counts(ctx, ctx->llCount.p, ctx->llOffset.p, (int)nLL, 0));
-            ctx->launches++;
-            k_total<<<1, 1, 0, ctx->stream>>>(ctx->llOffset.p, ctx->llCount.p, (int)nLL, ctx->hScalars + 1);
+            k_bp_bounds<<<std::min(grid_for(nB, 256), 148 * 4), 256, 0, ctx->stream>>>(B, ctx->binned.p, nB, dt,
+                                                                                          ctx->bounds.p);
             LAUNCHED();
+            k_bp_params<<<1, 1, 0, ctx->stream>>>(ctx->bounds.p, ctx->binnedRadius, ctx->grid.p);
+            LAUNCHED();
+            CHECK(counting_pass());
         }
+        CHECK(large_large_count());
+        CU(cudaMemcpyAsync(ctx->hGrid, ctx->grid.p, sizeof(GridParams), cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaMemcpyAsync(ctx->hCounters, cnt, sizeof(StepCounters), cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaStreamSynchronize(ctx->stream));
+        if (nB && ctx->hGrid->capped)
+        {
+            // rare path: rescale the cells exactly as the reference does, then count again
+            CHECK(reset_tables());
+            host_grid_cap(*ctx->hGrid);
+            CU(cudaMemcpyAsync(ctx->grid.p, ctx->hGrid, sizeof(GridParams), cudaMemcpyHostToDevice, ctx->stream));
+            CU(cudaMemsetAsync(cnt, 0, sizeof(StepCounters), ctx->stream));
+            CHECK(counting_pass());
+            CHECK(large_large_count());
+            CU(cudaMemcpyAsync(ctx->hCounters, cnt, sizeof(StepCounters), cudaMemcpyDeviceToHost, ctx->stream));
+            CU(cudaStreamSynchronize(ctx->stream));
+            ctx->stats.grid_rescaled = 1;
+        }
         if (ctx->hCounters->error)
             return fail(ctx, AVBD_ERR_CAPACITY, "broadphase grid exceeds the cell cap");
         P1 = ctx->hScalars[0];
@@ -485,7 +638,8 @@ int broadphase(AvbdContext *ctx)
         {
             k_bp_pairs<true><<<grid_for(nB, 128), 128, 0, ctx->stream>>>(
                 B, F, dk.Current(), nB, ctx->cellStart.p, ctx->grid.p, ctx->large.p, nL, ctx->largeLo.p,
-                ctx->largeHi.p, dt, nullptr, ctx->pairOffset.p, M0, (unsigned long long)ctx->nextSeq, cnt);
+                ctx->largeHi.p, ctx->largeSorted, ctx->largeCellStart.p, ctx->largeGlobalStart.p, dt, nullptr,
+                ctx->pairOffset.p, M0, (unsigned long long)ctx->nextSeq, cnt);
             LAUNCHED();
         }
         if (P2 > 0)
@@ -496,10 +650,7 @@ int broadphase(AvbdContext *ctx)
             LAUNCHED();
         }
         if (nB)
-        {
-            k_bp_cell_start<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(dk.Current(), nB, ctx->cellStart.p, 0);
-            LAUNCHED();
-        }
+            CHECK(reset_tables());
     }
     ctx->stats.manifolds_created = P1 + P2;
     ctx->nMan = (int)(M0 + P1 + P2);
@@ -572,67 +723,57 @@ int colour_bodies(AvbdContext *ctx)
 {
     int n = ctx->n;
     DevBodies B = dev_bodies(ctx);
+    DevForces F = dev_forces(ctx);
     CHECK(reserve(ctx, ctx->colourState, n, false));
     CHECK(reserve(ctx, ctx->colour, n, false));
     CHECK(reserve(ctx, ctx->solveList, n, false));
     CHECK(reserve(ctx, ctx->colKeys, n, false));
     CHECK(reserve(ctx, ctx->colKeysAlt, n, false));
-    CHECK(reserve(ctx, ctx->remaining, 2, false));
-    CU(cudaMemsetAsync(ctx->remaining.p, 0, sizeof(int) * 2, ctx->stream));
-    k_colour_init<<<grid_for(n, 256), 256, 0, ctx->stream>>>(B, ctx->adjStart.p, ctx->colourState.p,
-                                                               ctx->remaining.p);
-    LAUNCHED();
-    CU(cudaMemcpyAsync(ctx->remaining.p + 1, ctx->remaining.p, sizeof(int), cudaMemcpyDeviceToDevice, ctx->stream));
-    DevForces F = dev_forces(ctx);
-    int rounds = 0;
-    int *hRem = (int *)(ctx->hScalars + 2);
-    const int batch = 4;
-    for (;;)
+    CHECK(reserve(ctx, ctx->colourStart, 257, false));
+    CHECK(reserve(ctx, ctx->colourCtl, 1, false));
+    if (n == 0)
     {
-        for (int k = 0; k < batch; ++k)
-        {
-            k_colour_round<<<grid_for(n, 256), 256, 0, ctx->stream>>>(F, n, rounds, ctx->colourState.p,
-                                                                        ctx->remaining.p, ctx->counters.p);
-            LAUNCHED();
-            rounds++;
-        }
-        CU(cudaMemcpyAsync(hRem, ctx->remaining.p, sizeof(int) * 2, cudaMemcpyDeviceToHost, ctx->stream));
-        CU(cudaStreamSynchronize(ctx->stream));
-        if (hRem[0] == 0)
-            break;
-        if (rounds > 60000)
-            return fail(ctx, AVBD_ERR_STATE, "colouring did not converge");
+        ctx->nColours = ctx->nSolve = 0;
+        ctx->hColourStart.assign(1, 0);
+        return AVBD_OK;
     }
-    int nVert = hRem[1];
-    CU(cudaMemcpyAsync(ctx->hCounters, ctx->counters.p, sizeof(StepCounters), cudaMemcpyDeviceToHost, ctx->stream));
-    CU(cudaStreamSynchronize(ctx->stream));
-    if (ctx->hCounters->error == DERR_TOO_MANY_COLOURS)
-        return fail(ctx, AVBD_ERR_CAPACITY, "constraint graph needs more than 256 colours");
-    int C = nVert > 0 ? ctx->hCounters->maxColour + 1 : 0;
-    ctx->nColours = C;
-    ctx->nSolve = nVert;
-    ctx->stats.colour_rounds = rounds;
+    CU(cudaMemsetAsync(ctx->colourCtl.p, 0, sizeof(ColourControl), ctx->stream));
+    int blocks = std::min(grid_for(n, 256), ctx->colourBlocks);
+    int mode = ctx->colourMode;
+    void *args[] = {&B, &F, &n, &mode, &ctx->colourState.p, &ctx->colourCtl.p, &ctx->counters.p};
+    CU(cudaLaunchCooperativeKernel((void *)k_colour_all, blocks, 256, args, 0, ctx->stream));
+    LAUNCHED();
     k_colour_keys<<<grid_for(n, 256), 256, 0, ctx->stream>>>(ctx->colourState.p, n, ctx->colour.p, ctx->colKeys.p);
     LAUNCHED();
-    ctx->hColourStart.assign((size_t)C + 1, 0);
-    if (nVert > 0)
-    {
-        cub::DoubleBuffer<unsigned long long> dk(ctx->colKeys.p, ctx->colKeysAlt.p);
-        size_t bytes = 0;
-        cub::DeviceRadixSort::SortKeys(nullptr, bytes, dk, n, 0, 64, ctx->stream);
-        CHECK(ensure_temp(ctx, bytes));
-        CU(cub::DeviceRadixSort::SortKeys(ctx->cubTemp.p, bytes, dk, n, 0, 64, ctx->stream));
-        ctx->launches++;
-        k_solve_list<<<grid_for(nVert, 256), 256, 0, ctx->stream>>>(dk.Current(), nVert, ctx->solveList.p);
-        LAUNCHED();
-        CHECK(reserve(ctx, ctx->colourStart, (size_t)C + 1, false));
-        k_segment_starts<<<grid_for(nVert, 256), 256, 0, ctx->stream>>>(dk.Current(), nVert, 32, C,
-                                                                          ctx->colourStart.p);
-        LAUNCHED();
-        CU(cudaMemcpyAsync(ctx->hColourStart.data(), ctx->colourStart.p, sizeof(int) * ((size_t)C + 1),
-                           cudaMemcpyDeviceToHost, ctx->stream));
-        CU(cudaStreamSynchronize(ctx->stream));
-    }
+    cub::DoubleBuffer<unsigned> dk(ctx->colKeys.p, ctx->colKeysAlt.p);
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortKeys(nullptr, bytes, dk, n, 0, 32, ctx->stream);
+    CHECK(ensure_temp(ctx, bytes));
+    CU(cub::DeviceRadixSort::SortKeys(ctx->cubTemp.p, bytes, dk, n, 0, 32, ctx->stream));
+    ctx->launches++;
+    // colour ranges for up to 256 colours are written from the sorted keys; the host reads
+    // them together with the colouring summary in one copy
+    CU(cudaMemsetAsync(ctx->colourStart.p, 0, sizeof(int) * 257, ctx->stream));
+    k_colour_count<<<1, 1, 0, ctx->stream>>>(ctx->colourCtl.p, ctx->colourStart.p + 257 - 257, ctx->hColourSummary);
+    LAUNCHED();
+    k_solve_list_all<<<grid_for(n, 256), 256, 0, ctx->stream>>>(dk.Current(), n, ctx->solveList.p, ctx->colourStart.p,
+                                                                 ctx->colourCtl.p);
+    LAUNCHED();
+    CU(cudaMemcpyAsync(ctx->hColourStarts, ctx->colourStart.p, sizeof(int) * 257, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CU(cudaMemcpyAsync(ctx->hCounters, ctx->counters.p, sizeof(StepCounters), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    const int *sum = ctx->hColourSummary; // vertices, rounds, maxColour, error
+    if (sum[3])
+        return fail(ctx, AVBD_ERR_STATE, "colouring did not finish (barrier wait expired or round cap reached)");
+    if (ctx->hCounters->error == DERR_TOO_MANY_COLOURS)
+        return fail(ctx, AVBD_ERR_CAPACITY, "constraint graph needs more than 256 colours");
+    int nVert = sum[0];
+    int C = nVert > 0 ? sum[2] + 1 : 0;
+    ctx->nColours = C;
+    ctx->nSolve = nVert;
+    ctx->stats.colour_rounds = sum[1];
+    ctx->hColourStart.assign(ctx->hColourStarts, ctx->hColourStarts + C + 1);
     return AVBD_OK;
 }
 
@@ -641,7 +782,8 @@ int iterate(AvbdContext *ctx)
     DevBodies B = dev_bodies(ctx);
     DevForces F = dev_forces(ctx);
     Params P = dev_params(ctx->params);
-    constexpr int GPB = PRIMAL_BLOCK / PRIMAL_GROUP;
+    const PrimalVariant &pv = kPrimalVariants[ctx->primalVariant];
+    const int GPB = PRIMAL_BLOCK / pv.group;
     for (int it = 0; it < ctx->params.iterations; ++it)
     {
         for (int c = 0; c < ctx->nColours; ++c)
@@ -651,8 +793,8 @@ int iterate(AvbdContext *ctx)
             if (count <= 0)
                 continue;
             PhaseScope ps(ctx, AVBD_PHASE_PRIMAL);
-            k_primal<PRIMAL_GROUP, PRIMAL_BLOCK><<<grid_for(count, GPB), PRIMAL_BLOCK, 0, ctx->stream>>>(
-                B, F, P, ctx->solveList.p, first, count);
+            pv.kernel<<<grid_for(count, GPB), PRIMAL_BLOCK, 0, ctx->stream>>>(B, F, P, ctx->solveList.p, first,
+                                                                               count);
             LAUNCHED();
         }
         PhaseScope ps(ctx, AVBD_PHASE_DUAL);
@@ -673,6 +815,7 @@ int iterate(AvbdContext *ctx)
 int step_once(AvbdContext *ctx)
 {
     CU(cudaMemsetAsync(ctx->counters.p, 0, sizeof(StepCounters), ctx->stream));
+    ctx->stats.grid_rescaled = 0;
     {
         PhaseScope ps(ctx, AVBD_PHASE_BROADPHASE);
         CHECK(broadphase(ctx));
@@ -830,6 +973,9 @@ int classify_bodies(AvbdContext *ctx, const float *radius, int n)
     CHECK(reserve(ctx, ctx->largeLo, std::max(nL, 1), false));
     CHECK(reserve(ctx, ctx->largeHi, std::max(nL, 1), false));
     CHECK(reserve(ctx, ctx->largeSphere, std::max(nL, 1), false));
+    CHECK(reserve(ctx, ctx->largeKeys, (size_t)std::max(nL, 1) * LARGE_MAX_CELLS + 1, false));
+    CHECK(reserve(ctx, ctx->largeKeysAlt, (size_t)std::max(nL, 1) * LARGE_MAX_CELLS + 1, false));
+    CHECK(reserve(ctx, ctx->largeGlobalStart, 1, false));
     CHECK(reserve(ctx, ctx->bpKeys, std::max(nB, 1), false));
     CHECK(reserve(ctx, ctx->bpKeysAlt, std::max(nB, 1), false));
     CHECK(reserve(ctx, ctx->pairCount, std::max(n, 1), false));
@@ -870,19 +1016,30 @@ int avbd_create(AvbdContext **out, int32_t device_ordinal, void *cuda_stream)
     }
     if (cudaMallocHost((void **)&ctx->hCounters, sizeof(StepCounters)) != cudaSuccess ||
         cudaMallocHost((void **)&ctx->hScalars, sizeof(long long) * 16) != cudaSuccess ||
+        cudaMallocHost((void **)&ctx->hColourSummary, sizeof(int) * 4) != cudaSuccess ||
+        cudaMallocHost((void **)&ctx->hGrid, sizeof(GridParams)) != cudaSuccess ||
+        cudaMallocHost((void **)&ctx->hColourStarts, sizeof(int) * 257) != cudaSuccess ||
         cudaEventCreate(&ctx->evStart) != cudaSuccess || cudaEventCreate(&ctx->evStop) != cudaSuccess)
     {
         avbd_destroy(ctx);
         return AVBD_ERR_CUDA;
     }
     memset(ctx->hCounters, 0, sizeof(StepCounters));
+    {
+        int sms = 0, perSm = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_ordinal);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_colour_all, 256, 0);
+        ctx->colourBlocks = std::max(1, sms * std::max(1, perSm));
+    }
     if (reserve(ctx, ctx->counters, 1, false) || reserve(ctx, ctx->bounds, 8, false) ||
-        reserve(ctx, ctx->grid, 1, false) || reserve(ctx, ctx->cellStart, CELL_TABLE, false))
+        reserve(ctx, ctx->grid, 1, false) || reserve(ctx, ctx->cellStart, CELL_TABLE, false) ||
+        reserve(ctx, ctx->largeCellStart, CELL_TABLE, false))
     {
         avbd_destroy(ctx);
         return AVBD_ERR_CUDA;
     }
     cudaMemsetAsync(ctx->cellStart.p, 0xFF, sizeof(unsigned) * CELL_TABLE, ctx->stream);
+    cudaMemsetAsync(ctx->largeCellStart.p, 0xFF, sizeof(unsigned) * CELL_TABLE, ctx->stream);
     ctx->params.dt = 1.0f / 60.0f;
     ctx->params.gravity = -10.0f;
     ctx->params.iterations = 10;
@@ -918,6 +1075,10 @@ void avbd_destroy(AvbdContext *ctx)
     release(ctx->pairOffset);
     release(ctx->llCount);
     release(ctx->llOffset);
+    release(ctx->largeGlobalStart);
+    release(ctx->largeKeys);
+    release(ctx->largeKeysAlt);
+    release(ctx->largeCellStart);
     for (cudaEvent_t e : ctx->evPool)
         cudaEventDestroy(e);
     for (ManBuf &m : ctx->man)
@@ -949,7 +1110,7 @@ void avbd_destroy(AvbdContext *ctx)
     release(ctx->colour);
     release(ctx->solveList);
     release(ctx->colourStart);
-    release(ctx->remaining);
+    release(ctx->colourCtl);
     release(ctx->colKeys);
     release(ctx->colKeysAlt);
     release(ctx->cubTemp);
@@ -960,6 +1121,12 @@ void avbd_destroy(AvbdContext *ctx)
         cudaFreeHost(ctx->hScalars);
     if (ctx->hStage)
         cudaFreeHost(ctx->hStage);
+    if (ctx->hColourSummary)
+        cudaFreeHost(ctx->hColourSummary);
+    if (ctx->hGrid)
+        cudaFreeHost(ctx->hGrid);
+    if (ctx->hColourStarts)
+        cudaFreeHost(ctx->hColourStarts);
     if (ctx->stageDone)
         cudaEventDestroy(ctx->stageDone);
     if (ctx->evStart)
@@ -1398,6 +1565,104 @@ int avbd_device_pose(AvbdContext *ctx, void **position4, void **orientation4)
         *position4 = ctx->pos.p;
     if (orientation4)
         *orientation4 = ctx->quat.p;
+    return AVBD_OK;
+}
+
+int avbd_num_primal_variants(int32_t *count, int32_t *group4, int32_t *min_blocks4)
+{
+    if (count)
+        *count = kNumPrimalVariants;
+    for (int v = 0; v < kNumPrimalVariants; ++v)
+    {
+        if (group4)
+            group4[v] = kPrimalVariants[v].group;
+        if (min_blocks4)
+            min_blocks4[v] = kPrimalVariants[v].minBlocks;
+    }
+    return AVBD_OK;
+}
+
+int avbd_set_primal_variant(AvbdContext *ctx, int32_t variant)
+{
+    if (!ctx)
+        return AVBD_ERR_ARGUMENT;
+    if (variant < 0 || variant >= kNumPrimalVariants)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "primal variant %d out of range [0, %d)", variant, kNumPrimalVariants);
+    ctx->primalVariant = variant;
+    return AVBD_OK;
+}
+
+int avbd_autotune(AvbdContext *ctx, int32_t repeats, int32_t *best_variant, float *variant_us)
+{
+    if (!ctx)
+        return AVBD_ERR_ARGUMENT;
+    if (ctx->errCode)
+        return AVBD_ERR_LATCHED;
+    if (!ctx->loaded || ctx->nSolve == 0)
+        return fail(ctx, AVBD_ERR_STATE, "autotune needs a stepped world (run avbd_step first)");
+    CU(cudaSetDevice(ctx->device));
+    int n = ctx->n;
+    DArr<float4> savePos, saveQuat;
+    CHECK(reserve(ctx, savePos, n, false));
+    CHECK(reserve(ctx, saveQuat, n, false));
+    CU(cudaMemcpyAsync(savePos.p, ctx->pos.p, sizeof(float4) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(saveQuat.p, ctx->quat.p, sizeof(float4) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+    DevBodies B = dev_bodies(ctx);
+    DevForces F = dev_forces(ctx);
+    Params P = dev_params(ctx->params);
+    repeats = std::max(1, repeats);
+    int best = ctx->primalVariant;
+    float bestUs = 1e30f;
+    for (int v = 0; v < kNumPrimalVariants; ++v)
+    {
+        const PrimalVariant &pv = kPrimalVariants[v];
+        int GPB = PRIMAL_BLOCK / pv.group;
+        float total = 0.0f;
+        for (int r = 0; r <= repeats; ++r)
+        {
+            CU(cudaEventRecord(ctx->evStart, ctx->stream));
+            for (int c = 0; c < ctx->nColours; ++c)
+            {
+                int first = ctx->hColourStart[c], count = ctx->hColourStart[c + 1] - first;
+                if (count > 0)
+                    pv.kernel<<<grid_for(count, GPB), PRIMAL_BLOCK, 0, ctx->stream>>>(B, F, P, ctx->solveList.p,
+                                                                                       first, count);
+            }
+            CU(cudaGetLastError());
+            CU(cudaEventRecord(ctx->evStop, ctx->stream));
+            CU(cudaMemcpyAsync(ctx->pos.p, savePos.p, sizeof(float4) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+            CU(cudaMemcpyAsync(ctx->quat.p, saveQuat.p, sizeof(float4) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+            CU(cudaEventSynchronize(ctx->evStop));
+            float ms = 0.0f;
+            CU(cudaEventElapsedTime(&ms, ctx->evStart, ctx->evStop));
+            if (r > 0) // first run warms caches and instruction memory
+                total += ms;
+        }
+        float us = total * 1e3f / repeats;
+        if (variant_us)
+            variant_us[v] = us;
+        if (us < bestUs)
+        {
+            bestUs = us;
+            best = v;
+        }
+    }
+    CU(cudaStreamSynchronize(ctx->stream));
+    release(savePos);
+    release(saveQuat);
+    ctx->primalVariant = best;
+    if (best_variant)
+        *best_variant = best;
+    return AVBD_OK;
+}
+
+int avbd_set_colouring(AvbdContext *ctx, int32_t mode)
+{
+    if (!ctx)
+        return AVBD_ERR_ARGUMENT;
+    if (mode != AVBD_COLOUR_GREEDY && mode != AVBD_COLOUR_HASHED)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "unknown colouring mode %d", mode);
+    ctx->colourMode = mode;
     return AVBD_OK;
 }
 

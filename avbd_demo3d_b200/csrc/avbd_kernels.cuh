@@ -81,6 +81,9 @@ struct GridParams
     float cellSize;
     int nx, ny, nz;
     unsigned long long numCells;
+    float extx, exty, extz; // bounds extent of the binned centres
+    float cellSize0;        // twice the binned radius, before the cell-count cap
+    int capped;             // 1: the cell-count cap applies; the host recomputes the grid
 };
 
 // Device-side counters of one step.
@@ -156,16 +159,18 @@ __global__ void k_bp_bounds_init(unsigned *bounds)
 {
     if (threadIdx.x < 3)
         bounds[threadIdx.x] = 0xFFFFFFFFu; // min slots
-    else if (threadIdx.x < 6)
-        bounds[threadIdx.x] = 0u; // max slots
+    else if (threadIdx.x < 7)
+        bounds[threadIdx.x] = 0u; // max slots; [6] = largest binned slack (non-negative float bits)
 }
 
-__global__ void k_bp_bounds(DevBodies B, const int *binned, int nBinned, unsigned *bounds)
+__global__ void k_bp_bounds(DevBodies B, const int *binned, int nBinned, float dt, unsigned *bounds)
 {
     unsigned lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, hi[3] = {0u, 0u, 0u};
+    float slack = 0.0f;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nBinned; k += gridDim.x * blockDim.x)
     {
-        float4 p = B.pos[binned[k]];
+        int b = binned[k];
+        float4 p = B.pos[b];
         unsigned v[3] = {float_order(p.x), float_order(p.y), float_order(p.z)};
 #pragma unroll
         for (int d = 0; d < 3; ++d)
@@ -173,16 +178,16 @@ __global__ void k_bp_bounds(DevBodies B, const int *binned, int nBinned, unsigne
             lo[d] = min(lo[d], v[d]);
             hi[d] = max(hi[d], v[d]);
         }
+        slack = fmaxf(slack, len(xyz(B.vel[b])) * dt);
     }
+    unsigned sl = __float_as_uint(slack);
 #pragma unroll
     for (int d = 0; d < 3; ++d)
     {
-        for (int o = 16; o > 0; o >>= 1)
-        {
-            lo[d] = min(lo[d], __shfl_xor_sync(0xFFFFFFFFu, lo[d], o));
-            hi[d] = max(hi[d], __shfl_xor_sync(0xFFFFFFFFu, hi[d], o));
-        }
+        lo[d] = __reduce_min_sync(0xFFFFFFFFu, lo[d]);
+        hi[d] = __reduce_max_sync(0xFFFFFFFFu, hi[d]);
     }
+    sl = __reduce_max_sync(0xFFFFFFFFu, sl);
     if ((threadIdx.x & 31) == 0)
     {
 #pragma unroll
@@ -191,6 +196,7 @@ __global__ void k_bp_bounds(DevBodies B, const int *binned, int nBinned, unsigne
             atomicMin(&bounds[d], lo[d]);
             atomicMax(&bounds[3 + d], hi[d]);
         }
+        atomicMax(&bounds[6], sl);
     }
 }
 
@@ -218,29 +224,31 @@ __global__ void k_bp_large(DevBodies B, const int *large, int nLarge, float dt, 
     sphere[k] = f4(p, sr.w);
 }
 
-// Cell size and grid dimensions with the reference's cell-count cap (solver.cpp:338-357)
-__global__ void k_bp_params(const unsigned *bounds, float binnedRadius, GridParams *gp, StepCounters *cnt)
+// Cell size and grid dimensions (solver.cpp:338-357). When the cell count exceeds the cap
+// the reference grows the cells by cbrtf factors; that rescaling is redone on the host with
+// the C library's cbrtf (the one the reference calls), so the device only flags it and
+// leaves a bounded placeholder grid.
+__global__ void k_bp_params(const unsigned *bounds, float binnedRadius, GridParams *gp)
 {
     float bminx = float_unorder(bounds[0]), bminy = float_unorder(bounds[1]), bminz = float_unorder(bounds[2]);
     float bmaxx = float_unorder(bounds[3]), bmaxy = float_unorder(bounds[4]), bmaxz = float_unorder(bounds[5]);
     float cellSize = binnedRadius * 2.0f;
     const unsigned long long maxCells = 1ull << 22;
     float3 extent = f3(bmaxx - bminx, bmaxy - bminy, bmaxz - bminz);
+    gp->extx = extent.x;
+    gp->exty = extent.y;
+    gp->extz = extent.z;
+    gp->cellSize0 = cellSize;
     int nx = (int)(extent.x / cellSize) + 1;
     int ny = (int)(extent.y / cellSize) + 1;
     int nz = (int)(extent.z / cellSize) + 1;
     unsigned long long numCells = (unsigned long long)nx * (unsigned long long)ny * (unsigned long long)nz;
-    int guard = 0;
-    while (numCells > maxCells && guard++ < 64)
-    {
-        cellSize *= rmax(cbrtf((float)numCells / (float)maxCells), 1.1f);
-        nx = (int)(extent.x / cellSize) + 1;
-        ny = (int)(extent.y / cellSize) + 1;
-        nz = (int)(extent.z / cellSize) + 1;
-        numCells = (unsigned long long)nx * (unsigned long long)ny * (unsigned long long)nz;
-    }
+    gp->capped = numCells > maxCells ? 1 : 0;
     if (numCells > maxCells)
-        cnt->error = DERR_TOO_MANY_CELLS;
+    {
+        nx = ny = nz = 1;
+        numCells = 1;
+    }
     gp->bminx = bminx;
     gp->bminy = bminy;
     gp->bminz = bminz;
@@ -279,11 +287,67 @@ __global__ void k_bp_cell_start(const unsigned long long *keys, int nBinned, uns
         cellStart[key] = set ? (unsigned)k : 0xFFFFFFFFu;
 }
 
+// Large bodies are binned into the same grid with their AABB inflated by an upper bound of
+// the reference's reach (binned radius + travel slacks + 4 margins, solver.cpp:449-458), so a
+// binned body only tests the large bodies listed for its own cell; the reference's exact
+// predicate still decides every pair. Bodies spanning more than LARGE_MAX_CELLS cells (a
+// ground slab) go to a global list that every binned body tests.
+constexpr int LARGE_MAX_CELLS = 64;
+constexpr unsigned LARGE_GLOBAL = 0xFFFFFFFFu;
+
+AVBD_DEV int grid_axis(float x, float bmin, float cellSize, int n)
+{
+    return (int)rclamp((x - bmin) / cellSize, 0.0f, (float)(n - 1));
+}
+
+__global__ void k_bp_large_cells(const float4 *largeLo, const float4 *largeHi, int nLarge, const GridParams *gp,
+                                 const unsigned *bounds, float binnedRadius, unsigned long long *keys)
+{
+    int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= nLarge)
+        return;
+    GridParams g = *gp;
+    float4 lo = largeLo[l], hi = largeHi[l];
+    float slackMax = __uint_as_float(bounds[6]);
+    float R = (binnedRadius + slackMax + lo.w + 4.0f * COLLISION_MARGIN) * 1.001f + 1.0e-4f;
+    int x0 = grid_axis(lo.x - R, g.bminx, g.cellSize, g.nx), x1 = grid_axis(hi.x + R, g.bminx, g.cellSize, g.nx);
+    int y0 = grid_axis(lo.y - R, g.bminy, g.cellSize, g.ny), y1 = grid_axis(hi.y + R, g.bminy, g.cellSize, g.ny);
+    int z0 = grid_axis(lo.z - R, g.bminz, g.cellSize, g.nz), z1 = grid_axis(hi.z + R, g.bminz, g.cellSize, g.nz);
+    long long cells = (long long)(x1 - x0 + 1) * (y1 - y0 + 1) * (z1 - z0 + 1);
+    bool finite = isfinite(lo.x) && isfinite(lo.y) && isfinite(lo.z) && isfinite(hi.x) && isfinite(hi.y) &&
+                  isfinite(hi.z) && isfinite(R);
+    unsigned long long *out = keys + (size_t)l * LARGE_MAX_CELLS;
+    int k = 0;
+    if (!finite || cells <= 0 || cells > LARGE_MAX_CELLS || g.numCells > CELL_TABLE_SIZE)
+        out[k++] = ((unsigned long long)LARGE_GLOBAL << 32) | (unsigned)l;
+    else
+        for (int z = z0; z <= z1; ++z)
+            for (int y = y0; y <= y1; ++y)
+                for (int x = x0; x <= x1; ++x)
+                    out[k++] = ((unsigned long long)(unsigned)(x + g.nx * (y + g.ny * z)) << 32) | (unsigned)l;
+    for (; k < LARGE_MAX_CELLS; ++k)
+        out[k] = 0xFFFFFFFFFFFFFFFFull;
+}
+
+// First index of the global run in the sorted large-cell keys (or the run's end if empty).
+__global__ void k_bp_large_global_start(const unsigned long long *keys, int total, int nLarge, int *globalStart)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= total)
+        return;
+    auto isGlobal = [&](unsigned long long v) {
+        return (unsigned)(v >> 32) == LARGE_GLOBAL && (unsigned)v < (unsigned)nLarge;
+    };
+    bool here = isGlobal(keys[k]) || keys[k] == 0xFFFFFFFFFFFFFFFFull;
+    bool before = k > 0 && (isGlobal(keys[k - 1]) || keys[k - 1] == 0xFFFFFFFFFFFFFFFFull);
+    if (here && !before)
+        *globalStart = k;
+}
+
 __constant__ int c_forward[13][3] = {{1, 0, 0},   {-1, 1, 0}, {0, 1, 0},  {1, 1, 0}, {-1, -1, 1},
                                      {0, -1, 1},  {1, -1, 1}, {-1, 0, 1}, {0, 0, 1}, {1, 0, 1},
                                      {-1, 1, 1},  {0, 1, 1},  {1, 1, 1}};
 
-constexpr int LARGE_TILE = 256;
 constexpr int LL_CHUNK = 128;
 
 // Warp-aggregated add of per-thread statistics (one atomic per warp).
@@ -295,65 +359,68 @@ AVBD_DEV void warp_add(unsigned long long *dst, unsigned v)
 }
 
 // One thread per sorted grid entry i (solver.cpp:405-465). EMIT == false counts new
-// (unconstrained) hits, EMIT == true writes them as fresh manifolds at base + offset[i]
-// in hit order. The large bodies are streamed through shared memory in tiles; each
-// thread still visits them in list order.
+// (unconstrained) hits, EMIT == true writes them as fresh manifolds at base + offset[i] in
+// hit order. Large bodies are visited in list order: the entry's cell candidates merged
+// with the global list, both sorted by large index.
 template <bool EMIT>
 __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, const unsigned long long *keys,
                                                   int nBinned, const unsigned *cellStart, const GridParams *gp,
                                                   const int *large, int nLarge, const float4 *largeLo,
-                                                  const float4 *largeHi, float dt, int *counts, const int *offsets,
-                                                  int base, unsigned long long seqBase, StepCounters *cnt)
+                                                  const float4 *largeHi, const unsigned long long *largeKeys,
+                                                  const unsigned *largeCellStart, const int *largeGlobalStart,
+                                                  float dt, int *counts, const int *offsets, int base,
+                                                  unsigned long long seqBase, StepCounters *cnt)
 {
-    __shared__ float4 sLo[LARGE_TILE], sHi[LARGE_TILE];
-    __shared__ int sId[LARGE_TILE];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = i < nBinned;
-    GridParams g = *gp;
-    unsigned akey = 0;
-    int a = 0;
-    float3 ac = f3(0, 0, 0);
-    float ar = 0.0f, aslack = 0.0f;
-    if (active)
-    {
-        unsigned long long ki = keys[i];
-        akey = (unsigned)(ki >> 32);
-        a = (int)(unsigned)ki;
-        ac = xyz(B.pos[a]);
-        ar = B.sizeRad[a].w;
-        aslack = len(xyz(B.vel[a])) * dt;
-    }
-    int found = 0;
-    int out = (EMIT && active) ? base + offsets[i] : 0;
     unsigned checks = 0, hits = 0, cons = 0;
-
-    auto hit = [&](int bIdx) {
-        hits++;
-        if (constrained(F, a, bIdx))
-        {
-            cons++;
-            return;
-        }
-        if (EMIT)
-        {
-            int m = out + found;
-            F.man.ab[m] = make_int2(a, bIdx);
-            F.man.seq[m] = seqBase + (unsigned long long)(m - base);
-            F.man.n[m] = 0;
-        }
-        found++;
-    };
-    auto test = [&](int j) {
-        checks++;
-        int bIdx = (int)(unsigned)keys[j];
-        float3 dp = sub(ac, xyz(B.pos[bIdx]));
-        float r = ar + B.sizeRad[bIdx].w;
-        if (!(dot(dp, dp) > r * r))
-            hit(bIdx);
-    };
-
     if (active)
     {
+        GridParams g = *gp;
+        unsigned long long ki = keys[i];
+        unsigned akey = (unsigned)(ki >> 32);
+        int a = (int)(unsigned)ki;
+        float3 ac = xyz(B.pos[a]);
+        float ar = B.sizeRad[a].w;
+        float aslack = len(xyz(B.vel[a])) * dt;
+        int found = 0;
+        int out = EMIT ? base + offsets[i] : 0;
+
+        auto hit = [&](int bIdx) {
+            hits++;
+            if (constrained(F, a, bIdx))
+            {
+                cons++;
+                return;
+            }
+            if (EMIT)
+            {
+                int m = out + found;
+                F.man.ab[m] = make_int2(a, bIdx);
+                F.man.seq[m] = seqBase + (unsigned long long)(m - base);
+                F.man.n[m] = 0;
+            }
+            found++;
+        };
+        auto test = [&](int j) {
+            checks++;
+            int bIdx = (int)(unsigned)keys[j];
+            float3 dp = sub(ac, xyz(B.pos[bIdx]));
+            float r = ar + B.sizeRad[bIdx].w;
+            if (!(dot(dp, dp) > r * r))
+                hit(bIdx);
+        };
+        const float margin4 = 4.0f * COLLISION_MARGIN;
+        auto test_large = [&](int l) {
+            float4 lo = largeLo[l], hi = largeHi[l];
+            float3 q = f3(rclamp(ac.x, lo.x, hi.x), rclamp(ac.y, lo.y, hi.y), rclamp(ac.z, lo.z, hi.z));
+            float3 dp = sub(ac, q);
+            float reach = ar + aslack + lo.w + margin4;
+            if (dot(dp, dp) > reach * reach)
+                return;
+            hit(large[l]);
+        };
+
         for (int j = i + 1; j < nBinned && (unsigned)(keys[j] >> 32) == akey; ++j)
             test(j);
         int ix = (int)(akey % (unsigned)g.nx);
@@ -374,37 +441,46 @@ __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, cons
             for (int j = (int)s; j < nBinned && (unsigned)(keys[j] >> 32) == nkey; ++j)
                 test(j);
         }
-    }
-    const float margin4 = 4.0f * COLLISION_MARGIN;
-    for (int t0 = 0; t0 < nLarge; t0 += LARGE_TILE)
-    {
-        int tn = min(LARGE_TILE, nLarge - t0);
-        __syncthreads();
-        for (int k = threadIdx.x; k < tn; k += blockDim.x)
+        if (nLarge > 0)
         {
-            sLo[k] = largeLo[t0 + k];
-            sHi[k] = largeHi[t0 + k];
-            sId[k] = large[t0 + k];
+            // the reference tests every large body; all that can pass are in these two lists
+            checks += (unsigned)nLarge;
+            unsigned cs = akey < CELL_TABLE_SIZE ? largeCellStart[akey] : 0xFFFFFFFFu;
+            int jc = cs == 0xFFFFFFFFu ? -1 : (int)cs;
+            int jg = *largeGlobalStart;
+            auto cellNext = [&]() -> unsigned {
+                if (jc < 0)
+                    return 0xFFFFFFFFu;
+                unsigned long long v = largeKeys[jc];
+                return (unsigned)(v >> 32) == akey ? (unsigned)v : 0xFFFFFFFFu;
+            };
+            auto globalNext = [&]() -> unsigned {
+                unsigned long long v = largeKeys[jg];
+                return ((unsigned)(v >> 32) == LARGE_GLOBAL && (unsigned)v < (unsigned)nLarge) ? (unsigned)v
+                                                                                                 : 0xFFFFFFFFu;
+            };
+            unsigned lc = cellNext(), lg = globalNext();
+            while (lc != 0xFFFFFFFFu || lg != 0xFFFFFFFFu)
+            {
+                if (lc < lg)
+                {
+                    test_large((int)lc);
+                    jc++;
+                    lc = cellNext();
+                }
+                else
+                {
+                    test_large((int)lg);
+                    jg++;
+                    lg = globalNext();
+                }
+            }
         }
-        __syncthreads();
-        if (!active)
-            continue;
-        for (int l = 0; l < tn; ++l)
-        {
-            checks++;
-            float4 lo = sLo[l], hi = sHi[l];
-            float3 q = f3(rclamp(ac.x, lo.x, hi.x), rclamp(ac.y, lo.y, hi.y), rclamp(ac.z, lo.z, hi.z));
-            float3 dp = sub(ac, q);
-            float reach = ar + aslack + lo.w + margin4;
-            if (dot(dp, dp) > reach * reach)
-                continue;
-            hit(sId[l]);
-        }
+        if (!EMIT)
+            counts[i] = found;
     }
     if (!EMIT)
     {
-        if (active)
-            counts[i] = found;
         warp_add(&cnt->pairChecks, checks);
         warp_add(&cnt->sphereHits, hits);
         warp_add(&cnt->constrainedHits, cons);
@@ -1165,63 +1241,159 @@ AVBD_DEV unsigned colour_priority(unsigned b)
     return h;
 }
 
-__global__ void k_colour_init(DevBodies B, const int *adjStart, int *state, int *remaining)
-{
-    int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= B.n)
-        return;
-    bool vertex = B.massMoment[b].x > 0 && adjStart[b + 1] > adjStart[b];
-    state[b] = vertex ? -1 : -2;
-    if (vertex)
-        atomicAdd(remaining, 1);
-}
+// Bounded grid-wide barrier for cooperative launches. Every wait has an iteration limit;
+// on expiry the kernel records an error and all blocks leave (the caller checks `error`).
+constexpr int MAX_COLOUR_ROUNDS = 4096;
+constexpr unsigned BARRIER_SPIN_LIMIT = 1u << 24;
 
-__global__ void k_colour_round(DevForces F, int n, int round, int *state, int *remaining, StepCounters *cnt)
+struct ColourControl
 {
-    int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= n || state[v] != -1)
-        return;
-    unsigned pv = colour_priority((unsigned)v);
-    unsigned long long used[4] = {0ull, 0ull, 0ull, 0ull};
-    for (int k = F.adjStart[v]; k < F.adjStart[v + 1]; ++k)
+    unsigned arrive;
+    unsigned generation;
+    int error;
+    int vertices;
+    int rounds;
+    int maxColour;
+    int coloured[MAX_COLOUR_ROUNDS];
+};
+
+AVBD_DEV bool grid_barrier(ColourControl *ctl)
+{
+    __syncthreads();
+    __shared__ int ok;
+    if (threadIdx.x == 0)
     {
-        unsigned e = F.adj[k];
-        if (adj_type(e) == ADJ_IGNORE)
-            continue;
-        int2 ab = force_bodies(F, e);
-        int u = ab.x == v ? ab.y : ab.x;
-        if (u < 0)
-            continue;
-        int s = state[u];
-        if (s == -2)
-            continue;
-        if (s == -1 || (s >> 16) == round)
+        volatile unsigned *gen = &ctl->generation;
+        unsigned g = *gen;
+        __threadfence();
+        if (atomicAdd(&ctl->arrive, 1u) == gridDim.x - 1)
         {
-            unsigned pu = colour_priority((unsigned)u);
-            if (!(pv > pu || (pv == pu && v > u)))
-                return;
+            ctl->arrive = 0;
+            __threadfence();
+            atomicAdd(&ctl->generation, 1u);
+            ok = 1;
         }
         else
         {
-            int c = s & 0xFFFF;
-            if (c < 256)
-                used[c >> 6] |= 1ull << (c & 63);
+            unsigned spins = 0;
+            while (*gen == g && ++spins < BARRIER_SPIN_LIMIT)
+                __nanosleep(64);
+            ok = spins < BARRIER_SPIN_LIMIT;
+            if (!ok)
+                atomicExch(&ctl->error, 1);
         }
+        __threadfence();
     }
-    int c = 0;
-    while (c < 256 && ((used[c >> 6] >> (c & 63)) & 1ull))
-        c++;
-    if (c >= 256)
-    {
-        cnt->error = DERR_TOO_MANY_COLOURS;
-        c = 255;
-    }
-    state[v] = (round << 16) | c;
-    atomicSub(remaining, 1);
-    atomicMax(&cnt->maxColour, c);
+    __syncthreads();
+    return ok && ((volatile int *)&ctl->error)[0] == 0;
 }
 
-__global__ void k_colour_keys(const int *state, int n, int *colour, unsigned long long *keys)
+AVBD_DEV int block_sum(int v)
+{
+    __shared__ int part[32];
+    v = __reduce_add_sync(0xFFFFFFFFu, v);
+    if ((threadIdx.x & 31) == 0)
+        part[threadIdx.x >> 5] = v;
+    __syncthreads();
+    int s = 0;
+    if (threadIdx.x < 32)
+    {
+        s = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0;
+        s = __reduce_add_sync(0xFFFFFFFFu, s);
+    }
+    __syncthreads();
+    return s; // valid in thread 0
+}
+
+// All Jones-Plassmann rounds in one cooperative launch. Priority mode 0: lower list index
+// first, which reproduces the sequential greedy colouring in list order; mode 1: hashed.
+__global__ void k_colour_all(DevBodies B, DevForces F, int n, int mode, int *state, ColourControl *ctl,
+                             StepCounters *cnt)
+{
+    const int stride = gridDim.x * blockDim.x;
+    int mine = 0;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += stride)
+    {
+        bool vertex = B.massMoment[b].x > 0 && F.adjStart[b + 1] > F.adjStart[b];
+        __stcg(&state[b], vertex ? -1 : -2);
+        mine += vertex ? 1 : 0;
+    }
+    int bs = block_sum(mine);
+    if (threadIdx.x == 0 && bs)
+        atomicAdd(&ctl->vertices, bs);
+    if (!grid_barrier(ctl))
+        return;
+    const int total = ((volatile int *)&ctl->vertices)[0];
+    int done = 0, round = 0;
+    for (; round < MAX_COLOUR_ROUNDS && done < total; ++round)
+    {
+        mine = 0;
+        for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride)
+        {
+            if (__ldcg(&state[v]) != -1)
+                continue;
+            unsigned pv = mode ? colour_priority((unsigned)v) : 0xFFFFFFFFu - (unsigned)v;
+            unsigned long long used[4] = {0ull, 0ull, 0ull, 0ull};
+            bool isMax = true;
+            for (int k = F.adjStart[v]; k < F.adjStart[v + 1]; ++k)
+            {
+                unsigned e = F.adj[k];
+                if (adj_type(e) == ADJ_IGNORE)
+                    continue;
+                int2 ab = force_bodies(F, e);
+                int u = ab.x == v ? ab.y : ab.x;
+                if (u < 0)
+                    continue;
+                int su = __ldcg(&state[u]);
+                if (su == -2)
+                    continue;
+                if (su == -1 || (su >> 16) == round)
+                {
+                    unsigned pu = mode ? colour_priority((unsigned)u) : 0xFFFFFFFFu - (unsigned)u;
+                    if (!(pv > pu || (pv == pu && v > u)))
+                    {
+                        isMax = false;
+                        break;
+                    }
+                }
+                else
+                {
+                    int c = su & 0xFFFF;
+                    if (c < 256)
+                        used[c >> 6] |= 1ull << (c & 63);
+                }
+            }
+            if (!isMax)
+                continue;
+            int c = 0;
+            while (c < 256 && ((used[c >> 6] >> (c & 63)) & 1ull))
+                c++;
+            if (c >= 256)
+            {
+                cnt->error = DERR_TOO_MANY_COLOURS;
+                c = 255;
+            }
+            __stcg(&state[v], (round << 16) | c);
+            atomicMax(&ctl->maxColour, c);
+            mine++;
+        }
+        bs = block_sum(mine);
+        if (threadIdx.x == 0 && bs)
+            atomicAdd(&ctl->coloured[round], bs);
+        if (!grid_barrier(ctl))
+            return;
+        done += ((volatile int *)ctl->coloured)[round];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+    {
+        ctl->rounds = round;
+        if (done < total)
+            ctl->error = 2;
+    }
+}
+
+// Solve-list keys: colour in the top 8 bits, body index (< 2^24) below; non-vertices last.
+__global__ void k_colour_keys(const int *state, int n, int *colour, unsigned *keys)
 {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= n)
@@ -1229,14 +1401,7 @@ __global__ void k_colour_keys(const int *state, int n, int *colour, unsigned lon
     int s = state[b];
     int c = s >= 0 ? (s & 0xFFFF) : -1;
     colour[b] = c;
-    keys[b] = c >= 0 ? (((unsigned long long)c << 32) | (unsigned)b) : 0xFFFFFFFFFFFFFFFFull;
-}
-
-__global__ void k_solve_list(const unsigned long long *keys, int count, int *list)
-{
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < count)
-        list[k] = (int)(unsigned)keys[k];
+    keys[b] = c >= 0 ? (((unsigned)c << 24) | (unsigned)b) : 0xFFFFFFFFu;
 }
 
 // ---------------------------------------------------------------------------
@@ -1268,7 +1433,17 @@ AVBD_DEV Pose load_pose(const DevBodies &B, int b)
     return s;
 }
 
-AVBD_DEV float mm_entry(const M3 &a, const M3 &b, int i, int j) { return dot(row(a, i), col(b, j)); }
+// a * diag(k): column j of a scaled by k[j]. The reference forms this product with full
+// row-by-column dots (jLinT * K, jAngT * K in manifold.cpp:218-221 and joint.cpp:89-95); the
+// two products with K's zero entries add +-0, which leaves every nonzero entry unchanged
+// and can only change the sign of an exact zero. These matrices feed only the left-hand
+// side, whose accumulators start at +0 or a positive mass term and so never hold -0: the
+// sums, and the step, are bit-identical.
+AVBD_DEV M3 times_diag(const M3 &a, float3 k)
+{
+    return rows(f3(a.r0.x * k.x, a.r0.y * k.y, a.r0.z * k.z), f3(a.r1.x * k.x, a.r1.y * k.y, a.r1.z * k.z),
+                f3(a.r2.x * k.x, a.r2.y * k.y, a.r2.z * k.z));
+}
 
 AVBD_DEV void store_terms(float *t, const M3 &LL, const M3 &LA, const M3 &LC, float3 RL, float3 RA)
 {
@@ -1349,12 +1524,12 @@ AVBD_DEV unsigned contact_term(const DevBodies &B, const DevForces &F, unsigned 
     M3 basis = rows(xyz(b0), xyz(bs[1]), xyz(bs[2]));
     ContactRec c = load_contact(F.man.contact + (size_t)m * 32 + 4 * ci);
     ContactEval e = eval_contact(A, Bp, basis, b0.w, c, alpha);
-    M3 K = diag(c.pen.x, c.pen.y, c.pen.z);
     const M3 &jLin = isA ? e.jALin : e.jBLin;
     const M3 &jAng = isA ? e.jAAng : e.jBAng;
     M3 jLinT = trans(jLin), jAngT = trans(jAng);
-    M3 jAngTk = mm(jAngT, K);
-    store_terms(t, mm(mm(jLinT, K), jLin), mm(jAngTk, jAng), mm(jAngTk, jLin), mv(jLinT, e.F), mv(jAngT, e.F));
+    M3 jAngTk = times_diag(jAngT, c.pen);
+    store_terms(t, mm(times_diag(jLinT, c.pen), jLin), mm(jAngTk, jAng), mm(jAngTk, jLin), mv(jLinT, e.F),
+                mv(jAngT, e.F));
     return KIND_FULL;
 }
 
@@ -1411,8 +1586,9 @@ AVBD_DEV unsigned joint_term(const DevBodies &B, const DevForces &F, unsigned j,
             M3 jLin = isA ? I : NI;
             M3 jAng = isA ? skew(neg(rAW)) : skew(rBW);
             M3 jLinT = trans(jLin), jAngT = trans(jAng);
-            M3 jAngTk = mm(jAngT, K);
-            store_terms(t, mm(mm(jLinT, K), jLin), mm(jAngTk, jAng), mm(jAngTk, jLin), mv(jLinT, Fv), mv(jAngT, Fv));
+            M3 jAngTk = times_diag(jAngT, penLin);
+            store_terms(t, mm(times_diag(jLinT, penLin), jLin), mm(jAngTk, jAng), mm(jAngTk, jLin), mv(jLinT, Fv),
+                        mv(jAngT, Fv));
             return KIND_FULL;
         }
         float3 r = isA ? rAW : neg(rBW);
@@ -1545,9 +1721,9 @@ AVBD_DEV void initial_system(const DevBodies &B, int b, float dt, float *t)
     store_terms(t, lhsLin, lhsAng, lhsCross, rhsLin, rhsAng);
 }
 
-template <int G, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_primal(DevBodies B, DevForces F, Params P, const int *list, int first,
-                                                  int count)
+template <int G, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_primal(DevBodies B, DevForces F, Params P, const int *list,
+                                                        int first, int count)
 {
     static_assert(BLOCK % G == 0 && 32 % G == 0, "group size");
     constexpr int GPB = BLOCK / G;

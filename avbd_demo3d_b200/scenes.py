@@ -440,3 +440,17 @@ def breakable(n: int = 10, m: int = 5, break_force: float = 90.0, params: Params
     for i in range(m):
         s.body((2, 1, 1), 1.0, 0.5, (0, 0, F32(i) * F32(2.0) + F32(8.0)))
     return s.build()
+
+
+def reference_pyramid(size: int = 16, params: Params | None = None) -> Scene:
+    """The reference's Pyramid scene (scenePyramid, scenes.h:59-68): 16 rows of 1x0.5x0.5
+    boxes at x = i*1.01 + r*0.5 - 8, z = r*0.85 + 0.5 on a static ground at z = -0.5,
+    with the solver's default parameters."""
+    s = SceneBuilder(f"refpyramid{size}", params or Params())
+    s.body((100, 100, 1), 0.0, 0.5, (0.0, 0.0, -0.5))
+    half = F32(size) / F32(2.0)
+    for r in range(size):
+        for i in range(size - r):
+            x = F32(i) * F32(1.01) + F32(r) * F32(0.5) - half
+            s.body((1, 0.5, 0.5), 1.0, 0.5, (x, 0.0, F32(r) * F32(0.85) + F32(0.5)))
+    return s.build()

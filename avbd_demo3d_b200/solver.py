@@ -260,6 +260,32 @@ class World:
                     "avbd_read_solve_order")
         return o[:k.value].copy()
 
+    @staticmethod
+    def primal_variants() -> list:
+        lib = _lib.load()
+        n = ctypes.c_int32()
+        lib.avbd_num_primal_variants(ctypes.byref(n), None, None)
+        g = np.zeros(n.value, np.int32)
+        m = np.zeros(n.value, np.int32)
+        lib.avbd_num_primal_variants(ctypes.byref(n), g.ctypes.data_as(_lib.c_int_p), m.ctypes.data_as(_lib.c_int_p))
+        return [{"group": int(a), "min_blocks": int(b)} for a, b in zip(g, m)]
+
+    def set_primal_variant(self, v: int):
+        self._check(self.lib.avbd_set_primal_variant(self.h, v), "avbd_set_primal_variant")
+
+    def autotune(self, repeats: int = 3):
+        """Time every primal variant on the current colouring and keep the fastest."""
+        n = len(self.primal_variants())
+        us = np.zeros(n, F32)
+        best = ctypes.c_int32()
+        self._check(self.lib.avbd_autotune(self.h, repeats, ctypes.byref(best), us.ctypes.data_as(_lib.c_float_p)),
+                    "avbd_autotune")
+        return best.value, us
+
+    def set_colouring(self, mode: int):
+        """0 = greedy colouring in list order (default), 1 = hashed priorities."""
+        self._check(self.lib.avbd_set_colouring(self.h, mode), "avbd_set_colouring")
+
     def set_profiling(self, on: bool = True):
         self._check(self.lib.avbd_set_profiling(self.h, 1 if on else 0), "avbd_set_profiling")
 

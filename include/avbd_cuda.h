@@ -177,6 +177,7 @@ typedef struct AvbdStats
     int64_t colours;
     int64_t colour_rounds;
     int64_t primal_rows;
+    int64_t grid_rescaled; /* 1 if the grid hit the reference's 2^22-cell cap this step */
     float step_ms;
 } AvbdStats;
 
@@ -251,6 +252,25 @@ typedef struct AvbdProfile
 } AvbdProfile;
 
 int avbd_set_profiling(AvbdContext *ctx, int32_t enable);
+
+/* Colouring of the primal sweep (no counterpart in the reference, whose CPU sweep is
+ * sequential in list order; the precedent is the WebGPU lane's greedy colouring in list
+ * order, avbd_gpu_solver.cpp:1817-1866). GREEDY (default) gives exactly that greedy
+ * colouring, computed in parallel as Jones-Plassmann with list-index priority; HASHED uses
+ * hashed priorities, which needs fewer rounds but sweeps in an order further from the
+ * reference's list order. */
+#define AVBD_COLOUR_GREEDY 0
+#define AVBD_COLOUR_HASHED 1
+int avbd_set_colouring(AvbdContext *ctx, int32_t mode);
+
+/* Autotuner for the primal sweep (no counterpart in the reference, whose primal loop is a
+ * serial CPU loop, solver.cpp:1177-1242). Variants differ in lanes per body and register
+ * budget; every variant gives bit-identical results. avbd_autotune times each variant on
+ * the current colouring (bodies' poses are restored after every trial) and selects the
+ * fastest; variant_us receives one time per variant (may be NULL). */
+int avbd_num_primal_variants(int32_t *count, int32_t *group, int32_t *min_blocks);
+int avbd_set_primal_variant(AvbdContext *ctx, int32_t variant);
+int avbd_autotune(AvbdContext *ctx, int32_t repeats, int32_t *best_variant, float *variant_us);
 int avbd_read_profile(AvbdContext *ctx, AvbdProfile *out);
 int avbd_reset_profile(AvbdContext *ctx);
 

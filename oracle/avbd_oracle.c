@@ -22,10 +22,11 @@
  * first (force.cpp:25-36). Here every force carries a creation sequence number and
  * per-body lists are rebuilt sorted by descending sequence, which is the same order.
  *
- * Colour order (orderMode 1): the primal sweep visits bodies grouped by a
- * Jones-Plassmann colouring of the dynamic-body constraint graph. Within one colour no
- * two bodies share a constraint, so this equals the reference run with its body list
- * relinked into colour order between prepareStep and iteratePrimalDualCpu.
+ * Colour order (orderMode 1 or 2): the primal sweep visits bodies grouped by a
+ * Jones-Plassmann colouring of the dynamic-body constraint graph (mode 1: priority by
+ * list index, equal to greedy colouring in list order; mode 2: hashed priority). Within
+ * one colour no two bodies share a constraint, so this equals the reference run with its
+ * body list relinked into colour order between prepareStep and iteratePrimalDualCpu.
  */
 #include "avbd_oracle.h"
 
@@ -1111,6 +1112,13 @@ uint32_t oracle_colour_priority(uint32_t b)
 
 static int prio_greater(uint32_t pv, int v, uint32_t pu, int u) { return pv > pu || (pv == pu && v > u); }
 
+/* orderMode 1: lower list index first, which makes the result the sequential greedy
+ * colouring in list order; orderMode 2: hashed priorities (fewer rounds). */
+static uint32_t priority_of(const OracleWorld *w, int v)
+{
+    return w->p.orderMode == 2 ? oracle_colour_priority((uint32_t)v) : 0xFFFFFFFFu - (uint32_t)v;
+}
+
 static int is_vertex(const OracleWorld *w, int b) { return b >= 0 && w->bodies[b].mass > 0 && degree(w, b) > 0; }
 
 static int other_end(const OracleWorld *w, const Incidence *e, int self)
@@ -1145,7 +1153,7 @@ static void colour_graph(OracleWorld *w)
             pick[v] = -1;
             if (round[v] != -1)
                 continue;
-            uint32_t pv = oracle_colour_priority((uint32_t)v);
+            uint32_t pv = priority_of(w, v);
             int isMax = 1;
             uint64_t used[4] = {0, 0, 0, 0};
             for (int k = w->adjStart[v]; k < w->adjStart[v + 1]; ++k)
@@ -1155,7 +1163,7 @@ static void colour_graph(OracleWorld *w)
                     continue;
                 if (round[u] == -1)
                 {
-                    if (!prio_greater(pv, v, oracle_colour_priority((uint32_t)u), u))
+                    if (!prio_greater(pv, v, priority_of(w, u), u))
                     {
                         isMax = 0;
                         break;
@@ -1268,7 +1276,7 @@ int oracle_prepare(OracleWorld *w)
             body->q = body->inertAng;
         }
     }
-    if (w->p.orderMode == 1)
+    if (w->p.orderMode == 1 || w->p.orderMode == 2)
         colour_graph(w);
     else
     {

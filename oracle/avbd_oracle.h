@@ -33,7 +33,8 @@ typedef struct OracleParams
     float betaAng;
     float gamma;
     int broadphase; /* 0 = all pairs, 1 = uniform grid (reference default), 2 = sweep and prune */
-    int orderMode;  /* 0 = primal sweep in list order, 1 = primal sweep in colour order */
+    int orderMode;  /* 0 = primal sweep in list order; colour order with 1 = list-index (greedy)
+                       priority, 2 = hashed priority */
 } OracleParams;
 
 enum

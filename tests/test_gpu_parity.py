@@ -37,9 +37,10 @@ def assert_same_state(g, o, where):
     assert np.array_equal(jg["broken"], jo["broken"]), where
 
 
-def lockstep(scene, steps, every=1):
+def lockstep(scene, steps, every=1, colour_mode=0):
     g = World(scene)
-    o = checkers.World(scene, "oracle", order_mode=1)
+    g.set_colouring(colour_mode)
+    o = checkers.World(scene, "oracle", order_mode=1 if colour_mode == 0 else 2)
     for s in range(1, steps + 1):
         g.step(1)
         o.step(1)
@@ -72,6 +73,28 @@ def test_small_scenes_bit_exact_60_steps(gpu, name):
 def test_pyramid_600_steps_matches_reference_fixture_pins(gpu):
     """The 210-box benchmark pyramid for the full 600 steps, checked every 20 steps."""
     lockstep(scenes.pyramid(20), 600, every=20)
+
+
+@pytest.mark.parametrize("name", ["pyramid20", "bridge", "mixed"])
+def test_hashed_colouring_mode(gpu, name):
+    """The alternative colouring (hashed priorities) is reproduced by the oracle as well."""
+    lockstep(SMALL[name](), 40, colour_mode=1)
+
+
+def test_grid_cell_cap_path(gpu):
+    """A box flung at 30 km/s stretches the grid past the reference's 2^22-cell cap, which
+    rescales cells with cbrtf (solver.cpp:341-357); the GPU stays bit-exact through it."""
+    sc = scenes.stack_grid(4, 4, 4, seed=12)
+    sc.vel[5] = (3.0e4, 3.0e4, 3.0e4)
+    g = World(sc)
+    o = checkers.World(sc, "oracle", order_mode=1)
+    rescaled = 0
+    for s in range(1, 21):
+        g.step(1)
+        o.step(1)
+        rescaled += g.stats()["grid_rescaled"]
+        assert_same_state(g, o, f"cap step {s}")
+    assert rescaled >= 10
 
 
 def test_all_pairs_broadphase(gpu):
@@ -115,12 +138,13 @@ def test_colour_order_fixture_from_reference(gpu):
 
 
 def test_list_order_drift_within_reference_gates(gpu):
-    """Against the reference's own list-order solve (what the CPU backend runs), the GPU's
-    colour-order sweep stays inside the reference's GPU-vs-CPU compare gates
-    (max position error < 0.05, viewer/package.json:24) over 120 frames."""
+    """Against the reference's own list-order solve (what its CPU backend runs), the GPU's
+    colour-order sweep stays inside the reference's GPU-vs-CPU compare gate (max position
+    error < 0.05 over 120 frames, viewer/package.json:24, native-backend-compare.mjs:99-104)
+    on the gate's box scenes, Pyramid and Rope, at the solver's default parameters."""
     if not checkers.ref_available():
         pytest.skip("reference library not built")
-    for sc in (scenes.pyramid(20), scenes.rope(20), scenes.stack_grid(6, 6, 8, seed=3)):
+    for sc in (scenes.reference_pyramid(16), scenes.rope(20, params=scenes.Params())):
         g = World(sc)
         r = checkers.World(sc, "ref")
         worst = 0.0

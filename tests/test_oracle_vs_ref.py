@@ -62,3 +62,42 @@ def test_narrowphase_random_pairs():
         b = checkers.collide_boxes("ref", *(c[i] for c in cases))
         assert a[0] == b[0] and np.array_equal(a[1], b[1]), i
         assert np.array_equal(bits(a[2]), bits(b[2])) and np.array_equal(bits(a[3]), bits(b[3])), i
+
+
+def _greedy_order(w, n, sc):
+    """Sequential greedy colouring in list order, computed independently in Python."""
+    m, j = w.manifolds(), w.joints()
+    mass = w.body_props()["mass"]
+    adj = [[] for _ in range(n)]
+    deg = np.zeros(n, int)
+    sp = sc.ftype == scenes.FORCE_SPRING
+    springs = [(n - 1 - a, n - 1 - b) for a, b in zip(sc.fa[sp], sc.fb[sp])]
+    for a, b in [tuple(x) for x in m["ab"]] + [tuple(x) for x in j["ab"]] + springs:
+        if a >= 0:
+            deg[a] += 1
+        deg[b] += 1
+        if a >= 0 and mass[a] > 0 and mass[b] > 0:
+            adj[a].append(b)
+            adj[b].append(a)
+    col = -np.ones(n, int)
+    for v in range(n):
+        if mass[v] <= 0 or deg[v] == 0:
+            continue
+        used = {col[u] for u in adj[v] if col[u] >= 0}
+        c = 0
+        while c in used:
+            c += 1
+        col[v] = c
+    return np.array([v for c in range(col.max() + 1) for v in range(n) if col[v] == c], np.int32)
+
+
+def test_colour_mode_1_is_greedy_list_order():
+    """Jones-Plassmann with list-index priority equals sequential greedy colouring."""
+    for sc in (scenes.reference_pyramid(16), scenes.bridge(), scenes.mixed_drop(1500, 10, 12, 0.05,
+                                                                               extent=(24, 24, 16), seed=5)):
+        o = checkers.World(sc, "oracle", order_mode=1)
+        for _ in range(20):
+            o.prepare()
+            assert np.array_equal(o.solve_order(), _greedy_order(o, sc.n_bodies, sc)), sc.name
+            o.iterate()
+            o.finish()

@@ -105,6 +105,8 @@ SIGNATURES = {
                                         ctypes.POINTER(ctypes.c_void_p)]),
     "avbd_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     "avbd_set_colouring": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    "avbd_colour_graph_noalloc": (ctypes.c_int, [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                 ctypes.c_int32, ctypes.c_void_p, c_int_p, ctypes.c_void_p]),
     "avbd_num_primal_variants": (ctypes.c_int, [c_int_p, c_int_p, c_int_p]),
     "avbd_set_primal_variant": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     "avbd_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, c_int_p, c_float_p]),

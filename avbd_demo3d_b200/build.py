@@ -42,7 +42,8 @@ def nvcc() -> str:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not stale():
         return OUT
-    cmd = [nvcc(), *NVCC_FLAGS, "-o", OUT + ".tmp", os.path.join(CSRC, "avbd_capi.cu")]
+    cmd = [nvcc(), *NVCC_FLAGS, "-o", OUT + ".tmp", os.path.join(CSRC, "avbd_capi.cu"),
+           os.path.join(CSRC, "avbd_noalloc.cu")]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

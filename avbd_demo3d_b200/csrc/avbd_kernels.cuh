@@ -15,6 +15,7 @@
 // Reference behaviour each kernel reproduces is cited at the kernel.
 #pragma once
 
+#include "avbd_colour.cuh"
 #include "avbd_math.cuh"
 
 namespace avbd
@@ -1229,81 +1230,6 @@ __global__ void k_finish(DevBodies B, Params P)
 // only on the graph, so the CPU oracle reproduces it exactly.
 // state: -2 not a vertex, -1 uncoloured, else round << 16 | colour
 // ---------------------------------------------------------------------------
-
-AVBD_DEV unsigned colour_priority(unsigned b)
-{
-    unsigned h = b * 0x9E3779B1u + 0x7F4A7C15u;
-    h ^= h >> 16;
-    h *= 0x85EBCA6Bu;
-    h ^= h >> 13;
-    h *= 0xC2B2AE35u;
-    h ^= h >> 16;
-    return h;
-}
-
-// Bounded grid-wide barrier for cooperative launches. Every wait has an iteration limit;
-// on expiry the kernel records an error and all blocks leave (the caller checks `error`).
-constexpr int MAX_COLOUR_ROUNDS = 4096;
-constexpr unsigned BARRIER_SPIN_LIMIT = 1u << 24;
-
-struct ColourControl
-{
-    unsigned arrive;
-    unsigned generation;
-    int error;
-    int vertices;
-    int rounds;
-    int maxColour;
-    int coloured[MAX_COLOUR_ROUNDS];
-};
-
-AVBD_DEV bool grid_barrier(ColourControl *ctl)
-{
-    __syncthreads();
-    __shared__ int ok;
-    if (threadIdx.x == 0)
-    {
-        volatile unsigned *gen = &ctl->generation;
-        unsigned g = *gen;
-        __threadfence();
-        if (atomicAdd(&ctl->arrive, 1u) == gridDim.x - 1)
-        {
-            ctl->arrive = 0;
-            __threadfence();
-            atomicAdd(&ctl->generation, 1u);
-            ok = 1;
-        }
-        else
-        {
-            unsigned spins = 0;
-            while (*gen == g && ++spins < BARRIER_SPIN_LIMIT)
-                __nanosleep(64);
-            ok = spins < BARRIER_SPIN_LIMIT;
-            if (!ok)
-                atomicExch(&ctl->error, 1);
-        }
-        __threadfence();
-    }
-    __syncthreads();
-    return ok && ((volatile int *)&ctl->error)[0] == 0;
-}
-
-AVBD_DEV int block_sum(int v)
-{
-    __shared__ int part[32];
-    v = __reduce_add_sync(0xFFFFFFFFu, v);
-    if ((threadIdx.x & 31) == 0)
-        part[threadIdx.x >> 5] = v;
-    __syncthreads();
-    int s = 0;
-    if (threadIdx.x < 32)
-    {
-        s = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0;
-        s = __reduce_add_sync(0xFFFFFFFFu, s);
-    }
-    __syncthreads();
-    return s; // valid in thread 0
-}
 
 // All Jones-Plassmann rounds in one cooperative launch. Priority mode 0: lower list index
 // first, which reproduces the sequential greedy colouring in list order; mode 1: hashed.

@@ -263,6 +263,35 @@ int avbd_set_profiling(AvbdContext *ctx, int32_t enable);
 #define AVBD_COLOUR_HASHED 1
 int avbd_set_colouring(AvbdContext *ctx, int32_t mode);
 
+/* Constraint-graph colouring that allocates nothing. It has no counterpart in the
+ * reference (the reference's CPU solver sweeps bodies one by one and never colours them).
+ *
+ * For callers that cannot call cudaMalloc: code that runs inside another framework's
+ * memory pool or allocator, real-time loops that must not allocate after start-up, and
+ * hosts that have already reserved the whole GPU. It computes the same colouring as the
+ * primal sweep of avbd_step (Jones-Plassmann; mode AVBD_COLOUR_GREEDY or
+ * AVBD_COLOUR_HASHED) for a graph the caller passes as a neighbour list, using only a
+ * fixed scratch array compiled into the library: about 4 MiB that every GPU loading the
+ * library keeps until the process exits.
+ *
+ * Inputs and outputs are device pointers except num_colours (host): n bodies (at most
+ * AVBD_NOALLOC_MAX_BODIES), vertex[n] (non-zero = a body to colour), adj_start[n + 1] and
+ * adj_other[adj_start[n]] (neighbours of body b are adj_other[adj_start[b] ..
+ * adj_start[b + 1]); entries outside [0, n) are skipped), colour[n] receives the colour of
+ * each vertex and -1 elsewhere. Runs on cuda_stream (NULL = default stream) and waits for
+ * it before returning.
+ *
+ * The first call on a device sets that device up (looks up the scratch array's device
+ * address and the co-resident block count); make that first call before any stream
+ * capture. All calls share the one scratch array: calls that overlap on the GPU (other
+ * streams, other threads) race and must be serialised by the caller.
+ * Returns AVBD_OK, AVBD_ERR_ARGUMENT (bad arguments), AVBD_ERR_CAPACITY (n above the
+ * maximum, or more than 256 colours), AVBD_ERR_STATE (colouring did not finish) or
+ * AVBD_ERR_CUDA. */
+#define AVBD_NOALLOC_MAX_BODIES (1 << 20)
+int avbd_colour_graph_noalloc(int32_t n, const int32_t *vertex, const int32_t *adj_start, const int32_t *adj_other,
+                              int32_t mode, int32_t *colour, int32_t *num_colours, void *cuda_stream);
+
 /* Autotuner for the primal sweep (no counterpart in the reference, whose primal loop is a
  * serial CPU loop, solver.cpp:1177-1242). Variants differ in lanes per body and register
  * budget; every variant gives bit-identical results. avbd_autotune times each variant on

@@ -1,0 +1,29 @@
+"""The drop-in: the reference's own SimulationHost scenes stepped with the CUDA backend
+installed as Solver::physicsBackend (the C++ adapter in avbd_demo3d_b200/host), checked
+against the reference's CPU solver in the GPU's colour order (bit-exact) and against its
+CPU backend (the reference's GPU-vs-CPU compare gate: max position error < 0.05 over
+120 frames on Pyramid and Rope, viewer/package.json:24)."""
+import json
+import os
+import subprocess
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DROPIN = os.path.join(ROOT, "oracle", "_ref", "avbd_dropin")
+
+
+def test_reference_scenes_through_the_backend_adapter(gpu):
+    if not os.path.exists(DROPIN):
+        pytest.skip("drop-in harness not built (needs the reference sources: make -C oracle dropin)")
+    out = subprocess.run([DROPIN, "--frames", "120"], capture_output=True, text=True, timeout=600)
+    rows = [json.loads(l) for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(rows) == 15, out.stdout + out.stderr
+    for r in rows:
+        assert r["backend"].startswith("CUDA AVBD"), r
+        assert r["bit_exact_vs_colour_order_reference"], r
+    gates = {r["scene"]: r for r in rows}
+    for scene in ("Pyramid", "Rope"):
+        assert gates[scene]["max_position_error_vs_cpu_backend"] < 0.05, gates[scene]
+    assert out.returncode == 0, out.stderr

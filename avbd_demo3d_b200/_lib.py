@@ -89,6 +89,9 @@ SIGNATURES = {
     "avbd_load_world": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AvbdBodies), ctypes.POINTER(AvbdJoints),
                                        ctypes.POINTER(AvbdSprings), ctypes.POINTER(AvbdIgnores),
                                        ctypes.POINTER(AvbdManifolds), ctypes.c_int64]),
+    "avbd_load_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, c_int_p, ctypes.POINTER(AvbdBodies),
+                                       ctypes.POINTER(AvbdJoints), ctypes.POINTER(AvbdSprings),
+                                       ctypes.POINTER(AvbdIgnores), ctypes.POINTER(AvbdManifolds), ctypes.c_int64]),
     "avbd_write_bodies": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AvbdBodies)]),
     "avbd_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     "avbd_synchronize": (ctypes.c_int, [ctypes.c_void_p]),

@@ -44,7 +44,6 @@ struct ManBuf
 };
 
 constexpr int PRIMAL_BLOCK = 128;
-constexpr unsigned CELL_TABLE = CELL_TABLE_SIZE;
 
 // Primal kernel variants: lanes per body (G) and the occupancy target given to the
 // compiler (resident blocks per SM; 1 = no register cap).
@@ -68,6 +67,7 @@ struct AvbdContext
 {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaMemPool_t pool = nullptr; // stream-ordered device allocations of this context
     bool ownStream = false;
     std::string err;
     int errCode = 0;
@@ -78,17 +78,26 @@ struct AvbdContext
     DArr<float4> pos, quat, initLin, initAng, inertLin, inertAng, vel, angvel, prevVel, massMoment, sizeRad;
     DArr<float> friction;
 
-    std::vector<int> hBinned, hLarge;
-    float binnedRadius = 0.0f;
+    // worlds: static per-world classification, per-step grids (one grid per world)
+    int W = 1;
+    std::vector<int> hWorldStart;      // W + 1 body ranges
+    std::vector<int> hBinned, hLarge;  // world by world, body order
+    std::vector<int> hWorldLargeStart; // W + 1 ranges in hLarge
+    std::vector<int4> hLLItems;        // large-large work items
+    DArr<int> bodyWorld, worldStart, worldLargeStart, worldBinned;
+    DArr<float> binnedRadiusW;
+    DArr<int4> llItems;
     DArr<int> binned, large;
     DArr<float4> largeLo, largeHi, largeSphere;
-    DArr<int> llCount, llOffset, largeGlobalStart;
+    DArr<int> llCount, llOffset;
     DArr<unsigned long long> largeKeys, largeKeysAlt;
-    DArr<unsigned> largeCellStart;
     const unsigned long long *largeSorted = nullptr;
-    DArr<unsigned> bounds;
-    DArr<GridParams> grid;
-    DArr<unsigned> cellStart;
+    DArr<unsigned> bounds;  // 8 words per world
+    DArr<GridParams> grid;  // per world
+    DArr<int> cappedAny;
+    DArr<unsigned long long> cellHashKeys, largeHashKeys;
+    DArr<unsigned> cellHashVals, largeHashVals;
+    unsigned cellHashMask = 0, largeHashMask = 0;
     DArr<unsigned long long> bpKeys, bpKeysAlt;
     DArr<int> pairCount, pairOffset;
 
@@ -125,7 +134,9 @@ struct AvbdContext
     DArr<StepCounters> counters;
     StepCounters *hCounters = nullptr;
     long long *hScalars = nullptr; // pinned scratch for small readbacks
-    GridParams *hGrid = nullptr;   // pinned copy of the grid parameters
+    GridParams *hGrid = nullptr;   // pinned copy of the per-world grid parameters
+    size_t hGridCap = 0;
+    int *hCapped = nullptr;        // pinned: any world over the cell cap
     float4 *hStage = nullptr;      // pinned staging for body state transfers
     size_t hStageCap = 0;
     cudaEvent_t stageDone = nullptr; // staging copies issued before this event are complete
@@ -191,6 +202,8 @@ int fail(AvbdContext *ctx, int code, const char *fmt, ...)
                         __LINE__);                                                                                 \
     } while (0)
 
+// Growth is stream-ordered (the context's memory pool keeps freed blocks cached), so a
+// buffer that grows mid-run never synchronises the device.
 template <class T>
 int reserve(AvbdContext *ctx, DArr<T> &a, size_t count, bool preserve, size_t used = 0)
 {
@@ -199,13 +212,12 @@ int reserve(AvbdContext *ctx, DArr<T> &a, size_t count, bool preserve, size_t us
     size_t cap = std::max(count, a.cap + a.cap / 2);
     cap = std::max<size_t>(cap, 16);
     T *p = nullptr;
-    CU(cudaMalloc((void **)&p, cap * sizeof(T)));
+    CU(cudaMallocFromPoolAsync((void **)&p, cap * sizeof(T), ctx->pool, ctx->stream));
     if (a.p)
     {
         if (preserve && used)
             CU(cudaMemcpyAsync(p, a.p, std::min(used, a.cap) * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
-        CU(cudaStreamSynchronize(ctx->stream));
-        CU(cudaFree(a.p));
+        CU(cudaFreeAsync(a.p, ctx->stream));
     }
     a.p = p;
     a.cap = cap;
@@ -216,7 +228,7 @@ template <class T>
 void release(DArr<T> &a)
 {
     if (a.p)
-        cudaFree(a.p);
+        cudaFree(a.p); // only at destruction, after the stream has drained
     a.p = nullptr;
     a.cap = 0;
 }
@@ -334,6 +346,30 @@ DevForces dev_forces(AvbdContext *ctx)
     F.adjStart = ctx->adjStart.p;
     F.adj = ctx->adj.p;
     return F;
+}
+
+DevGrid dev_grid(AvbdContext *ctx)
+{
+    DevGrid G;
+    G.W = ctx->W;
+    G.bodyWorld = ctx->bodyWorld.p;
+    G.worldStart = ctx->worldStart.p;
+    G.binnedRadius = ctx->binnedRadiusW.p;
+    G.worldLargeStart = ctx->worldLargeStart.p;
+    G.bounds = ctx->bounds.p;
+    G.grid = ctx->grid.p;
+    G.cappedAny = ctx->cappedAny.p;
+    return G;
+}
+
+HashTable cell_hash(AvbdContext *ctx)
+{
+    return HashTable{ctx->cellHashKeys.p, ctx->cellHashVals.p, ctx->cellHashMask};
+}
+
+HashTable large_hash(AvbdContext *ctx)
+{
+    return HashTable{ctx->largeHashKeys.p, ctx->largeHashVals.p, ctx->largeHashMask};
 }
 
 Params dev_params(const AvbdParams &p)
@@ -463,20 +499,17 @@ void host_grid_cap(GridParams &g)
     g.capped = 0;
 }
 
-// Large bodies binned into the grid cells their inflated AABB touches (sorted (cell, index)
-// keys, a cell-start table, and the global run for bodies spanning too many cells).
+// Large bodies binned into the grid cells of their world that their inflated AABB touches:
+// sorted (world, cell, index) keys and a hash table of run starts, including each world's
+// global run for bodies spanning too many cells.
 int large_cell_lists(AvbdContext *ctx, int nL)
 {
-    int total = nL * LARGE_MAX_CELLS;
-    CU(cudaMemsetAsync(ctx->largeGlobalStart.p, 0, sizeof(int), ctx->stream));
+    ctx->largeSorted = ctx->largeKeys.p;
     if (!nL)
-    {
-        ctx->largeSorted = ctx->largeKeys.p;
         return AVBD_OK;
-    }
-    k_bp_large_cells<<<grid_for(nL, 128), 128, 0, ctx->stream>>>(ctx->largeLo.p, ctx->largeHi.p, nL, ctx->grid.p,
-                                                                   ctx->bounds.p, ctx->binnedRadius,
-                                                                   ctx->largeKeys.p);
+    int total = nL * LARGE_MAX_CELLS;
+    k_bp_large_cells<<<grid_for(nL, 128), 128, 0, ctx->stream>>>(dev_grid(ctx), ctx->large.p, ctx->largeLo.p,
+                                                                   ctx->largeHi.p, nL, ctx->largeKeys.p);
     LAUNCHED();
     cub::DoubleBuffer<unsigned long long> lk(ctx->largeKeys.p, ctx->largeKeysAlt.p);
     size_t bytes = 0;
@@ -485,25 +518,23 @@ int large_cell_lists(AvbdContext *ctx, int nL)
     CU(cub::DeviceRadixSort::SortKeys(ctx->cubTemp.p, bytes, lk, total, 0, 64, ctx->stream));
     ctx->launches++;
     ctx->largeSorted = lk.Current();
-    // sentinel after the sorted keys, and the global-run start defaults to it
+    // sentinel after the sorted keys: candidate walks stop at it
     CU(cudaMemsetAsync(lk.Current() + total, 0xFF, sizeof(unsigned long long), ctx->stream));
-    k_fill_int<<<1, 1, 0, ctx->stream>>>(ctx->largeGlobalStart.p, total);
-    LAUNCHED();
-    k_bp_large_global_start<<<grid_for(total, 256), 256, 0, ctx->stream>>>(lk.Current(), total, nL,
-                                                                             ctx->largeGlobalStart.p);
-    LAUNCHED();
-    k_bp_cell_start<<<grid_for(total, 256), 256, 0, ctx->stream>>>(lk.Current(), total, ctx->largeCellStart.p, 1);
+    CU(cudaMemsetAsync(ctx->largeHashKeys.p, 0xFF, sizeof(unsigned long long) * ((size_t)ctx->largeHashMask + 1),
+                       ctx->stream));
+    k_bp_hash_large_runs<<<grid_for(total, 256), 256, 0, ctx->stream>>>(lk.Current(), total, large_hash(ctx));
     LAUNCHED();
     return AVBD_OK;
 }
 
-// Broadphase: appends new manifolds after the existing ones.
+// Broadphase of every world: appends new manifolds after the existing ones.
 int broadphase(AvbdContext *ctx)
 {
     int n = ctx->n;
     if (n < 2)
         return AVBD_OK;
     DevBodies B = dev_bodies(ctx);
+    DevGrid G = dev_grid(ctx);
     float dt = ctx->params.dt;
     StepCounters *cnt = ctx->counters.p;
     int M0 = ctx->nMan;
@@ -514,10 +545,11 @@ int broadphase(AvbdContext *ctx)
         CHECK(reserve(ctx, ctx->pairCount, n, false));
         CHECK(reserve(ctx, ctx->pairOffset, n, false));
         DevForces F = dev_forces(ctx);
-        k_bp_all_pairs<false><<<grid_for(n, 128), 128, 0, ctx->stream>>>(B, F, n, ctx->pairCount.p, nullptr, 0, 0,
+        k_bp_all_pairs<false><<<grid_for(n, 128), 128, 0, ctx->stream>>>(B, F, G, n, ctx->pairCount.p, nullptr, 0, 0,
                                                                           cnt);
         LAUNCHED();
         CHECK(scan_counts(ctx, ctx->pairCount.p, ctx->pairOffset.p, n, 0));
+        ctx->launches++;
         k_total<<<1, 1, 0, ctx->stream>>>(ctx->pairOffset.p, ctx->pairCount.p, n, ctx->hScalars);
         LAUNCHED();
         CU(cudaStreamSynchronize(ctx->stream));
@@ -526,8 +558,8 @@ int broadphase(AvbdContext *ctx)
         {
             CHECK(reserve_manifolds(ctx, ctx->man[ctx->cur], (size_t)(M0 + P1), (size_t)M0));
             DevForces F2 = dev_forces(ctx);
-            k_bp_all_pairs<true><<<grid_for(n, 128), 128, 0, ctx->stream>>>(B, F2, n, nullptr, ctx->pairOffset.p, M0,
-                                                                             (unsigned long long)ctx->nextSeq, cnt);
+            k_bp_all_pairs<true><<<grid_for(n, 128), 128, 0, ctx->stream>>>(
+                B, F2, G, n, nullptr, ctx->pairOffset.p, M0, (unsigned long long)ctx->nextSeq, cnt);
             LAUNCHED();
         }
     }
@@ -535,9 +567,8 @@ int broadphase(AvbdContext *ctx)
     {
         if (mode != AVBD_BROADPHASE_GRID)
             return fail(ctx, AVBD_ERR_ARGUMENT, "broadphase mode %d is not implemented on the GPU", mode);
-        int nB = (int)ctx->hBinned.size(), nL = (int)ctx->hLarge.size();
-        int nChunks = (nL + LL_CHUNK - 1) / LL_CHUNK;
-        long long nLL = (long long)nL * nChunks;
+        const int nB = (int)ctx->hBinned.size(), nL = (int)ctx->hLarge.size();
+        const int nItems = (int)ctx->hLLItems.size();
         if (nL)
         {
             k_bp_large<<<grid_for(nL, 64), 64, 0, ctx->stream>>>(B, ctx->large.p, nL, dt, ctx->largeLo.p,
@@ -548,9 +579,9 @@ int broadphase(AvbdContext *ctx)
         ctx->hScalars[0] = 0;
         ctx->hScalars[1] = 0;
         DevForces F = dev_forces(ctx);
-        // keys -> sorted entries -> cell tables -> large-body lists -> counted new pairs
+        // keys -> sorted entries -> cell runs -> large-body lists -> counted new pairs
         auto counting_pass = [&]() -> int {
-            k_bp_keys<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(B, ctx->binned.p, nB, ctx->grid.p, ctx->bpKeys.p);
+            k_bp_keys<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(B, G, ctx->binned.p, nB, ctx->bpKeys.p);
             LAUNCHED();
             dk = cub::DoubleBuffer<unsigned long long>(ctx->bpKeys.p, ctx->bpKeysAlt.p);
             size_t bytes = 0;
@@ -558,13 +589,14 @@ int broadphase(AvbdContext *ctx)
             CHECK(ensure_temp(ctx, bytes));
             CU(cub::DeviceRadixSort::SortKeys(ctx->cubTemp.p, bytes, dk, nB, 0, 64, ctx->stream));
             ctx->launches++;
-            k_bp_cell_start<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(dk.Current(), nB, ctx->cellStart.p, 1);
+            CU(cudaMemsetAsync(ctx->cellHashKeys.p, 0xFF,
+                               sizeof(unsigned long long) * ((size_t)ctx->cellHashMask + 1), ctx->stream));
+            k_bp_hash_runs<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(dk.Current(), nB, cell_hash(ctx));
             LAUNCHED();
             CHECK(large_cell_lists(ctx, nL));
             k_bp_pairs<false><<<grid_for(nB, 128), 128, 0, ctx->stream>>>(
-                B, F, dk.Current(), nB, ctx->cellStart.p, ctx->grid.p, ctx->large.p, nL, ctx->largeLo.p,
-                ctx->largeHi.p, ctx->largeSorted, ctx->largeCellStart.p, ctx->largeGlobalStart.p, dt,
-                ctx->pairCount.p, nullptr, 0, 0, cnt);
+                B, F, G, dk.Current(), nB, cell_hash(ctx), ctx->large.p, ctx->largeLo.p, ctx->largeHi.p,
+                ctx->largeSorted, large_hash(ctx), dt, ctx->pairCount.p, nullptr, 0, 0, cnt);
             LAUNCHED();
             CHECK(scan_counts(ctx, ctx->pairCount.p, ctx->pairOffset.p, nB, 0));
             ctx->launches++;
@@ -573,53 +605,44 @@ int broadphase(AvbdContext *ctx)
             return AVBD_OK;
         };
         auto large_large_count = [&]() -> int {
-            if (nL > 1)
+            if (nItems > 0)
             {
-                CHECK(reserve(ctx, ctx->llCount, (size_t)nLL, false));
-                CHECK(reserve(ctx, ctx->llOffset, (size_t)nLL, false));
-                k_bp_large_large<false><<<grid_for(nLL, 128), 128, 0, ctx->stream>>>(
-                    F, ctx->large.p, ctx->largeSphere.p, nL, nChunks, ctx->llCount.p, nullptr, 0, 0, cnt);
+                k_bp_large_large<false><<<grid_for(nItems, 128), 128, 0, ctx->stream>>>(
+                    F, ctx->large.p, ctx->largeSphere.p, ctx->llItems.p, nItems, ctx->llCount.p, nullptr, 0, 0, cnt);
                 LAUNCHED();
-                CHECK(scan_counts(ctx, ctx->llCount.p, ctx->llOffset.p, (int)nLL, 0));
+                CHECK(scan_counts(ctx, ctx->llCount.p, ctx->llOffset.p, nItems, 0));
                 ctx->launches++;
-                k_total<<<1, 1, 0, ctx->stream>>>(ctx->llOffset.p, ctx->llCount.p, (int)nLL, ctx->hScalars + 1);
+                k_total<<<1, 1, 0, ctx->stream>>>(ctx->llOffset.p, ctx->llCount.p, nItems, ctx->hScalars + 1);
                 LAUNCHED();
             }
             return AVBD_OK;
         };
-        auto reset_tables = [&]() -> int {
-            k_bp_cell_start<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(dk.Current(), nB, ctx->cellStart.p, 0);
-            LAUNCHED();
-            if (nL)
-            {
-                int total = nL * LARGE_MAX_CELLS;
-                k_bp_cell_start<<<grid_for(total, 256), 256, 0, ctx->stream>>>(ctx->largeSorted, total,
-                                                                                 ctx->largeCellStart.p, 0);
-                LAUNCHED();
-            }
-            return AVBD_OK;
-        };
+        CU(cudaMemsetAsync(ctx->cappedAny.p, 0, sizeof(int), ctx->stream));
         if (nB)
         {
-            k_bp_bounds_init<<<1, 32, 0, ctx->stream>>>(ctx->bounds.p);
+            k_bp_bounds_init<<<grid_for(8ll * ctx->W, 256), 256, 0, ctx->stream>>>(ctx->bounds.p, ctx->W);
             LAUNCHED();
-            k_bp_bounds<<<std::min(grid_for(nB, 256), 148 * 4), 256, 0, ctx->stream>>>(B, ctx->binned.p, nB, dt,
-                                                                                          ctx->bounds.p);
+            k_bp_bounds<<<std::min(grid_for(nB, 256), 148 * 8), 256, 0, ctx->stream>>>(B, G, ctx->binned.p, nB, dt);
             LAUNCHED();
-            k_bp_params<<<1, 1, 0, ctx->stream>>>(ctx->bounds.p, ctx->binnedRadius, ctx->grid.p);
+            k_bp_params<<<grid_for(ctx->W, 128), 128, 0, ctx->stream>>>(G, ctx->worldBinned.p);
             LAUNCHED();
             CHECK(counting_pass());
         }
         CHECK(large_large_count());
-        CU(cudaMemcpyAsync(ctx->hGrid, ctx->grid.p, sizeof(GridParams), cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaMemcpyAsync(ctx->hCapped, ctx->cappedAny.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaMemcpyAsync(ctx->hCounters, cnt, sizeof(StepCounters), cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaStreamSynchronize(ctx->stream));
-        if (nB && ctx->hGrid->capped)
+        if (nB && *ctx->hCapped)
         {
-            // rare path: rescale the cells exactly as the reference does, then count again
-            CHECK(reset_tables());
-            host_grid_cap(*ctx->hGrid);
-            CU(cudaMemcpyAsync(ctx->grid.p, ctx->hGrid, sizeof(GridParams), cudaMemcpyHostToDevice, ctx->stream));
+            // rare path: rescale the capped worlds' cells exactly as the reference does, recount
+            CU(cudaMemcpyAsync(ctx->hGrid, ctx->grid.p, sizeof(GridParams) * ctx->W, cudaMemcpyDeviceToHost,
+                               ctx->stream));
+            CU(cudaStreamSynchronize(ctx->stream));
+            for (int w = 0; w < ctx->W; ++w)
+                if (ctx->hGrid[w].capped)
+                    host_grid_cap(ctx->hGrid[w]);
+            CU(cudaMemcpyAsync(ctx->grid.p, ctx->hGrid, sizeof(GridParams) * ctx->W, cudaMemcpyHostToDevice,
+                               ctx->stream));
             CU(cudaMemsetAsync(cnt, 0, sizeof(StepCounters), ctx->stream));
             CHECK(counting_pass());
             CHECK(large_large_count());
@@ -637,20 +660,18 @@ int broadphase(AvbdContext *ctx)
         if (P1 > 0)
         {
             k_bp_pairs<true><<<grid_for(nB, 128), 128, 0, ctx->stream>>>(
-                B, F, dk.Current(), nB, ctx->cellStart.p, ctx->grid.p, ctx->large.p, nL, ctx->largeLo.p,
-                ctx->largeHi.p, ctx->largeSorted, ctx->largeCellStart.p, ctx->largeGlobalStart.p, dt, nullptr,
-                ctx->pairOffset.p, M0, (unsigned long long)ctx->nextSeq, cnt);
+                B, F, G, dk.Current(), nB, cell_hash(ctx), ctx->large.p, ctx->largeLo.p, ctx->largeHi.p,
+                ctx->largeSorted, large_hash(ctx), dt, nullptr, ctx->pairOffset.p, M0,
+                (unsigned long long)ctx->nextSeq, cnt);
             LAUNCHED();
         }
         if (P2 > 0)
         {
-            k_bp_large_large<true><<<grid_for(nLL, 128), 128, 0, ctx->stream>>>(
-                F, ctx->large.p, ctx->largeSphere.p, nL, nChunks, nullptr, ctx->llOffset.p, (int)(M0 + P1),
+            k_bp_large_large<true><<<grid_for(nItems, 128), 128, 0, ctx->stream>>>(
+                F, ctx->large.p, ctx->largeSphere.p, ctx->llItems.p, nItems, nullptr, ctx->llOffset.p, (int)(M0 + P1),
                 (unsigned long long)(ctx->nextSeq + P1), cnt);
             LAUNCHED();
         }
-        if (nB)
-            CHECK(reset_tables());
     }
     ctx->stats.manifolds_created = P1 + P2;
     ctx->nMan = (int)(M0 + P1 + P2);
@@ -952,34 +973,92 @@ int upload_bodies(AvbdContext *ctx, const AvbdBodies *b, bool props)
     return AVBD_OK;
 }
 
-// Grid classification: bodies above the 95th-percentile bounding radius are "large"
-// (solver.cpp:297-329). Radii never change, so this is fixed per world.
-int classify_bodies(AvbdContext *ctx, const float *radius, int n)
+// Grid classification per world: bodies above the world's 95th-percentile bounding radius
+// are "large" (solver.cpp:297-329). Radii never change, so this is fixed per load. Worlds
+// with fewer than two bodies take no part in the broadphase (solver.cpp:292-293).
+int classify_bodies(AvbdContext *ctx, const float *radius)
 {
+    const int W = ctx->W;
     ctx->hBinned.clear();
     ctx->hLarge.clear();
-    if (n >= 2)
+    ctx->hLLItems.clear();
+    ctx->hWorldLargeStart.assign(1, 0);
+    std::vector<float> binnedR(W, 1e-3f);
+    std::vector<int> worldBinned(W, 0);
+    std::vector<int> bodyWorld(ctx->n);
+    for (int w = 0; w < W; ++w)
     {
-        std::vector<float> r(radius, radius + n);
-        size_t pct = std::min<size_t>((size_t)n - 1, (size_t)n * 95 / 100);
-        std::nth_element(r.begin(), r.begin() + pct, r.end());
-        ctx->binnedRadius = r[pct] > 1e-3f ? r[pct] : 1e-3f;
-        for (int i = 0; i < n; ++i)
-            (radius[i] > ctx->binnedRadius ? ctx->hLarge : ctx->hBinned).push_back(i);
+        int b0 = ctx->hWorldStart[w], b1 = ctx->hWorldStart[w + 1], nw = b1 - b0;
+        for (int b = b0; b < b1; ++b)
+            bodyWorld[b] = w;
+        if (nw >= 2)
+        {
+            std::vector<float> r(radius + b0, radius + b1);
+            size_t pct = std::min<size_t>((size_t)nw - 1, (size_t)nw * 95 / 100);
+            std::nth_element(r.begin(), r.begin() + pct, r.end());
+            binnedR[w] = r[pct] > 1e-3f ? r[pct] : 1e-3f;
+            int l0 = (int)ctx->hLarge.size();
+            for (int b = b0; b < b1; ++b)
+            {
+                if (radius[b] > binnedR[w])
+                    ctx->hLarge.push_back(b);
+                else
+                {
+                    ctx->hBinned.push_back(b);
+                    worldBinned[w]++;
+                }
+            }
+            int L = (int)ctx->hLarge.size() - l0;
+            int chunks = (L + LL_CHUNK - 1) / LL_CHUNK;
+            for (int i = 0; i < L; ++i)
+                for (int c = 0; c < chunks; ++c)
+                    ctx->hLLItems.push_back(make_int4(l0, L, i, c));
+        }
+        ctx->hWorldLargeStart.push_back((int)ctx->hLarge.size());
     }
-    int nB = (int)ctx->hBinned.size(), nL = (int)ctx->hLarge.size();
+    int nB = (int)ctx->hBinned.size(), nL = (int)ctx->hLarge.size(), nI = (int)ctx->hLLItems.size();
+    CHECK(upload(ctx, ctx->bodyWorld, bodyWorld.data(), ctx->n));
+    CHECK(upload(ctx, ctx->worldStart, ctx->hWorldStart.data(), (size_t)W + 1));
+    CHECK(upload(ctx, ctx->worldLargeStart, ctx->hWorldLargeStart.data(), (size_t)W + 1));
+    CHECK(upload(ctx, ctx->worldBinned, worldBinned.data(), W));
+    CHECK(upload(ctx, ctx->binnedRadiusW, binnedR.data(), W));
     CHECK(upload(ctx, ctx->binned, ctx->hBinned.data(), nB));
     CHECK(upload(ctx, ctx->large, ctx->hLarge.data(), nL));
+    CHECK(upload(ctx, ctx->llItems, ctx->hLLItems.data(), nI));
+    CHECK(reserve(ctx, ctx->llCount, std::max(nI, 1), false));
+    CHECK(reserve(ctx, ctx->llOffset, std::max(nI, 1), false));
     CHECK(reserve(ctx, ctx->largeLo, std::max(nL, 1), false));
     CHECK(reserve(ctx, ctx->largeHi, std::max(nL, 1), false));
     CHECK(reserve(ctx, ctx->largeSphere, std::max(nL, 1), false));
     CHECK(reserve(ctx, ctx->largeKeys, (size_t)std::max(nL, 1) * LARGE_MAX_CELLS + 1, false));
     CHECK(reserve(ctx, ctx->largeKeysAlt, (size_t)std::max(nL, 1) * LARGE_MAX_CELLS + 1, false));
-    CHECK(reserve(ctx, ctx->largeGlobalStart, 1, false));
     CHECK(reserve(ctx, ctx->bpKeys, std::max(nB, 1), false));
     CHECK(reserve(ctx, ctx->bpKeysAlt, std::max(nB, 1), false));
-    CHECK(reserve(ctx, ctx->pairCount, std::max(n, 1), false));
-    CHECK(reserve(ctx, ctx->pairOffset, std::max(n, 1), false));
+    CHECK(reserve(ctx, ctx->pairCount, std::max(ctx->n, 1), false));
+    CHECK(reserve(ctx, ctx->pairOffset, std::max(ctx->n, 1), false));
+    CHECK(reserve(ctx, ctx->bounds, 8 * (size_t)W, false));
+    CHECK(reserve(ctx, ctx->grid, W, false));
+    CHECK(reserve(ctx, ctx->cappedAny, 1, false));
+    auto pow2 = [](size_t x) {
+        size_t p = 64;
+        while (p < x)
+            p <<= 1;
+        return p;
+    };
+    size_t ch = pow2(2 * (size_t)nB), lh = pow2(2 * ((size_t)nL * LARGE_MAX_CELLS + W));
+    CHECK(reserve(ctx, ctx->cellHashKeys, ch, false));
+    CHECK(reserve(ctx, ctx->cellHashVals, ch, false));
+    CHECK(reserve(ctx, ctx->largeHashKeys, lh, false));
+    CHECK(reserve(ctx, ctx->largeHashVals, lh, false));
+    ctx->cellHashMask = (unsigned)(ch - 1);
+    ctx->largeHashMask = (unsigned)(lh - 1);
+    if (ctx->hGridCap < (size_t)W)
+    {
+        if (ctx->hGrid)
+            CU(cudaFreeHost(ctx->hGrid));
+        CU(cudaMallocHost((void **)&ctx->hGrid, sizeof(GridParams) * W));
+        ctx->hGridCap = W;
+    }
     return AVBD_OK;
 }
 
@@ -1014,10 +1093,23 @@ int avbd_create(AvbdContext **out, int32_t device_ordinal, void *cuda_stream)
         }
         ctx->ownStream = true;
     }
+    {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device_ordinal;
+        if (cudaMemPoolCreate(&ctx->pool, &props) != cudaSuccess)
+        {
+            avbd_destroy(ctx);
+            return AVBD_ERR_CUDA;
+        }
+        unsigned long long keep = ~0ull; // keep freed blocks for reuse instead of returning them
+        cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     if (cudaMallocHost((void **)&ctx->hCounters, sizeof(StepCounters)) != cudaSuccess ||
         cudaMallocHost((void **)&ctx->hScalars, sizeof(long long) * 16) != cudaSuccess ||
         cudaMallocHost((void **)&ctx->hColourSummary, sizeof(int) * 4) != cudaSuccess ||
-        cudaMallocHost((void **)&ctx->hGrid, sizeof(GridParams)) != cudaSuccess ||
+        cudaMallocHost((void **)&ctx->hCapped, sizeof(int)) != cudaSuccess ||
         cudaMallocHost((void **)&ctx->hColourStarts, sizeof(int) * 257) != cudaSuccess ||
         cudaEventCreate(&ctx->evStart) != cudaSuccess || cudaEventCreate(&ctx->evStop) != cudaSuccess)
     {
@@ -1032,14 +1124,11 @@ int avbd_create(AvbdContext **out, int32_t device_ordinal, void *cuda_stream)
         ctx->colourBlocks = std::max(1, sms * std::max(1, perSm));
     }
     if (reserve(ctx, ctx->counters, 1, false) || reserve(ctx, ctx->bounds, 8, false) ||
-        reserve(ctx, ctx->grid, 1, false) || reserve(ctx, ctx->cellStart, CELL_TABLE, false) ||
-        reserve(ctx, ctx->largeCellStart, CELL_TABLE, false))
+        reserve(ctx, ctx->grid, 1, false))
     {
         avbd_destroy(ctx);
         return AVBD_ERR_CUDA;
     }
-    cudaMemsetAsync(ctx->cellStart.p, 0xFF, sizeof(unsigned) * CELL_TABLE, ctx->stream);
-    cudaMemsetAsync(ctx->largeCellStart.p, 0xFF, sizeof(unsigned) * CELL_TABLE, ctx->stream);
     ctx->params.dt = 1.0f / 60.0f;
     ctx->params.gravity = -10.0f;
     ctx->params.iterations = 10;
@@ -1068,17 +1157,25 @@ void avbd_destroy(AvbdContext *ctx)
     release(ctx->large);
     release(ctx->bounds);
     release(ctx->grid);
-    release(ctx->cellStart);
+    release(ctx->bodyWorld);
+    release(ctx->worldStart);
+    release(ctx->worldLargeStart);
+    release(ctx->worldBinned);
+    release(ctx->binnedRadiusW);
+    release(ctx->llItems);
+    release(ctx->cappedAny);
+    release(ctx->cellHashKeys);
+    release(ctx->cellHashVals);
+    release(ctx->largeHashKeys);
+    release(ctx->largeHashVals);
     release(ctx->bpKeys);
     release(ctx->bpKeysAlt);
     release(ctx->pairCount);
     release(ctx->pairOffset);
     release(ctx->llCount);
     release(ctx->llOffset);
-    release(ctx->largeGlobalStart);
     release(ctx->largeKeys);
     release(ctx->largeKeysAlt);
-    release(ctx->largeCellStart);
     for (cudaEvent_t e : ctx->evPool)
         cudaEventDestroy(e);
     for (ManBuf &m : ctx->man)
@@ -1125,6 +1222,8 @@ void avbd_destroy(AvbdContext *ctx)
         cudaFreeHost(ctx->hColourSummary);
     if (ctx->hGrid)
         cudaFreeHost(ctx->hGrid);
+    if (ctx->hCapped)
+        cudaFreeHost(ctx->hCapped);
     if (ctx->hColourStarts)
         cudaFreeHost(ctx->hColourStarts);
     if (ctx->stageDone)
@@ -1133,6 +1232,8 @@ void avbd_destroy(AvbdContext *ctx)
         cudaEventDestroy(ctx->evStart);
     if (ctx->evStop)
         cudaEventDestroy(ctx->evStop);
+    if (ctx->pool)
+        cudaMemPoolDestroy(ctx->pool);
     if (ctx->ownStream && ctx->stream)
         cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -1164,26 +1265,49 @@ int avbd_set_params(AvbdContext *ctx, const AvbdParams *params)
 int avbd_load_world(AvbdContext *ctx, const AvbdBodies *bodies, const AvbdJoints *joints, const AvbdSprings *springs,
                     const AvbdIgnores *ignores, const AvbdManifolds *manifolds, int64_t next_seq)
 {
-    if (!ctx || !bodies)
+    int32_t ws[2] = {0, bodies ? bodies->count : 0};
+    return avbd_load_batch(ctx, 1, ws, bodies, joints, springs, ignores, manifolds, next_seq);
+}
+
+int avbd_load_batch(AvbdContext *ctx, int32_t num_worlds, const int32_t *world_start, const AvbdBodies *bodies,
+                    const AvbdJoints *joints, const AvbdSprings *springs, const AvbdIgnores *ignores,
+                    const AvbdManifolds *manifolds, int64_t next_seq)
+{
+    if (!ctx || !bodies || !world_start)
         return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
     if (ctx->errCode)
         return AVBD_ERR_LATCHED;
     int n = bodies->count;
     if (n < 0 || n >= (int)KEY_NO_BODY)
         return fail(ctx, AVBD_ERR_ARGUMENT, "body count %d out of range", n);
+    if (num_worlds < 1 || num_worlds >= (1 << 16))
+        return fail(ctx, AVBD_ERR_ARGUMENT, "world count %d out of range [1, 65535]", num_worlds);
+    if (world_start[0] != 0 || world_start[num_worlds] != n)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "world ranges must start at 0 and end at the body count");
+    for (int w = 0; w < num_worlds; ++w)
+        if (world_start[w + 1] < world_start[w])
+            return fail(ctx, AVBD_ERR_ARGUMENT, "world ranges must be non-decreasing");
     if (n > 0 && (!bodies->position3 || !bodies->size3 || !bodies->mass || !bodies->moment3 ||
                   !bodies->friction || !bodies->radius || !bodies->velocity3))
         return fail(ctx, AVBD_ERR_ARGUMENT, "missing body arrays");
     CU(cudaSetDevice(ctx->device));
     ctx->n = n;
+    ctx->W = num_worlds;
+    ctx->hWorldStart.assign(world_start, world_start + num_worlds + 1);
+    std::vector<int> worldOf(n);
+    for (int w = 0; w < num_worlds; ++w)
+        for (int b = world_start[w]; b < world_start[w + 1]; ++b)
+            worldOf[b] = w;
     CHECK(upload_bodies(ctx, bodies, true));
-    CHECK(classify_bodies(ctx, bodies->radius, n));
+    CHECK(classify_bodies(ctx, bodies->radius));
 
     auto check_ab = [&](const int32_t *ab, int count, bool allowWorldA) -> bool {
         for (int i = 0; i < count; ++i)
         {
             int a = ab[2 * i], b = ab[2 * i + 1];
             if (b < 0 || b >= n || a >= n || (a < 0 && !(allowWorldA && a == -1)) || a == b)
+                return false;
+            if (a >= 0 && worldOf[a] != worldOf[b]) // forces never join two worlds
                 return false;
         }
         return true;

@@ -73,8 +73,8 @@ struct DevForces
     unsigned *adj;
 };
 
-// Capacity of the cell-start table; the reference caps the grid at 2^22 cells.
-constexpr unsigned CELL_TABLE_SIZE = 1u << 22;
+// The reference caps each grid at 2^22 cells (solver.cpp:341-357).
+constexpr unsigned long long MAX_GRID_CELLS = 1ull << 22;
 
 struct GridParams
 {
@@ -144,10 +144,85 @@ AVBD_DEV bool constrained(const DevForces &F, int a, int b)
 }
 
 // ---------------------------------------------------------------------------
-// Broadphase: the reference's uniform grid (solver.cpp:284-486), run on the GPU.
-// Pairs come out in the reference's creation order: sorted entry i, then the rest of
-// its own cell, the 13 forward cells, the large bodies; large-large pairs last.
+// Broadphase: the reference's uniform grid (solver.cpp:284-486), one grid per world.
+// W independent worlds are stepped together (W = 1 for one solver); each keeps its own
+// 95th-percentile split, bounds, cell size, cell cap and large-body list, and pairs never
+// cross worlds. Pairs come out in each world's creation order: sorted entry i, then the
+// rest of its own cell, the 13 forward cells, the large bodies; large-large pairs last.
+// Grid cells are found through hash tables keyed by (world, cell).
 // ---------------------------------------------------------------------------
+
+struct DevGrid
+{
+    int W;
+    const int *bodyWorld;       // world of each body
+    const int *worldStart;      // W + 1 body ranges
+    const float *binnedRadius;  // per world
+    const int *worldLargeStart; // W + 1 ranges in the large-body list
+    unsigned *bounds;           // per world 8 words: ordered min xyz, max xyz, max binned slack
+    GridParams *grid;           // per world
+    int *cappedAny;
+};
+
+struct HashTable
+{
+    unsigned long long *keys;
+    unsigned *vals;
+    unsigned mask;
+};
+
+constexpr unsigned long long HASH_EMPTY = 0xFFFFFFFFFFFFFFFFull;
+constexpr unsigned HASH_NONE = 0xFFFFFFFFu;
+
+AVBD_DEV unsigned hash_slot(unsigned long long k, unsigned mask)
+{
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdull;
+    k ^= k >> 33;
+    k *= 0xc4ceb9fe1a85ec53ull;
+    k ^= k >> 33;
+    return (unsigned)k & mask;
+}
+
+AVBD_DEV void hash_insert(const HashTable &t, unsigned long long key, unsigned val)
+{
+    unsigned h = hash_slot(key, t.mask);
+    for (unsigned probe = 0; probe <= t.mask; ++probe)
+    {
+        unsigned long long prev = atomicCAS(&t.keys[h], HASH_EMPTY, key);
+        if (prev == HASH_EMPTY || prev == key)
+        {
+            t.vals[h] = val;
+            return;
+        }
+        h = (h + 1) & t.mask;
+    }
+}
+
+AVBD_DEV unsigned hash_find(const HashTable &t, unsigned long long key)
+{
+    unsigned h = hash_slot(key, t.mask);
+    for (unsigned probe = 0; probe <= t.mask; ++probe)
+    {
+        unsigned long long k = t.keys[h];
+        if (k == key)
+            return t.vals[h];
+        if (k == HASH_EMPTY)
+            return HASH_NONE;
+        h = (h + 1) & t.mask;
+    }
+    return HASH_NONE;
+}
+
+// Sorted grid entry: world (16 bits) | cell (22) | body (24); its run id (world, cell)
+// is key >> 24. Body indices within a world keep the world's list order.
+AVBD_DEV unsigned long long grid_key(int w, unsigned cell, int b)
+{
+    return ((unsigned long long)w << 46) | ((unsigned long long)cell << 24) | (unsigned)b;
+}
+AVBD_DEV int key_body(unsigned long long k) { return (int)(k & 0xFFFFFFull); }
+AVBD_DEV int key_world(unsigned long long k) { return (int)(k >> 46); }
+AVBD_DEV unsigned key_cell(unsigned long long k) { return (unsigned)((k >> 24) & 0x3FFFFFull); }
 
 AVBD_DEV unsigned float_order(float f)
 {
@@ -156,52 +231,59 @@ AVBD_DEV unsigned float_order(float f)
 }
 AVBD_DEV float float_unorder(unsigned u) { return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u); }
 
-__global__ void k_bp_bounds_init(unsigned *bounds)
+__global__ void k_bp_bounds_init(unsigned *bounds, int W)
 {
-    if (threadIdx.x < 3)
-        bounds[threadIdx.x] = 0xFFFFFFFFu; // min slots
-    else if (threadIdx.x < 7)
-        bounds[threadIdx.x] = 0u; // max slots; [6] = largest binned slack (non-negative float bits)
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= 8 * W)
+        return;
+    int slot = k & 7;
+    bounds[k] = slot < 3 ? 0xFFFFFFFFu : 0u; // min slots, then max slots and the largest binned slack
 }
 
-__global__ void k_bp_bounds(DevBodies B, const int *binned, int nBinned, float dt, unsigned *bounds)
+// Bounds of each world's binned centres and its largest binned travel slack
+// (solver.cpp:306-333); warps inside one world reduce before their atomics.
+__global__ void k_bp_bounds(DevBodies B, DevGrid G, const int *binned, int nBinned, float dt)
 {
-    unsigned lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, hi[3] = {0u, 0u, 0u};
-    float slack = 0.0f;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nBinned; k += gridDim.x * blockDim.x)
+    for (int k0 = blockIdx.x * blockDim.x; k0 < nBinned; k0 += gridDim.x * blockDim.x)
     {
-        int b = binned[k];
-        float4 p = B.pos[b];
-        unsigned v[3] = {float_order(p.x), float_order(p.y), float_order(p.z)};
-#pragma unroll
-        for (int d = 0; d < 3; ++d)
+        int k = k0 + threadIdx.x;
+        bool active = k < nBinned;
+        int b = active ? binned[k] : 0;
+        int w = active ? G.bodyWorld[b] : -1;
+        unsigned v[7] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u, 0u};
+        if (active)
         {
-            lo[d] = min(lo[d], v[d]);
-            hi[d] = max(hi[d], v[d]);
+            float4 p = B.pos[b];
+            v[0] = v[3] = float_order(p.x);
+            v[1] = v[4] = float_order(p.y);
+            v[2] = v[5] = float_order(p.z);
+            v[6] = __float_as_uint(len(xyz(B.vel[b])) * dt);
         }
-        slack = fmaxf(slack, len(xyz(B.vel[b])) * dt);
-    }
-    unsigned sl = __float_as_uint(slack);
-#pragma unroll
-    for (int d = 0; d < 3; ++d)
-    {
-        lo[d] = __reduce_min_sync(0xFFFFFFFFu, lo[d]);
-        hi[d] = __reduce_max_sync(0xFFFFFFFFu, hi[d]);
-    }
-    sl = __reduce_max_sync(0xFFFFFFFFu, sl);
-    if ((threadIdx.x & 31) == 0)
-    {
-#pragma unroll
-        for (int d = 0; d < 3; ++d)
+        int w0 = __shfl_sync(0xFFFFFFFFu, w, 0);
+        bool uniform = __all_sync(0xFFFFFFFFu, w == w0 || w < 0);
+        if (uniform)
         {
-            atomicMin(&bounds[d], lo[d]);
-            atomicMax(&bounds[3 + d], hi[d]);
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                v[d] = __reduce_min_sync(0xFFFFFFFFu, v[d]);
+#pragma unroll
+            for (int d = 3; d < 7; ++d)
+                v[d] = __reduce_max_sync(0xFFFFFFFFu, v[d]);
+            if ((threadIdx.x & 31) != 0 || w0 < 0)
+                continue;
+            w = w0;
         }
-        atomicMax(&bounds[6], sl);
+        else if (!active)
+            continue;
+        unsigned *bw = G.bounds + 8 * w;
+        for (int d = 0; d < 3; ++d)
+            atomicMin(&bw[d], v[d]);
+        for (int d = 3; d < 7; ++d)
+            atomicMax(&bw[d], v[d]);
     }
 }
 
-// World AABB plus travel slack of the few bodies too large for the grid (solver.cpp:311-327)
+// World AABB plus travel slack of the bodies too large for the grid (solver.cpp:311-327)
 __global__ void k_bp_large(DevBodies B, const int *large, int nLarge, float dt, float4 *lo, float4 *hi,
                            float4 *sphere)
 {
@@ -225,92 +307,123 @@ __global__ void k_bp_large(DevBodies B, const int *large, int nLarge, float dt, 
     sphere[k] = f4(p, sr.w);
 }
 
-// Cell size and grid dimensions (solver.cpp:338-357). When the cell count exceeds the cap
-// the reference grows the cells by cbrtf factors; that rescaling is redone on the host with
-// the C library's cbrtf (the one the reference calls), so the device only flags it and
-// leaves a bounded placeholder grid.
-__global__ void k_bp_params(const unsigned *bounds, float binnedRadius, GridParams *gp)
+// Cell size and grid dimensions per world (solver.cpp:338-357). When the cell count
+// exceeds the cap the reference grows the cells by cbrtf factors; that rescaling is redone
+// on the host with the C library's cbrtf (the one the reference calls), so the device only
+// flags it and leaves a one-cell placeholder grid.
+__global__ void k_bp_params(DevGrid G, const int *worldBinned)
 {
-    float bminx = float_unorder(bounds[0]), bminy = float_unorder(bounds[1]), bminz = float_unorder(bounds[2]);
-    float bmaxx = float_unorder(bounds[3]), bmaxy = float_unorder(bounds[4]), bmaxz = float_unorder(bounds[5]);
-    float cellSize = binnedRadius * 2.0f;
-    const unsigned long long maxCells = 1ull << 22;
+    int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= G.W)
+        return;
+    GridParams g;
+    const unsigned *bw = G.bounds + 8 * w;
+    float cellSize = G.binnedRadius[w] * 2.0f;
+    if (worldBinned[w] == 0)
+    {
+        g.bminx = g.bminy = g.bminz = 0.0f;
+        g.extx = g.exty = g.extz = 0.0f;
+        g.cellSize = g.cellSize0 = cellSize;
+        g.nx = g.ny = g.nz = 1;
+        g.numCells = 1;
+        g.capped = 0;
+        G.grid[w] = g;
+        return;
+    }
+    float bminx = float_unorder(bw[0]), bminy = float_unorder(bw[1]), bminz = float_unorder(bw[2]);
+    float bmaxx = float_unorder(bw[3]), bmaxy = float_unorder(bw[4]), bmaxz = float_unorder(bw[5]);
     float3 extent = f3(bmaxx - bminx, bmaxy - bminy, bmaxz - bminz);
-    gp->extx = extent.x;
-    gp->exty = extent.y;
-    gp->extz = extent.z;
-    gp->cellSize0 = cellSize;
+    g.extx = extent.x;
+    g.exty = extent.y;
+    g.extz = extent.z;
+    g.cellSize0 = cellSize;
     int nx = (int)(extent.x / cellSize) + 1;
     int ny = (int)(extent.y / cellSize) + 1;
     int nz = (int)(extent.z / cellSize) + 1;
     unsigned long long numCells = (unsigned long long)nx * (unsigned long long)ny * (unsigned long long)nz;
-    gp->capped = numCells > maxCells ? 1 : 0;
-    if (numCells > maxCells)
+    g.capped = numCells > MAX_GRID_CELLS ? 1 : 0;
+    if (g.capped)
     {
         nx = ny = nz = 1;
         numCells = 1;
+        atomicOr(G.cappedAny, 1);
     }
-    gp->bminx = bminx;
-    gp->bminy = bminy;
-    gp->bminz = bminz;
-    gp->cellSize = cellSize;
-    gp->nx = nx;
-    gp->ny = ny;
-    gp->nz = nz;
-    gp->numCells = numCells;
+    g.bminx = bminx;
+    g.bminy = bminy;
+    g.bminz = bminz;
+    g.cellSize = cellSize;
+    g.nx = nx;
+    g.ny = ny;
+    g.nz = nz;
+    g.numCells = numCells;
+    G.grid[w] = g;
 }
-
-__global__ void k_bp_keys(DevBodies B, const int *binned, int nBinned, const GridParams *gp,
-                          unsigned long long *keys)
-{
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nBinned)
-        return;
-    int b = binned[k];
-    float4 c = B.pos[b];
-    GridParams g = *gp;
-    int ix = (int)rclamp((c.x - g.bminx) / g.cellSize, 0.0f, (float)(g.nx - 1));
-    int iy = (int)rclamp((c.y - g.bminy) / g.cellSize, 0.0f, (float)(g.ny - 1));
-    int iz = (int)rclamp((c.z - g.bminz) / g.cellSize, 0.0f, (float)(g.nz - 1));
-    unsigned key = (unsigned)(ix + g.nx * (iy + g.ny * iz));
-    if (g.numCells > CELL_TABLE_SIZE || key >= CELL_TABLE_SIZE)
-        key = 0; // only reachable with non-finite positions; the step reports DERR_TOO_MANY_CELLS
-    keys[k] = ((unsigned long long)key << 32) | (unsigned)b;
-}
-
-__global__ void k_bp_cell_start(const unsigned long long *keys, int nBinned, unsigned *cellStart, int set)
-{
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nBinned)
-        return;
-    unsigned key = (unsigned)(keys[k] >> 32);
-    if (key < CELL_TABLE_SIZE && (k == 0 || (unsigned)(keys[k - 1] >> 32) != key))
-        cellStart[key] = set ? (unsigned)k : 0xFFFFFFFFu;
-}
-
-// Large bodies are binned into the same grid with their AABB inflated by an upper bound of
-// the reference's reach (binned radius + travel slacks + 4 margins, solver.cpp:449-458), so a
-// binned body only tests the large bodies listed for its own cell; the reference's exact
-// predicate still decides every pair. Bodies spanning more than LARGE_MAX_CELLS cells (a
-// ground slab) go to a global list that every binned body tests.
-constexpr int LARGE_MAX_CELLS = 64;
-constexpr unsigned LARGE_GLOBAL = 0xFFFFFFFFu;
 
 AVBD_DEV int grid_axis(float x, float bmin, float cellSize, int n)
 {
     return (int)rclamp((x - bmin) / cellSize, 0.0f, (float)(n - 1));
 }
 
-__global__ void k_bp_large_cells(const float4 *largeLo, const float4 *largeHi, int nLarge, const GridParams *gp,
-                                 const unsigned *bounds, float binnedRadius, unsigned long long *keys)
+__global__ void k_bp_keys(DevBodies B, DevGrid G, const int *binned, int nBinned, unsigned long long *keys)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nBinned)
+        return;
+    int b = binned[k];
+    int w = G.bodyWorld[b];
+    float4 c = B.pos[b];
+    GridParams g = G.grid[w];
+    int ix = grid_axis(c.x, g.bminx, g.cellSize, g.nx);
+    int iy = grid_axis(c.y, g.bminy, g.cellSize, g.ny);
+    int iz = grid_axis(c.z, g.bminz, g.cellSize, g.nz);
+    unsigned cell = (unsigned)(ix + g.nx * (iy + g.ny * iz));
+    if (g.numCells > MAX_GRID_CELLS || cell >= MAX_GRID_CELLS)
+        cell = 0; // only with a placeholder grid or non-finite positions; that step is recounted
+    keys[k] = grid_key(w, cell, b);
+}
+
+// First entry of every (world, cell) run, into a hash table (the reference's cell-start table).
+__global__ void k_bp_hash_runs(const unsigned long long *keys, int n, HashTable t)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n)
+        return;
+    unsigned long long run = keys[k] >> 24;
+    if (keys[k] == HASH_EMPTY)
+        return;
+    if (k == 0 || (keys[k - 1] >> 24) != run)
+        hash_insert(t, run, (unsigned)k);
+}
+
+// Large bodies are binned into their world's grid with their AABB inflated by an upper
+// bound of the reference's reach (binned radius + travel slacks + 4 margins,
+// solver.cpp:449-458), so a binned body only tests the large bodies listed for its own
+// cell; the reference's exact predicate still decides every pair. Bodies spanning more than
+// LARGE_MAX_CELLS cells (ground slabs) go to their world's global list, which every binned
+// body of that world tests. Key: world (16) | global (1) | cell (22) | large index (24).
+constexpr int LARGE_MAX_CELLS = 64;
+
+AVBD_DEV unsigned long long large_key(int w, int global, unsigned cell, int l)
+{
+    return ((unsigned long long)w << 47) | ((unsigned long long)global << 46) | ((unsigned long long)cell << 24) |
+           (unsigned)l;
+}
+AVBD_DEV unsigned long long large_run(int w, int global, unsigned cell)
+{
+    return ((unsigned long long)w << 23) | ((unsigned long long)global << 22) | cell;
+}
+
+__global__ void k_bp_large_cells(DevGrid G, const int *large, const float4 *largeLo, const float4 *largeHi, int nLarge,
+                                 unsigned long long *keys)
 {
     int l = blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= nLarge)
         return;
-    GridParams g = *gp;
+    int w = G.bodyWorld[large[l]];
+    GridParams g = G.grid[w];
     float4 lo = largeLo[l], hi = largeHi[l];
-    float slackMax = __uint_as_float(bounds[6]);
-    float R = (binnedRadius + slackMax + lo.w + 4.0f * COLLISION_MARGIN) * 1.001f + 1.0e-4f;
+    float slackMax = __uint_as_float(G.bounds[8 * w + 6]);
+    float R = (G.binnedRadius[w] + slackMax + lo.w + 4.0f * COLLISION_MARGIN) * 1.001f + 1.0e-4f;
     int x0 = grid_axis(lo.x - R, g.bminx, g.cellSize, g.nx), x1 = grid_axis(hi.x + R, g.bminx, g.cellSize, g.nx);
     int y0 = grid_axis(lo.y - R, g.bminy, g.cellSize, g.ny), y1 = grid_axis(hi.y + R, g.bminy, g.cellSize, g.ny);
     int z0 = grid_axis(lo.z - R, g.bminz, g.cellSize, g.nz), z1 = grid_axis(hi.z + R, g.bminz, g.cellSize, g.nz);
@@ -319,30 +432,25 @@ __global__ void k_bp_large_cells(const float4 *largeLo, const float4 *largeHi, i
                   isfinite(hi.z) && isfinite(R);
     unsigned long long *out = keys + (size_t)l * LARGE_MAX_CELLS;
     int k = 0;
-    if (!finite || cells <= 0 || cells > LARGE_MAX_CELLS || g.numCells > CELL_TABLE_SIZE)
-        out[k++] = ((unsigned long long)LARGE_GLOBAL << 32) | (unsigned)l;
+    if (!finite || cells <= 0 || cells > LARGE_MAX_CELLS || g.numCells > MAX_GRID_CELLS)
+        out[k++] = large_key(w, 1, 0u, l);
     else
         for (int z = z0; z <= z1; ++z)
             for (int y = y0; y <= y1; ++y)
                 for (int x = x0; x <= x1; ++x)
-                    out[k++] = ((unsigned long long)(unsigned)(x + g.nx * (y + g.ny * z)) << 32) | (unsigned)l;
+                    out[k++] = large_key(w, 0, (unsigned)(x + g.nx * (y + g.ny * z)), l);
     for (; k < LARGE_MAX_CELLS; ++k)
-        out[k] = 0xFFFFFFFFFFFFFFFFull;
+        out[k] = HASH_EMPTY;
 }
 
-// First index of the global run in the sorted large-cell keys (or the run's end if empty).
-__global__ void k_bp_large_global_start(const unsigned long long *keys, int total, int nLarge, int *globalStart)
+__global__ void k_bp_hash_large_runs(const unsigned long long *keys, int n, HashTable t)
 {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= total)
+    if (k >= n || keys[k] == HASH_EMPTY)
         return;
-    auto isGlobal = [&](unsigned long long v) {
-        return (unsigned)(v >> 32) == LARGE_GLOBAL && (unsigned)v < (unsigned)nLarge;
-    };
-    bool here = isGlobal(keys[k]) || keys[k] == 0xFFFFFFFFFFFFFFFFull;
-    bool before = k > 0 && (isGlobal(keys[k - 1]) || keys[k - 1] == 0xFFFFFFFFFFFFFFFFull);
-    if (here && !before)
-        *globalStart = k;
+    unsigned long long run = keys[k] >> 24;
+    if (k == 0 || (keys[k - 1] >> 24) != run)
+        hash_insert(t, run, (unsigned)k);
 }
 
 __constant__ int c_forward[13][3] = {{1, 0, 0},   {-1, 1, 0}, {0, 1, 0},  {1, 1, 0}, {-1, -1, 1},
@@ -362,25 +470,26 @@ AVBD_DEV void warp_add(unsigned long long *dst, unsigned v)
 // One thread per sorted grid entry i (solver.cpp:405-465). EMIT == false counts new
 // (unconstrained) hits, EMIT == true writes them as fresh manifolds at base + offset[i] in
 // hit order. Large bodies are visited in list order: the entry's cell candidates merged
-// with the global list, both sorted by large index.
+// with its world's global list, both sorted by large index.
 template <bool EMIT>
-__global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, const unsigned long long *keys,
-                                                  int nBinned, const unsigned *cellStart, const GridParams *gp,
-                                                  const int *large, int nLarge, const float4 *largeLo,
-                                                  const float4 *largeHi, const unsigned long long *largeKeys,
-                                                  const unsigned *largeCellStart, const int *largeGlobalStart,
-                                                  float dt, int *counts, const int *offsets, int base,
-                                                  unsigned long long seqBase, StepCounters *cnt)
+__global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, DevGrid G, const unsigned long long *keys,
+                                                  int nBinned, HashTable cells, const int *large,
+                                                  const float4 *largeLo, const float4 *largeHi,
+                                                  const unsigned long long *largeKeys, HashTable largeCells, float dt,
+                                                  int *counts, const int *offsets, int base, unsigned long long seqBase,
+                                                  StepCounters *cnt)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = i < nBinned;
     unsigned checks = 0, hits = 0, cons = 0;
     if (active)
     {
-        GridParams g = *gp;
         unsigned long long ki = keys[i];
-        unsigned akey = (unsigned)(ki >> 32);
-        int a = (int)(unsigned)ki;
+        const int w = key_world(ki);
+        const unsigned akey = key_cell(ki);
+        const unsigned long long arun = ki >> 24;
+        const int a = key_body(ki);
+        GridParams g = G.grid[w];
         float3 ac = xyz(B.pos[a]);
         float ar = B.sizeRad[a].w;
         float aslack = len(xyz(B.vel[a])) * dt;
@@ -405,7 +514,7 @@ __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, cons
         };
         auto test = [&](int j) {
             checks++;
-            int bIdx = (int)(unsigned)keys[j];
+            int bIdx = key_body(keys[j]);
             float3 dp = sub(ac, xyz(B.pos[bIdx]));
             float r = ar + B.sizeRad[bIdx].w;
             if (!(dot(dp, dp) > r * r))
@@ -422,7 +531,7 @@ __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, cons
             hit(large[l]);
         };
 
-        for (int j = i + 1; j < nBinned && (unsigned)(keys[j] >> 32) == akey; ++j)
+        for (int j = i + 1; j < nBinned && (keys[j] >> 24) == arun; ++j)
             test(j);
         int ix = (int)(akey % (unsigned)g.nx);
         unsigned t = akey / (unsigned)g.nx;
@@ -433,47 +542,41 @@ __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, cons
             int cx = ix + c_forward[d][0], cy = iy + c_forward[d][1], cz = iz + c_forward[d][2];
             if (cx < 0 || cx >= g.nx || cy < 0 || cy >= g.ny || cz < 0 || cz >= g.nz)
                 continue;
-            unsigned nkey = (unsigned)(cx + g.nx * (cy + g.ny * cz));
-            if (nkey >= CELL_TABLE_SIZE)
+            unsigned long long nrun = ((unsigned long long)w << 22) | (unsigned)(cx + g.nx * (cy + g.ny * cz));
+            unsigned s = hash_find(cells, nrun);
+            if (s == HASH_NONE)
                 continue;
-            unsigned s = cellStart[nkey];
-            if (s == 0xFFFFFFFFu)
-                continue;
-            for (int j = (int)s; j < nBinned && (unsigned)(keys[j] >> 32) == nkey; ++j)
+            for (int j = (int)s; j < nBinned && (keys[j] >> 24) == nrun; ++j)
                 test(j);
         }
-        if (nLarge > 0)
+        const int nLargeW = G.worldLargeStart[w + 1] - G.worldLargeStart[w];
+        if (nLargeW > 0)
         {
-            // the reference tests every large body; all that can pass are in these two lists
-            checks += (unsigned)nLarge;
-            unsigned cs = akey < CELL_TABLE_SIZE ? largeCellStart[akey] : 0xFFFFFFFFu;
-            int jc = cs == 0xFFFFFFFFu ? -1 : (int)cs;
-            int jg = *largeGlobalStart;
-            auto cellNext = [&]() -> unsigned {
-                if (jc < 0)
+            // the reference tests every large body of the world; all that can pass are here
+            checks += (unsigned)nLargeW;
+            const unsigned long long crun = large_run(w, 0, akey), grun = large_run(w, 1, 0u);
+            unsigned cs = hash_find(largeCells, crun);
+            unsigned gs = hash_find(largeCells, grun);
+            int jc = cs == HASH_NONE ? -1 : (int)cs;
+            int jg = gs == HASH_NONE ? -1 : (int)gs;
+            auto next = [&](int j, unsigned long long run) -> unsigned {
+                if (j < 0)
                     return 0xFFFFFFFFu;
-                unsigned long long v = largeKeys[jc];
-                return (unsigned)(v >> 32) == akey ? (unsigned)v : 0xFFFFFFFFu;
+                unsigned long long v = largeKeys[j];
+                return (v != HASH_EMPTY && (v >> 24) == run) ? (unsigned)(v & 0xFFFFFFull) : 0xFFFFFFFFu;
             };
-            auto globalNext = [&]() -> unsigned {
-                unsigned long long v = largeKeys[jg];
-                return ((unsigned)(v >> 32) == LARGE_GLOBAL && (unsigned)v < (unsigned)nLarge) ? (unsigned)v
-                                                                                                 : 0xFFFFFFFFu;
-            };
-            unsigned lc = cellNext(), lg = globalNext();
+            unsigned lc = next(jc, crun), lg = next(jg, grun);
             while (lc != 0xFFFFFFFFu || lg != 0xFFFFFFFFu)
             {
                 if (lc < lg)
                 {
                     test_large((int)lc);
-                    jc++;
-                    lc = cellNext();
+                    lc = next(++jc, crun);
                 }
                 else
                 {
                     test_large((int)lg);
-                    jg++;
-                    lg = globalNext();
+                    lg = next(++jg, grun);
                 }
             }
         }
@@ -488,35 +591,36 @@ __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, cons
     }
 }
 
-// Large-vs-large pairs (solver.cpp:476-479), which the reference tests serially after
-// all grid pairs. Work item w = (i, chunk) covers j in one LL_CHUNK-wide slice of (i, n);
-// items in (i, chunk) order reproduce the serial i < j order.
+// Large-vs-large pairs of each world (solver.cpp:476-479), tested by the reference serially
+// after all grid pairs. Work item = (world's large base, world's large count, i, chunk); the
+// items are ordered by world, i, chunk, which reproduces each world's serial i < j order.
 template <bool EMIT>
-__global__ void k_bp_large_large(DevForces F, const int *large, const float4 *largeSphere, int nLarge, int nChunks,
-                                 int *counts, const int *offsets, int base, unsigned long long seqBase,
+__global__ void k_bp_large_large(DevForces F, const int *large, const float4 *largeSphere, const int4 *items,
+                                 int nItems, int *counts, const int *offsets, int base, unsigned long long seqBase,
                                  StepCounters *cnt)
 {
-    const long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool active = w < (long long)nLarge * nChunks;
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = w < nItems;
     unsigned checks = 0, hits = 0, cons = 0;
     if (active)
     {
-        int i = (int)(w / nChunks), c = (int)(w % nChunks);
-        int jBeg = max(i + 1, c * LL_CHUNK), jEnd = min(nLarge, (c + 1) * LL_CHUNK);
-        float4 si = largeSphere[i];
-        int a = large[i];
+        int4 it = items[w];
+        int lbase = it.x, nL = it.y, i = it.z, c = it.w;
+        int jBeg = max(i + 1, c * LL_CHUNK), jEnd = min(nL, (c + 1) * LL_CHUNK);
+        float4 si = largeSphere[lbase + i];
+        int a = large[lbase + i];
         int found = 0;
         int out = EMIT ? base + offsets[w] : 0;
         for (int j = jBeg; j < jEnd; ++j)
         {
             checks++;
-            float4 sj = largeSphere[j];
+            float4 sj = largeSphere[lbase + j];
             float3 dp = sub(xyz(si), xyz(sj));
             float r = si.w + sj.w;
             if (!(dot(dp, dp) <= r * r))
                 continue;
             hits++;
-            int b = large[j];
+            int b = large[lbase + j];
             if (constrained(F, a, b))
             {
                 cons++;
@@ -542,20 +646,21 @@ __global__ void k_bp_large_large(DevForces F, const int *large, const float4 *la
     }
 }
 
-// All-pairs broadphase (solver.cpp:176-185): thread per body a, pairs (a, b > a) in order.
+// All-pairs broadphase (solver.cpp:176-185): thread per body a, pairs (a, b > a) of its world.
 template <bool EMIT>
-__global__ void k_bp_all_pairs(DevBodies B, DevForces F, int n, int *counts, const int *offsets, int base,
+__global__ void k_bp_all_pairs(DevBodies B, DevForces F, DevGrid G, int n, int *counts, const int *offsets, int base,
                                unsigned long long seqBase, StepCounters *cnt)
 {
     int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= n)
         return;
+    int wEnd = G.worldStart[G.bodyWorld[a] + 1];
     float3 pa = xyz(B.pos[a]);
     float ra = B.sizeRad[a].w;
     int found = 0;
     int out = EMIT ? base + offsets[a] : 0;
     unsigned long long hits = 0, cons = 0;
-    for (int b = a + 1; b < n; ++b)
+    for (int b = a + 1; b < wEnd; ++b)
     {
         float3 dp = sub(pa, xyz(B.pos[b]));
         float r = ra + B.sizeRad[b].w;
@@ -579,7 +684,7 @@ __global__ void k_bp_all_pairs(DevBodies B, DevForces F, int n, int *counts, con
     if (!EMIT)
     {
         counts[a] = found;
-        atomicAdd(&cnt->pairChecks, (unsigned long long)(n - 1 - a));
+        atomicAdd(&cnt->pairChecks, (unsigned long long)(wEnd - 1 - a));
         atomicAdd(&cnt->sphereHits, hits);
         atomicAdd(&cnt->constrainedHits, cons);
     }

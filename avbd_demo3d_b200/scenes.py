@@ -454,3 +454,89 @@ def reference_pyramid(size: int = 16, params: Params | None = None) -> Scene:
             x = F32(i) * F32(1.01) + F32(r) * F32(0.5) - half
             s.body((1, 0.5, 0.5), 1.0, 0.5, (x, 0.0, F32(r) * F32(0.85) + F32(0.5)))
     return s.build()
+
+
+# ---------------------------------------------------------------------------
+# Batched uneven worlds
+# ---------------------------------------------------------------------------
+
+
+def _world_stack(b: SceneBuilder, n: int, rs: Stream):
+    """Columns of random height 1..16 on a 2 m pitch until n boxes (stack-grid distributions)."""
+    heights = []
+    left = n
+    while left > 0:
+        h = int(min(left, 1 + int(rs.uniform(1)[0] * 16)))
+        heights.append(h)
+        left -= h
+    cols = len(heights)
+    side = int(math.ceil(math.sqrt(cols)))
+    d = rs.uniform(n * 7).reshape(n, 7)
+    half = F32(0.25 + 0.5 * d[:, 0:3]).astype(np.float64)
+    pos = np.zeros((n, 3))
+    k = 0
+    for c, h in enumerate(heights):
+        gx, gy = c % side, c // side
+        z = 0.0
+        for _ in range(h):
+            pos[k] = ((gx - (side - 1) / 2.0) * 2.0 - 0.05 + 0.1 * d[k, 4],
+                      (gy - (side - 1) / 2.0) * 2.0 - 0.05 + 0.1 * d[k, 5], z + half[k, 2])
+            z += 2.0 * half[k, 2]
+            k += 1
+    b.bodies(2.0 * half, 0.5 + 1.5 * d[:, 3], 0.3 + 0.5 * d[:, 6], pos)
+
+
+def _world_chain(b: SceneBuilder, n: int, rs: Stream):
+    """One chain of n boxes linked by ball joints at touching face centres, first link
+    anchored to the world, laid out horizontally above the ground (links' half-extents
+    log-uniform in [0.1,1], one random yaw for the chain)."""
+    half = F32(rs.log_uniform(n * 3, 0.1, 1.0)).astype(np.float64).reshape(n, 3)
+    yaw = rs.uniform(1, 0.0, 2.0 * math.pi)[0]
+    q = np.array([0.0, 0.0, math.sin(yaw / 2), math.cos(yaw / 2)])
+    axis = np.array([math.cos(yaw), math.sin(yaw), 0.0])
+    offs = np.cumsum(2.0 * half[:, 0]) - half[:, 0]
+    start = np.array([0.0, 0.0, 2.0 + half[:, 1:].max() * 2.0])
+    pos = start[None, :] + (offs - offs.mean())[:, None] * axis[None, :]
+    first = b.bodies(2.0 * half, rs.uniform(n, 0.5, 2.0), rs.uniform(n, 0.3, 0.8), pos,
+                     quat=np.tile(q, (n, 1)))
+    b.joint(None, int(first[0]), pos[0] - axis * half[0, 0], (-half[0, 0], 0, 0))
+    for k in range(1, n):
+        b.joint(int(first[k - 1]), int(first[k]), (half[k - 1, 0], 0, 0), (-half[k, 0], 0, 0))
+
+
+def _world_pile(b: SceneBuilder, n: int, rs: Stream):
+    """n boxes with log-uniform half-extents and random orientations dropped from a volume:
+    jittered lattice points spaced beyond two bounding radii, so nothing overlaps at spawn."""
+    half = F32(rs.log_uniform(n * 3, 0.1, 1.0)).astype(np.float64).reshape(n, 3)
+    q = rs.unit_quaternions(n)
+    side = int(math.ceil(n ** (1.0 / 3.0)))
+    idx = np.arange(n)
+    lattice = np.stack([idx % side, (idx // side) % side, idx // (side * side)], axis=1).astype(np.float64)
+    spacing = 3.6
+    jitter = rs.uniform(n * 3, -0.05, 0.05).reshape(n, 3)
+    pos = (lattice - (side - 1) / 2.0) * spacing + jitter
+    pos[:, 2] += (side - 1) / 2.0 * spacing + 2.0
+    b.bodies(2.0 * half, rs.uniform(n, 0.5, 2.0), rs.uniform(n, 0.3, 0.8), pos,
+             quat=q / np.linalg.norm(q, axis=1, keepdims=True))
+
+
+def batched_worlds(n_worlds: int = 4096, seed: int = 3, lo: int = 8, hi: int = 2048,
+                   params: Params | None = None) -> list:
+    """Independent worlds with box counts log-uniform in [lo, hi]; each is, with equal
+    probability, a random-height stack field, a jointed chain or a drop pile (the mixed-scene
+    distributions), on its own static ground. 4,096 worlds is the batched benchmark."""
+    rs = Stream(seed)
+    counts = np.floor(np.exp(rs.uniform(n_worlds, math.log(lo), math.log(hi)))).astype(int)
+    kinds = (rs.uniform(n_worlds) * 3).astype(int)
+    worlds = []
+    for w in range(n_worlds):
+        b = SceneBuilder(f"world{w}", params or baseline_params())
+        n = int(counts[w])
+        extent = 40.0 + 4.0 * math.sqrt(n)
+        if kinds[w] == 1:
+            extent = max(extent, 4.0 * n)  # a chain lying down needs room
+        b.body((extent, extent, 1), 0.0, 0.5, (0, 0, -0.5))
+        wr = Stream(seed * 1000003 + w)
+        (_world_stack, _world_chain, _world_pile)[kinds[w]](b, n, wr)
+        worlds.append(b.build())
+    return worlds

@@ -77,19 +77,23 @@ def box_properties(size: np.ndarray, density: np.ndarray):
 
 
 class World:
-    """A scene resident on one GPU. Body arrays are in list order (index 0 = newest body,
-    the head of the reference's Solver::bodies)."""
+    """Scenes resident on one GPU. A single scene is one world; a list of scenes is a batch of
+    independent worlds stepped together (each evolves exactly as it would alone). Body
+    arrays are in list order per world (index 0 of a world = its newest body, the head of
+    the reference's Solver::bodies), worlds concatenated; `world_start` gives the ranges."""
 
-    def __init__(self, scene: _scenes.Scene, device: int = 0, stream: int | None = None):
+    def __init__(self, scene, device: int = 0, stream: int | None = None):
         self.lib = _lib.load()
         self.h = ctypes.c_void_p()
         rc = self.lib.avbd_create(ctypes.byref(self.h), device, stream)
         if rc != _lib.AVBD_OK:
             raise _lib.AvbdError(f"avbd_create failed ({rc}); is a CUDA device present?")
-        self.scene = scene
-        self.n = scene.n_bodies
-        self.set_params(scene.params)
-        self._load(scene)
+        self.scenes = list(scene) if isinstance(scene, (list, tuple)) else [scene]
+        self.scene = self.scenes[0]
+        self.n = sum(sc.n_bodies for sc in self.scenes)
+        self.world_start = np.concatenate([[0], np.cumsum([sc.n_bodies for sc in self.scenes])]).astype(np.int32)
+        self.set_params(self.scene.params)
+        self._load(self.scenes)
 
     # -- helpers
     def _check(self, rc: int, what: str):
@@ -118,75 +122,84 @@ class World:
         """Creation order -> list order (the reference prepends every new body)."""
         return np.ascontiguousarray(a[::-1])
 
-    def _load(self, sc: _scenes.Scene):
+    @staticmethod
+    def _scene_arrays(sc: _scenes.Scene, offset: int, seq0: int):
+        """One world's bodies (list order) and forces (global body indices, sequence numbers
+        from seq0 in creation order)."""
         n = sc.n_bodies
-        mass, moment, radius = box_properties(sc.size, sc.density)
-        L = self.list_order
-        self._body_arrays = dict(
-            position3=L(sc.pos), orientation4=L(sc.quat), velocity3=L(sc.vel), angular3=np.zeros((n, 3), F32),
-            prev_velocity3=L(sc.vel), size3=L(sc.size), mass=L(mass), moment3=L(moment), friction=L(sc.friction),
-            radius=L(radius))
-        self.props = {"mass": self._body_arrays["mass"], "moment": self._body_arrays["moment3"],
-                      "radius": self._body_arrays["radius"], "size": self._body_arrays["size3"],
-                      "friction": self._body_arrays["friction"]}
-        bodies = _lib.AvbdBodies(n, *[_ptr(self._body_arrays[k]) for k in (
-            "position3", "orientation4", "velocity3", "angular3", "prev_velocity3", "size3", "mass", "moment3",
-            "friction", "radius")])
-        # forces: creation index -> list index, sequence numbers in creation order
         if sc.n_forces and (sc.fb.min() < 0 or sc.fb.max() >= n or sc.fa.max() >= n or sc.fa.min() < -1):
             raise _lib.AvbdError("avbd_load_world failed (argument): force body index out of range")
-        to_list = lambda c: np.where(c >= 0, n - 1 - c, -1).astype(np.int32)
-        seq = np.arange(sc.n_forces, dtype=np.int64)
-        fa, fb = to_list(sc.fa), to_list(sc.fb)
+        mass, moment, radius = box_properties(sc.size, sc.density)
+        L = World.list_order
+        body = dict(position3=L(sc.pos), orientation4=L(sc.quat), velocity3=L(sc.vel),
+                    angular3=np.zeros((n, 3), F32), prev_velocity3=L(sc.vel), size3=L(sc.size), mass=L(mass),
+                    moment3=L(moment), friction=L(sc.friction), radius=L(radius))
+        local = lambda c: np.where(c >= 0, n - 1 - c, -1).astype(np.int32)
+        glob = lambda c: np.where(c >= 0, c + offset, -1).astype(np.int32)
+        seq = np.arange(seq0, seq0 + sc.n_forces, dtype=np.int64)
+        fa, fb = local(sc.fa), local(sc.fb)
         jm = sc.ftype == _scenes.FORCE_JOINT
         sm = sc.ftype == _scenes.FORCE_SPRING
         im = sc.ftype == _scenes.FORCE_IGNORE
-        lp = self._body_arrays["position3"]
-        lq = self._body_arrays["orientation4"]
-        lsize = self._body_arrays["size3"]
+        lp, lq, lsize = body["position3"], body["orientation4"], body["size3"]
         # joints (joint.cpp:25-33): torqueArm = lengthSq(sizeA + sizeB)
         J = int(jm.sum())
-        j_ab = _c(np.stack([fa[jm], fb[jm]], axis=1), np.int32, (J, 2))
         j_state = np.zeros((J, 28), F32)
         if J:
             sa = np.where((fa[jm] >= 0)[:, None], lsize[np.maximum(fa[jm], 0)], F32(0.0)).astype(F32)
             ssum = sa + lsize[fb[jm]]
             j_state[:, 0:3] = sc.frA[jm]
             j_state[:, 3:6] = sc.frB[jm]
-            j_state[:, 24] = sc.fparam[jm][:, 0]
-            j_state[:, 25] = sc.fparam[jm][:, 1]
-            j_state[:, 26] = sc.fparam[jm][:, 2]
+            j_state[:, 24:27] = sc.fparam[jm]
             j_state[:, 27] = _dot32(ssum, ssum)
         # springs (spring.cpp:14-25): rest < 0 -> initial distance of the anchor points
         S = int(sm.sum())
-        s_ab = _c(np.stack([fa[sm], fb[sm]], axis=1), np.int32, (S, 2))
         s_state = np.zeros((S, 8), F32)
         if S:
             a, b = fa[sm], fb[sm]
             rA, rB = sc.frA[sm], sc.frB[sm]
-            pA = rotate32(lq[a], rA) + lp[a]
-            pB = rotate32(lq[b], rB) + lp[b]
-            d = pA - pB
+            d = (rotate32(lq[a], rA) + lp[a]) - (rotate32(lq[b], rB) + lp[b])
             dist = np.sqrt(_dot32(d, d))
             rest = sc.fparam[sm][:, 1].copy()
-            rest = np.where(rest < 0, dist, rest).astype(F32)
             s_state[:, 0:3] = rA
             s_state[:, 3:6] = rB
-            s_state[:, 6] = rest
+            s_state[:, 6] = np.where(rest < 0, dist, rest).astype(F32)
             s_state[:, 7] = sc.fparam[sm][:, 0]
-        I = int(im.sum())
-        i_ab = _c(np.stack([fa[im], fb[im]], axis=1), np.int32, (I, 2))
-        self._force_arrays = dict(j_ab=j_ab, j_seq=_c(seq[jm], np.int64), j_state=j_state,
-                                  j_broken=np.zeros(J, np.int32), s_ab=s_ab, s_seq=_c(seq[sm], np.int64),
-                                  s_state=s_state, i_ab=i_ab, i_seq=_c(seq[im], np.int64))
-        fa_ = self._force_arrays
-        joints = _lib.AvbdJoints(J, _ptr(fa_["j_ab"]), _ptr(fa_["j_seq"]), _ptr(fa_["j_state"]), _ptr(fa_["j_broken"]))
-        springs = _lib.AvbdSprings(S, _ptr(fa_["s_ab"]), _ptr(fa_["s_seq"]), _ptr(fa_["s_state"]))
-        ignores = _lib.AvbdIgnores(I, _ptr(fa_["i_ab"]), _ptr(fa_["i_seq"]))
+        ab = lambda m: np.stack([glob(fa[m]), glob(fb[m])], axis=1).reshape(-1, 2).astype(np.int32)
+        forces = dict(j_ab=ab(jm), j_seq=seq[jm], j_state=j_state, j_broken=np.zeros(J, np.int32), s_ab=ab(sm),
+                      s_seq=seq[sm], s_state=s_state, i_ab=ab(im), i_seq=seq[im])
+        return body, forces
+
+    def _load(self, scenes_list):
+        bodies, forces = [], []
+        offset, seq0 = 0, 0
+        for sc in scenes_list:
+            b, f = self._scene_arrays(sc, offset, seq0)
+            bodies.append(b)
+            forces.append(f)
+            offset += sc.n_bodies
+            seq0 += sc.n_forces
+        self._body_arrays = {k: np.ascontiguousarray(np.concatenate([b[k] for b in bodies])) for k in bodies[0]}
+        self._force_arrays = {k: np.ascontiguousarray(np.concatenate([f[k] for f in forces])) for k in forces[0]}
+        for k in ("j_ab", "s_ab", "i_ab"):
+            self._force_arrays[k] = self._force_arrays[k].reshape(-1, 2).astype(np.int32)
+        self.props = {"mass": self._body_arrays["mass"], "moment": self._body_arrays["moment3"],
+                      "radius": self._body_arrays["radius"], "size": self._body_arrays["size3"],
+                      "friction": self._body_arrays["friction"]}
+        ba, fa_ = self._body_arrays, self._force_arrays
+        bodies_s = _lib.AvbdBodies(self.n, *[_ptr(ba[k]) for k in (
+            "position3", "orientation4", "velocity3", "angular3", "prev_velocity3", "size3", "mass", "moment3",
+            "friction", "radius")])
+        joints = _lib.AvbdJoints(len(fa_["j_seq"]), _ptr(fa_["j_ab"]), _ptr(fa_["j_seq"]), _ptr(fa_["j_state"]),
+                                 _ptr(fa_["j_broken"]))
+        springs = _lib.AvbdSprings(len(fa_["s_seq"]), _ptr(fa_["s_ab"]), _ptr(fa_["s_seq"]), _ptr(fa_["s_state"]))
+        ignores = _lib.AvbdIgnores(len(fa_["i_seq"]), _ptr(fa_["i_ab"]), _ptr(fa_["i_seq"]))
         manifolds = _lib.AvbdManifolds(0)
-        self._check(self.lib.avbd_load_world(self.h, ctypes.byref(bodies), ctypes.byref(joints), ctypes.byref(springs),
-                                             ctypes.byref(ignores), ctypes.byref(manifolds), sc.n_forces),
-                    "avbd_load_world")
+        ws = np.ascontiguousarray(self.world_start)
+        self._check(self.lib.avbd_load_batch(self.h, len(scenes_list), ws.ctypes.data_as(_lib.c_int_p),
+                                             ctypes.byref(bodies_s), ctypes.byref(joints), ctypes.byref(springs),
+                                             ctypes.byref(ignores), ctypes.byref(manifolds), seq0),
+                    "avbd_load_batch")
 
     # -- stepping
     def step(self, n: int = 1, sync: bool = True):

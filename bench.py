@@ -211,6 +211,7 @@ def run_cuda(args):
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(scene)
+    batched = batched_line(args, local, stream) if not args.no_batched else None
     w.close()
     if world_size > 1:
         dist.barrier()
@@ -223,11 +224,62 @@ def run_cuda(args):
                            "l2": "flushed before every timed step (256 MiB device write)",
                            "timing": "CUDA events on the solver stream, summed per step, max over ranks"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(),
-                "gpu_launches": prof["launches"], "phases_ms_per_step": phases,
+                "gpu_launches": prof["launches"], "phases_ms_per_step": phases, "batched": batched,
                 "autotune": {"primal_variant": World.primal_variants()[tuned],
                              "sweep_us": [round(float(x), 1) for x in variant_us]},
                 "step_ms_min_max": [min(step_ms), max(step_ms)]}
         print(json.dumps(line), flush=True)
+
+
+def batched_line(args, local, stream):
+    """World-steps/s of the 4,096-world uneven batch, one context, against looping the plain
+    single-world step over a sample of the same worlds (one resident context per world)."""
+    import torch
+
+    from avbd_demo3d_b200 import World, scenes
+
+    worlds = scenes.batched_worlds(4096, seed=3)
+    w = World(worlds, device=local, stream=stream.cuda_stream)
+    w.step(max(3, args.warmup))
+    steps = max(3, min(args.steps, 10))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+    w.step(steps, sync=False)
+    with torch.cuda.stream(stream):
+        ev1.record(stream)
+    torch.cuda.synchronize()
+    batched_s = ev0.elapsed_time(ev1) / 1e3
+    n_bodies = int(sum(sc.n_bodies - 1 for sc in worlds))
+    w.close()
+    # loop baseline: the plain step looped over a sample of worlds, each resident
+    sample = worlds[:: max(1, len(worlds) // 128)][:128]
+    ctxs = [World(sc, device=local, stream=stream.cuda_stream) for sc in sample]
+    for c in ctxs:
+        c.step(3)
+    loop_steps = 3
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+    for _ in range(loop_steps):
+        for c in ctxs:
+            c.step(1, sync=False)
+    with torch.cuda.stream(stream):
+        ev1.record(stream)
+    torch.cuda.synchronize()
+    loop_s = ev0.elapsed_time(ev1) / 1e3
+    for c in ctxs:
+        c.close()
+    batched_rate = len(worlds) * steps / batched_s
+    loop_rate = len(sample) * loop_steps / loop_s
+    return {"metric": "world-steps/s", "worlds": len(worlds), "bodies": n_bodies, "steps": steps,
+            "value": batched_rate, "ms_per_step": batched_s * 1e3 / steps,
+            "body_steps_per_s": n_bodies * steps / batched_s,
+            "loop_plain_step": {"value": loop_rate, "sample_worlds": len(sample), "steps": loop_steps},
+            "speedup_vs_loop": batched_rate / loop_rate,
+            "workload": "4,096 worlds, box counts log-uniform in [8, 2048] (seed 3): stack fields, jointed "
+                        "chains and drop piles, one ground each; same solver parameters"}
 
 
 def reference_world(scene):
@@ -291,6 +343,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("cuda", "reference"), default="cuda")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

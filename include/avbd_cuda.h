@@ -201,6 +201,17 @@ int avbd_load_world(AvbdContext *ctx, const AvbdBodies *bodies, const AvbdJoints
                     const AvbdSprings *springs, const AvbdIgnores *ignores, const AvbdManifolds *manifolds,
                     int64_t next_seq);
 
+/* Batched worlds: num_worlds independent worlds in one context, stepped together by one
+ * launch sequence per step (no counterpart in the reference, where each Solver is one
+ * world). Bodies are given world by world: world w owns bodies [world_start[w],
+ * world_start[w + 1]) in that world's list order; forces use these global indices and never
+ * join two worlds; sequence numbers must increase with creation time within each world.
+ * Every world keeps its own broadphase grid, so each evolves exactly as it would alone.
+ * avbd_load_world is this call with one world. */
+int avbd_load_batch(AvbdContext *ctx, int32_t num_worlds, const int32_t *world_start, const AvbdBodies *bodies,
+                    const AvbdJoints *joints, const AvbdSprings *springs, const AvbdIgnores *ignores,
+                    const AvbdManifolds *manifolds, int64_t next_seq);
+
 /* Overwrite body state only (positions/orientations/velocities edited between steps,
  * e.g. scenes.h:45). Same layout and order as avbd_load_world's bodies. */
 int avbd_write_bodies(AvbdContext *ctx, const AvbdBodies *bodies);

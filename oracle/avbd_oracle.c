@@ -257,6 +257,11 @@ typedef struct
     M3 basis;
     int n;
     float friction;
+    /* tape bookkeeping: index in the previous step's list (-1 = created this step), the
+     * matched previous contact of each contact (-1 = new) and its penalty clamp flags */
+    int oldIndex;
+    int srcSlot[8];
+    unsigned char iflags[8];
 } Manifold;
 
 typedef struct
@@ -316,6 +321,11 @@ struct OracleWorld
     int *solveOrder;
     int nSolve;
     int64_t counters[9];
+    /* frozen-branch tape (oracle_tape_begin) */
+    int recording;
+    int curIter;
+    OracleTapeStep *tape;
+    int tapeSteps, tapeCap;
 };
 
 static int cmp_incidence(const void *pa, const void *pb)
@@ -1051,10 +1061,12 @@ static int manifold_init(OracleWorld *w, Manifold *m)
         merged[i].key = nc[i].key;
         merged[i].rA = nc[i].rA;
         merged[i].rB = nc[i].rB;
+        m->srcSlot[i] = -1;
         for (int j = 0; j < m->n; ++j)
             if (nc[i].key == m->c[j].key)
             {
                 merged[i] = m->c[j];
+                m->srcSlot[i] = j;
                 if (!m->c[j].stick)
                 {
                     merged[i].rA = nc[i].rA;
@@ -1073,7 +1085,17 @@ static int manifold_init(OracleWorld *w, Manifold *m)
         V3 xB = vadd(B->pos, qrotate(B->q, c->rB));
         c->C0 = vadd(mvmul(m->basis, vsub(xA, xB)), v3(COLLISION_MARGIN, 0, 0));
         c->lambda = vmul(vmul(c->lambda, w->p.alpha), w->p.gamma);
-        c->penalty = vclampf(vmul(c->penalty, w->p.gamma), PENALTY_MIN, PENALTY_MAX);
+        V3 pg = vmul(c->penalty, w->p.gamma);
+        unsigned char f = 0;
+        for (int k = 0; k < 3; ++k)
+        {
+            if (VE(pg, k) > PENALTY_MAX)
+                f |= (unsigned char)(ORACLE_IF_HI_X << k);
+            else if (VE(pg, k) < PENALTY_MIN)
+                f |= (unsigned char)(ORACLE_IF_LO_X << k);
+        }
+        m->iflags[i] = f;
+        c->penalty = vclampf(pg, PENALTY_MIN, PENALTY_MAX);
     }
     return nn > 0;
 }
@@ -1203,10 +1225,17 @@ static void colour_graph(OracleWorld *w)
 /* Step                                                                      */
 /* ------------------------------------------------------------------------- */
 
+static void tape_begin_step(OracleWorld *w);
+static void tape_record_prepared(OracleWorld *w);
+
 int oracle_prepare(OracleWorld *w)
 {
     for (int k = 0; k < 9; ++k)
         w->counters[k] = 0;
+    if (w->recording)
+        tape_begin_step(w);
+    for (int i = 0; i < w->nMan; ++i)
+        w->man[i].oldIndex = i;
     /* broadphase (solver.cpp:1074-1083) */
     PairList hits = {0, 0, 0};
     if (w->p.broadphase == 1)
@@ -1229,6 +1258,7 @@ int oracle_prepare(OracleWorld *w)
         m->a = hits.v[k].a;
         m->b = hits.v[k].b;
         m->seq = w->nextSeq++;
+        m->oldIndex = -1;
     }
     w->counters[3] = hits.n;
     free(hits.v);
@@ -1260,9 +1290,23 @@ int oracle_prepare(OracleWorld *w)
         body->inertAng = qstep(body->q, vmul(body->angvel, dt));
         V3 accel = vdiv(vsub(body->vel, body->prevVel), dt);
         float accelExt = accel.z * rsign(g);
-        float accelWeight = rclamp(accelExt / fabsf(g), 0.0f, 1.0f);
+        float accelRaw = accelExt / fabsf(g);
+        float accelWeight = rclamp(accelRaw, 0.0f, 1.0f);
         if (!isfinite(accelWeight))
             accelWeight = 0.0f;
+        if (w->recording)
+        {
+            unsigned char f = 0;
+            if (body->mass > 0)
+                f |= ORACLE_BF_DYNAMIC;
+            if (degree(w, b) > 0)
+                f |= ORACLE_BF_FORCES;
+            if (isfinite(accelWeight) && accelRaw > 0.0f && accelRaw < 1.0f)
+                f |= ORACLE_BF_ACCEL_IN;
+            else if (accelWeight == 1.0f)
+                f |= ORACLE_BF_ACCEL_ONE;
+            w->tape[w->tapeSteps - 1].bodyFlags[b] = f;
+        }
         body->initLin = body->pos;
         body->initAng = body->q;
         if (body->mass > 0)
@@ -1291,6 +1335,8 @@ int oracle_prepare(OracleWorld *w)
     }
     w->counters[7] = w->nSolve;
     w->counters[8] = w->nColours;
+    if (w->recording)
+        tape_record_prepared(w);
     return 0;
 }
 
@@ -1322,6 +1368,7 @@ static void manifold_primal(const OracleWorld *w, const Manifold *m, int bodyIsA
                          mvmul(jAAng, dqAAng)),
                     mvmul(jBAng, dqBAng));
         V3 F = vadd(mvmul(K, C), c->lambda);
+        unsigned short flags = F.x < 0.0f ? 0 : ORACLE_EF_NCLAMP;
         F.x = rmin(F.x, 0.0f);
         float bounds = fabsf(F.x) * m->friction;
         float fs = sqrtf(F.y * F.y + F.z * F.z);
@@ -1329,6 +1376,13 @@ static void manifold_primal(const OracleWorld *w, const Manifold *m, int bodyIsA
         {
             F.y *= bounds / fs;
             F.z *= bounds / fs;
+            flags |= ORACLE_EF_CONE;
+        }
+        if (w->recording)
+        {
+            const OracleTapeStep *t = &w->tape[w->tapeSteps - 1];
+            size_t slot = (size_t)(m - w->man) * 8 + (size_t)i;
+            t->flags[((size_t)w->curIter * (size_t)t->nMan * 8 + slot) * 3 + (bodyIsA ? 0 : 1)] = flags;
         }
         M3 jLin = bodyIsA ? jALin : jBLin;
         M3 jAng = bodyIsA ? jAAng : jBAng;
@@ -1482,6 +1536,7 @@ static void manifold_dual(OracleWorld *w, Manifold *m, float alpha)
                          mvmul(jAAng, dqAAng)),
                     mvmul(jBAng, dqBAng));
         V3 F = vadd(mvmul(K, C), c->lambda);
+        unsigned short flags = F.x < 0.0f ? 0 : ORACLE_EF_NCLAMP;
         F.x = rmin(F.x, 0.0f);
         float bounds = fabsf(F.x) * m->friction;
         float fs = sqrtf(F.y * F.y + F.z * F.z);
@@ -1489,6 +1544,26 @@ static void manifold_dual(OracleWorld *w, Manifold *m, float alpha)
         {
             F.y *= bounds / fs;
             F.z *= bounds / fs;
+            flags |= ORACLE_EF_CONE;
+        }
+        if (w->recording)
+        {
+            if (fs <= bounds)
+                flags |= ORACLE_EF_RAMP_T;
+            for (int k = 0; k < 3; ++k)
+            {
+                float ck = VE(C, k);
+                if (ck < 0)
+                    flags |= (unsigned short)(ORACLE_EF_NEG_X << k);
+                else if (ck > 0)
+                    flags |= (unsigned short)(ORACLE_EF_POS_X << k);
+                int ramps = k == 0 ? F.x < 0 : fs <= bounds;
+                if (ramps && !(VE(c->penalty, k) + w->p.betaLin * fabsf(ck) < PENALTY_MAX))
+                    flags |= (unsigned short)(ORACLE_EF_CAP_X << k);
+            }
+            const OracleTapeStep *t = &w->tape[w->tapeSteps - 1];
+            size_t slot = (size_t)(m - w->man) * 8 + (size_t)i;
+            t->flags[((size_t)w->curIter * (size_t)t->nMan * 8 + slot) * 3 + 2] = flags;
         }
         c->lambda = F;
         if (F.x < 0)
@@ -1543,6 +1618,7 @@ int oracle_iterate(OracleWorld *w)
 {
     for (int it = 0; it < w->p.iterations; ++it)
     {
+        w->curIter = it;
         for (int k = 0; k < w->nSolve; ++k)
             body_primal(w, w->solveOrder[k]);
         for (int i = 0; i < w->nMan; ++i)
@@ -1674,6 +1750,7 @@ void oracle_destroy(OracleWorld *w)
 {
     if (!w)
         return;
+    oracle_tape_end(w);
     free(w->bodies);
     free(w->man);
     free(w->joints);
@@ -1873,4 +1950,141 @@ int oracle_collide_boxes(const float *posA3, const float *quatA4, const float *s
     }
     memcpy(basis9, &basis, 36);
     return n;
+}
+
+void oracle_get_params(const OracleWorld *w, OracleParams *out) { *out = w->p; }
+
+/* ------------------------------------------------------------------------- */
+/* Frozen-branch tape                                                        */
+/* ------------------------------------------------------------------------- */
+
+static void tape_free_step(OracleTapeStep *t)
+{
+    free(t->bodyIn);
+    free(t->bodyFlags);
+    free(t->ab);
+    free(t->basis);
+    free(t->friction);
+    free(t->ncontacts);
+    free(t->keys);
+    free(t->geo);
+    free(t->init);
+    free(t->src);
+    free(t->initFlags);
+    free(t->solveOrder);
+    free(t->colourStart);
+    free(t->flags);
+    memset(t, 0, sizeof(*t));
+}
+
+int oracle_tape_begin(OracleWorld *w)
+{
+    oracle_tape_end(w);
+    if (w->nJoints > 0 || w->nSprings > 0)
+        return -1;
+    w->recording = 1;
+    return 0;
+}
+
+void oracle_tape_end(OracleWorld *w)
+{
+    for (int s = 0; s < w->tapeSteps; ++s)
+        tape_free_step(&w->tape[s]);
+    free(w->tape);
+    w->tape = NULL;
+    w->tapeSteps = w->tapeCap = 0;
+    w->recording = 0;
+}
+
+int oracle_tape_steps(const OracleWorld *w) { return w->tapeSteps; }
+
+const OracleTapeStep *oracle_tape_step(const OracleWorld *w, int s)
+{
+    return s >= 0 && s < w->tapeSteps ? &w->tape[s] : NULL;
+}
+
+/* step start: body state before anything of the step runs */
+static void tape_begin_step(OracleWorld *w)
+{
+    if (w->tapeSteps == w->tapeCap)
+    {
+        w->tapeCap = w->tapeCap ? 2 * w->tapeCap : 64;
+        w->tape = (OracleTapeStep *)realloc(w->tape, sizeof(OracleTapeStep) * (size_t)w->tapeCap);
+    }
+    OracleTapeStep *t = &w->tape[w->tapeSteps++];
+    memset(t, 0, sizeof(*t));
+    size_t n = (size_t)(w->n > 0 ? w->n : 1);
+    t->bodyIn = (float *)calloc(n * 16, sizeof(float));
+    t->bodyFlags = (unsigned char *)calloc(n, 1);
+    for (int b = 0; b < w->n; ++b)
+    {
+        const Body *x = &w->bodies[b];
+        float *o = t->bodyIn + 16 * (size_t)b;
+        memcpy(o, &x->pos, 12);
+        memcpy(o + 3, &x->q, 16);
+        memcpy(o + 7, &x->vel, 12);
+        memcpy(o + 10, &x->angvel, 12);
+        memcpy(o + 13, &x->prevVel, 12);
+    }
+}
+
+/* end of prepare: the step's manifolds, their links to the previous step, the sweep order
+ * and room for the iteration flags */
+static void tape_record_prepared(OracleWorld *w)
+{
+    OracleTapeStep *t = &w->tape[w->tapeSteps - 1];
+    int M = w->nMan;
+    size_t m1 = (size_t)(M > 0 ? M : 1);
+    t->nMan = M;
+    t->iterations = w->p.iterations;
+    t->ab = (int *)calloc(m1 * 2, sizeof(int));
+    t->basis = (float *)calloc(m1 * 9, sizeof(float));
+    t->friction = (float *)calloc(m1, sizeof(float));
+    t->ncontacts = (int *)calloc(m1, sizeof(int));
+    t->keys = (int *)calloc(m1 * 8, sizeof(int));
+    t->geo = (float *)calloc(m1 * 8 * 6, sizeof(float));
+    t->init = (float *)calloc(m1 * 8 * 9, sizeof(float));
+    t->src = (int *)calloc(m1 * 8, sizeof(int));
+    t->initFlags = (unsigned char *)calloc(m1 * 8, 1);
+    for (int i = 0; i < M; ++i)
+    {
+        const Manifold *m = &w->man[i];
+        t->ab[2 * i] = m->a;
+        t->ab[2 * i + 1] = m->b;
+        memcpy(t->basis + 9 * (size_t)i, &m->basis, 36);
+        t->friction[i] = m->friction;
+        t->ncontacts[i] = m->n;
+        for (int k = 0; k < 8; ++k)
+        {
+            size_t slot = (size_t)i * 8 + (size_t)k;
+            t->src[slot] = -1;
+            if (k >= m->n)
+                continue;
+            const Contact *c = &m->c[k];
+            t->keys[slot] = c->key;
+            memcpy(t->geo + 6 * slot, &c->rA, 12);
+            memcpy(t->geo + 6 * slot + 3, &c->rB, 12);
+            memcpy(t->init + 9 * slot, &c->C0, 12);
+            memcpy(t->init + 9 * slot + 3, &c->lambda, 12);
+            memcpy(t->init + 9 * slot + 6, &c->penalty, 12);
+            t->initFlags[slot] = m->iflags[k];
+            if (m->oldIndex >= 0 && m->srcSlot[k] >= 0)
+                t->src[slot] = m->oldIndex * 8 + m->srcSlot[k];
+        }
+    }
+    t->nSolve = w->nSolve;
+    t->nColours = w->nColours;
+    t->solveOrder = (int *)calloc((size_t)(w->nSolve > 0 ? w->nSolve : 1), sizeof(int));
+    memcpy(t->solveOrder, w->solveOrder, sizeof(int) * (size_t)w->nSolve);
+    t->colourStart = (int *)calloc((size_t)w->nColours + 1, sizeof(int));
+    if (w->nColours > 0)
+    {
+        for (int k = 0; k < w->nSolve; ++k)
+            t->colourStart[w->colour[w->solveOrder[k]] + 1]++;
+        for (int c = 0; c < w->nColours; ++c)
+            t->colourStart[c + 1] += t->colourStart[c];
+    }
+    else
+        t->colourStart[0] = w->nSolve;
+    t->flags = (unsigned short *)calloc((size_t)w->p.iterations * m1 * 8 * 3, sizeof(unsigned short));
 }

@@ -104,6 +104,69 @@ int oracle_collide_boxes(const float *posA3, const float *quatA4, const float *s
 /* Colour priority used by the Jones-Plassmann colouring (shared contract with the CUDA path). */
 uint32_t oracle_colour_priority(uint32_t bodyIndex);
 
+void oracle_get_params(const OracleWorld *w, OracleParams *out);
+
+/* ------------------------------------------------------------------------- */
+/* Frozen-branch tape, for the checks of the differentiable step.            */
+/* ------------------------------------------------------------------------- */
+
+/* Branch outcomes recorded per contact evaluation (primal as body A, primal as body B,
+ * dual), per carried-over contact and per body. The values equal the EvalFlags,
+ * InitFlags and BodyFlags of avbd_demo3d_b200/csrc/avbd_diff.h. */
+enum
+{
+    ORACLE_EF_NCLAMP = 1,   /* F.n >= 0 -> 0 (manifold.cpp:201) */
+    ORACLE_EF_CONE = 2,     /* friction cone scaling (manifold.cpp:206-210) */
+    ORACLE_EF_RAMP_T = 4,   /* dual: tangential ramp (manifold.cpp:271) */
+    ORACLE_EF_CAP_X = 8,    /* dual: ramp reached PENALTY_MAX */
+    ORACLE_EF_CAP_Y = 16,
+    ORACLE_EF_CAP_Z = 32,
+    ORACLE_EF_NEG_X = 64,   /* dual: C < 0 */
+    ORACLE_EF_NEG_Y = 128,
+    ORACLE_EF_NEG_Z = 256,
+    ORACLE_EF_POS_X = 512,  /* dual: C > 0 */
+    ORACLE_EF_POS_Y = 1024,
+    ORACLE_EF_POS_Z = 2048,
+    ORACLE_IF_LO_X = 1,     /* carried penalty * gamma < PENALTY_MIN (manifold.cpp:170) */
+    ORACLE_IF_LO_Y = 2,
+    ORACLE_IF_LO_Z = 4,
+    ORACLE_IF_HI_X = 8,     /* carried penalty * gamma > PENALTY_MAX */
+    ORACLE_IF_HI_Y = 16,
+    ORACLE_IF_HI_Z = 32,
+    ORACLE_BF_DYNAMIC = 1,  /* mass > 0 */
+    ORACLE_BF_FORCES = 2,   /* non-empty force list */
+    ORACLE_BF_ACCEL_IN = 4, /* adaptive warm-start weight inside (0, 1) (solver.cpp:1146-1150) */
+    ORACLE_BF_ACCEL_ONE = 8 /* adaptive weight clamped at 1 */
+};
+
+/* One recorded step. Manifolds are the list after Manifold::initialize and removal, in
+ * creation order; contact slot = manifold * 8 + contact. */
+typedef struct OracleTapeStep
+{
+    int nMan, nSolve, nColours, iterations;
+    float *bodyIn;            /* n x 16: pos3 quat4 vel3 angvel3 prevVel3 at step start */
+    unsigned char *bodyFlags; /* n */
+    int *ab;                  /* nMan x 2 */
+    float *basis;             /* nMan x 9: rows normal, tangent 1, tangent 2 */
+    float *friction;          /* nMan */
+    int *ncontacts;           /* nMan */
+    int *keys;                /* nMan x 8 */
+    float *geo;               /* nMan x 8 x 6: rA, rB */
+    float *init;              /* nMan x 8 x 9: C0, lambda, penalty after initialization */
+    int *src;                 /* nMan x 8: slot in the previous step's list, -1 = new contact */
+    unsigned char *initFlags; /* nMan x 8 */
+    int *solveOrder;          /* nSolve, the primal sweep order */
+    int *colourStart;         /* nColours + 1 */
+    unsigned short *flags;    /* iterations x nMan x 8 x 3 */
+} OracleTapeStep;
+
+/* Start recording every following step (clears an earlier tape). Worlds with joints or
+ * springs are not recorded: the differentiable step covers contacts. Returns 0, or -1. */
+int oracle_tape_begin(OracleWorld *w);
+void oracle_tape_end(OracleWorld *w);
+int oracle_tape_steps(const OracleWorld *w);
+const OracleTapeStep *oracle_tape_step(const OracleWorld *w, int s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -29,10 +29,14 @@ class _Params(ctypes.Structure):
                 ("gamma", ctypes.c_float), ("broadphase", ctypes.c_int), ("orderMode", ctypes.c_int)]
 
 
+ORACLE_SOURCES = [os.path.join(HERE, f) for f in ("avbd_oracle.c", "avbd_oracle.h", "adjoint_ref.cpp")] + [
+    os.path.join(HERE, "..", "avbd_demo3d_b200", "csrc", "avbd_diff.h")]
+
+
 def build_oracle() -> str:
-    """Compile liboracle.so if missing or stale (gcc only; works on any box)."""
-    src = os.path.join(HERE, "avbd_oracle.c")
-    if not os.path.exists(ORACLE_LIB) or os.path.getmtime(ORACLE_LIB) < os.path.getmtime(src):
+    """Compile liboracle.so if missing or stale (gcc/g++ only; works on any box)."""
+    newest = max(os.path.getmtime(f) for f in ORACLE_SOURCES if os.path.exists(f))
+    if not os.path.exists(ORACLE_LIB) or os.path.getmtime(ORACLE_LIB) < newest:
         subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
     return ORACLE_LIB
 
@@ -90,6 +94,27 @@ def _lib(kind: str) -> ctypes.CDLL:
         lib.oracle_set_bodies.restype = None
         lib.oracle_colour_priority.argtypes = [ctypes.c_uint32]
         lib.oracle_colour_priority.restype = ctypes.c_uint32
+        lib.oracle_tape_begin.argtypes = [vp]
+        lib.oracle_tape_begin.restype = ip
+        lib.oracle_tape_end.argtypes = [vp]
+        lib.oracle_tape_end.restype = None
+        lib.oracle_tape_steps.argtypes = [vp]
+        lib.oracle_tape_steps.restype = ip
+        for name in ("adjref_num_params", "adjref_num_pairs"):
+            getattr(lib, name).argtypes = [vp]
+            getattr(lib, name).restype = ip
+        lib.adjref_pairs.argtypes = [vp, fp, fp]
+        lib.adjref_pairs.restype = None
+        lib.adjref_theta0.argtypes = [vp, fp]
+        lib.adjref_theta0.restype = None
+        lib.adjref_loss.argtypes = [vp, fp, fp, fp]
+        lib.adjref_loss.restype = ctypes.c_double
+        lib.adjref_gradient.argtypes = [vp, fp, fp, fp]
+        lib.adjref_gradient.restype = ctypes.c_double
+        lib.adjref_fd.argtypes = [vp, fp, fp, ip, fp, ctypes.c_double, ip, fp]
+        lib.adjref_fd.restype = None
+        lib.adjref_selftest.argtypes = []
+        lib.adjref_selftest.restype = ctypes.c_double
     else:
         lib.ref_iterate_ordered.argtypes = [vp, fp, ip]
         lib.ref_iterate_ordered.restype = ip
@@ -207,6 +232,57 @@ class World:
                "inert_lin": np.zeros((n, 3), np.float32), "inert_ang": np.zeros((n, 4), np.float32)}
         self.lib.oracle_get_body_aux(self.h, *[_ptr(out[k]) for k in ("init_lin", "init_ang", "inert_lin", "inert_ang")])
         return out
+
+
+    # frozen-branch tape, FP64 replay and reference adjoint (oracle only)
+    def tape_begin(self):
+        if self.lib.oracle_tape_begin(self.h) != 0:
+            raise ValueError("the differentiable step covers contact-only worlds")
+
+    def tape_steps(self) -> int:
+        return int(self.lib.oracle_tape_steps(self.h))
+
+    def adj_pairs(self):
+        """Friction pairs (lo, hi) in parameter order and their nominal coefficients."""
+        P = self.lib.adjref_num_pairs(self.h)
+        lohi = np.zeros((max(P, 0), 2), np.int32)
+        mu = np.zeros(max(P, 0), np.float32)
+        self.lib.adjref_pairs(self.h, _ptr(lohi), _ptr(mu))
+        return lohi, mu
+
+    def adj_theta0(self) -> np.ndarray:
+        th = np.zeros(self.lib.adjref_num_params(self.h), np.float64)
+        self.lib.adjref_theta0(self.h, _ptr(th))
+        return th
+
+    def adj_loss(self, theta, target):
+        theta = np.ascontiguousarray(theta, np.float64)
+        target = np.ascontiguousarray(target, np.float64)
+        pos = np.zeros((self.n, 3), np.float64)
+        loss = self.lib.adjref_loss(self.h, _ptr(theta), _ptr(target), _ptr(pos))
+        return float(loss), pos
+
+    def adj_gradient(self, theta, target):
+        theta = np.ascontiguousarray(theta, np.float64)
+        target = np.ascontiguousarray(target, np.float64)
+        g = np.zeros_like(theta)
+        loss = self.lib.adjref_gradient(self.h, _ptr(theta), _ptr(target), _ptr(g))
+        return float(loss), g
+
+    def adj_fd(self, theta, target, dirs, h=1e-4, threads=None):
+        theta = np.ascontiguousarray(theta, np.float64)
+        target = np.ascontiguousarray(target, np.float64)
+        dirs = np.ascontiguousarray(dirs, np.float64)
+        out = np.zeros(2 * dirs.shape[0], np.float64)
+        threads = threads or max(1, min(os.cpu_count() or 1, 2 * dirs.shape[0]))
+        self.lib.adjref_fd(self.h, _ptr(theta), _ptr(target), int(dirs.shape[0]), _ptr(dirs), float(h),
+                           int(threads), _ptr(out))
+        return out[:dirs.shape[0]].copy()
+
+
+def adjoint_selftest() -> float:
+    """Largest relative error of the step's VJP primitives against central differences."""
+    return float(_lib("oracle").adjref_selftest())
 
 
 def collide_boxes(kind: str, pA, qA, sA, pB, qB, sB):

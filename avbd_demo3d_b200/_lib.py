@@ -78,6 +78,12 @@ class AvbdProfile(ctypes.Structure):
                 ("phase_spans", ctypes.c_int64 * len(PHASES)), ("launches", ctypes.c_int64)]
 
 
+class AvbdAdjointGrad(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in (
+        "position", "orientation", "velocity", "angular_velocity", "prev_velocity", "mass", "pair_friction",
+        "body_friction")]
+
+
 # name -> (restype, argtypes); every symbol declared in include/avbd_cuda.h
 SIGNATURES = {
     "avbd_create": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int32, ctypes.c_void_p]),
@@ -115,6 +121,14 @@ SIGNATURES = {
     "avbd_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, c_int_p, c_float_p]),
     "avbd_read_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AvbdProfile)]),
     "avbd_reset_profile": (ctypes.c_int, [ctypes.c_void_p]),
+    "avbd_adjoint_forward": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]),
+    "avbd_adjoint_num_pairs": (ctypes.c_int, [ctypes.c_void_p, c_int_p]),
+    "avbd_adjoint_read_pairs": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_float_p]),
+    "avbd_adjoint_backward": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 4
+                              + [ctypes.POINTER(AvbdAdjointGrad)]),
+    "avbd_adjoint_replay_state": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 4),
+    "avbd_adjoint_tape_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, c_int_p, ctypes.c_void_p,
+                                              ctypes.c_void_p, c_int_p]),
 }
 
 _lib = None

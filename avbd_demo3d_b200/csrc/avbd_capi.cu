@@ -63,6 +63,8 @@ constexpr int kNumPrimalVariants = (int)(sizeof(kPrimalVariants) / sizeof(kPrima
 
 } // namespace
 
+struct AdjointState; // avbd_adjoint.cuh
+
 struct AvbdContext
 {
     int device = 0;
@@ -155,6 +157,10 @@ struct AvbdContext
     long long phaseLaunches[AVBD_PHASE_COUNT] = {0};
     long long launches = 0;
     long long stepsProfiled = 0;
+
+    // adjoint: checkpoints, tape and adjoint buffers; `recording` while a step is taped
+    AdjointState *adjoint = nullptr;
+    bool recording = false;
 };
 
 namespace
@@ -798,6 +804,13 @@ int colour_bodies(AvbdContext *ctx)
     return AVBD_OK;
 }
 
+// recording hooks of the adjoint (avbd_adjoint.cuh)
+int rec_step_begin(AvbdContext *ctx);
+int rec_prepared(AvbdContext *ctx);
+int rec_iteration(AvbdContext *ctx, int it);
+void adjoint_release(AvbdContext *ctx);
+void adjoint_invalidate(AvbdContext *ctx); // the world changed: no backward for the last forward
+
 int iterate(AvbdContext *ctx)
 {
     DevBodies B = dev_bodies(ctx);
@@ -807,6 +820,8 @@ int iterate(AvbdContext *ctx)
     const int GPB = PRIMAL_BLOCK / pv.group;
     for (int it = 0; it < ctx->params.iterations; ++it)
     {
+        if (ctx->recording)
+            CHECK(rec_iteration(ctx, it));
         for (int c = 0; c < ctx->nColours; ++c)
         {
             int first = ctx->hColourStart[c];
@@ -830,11 +845,15 @@ int iterate(AvbdContext *ctx)
             LAUNCHED();
         }
     }
+    if (ctx->recording)
+        CHECK(rec_iteration(ctx, ctx->params.iterations));
     return AVBD_OK;
 }
 
 int step_once(AvbdContext *ctx)
 {
+    if (ctx->recording)
+        CHECK(rec_step_begin(ctx));
     CU(cudaMemsetAsync(ctx->counters.p, 0, sizeof(StepCounters), ctx->stream));
     ctx->stats.grid_rescaled = 0;
     {
@@ -861,6 +880,8 @@ int step_once(AvbdContext *ctx)
         PhaseScope ps(ctx, AVBD_PHASE_COLOURING);
         CHECK(colour_bodies(ctx));
     }
+    if (ctx->recording)
+        CHECK(rec_prepared(ctx));
     CHECK(iterate(ctx));
     if (ctx->n)
     {
@@ -1148,6 +1169,7 @@ void avbd_destroy(AvbdContext *ctx)
     cudaSetDevice(ctx->device);
     if (ctx->stream)
         cudaStreamSynchronize(ctx->stream);
+    adjoint_release(ctx);
     for (DArr<float4> *a : {&ctx->pos, &ctx->quat, &ctx->initLin, &ctx->initAng, &ctx->inertLin, &ctx->inertAng,
                             &ctx->vel, &ctx->angvel, &ctx->prevVel, &ctx->massMoment, &ctx->sizeRad, &ctx->largeLo,
                             &ctx->largeHi, &ctx->largeSphere, &ctx->spring, &ctx->joint[0], &ctx->joint[1]})
@@ -1277,6 +1299,7 @@ int avbd_load_batch(AvbdContext *ctx, int32_t num_worlds, const int32_t *world_s
         return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
     if (ctx->errCode)
         return AVBD_ERR_LATCHED;
+    adjoint_invalidate(ctx);
     int n = bodies->count;
     if (n < 0 || n >= (int)KEY_NO_BODY)
         return fail(ctx, AVBD_ERR_ARGUMENT, "body count %d out of range", n);
@@ -1437,6 +1460,7 @@ int avbd_write_bodies(AvbdContext *ctx, const AvbdBodies *bodies)
     if (!ctx->loaded || bodies->count != ctx->n)
         return fail(ctx, AVBD_ERR_STATE, "body count does not match the loaded world");
     CU(cudaSetDevice(ctx->device));
+    adjoint_invalidate(ctx);
     CHECK(upload_bodies(ctx, bodies, false));
     return AVBD_OK;
 }
@@ -1449,6 +1473,7 @@ int avbd_step(AvbdContext *ctx, int32_t nsteps)
         return AVBD_ERR_LATCHED;
     if (!ctx->loaded)
         return fail(ctx, AVBD_ERR_STATE, "no world loaded");
+    adjoint_invalidate(ctx);
     CU(cudaSetDevice(ctx->device));
     for (int s = 0; s < nsteps; ++s)
         CHECK(step_once(ctx));
@@ -1829,3 +1854,5 @@ int avbd_reset_profile(AvbdContext *ctx)
 }
 
 } // extern "C"
+
+#include "avbd_adjoint.cuh"

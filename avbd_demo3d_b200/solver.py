@@ -299,6 +299,62 @@ class World:
         """0 = greedy colouring in list order (default), 1 = hashed priorities."""
         self._check(self.lib.avbd_set_colouring(self.h, mode), "avbd_set_colouring")
 
+    # -- differentiable step
+    def adjoint_forward(self, steps: int, checkpoint_every: int = 10, sync: bool = True):
+        """Step like step(steps), keeping a state snapshot every checkpoint_every steps for
+        adjoint_backward."""
+        self._check(self.lib.avbd_adjoint_forward(self.h, steps, checkpoint_every), "avbd_adjoint_forward")
+        if sync:
+            self.synchronize()
+
+    def adjoint_pairs(self):
+        """Friction pairs (lo, hi) of the last adjoint_forward and their nominal coefficients."""
+        k = ctypes.c_int32()
+        self._check(self.lib.avbd_adjoint_num_pairs(self.h, ctypes.byref(k)), "avbd_adjoint_num_pairs")
+        lohi = np.zeros((k.value, 2), np.int32)
+        mu = np.zeros(k.value, F32)
+        self._check(self.lib.avbd_adjoint_read_pairs(self.h, lohi.ctypes.data_as(_lib.c_int_p),
+                                                     mu.ctypes.data_as(_lib.c_float_p)), "avbd_adjoint_read_pairs")
+        return lohi, mu
+
+    def adjoint_replay_state(self) -> dict:
+        """Double-precision final state of the frozen-branch replay of the last forward."""
+        n = self.n
+        out = {"pos": np.zeros((n, 3)), "quat": np.zeros((n, 4)), "vel": np.zeros((n, 3)), "angvel": np.zeros((n, 3))}
+        self._check(self.lib.avbd_adjoint_replay_state(self.h, *[_ptr(out[k]) for k in ("pos", "quat", "vel",
+                                                                                         "angvel")]),
+                    "avbd_adjoint_replay_state")
+        return out
+
+    def adjoint_tape(self, step: int) -> dict:
+        """Parity dump of the forward's tape for one step (avbd_adjoint_tape_step)."""
+        m = ctypes.c_int32()
+        self._check(self.lib.avbd_adjoint_tape_step(self.h, step, ctypes.byref(m), None, None, None),
+                    "avbd_adjoint_tape_step")
+        it = self.params.iterations
+        flags = np.zeros((it, m.value, 8), np.uint16)
+        bflags = np.zeros(self.n, np.uint8)
+        link = np.zeros((m.value, 8), np.int32)
+        self._check(self.lib.avbd_adjoint_tape_step(self.h, step, ctypes.byref(m), _ptr(flags), _ptr(bflags),
+                                                    link.ctypes.data_as(_lib.c_int_p)), "avbd_adjoint_tape_step")
+        return {"nMan": m.value, "flags": flags, "body_flags": bflags, "src": link}
+
+    def adjoint_backward(self, d_pos=None, d_quat=None, d_vel=None, d_angvel=None) -> dict:
+        """Gradient with respect to the state before adjoint_forward and to the parameters,
+        given the gradient of a loss with respect to the final state (list order)."""
+        n = self.n
+        k = ctypes.c_int32()
+        self._check(self.lib.avbd_adjoint_num_pairs(self.h, ctypes.byref(k)), "avbd_adjoint_num_pairs")
+        out = {"pos": np.zeros((n, 3)), "quat": np.zeros((n, 4)), "vel": np.zeros((n, 3)),
+               "angvel": np.zeros((n, 3)), "prevvel": np.zeros((n, 3)), "mass": np.zeros(n),
+               "pair_friction": np.zeros(k.value), "friction": np.zeros(n)}
+        g = _lib.AvbdAdjointGrad(*[_ptr(out[key]) for key in (
+            "pos", "quat", "vel", "angvel", "prevvel", "mass", "pair_friction", "friction")])
+        ins = [None if a is None else _c(a, np.float64) for a in (d_pos, d_quat, d_vel, d_angvel)]
+        self._check(self.lib.avbd_adjoint_backward(self.h, *[_ptr(a) for a in ins], ctypes.byref(g)),
+                    "avbd_adjoint_backward")
+        return out
+
     def set_profiling(self, on: bool = True):
         self._check(self.lib.avbd_set_profiling(self.h, 1 if on else 0), "avbd_set_profiling")
 

@@ -314,6 +314,71 @@ int avbd_autotune(AvbdContext *ctx, int32_t repeats, int32_t *best_variant, floa
 int avbd_read_profile(AvbdContext *ctx, AvbdProfile *out);
 int avbd_reset_profile(AvbdContext *ctx);
 
+/* Differentiable step: a forward / backward pair over several steps. The reference has no
+ * differentiation; the map that is differentiated is its step (solver.cpp:1036-1298) with
+ * the integer decisions of the run held fixed (contact set and contact geometry, colouring,
+ * force clamps, friction-cone and penalty-ramp branches, warm-start clamps), which leaves
+ * a smooth function of the initial body state, the masses and the friction coefficients.
+ * The FP32 forward is the ordinary step; derivatives are evaluated and accumulated in
+ * double precision.
+ *
+ * avbd_adjoint_forward runs nsteps steps exactly like avbd_step(ctx, nsteps) and keeps a
+ * snapshot of the dynamic state every checkpoint_every steps. Worlds with joints or springs
+ * are rejected (AVBD_ERR_ARGUMENT): the differentiable step covers contacts.
+ *
+ * Along the way it tapes every step's decisions and replays the frozen-branch map in double
+ * precision, keeping a snapshot of that replay every checkpoint_every steps; the FP32 world
+ * ends exactly where avbd_step(ctx, nsteps) would leave it.
+ *
+ * avbd_adjoint_backward takes the gradient of a loss with respect to the final state
+ * (host arrays in list order: position n x 3, orientation n x 4 (x, y, z, w), velocity
+ * n x 3, angular velocity n x 3; NULL = zero) and writes into the non-NULL host arrays of
+ * AvbdAdjointGrad the gradient with respect to the state before the forward steps and the
+ * parameters. Per checkpoint segment it replays the segment again, keeping the state at
+ * every iteration, and sweeps it in reverse. It leaves the FP32 world untouched. The
+ * forward must be the last thing that changed the world (a step, a body write or a load
+ * in between is refused), and parameters and colouring mode must be the same.
+ *
+ * Friction parameters are per body pair: mu of every manifold between bodies a and b
+ * (manifold.cpp:103, sqrt(mu_a mu_b) in the forward). Pairs are the (min, max) body pairs of
+ * every manifold the forward met, in ascending order; avbd_adjoint_read_pairs lists them
+ * and their nominal coefficients. body_friction chains the pair gradients through
+ * mu = sqrt(mu_a mu_b) onto Rigid::friction. */
+typedef struct AvbdAdjointGrad
+{
+    double *position;         /* n x 3 */
+    double *orientation;      /* n x 4 */
+    double *velocity;         /* n x 3 */
+    double *angular_velocity; /* n x 3 */
+    double *prev_velocity;    /* n x 3: Rigid::prevVelocityLin (the adaptive warm start reads it) */
+    double *mass;             /* n: the moment scales with the mass (rigid.cpp:34-39) */
+    double *pair_friction;    /* num_pairs */
+    double *body_friction;    /* n */
+} AvbdAdjointGrad;
+
+int avbd_adjoint_forward(AvbdContext *ctx, int32_t nsteps, int32_t checkpoint_every);
+int avbd_adjoint_num_pairs(AvbdContext *ctx, int32_t *count);
+int avbd_adjoint_read_pairs(AvbdContext *ctx, int32_t *lohi2, float *friction);
+int avbd_adjoint_backward(AvbdContext *ctx, const double *d_position3, const double *d_orientation4,
+                          const double *d_velocity3, const double *d_angular_velocity3, const AvbdAdjointGrad *out);
+
+/* Final state of the double-precision frozen-branch replay of the last forward (list
+ * order; NULL outputs skipped): the state whose derivatives avbd_adjoint_backward takes.
+ * It differs from the FP32 world only by rounding; evaluate a loss's gradient here for the
+ * exact gradient of the differentiated map. */
+int avbd_adjoint_replay_state(AvbdContext *ctx, double *position3, double *orientation4, double *velocity3,
+                              double *angular_velocity3);
+
+/* Parity dump of the forward's tape for one step: the manifold count, the branch outcomes
+ * of every contact slot per iteration (iterations x num_manifolds x 8; bits 0-11 the dual
+ * update, 12-13 the primal evaluation for body A, 14-15 for body B: 1 = normal force
+ * clamped, 2 = friction cone; dual bits 4 tangential ramp, 8/16/32 penalty cap, 64/128/256
+ * C < 0, 512/1024/2048 C > 0), the warm-start outcome per body (1 dynamic, 2 has forces,
+ * 4 adaptive weight inside (0, 1), 8 weight clamped at 1) and the link of every contact to
+ * the previous step's slot (manifold * 8 + contact, -1 = new). NULL outputs are skipped. */
+int avbd_adjoint_tape_step(AvbdContext *ctx, int32_t step, int32_t *num_manifolds, uint16_t *flags,
+                           uint8_t *body_flags, int32_t *link);
+
 #ifdef __cplusplus
 }
 #endif

@@ -139,8 +139,10 @@ bool build_problem(const OracleWorld *w, Problem &pb)
             cnt[b + 1] += cnt[b];
         pb.bodyStart[s] = cnt;
         pb.bodyMan[s].assign(cnt[n], 0);
+        // each body's rows newest manifold first, the order of the reference's per-body force
+        // lists (force.cpp:25-36); manifolds are in creation order
         std::vector<int> fill(cnt.begin(), cnt.end() - 1);
-        for (int m = 0; m < t->nMan; ++m)
+        for (int m = t->nMan - 1; m >= 0; --m)
         {
             pb.bodyMan[s][fill[t->ab[2 * m]]++] = 2 * m + 1;
             pb.bodyMan[s][fill[t->ab[2 * m + 1]]++] = 2 * m;

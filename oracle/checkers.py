@@ -33,6 +33,18 @@ ORACLE_SOURCES = [os.path.join(HERE, f) for f in ("avbd_oracle.c", "avbd_oracle.
     os.path.join(HERE, "..", "avbd_demo3d_b200", "csrc", "avbd_diff.h")]
 
 
+class _TapeStep(ctypes.Structure):
+    _fields_ = [("nMan", ctypes.c_int), ("nSolve", ctypes.c_int), ("nColours", ctypes.c_int),
+                ("iterations", ctypes.c_int), ("bodyIn", ctypes.POINTER(ctypes.c_float)),
+                ("bodyFlags", ctypes.POINTER(ctypes.c_uint8)), ("ab", ctypes.POINTER(ctypes.c_int)),
+                ("basis", ctypes.POINTER(ctypes.c_float)), ("friction", ctypes.POINTER(ctypes.c_float)),
+                ("ncontacts", ctypes.POINTER(ctypes.c_int)), ("keys", ctypes.POINTER(ctypes.c_int)),
+                ("geo", ctypes.POINTER(ctypes.c_float)), ("init", ctypes.POINTER(ctypes.c_float)),
+                ("src", ctypes.POINTER(ctypes.c_int)), ("initFlags", ctypes.POINTER(ctypes.c_uint8)),
+                ("solveOrder", ctypes.POINTER(ctypes.c_int)), ("colourStart", ctypes.POINTER(ctypes.c_int)),
+                ("flags", ctypes.POINTER(ctypes.c_uint16))]
+
+
 def build_oracle() -> str:
     """Compile liboracle.so if missing or stale (gcc/g++ only; works on any box)."""
     newest = max(os.path.getmtime(f) for f in ORACLE_SOURCES if os.path.exists(f))
@@ -100,6 +112,8 @@ def _lib(kind: str) -> ctypes.CDLL:
         lib.oracle_tape_end.restype = None
         lib.oracle_tape_steps.argtypes = [vp]
         lib.oracle_tape_steps.restype = ip
+        lib.oracle_tape_step.argtypes = [vp, ip]
+        lib.oracle_tape_step.restype = ctypes.POINTER(_TapeStep)
         for name in ("adjref_num_params", "adjref_num_pairs"):
             getattr(lib, name).argtypes = [vp]
             getattr(lib, name).restype = ip
@@ -241,6 +255,16 @@ class World:
 
     def tape_steps(self) -> int:
         return int(self.lib.oracle_tape_steps(self.h))
+
+    def tape_step(self, s: int) -> dict:
+        """One recorded step: flags (iterations x nMan x 8 x 3: primal as A, as B, dual),
+        body flags, links to the previous step's slots, initialisation clamp flags."""
+        t = self.lib.oracle_tape_step(self.h, s).contents
+        M, n, it = t.nMan, self.n, t.iterations
+        arr = lambda ptr, count: np.ctypeslib.as_array(ptr, shape=(count,)).copy() if count else np.zeros(0)
+        return {"nMan": M, "flags": arr(t.flags, it * M * 8 * 3).reshape(it, M, 8, 3),
+                "body_flags": arr(t.bodyFlags, n), "src": arr(t.src, M * 8).reshape(M, 8),
+                "init_flags": arr(t.initFlags, M * 8).reshape(M, 8), "ncontacts": arr(t.ncontacts, M)}
 
     def adj_pairs(self):
         """Friction pairs (lo, hi) in parameter order and their nominal coefficients."""

@@ -81,7 +81,36 @@ struct Snap64
     const double4 *pose;   // per iteration boundary t: 2n (p, q)
     const double4 *lp;     // per iteration boundary t: 16 nMan (lambda of every slot, then penalty)
     const double4 *c0;     // 8 nMan
+    const double *ldl;     // per iteration t and body: LDL_STRIDE doubles (D, strict lower L, dx)
 };
+
+// A body's 6x6 factorisation and step as the replay computed them: D (6), the strict
+// lower triangle of L row by row (15) and dx (6).
+constexpr int LDL_STRIDE = 28;
+
+AVBD_DEV void store_ldl(double *o, const ad::Ldl6<D> &f, const D dx[6])
+{
+    int k = 0;
+    for (int i = 0; i < 6; ++i)
+        o[k++] = f.D[i];
+    for (int i = 1; i < 6; ++i)
+        for (int j = 0; j < i; ++j)
+            o[k++] = f.L[i][j];
+    for (int i = 0; i < 6; ++i)
+        o[k++] = dx[i];
+}
+
+AVBD_DEV void load_ldl(const double *o, ad::Ldl6<D> &f, D dx[6])
+{
+    int k = 0;
+    for (int i = 0; i < 6; ++i)
+        f.D[i] = o[k++];
+    for (int i = 1; i < 6; ++i)
+        for (int j = 0; j < i; ++j)
+            f.L[i][j] = o[k++];
+    for (int i = 0; i < 6; ++i)
+        dx[i] = o[k++];
+}
 
 struct AdjView
 {
@@ -221,6 +250,24 @@ __global__ void k_rec_lp(const float4 *contact, int nMan, float4 *out)
     const float4 *c = contact + (size_t)m * 32 + 4 * ci;
     out[2 * s] = c[2];
     out[2 * s + 1] = c[3];
+}
+
+// FP32 state at an iteration boundary: body poses and contact words 2, 3 of every slot
+__global__ void k_rec_iteration(const float4 *pos, const float4 *quat, int n, const float4 *contact, int nMan,
+                                float4 *pose, float4 *lp)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+    {
+        pose[i] = pos[i];
+        pose[n + i] = quat[i];
+    }
+    if (i < 8 * nMan)
+    {
+        const float4 *c = contact + (size_t)(i >> 3) * 32 + 4 * (i & 7);
+        lp[2 * i] = c[2];
+        lp[2 * i + 1] = c[3];
+    }
 }
 
 // body-local anchors of every slot
@@ -464,43 +511,90 @@ AVBD_DEV ad::Pose<D> pose_state(const State64 &S, int b)
     return r;
 }
 
-// body primal for the bodies of one colour (solver.cpp:1177-1242)
-__global__ void __launch_bounds__(128) k_rep_primal(StepTape T, DevBodies B, State64 S, AdjParams Q, int t, int first,
-                                                    int count)
+// Per-body work is spread over a group of G lanes: the body's contact rows (its manifold
+// entries in force order, each contact a row) go round-robin to the lanes, each lane stamps
+// its rows into a private 6x6 system, and a butterfly over the group sums them. Every lane
+// then holds the same system and factors it, so no lane waits for a broadcast.
+constexpr int ADJ_G = 8;
+constexpr int ADJ_BLOCK = 64;
+
+template <int G> AVBD_DEV unsigned group_mask()
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= count)
+    return G == 32 ? 0xFFFFFFFFu : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
+}
+
+template <int G> AVBD_DEV D group_sum(D v, unsigned mask)
+{
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1)
+        v += __shfl_xor_sync(mask, v, o, G);
+    return v;
+}
+
+template <int G> AVBD_DEV void group_sum_sys(ad::Sys6<D> &s, unsigned mask)
+{
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+    {
+        s.g[i] = group_sum<G>(s.g[i], mask);
+#pragma unroll
+        for (int j = 0; j < 6; ++j)
+            s.H[i][j] = group_sum<G>(s.H[i][j], mask);
+    }
+}
+
+// body primal for the bodies of one colour (solver.cpp:1177-1242)
+__global__ void __launch_bounds__(ADJ_BLOCK) k_rep_primal(StepTape T, DevBodies B, State64 S, AdjParams Q, int t,
+                                                          int first, int count, double *ldlOut)
+{
+    constexpr int G = ADJ_G;
+    const int lane = threadIdx.x % G;
+    const int gid = blockIdx.x * (ADJ_BLOCK / G) + threadIdx.x / G;
+    if (gid >= count)
         return;
-    const int b = T.solveList[first + i];
+    const unsigned mask = group_mask<G>();
+    const int b = T.solveList[first + gid];
     float4 mm = B.massMoment[b];
     ad::Pose<D> own = pose_state(S, b);
+    const unsigned short *fl = T.flags + (size_t)t * 8 * T.nMan;
     ad::Sys6<D> sys;
     ad::sys_zero(sys);
-    ad::stamp_inertia(sys, (D)mm.x, shape_of(mm), own.p, ld3(S.tLin + b), own.q, ld4(S.tAng + b), Q.dt);
-    const unsigned short *fl = T.flags + (size_t)t * 8 * T.nMan;
+    int row = 0;
     for (int k = T.adjStart[b]; k < T.adjStart[b + 1]; ++k)
     {
         unsigned e = T.adj[k];
         if (adj_type(e) != ADJ_MANIFOLD)
             continue;
         int m = (int)adj_index(e);
+        int nc = T.nc[m];
+        int mine = row % G <= lane ? lane - row % G : lane - row % G + G; // first owned contact
+        row += nc;
+        if (mine >= nc)
+            continue;
         bool isA = adj_isA(e) != 0;
         int2 ab = T.ab[m];
         ad::Pose<D> A = isA ? own : pose_state(S, ab.x);
         ad::Pose<D> Bp = isA ? pose_state(S, ab.y) : own;
-        for (int ci = 0; ci < T.nc[m]; ++ci)
+        for (int ci = mine; ci < nc; ci += G)
         {
             int s = m * 8 + ci;
             ad::ContactIn<D> c = contact64(T, m, ci, ld3(S.c0 + s), ld3(S.lam + s), ld3(S.pen + s));
             ad::stamp_contact(sys, c, ad::contact_forward(A, Bp, c, Q.alpha, primal_bits(fl[s], isA)), isA);
         }
     }
+    group_sum_sys<G>(sys, mask);
+    ad::stamp_inertia(sys, (D)mm.x, shape_of(mm), own.p, ld3(S.tLin + b), own.q, ld4(S.tAng + b), Q.dt);
     ad::Ldl6<D> f;
     ad::ldl_factor(sys.H, f);
     D dx[6];
     ad::body_dx(f, sys, dx);
-    st3(S.p + b, own.p + ad::v3<D>(dx[0], dx[1], dx[2]));
-    st4(S.q + b, ad::qstep(own.q, ad::v3<D>(dx[3], dx[4], dx[5])));
+    if (lane == 0)
+    {
+        st3(S.p + b, own.p + ad::v3<D>(dx[0], dx[1], dx[2]));
+        st4(S.q + b, ad::qstep(own.q, ad::v3<D>(dx[3], dx[4], dx[5])));
+        if (ldlOut)
+            store_ldl(ldlOut + ((size_t)t * T.n + b) * LDL_STRIDE, f, dx);
+    }
 }
 
 // Manifold::updateDual (manifold.cpp:231-279)
@@ -534,6 +628,36 @@ __global__ void k_rep_finish(StepTape T, DevBodies B, State64 S, AdjParams Q)
     D idt = D(1) / Q.dt;
     st3(S.v + b, (ld3(S.p + b) - ld3(S.iLin + b)) * idt);
     st3(S.w + b, ad::qdiff(ld4(S.q + b), ld4(S.iAng + b)) * idt);
+}
+
+// replay state at an iteration boundary: poses of every body, lambda and penalty of every slot
+__global__ void k_snapshot(State64 S, int n, int nMan, double4 *pose, double4 *lp)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+    {
+        pose[i] = S.p[i];
+        pose[n + i] = S.q[i];
+    }
+    int slots = 8 * nMan;
+    if (i < slots)
+    {
+        lp[i] = S.lam[i];
+        lp[slots + i] = S.pen[i];
+    }
+}
+
+// body state at step start
+__global__ void k_snapshot_bodies(State64 S, int n, double4 *out)
+{
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n)
+        return;
+    out[b] = S.p[b];
+    out[n + b] = S.q[b];
+    out[2 * n + b] = S.v[b];
+    out[3 * n + b] = S.w[b];
+    out[4 * n + b] = S.vp[b];
 }
 
 // ---------------------------------------------------------------------------
@@ -624,112 +748,114 @@ __global__ void k_adj_dual(StepTape T, Snap64 X, DevBodies B, AdjView A, AdjPara
         atomicAdd(A.mu + T.pairIdx[m], mub);
 }
 
-// body primal of iteration t for the bodies of colour c
-__global__ void __launch_bounds__(128) k_adj_primal(StepTape T, Snap64 X, DevBodies B, AdjView A, AdjParams Q, int t,
-                                                    int c, int first, int count)
+// body primal of iteration t for the bodies of colour c, lanes as in k_rep_primal
+__global__ void __launch_bounds__(ADJ_BLOCK) k_adj_primal(StepTape T, Snap64 X, DevBodies B, AdjView A, AdjParams Q,
+                                                          int t, int c, int first, int count)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= count)
+    constexpr int G = ADJ_G;
+    const int lane = threadIdx.x % G;
+    const int gid = blockIdx.x * (ADJ_BLOCK / G) + threadIdx.x / G;
+    if (gid >= count)
         return;
+    const unsigned mask = group_mask<G>();
     const int n = T.n;
-    const int b = T.solveList[first + i];
+    const int b = T.solveList[first + gid];
     auto partner = [&](int x) {
         int cx = T.colour[x];
         return pose_snap(X, n, (cx >= 0 && cx < c) ? t + 1 : t, x);
     };
     const unsigned short *fl = T.flags + (size_t)t * 8 * T.nMan;
     ad::Pose<D> own = pose_snap(X, n, t, b);
+    const int start = T.adjStart[b], end = T.adjStart[b + 1];
     float4 mm = B.massMoment[b];
     D mass = mm.x;
     ad::V3<D> shape = shape_of(mm);
-    // the inertial pose as the replay formed it
     ad::WarmOut<D> wo = ad::warm_start(ld3(X.bodyIn + b), ld4(X.bodyIn + n + b), ld3(X.bodyIn + 2 * n + b),
                                        ld3(X.bodyIn + 3 * n + b), ld3(X.bodyIn + 4 * n + b), Q.dt, Q.g, T.bflags[b]);
-    ad::Sys6<D> sys;
-    ad::sys_zero(sys);
-    ad::stamp_inertia(sys, mass, shape, own.p, wo.inertLin, own.q, wo.inertAng, Q.dt);
-    const int start = T.adjStart[b], end = T.adjStart[b + 1];
-    for (int k = start; k < end; ++k)
-    {
-        unsigned e = T.adj[k];
-        if (adj_type(e) != ADJ_MANIFOLD)
-            continue;
-        int m = (int)adj_index(e);
-        bool isA = adj_isA(e) != 0;
-        int2 ab = T.ab[m];
-        ad::Pose<D> PA = isA ? own : partner(ab.x);
-        ad::Pose<D> PB = isA ? partner(ab.y) : own;
-        for (int ci = 0; ci < T.nc[m]; ++ci)
-        {
-            ad::ContactIn<D> cc = contact_snap(T, X, t, m, ci);
-            ad::stamp_contact(sys, cc, ad::contact_forward(PA, PB, cc, Q.alpha, primal_bits(fl[m * 8 + ci], isA)),
-                              isA);
-        }
-    }
+    // the factorisation and step the replay stored for this body and iteration
     ad::Ldl6<D> f;
-    ad::ldl_factor(sys.H, f);
     D dx[6];
-    ad::body_dx(f, sys, dx);
-    ad::V3<D> pbar = ld3(A.p + b);
-    D dxbar[6] = {pbar.x, pbar.y, pbar.z, 0, 0, 0};
-    ad::Q4<D> qbar = ad::qzero<D>();
+    load_ldl(X.ldl + ((size_t)t * n + b) * LDL_STRIDE, f, dx);
+    // pose update p += dx_lin, q = q (+) dx_ang
+    ad::V3<D> pnew = ld3(A.p + b);
+    D dxbar[6] = {pnew.x, pnew.y, pnew.z, 0, 0, 0};
+    ad::Q4<D> qbarPre = ad::qzero<D>();
     ad::V3<D> wdx = ad::vzero<D>();
-    ad::qstep_vjp(own.q, ad::v3<D>(dx[3], dx[4], dx[5]), ld4(A.q + b), qbar, wdx);
+    ad::qstep_vjp(own.q, ad::v3<D>(dx[3], dx[4], dx[5]), ld4(A.q + b), qbarPre, wdx);
     dxbar[3] = wdx.x;
     dxbar[4] = wdx.y;
     dxbar[5] = wdx.z;
-    ad::Sys6<D> bar;
-    ad::body_dx_vjp(f, dx, dxbar, bar);
+    D u[6];
+    ad::body_dx_vjp_u(f, dxbar, u);
+    // each lane's rows
+    ad::PoseBar<D> mineBar = ad::posebar_zero<D>();
+    {
+        int row = 0;
+        for (int k = start; k < end; ++k)
+        {
+            unsigned e = T.adj[k];
+            if (adj_type(e) != ADJ_MANIFOLD)
+                continue;
+            int m = (int)adj_index(e);
+            int nc = T.nc[m];
+            int mine = row % G <= lane ? lane - row % G : lane - row % G + G;
+            row += nc;
+            if (mine >= nc)
+                continue;
+            bool isA = adj_isA(e) != 0;
+            int2 ab = T.ab[m];
+            ad::Pose<D> PA = isA ? own : partner(ab.x);
+            ad::Pose<D> PB = isA ? partner(ab.y) : own;
+            ad::PoseBar<D> Ob = ad::posebar_zero<D>();
+            D mub = 0;
+            for (int ci = mine; ci < nc; ci += G)
+            {
+                int s = m * 8 + ci;
+                ad::ContactIn<D> cc = contact_snap(T, X, t, m, ci);
+                ad::PoseBar<D> Ab = ad::posebar_zero<D>(), Bb = ad::posebar_zero<D>();
+                ad::V3<D> lb = ld3(A.lam + s), pnb = ld3(A.pen + s), c0b = ld3(A.c0 + s);
+                ad::contact_primal_vjp_outer(PA, PB, cc, Q.alpha, primal_bits(fl[s], isA), isA, u, dx, Ab, Bb, lb,
+                                             pnb, c0b, mub);
+                st3(A.lam + s, lb);
+                st3(A.pen + s, pnb);
+                st3(A.c0 + s, c0b);
+                const ad::PoseBar<D> &me = isA ? Ab : Bb;
+                const ad::PoseBar<D> &them = isA ? Bb : Ab;
+                mineBar.p += me.p;
+                mineBar.q += me.q;
+                mineBar.pi += me.pi;
+                mineBar.qi += me.qi;
+                Ob.p += them.p;
+                Ob.q += them.q;
+                Ob.pi += them.pi;
+                Ob.qi += them.qi;
+            }
+            scatter_pose(B, A, isA ? ab.y : ab.x, Ob);
+            if (mub != 0 && T.pairIdx[m] >= 0)
+                atomicAdd(A.mu + T.pairIdx[m], mub);
+        }
+    }
+    // the body's own share, summed over the group
+    D r[14] = {mineBar.p.x, mineBar.p.y, mineBar.p.z, mineBar.q.x, mineBar.q.y, mineBar.q.z, mineBar.q.w,
+               mineBar.pi.x, mineBar.pi.y, mineBar.pi.z, mineBar.qi.x, mineBar.qi.y, mineBar.qi.z, mineBar.qi.w};
+#pragma unroll
+    for (int k = 0; k < 14; ++k)
+        r[k] = group_sum<G>(r[k], mask);
+    if (lane != 0)
+        return;
+    ad::V3<D> pbar = pnew + ad::v3<D>(r[0], r[1], r[2]);
+    ad::Q4<D> qbar = qbarPre + ad::q4<D>(r[3], r[4], r[5], r[6]);
     D mb = 0;
     ad::V3<D> tLinBar = ad::vzero<D>();
     ad::Q4<D> tAngBar = ad::qzero<D>();
-    ad::stamp_inertia_vjp(bar, mass, shape, own.p, wo.inertLin, own.q, wo.inertAng, Q.dt, mb, pbar, tLinBar, qbar,
-                          tAngBar);
-    ad::V3<D> iLinBar = ad::vzero<D>();
-    ad::Q4<D> iAngBar = ad::qzero<D>();
-    for (int k = start; k < end; ++k)
-    {
-        unsigned e = T.adj[k];
-        if (adj_type(e) != ADJ_MANIFOLD)
-            continue;
-        int m = (int)adj_index(e);
-        bool isA = adj_isA(e) != 0;
-        int2 ab = T.ab[m];
-        ad::Pose<D> PA = isA ? own : partner(ab.x);
-        ad::Pose<D> PB = isA ? partner(ab.y) : own;
-        ad::PoseBar<D> Ob = ad::posebar_zero<D>();
-        D mub = 0;
-        for (int ci = 0; ci < T.nc[m]; ++ci)
-        {
-            int s = m * 8 + ci;
-            ad::ContactIn<D> cc = contact_snap(T, X, t, m, ci);
-            ad::PoseBar<D> Ab = ad::posebar_zero<D>(), Bb = ad::posebar_zero<D>();
-            ad::V3<D> lb = ld3(A.lam + s), pnb = ld3(A.pen + s), c0b = ld3(A.c0 + s);
-            ad::contact_primal_vjp(PA, PB, cc, Q.alpha, primal_bits(fl[s], isA), isA, bar, Ab, Bb, lb, pnb, c0b, mub);
-            st3(A.lam + s, lb);
-            st3(A.pen + s, pnb);
-            st3(A.c0 + s, c0b);
-            const ad::PoseBar<D> &mine = isA ? Ab : Bb;
-            const ad::PoseBar<D> &theirs = isA ? Bb : Ab;
-            pbar += mine.p;
-            qbar += mine.q;
-            iLinBar += mine.pi;
-            iAngBar += mine.qi;
-            Ob.p += theirs.p;
-            Ob.q += theirs.q;
-            Ob.pi += theirs.pi;
-            Ob.qi += theirs.qi;
-        }
-        scatter_pose(B, A, isA ? ab.y : ab.x, Ob);
-        if (mub != 0 && T.pairIdx[m] >= 0)
-            atomicAdd(A.mu + T.pairIdx[m], mub);
-    }
+    ad::stamp_inertia_vjp_outer(u, dx, mass, shape, own.p, wo.inertLin, own.q, wo.inertAng, Q.dt, mb, pbar, tLinBar,
+                                qbar, tAngBar);
     st3(A.p + b, pbar);
     st4(A.q + b, qbar);
     A.m[b] += mb;
-    st3(A.iLin + b, ld3(A.iLin + b) + iLinBar);
+    st3(A.iLin + b, ld3(A.iLin + b) + ad::v3<D>(r[7], r[8], r[9]));
     ad::Q4<D> ia = ld4(A.iAng + b);
-    ia += iAngBar;
+    ia += ad::q4<D>(r[10], r[11], r[12], r[13]);
     st4(A.iAng + b, ia);
     st3(A.tLin + b, ld3(A.tLin + b) + tLinBar);
     ad::Q4<D> ta = ld4(A.tAng + b);
@@ -838,6 +964,7 @@ struct Checkpoint64
 struct SegSnap
 {
     DArr<double4> bodyIn, pose, lp, c0;
+    DArr<double> ldl;
 };
 
 } // namespace
@@ -922,6 +1049,7 @@ void adjoint_release(AvbdContext *ctx)
         release(s.pose);
         release(s.lp);
         release(s.c0);
+        release(s.ldl);
     }
     release(a->keys);
     release(a->pairs);
@@ -1027,15 +1155,10 @@ int rec_iteration(AvbdContext *ctx, int it)
 {
     AdjointState *a = ctx->adjoint;
     int n = ctx->n, M = ctx->nMan;
-    float4 *pose = a->pose32.p + (size_t)it * 2 * n;
-    CHECK(copy_d2d(ctx, pose, ctx->pos.p, n));
-    CHECK(copy_d2d(ctx, pose + n, ctx->quat.p, n));
-    if (M)
-    {
-        k_rec_lp<<<grid_for(8ll * M, 256), 256, 0, ctx->stream>>>(ctx->man[ctx->cur].contact.p, M,
-                                                                   a->lp32.p + (size_t)it * 16 * M);
-        LAUNCHED();
-    }
+    k_rec_iteration<<<grid_for(std::max<long long>(n, 8ll * M), 256), 256, 0, ctx->stream>>>(
+        ctx->pos.p, ctx->quat.p, n, ctx->man[ctx->cur].contact.p, M, a->pose32.p + (size_t)it * 2 * n,
+        a->lp32.p + (size_t)it * 16 * M);
+    LAUNCHED();
     return AVBD_OK;
 }
 
@@ -1161,9 +1284,9 @@ int replay_step(AvbdContext *ctx, int s, SegSnap *snap)
         CHECK(reserve(ctx, snap->pose, T1 * 2 * (size_t)std::max(n, 1), false));
         CHECK(reserve(ctx, snap->lp, T1 * 16 * m1, false));
         CHECK(reserve(ctx, snap->c0, 8 * m1, false));
-        double4 *src[5] = {S.p, S.q, S.v, S.w, S.vp};
-        for (int k = 0; k < 5; ++k)
-            CHECK(copy_d2d(ctx, snap->bodyIn.p + (size_t)k * n, (const double4 *)src[k], n));
+        CHECK(reserve(ctx, snap->ldl, (size_t)ts.iterations * std::max(n, 1) * LDL_STRIDE, false));
+        k_snapshot_bodies<<<grid_for(n, 256), 256, 0, ctx->stream>>>(S, n, snap->bodyIn.p);
+        LAUNCHED();
     }
     if (M)
     {
@@ -1178,12 +1301,9 @@ int replay_step(AvbdContext *ctx, int s, SegSnap *snap)
     auto snapshot = [&](int t) -> int {
         if (!snap)
             return AVBD_OK;
-        double4 *pose = snap->pose.p + (size_t)t * 2 * n;
-        CHECK(copy_d2d(ctx, pose, (const double4 *)S.p, n));
-        CHECK(copy_d2d(ctx, pose + n, (const double4 *)S.q, n));
-        double4 *lp = snap->lp.p + (size_t)t * 16 * M;
-        CHECK(copy_d2d(ctx, lp, (const double4 *)S.lam, 8 * (size_t)M));
-        CHECK(copy_d2d(ctx, lp + 8 * (size_t)M, (const double4 *)S.pen, 8 * (size_t)M));
+        k_snapshot<<<grid_for(std::max<long long>(n, 8ll * M), 256), 256, 0, ctx->stream>>>(
+            S, n, M, snap->pose.p + (size_t)t * 2 * n, snap->lp.p + (size_t)t * 16 * M);
+        LAUNCHED();
         return AVBD_OK;
     };
     for (int t = 0; t < ts.iterations; ++t)
@@ -1194,7 +1314,8 @@ int replay_step(AvbdContext *ctx, int s, SegSnap *snap)
             int first = ts.colourStart[c], count = ts.colourStart[c + 1] - first;
             if (count <= 0)
                 continue;
-            k_rep_primal<<<grid_for(count, 128), 128, 0, ctx->stream>>>(T, B, S, Q, t, first, count);
+            k_rep_primal<<<grid_for(count, ADJ_BLOCK / ADJ_G), ADJ_BLOCK, 0, ctx->stream>>>(
+                T, B, S, Q, t, first, count, snap ? snap->ldl.p : nullptr);
             LAUNCHED();
         }
         if (M)
@@ -1284,6 +1405,7 @@ Snap64 snap_view(const SegSnap &s)
     X.pose = s.pose.p;
     X.lp = s.lp.p;
     X.c0 = s.c0.p;
+    X.ldl = s.ldl.p;
     return X;
 }
 
@@ -1316,7 +1438,8 @@ int reverse_step(AvbdContext *ctx, int s, const SegSnap &snap)
             int first = ts.colourStart[c], count = ts.colourStart[c + 1] - first;
             if (count <= 0)
                 continue;
-            k_adj_primal<<<grid_for(count, 128), 128, 0, ctx->stream>>>(T, X, B, A, Q, t, c, first, count);
+            k_adj_primal<<<grid_for(count, ADJ_BLOCK / ADJ_G), ADJ_BLOCK, 0, ctx->stream>>>(T, X, B, A, Q, t, c,
+                                                                                              first, count);
             LAUNCHED();
         }
     }

@@ -559,9 +559,71 @@ template <class S> DHD void body_dx_vjp(const Ldl6<S> &f, const S dx[6], const S
     }
 }
 
+// The system adjoint of dx = -H^-1 g is rank one: Hbar = -u dx^T, gbar = -u with
+// u = H^-1 dxbar. These forms of the stamp VJPs take (u, dx) instead of the 42 entries.
+template <class S> DHD void body_dx_vjp_u(const Ldl6<S> &f, const S dxbar[6], S u[6]) { ldl_solve(f, dxbar, u); }
+
+// stamp_contact_vjp for Hbar = -u dx^T, gbar = -u: with a_k = J_k . u and d_k = J_k . dx,
+// Fbar_k = -a_k, Kbar_k = -a_k d_k, Jbar_k = -u F_k - K_k (u d_k + dx a_k).
+template <class S> DHD void stamp_contact_vjp_outer(const S u[6], const S dx[6], const ContactIn<S> &c,
+                                                    const ContactFwd<S> &f, bool isA, V3<S> &Fbar, V3<S> &penbar,
+                                                    V3<S> jbar[3])
+{
+    S J[3][6];
+    contact_rows(c, f, isA, J);
+    S K[3] = {c.pen.x, c.pen.y, c.pen.z};
+    S F[3] = {f.F.x, f.F.y, f.F.z};
+    for (int k = 0; k < 3; ++k)
+    {
+        S a = S(0), d = S(0);
+        for (int i = 0; i < 6; ++i)
+        {
+            a += J[k][i] * u[i];
+            d += J[k][i] * dx[i];
+        }
+        add_comp(Fbar, k, -a);
+        add_comp(penbar, k, -a * d);
+        S Jb[3];
+        for (int i = 3; i < 6; ++i)
+            Jb[i - 3] = -u[i] * F[k] - K[k] * (u[i] * d + dx[i] * a);
+        jbar[k] += v3(Jb[0], Jb[1], Jb[2]);
+    }
+}
+
+template <class S> DHD void stamp_inertia_vjp_outer(const S u[6], const S dx[6], S m, V3<S> shape, V3<S> p, V3<S> pt,
+                                                    Q4<S> q, Q4<S> qt, S dt, S &mbar, V3<S> &pbar, V3<S> &ptbar,
+                                                    Q4<S> &qbar, Q4<S> &qtbar)
+{
+    Sys6<S> bar;
+    for (int i = 0; i < 6; ++i)
+    {
+        bar.g[i] = -u[i];
+        bar.H[i][i] = -u[i] * dx[i];
+    }
+    // stamp_inertia_vjp reads gbar and the diagonal of Hbar only
+    S idt2 = S(1) / (dt * dt);
+    V3<S> d = p - pt, a = qdiff(q, qt);
+    V3<S> I = shape * m;
+    mbar += (bar.g[0] * d.x + bar.g[1] * d.y + bar.g[2] * d.z + bar.H[0][0] + bar.H[1][1] + bar.H[2][2]) * idt2;
+    mbar += (shape.x * (bar.g[3] * a.x + bar.H[3][3]) + shape.y * (bar.g[4] * a.y + bar.H[4][4]) +
+             shape.z * (bar.g[5] * a.z + bar.H[5][5])) *
+            idt2;
+    V3<S> dbar = v3(bar.g[0], bar.g[1], bar.g[2]) * (m * idt2);
+    pbar += dbar;
+    ptbar += -dbar;
+    V3<S> abar = v3(I.x * bar.g[3], I.y * bar.g[4], I.z * bar.g[5]) * idt2;
+    qdiff_vjp(q, qt, abar, qbar, qtbar);
+}
+
 // ---------------------------------------------------------------------------
 // Per-contact pieces of the step
 // ---------------------------------------------------------------------------
+
+// Rest of a contact row's primal adjoint once the stamp is reversed (Fbar, jb).
+template <class S> DHD void contact_row_vjp(const Pose<S> &A, const Pose<S> &B, const ContactIn<S> &c,
+                                            const ContactFwd<S> &f, S alpha, unsigned flags, bool isA, V3<S> Fbar,
+                                            const V3<S> jb[3], PoseBar<S> &Ab, PoseBar<S> &Bb, V3<S> &lambar,
+                                            V3<S> &penbar, V3<S> &C0bar, S &mubar);
 
 // Primal adjoint of one contact row for the body being solved: from the system adjoint to
 // both poses, lambda, penalty, C0 and friction.
@@ -573,6 +635,27 @@ template <class S> DHD void contact_primal_vjp(const Pose<S> &A, const Pose<S> &
     V3<S> Fbar = vzero<S>();
     V3<S> jb[3] = {vzero<S>(), vzero<S>(), vzero<S>()};
     stamp_contact_vjp(sysbar, c, f, isA, Fbar, penbar, jb);
+    contact_row_vjp(A, B, c, f, alpha, flags, isA, Fbar, jb, Ab, Bb, lambar, penbar, C0bar, mubar);
+}
+
+// The same with the rank-one system adjoint (u, dx).
+template <class S> DHD void contact_primal_vjp_outer(const Pose<S> &A, const Pose<S> &B, const ContactIn<S> &c,
+                                                     S alpha, unsigned flags, bool isA, const S u[6], const S dx[6],
+                                                     PoseBar<S> &Ab, PoseBar<S> &Bb, V3<S> &lambar, V3<S> &penbar,
+                                                     V3<S> &C0bar, S &mubar)
+{
+    ContactFwd<S> f = contact_forward(A, B, c, alpha, flags);
+    V3<S> Fbar = vzero<S>();
+    V3<S> jb[3] = {vzero<S>(), vzero<S>(), vzero<S>()};
+    stamp_contact_vjp_outer(u, dx, c, f, isA, Fbar, penbar, jb);
+    contact_row_vjp(A, B, c, f, alpha, flags, isA, Fbar, jb, Ab, Bb, lambar, penbar, C0bar, mubar);
+}
+
+template <class S> DHD void contact_row_vjp(const Pose<S> &A, const Pose<S> &B, const ContactIn<S> &c,
+                                            const ContactFwd<S> &f, S alpha, unsigned flags, bool isA, V3<S> Fbar,
+                                            const V3<S> jb[3], PoseBar<S> &Ab, PoseBar<S> &Bb, V3<S> &lambar,
+                                            V3<S> &penbar, V3<S> &C0bar, S &mubar)
+{
     V3<S> Fpb = force_clamp_vjp(f, Fbar, flags, c.mu, mubar);
     lambar += Fpb;
     penbar += hadamard(Fpb, f.C);

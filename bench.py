@@ -1,4 +1,5 @@
-"""Benchmark: body-steps/s of the AVBD step on the 65,536-box stack grid.
+"""Benchmark: body-steps/s of the AVBD step on the 65,536-box stack grid, with the batched
+(4,096 uneven worlds) and differentiable (1,000-box tower, bwd/fwd) forms in the same line.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
 
@@ -212,6 +213,7 @@ def run_cuda(args):
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(scene)
     batched = batched_line(args, local, stream) if not args.no_batched else None
+    adjoint = adjoint_line(args, local, stream) if not args.no_adjoint else None
     w.close()
     if world_size > 1:
         dist.barrier()
@@ -225,6 +227,7 @@ def run_cuda(args):
                            "timing": "CUDA events on the solver stream, summed per step, max over ranks"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(),
                 "gpu_launches": prof["launches"], "phases_ms_per_step": phases, "batched": batched,
+                "adjoint": adjoint,
                 "autotune": {"primal_variant": World.primal_variants()[tuned],
                              "sweep_us": [round(float(x), 1) for x in variant_us]},
                 "step_ms_min_max": [min(step_ms), max(step_ms)]}
@@ -280,6 +283,93 @@ def batched_line(args, local, stream):
             "speedup_vs_loop": batched_rate / loop_rate,
             "workload": "4,096 worlds, box counts log-uniform in [8, 2048] (seed 3): stack fields, jointed "
                         "chains and drop piles, one ground each; same solver parameters"}
+
+
+def adjoint_line(args, local, stream):
+    """Differentiable step on the 1,000-box tower (10 x 10 stacks x 10 high, seed 4): 120 steps
+    at 10 iterations, a checkpoint every 10 steps, loss |COM(x_120) - target|^2. Times the
+    plain forward (avbd_step), the taping forward (avbd_adjoint_forward) and the backward
+    (avbd_adjoint_backward) with a host timer around the C-ABI calls, and checks the gradient
+    against FP64 central differences (h = 1e-4, 32 seeded unit directions over initial
+    velocities, angular velocities, masses and per-pair friction) of the frozen-branch
+    replay recorded by the oracle's bit-identical FP32 run."""
+    import torch
+
+    from avbd_demo3d_b200 import World, scenes
+    from avbd_demo3d_b200.solver import box_properties
+
+    scene = scenes.tower(10, 10, 10, seed=4)
+    T, every = 120, 10
+    mass = np.ascontiguousarray(box_properties(scene.size, scene.density)[0][::-1]).astype(np.float64)
+    dyn = mass > 0
+    M = float(mass[dyn].sum())
+    pos0 = np.ascontiguousarray(scene.pos[::-1]).astype(np.float64)
+    com0 = (mass[dyn, None] * pos0[dyn]).sum(0) / M
+    target = com0 + np.random.default_rng(7).uniform(-1, 1, 3)
+
+    def clock(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, out
+
+    fwd, afwd, bwd = [], [], []
+    grad = None
+    for rep in range(4):  # the first repetition warms up and is not counted
+        w = World(scene, device=local, stream=stream.cuda_stream)
+        f_s, _ = clock(lambda: w.step(T))
+        w.close()
+        w = World(scene, device=local, stream=stream.cuda_stream)
+        a_s, _ = clock(lambda: w.adjoint_forward(T, every))
+        final = w.adjoint_replay_state()["pos"]
+        com = (mass[dyn, None] * final[dyn]).sum(0) / M
+        r = com - target
+        dpos = np.zeros_like(final)
+        dpos[dyn] = 2.0 * r[None, :] * (mass[dyn, None] / M)
+        b_s, g = clock(lambda: w.adjoint_backward(d_pos=dpos))
+        w.close()
+        if rep:
+            fwd.append(f_s)
+            afwd.append(a_s)
+            bwd.append(b_s)
+        dmass = np.zeros(len(mass))
+        dmass[dyn] = 2.0 * ((final[dyn] - com) @ r) / M
+        grad = np.concatenate([(g["vel"] + g["prevvel"]).ravel(), g["angvel"].ravel(), g["mass"] + dmass,
+                               g["pair_friction"]])
+    f_s, a_s, b_s = (statistics.median(x) for x in (fwd, afwd, bwd))
+    out = {"workload": "tower 10x10x10 = 1,000 boxes + ground (seed 4), 120 steps, 10 iterations, checkpoint "
+                       "every 10 steps; loss |COM(x_120) - target|^2, target = COM_0 + U[-1,1]^3 (seed 7)",
+           "forward_ms": f_s * 1e3, "adjoint_forward_ms": a_s * 1e3, "backward_ms": b_s * 1e3,
+           "bwd_over_fwd": b_s / f_s, "fwd_plus_bwd_over_fwd": (a_s + b_s) / f_s,
+           "timing": "host timer around the C-ABI calls (the step itself reads a few counts per step), "
+                     "median of 3 after one warm-up", "params": int(grad.size)}
+    if not args.no_adjoint_check:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import checkers
+
+        ref = checkers.World(scene, "oracle", order_mode=1)
+        ref.tape_begin()
+        ref.step(T)
+        th = ref.adj_theta0()
+        n = ref.n
+        mask = np.zeros(th.size, bool)
+        mask[:3 * n] = np.repeat(dyn, 3)
+        mask[3 * n:6 * n] = np.repeat(dyn, 3)
+        mask[6 * n:7 * n] = dyn
+        mask[7 * n:] = True
+        dirs = np.random.default_rng(1).standard_normal((32, th.size)) * mask
+        dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+        fd = ref.adj_fd(th, target, dirs, h=1e-4)
+        t0 = time.perf_counter()
+        _, rg = ref.adj_gradient(th, target)
+        ref_s = time.perf_counter() - t0
+        ad = dirs @ grad
+        out["check"] = {"fd_directions": 32, "fd_h": 1e-4,
+                        "max_rel_err_vs_fd": float((np.abs(ad - fd) / np.abs(fd)).max()),
+                        "rel_err_vs_reference_adjoint": float(np.linalg.norm(grad - rg) / np.linalg.norm(rg)),
+                        "cpu_reference_adjoint_s": ref_s, "cpu_reference_cores": 1}
+    return out
 
 
 def reference_world(scene):
@@ -344,6 +434,8 @@ def main():
     ap.add_argument("--impl", choices=("cuda", "reference"), default="cuda")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-adjoint-check", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

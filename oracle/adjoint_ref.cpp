@@ -939,6 +939,41 @@ double adjref_selftest(void)
         if (flags & EF_CONE)
             worst = std::max(worst, rel(fd_of([&](Pose<S> &, Pose<S> &, ContactIn<S> *cc, S &, S d) { cc[0].mu += d; }),
                                         mub[0]));
+        // rank-one system adjoint forms against the general ones
+        {
+            S dxr[6], dxbr[6], ur[6];
+            for (int k = 0; k < 6; ++k)
+            {
+                dxr[k] = r.u();
+                dxbr[k] = r.u();
+            }
+            Ldl6<S> fr;
+            ldl_factor(sys.H, fr);
+            body_dx_vjp_u(fr, dxbr, ur);
+            Sys6<S> full;
+            body_dx_vjp(fr, dxr, dxbr, full);
+            PoseBar<S> A1 = posebar_zero<S>(), B1 = posebar_zero<S>(), A2 = posebar_zero<S>(), B2 = posebar_zero<S>();
+            V3<S> l1 = vzero<S>(), l2 = vzero<S>(), p1 = vzero<S>(), p2 = vzero<S>(), z1 = vzero<S>(), z2 = vzero<S>();
+            S m1 = 0, m2 = 0;
+            contact_primal_vjp(A, B, c[1], alpha, flags, false, full, A1, B1, l1, p1, z1, m1);
+            contact_primal_vjp_outer(A, B, c[1], alpha, flags, false, ur, dxr, A2, B2, l2, p2, z2, m2);
+            for (int k = 0; k < 3; ++k)
+            {
+                worst = std::max(worst, rel(((S *)&l1)[k], ((S *)&l2)[k]));
+                worst = std::max(worst, rel(((S *)&p1)[k], ((S *)&p2)[k]));
+                worst = std::max(worst, rel(((S *)&A1.p)[k], ((S *)&A2.p)[k]));
+            }
+            for (int k = 0; k < 4; ++k)
+                worst = std::max(worst, rel(((S *)&B1.q)[k], ((S *)&B2.q)[k]));
+            S mb1 = 0, mb2 = 0;
+            V3<S> pb1 = vzero<S>(), pb2 = vzero<S>(), tb1 = vzero<S>(), tb2 = vzero<S>();
+            Q4<S> qb1 = qzero<S>(), qb2 = qzero<S>(), qt1 = qzero<S>(), qt2 = qzero<S>();
+            stamp_inertia_vjp(full, m, shape, A.p, it, A.q, iq, dt, mb1, pb1, tb1, qb1, qt1);
+            stamp_inertia_vjp_outer(ur, dxr, m, shape, A.p, it, A.q, iq, dt, mb2, pb2, tb2, qb2, qt2);
+            worst = std::max(worst, rel(mb1, mb2));
+            for (int k = 0; k < 4; ++k)
+                worst = std::max(worst, rel(((S *)&qb1)[k], ((S *)&qb2)[k]));
+        }
         // dual update of contact 0
         unsigned dflags = flags | EF_NEG_X | EF_POS_Y | EF_NEG_Z | ((flags & EF_CONE) ? 0u : EF_RAMP_T);
         V3<S> lbN = r.v(), pbN = r.v();

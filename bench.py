@@ -26,6 +26,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from avbd_demo3d_b200.sharding import max_over_ranks  # noqa: E402
+
 METRIC = "body-steps/s at 65k boxes"
 UNIT = "body-steps/s"
 GRID = (64, 64, 16)
@@ -164,10 +166,7 @@ def run_cuda(args):
     total_ms = float(sum(step_ms))
     prof = w.profile()
     w.set_profiling(False)
-    t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
-    if world_size > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
+    max_ms = max_over_ranks(total_ms, device=f"cuda:{local}")
     bodies = scene.n_bodies - 1  # the static ground is not counted
     value = world_size * bodies * args.steps / (max_ms / 1e3)
 
@@ -202,18 +201,16 @@ def run_cuda(args):
         host = w.bodies()
     e2e_s = time.perf_counter() - t0
     d2h = sum(host[k].nbytes for k in ("pos", "quat", "vel", "angvel", "prevvel"))
-    t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
-    if world_size > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e = {"value": world_size * bodies * e2e_steps / float(t.item()), "unit": UNIT, "h2d_bytes_per_step": h2d,
+    e2e_max = max_over_ranks(e2e_s, device=f"cuda:{local}")
+    e2e = {"value": world_size * bodies * e2e_steps / e2e_max, "unit": UNIT, "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h, "steps": e2e_steps,
            "path": "avbd_write_bodies (pinned staging H2D) + avbd_step + avbd_read_bodies (D2H), host timer"}
 
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(scene)
-    batched = batched_line(args, local, stream) if not args.no_batched else None
-    adjoint = adjoint_line(args, local, stream) if not args.no_adjoint else None
+    batched = batched_line(args, rank, world_size, local, stream) if not args.no_batched else None
+    adjoint = adjoint_line(args, local, stream) if (rank == 0 and not args.no_adjoint) else None
     w.close()
     if world_size > 1:
         dist.barrier()
@@ -234,18 +231,26 @@ def run_cuda(args):
         print(json.dumps(line), flush=True)
 
 
-def batched_line(args, local, stream):
-    """World-steps/s of the 4,096-world uneven batch, one context, against looping the plain
-    single-world step over a sample of the same worlds (one resident context per world)."""
+def batched_line(args, rank, world_size, local, stream):
+    """World-steps/s of the 4,096-world uneven batch against looping the plain single-world
+    step over a sample of the same worlds (one resident context per world). With N ranks the
+    worlds are sharded (size-balanced) and each rank steps its shard in one context; the
+    time is the slowest rank's."""
     import torch
+    import torch.distributed as dist
 
     from avbd_demo3d_b200 import World, scenes
+    from avbd_demo3d_b200.sharding import shard_worlds
 
-    worlds = scenes.batched_worlds(4096, seed=3)
+    all_worlds = scenes.batched_worlds(4096, seed=3)
+    shard = shard_worlds([sc.n_bodies for sc in all_worlds], world_size)[rank]
+    worlds = [all_worlds[i] for i in shard]
     w = World(worlds, device=local, stream=stream.cuda_stream)
     w.step(max(3, args.warmup))
     steps = max(3, min(args.steps, 10))
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world_size > 1:
+        dist.barrier()
     torch.cuda.synchronize()
     with torch.cuda.stream(stream):
         ev0.record(stream)
@@ -253,10 +258,10 @@ def batched_line(args, local, stream):
     with torch.cuda.stream(stream):
         ev1.record(stream)
     torch.cuda.synchronize()
-    batched_s = ev0.elapsed_time(ev1) / 1e3
-    n_bodies = int(sum(sc.n_bodies - 1 for sc in worlds))
+    batched_s = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, device=f"cuda:{local}")
+    n_bodies = int(sum(sc.n_bodies - 1 for sc in all_worlds))
     w.close()
-    # loop baseline: the plain step looped over a sample of worlds, each resident
+    # loop baseline: the plain step looped over a sample of this rank's worlds, each resident
     sample = worlds[:: max(1, len(worlds) // 128)][:128]
     ctxs = [World(sc, device=local, stream=stream.cuda_stream) for sc in sample]
     for c in ctxs:
@@ -274,11 +279,13 @@ def batched_line(args, local, stream):
     loop_s = ev0.elapsed_time(ev1) / 1e3
     for c in ctxs:
         c.close()
-    batched_rate = len(worlds) * steps / batched_s
-    loop_rate = len(sample) * loop_steps / loop_s
-    return {"metric": "world-steps/s", "worlds": len(worlds), "bodies": n_bodies, "steps": steps,
+    batched_rate = len(all_worlds) * steps / batched_s
+    # the looped plain step would run on every rank too
+    loop_rate = world_size * len(sample) * loop_steps / max_over_ranks(loop_s, device=f"cuda:{local}")
+    return {"metric": "world-steps/s", "worlds": len(all_worlds), "bodies": n_bodies, "steps": steps,
             "value": batched_rate, "ms_per_step": batched_s * 1e3 / steps,
             "body_steps_per_s": n_bodies * steps / batched_s,
+            "sharding": f"{world_size} rank(s), size-balanced; {len(worlds)} worlds on rank {rank}",
             "loop_plain_step": {"value": loop_rate, "sample_worlds": len(sample), "steps": loop_steps},
             "speedup_vs_loop": batched_rate / loop_rate,
             "workload": "4,096 worlds, box counts log-uniform in [8, 2048] (seed 3): stack fields, jointed "

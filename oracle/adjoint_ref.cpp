@@ -19,6 +19,11 @@
  *                    threaded over the directions.
  * The per-element maps and their VJPs come from avbd_demo3d_b200/csrc/avbd_diff.h.
  *
+ * Parity: the reference computes no gradients, so this path is parity unpinned by the
+ * reference. The tape comes from the oracle's FP32 run, which is bit-exact to the reference;
+ * the gradients are pinned by central finite differences of the double-precision replay
+ * (tests/test_adjoint_ref.py, tests/test_gpu_adjoint.py).
+ *
  * Parameter vector (list order of bodies, n bodies, P friction pairs):
  *   [ v0 (3n) | w0 (3n) | mass (n) | mu (P) ]
  * v0 is the constructor velocity: it sets the velocity and the previous velocity

@@ -58,6 +58,7 @@ const PrimalVariant kPrimalVariants[] = {
     {8, 8, k_primal<8, PRIMAL_BLOCK, 8>},   {4, 1, k_primal<4, PRIMAL_BLOCK, 1>},
     {4, 6, k_primal<4, PRIMAL_BLOCK, 6>},   {16, 1, k_primal<16, PRIMAL_BLOCK, 1>},
     {16, 6, k_primal<16, PRIMAL_BLOCK, 6>}, {32, 1, k_primal<32, PRIMAL_BLOCK, 1>},
+    {4, 8, k_primal<4, PRIMAL_BLOCK, 8>},   {2, 8, k_primal<2, PRIMAL_BLOCK, 8>},
 };
 constexpr int kNumPrimalVariants = (int)(sizeof(kPrimalVariants) / sizeof(kPrimalVariants[0]));
 
@@ -78,6 +79,7 @@ struct AvbdContext
 
     int n = 0;
     DArr<float4> pos, quat, initLin, initAng, inertLin, inertAng, vel, angvel, prevVel, massMoment, sizeRad;
+    DArr<float4> dqLin, dqAng; // pose - initial pose (linear, qdiff), refreshed wherever the pose is written
     DArr<float> friction;
 
     // worlds: static per-world classification, per-step grids (one grid per world)
@@ -311,6 +313,8 @@ DevBodies dev_bodies(AvbdContext *ctx)
     B.quat = ctx->quat.p;
     B.initLin = ctx->initLin.p;
     B.initAng = ctx->initAng.p;
+    B.dqLin = ctx->dqLin.p;
+    B.dqAng = ctx->dqAng.p;
     B.inertLin = ctx->inertLin.p;
     B.inertAng = ctx->inertAng.p;
     B.vel = ctx->vel.p;
@@ -984,7 +988,7 @@ int upload_bodies(AvbdContext *ctx, const AvbdBodies *b, bool props)
             tmp[i] = make_float4(b->size3[3 * i], b->size3[3 * i + 1], b->size3[3 * i + 2], b->radius[i]);
         CHECK(upload(ctx, ctx->sizeRad, tmp.data(), n));
         CHECK(upload(ctx, ctx->friction, b->friction, n));
-        for (DArr<float4> *a : {&ctx->initLin, &ctx->initAng, &ctx->inertLin, &ctx->inertAng})
+        for (DArr<float4> *a : {&ctx->initLin, &ctx->initAng, &ctx->inertLin, &ctx->inertAng, &ctx->dqLin, &ctx->dqAng})
         {
             CHECK(reserve(ctx, *a, std::max(n, 1), false));
             CU(cudaMemsetAsync(a->p, 0, sizeof(float4) * std::max(n, 1), ctx->stream));
@@ -1171,6 +1175,7 @@ void avbd_destroy(AvbdContext *ctx)
         cudaStreamSynchronize(ctx->stream);
     adjoint_release(ctx);
     for (DArr<float4> *a : {&ctx->pos, &ctx->quat, &ctx->initLin, &ctx->initAng, &ctx->inertLin, &ctx->inertAng,
+                            &ctx->dqLin, &ctx->dqAng,
                             &ctx->vel, &ctx->angvel, &ctx->prevVel, &ctx->massMoment, &ctx->sizeRad, &ctx->largeLo,
                             &ctx->largeHi, &ctx->largeSphere, &ctx->spring, &ctx->joint[0], &ctx->joint[1]})
         release(*a);
@@ -1751,11 +1756,15 @@ int avbd_autotune(AvbdContext *ctx, int32_t repeats, int32_t *best_variant, floa
         return fail(ctx, AVBD_ERR_STATE, "autotune needs a stepped world (run avbd_step first)");
     CU(cudaSetDevice(ctx->device));
     int n = ctx->n;
-    DArr<float4> savePos, saveQuat;
+    DArr<float4> savePos, saveQuat, saveDqLin, saveDqAng;
     CHECK(reserve(ctx, savePos, n, false));
     CHECK(reserve(ctx, saveQuat, n, false));
+    CHECK(reserve(ctx, saveDqLin, n, false));
+    CHECK(reserve(ctx, saveDqAng, n, false));
     CU(cudaMemcpyAsync(savePos.p, ctx->pos.p, sizeof(float4) * n, cudaMemcpyDeviceToDevice, ctx->stream));
     CU(cudaMemcpyAsync(saveQuat.p, ctx->quat.p, sizeof(float4) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(saveDqLin.p, ctx->dqLin.p, sizeof(float4) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(saveDqAng.p, ctx->dqAng.p, sizeof(float4) * n, cudaMemcpyDeviceToDevice, ctx->stream));
     DevBodies B = dev_bodies(ctx);
     DevForces F = dev_forces(ctx);
     Params P = dev_params(ctx->params);
@@ -1781,6 +1790,8 @@ int avbd_autotune(AvbdContext *ctx, int32_t repeats, int32_t *best_variant, floa
             CU(cudaEventRecord(ctx->evStop, ctx->stream));
             CU(cudaMemcpyAsync(ctx->pos.p, savePos.p, sizeof(float4) * n, cudaMemcpyDeviceToDevice, ctx->stream));
             CU(cudaMemcpyAsync(ctx->quat.p, saveQuat.p, sizeof(float4) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+            CU(cudaMemcpyAsync(ctx->dqLin.p, saveDqLin.p, sizeof(float4) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+            CU(cudaMemcpyAsync(ctx->dqAng.p, saveDqAng.p, sizeof(float4) * n, cudaMemcpyDeviceToDevice, ctx->stream));
             CU(cudaEventSynchronize(ctx->evStop));
             float ms = 0.0f;
             CU(cudaEventElapsedTime(&ms, ctx->evStart, ctx->evStop));
@@ -1799,6 +1810,8 @@ int avbd_autotune(AvbdContext *ctx, int32_t repeats, int32_t *best_variant, floa
     CU(cudaStreamSynchronize(ctx->stream));
     release(savePos);
     release(saveQuat);
+    release(saveDqLin);
+    release(saveDqAng);
     ctx->primalVariant = best;
     if (best_variant)
         *best_variant = best;

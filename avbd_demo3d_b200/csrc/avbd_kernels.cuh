@@ -41,6 +41,8 @@ struct DevBodies
 {
     int n;
     float4 *pos, *quat, *initLin, *initAng, *inertLin, *inertAng, *vel, *angvel, *prevVel;
+    // pose - initial pose: (pos - initLin, qdiff(quat, initAng)), written with the pose
+    float4 *dqLin, *dqAng;
     float4 *massMoment, *sizeRad;
     float *friction;
 };
@@ -1295,6 +1297,8 @@ __global__ void k_warm_start(DevBodies B, const int *adjStart, Params P)
     float accelWeight = rclamp(accelExt / fabsf(g), 0.0f, 1.0f);
     if (!isfinite(accelWeight))
         accelWeight = 0.0f;
+    const float3 pos0 = pos;
+    const float4 q0 = q;
     B.initLin[b] = f4(pos, 0.0f);
     B.initAng[b] = q;
     if (mass > 0)
@@ -1311,6 +1315,8 @@ __global__ void k_warm_start(DevBodies B, const int *adjStart, Params P)
     B.quat[b] = q;
     B.inertLin[b] = f4(inertLin, 0.0f);
     B.inertAng[b] = inertAng;
+    B.dqLin[b] = f4(sub(pos, pos0), 0.0f);
+    B.dqAng[b] = f4(qdiff(q, q0), 0.0f);
 }
 
 // finishStep velocities (solver.cpp:1275-1287); rolling friction is sphere-only
@@ -1454,14 +1460,32 @@ struct Pose
     float4 q, iq;
 };
 
-AVBD_DEV Pose load_pose(const DevBodies &B, int b)
+// What a contact row reads of a body: its orientation and its pose difference from the
+// step start, dLin = p - p0 and dAng = qdiff(q, q0) (manifold.cpp:185-188). The differences
+// are stored with the pose (k_warm_start, k_primal) instead of being recomputed by every row;
+// they are the same functions of the same floats, so every row sees the same bits.
+struct Motion
 {
-    Pose s;
-    s.p = xyz(B.pos[b]);
-    s.q = B.quat[b];
-    s.ip = xyz(B.initLin[b]);
-    s.iq = B.initAng[b];
-    return s;
+    float4 q;
+    float3 dLin, dAng;
+};
+
+AVBD_DEV Motion motion_of(const Pose &s)
+{
+    Motion m;
+    m.q = s.q;
+    m.dLin = sub(s.p, s.ip);
+    m.dAng = qdiff(s.q, s.iq);
+    return m;
+}
+
+AVBD_DEV Motion load_motion(const DevBodies &B, int b)
+{
+    Motion m;
+    m.q = B.quat[b];
+    m.dLin = xyz(B.dqLin[b]);
+    m.dAng = xyz(B.dqAng[b]);
+    return m;
 }
 
 // a * diag(k): column j of a scaled by k[j]. The reference forms this product with full
@@ -1515,14 +1539,14 @@ struct ContactEval
     float fs, bounds;
 };
 
-AVBD_DEV ContactEval eval_contact(const Pose &A, const Pose &Bp, const M3 &basis, float friction,
+AVBD_DEV ContactEval eval_contact(const Motion &A, const Motion &Bp, const M3 &basis, float friction,
                                   const ContactRec &c, float alpha)
 {
     ContactEval e;
-    float3 dqALin = sub(A.p, A.ip);
-    float3 dqAAng = qdiff(A.q, A.iq);
-    float3 dqBLin = sub(Bp.p, Bp.ip);
-    float3 dqBAng = qdiff(Bp.q, Bp.iq);
+    const float3 &dqALin = A.dLin;
+    const float3 &dqAAng = A.dAng;
+    const float3 &dqBLin = Bp.dLin;
+    const float3 &dqBAng = Bp.dAng;
     float3 rAW = rotate(A.q, c.rA);
     float3 rBW = rotate(Bp.q, c.rB);
     e.jALin = basis;
@@ -1545,11 +1569,17 @@ AVBD_DEV ContactEval eval_contact(const Pose &A, const Pose &Bp, const M3 &basis
     return e;
 }
 
+AVBD_DEV ContactEval eval_contact(const Pose &A, const Pose &Bp, const M3 &basis, float friction,
+                                  const ContactRec &c, float alpha)
+{
+    return eval_contact(motion_of(A), motion_of(Bp), basis, friction, c, alpha);
+}
+
 AVBD_DEV unsigned contact_term(const DevBodies &B, const DevForces &F, unsigned m, int ci, bool isA, float alpha,
                                float *t)
 {
     int2 ab = F.man.ab[m];
-    Pose A = load_pose(B, ab.x), Bp = load_pose(B, ab.y);
+    Motion A = load_motion(B, ab.x), Bp = load_motion(B, ab.y);
     const float4 *bs = F.man.basis + 3 * (size_t)m;
     float4 b0 = bs[0];
     M3 basis = rows(xyz(b0), xyz(bs[1]), xyz(bs[2]));
@@ -1840,8 +1870,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_primal(DevBodies B, DevForces F
     {
         float3 dxl, dxa;
         ldl_solve27(sTerm[g][0], dxl, dxa);
-        B.pos[b] = f4(add(xyz(B.pos[b]), dxl), 0.0f);
-        B.quat[b] = qstep(B.quat[b], dxa);
+        float3 p = add(xyz(B.pos[b]), dxl);
+        float4 q = qstep(B.quat[b], dxa);
+        B.pos[b] = f4(p, 0.0f);
+        B.quat[b] = q;
+        B.dqLin[b] = f4(sub(p, xyz(B.initLin[b])), 0.0f);
+        B.dqAng[b] = f4(qdiff(q, B.initAng[b]), 0.0f);
     }
 }
 
@@ -1857,7 +1891,7 @@ __global__ void k_dual_contacts(DevBodies B, DevManifolds M, int nMan, Params P)
     if (m >= nMan || ci >= M.n[m])
         return;
     int2 ab = M.ab[m];
-    Pose A = load_pose(B, ab.x), Bp = load_pose(B, ab.y);
+    Motion A = load_motion(B, ab.x), Bp = load_motion(B, ab.y);
     const float4 *bs = M.basis + 3 * (size_t)m;
     float4 b0 = bs[0];
     M3 basis = rows(xyz(b0), xyz(bs[1]), xyz(bs[2]));

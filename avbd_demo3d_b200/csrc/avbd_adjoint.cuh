@@ -993,7 +993,11 @@ struct AdjointState
     DArr<double4> rlam[2], rpen[2], rc0;
     int rcur = 0;
     size_t rCap = 0;
-    std::vector<SegSnap> snap;
+    std::vector<SegSnap> snap; // two sets of `every` steps: replay of one segment, reverse of another
+    // The double-precision replay runs on its own stream, overlapping the FP32 steps (forward)
+    // and the reverse sweep of the next segment (backward); events order the two.
+    cudaStream_t side = nullptr;
+    cudaEvent_t evMain = nullptr, evSide = nullptr, evRep[2] = {nullptr, nullptr}, evRev[2] = {nullptr, nullptr};
     // adjoints
     DArr<double4> ap, aq, av, aw, avp, aiLin, aiAng, atLin, atAng;
     DArr<double> am, amu;
@@ -1009,6 +1013,53 @@ template <class T> int copy_d2d(AvbdContext *ctx, T *dst, const T *src, size_t c
 {
     if (count)
         CU(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyDeviceToDevice, ctx->stream));
+    return AVBD_OK;
+}
+
+template <class T> int copy_on(AvbdContext *ctx, cudaStream_t st, T *dst, const T *src, size_t count)
+{
+    if (count)
+        CU(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyDeviceToDevice, st));
+    return AVBD_OK;
+}
+
+int side_init(AvbdContext *ctx)
+{
+    AdjointState *a = ctx->adjoint;
+    if (a->side)
+        return AVBD_OK;
+    CU(cudaStreamCreateWithFlags(&a->side, cudaStreamNonBlocking));
+    for (cudaEvent_t *e : {&a->evMain, &a->evSide, &a->evRep[0], &a->evRep[1], &a->evRev[0], &a->evRev[1]})
+        CU(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    return AVBD_OK;
+}
+
+// the replay stream waits for the work queued so far on the context stream, and back
+int side_after_main(AvbdContext *ctx)
+{
+    AdjointState *a = ctx->adjoint;
+    CU(cudaEventRecord(a->evMain, ctx->stream));
+    CU(cudaStreamWaitEvent(a->side, a->evMain, 0));
+    return AVBD_OK;
+}
+
+int main_after_side(AvbdContext *ctx)
+{
+    AdjointState *a = ctx->adjoint;
+    CU(cudaEventRecord(a->evSide, a->side));
+    CU(cudaStreamWaitEvent(ctx->stream, a->evSide, 0));
+    return AVBD_OK;
+}
+
+// Growth of a buffer the replay stream uses: the context stream (which allocates and frees)
+// first waits for the replay stream, and the replay stream then waits for the new buffer.
+template <class T> int side_reserve(AvbdContext *ctx, DArr<T> &a, size_t count, bool preserve, size_t used = 0)
+{
+    if (count <= a.cap && a.p)
+        return AVBD_OK;
+    CHECK(main_after_side(ctx));
+    CHECK(reserve(ctx, a, count, preserve, used));
+    CHECK(side_after_main(ctx));
     return AVBD_OK;
 }
 
@@ -1034,6 +1085,14 @@ void adjoint_release(AvbdContext *ctx)
     AdjointState *a = ctx->adjoint;
     if (!a)
         return;
+    if (a->side)
+    {
+        cudaStreamSynchronize(a->side);
+        cudaStreamDestroy(a->side);
+    }
+    for (cudaEvent_t e : {a->evMain, a->evSide, a->evRep[0], a->evRep[1], a->evRev[0], a->evRev[1]})
+        if (e)
+            cudaEventDestroy(e);
     for (auto &s : a->tape)
         release_tape(s);
     for (auto &c : a->ck)
@@ -1235,10 +1294,10 @@ int ensure_replay(AvbdContext *ctx, size_t slots)
         return AVBD_OK;
     for (int k = 0; k < 2; ++k)
     {
-        CHECK(reserve(ctx, a->rlam[k], slots, true, a->rCap));
-        CHECK(reserve(ctx, a->rpen[k], slots, true, a->rCap));
+        CHECK(side_reserve(ctx, a->rlam[k], slots, true, a->rCap));
+        CHECK(side_reserve(ctx, a->rpen[k], slots, true, a->rCap));
     }
-    CHECK(reserve(ctx, a->rc0, slots, false));
+    CHECK(side_reserve(ctx, a->rc0, slots, false));
     a->rCap = std::min({a->rlam[0].cap, a->rlam[1].cap, a->rpen[0].cap, a->rpen[1].cap, a->rc0.cap});
     return AVBD_OK;
 }
@@ -1265,10 +1324,11 @@ State64 state_view(AdjointState *a)
 
 int prev_man(AdjointState *a, int s) { return s > 0 ? a->tape[s - 1].nMan : a->nMan0; }
 
-// Replays taped step s; with `snap`, keeps what the reverse sweep reads.
+// Replays taped step s on the replay stream; with `snap`, keeps what the reverse sweep reads.
 int replay_step(AvbdContext *ctx, int s, SegSnap *snap)
 {
     AdjointState *a = ctx->adjoint;
+    cudaStream_t st = a->side;
     const TapeStep &ts = a->tape[s];
     int n = ctx->n, M = ts.nMan;
     size_t m1 = (size_t)std::max(M, 1);
@@ -1280,28 +1340,28 @@ int replay_step(AvbdContext *ctx, int s, SegSnap *snap)
     size_t T1 = (size_t)ts.iterations + 1;
     if (snap)
     {
-        CHECK(reserve(ctx, snap->bodyIn, 5 * (size_t)std::max(n, 1), false));
-        CHECK(reserve(ctx, snap->pose, T1 * 2 * (size_t)std::max(n, 1), false));
-        CHECK(reserve(ctx, snap->lp, T1 * 16 * m1, false));
-        CHECK(reserve(ctx, snap->c0, 8 * m1, false));
-        CHECK(reserve(ctx, snap->ldl, (size_t)ts.iterations * std::max(n, 1) * LDL_STRIDE, false));
-        k_snapshot_bodies<<<grid_for(n, 256), 256, 0, ctx->stream>>>(S, n, snap->bodyIn.p);
+        CHECK(side_reserve(ctx, snap->bodyIn, 5 * (size_t)std::max(n, 1), false));
+        CHECK(side_reserve(ctx, snap->pose, T1 * 2 * (size_t)std::max(n, 1), false));
+        CHECK(side_reserve(ctx, snap->lp, T1 * 16 * m1, false));
+        CHECK(side_reserve(ctx, snap->c0, 8 * m1, false));
+        CHECK(side_reserve(ctx, snap->ldl, (size_t)ts.iterations * std::max(n, 1) * LDL_STRIDE, false));
+        k_snapshot_bodies<<<grid_for(n, 256), 256, 0, st>>>(S, n, snap->bodyIn.p);
         LAUNCHED();
     }
     if (M)
     {
-        k_rep_init<<<grid_for(8ll * M, 128), 128, 0, ctx->stream>>>(T, S, Q);
+        k_rep_init<<<grid_for(8ll * M, 128), 128, 0, st>>>(T, S, Q);
         LAUNCHED();
     }
     if (snap)
-        CHECK(copy_d2d(ctx, snap->c0.p, (const double4 *)S.c0, 8 * (size_t)M));
-    k_rep_warm<<<grid_for(n, 128), 128, 0, ctx->stream>>>(T, B, S, Q);
+        CHECK(copy_on(ctx, st, snap->c0.p, (const double4 *)S.c0, 8 * (size_t)M));
+    k_rep_warm<<<grid_for(n, 128), 128, 0, st>>>(T, B, S, Q);
     LAUNCHED();
     int C = (int)ts.colourStart.size() - 1;
     auto snapshot = [&](int t) -> int {
         if (!snap)
             return AVBD_OK;
-        k_snapshot<<<grid_for(std::max<long long>(n, 8ll * M), 256), 256, 0, ctx->stream>>>(
+        k_snapshot<<<grid_for(std::max<long long>(n, 8ll * M), 256), 256, 0, st>>>(
             S, n, M, snap->pose.p + (size_t)t * 2 * n, snap->lp.p + (size_t)t * 16 * M);
         LAUNCHED();
         return AVBD_OK;
@@ -1314,18 +1374,18 @@ int replay_step(AvbdContext *ctx, int s, SegSnap *snap)
             int first = ts.colourStart[c], count = ts.colourStart[c + 1] - first;
             if (count <= 0)
                 continue;
-            k_rep_primal<<<grid_for(count, ADJ_BLOCK / ADJ_G), ADJ_BLOCK, 0, ctx->stream>>>(
+            k_rep_primal<<<grid_for(count, ADJ_BLOCK / ADJ_G), ADJ_BLOCK, 0, st>>>(
                 T, B, S, Q, t, first, count, snap ? snap->ldl.p : nullptr);
             LAUNCHED();
         }
         if (M)
         {
-            k_rep_dual<<<grid_for(8ll * M, 128), 128, 0, ctx->stream>>>(T, S, Q, t);
+            k_rep_dual<<<grid_for(8ll * M, 128), 128, 0, st>>>(T, S, Q, t);
             LAUNCHED();
         }
     }
     CHECK(snapshot(ts.iterations));
-    k_rep_finish<<<grid_for(n, 128), 128, 0, ctx->stream>>>(T, B, S, Q);
+    k_rep_finish<<<grid_for(n, 128), 128, 0, st>>>(T, B, S, Q);
     LAUNCHED();
     a->rcur ^= 1;
     return AVBD_OK;
@@ -1335,13 +1395,13 @@ int save_replay(AvbdContext *ctx, Checkpoint64 &c, int nMan)
 {
     AdjointState *a = ctx->adjoint;
     int n = ctx->n;
-    CHECK(reserve(ctx, c.body, 5 * (size_t)std::max(n, 1), false));
-    CHECK(reserve(ctx, c.lp, 16 * (size_t)std::max(nMan, 1), false));
+    CHECK(side_reserve(ctx, c.body, 5 * (size_t)std::max(n, 1), false));
+    CHECK(side_reserve(ctx, c.lp, 16 * (size_t)std::max(nMan, 1), false));
     const DArr<double4> *src[5] = {&a->p, &a->q, &a->v, &a->w, &a->vp};
     for (int k = 0; k < 5; ++k)
-        CHECK(copy_d2d(ctx, c.body.p + (size_t)k * n, (const double4 *)src[k]->p, n));
-    CHECK(copy_d2d(ctx, c.lp.p, (const double4 *)a->rlam[a->rcur].p, 8 * (size_t)nMan));
-    CHECK(copy_d2d(ctx, c.lp.p + 8 * (size_t)nMan, (const double4 *)a->rpen[a->rcur].p, 8 * (size_t)nMan));
+        CHECK(copy_on(ctx, a->side, c.body.p + (size_t)k * n, (const double4 *)src[k]->p, n));
+    CHECK(copy_on(ctx, a->side, c.lp.p, (const double4 *)a->rlam[a->rcur].p, 8 * (size_t)nMan));
+    CHECK(copy_on(ctx, a->side, c.lp.p + 8 * (size_t)nMan, (const double4 *)a->rpen[a->rcur].p, 8 * (size_t)nMan));
     c.nMan = nMan;
     return AVBD_OK;
 }
@@ -1353,9 +1413,9 @@ int restore_replay(AvbdContext *ctx, const Checkpoint64 &c)
     CHECK(ensure_replay(ctx, 8 * (size_t)std::max(c.nMan, 1)));
     DArr<double4> *dst[5] = {&a->p, &a->q, &a->v, &a->w, &a->vp};
     for (int k = 0; k < 5; ++k)
-        CHECK(copy_d2d(ctx, dst[k]->p, (const double4 *)c.body.p + (size_t)k * n, n));
-    CHECK(copy_d2d(ctx, a->rlam[a->rcur].p, (const double4 *)c.lp.p, 8 * (size_t)c.nMan));
-    CHECK(copy_d2d(ctx, a->rpen[a->rcur].p, (const double4 *)c.lp.p + 8 * (size_t)c.nMan, 8 * (size_t)c.nMan));
+        CHECK(copy_on(ctx, a->side, dst[k]->p, (const double4 *)c.body.p + (size_t)k * n, n));
+    CHECK(copy_on(ctx, a->side, a->rlam[a->rcur].p, (const double4 *)c.lp.p, 8 * (size_t)c.nMan));
+    CHECK(copy_on(ctx, a->side, a->rpen[a->rcur].p, (const double4 *)c.lp.p + 8 * (size_t)c.nMan, 8 * (size_t)c.nMan));
     return AVBD_OK;
 }
 
@@ -1519,6 +1579,7 @@ int avbd_adjoint_forward(AvbdContext *ctx, int32_t nsteps, int32_t checkpoint_ev
         CHECK(reserve(ctx, *d, n1, false));
     a->nMan0 = ctx->nMan;
     a->rcur = 0;
+    CHECK(side_init(ctx));
     CHECK(ensure_replay(ctx, 8 * (size_t)std::max(ctx->nMan, 1)));
     k_state_to_double<<<grid_for(n, 256), 256, 0, ctx->stream>>>(dev_bodies(ctx), state_view(a));
     LAUNCHED();
@@ -1528,6 +1589,7 @@ int avbd_adjoint_forward(AvbdContext *ctx, int32_t nsteps, int32_t checkpoint_ev
             ctx->man[ctx->cur].contact.p, ctx->nMan, a->rlam[a->rcur].p, a->rpen[a->rcur].p);
         LAUNCHED();
     }
+    CHECK(side_after_main(ctx));
     for (int s = 0; s < nsteps; ++s)
     {
         if (s % checkpoint_every == 0)
@@ -1547,9 +1609,12 @@ int avbd_adjoint_forward(AvbdContext *ctx, int32_t nsteps, int32_t checkpoint_ev
             LAUNCHED();
             a->nKeys += ctx->nMan;
         }
+        // step s is taped: its replay runs while the next FP32 step proceeds
+        CHECK(side_after_main(ctx));
         CHECK(replay_step(ctx, s, nullptr));
     }
     CHECK(save_replay(ctx, a->last, a->tape.back().nMan));
+    CHECK(main_after_side(ctx));
     CHECK(prof_collect(ctx));
     // friction pairs: sorted unique (min, max) body pairs of every manifold met
     int P = 0;
@@ -1717,18 +1782,40 @@ int avbd_adjoint_backward(AvbdContext *ctx, const double *d_position3, const dou
     CU(cudaMemsetAsync(a->apen[0].p, 0, sizeof(double4) * finalSlots, ctx->stream));
 
     int every = a->every;
-    if ((int)a->snap.size() < every)
-        a->snap.resize(every);
+    if ((int)a->snap.size() < 2 * every)
+        a->snap.resize(2 * every);
     int nck = (int)a->ck.size();
-    for (int seg = nck - 1; seg >= 0; --seg)
-    {
+    CHECK(side_init(ctx));
+    CHECK(side_after_main(ctx));
+    // Segment k is replayed into snapshot set k % 2 on the replay stream while segment k + 1
+    // is reversed on the context stream; a set is refilled only after the reverse that read
+    // it has finished.
+    auto replay_segment = [&](int seg) -> int {
+        int set = seg & 1;
         int s0 = seg * every, s1 = std::min(a->steps, s0 + every);
         CHECK(restore_replay(ctx, a->ck[seg]));
         for (int s = s0; s < s1; ++s)
-            CHECK(replay_step(ctx, s, &a->snap[s - s0]));
+            CHECK(replay_step(ctx, s, &a->snap[set * every + (s - s0)]));
+        CU(cudaEventRecord(a->evRep[set], a->side));
+        return AVBD_OK;
+    };
+    CHECK(replay_segment(nck - 1));
+    for (int seg = nck - 1; seg >= 0; --seg)
+    {
+        int set = seg & 1;
+        if (seg > 0)
+        {
+            if (seg + 1 < nck)
+                CU(cudaStreamWaitEvent(a->side, a->evRev[(seg - 1) & 1], 0));
+            CHECK(replay_segment(seg - 1));
+        }
+        CU(cudaStreamWaitEvent(ctx->stream, a->evRep[set], 0));
+        int s0 = seg * every, s1 = std::min(a->steps, s0 + every);
         for (int s = s1 - 1; s >= s0; --s)
-            CHECK(reverse_step(ctx, s, a->snap[s - s0]));
+            CHECK(reverse_step(ctx, s, a->snap[set * every + (s - s0)]));
+        CU(cudaEventRecord(a->evRev[set], ctx->stream));
     }
+    CHECK(main_after_side(ctx));
     // outputs
     auto fetch = [&](const DArr<double4> &src, double *dst, int dim) -> int {
         if (!dst)

@@ -104,6 +104,7 @@ struct AvbdContext
     unsigned cellHashMask = 0, largeHashMask = 0;
     DArr<unsigned long long> bpKeys, bpKeysAlt;
     DArr<int> pairCount, pairOffset;
+    DArr<int> sapVals, sapValsAlt, sapAxis; // sweep and prune: sorted bodies, axis per world
 
     ManBuf man[2];
     int cur = 0;
@@ -570,6 +571,54 @@ int broadphase(AvbdContext *ctx)
             DevForces F2 = dev_forces(ctx);
             k_bp_all_pairs<true><<<grid_for(n, 128), 128, 0, ctx->stream>>>(
                 B, F2, G, n, nullptr, ctx->pairOffset.p, M0, (unsigned long long)ctx->nextSeq, cnt);
+            LAUNCHED();
+        }
+    }
+    else if (mode == AVBD_BROADPHASE_SAP)
+    {
+        // axis per world -> interval keys -> stable sort -> counted sweep -> emitted pairs
+        const int W = ctx->W;
+        CHECK(reserve(ctx, ctx->sapAxis, (size_t)W, false));
+        CHECK(reserve(ctx, ctx->bpKeys, n, false));
+        CHECK(reserve(ctx, ctx->bpKeysAlt, n, false));
+        CHECK(reserve(ctx, ctx->sapVals, n, false));
+        CHECK(reserve(ctx, ctx->sapValsAlt, n, false));
+        CHECK(reserve(ctx, ctx->pairCount, n, false));
+        CHECK(reserve(ctx, ctx->pairOffset, n, false));
+        k_sap_axis<<<W, SAP_TILE, 0, ctx->stream>>>(B, ctx->worldStart.p, ctx->sapAxis.p);
+        LAUNCHED();
+        k_sap_keys<<<grid_for(n, 256), 256, 0, ctx->stream>>>(B, ctx->bodyWorld.p, ctx->sapAxis.p, ctx->bpKeys.p,
+                                                              ctx->sapVals.p);
+        LAUNCHED();
+        cub::DoubleBuffer<unsigned long long> dk(ctx->bpKeys.p, ctx->bpKeysAlt.p);
+        cub::DoubleBuffer<int> dv(ctx->sapVals.p, ctx->sapValsAlt.p);
+        int endBit = 32;
+        while ((1 << (endBit - 32)) < W)
+            ++endBit;
+        size_t bytes = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, bytes, dk, dv, n, 0, endBit, ctx->stream);
+        CHECK(ensure_temp(ctx, bytes));
+        CU(cub::DeviceRadixSort::SortPairs(ctx->cubTemp.p, bytes, dk, dv, n, 0, endBit, ctx->stream));
+        ctx->launches++;
+        DevForces F = dev_forces(ctx);
+        k_sap_sweep<false><<<grid_for(n, 128), 128, 0, ctx->stream>>>(B, F, ctx->sapAxis.p, dk.Current(),
+                                                                       dv.Current(), n, ctx->pairCount.p, nullptr, 0,
+                                                                       0, cnt);
+        LAUNCHED();
+        CHECK(scan_counts(ctx, ctx->pairCount.p, ctx->pairOffset.p, n, 0));
+        ctx->launches++;
+        k_total<<<1, 1, 0, ctx->stream>>>(ctx->pairOffset.p, ctx->pairCount.p, n, ctx->hScalars);
+        LAUNCHED();
+        CU(cudaStreamSynchronize(ctx->stream));
+        P1 = ctx->hScalars[0];
+        if (P1 > 0)
+        {
+            CHECK(reserve_manifolds(ctx, ctx->man[ctx->cur], (size_t)(M0 + P1), (size_t)M0));
+            DevForces F2 = dev_forces(ctx);
+            k_sap_sweep<true><<<grid_for(n, 128), 128, 0, ctx->stream>>>(B, F2, ctx->sapAxis.p, dk.Current(),
+                                                                          dv.Current(), n, nullptr,
+                                                                          ctx->pairOffset.p, M0,
+                                                                          (unsigned long long)ctx->nextSeq, cnt);
             LAUNCHED();
         }
     }
@@ -1196,6 +1245,9 @@ void avbd_destroy(AvbdContext *ctx)
     release(ctx->largeHashKeys);
     release(ctx->largeHashVals);
     release(ctx->bpKeys);
+    release(ctx->sapVals);
+    release(ctx->sapValsAlt);
+    release(ctx->sapAxis);
     release(ctx->bpKeysAlt);
     release(ctx->pairCount);
     release(ctx->pairOffset);
@@ -1283,7 +1335,8 @@ int avbd_set_params(AvbdContext *ctx, const AvbdParams *params)
         return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
     if (!(params->dt > 0.0f) || params->iterations < 0)
         return fail(ctx, AVBD_ERR_ARGUMENT, "invalid dt or iteration count");
-    if (params->broadphase != AVBD_BROADPHASE_GRID && params->broadphase != AVBD_BROADPHASE_ALL_PAIRS)
+    if (params->broadphase != AVBD_BROADPHASE_GRID && params->broadphase != AVBD_BROADPHASE_ALL_PAIRS &&
+        params->broadphase != AVBD_BROADPHASE_SAP)
         return fail(ctx, AVBD_ERR_ARGUMENT, "broadphase mode %d is not available on the GPU", params->broadphase);
     ctx->params = *params;
     return AVBD_OK;

@@ -649,6 +649,139 @@ __global__ void k_bp_large_large(DevForces F, const int *large, const float4 *la
 }
 
 // All-pairs broadphase (solver.cpp:176-185): thread per body a, pairs (a, b > a) of its world.
+// ---------------------------------------------------------------------------
+// Sweep and prune (broadphaseSweepAndPrune, solver.cpp:488-577), one sweep per world.
+// ---------------------------------------------------------------------------
+
+// Sweep axis of each world: the axis of largest centre variance. The reference sums the
+// centres and the squared deviations serially in list order; one block per world stages
+// the positions through shared memory and one thread adds them in that order, so the
+// float sums (and the chosen axis) are the reference's.
+constexpr int SAP_TILE = 256;
+
+__global__ void __launch_bounds__(SAP_TILE) k_sap_axis(DevBodies B, const int *worldStart, int *axisOut)
+{
+    __shared__ float3 tile[SAP_TILE];
+    __shared__ float3 mean;
+    const int w = blockIdx.x;
+    const int b0 = worldStart[w], b1 = worldStart[w + 1];
+    float3 acc = f3(0, 0, 0);
+    for (int pass = 0; pass < 2; ++pass)
+    {
+        if (pass == 1)
+        {
+            if (threadIdx.x == 0)
+                mean = divs(acc, (float)(b1 - b0));
+            acc = f3(0, 0, 0);
+            __syncthreads();
+        }
+        for (int base = b0; base < b1; base += SAP_TILE)
+        {
+            int k = base + (int)threadIdx.x;
+            if (k < b1)
+            {
+                float3 p = xyz(B.pos[k]);
+                if (pass == 1)
+                {
+                    float3 d = sub(p, mean);
+                    p = f3(d.x * d.x, d.y * d.y, d.z * d.z);
+                }
+                tile[threadIdx.x] = p;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0)
+            {
+                int m = min(SAP_TILE, b1 - base);
+                for (int i = 0; i < m; ++i)
+                    acc = add(acc, tile[i]);
+            }
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0)
+    {
+        int axis = 0;
+        if (acc.y > comp(acc, axis))
+            axis = 1;
+        if (acc.z > comp(acc, axis))
+            axis = 2;
+        axisOut[w] = axis;
+    }
+}
+
+// Interval keys: (world, order-preserving bits of min = centre - radius on the world's axis);
+// the value is the body. A stable sort of bodies given in list order then orders equal
+// minima by body index, as the reference's comparator does.
+__global__ void k_sap_keys(DevBodies B, const int *bodyWorld, const int *axis, unsigned long long *keys, int *vals)
+{
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B.n)
+        return;
+    int w = bodyWorld[b];
+    float c = comp(xyz(B.pos[b]), axis[w]);
+    float lo = c - B.sizeRad[b].w;
+    keys[b] = ((unsigned long long)w << 32) | float_order(lo);
+    vals[b] = b;
+}
+
+// Sweep from sorted interval i over the following intervals of its world until one starts
+// past its maximum; bounding-sphere hits become new manifolds (A = interval i's body,
+// B = the later one) unless the bodies are already constrained, in sweep order.
+template <bool EMIT>
+__global__ void k_sap_sweep(DevBodies B, DevForces F, const int *axis, const unsigned long long *keys,
+                            const int *vals, int n, int *counts, const int *offsets, int base,
+                            unsigned long long seqBase, StepCounters *cnt)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const unsigned world = (unsigned)(keys[i] >> 32);
+    const int a = vals[i];
+    const int ax = axis[world];
+    float3 pa = xyz(B.pos[a]);
+    float ra = B.sizeRad[a].w;
+    float ahi = comp(pa, ax) + ra;
+    int found = 0;
+    int out = EMIT ? base + offsets[i] : 0;
+    unsigned long long checks = 0, hits = 0, cons = 0;
+    for (int j = i + 1; j < n; ++j)
+    {
+        if ((unsigned)(keys[j] >> 32) != world)
+            break;
+        int b = vals[j];
+        float3 pb = xyz(B.pos[b]);
+        float rb = B.sizeRad[b].w;
+        if (comp(pb, ax) - rb > ahi)
+            break;
+        checks++;
+        float3 dp = sub(pa, pb);
+        float r = ra + rb;
+        if (dot(dp, dp) > r * r)
+            continue;
+        hits++;
+        if (constrained(F, a, b))
+        {
+            cons++;
+            continue;
+        }
+        if (EMIT)
+        {
+            int m = out + found;
+            F.man.ab[m] = make_int2(a, b);
+            F.man.seq[m] = seqBase + (unsigned long long)(m - base);
+            F.man.n[m] = 0;
+        }
+        found++;
+    }
+    if (!EMIT)
+    {
+        counts[i] = found;
+        atomicAdd(&cnt->pairChecks, checks);
+        atomicAdd(&cnt->sphereHits, hits);
+        atomicAdd(&cnt->constrainedHits, cons);
+    }
+}
+
 template <bool EMIT>
 __global__ void k_bp_all_pairs(DevBodies B, DevForces F, DevGrid G, int n, int *counts, const int *offsets, int base,
                                unsigned long long seqBase, StepCounters *cnt)

@@ -18,8 +18,11 @@ def per_world(arr, ws, w):
     return arr[ws[w]:ws[w + 1]]
 
 
-def test_uneven_batch_matches_each_world_alone(gpu):
+@pytest.mark.parametrize("mode", [scenes.BROADPHASE_GRID, scenes.BROADPHASE_SAP])
+def test_uneven_batch_matches_each_world_alone(gpu, mode):
     worlds = scenes.batched_worlds(24, seed=11, lo=8, hi=160)
+    for sc in worlds:
+        sc.params.broadphase = mode  # one sweep axis (or grid) per world
     g = World(worlds)
     oracles = [checkers.World(sc, "oracle", order_mode=1) for sc in worlds]
     ws = g.world_start

@@ -103,6 +103,14 @@ def test_all_pairs_broadphase(gpu):
     lockstep(sc, 40)
 
 
+@pytest.mark.parametrize("name", ["stacks", "mixed", "pyramid20", "cluster"])
+def test_sweep_and_prune_broadphase(gpu, name):
+    """broadphaseSweepAndPrune: axis by centre variance, sweep in sorted-interval order."""
+    sc = SMALL[name]()
+    sc.params.broadphase = scenes.BROADPHASE_SAP
+    lockstep(sc, 60, every=10)
+
+
 def test_stacks_4096_bit_exact(gpu):
     st = lockstep(scenes.stack_grid(16, 16, 16, seed=1), 60, every=10)
     assert st["manifold_count"] >= 4096 and st["colours"] >= 2
@@ -117,6 +125,15 @@ def test_mixed_joints_springs_fracture(gpu):
 def test_benchmark_scene_65536_boxes_first_steps(gpu):
     """Full-size benchmark scene: the first steps bit-exact (the oracle is serial, so only a few)."""
     lockstep(scenes.stack_grid(64, 64, 16, seed=1), 3)
+
+
+@pytest.mark.slow
+def test_mixed_scene_200k_first_steps(gpu):
+    """Full-size mixed-constraint scene: 200,000 boxes of which 2,048 jointed chains of 48 and
+    5% of the rest paired by springs; the first steps bit-exact (the oracle is serial)."""
+    st = lockstep(scenes.mixed_drop(), 3)
+    assert st["body_count"] == 200_001
+    assert st["joint_count"] == 2048 * 47 and st["spring_count"] > 0
 
 
 def test_colour_order_fixture_from_reference(gpu):

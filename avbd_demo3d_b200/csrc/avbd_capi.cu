@@ -123,6 +123,8 @@ struct AvbdContext
 
     DArr<int> adjStart;
     DArr<unsigned> adj, incVals, incValsAlt;
+    DArr<int> rowCount, entryRow, rowStart; // rows per force-list entry, their offsets, ranges per body
+    DArr<int2> rows;
     DArr<unsigned long long> incKeys, incKeysAlt;
 
     DArr<int> colourState, colour, solveList, colourStart;
@@ -356,6 +358,8 @@ DevForces dev_forces(AvbdContext *ctx)
     F.ignoreSeq = ctx->ignoreSeq.p;
     F.adjStart = ctx->adjStart.p;
     F.adj = ctx->adj.p;
+    F.rowStart = ctx->rowStart.p;
+    F.rows = ctx->rows.p;
     return F;
 }
 
@@ -447,6 +451,8 @@ __global__ void k_u8_to_int(const unsigned char *in, int *out, int n)
 }
 
 // Per-body force lists (CSR) sorted newest first.
+int build_rows(AvbdContext *ctx, const unsigned long long *sortedKeys, int total);
+
 int build_adjacency(AvbdContext *ctx)
 {
     int n = ctx->n;
@@ -455,7 +461,7 @@ int build_adjacency(AvbdContext *ctx)
     if (T == 0)
     {
         CU(cudaMemsetAsync(ctx->adjStart.p, 0, sizeof(int) * ((size_t)n + 1), ctx->stream));
-        return AVBD_OK;
+        return build_rows(ctx, nullptr, 0);
     }
     if (T > (long long)ADJ_INDEX_MASK)
         return fail(ctx, AVBD_ERR_CAPACITY, "too many force incidences (%lld)", T);
@@ -478,6 +484,36 @@ int build_adjacency(AvbdContext *ctx)
                                                                   ctx->adjStart.p);
     LAUNCHED();
     k_copy_adj<<<grid_for(T, 256), 256, 0, ctx->stream>>>(dv.Current(), ctx->adj.p, (int)T);
+    LAUNCHED();
+    return build_rows(ctx, dk.Current(), (int)T);
+}
+
+// The primal's row list, one (entry, row) pair per constraint row in force order, for the
+// dynamic bodies (no host read: sized by an upper bound, ranges from a device scan).
+int build_rows(AvbdContext *ctx, const unsigned long long *sortedKeys, int total)
+{
+    int n = ctx->n;
+    CHECK(reserve(ctx, ctx->rowStart, (size_t)n + 1, false));
+    if (total == 0)
+    {
+        CU(cudaMemsetAsync(ctx->rowStart.p, 0, sizeof(int) * ((size_t)n + 1), ctx->stream));
+        return AVBD_OK;
+    }
+    CHECK(reserve(ctx, ctx->rowCount, (size_t)total + 1, false));
+    CHECK(reserve(ctx, ctx->entryRow, (size_t)total + 1, false));
+    size_t bound = 16 * (size_t)ctx->nMan + 6 * (size_t)ctx->nJoint + 2 * (size_t)ctx->nSpring;
+    CHECK(reserve(ctx, ctx->rows, std::max<size_t>(bound, 1), false));
+    DevForces F = dev_forces(ctx);
+    k_entry_rows<<<grid_for((long long)total + 1, 256), 256, 0, ctx->stream>>>(F, dev_bodies(ctx), sortedKeys, total,
+                                                                               KEY_BODY_SHIFT, ctx->rowCount.p);
+    LAUNCHED();
+    CHECK(scan_counts(ctx, ctx->rowCount.p, ctx->entryRow.p, total + 1, 0));
+    ctx->launches++;
+    k_row_starts<<<grid_for((long long)n + 1, 256), 256, 0, ctx->stream>>>(ctx->adjStart.p, ctx->entryRow.p, n,
+                                                                           ctx->rowStart.p);
+    LAUNCHED();
+    F = dev_forces(ctx);
+    k_entry_fill<<<grid_for(total, 256), 256, 0, ctx->stream>>>(F, ctx->entryRow.p, ctx->rowCount.p, total);
     LAUNCHED();
     return AVBD_OK;
 }
@@ -1245,6 +1281,10 @@ void avbd_destroy(AvbdContext *ctx)
     release(ctx->largeHashKeys);
     release(ctx->largeHashVals);
     release(ctx->bpKeys);
+    release(ctx->rowCount);
+    release(ctx->entryRow);
+    release(ctx->rowStart);
+    release(ctx->rows);
     release(ctx->sapVals);
     release(ctx->sapValsAlt);
     release(ctx->sapAxis);

@@ -73,6 +73,9 @@ struct DevForces
     unsigned long long *ignoreSeq;
     int *adjStart; // n + 1
     unsigned *adj;
+    // the constraint rows each body's primal solve stamps, in force order (rows_listed)
+    int *rowStart; // n + 1
+    int2 *rows;    // (force-list entry, row of that force)
 };
 
 // The reference caps each grid at 2^22 cells (solver.cpp:341-357).
@@ -1856,21 +1859,19 @@ AVBD_DEV unsigned spring_term(const DevBodies &B, const DevForces &F, unsigned s
     return KIND_FULL;
 }
 
-AVBD_DEV int rows_of(const DevForces &F, unsigned e)
+// Rows a force can stamp during one step, in the order the primal adds them: the contacts
+// of a manifold (fixed once Manifold::initialize ran), a joint's linear stamp, its
+// geometric stiffness and its angular stamp (each present while its penalty is nonzero,
+// joint.cpp:60, 103), a spring. Listed once per step; joint parts that are off (a
+// fractured joint, a zero stiffness) stamp nothing, exactly as if they were not listed.
+AVBD_DEV int rows_listed(const DevForces &F, unsigned e)
 {
-    if (e == ADJ_NONE)
-        return 0;
-    unsigned i = adj_index(e);
     switch (adj_type(e))
     {
     case ADJ_MANIFOLD:
-        return F.man.n[i];
+        return F.man.n[adj_index(e)];
     case ADJ_JOINT:
-    {
-        const float4 *d = F.joint + 8 * (size_t)i;
-        int r = lensq(xyz(d[4])) > 0 ? 2 : 0;
-        return r + (lensq(xyz(d[5])) > 0 ? 1 : 0);
-    }
+        return 3;
     case ADJ_SPRING:
         return 1;
     default:
@@ -1878,20 +1879,59 @@ AVBD_DEV int rows_of(const DevForces &F, unsigned e)
     }
 }
 
-AVBD_DEV unsigned row_term(const DevBodies &B, const DevForces &F, unsigned e, int sub, float alpha, float *t)
+// Row list, built in parallel over the force-list entries (sorted incidence keys carry the
+// body): entry k contributes rows_listed rows unless its body is static (never solved).
+// Incidences without a body (the world side of an anchored joint) sort after the last body
+// and contribute none.
+__global__ void k_entry_rows(DevForces F, DevBodies B, const unsigned long long *sortedKeys, int total, int shift,
+                             int *count)
 {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > total)
+        return;
+    int r = 0;
+    if (k < total)
+    {
+        unsigned long long b = sortedKeys[k] >> shift;
+        if (b < (unsigned long long)B.n && B.massMoment[b].x > 0)
+            r = rows_listed(F, F.adj[k]);
+    }
+    count[k] = r; // count[total] = 0, so the exclusive scan ends with the row total
+}
+
+__global__ void k_row_starts(const int *adjStart, const int *entryRow, int n, int *rowStart)
+{
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b <= n)
+        rowStart[b] = entryRow[adjStart[b]];
+}
+
+__global__ void k_entry_fill(DevForces F, const int *entryRow, const int *count, int total)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= total)
+        return;
+    int out = entryRow[k];
+    unsigned e = F.adj[k];
+    for (int sub = 0; sub < count[k]; ++sub)
+        F.rows[out + sub] = make_int2((int)e, sub);
+}
+
+// One listed row's contribution (Manifold/Joint/Spring::updatePrimal).
+AVBD_DEV unsigned listed_row_term(const DevBodies &B, const DevForces &F, int2 row, float alpha, float *t)
+{
+    unsigned e = (unsigned)row.x;
     unsigned i = adj_index(e);
     bool isA = adj_isA(e) != 0;
     switch (adj_type(e))
     {
     case ADJ_MANIFOLD:
-        return contact_term(B, F, i, sub, isA, alpha, t);
+        return contact_term(B, F, i, row.y, isA, alpha, t);
     case ADJ_JOINT:
     {
         const float4 *d = F.joint + 8 * (size_t)i;
-        bool lin = lensq(xyz(d[4])) > 0;
-        int part = lin ? sub : 2;
-        return joint_term(B, F, i, part, isA, alpha, t);
+        bool on = row.y < 2 ? lensq(xyz(d[4])) > 0 : lensq(xyz(d[5])) > 0;
+        return on ? joint_term(B, F, i, row.y, isA, alpha, t) : KIND_NONE;
     }
     case ADJ_SPRING:
         return spring_term(B, F, i, isA, t);
@@ -1924,8 +1964,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_primal(DevBodies B, DevForces F
     constexpr int OWN = (E_COUNT + G - 1) / G;
     __shared__ float sTerm[GPB][G][E_COUNT];
     __shared__ unsigned sKind[GPB][G];
-    __shared__ unsigned sEnt[GPB][G];
-    __shared__ int sOff[GPB][G];
 
     const int g = threadIdx.x / G;
     const int lane = threadIdx.x % G;
@@ -1947,49 +1985,28 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_primal(DevBodies B, DevForces F
     }
     __syncwarp(gmask);
 
-    const int start = F.adjStart[b], end = F.adjStart[b + 1];
-    for (int base = start; base < end; base += G)
+    // the body's rows in force order, G at a time: lane j evaluates row base + j, then every
+    // lane adds the entries it owns row by row, so each sum keeps the reference's order
+    const int r0 = F.rowStart[b], r1 = F.rowStart[b + 1];
+    for (int base = r0; base < r1; base += G)
     {
-        int k = base + lane;
-        unsigned ent = k < end ? F.adj[k] : ADJ_NONE;
-        int nr = rows_of(F, ent);
-        int incl = nr;
-#pragma unroll
-        for (int o = 1; o < G; o <<= 1)
-        {
-            int v = __shfl_up_sync(gmask, incl, o, G);
-            if (lane >= o)
-                incl += v;
-        }
-        int total = __shfl_sync(gmask, incl, G - 1, G);
-        sEnt[g][lane] = ent;
-        sOff[g][lane] = incl - nr;
+        int r = base + lane;
+        if (r < r1)
+            sKind[g][lane] = listed_row_term(B, F, F.rows[r], P.alpha, sTerm[g][lane]);
         __syncwarp(gmask);
-        for (int rb = 0; rb < total; rb += G)
+        int nrows = min(G, r1 - base);
+        for (int rr = 0; rr < nrows; ++rr)
         {
-            int r = rb + lane;
-            if (r < total)
-            {
-                int j = G - 1;
-                while (sOff[g][j] > r)
-                    --j;
-                sKind[g][lane] = row_term(B, F, sEnt[g][j], r - sOff[g][j], P.alpha, sTerm[g][lane]);
-            }
-            __syncwarp(gmask);
-            int nrows = min(G, total - rb);
-            for (int rr = 0; rr < nrows; ++rr)
-            {
-                unsigned kind = sKind[g][rr];
+            unsigned kind = sKind[g][rr];
 #pragma unroll
-                for (int kk = 0; kk < OWN; ++kk)
-                {
-                    int e = lane + kk * G;
-                    if (e < E_COUNT && ((kind >> e) & 1u))
-                        acc[kk] = acc[kk] + sTerm[g][rr][e];
-                }
+            for (int kk = 0; kk < OWN; ++kk)
+            {
+                int e = lane + kk * G;
+                if (e < E_COUNT && ((kind >> e) & 1u))
+                    acc[kk] = acc[kk] + sTerm[g][rr][e];
             }
-            __syncwarp(gmask);
         }
+        __syncwarp(gmask);
     }
 #pragma unroll
     for (int k = 0; k < OWN; ++k)

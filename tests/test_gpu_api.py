@@ -25,8 +25,11 @@ def test_invalid_arguments_are_reported(gpu):
     bad = _lib.AvbdParams(0.0, -10.0, 10, 0.99, 1e4, 100.0, 0.999, 1)
     assert lib.avbd_set_params(h, ctypes.byref(bad)) == -1
     lib.avbd_clear_error(h)
-    sap = _lib.AvbdParams(1 / 60, -10.0, 10, 0.99, 1e4, 100.0, 0.999, 2)
-    assert lib.avbd_set_params(h, ctypes.byref(sap)) == -1
+    unknown = _lib.AvbdParams(1 / 60, -10.0, 10, 0.99, 1e4, 100.0, 0.999, 7)  # no such broadphase mode
+    assert lib.avbd_set_params(h, ctypes.byref(unknown)) == -1
+    lib.avbd_clear_error(h)
+    sap = _lib.AvbdParams(1 / 60, -10.0, 10, 0.99, 1e4, 100.0, 0.999, 2)  # sweep and prune
+    assert lib.avbd_set_params(h, ctypes.byref(sap)) == 0
     lib.avbd_destroy(h)
 
 

@@ -101,6 +101,7 @@ SIGNATURES = {
     "avbd_write_bodies": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AvbdBodies)]),
     "avbd_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     "avbd_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
+    "avbd_broadphase_only": (ctypes.c_int, [ctypes.c_void_p]),
     "avbd_read_bodies": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AvbdBodyState)]),
     "avbd_num_manifolds": (ctypes.c_int, [ctypes.c_void_p, c_int_p]),
     "avbd_read_manifolds": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AvbdManifoldsOut)]),

@@ -1578,6 +1578,42 @@ int avbd_step(AvbdContext *ctx, int32_t nsteps)
     return AVBD_OK;
 }
 
+int avbd_broadphase_only(AvbdContext *ctx)
+{
+    if (!ctx)
+        return AVBD_ERR_ARGUMENT;
+    if (ctx->errCode)
+        return AVBD_ERR_LATCHED;
+    if (!ctx->loaded)
+        return fail(ctx, AVBD_ERR_STATE, "no world loaded");
+    adjoint_invalidate(ctx);
+    CU(cudaSetDevice(ctx->device));
+    // Solver::benchmarkBroadphaseOnly (solver.cpp:989-1034): every manifold goes, so only
+    // joints, springs and ignore pairs count as constraints for the broadphase
+    ctx->nMan = 0;
+    CHECK(build_adjacency(ctx));
+    CU(cudaMemsetAsync(ctx->counters.p, 0, sizeof(StepCounters), ctx->stream));
+    ctx->stats.grid_rescaled = 0;
+    {
+        PhaseScope ps(ctx, AVBD_PHASE_BROADPHASE);
+        CHECK(broadphase(ctx));
+    }
+    // the new manifolds join their bodies' force lists (no contacts until a step)
+    CHECK(build_adjacency(ctx));
+    CU(cudaMemcpyAsync(ctx->hCounters, ctx->counters.p, sizeof(StepCounters), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    ctx->stats.body_count = ctx->n;
+    ctx->stats.manifold_count = ctx->nMan;
+    ctx->stats.contact_count = 0;
+    ctx->stats.pair_checks = (int64_t)ctx->hCounters->pairChecks;
+    ctx->stats.sphere_hits = (int64_t)ctx->hCounters->sphereHits;
+    ctx->stats.constrained_hits = (int64_t)ctx->hCounters->constrainedHits;
+    if (ctx->profiling)
+        ctx->stepsProfiled++;
+    CHECK(prof_collect(ctx));
+    return AVBD_OK;
+}
+
 int avbd_synchronize(AvbdContext *ctx)
 {
     if (!ctx)

@@ -207,6 +207,10 @@ class World:
         if sync:
             self.synchronize()
 
+    def broadphase_only(self):
+        """The reference's collision-only step: drop every manifold, run the broadphase alone."""
+        self._check(self.lib.avbd_broadphase_only(self.h), "avbd_broadphase_only")
+
     def synchronize(self):
         self._check(self.lib.avbd_synchronize(self.h), "avbd_synchronize")
 

@@ -206,6 +206,8 @@ def run_cuda(args):
            "d2h_bytes_per_step": d2h, "steps": e2e_steps,
            "path": "avbd_write_bodies (pinned staging H2D) + avbd_step + avbd_read_bodies (D2H), host timer"}
 
+    collision = collision_only(w, scene, rank, world_size, local, reference=not args.no_cpu_baseline)
+
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(scene)
@@ -224,11 +226,40 @@ def run_cuda(args):
                            "timing": "CUDA events on the solver stream, summed per step, max over ranks"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(),
                 "gpu_launches": prof["launches"], "phases_ms_per_step": phases, "batched": batched,
-                "adjoint": adjoint,
+                "adjoint": adjoint, "collision_only": collision,
                 "autotune": {"primal_variant": World.primal_variants()[tuned],
                              "sweep_us": [round(float(x), 1) for x in variant_us]},
                 "step_ms_min_max": [min(step_ms), max(step_ms)]}
         print(json.dumps(line), flush=True)
+
+
+def collision_only(w, scene, rank, world_size, local, reference: bool, frames: int = 10):
+    """The reference's collision-only benchmark frame (Solver::benchmarkBroadphaseOnly: drop
+    every manifold, run the grid broadphase alone) on the same scene, after the timed steps;
+    host timer around the C-ABI call, which waits for its result. The reference's own CPU
+    frame is timed beside it on the same state (rank 0, one process, 2 frames)."""
+    import torch
+
+    w.broadphase_only()  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(frames):
+        w.broadphase_only()
+    dt = max_over_ranks((time.perf_counter() - t0) / frames, device=f"cuda:{local}")
+    st = w.stats()
+    out = {"ms_per_frame": dt * 1e3, "bodies_per_s": world_size * (scene.n_bodies - 1) / dt,
+           "new_pairs": int(st["manifold_count"]), "pair_checks": int(st["pair_checks"]), "frames": frames}
+    if reference and rank == 0:
+        ref, kind = reference_world(scene)
+        ref.step(1)
+        t0 = time.perf_counter()
+        for _ in range(2):
+            ref.broadphase_only()
+        out["cpu_reference"] = {"ms_per_frame": (time.perf_counter() - t0) / 2 * 1e3, "kind": kind,
+                                "cores": cpu_cores(kind),
+                                "state": "the scene after one step (the GPU frames ran on the state after the "
+                                         "timed steps; the pair count is of the same order)"}
+    return out
 
 
 def batched_line(args, rank, world_size, local, stream):

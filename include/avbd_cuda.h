@@ -223,6 +223,12 @@ int avbd_step(AvbdContext *ctx, int32_t nsteps);
 /* Wait for the context stream. */
 int avbd_synchronize(AvbdContext *ctx);
 
+/* Solver::benchmarkBroadphaseOnly (solver.cpp:989-1034), the reference's collision-only
+ * benchmark step (headless_server.cpp:664-690): every manifold is deleted and the selected
+ * broadphase alone runs, leaving a contact-less manifold for every non-constrained hit pair.
+ * Bodies do not move. Counters land in avbd_get_stats. */
+int avbd_broadphase_only(AvbdContext *ctx);
+
 /* Post-step readback (the contract of readbackAndApply, avbd_gpu_solver.cpp:1970-2022). */
 int avbd_read_bodies(AvbdContext *ctx, const AvbdBodyState *out);
 int avbd_num_manifolds(AvbdContext *ctx, int32_t *count);

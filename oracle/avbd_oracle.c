@@ -1228,15 +1228,10 @@ static void colour_graph(OracleWorld *w)
 static void tape_begin_step(OracleWorld *w);
 static void tape_record_prepared(OracleWorld *w);
 
-int oracle_prepare(OracleWorld *w)
+/* Broadphase (solver.cpp:1074-1083) and the new manifolds in hit order
+ * (applyBroadphaseChunks, solver.cpp:220-248). */
+static void run_broadphase(OracleWorld *w)
 {
-    for (int k = 0; k < 9; ++k)
-        w->counters[k] = 0;
-    if (w->recording)
-        tape_begin_step(w);
-    for (int i = 0; i < w->nMan; ++i)
-        w->man[i].oldIndex = i;
-    /* broadphase (solver.cpp:1074-1083) */
     PairList hits = {0, 0, 0};
     if (w->p.broadphase == 1)
         broadphase_grid(w, &hits);
@@ -1244,7 +1239,6 @@ int oracle_prepare(OracleWorld *w)
         broadphase_sap(w, &hits);
     else
         broadphase_all_pairs(w, &hits);
-    /* new manifolds in hit order (applyBroadphaseChunks, solver.cpp:220-248) */
     if (w->nMan + hits.n > w->capMan)
     {
         while (w->nMan + hits.n > w->capMan)
@@ -1262,6 +1256,31 @@ int oracle_prepare(OracleWorld *w)
     }
     w->counters[3] = hits.n;
     free(hits.v);
+}
+
+/* Solver::benchmarkBroadphaseOnly (solver.cpp:989-1034): delete every manifold, run the
+ * broadphase alone; the new manifolds keep no contacts until a step initialises them. */
+int oracle_broadphase_only(OracleWorld *w)
+{
+    for (int k = 0; k < 9; ++k)
+        w->counters[k] = 0;
+    w->nMan = 0;
+    build_adjacency(w);
+    run_broadphase(w);
+    build_adjacency(w);
+    w->counters[4] = w->nMan;
+    return 0;
+}
+
+int oracle_prepare(OracleWorld *w)
+{
+    for (int k = 0; k < 9; ++k)
+        w->counters[k] = 0;
+    if (w->recording)
+        tape_begin_step(w);
+    for (int i = 0; i < w->nMan; ++i)
+        w->man[i].oldIndex = i;
+    run_broadphase(w);
 
     /* force initialisation and removal of inactive forces (solver.cpp:1085-1132) */
     int keep = 0;

@@ -59,6 +59,10 @@ OracleWorld *oracle_create(const OracleParams *params, int nBodies, const float 
 void oracle_destroy(OracleWorld *w);
 void oracle_set_params(OracleWorld *w, const OracleParams *params);
 
+/* Solver::benchmarkBroadphaseOnly (solver.cpp:989-1034): every manifold is deleted and the
+ * broadphase alone runs, creating contact-less manifolds for the hit pairs. */
+int oracle_broadphase_only(OracleWorld *w);
+
 /* One full step = prepare + iterate + finish (solver.cpp:1036-1041). */
 int oracle_step(OracleWorld *w, int nsteps);
 int oracle_prepare(OracleWorld *w);

@@ -76,7 +76,7 @@ def _lib(kind: str) -> ctypes.CDLL:
     for name in ("destroy",):
         getattr(lib, p + name).argtypes = [vp]
         getattr(lib, p + name).restype = None
-    for name in ("prepare", "iterate", "finish", "num_bodies", "num_manifolds", "num_joints"):
+    for name in ("prepare", "iterate", "finish", "num_bodies", "num_manifolds", "num_joints", "broadphase_only"):
         getattr(lib, p + name).argtypes = [vp]
         getattr(lib, p + name).restype = ip
     getattr(lib, p + "step").argtypes = [vp, ip]
@@ -177,6 +177,9 @@ class World:
 
     def step(self, n: int = 1):
         self._f("step")(self.h, n)
+
+    def broadphase_only(self):
+        self._f("broadphase_only")(self.h)
 
     def prepare(self):
         self._f("prepare")(self.h)

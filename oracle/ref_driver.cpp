@@ -128,6 +128,13 @@ int ref_step(void *p, int nsteps)
     return 0;
 }
 
+int ref_broadphase_only(void *p)
+{
+    RefWorld *w = (RefWorld *)p;
+    w->solver.benchmarkBroadphaseOnly();
+    return 0;
+}
+
 int ref_prepare(void *p)
 {
     ((RefWorld *)p)->solver.prepareStep();

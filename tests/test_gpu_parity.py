@@ -111,6 +111,33 @@ def test_sweep_and_prune_broadphase(gpu, name):
     lockstep(sc, 60, every=10)
 
 
+@pytest.mark.parametrize("mode", [scenes.BROADPHASE_GRID, scenes.BROADPHASE_SAP, scenes.BROADPHASE_ALL_PAIRS])
+def test_broadphase_only(gpu, mode):
+    """avbd_broadphase_only (the collision-only benchmark step) against the oracle's
+    Solver::benchmarkBroadphaseOnly: same new pairs in the same order, same counters, and
+    stepping afterwards stays bit-exact."""
+    sc = scenes.mixed_drop(3000, 20, 12, 0.05, extent=(30, 30, 20), seed=5)
+    sc.params.broadphase = mode
+    g = World(sc)
+    o = checkers.World(sc, "oracle", order_mode=1)
+    g.step(40)
+    o.step(40)
+    for _ in range(2):  # twice in a row: the second pass starts from contact-less manifolds
+        g.broadphase_only()
+        o.broadphase_only()
+        mg, mo = g.manifolds(), o.manifolds()
+        assert len(mg["ab"]) > 0 and np.array_equal(mg["ab"], mo["ab"]) and np.array_equal(mg["seq"], mo["seq"])
+        assert np.all(mg["n"] == 0)
+        st, c = g.stats(), o.counters()
+        assert (st["pair_checks"], st["sphere_hits"], st["constrained_hits"], st["manifold_count"]) == \
+            (c[0], c[1], c[2], c[4])
+    for s in range(1, 11):
+        g.step(1)
+        o.step(1)
+        assert_same_state(g, o, f"after broadphase_only, step {s}")
+    g.close()
+
+
 def test_stacks_4096_bit_exact(gpu):
     st = lockstep(scenes.stack_grid(16, 16, 16, seed=1), 60, every=10)
     assert st["manifold_count"] >= 4096 and st["colours"] >= 2

@@ -108,6 +108,9 @@ SIGNATURES = {
     "avbd_num_joints": (ctypes.c_int, [ctypes.c_void_p, c_int_p]),
     "avbd_read_joints": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AvbdJointsOut)]),
     "avbd_next_seq": (ctypes.c_int, [ctypes.c_void_p, c_i64_p]),
+    "avbd_add_joints": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AvbdJoints)]),
+    "avbd_remove_joints": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, c_i64_p]),
+    "avbd_write_joints": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AvbdJoints)]),
     "avbd_read_colours": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p]),
     "avbd_read_solve_order": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_int_p]),
     "avbd_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AvbdStats)]),

@@ -117,6 +117,10 @@ struct AvbdContext
     DArr<unsigned long long> jointSeq[2];
     DArr<float4> joint[2];
     int jcur = 0;
+    DArr<unsigned long long> editSeq; // joint edits between steps: sorted sequence numbers,
+    DArr<int2> editAB;                // their bodies, packed states (8 float4 each),
+    DArr<float4> editData;            // matched joint per edit, then the match count
+    DArr<int> editJoint;
     DArr<int2> springAB, ignoreAB;
     DArr<unsigned long long> springSeq, ignoreSeq;
     DArr<float4> spring;
@@ -1312,6 +1316,10 @@ void avbd_destroy(AvbdContext *ctx)
         release(ctx->jointAB[k]);
         release(ctx->jointSeq[k]);
     }
+    release(ctx->editSeq);
+    release(ctx->editAB);
+    release(ctx->editData);
+    release(ctx->editJoint);
     release(ctx->springAB);
     release(ctx->springSeq);
     release(ctx->ignoreAB);
@@ -1389,6 +1397,22 @@ int avbd_load_world(AvbdContext *ctx, const AvbdBodies *bodies, const AvbdJoints
     return avbd_load_batch(ctx, 1, ws, bodies, joints, springs, ignores, manifolds, next_seq);
 }
 
+// Device layout of one joint: (rA, kLin) (rB, kAng) (C0Lin, fracture) (C0Ang, torqueArm)
+// (penaltyLin, broken) (penaltyAng) (lambdaLin) (lambdaAng).
+void pack_joint(const AvbdJoints *joints, int j, float4 *d)
+{
+    const float *s = joints->state28 + 28 * (size_t)j;
+    float broken = joints->broken && joints->broken[j] ? 1.0f : 0.0f;
+    d[0] = make_float4(s[0], s[1], s[2], s[24]);
+    d[1] = make_float4(s[3], s[4], s[5], s[25]);
+    d[2] = make_float4(s[6], s[7], s[8], s[26]);
+    d[3] = make_float4(s[9], s[10], s[11], s[27]);
+    d[4] = make_float4(s[12], s[13], s[14], broken);
+    d[5] = make_float4(s[15], s[16], s[17], 0.0f);
+    d[6] = make_float4(s[18], s[19], s[20], 0.0f);
+    d[7] = make_float4(s[21], s[22], s[23], 0.0f);
+}
+
 int avbd_load_batch(AvbdContext *ctx, int32_t num_worlds, const int32_t *world_start, const AvbdBodies *bodies,
                     const AvbdJoints *joints, const AvbdSprings *springs, const AvbdIgnores *ignores,
                     const AvbdManifolds *manifolds, int64_t next_seq)
@@ -1446,18 +1470,7 @@ int avbd_load_batch(AvbdContext *ctx, int32_t num_worlds, const int32_t *world_s
     {
         std::vector<float4> d((size_t)8 * J);
         for (int j = 0; j < J; ++j)
-        {
-            const float *s = joints->state28 + 28 * (size_t)j;
-            float broken = joints->broken && joints->broken[j] ? 1.0f : 0.0f;
-            d[8 * j + 0] = make_float4(s[0], s[1], s[2], s[24]);
-            d[8 * j + 1] = make_float4(s[3], s[4], s[5], s[25]);
-            d[8 * j + 2] = make_float4(s[6], s[7], s[8], s[26]);
-            d[8 * j + 3] = make_float4(s[9], s[10], s[11], s[27]);
-            d[8 * j + 4] = make_float4(s[12], s[13], s[14], broken);
-            d[8 * j + 5] = make_float4(s[15], s[16], s[17], 0.0f);
-            d[8 * j + 6] = make_float4(s[18], s[19], s[20], 0.0f);
-            d[8 * j + 7] = make_float4(s[21], s[22], s[23], 0.0f);
-        }
+            pack_joint(joints, j, &d[8 * (size_t)j]);
         ctx->jcur = 0;
         CHECK(upload(ctx, ctx->joint[0], d.data(), d.size()));
         CHECK(upload(ctx, ctx->jointAB[0], (const int2 *)(J ? joints->body_ab2 : nullptr), J));
@@ -1795,6 +1808,177 @@ int avbd_next_seq(AvbdContext *ctx, int64_t *next_seq)
     if (!ctx || !next_seq)
         return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
     *next_seq = ctx->nextSeq;
+    return AVBD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Joint edits between steps (SimulationHost's drag: simulation_host.cpp:242-274)
+// ---------------------------------------------------------------------------
+
+int edit_begin(AvbdContext *ctx)
+{
+    if (!ctx)
+        return AVBD_ERR_ARGUMENT;
+    if (ctx->errCode)
+        return AVBD_ERR_LATCHED;
+    if (!ctx->loaded)
+        return fail(ctx, AVBD_ERR_STATE, "no world loaded");
+    CU(cudaSetDevice(ctx->device));
+    adjoint_invalidate(ctx);
+    return AVBD_OK;
+}
+
+int world_of(const AvbdContext *ctx, int body)
+{
+    const std::vector<int> &ws = ctx->hWorldStart;
+    return (int)(std::upper_bound(ws.begin(), ws.end(), body) - ws.begin()) - 1;
+}
+
+// Matches `count` sorted sequence numbers (with their bodies, when ab is given) against the
+// device joints; keep (optional) receives the survivors of a removal. Returns the matches.
+int match_joints(AvbdContext *ctx, const std::vector<unsigned long long> &seq, const std::vector<int2> *ab,
+                 bool removal, int &matched)
+{
+    int E = (int)seq.size(), J = ctx->nJoint;
+    CHECK(upload(ctx, ctx->editSeq, seq.data(), (size_t)E));
+    if (ab)
+        CHECK(upload(ctx, ctx->editAB, ab->data(), (size_t)E));
+    CHECK(reserve(ctx, ctx->editJoint, (size_t)E + 1, false));
+    int *counter = ctx->editJoint.p + E;
+    CU(cudaMemsetAsync(ctx->editJoint.p, 0xFF, sizeof(int) * E, ctx->stream));
+    CU(cudaMemsetAsync(counter, 0, sizeof(int), ctx->stream));
+    if (removal)
+        CHECK(reserve(ctx, ctx->keep, (size_t)std::max(J, 1), false));
+    if (J)
+    {
+        k_joint_match<<<grid_for(J, 128), 128, 0, ctx->stream>>>(
+            J, ctx->jointSeq[ctx->jcur].p, ctx->jointAB[ctx->jcur].p, E, ctx->editSeq.p, ab ? ctx->editAB.p : nullptr,
+            ctx->editJoint.p, removal ? ctx->keep.p : nullptr, counter);
+        LAUNCHED();
+    }
+    int *h = (int *)(ctx->hScalars + 8);
+    CU(cudaMemcpyAsync(h, counter, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    matched = *h;
+    return AVBD_OK;
+}
+
+int avbd_add_joints(AvbdContext *ctx, const AvbdJoints *joints)
+{
+    CHECK(edit_begin(ctx));
+    if (!joints || joints->count < 0)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "null or negative joint list");
+    int E = joints->count, J = ctx->nJoint, n = ctx->n;
+    if (!E)
+        return AVBD_OK;
+    if (!joints->body_ab2 || !joints->seq || !joints->state28)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "missing joint arrays");
+    for (int e = 0; e < E; ++e)
+    {
+        int a = joints->body_ab2[2 * e], b = joints->body_ab2[2 * e + 1];
+        if (b < 0 || b >= n || a < -1 || a >= n || a == b || (a >= 0 && world_of(ctx, a) != world_of(ctx, b)))
+            return fail(ctx, AVBD_ERR_ARGUMENT, "joint %d: invalid bodies (%d, %d)", e, a, b);
+        long long prev = e ? (long long)joints->seq[e - 1] : ctx->nextSeq - 1;
+        // a new Joint is the newest force (force.cpp:17-35): sequence numbers keep growing
+        if ((long long)joints->seq[e] <= prev || (unsigned long long)joints->seq[e] > KEY_SEQ_MASK)
+            return fail(ctx, AVBD_ERR_ARGUMENT, "joint %d: sequence %lld is not above %lld", e,
+                        (long long)joints->seq[e], prev);
+    }
+    std::vector<float4> d((size_t)8 * E);
+    std::vector<unsigned long long> sq(E);
+    for (int e = 0; e < E; ++e)
+    {
+        pack_joint(joints, e, &d[8 * (size_t)e]);
+        sq[e] = (unsigned long long)joints->seq[e];
+    }
+    int c = ctx->jcur;
+    CHECK(reserve(ctx, ctx->jointAB[c], (size_t)J + E, true, (size_t)J));
+    CHECK(reserve(ctx, ctx->jointSeq[c], (size_t)J + E, true, (size_t)J));
+    CHECK(reserve(ctx, ctx->joint[c], 8 * ((size_t)J + E), true, 8 * (size_t)J));
+    CU(cudaMemcpyAsync(ctx->jointAB[c].p + J, joints->body_ab2, sizeof(int2) * E, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CU(cudaMemcpyAsync(ctx->jointSeq[c].p + J, sq.data(), sizeof(unsigned long long) * E, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CU(cudaMemcpyAsync(ctx->joint[c].p + 8 * (size_t)J, d.data(), sizeof(float4) * 8 * E, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    ctx->nJoint = J + E;
+    ctx->nextSeq = (long long)sq[E - 1] + 1;
+    CHECK(build_adjacency(ctx));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return AVBD_OK;
+}
+
+int avbd_remove_joints(AvbdContext *ctx, int32_t count, const int64_t *seq)
+{
+    CHECK(edit_begin(ctx));
+    if (count < 0 || (count && !seq))
+        return fail(ctx, AVBD_ERR_ARGUMENT, "null or negative sequence list");
+    if (!count)
+        return AVBD_OK;
+    std::vector<unsigned long long> sq(seq, seq + count);
+    std::sort(sq.begin(), sq.end());
+    if (std::adjacent_find(sq.begin(), sq.end()) != sq.end())
+        return fail(ctx, AVBD_ERR_ARGUMENT, "repeated joint sequence number");
+    int J = ctx->nJoint, matched = 0;
+    CHECK(match_joints(ctx, sq, nullptr, true, matched));
+    if (matched != count)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "%d of %d sequence numbers name no joint", count - matched, count);
+    int newJ = J - matched, o = ctx->jcur ^ 1; // matched counts the joints cleared from keep
+    CHECK(reserve(ctx, ctx->keepIdx, (size_t)std::max(J, 1) * 2, false));
+    int *idx = ctx->keepIdx.p, *cnt32 = ctx->keepIdx.p + std::max(J, 1);
+    k_u8_to_int<<<grid_for(J, 256), 256, 0, ctx->stream>>>(ctx->keep.p, cnt32, J);
+    LAUNCHED();
+    CHECK(scan_counts(ctx, cnt32, idx, J, 0));
+    CHECK(reserve(ctx, ctx->jointAB[o], (size_t)std::max(newJ, 1), false));
+    CHECK(reserve(ctx, ctx->jointSeq[o], (size_t)std::max(newJ, 1), false));
+    CHECK(reserve(ctx, ctx->joint[o], 8 * (size_t)std::max(newJ, 1), false));
+    k_joint_compact<<<grid_for(J, 128), 128, 0, ctx->stream>>>(
+        J, ctx->keep.p, idx, ctx->jointAB[ctx->jcur].p, ctx->jointSeq[ctx->jcur].p, ctx->joint[ctx->jcur].p,
+        ctx->jointAB[o].p, ctx->jointSeq[o].p, ctx->joint[o].p);
+    LAUNCHED();
+    ctx->jcur = o;
+    ctx->nJoint = newJ;
+    CHECK(build_adjacency(ctx));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return AVBD_OK;
+}
+
+int avbd_write_joints(AvbdContext *ctx, const AvbdJoints *joints)
+{
+    CHECK(edit_begin(ctx));
+    if (!joints || joints->count < 0)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "null or negative joint list");
+    int E = joints->count;
+    if (!E)
+        return AVBD_OK;
+    if (!joints->body_ab2 || !joints->seq || !joints->state28)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "missing joint arrays");
+    std::vector<int> order(E);
+    for (int e = 0; e < E; ++e)
+        order[e] = e;
+    std::sort(order.begin(), order.end(), [&](int x, int y) { return joints->seq[x] < joints->seq[y]; });
+    std::vector<unsigned long long> sq(E);
+    std::vector<int2> ab(E);
+    std::vector<float4> d((size_t)8 * E);
+    for (int i = 0; i < E; ++i)
+    {
+        int e = order[i];
+        sq[i] = (unsigned long long)joints->seq[e];
+        ab[i] = make_int2(joints->body_ab2[2 * e], joints->body_ab2[2 * e + 1]);
+        pack_joint(joints, e, &d[8 * (size_t)i]);
+        if (i && sq[i] == sq[i - 1])
+            return fail(ctx, AVBD_ERR_ARGUMENT, "repeated joint sequence number");
+    }
+    int matched = 0;
+    CHECK(match_joints(ctx, sq, &ab, false, matched));
+    if (matched != E)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "%d of %d joints match no device joint (sequence and bodies)",
+                    E - matched, E);
+    CHECK(upload(ctx, ctx->editData, d.data(), d.size()));
+    k_joint_write<<<grid_for(8 * E, 128), 128, 0, ctx->stream>>>(E, ctx->editJoint.p, ctx->editData.p,
+                                                                  ctx->joint[ctx->jcur].p, ctx->nJoint);
+    LAUNCHED();
+    CU(cudaStreamSynchronize(ctx->stream));
     return AVBD_OK;
 }
 

@@ -1322,6 +1322,49 @@ __global__ void k_joint_compact(int count, const unsigned char *keep, const int 
         dD[8 * (size_t)d + k] = dS[8 * (size_t)j + k];
 }
 
+// Joint edits between steps. Each device joint looks its sequence number up in the sorted
+// edit list; a match records the joint index per edit (bodies must agree) and, for a
+// removal, clears the joint's keep flag. matched[0] counts the matches.
+__global__ void k_joint_match(int count, const unsigned long long *seq, const int2 *ab, int edits,
+                              const unsigned long long *editSeq, const int2 *editAB, int *editJoint,
+                              unsigned char *keep, int *matched)
+{
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= count)
+        return;
+    unsigned long long s = seq[j];
+    int lo = 0, hi = edits;
+    while (lo < hi)
+    {
+        int mid = (lo + hi) >> 1;
+        if (editSeq[mid] < s)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    bool hit = lo < edits && editSeq[lo] == s;
+    if (hit && editAB)
+        hit = editAB[lo].x == ab[j].x && editAB[lo].y == ab[j].y;
+    if (keep)
+        keep[j] = hit ? 0 : 1;
+    if (hit)
+    {
+        if (editJoint)
+            editJoint[lo] = j;
+        atomicAdd(matched, 1);
+    }
+}
+
+__global__ void k_joint_write(int edits, const int *editJoint, const float4 *editData, float4 *joint, int count)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 8 * edits)
+        return;
+    int e = t >> 3, k = t & 7, j = editJoint[e];
+    if (j >= 0 && j < count) // -1: the edit matched no joint
+        joint[8 * (size_t)j + k] = editData[t];
+}
+
 // ---------------------------------------------------------------------------
 // Adjacency (per-body force lists, newest first)
 // ---------------------------------------------------------------------------

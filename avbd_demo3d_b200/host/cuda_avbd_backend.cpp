@@ -3,8 +3,11 @@
 //
 // step(Solver&) keeps the reference's object graph as the source of truth at step
 // boundaries, as the WebGPU lane does (avbd_gpu_solver.cpp:2110-2185):
-//   1. if the bodies or forces changed since the last step (scene load, drag joint,
-//      mesh import), upload the whole world; otherwise push only body state;
+//   1. if the body list changed since the last step (scene load, mesh import), upload the
+//      whole world. Otherwise diff the force list against the one mirrored after the last
+//      step: joints created, deleted or edited between steps (SimulationHost's drag,
+//      simulation_host.cpp:242-274) go to the device as joint edits; any other change of
+//      forces reloads the world; body state is pushed every step;
 //   2. run Solver::step's work on the GPU (avbd_step);
 //   3. write bodies back, mirror created/removed manifolds and removed joints into the
 //      object graph in the device's creation order, copy contact and joint state, and
@@ -45,7 +48,10 @@ class CudaAvbdBackend : public PhysicsBackend
             return;
         if (!checkShapes(solver))
             return;
-        if (!loaded_ || topologyChanged(solver))
+        int sync = loaded_ && !bodiesChanged(solver) ? syncForces(solver) : SYNC_RELOAD;
+        if (sync == SYNC_FAILED)
+            return;
+        if (sync == SYNC_RELOAD)
         {
             if (!upload(solver))
                 return;
@@ -60,15 +66,36 @@ class CudaAvbdBackend : public PhysicsBackend
     }
 
     AvbdContext *context() const { return ctx_; }
+    int uploads() const { return uploads_; }
+    int jointEdits() const { return jointEdits_; }
 
   private:
     AvbdContext *ctx_ = nullptr;
     bool failed_ = false;
     bool loaded_ = false;
+    int uploads_ = 0, jointEdits_ = 0;
     std::vector<Rigid *> bodies_; // list order at upload
     std::unordered_map<const Rigid *, int> index_;
-    std::vector<Force *> forcesSeen_; // solver.forces after the last mirror, newest first
     std::unordered_map<int64_t, Force *> bySeq_;
+
+    // solver.forces as mirrored after the last step, newest first, with what a later diff
+    // compares: type, bodies and (joints) the 28-float state the device holds
+    struct Seen
+    {
+        Force *f;
+        int64_t seq;
+        int type;
+        const Rigid *a, *b;
+        float st[28];
+        int32_t broken;
+    };
+    std::vector<Seen> seen_;
+    enum
+    {
+        SYNC_DONE = 0,
+        SYNC_RELOAD = 1,
+        SYNC_FAILED = 2
+    };
 
     bool ok(int rc, const char *what)
     {
@@ -81,7 +108,9 @@ class CudaAvbdBackend : public PhysicsBackend
 
     static int32_t broadphaseOf(const Solver &s)
     {
-        return s.broadphaseMode == BROADPHASE_ALL_PAIRS ? AVBD_BROADPHASE_ALL_PAIRS : AVBD_BROADPHASE_GRID;
+        return s.broadphaseMode == BROADPHASE_ALL_PAIRS       ? AVBD_BROADPHASE_ALL_PAIRS
+               : s.broadphaseMode == BROADPHASE_SWEEP_AND_PRUNE ? AVBD_BROADPHASE_SAP
+                                                                : AVBD_BROADPHASE_GRID;
     }
 
     bool checkShapes(Solver &solver)
@@ -93,28 +122,136 @@ class CudaAvbdBackend : public PhysicsBackend
                 failed_ = true;
                 return false;
             }
-        if (solver.broadphaseMode == BROADPHASE_SWEEP_AND_PRUNE)
-        {
-            std::fprintf(stderr, "CUDA AVBD backend: sweep-and-prune broadphase is not available on the GPU\n");
-            failed_ = true;
-            return false;
-        }
         return true;
     }
 
-    bool topologyChanged(Solver &solver)
+    bool bodiesChanged(Solver &solver) const
     {
         size_t i = 0;
         for (Rigid *b = solver.bodies; b; b = b->next, ++i)
             if (i >= bodies_.size() || bodies_[i] != b)
                 return true;
-        if (i != bodies_.size())
-            return true;
-        i = 0;
-        for (Force *f = solver.forces; f; f = f->next, ++i)
-            if (i >= forcesSeen_.size() || forcesSeen_[i] != f)
-                return true;
-        return i != forcesSeen_.size();
+        return i != bodies_.size();
+    }
+
+    static void jointState(const Joint *j, float *st, int32_t *broken)
+    {
+        const float3 *v[] = {&j->rA,         &j->rB,         &j->C0Lin,     &j->C0Ang,
+                             &j->penaltyLin, &j->penaltyAng, &j->lambdaLin, &j->lambdaAng};
+        for (int k = 0; k < 8; ++k)
+        {
+            st[3 * k] = v[k]->x;
+            st[3 * k + 1] = v[k]->y;
+            st[3 * k + 2] = v[k]->z;
+        }
+        st[24] = j->stiffnessLin;
+        st[25] = j->stiffnessAng;
+        st[26] = j->fracture;
+        st[27] = j->torqueArm;
+        *broken = j->broken ? 1 : 0;
+    }
+
+    // Diff solver.forces against seen_. The reference only ever prepends a new force
+    // (force.cpp:17-22) and unlinks a deleted one, so the survivors keep their order: a walk
+    // from the oldest end matches them, and what is left at the head is new. A new force
+    // that reuses a deleted one's address and is matched in its place keeps the same order
+    // relative to every survivor, and differs in type, bodies or state, which the checks
+    // below see. Joint creation, deletion and edits become device edits; anything else
+    // asks for a reload.
+    int syncForces(Solver &solver)
+    {
+        std::vector<Force *> cur;
+        for (Force *f = solver.forces; f; f = f->next)
+            cur.push_back(f);
+        std::vector<long> match(seen_.size(), -1);
+        long i = (long)cur.size() - 1;
+        for (long k = (long)seen_.size() - 1; k >= 0 && i >= 0; --k)
+            if (cur[(size_t)i] == seen_[(size_t)k].f)
+                match[(size_t)k] = i--;
+        long fresh = i + 1; // cur[0, fresh) were created since the last step
+
+        std::vector<int64_t> removed;
+        std::vector<int32_t> wab;
+        std::vector<int64_t> wseq;
+        std::vector<float> wst;
+        std::vector<int32_t> wbroken;
+        float st[28];
+        int32_t broken;
+        for (size_t k = 0; k < seen_.size(); ++k)
+        {
+            const Seen &s = seen_[k];
+            if (s.seq < 0)
+                return SYNC_RELOAD;
+            if (match[k] < 0)
+            {
+                if (s.type != SIM_CONSTRAINT_JOINT)
+                    return SYNC_RELOAD;
+                removed.push_back(s.seq);
+                continue;
+            }
+            Force *f = cur[(size_t)match[k]];
+            if (f->type != s.type || f->bodyA != s.a || f->bodyB != s.b)
+                return SYNC_RELOAD;
+            if (f->type != SIM_CONSTRAINT_JOINT)
+                continue;
+            jointState((Joint *)f, st, &broken);
+            if (std::memcmp(st, s.st, sizeof(st)) != 0 || broken != s.broken)
+            {
+                wab.push_back(indexOf(f->bodyA));
+                wab.push_back(indexOf(f->bodyB));
+                wseq.push_back(s.seq);
+                wst.insert(wst.end(), st, st + 28);
+                wbroken.push_back(broken);
+            }
+        }
+        std::vector<Joint *> added;
+        std::vector<int32_t> aab;
+        std::vector<float> ast;
+        std::vector<int32_t> abroken;
+        for (long c = fresh - 1; c >= 0; --c) // creation order
+        {
+            Force *f = cur[(size_t)c];
+            if (f->type != SIM_CONSTRAINT_JOINT || indexOf(f->bodyB) < 0 || (f->bodyA && indexOf(f->bodyA) < 0))
+                return SYNC_RELOAD;
+            added.push_back((Joint *)f);
+            aab.push_back(indexOf(f->bodyA));
+            aab.push_back(indexOf(f->bodyB));
+            jointState((Joint *)f, st, &broken);
+            ast.insert(ast.end(), st, st + 28);
+            abroken.push_back(broken);
+        }
+        if (!removed.empty())
+        {
+            if (!ok(avbd_remove_joints(ctx_, (int32_t)removed.size(), removed.data()), "avbd_remove_joints"))
+                return SYNC_FAILED;
+            jointEdits_++;
+            for (int64_t s : removed)
+                bySeq_.erase(s); // the caller deleted the object
+        }
+        if (!added.empty())
+        {
+            int64_t next = 0;
+            if (!ok(avbd_next_seq(ctx_, &next), "avbd_next_seq"))
+                return SYNC_FAILED;
+            std::vector<int64_t> aseq(added.size());
+            for (size_t a = 0; a < added.size(); ++a)
+            {
+                aseq[a] = next + (int64_t)a;
+                bySeq_[aseq[a]] = added[a];
+            }
+            AvbdJoints jv{(int32_t)added.size(), aab.data(), aseq.data(), ast.data(), abroken.data()};
+            if (!ok(avbd_add_joints(ctx_, &jv), "avbd_add_joints"))
+                return SYNC_FAILED;
+            jointEdits_++;
+        }
+        if (!wseq.empty())
+        {
+            AvbdJoints jv{(int32_t)wseq.size(), wab.data(), wseq.data(), wst.data(), wbroken.data()};
+            if (!ok(avbd_write_joints(ctx_, &jv), "avbd_write_joints"))
+                return SYNC_FAILED;
+            jointEdits_++;
+        }
+        return SYNC_DONE;
     }
 
     int indexOf(const Rigid *b) const
@@ -207,19 +344,11 @@ class CudaAvbdBackend : public PhysicsBackend
                 jab.push_back(a0);
                 jab.push_back(b0);
                 jseq.push_back(seq);
-                const float3 *v[] = {&j->rA, &j->rB, &j->C0Lin, &j->C0Ang, &j->penaltyLin, &j->penaltyAng,
-                                     &j->lambdaLin, &j->lambdaAng};
-                for (const float3 *x : v)
-                {
-                    jst.push_back(x->x);
-                    jst.push_back(x->y);
-                    jst.push_back(x->z);
-                }
-                jst.push_back(j->stiffnessLin);
-                jst.push_back(j->stiffnessAng);
-                jst.push_back(j->fracture);
-                jst.push_back(j->torqueArm);
-                jbroken.push_back(j->broken ? 1 : 0);
+                float st[28];
+                int32_t broken;
+                jointState(j, st, &broken);
+                jst.insert(jst.end(), st, st + 28);
+                jbroken.push_back(broken);
             }
             else if (f->type == SIM_CONSTRAINT_SPRING)
             {
@@ -274,6 +403,7 @@ class CudaAvbdBackend : public PhysicsBackend
         if (!ok(avbd_load_world(ctx_, &bv, &jv, &sv, &iv, &mv, total), "avbd_load_world"))
             return false;
         loaded_ = true;
+        uploads_++;
         return true;
     }
 
@@ -381,9 +511,23 @@ class CudaAvbdBackend : public PhysicsBackend
             jt->broken = jbroken[j] != 0;
         }
 
-        forcesSeen_.clear();
+        std::unordered_map<const Force *, int64_t> seqOf;
+        for (auto &kv : bySeq_)
+            seqOf[kv.second] = kv.first;
+        seen_.clear();
         for (Force *f = solver.forces; f; f = f->next)
-            forcesSeen_.push_back(f);
+        {
+            Seen s{};
+            s.f = f;
+            auto it = seqOf.find(f);
+            s.seq = it == seqOf.end() ? -1 : it->second;
+            s.type = f->type;
+            s.a = f->bodyA;
+            s.b = f->bodyB;
+            if (f->type == SIM_CONSTRAINT_JOINT)
+                jointState((Joint *)f, s.st, &s.broken);
+            seen_.push_back(s);
+        }
 
         AvbdStats stats{};
         avbd_get_stats(ctx_, &stats);
@@ -421,4 +565,16 @@ AvbdContext *cudaAvbdBackendContext(PhysicsBackend *backend)
 {
     CudaAvbdBackend *b = dynamic_cast<CudaAvbdBackend *>(backend);
     return b ? b->context() : nullptr;
+}
+
+int cudaAvbdBackendUploads(PhysicsBackend *backend)
+{
+    CudaAvbdBackend *b = dynamic_cast<CudaAvbdBackend *>(backend);
+    return b ? b->uploads() : 0;
+}
+
+int cudaAvbdBackendJointEdits(PhysicsBackend *backend)
+{
+    CudaAvbdBackend *b = dynamic_cast<CudaAvbdBackend *>(backend);
+    return b ? b->jointEdits() : 0;
 }

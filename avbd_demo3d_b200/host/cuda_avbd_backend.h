@@ -18,3 +18,9 @@ std::unique_ptr<PhysicsBackend> makeCudaAvbdPhysicsBackend(int device = 0);
 // The device context behind a backend made by makeCudaAvbdPhysicsBackend (null for any
 // other backend), for callers that query the ABI directly (colouring, profiles).
 AvbdContext *cudaAvbdBackendContext(PhysicsBackend *backend);
+
+// Whole-world uploads and joint-edit calls made so far by a backend made by
+// makeCudaAvbdPhysicsBackend (0 for any other backend): a session whose only changes
+// are drags and parameter commands uploads once.
+int cudaAvbdBackendUploads(PhysicsBackend *backend);
+int cudaAvbdBackendJointEdits(PhysicsBackend *backend);

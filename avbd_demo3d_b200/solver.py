@@ -263,6 +263,53 @@ class World:
         out["state"] = np.ascontiguousarray(out["state28"][:, 6:24])
         return out
 
+    # -- joint edits between steps (SimulationHost's drag, simulation_host.cpp:242-274)
+    def next_seq(self) -> int:
+        q = ctypes.c_int64()
+        self._check(self.lib.avbd_next_seq(self.h, ctypes.byref(q)), "avbd_next_seq")
+        return q.value
+
+    def add_joint(self, a, b, rA, rB, stiff_lin=float("inf"), stiff_ang=0.0, fracture=float("inf")) -> int:
+        """new Joint(solver, a, b, rA, rB, stiffLin, stiffAng, fracture) (joint.cpp:25-33) on
+        list-order bodies (a = -1: anchored to the world point rA). Returns its sequence number."""
+        seq = self.next_seq()
+        size = self.props["size"]
+        sa = size[a] if a >= 0 else np.zeros(3, F32)
+        ssum = (sa + size[b]).astype(F32)
+        state = np.zeros((1, 28), F32)
+        state[0, 0:3] = rA
+        state[0, 3:6] = rB
+        state[0, 24:27] = (stiff_lin, stiff_ang, fracture)
+        state[0, 27] = _dot32(ssum[None], ssum[None])[0]
+        self._edit_joints("avbd_add_joints", np.array([[a, b]], np.int32), np.array([seq], np.int64), state)
+        return seq
+
+    def _edit_joints(self, fn, ab, seq, state, broken=None):
+        ab, seq, state = _c(ab, np.int32), _c(seq, np.int64), _c(state, F32)
+        broken = _c(np.zeros(len(seq), np.int32) if broken is None else broken, np.int32)
+        j = _lib.AvbdJoints(len(seq), _ptr(ab), _ptr(seq), _ptr(state), _ptr(broken))
+        self._check(getattr(self.lib, fn)(self.h, ctypes.byref(j)), fn)
+
+    def write_joints(self, ab, seq, state28, broken=None):
+        """Overwrite the state of existing joints, matched by sequence number."""
+        self._edit_joints("avbd_write_joints", ab, seq, state28, broken)
+
+    def set_joint_anchor(self, seq, rA):
+        """Joint::rA = rA (updateDrag)."""
+        j = self.joints()
+        k = np.flatnonzero(j["seq"] == seq)
+        if k.size != 1:
+            raise _lib.AvbdError(f"no joint with sequence number {seq}")
+        st = j["state28"][k].copy()
+        st[0, 0:3] = rA
+        self.write_joints(j["ab"][k], j["seq"][k], st, j["broken"][k])
+
+    def remove_joint(self, seq):
+        """delete joint (releaseDrag)."""
+        q = np.array([seq], np.int64)
+        self._check(self.lib.avbd_remove_joints(self.h, 1, q.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))),
+                    "avbd_remove_joints")
+
     def colours(self):
         c = np.zeros(max(self.n, 1), np.int32)
         nc = ctypes.c_int32()

@@ -237,6 +237,23 @@ int avbd_num_joints(AvbdContext *ctx, int32_t *count);
 int avbd_read_joints(AvbdContext *ctx, const AvbdJointsOut *out);
 int avbd_next_seq(AvbdContext *ctx, int64_t *next_seq);
 
+/* Joint edits between steps, as SimulationHost makes them for a mouse drag
+ * (beginDrag / updateDrag / releaseDrag, simulation_host.cpp:242-274; Joint constructor
+ * joint.cpp:25-33, Force constructor / destructor force.cpp:14-39 / 42-). None of them
+ * reloads the world.
+ *
+ * avbd_add_joints appends joints as the newest forces: their sequence numbers must be
+ * strictly increasing and at or above avbd_next_seq (which then moves past the last);
+ * body_a may be -1 (anchored to the world point rA) and both bodies lie in one world.
+ * avbd_remove_joints deletes the joints with the given sequence numbers (every number
+ * must name a joint; nothing changes otherwise).
+ * avbd_write_joints overwrites state28 and broken of existing joints, matched by sequence
+ * number; body_ab2 must equal the joint's bodies (it is a check, not an edit).
+ * Each call drops the recorded forward of the differentiable step. */
+int avbd_add_joints(AvbdContext *ctx, const AvbdJoints *joints);
+int avbd_remove_joints(AvbdContext *ctx, int32_t count, const int64_t *seq);
+int avbd_write_joints(AvbdContext *ctx, const AvbdJoints *joints);
+
 /* Parity dumps: colour per body of the last step (-1 = not solved) and colour count;
  * the primal sweep order (bodies grouped by colour). */
 int avbd_read_colours(AvbdContext *ctx, int32_t *colour, int32_t *num_colours);

@@ -1679,6 +1679,70 @@ int oracle_step(OracleWorld *w, int nsteps)
 /* Construction and queries                                                  */
 /* ------------------------------------------------------------------------- */
 
+/* Joint constructor (joint.cpp:25-33): the newest force, zero penalty and lambda. */
+static Joint *new_joint(OracleWorld *w, int a, int b, V3 rA, V3 rB, float stiffLin, float stiffAng, float fracture)
+{
+    w->joints = (Joint *)realloc(w->joints, sizeof(Joint) * (size_t)(w->nJoints + 1));
+    Joint *j = &w->joints[w->nJoints++];
+    memset(j, 0, sizeof(*j));
+    j->a = a;
+    j->b = b;
+    j->seq = w->nextSeq++;
+    j->rA = rA;
+    j->rB = rB;
+    j->stiffLin = stiffLin;
+    j->stiffAng = stiffAng;
+    j->fracture = fracture;
+    V3 sa = a >= 0 ? w->bodies[a].size : v3(0, 0, 0);
+    j->torqueArm = vlensq(vadd(sa, w->bodies[b].size));
+    return j;
+}
+
+static Joint *joint_by_seq(OracleWorld *w, int64_t seq)
+{
+    for (int i = 0; i < w->nJoints; ++i)
+        if (w->joints[i].seq == seq)
+            return &w->joints[i];
+    return NULL;
+}
+
+int64_t oracle_add_joint(OracleWorld *w, int a, int b, const float *rA3, const float *rB3, float stiffLin,
+                         float stiffAng, float fracture)
+{
+    if (b < 0 || b >= w->n || a >= w->n || a < -1 || a == b)
+        return -1;
+    Joint *j = new_joint(w, a, b, v3(rA3[0], rA3[1], rA3[2]), v3(rB3[0], rB3[1], rB3[2]), stiffLin, stiffAng,
+                         fracture);
+    build_adjacency(w);
+    return j->seq;
+}
+
+int oracle_set_joint_anchor(OracleWorld *w, int64_t seq, const float *rA3)
+{
+    Joint *j = joint_by_seq(w, seq);
+    if (!j)
+        return -1;
+    j->rA = v3(rA3[0], rA3[1], rA3[2]);
+    return 0;
+}
+
+int oracle_remove_joint(OracleWorld *w, int64_t seq)
+{
+    int keep = 0, found = 0;
+    for (int i = 0; i < w->nJoints; ++i)
+    {
+        if (w->joints[i].seq == seq)
+        {
+            found = 1;
+            continue;
+        }
+        w->joints[keep++] = w->joints[i];
+    }
+    w->nJoints = keep;
+    build_adjacency(w);
+    return found ? 0 : -1;
+}
+
 OracleWorld *oracle_create(const OracleParams *params, int nBodies, const float *size3, const float *density,
                            const float *friction, const float *pos3, const float *vel3, const float *quat4,
                            int nForces, const int *ftype, const int *fa, const int *fb, const float *frA3,
@@ -1715,25 +1779,13 @@ OracleWorld *oracle_create(const OracleParams *params, int nBodies, const float 
         int b = nBodies - 1 - fb[k];
         V3 rA = v3(frA3[3 * k], frA3[3 * k + 1], frA3[3 * k + 2]);
         V3 rB = v3(frB3[3 * k], frB3[3 * k + 1], frB3[3 * k + 2]);
-        int64_t seq = w->nextSeq++;
         if (ftype[k] == ORACLE_FORCE_JOINT)
         {
-            w->joints = (Joint *)realloc(w->joints, sizeof(Joint) * (size_t)(w->nJoints + 1));
-            Joint *j = &w->joints[w->nJoints++];
-            memset(j, 0, sizeof(*j));
-            j->a = a;
-            j->b = b;
-            j->seq = seq;
-            j->rA = rA;
-            j->rB = rB;
-            j->stiffLin = fparam3[3 * k];
-            j->stiffAng = fparam3[3 * k + 1];
-            j->fracture = fparam3[3 * k + 2];
-            /* joint.cpp:25-33 */
-            V3 sa = a >= 0 ? w->bodies[a].size : v3(0, 0, 0);
-            j->torqueArm = vlensq(vadd(sa, w->bodies[b].size));
+            new_joint(w, a, b, rA, rB, fparam3[3 * k], fparam3[3 * k + 1], fparam3[3 * k + 2]);
+            continue;
         }
-        else if (ftype[k] == ORACLE_FORCE_SPRING)
+        int64_t seq = w->nextSeq++;
+        if (ftype[k] == ORACLE_FORCE_SPRING)
         {
             w->springs = (Spring *)realloc(w->springs, sizeof(Spring) * (size_t)(w->nSprings + 1));
             Spring *s = &w->springs[w->nSprings++];

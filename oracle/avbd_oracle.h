@@ -63,6 +63,14 @@ void oracle_set_params(OracleWorld *w, const OracleParams *params);
  * broadphase alone runs, creating contact-less manifolds for the hit pairs. */
 int oracle_broadphase_only(OracleWorld *w);
 
+/* Joint edits between steps, as SimulationHost's drag makes them (simulation_host.cpp:242-274):
+ * a new Joint (the newest force; a = -1 anchors it to the world point rA) returns its
+ * sequence number; the anchor rA moves; the joint is deleted. Bodies in list order. */
+int64_t oracle_add_joint(OracleWorld *w, int a, int b, const float *rA3, const float *rB3, float stiffLin,
+                         float stiffAng, float fracture);
+int oracle_set_joint_anchor(OracleWorld *w, int64_t seq, const float *rA3);
+int oracle_remove_joint(OracleWorld *w, int64_t seq);
+
 /* One full step = prepare + iterate + finish (solver.cpp:1036-1041). */
 int oracle_step(OracleWorld *w, int nsteps);
 int oracle_prepare(OracleWorld *w);

@@ -79,6 +79,12 @@ def _lib(kind: str) -> ctypes.CDLL:
     for name in ("prepare", "iterate", "finish", "num_bodies", "num_manifolds", "num_joints", "broadphase_only"):
         getattr(lib, p + name).argtypes = [vp]
         getattr(lib, p + name).restype = ip
+    getattr(lib, p + "add_joint").argtypes = [vp, ip, ip, fp, fp, ctypes.c_float, ctypes.c_float, ctypes.c_float]
+    getattr(lib, p + "add_joint").restype = ctypes.c_int64
+    getattr(lib, p + "set_joint_anchor").argtypes = [vp, ctypes.c_int64, fp]
+    getattr(lib, p + "set_joint_anchor").restype = ip
+    getattr(lib, p + "remove_joint").argtypes = [vp, ctypes.c_int64]
+    getattr(lib, p + "remove_joint").restype = ip
     getattr(lib, p + "step").argtypes = [vp, ip]
     getattr(lib, p + "step").restype = ip
     getattr(lib, p + "set_params").argtypes = [vp, ctypes.POINTER(_Params)]
@@ -180,6 +186,24 @@ class World:
 
     def broadphase_only(self):
         self._f("broadphase_only")(self.h)
+
+    # joint edits between steps (list-order bodies; a = -1 anchors to the world point rA)
+    def add_joint(self, a, b, rA, rB, stiff_lin=float("inf"), stiff_ang=0.0, fracture=float("inf")) -> int:
+        rA = np.ascontiguousarray(rA, np.float32)
+        rB = np.ascontiguousarray(rB, np.float32)
+        h = self._f("add_joint")(self.h, int(a), int(b), _ptr(rA), _ptr(rB), stiff_lin, stiff_ang, fracture)
+        if h < 0:
+            raise ValueError("add_joint refused")
+        return int(h)
+
+    def set_joint_anchor(self, handle, rA):
+        rA = np.ascontiguousarray(rA, np.float32)
+        if self._f("set_joint_anchor")(self.h, int(handle), _ptr(rA)) != 0:
+            raise ValueError("unknown joint")
+
+    def remove_joint(self, handle):
+        if self._f("remove_joint")(self.h, int(handle)) != 0:
+            raise ValueError("unknown joint")
 
     def prepare(self):
         self._f("prepare")(self.h)

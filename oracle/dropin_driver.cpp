@@ -6,6 +6,8 @@
  *   - the reference's CPU solver run in the GPU's colour order (prepareStep, body list
  *     relinked into the sweep order read from the device, iteratePrimalDualCpu,
  *     finishStep): must be bit-identical.
+ * With --commands, every host gets the same scripted bridge commands between frames
+ * (drag begin / move / end, iterations, broadphase, time step, gravity).
  * Built by oracle/Makefile (target `dropin`) from the reference's sources plus the
  * adapter avbd_demo3d_b200/host/cuda_avbd_backend.cpp; prints one JSON line per scene.
  */
@@ -52,6 +54,84 @@ static void iterate_in_order(Solver &s, const std::vector<int> &order)
 
 static bool same_bits(const void *a, const void *b, size_t n) { return std::memcmp(a, b, n) == 0; }
 
+// The n-th dynamic body of the dense SimWorld (a drag target), or -1.
+static int dynamic_body(const SimulationHost &h, int nth)
+{
+    const SimWorld &w = h.world();
+    for (size_t id = 0; id < w.bodies.size(); ++id)
+    {
+        const SimBodyData &d = w.bodies[id];
+        if (d.active && d.source && d.source->mass > 0.0f && nth-- == 0)
+            return (int)id;
+    }
+    return -1;
+}
+
+// A scripted session of the bridge's commands (SimulationHost::applyCommand,
+// simulation_host.cpp:121-226), given before frame f: drag one body along a path,
+// release it, drag another (a new joint, possibly at the freed address), change the
+// iteration count, broadphase, time step and gravity.
+static void apply_commands(SimulationHost &h, int f, float3 &anchor)
+{
+    auto cmd = [&](const char *name) {
+        SimulationCommand c;
+        c.command = name;
+        return c;
+    };
+    if (f == 5 || f == 70)
+    {
+        int id = dynamic_body(h, f == 5 ? 0 : 1);
+        if (id < 0)
+            return;
+        SimulationCommand c = cmd("beginDrag");
+        c.bodyId = (uint32_t)id;
+        c.hasBodyId = true;
+        anchor = h.world().bodies[id].source->positionLin;
+        c.worldHit = anchor;
+        c.hasWorldHit = true;
+        c.localHit = float3{0.1f, -0.05f, 0.2f};
+        c.hasLocalHit = true;
+        h.applyCommand(c);
+    }
+    if ((f > 5 && f < 60) || (f > 70 && f < 100))
+    {
+        SimulationCommand c = cmd("updateDrag");
+        float t = (float)(f % 60);
+        c.worldTarget = float3{anchor.x + 0.03f * t, anchor.y + 0.02f * t, anchor.z + 0.04f * t};
+        c.hasWorldTarget = true;
+        h.applyCommand(c);
+    }
+    if (f == 60 || f == 100)
+        h.applyCommand(cmd("endDrag"));
+    if (f == 30)
+    {
+        SimulationCommand c = cmd("setIterations");
+        c.numberValue = 7;
+        c.hasNumber = true;
+        h.applyCommand(c);
+    }
+    if (f == 45)
+    {
+        SimulationCommand c = cmd("setBroadphase");
+        c.stringValue = "sap";
+        h.applyCommand(c);
+    }
+    if (f == 80)
+    {
+        SimulationCommand c = cmd("setDt");
+        c.numberValue = 1.0 / 120.0;
+        c.hasNumber = true;
+        h.applyCommand(c);
+    }
+    if (f == 90)
+    {
+        SimulationCommand c = cmd("setGravity");
+        c.numberValue = -4.0;
+        c.hasNumber = true;
+        h.applyCommand(c);
+    }
+}
+
 static double qdist(quat a, quat b)
 {
     double d = 0, f = 0;
@@ -66,11 +146,14 @@ static double qdist(quat a, quat b)
 int main(int argc, char **argv)
 {
     int frames = 120;
+    bool commands = false;
     std::vector<std::string> names;
     for (int i = 1; i < argc; ++i)
     {
         if (!std::strcmp(argv[i], "--frames") && i + 1 < argc)
             frames = std::atoi(argv[++i]);
+        else if (!std::strcmp(argv[i], "--commands"))
+            commands = true;
         else
             names.push_back(argv[i]);
     }
@@ -94,8 +177,15 @@ int main(int argc, char **argv)
         int firstMismatch = -1;
         double maxPos = 0, maxRot = 0, sumSq = 0;
         long count = 0;
+        float3 anchors[3] = {};
         for (int f = 1; f <= frames; ++f)
         {
+            if (commands)
+            {
+                apply_commands(gpu, f, anchors[0]);
+                apply_commands(cpu, f, anchors[1]);
+                apply_commands(colour, f, anchors[2]);
+            }
             gpu.stepFrame();
             cpu.stepFrame();
             int32_t nSolve = 0;
@@ -138,13 +228,14 @@ int main(int argc, char **argv)
             cm += f->type == SIM_CONSTRAINT_MANIFOLD;
         bool exact = firstMismatch < 0 && gm == cm;
         failures += exact ? 0 : 1;
-        std::printf("{\"scene\": \"%s\", \"backend\": \"%s\", \"frames\": %d, \"bodies\": %d, \"manifolds\": %d, "
+        std::printf("{\"scene\": \"%s\", \"commands\": %s, \"backend\": \"%s\", \"frames\": %d, \"bodies\": %d, \"manifolds\": %d, "
                     "\"bit_exact_vs_colour_order_reference\": %s, \"first_mismatch_frame\": %d, "
                     "\"max_position_error_vs_cpu_backend\": %.6g, \"rms_position_error_vs_cpu_backend\": %.6g, "
-                    "\"max_rotation_error_vs_cpu_backend\": %.6g}\n",
-                    name.c_str(), gpu.solver().physicsBackend->name(), frames, (int)list_of(gpu.solver()).size(),
+                    "\"max_rotation_error_vs_cpu_backend\": %.6g, \"world_uploads\": %d, \"joint_edits\": %d}\n",
+                    name.c_str(), commands ? "true" : "false", gpu.solver().physicsBackend->name(), frames, (int)list_of(gpu.solver()).size(),
                     gm, exact ? "true" : "false", firstMismatch, maxPos, count ? std::sqrt(sumSq / count) : 0.0,
-                    maxRot);
+                    maxRot, cudaAvbdBackendUploads(gpu.solver().physicsBackend.get()),
+                    cudaAvbdBackendJointEdits(gpu.solver().physicsBackend.get()));
         std::fflush(stdout);
     }
     return failures ? 1 : 0;

@@ -27,6 +27,7 @@ struct RefWorld
     Solver solver;
     std::vector<Rigid *> list; // list order: index 0 = solver.bodies head
     std::unordered_map<const Rigid *, int> index;
+    std::vector<Joint *> added; // joints created between steps, by handle
 };
 
 void rebuild_index(RefWorld *w)
@@ -125,6 +126,41 @@ int ref_step(void *p, int nsteps)
     RefWorld *w = (RefWorld *)p;
     for (int s = 0; s < nsteps; ++s)
         w->solver.step();
+    return 0;
+}
+
+/* Joint edits between steps with the reference's own constructor / fields / destructor
+ * (SimulationHost::beginDrag / updateDrag / releaseDrag, simulation_host.cpp:242-274).
+ * The handle is the joint's index among the joints added this way. */
+int64_t ref_add_joint(void *p, int a, int b, const float *rA3, const float *rB3, float stiffLin, float stiffAng,
+                      float fracture)
+{
+    RefWorld *w = (RefWorld *)p;
+    Rigid *A = a >= 0 ? w->list[a] : 0;
+    Joint *j = new Joint(&w->solver, A, w->list[b], float3{rA3[0], rA3[1], rA3[2]}, float3{rB3[0], rB3[1], rB3[2]},
+                         stiffLin, stiffAng, fracture);
+    w->solver.world.syncFromLegacy(w->solver);
+    w->added.push_back(j);
+    return (int64_t)w->added.size() - 1;
+}
+
+int ref_set_joint_anchor(void *p, int64_t handle, const float *rA3)
+{
+    RefWorld *w = (RefWorld *)p;
+    if (handle < 0 || handle >= (int64_t)w->added.size() || !w->added[handle])
+        return -1;
+    w->added[handle]->rA = float3{rA3[0], rA3[1], rA3[2]};
+    return 0;
+}
+
+int ref_remove_joint(void *p, int64_t handle)
+{
+    RefWorld *w = (RefWorld *)p;
+    if (handle < 0 || handle >= (int64_t)w->added.size() || !w->added[handle])
+        return -1;
+    delete w->added[handle];
+    w->added[handle] = 0;
+    w->solver.world.syncFromLegacy(w->solver);
     return 0;
 }
 

@@ -27,3 +27,22 @@ def test_reference_scenes_through_the_backend_adapter(gpu):
     for scene in ("Pyramid", "Rope"):
         assert gates[scene]["max_position_error_vs_cpu_backend"] < 0.05, gates[scene]
     assert out.returncode == 0, out.stderr
+
+
+def test_bridge_commands_through_the_backend_adapter(gpu):
+    """The bridge's commands between frames on every scene (drag begin / move / end twice,
+    setIterations, setBroadphase sap, setDt, setGravity): the adapter turns the drag joint's
+    creation, anchor moves and deletion into device joint edits and stays bit-exact with
+    the reference's CPU solver in the GPU's colour order."""
+    if not os.path.exists(DROPIN):
+        pytest.skip("drop-in harness not built (needs the reference sources: make -C oracle dropin)")
+    out = subprocess.run([DROPIN, "--frames", "120", "--commands"], capture_output=True, text=True, timeout=600)
+    rows = [json.loads(l) for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(rows) == 15, out.stdout + out.stderr
+    for r in rows:
+        assert r["commands"] and r["backend"].startswith("CUDA AVBD"), r
+        assert r["bit_exact_vs_colour_order_reference"], r
+        assert r["world_uploads"] == 1, r  # drags are joint edits, not reloads
+    dragged = [r for r in rows if r["joint_edits"] > 0]
+    assert len(dragged) >= 10, rows  # every scene with a dynamic body was dragged
+    assert out.returncode == 0, out.stderr

@@ -77,6 +77,48 @@ def test_broadphase_only_matches_reference(mode):
         assert np.array_equal(bits(bo[k]), bits(br[k])), k
 
 
+def _drag_script(w, props, steps=60):
+    """SimulationHost's drag between steps: beginDrag (a world-anchored Joint, stiffness 5000,
+    0), updateDrag moving the anchor every step, a body-body joint added on the way,
+    releaseDrag, then a few free steps. Yields after every step."""
+    b = int(np.flatnonzero(props["mass"] > 0)[-1])
+    pos = w.bodies()["pos"][b].astype(np.float64)
+    local = np.array([0.1, -0.05, 0.2], np.float32)
+    h = w.add_joint(-1, b, pos.astype(np.float32), local, 5000.0, 0.0)
+    link = None
+    for s in range(steps):
+        target = (pos + np.array([0.05 * s, 0.02 * s, 0.04 * s])).astype(np.float32)
+        w.set_joint_anchor(h, target)
+        if s == 20:
+            link = w.add_joint(b, b - 1, [0.0, 0.5, 0.0], [0.0, -0.5, 0.0], float("inf"), 100.0, 1e4)
+        if s == 40:
+            w.remove_joint(link)
+        w.step(1)
+        yield s
+    w.remove_joint(h)
+    for s in range(10):
+        w.step(1)
+        yield steps + s
+
+
+def test_drag_edits_match_reference():
+    """Joint edits between steps (drag begin / move / release, a body-body joint added and
+    deleted) keep the oracle bit-identical to the reference."""
+    sc = scenes.mixed_drop(1200, 8, 10, 0.1, extent=(20, 20, 14), seed=31)
+    o = checkers.World(sc, "oracle", order_mode=0)
+    r = checkers.World(sc, "ref")
+    o.step(20)
+    r.step(20)
+    props = o.body_props()
+    for so, sr in zip(_drag_script(o, props), _drag_script(r, props)):
+        assert so == sr
+        bo, br = o.bodies(), r.bodies()
+        for k in bo:
+            assert np.array_equal(bits(bo[k]), bits(br[k])), (so, k)
+        jo, jr = o.joints(), r.joints()
+        assert np.array_equal(jo["ab"], jr["ab"]) and np.array_equal(bits(jo["state"]), bits(jr["state"])), so
+
+
 def test_narrowphase_random_pairs():
     import make_golden
 

@@ -50,7 +50,7 @@ constexpr int PRIMAL_BLOCK = 128;
 struct PrimalVariant
 {
     int group, minBlocks;
-    void (*kernel)(DevBodies, DevForces, Params, const int *, int, int);
+    void (*kernel)(DevBodies, DevForces, Params, const int4 *, int, int);
 };
 
 const PrimalVariant kPrimalVariants[] = {
@@ -132,6 +132,7 @@ struct AvbdContext
     DArr<unsigned long long> incKeys, incKeysAlt;
 
     DArr<int> colourState, colour, solveList, colourStart;
+    DArr<int4> solveEntry; // solve list with each body's row range, for the primal
     DArr<unsigned> colKeys, colKeysAlt;
     DArr<ColourControl> colourCtl;
     int colourBlocks = 148;   // co-resident blocks for the cooperative colouring launch
@@ -429,7 +430,8 @@ __global__ void k_colour_count(const ColourControl *ctl, int *unused, int *summa
     summary[3] = ctl->error;
 }
 
-__global__ void k_solve_list_all(const unsigned *keys, int n, int *list, int *colourStart, const ColourControl *ctl)
+__global__ void k_solve_list_all(const unsigned *keys, int n, int *list, int *colourStart, const ColourControl *ctl,
+                                 const int *rowStart, int4 *entries)
 {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     int count = ctl->vertices;
@@ -437,7 +439,9 @@ __global__ void k_solve_list_all(const unsigned *keys, int n, int *list, int *co
     if (k >= count)
         return;
     unsigned key = keys[k];
-    list[k] = (int)(key & 0xFFFFFFu);
+    int b = (int)(key & 0xFFFFFFu);
+    list[k] = b;
+    entries[k] = make_int4(b, rowStart[b], rowStart[b + 1], 0);
     int c = (int)(key >> 24);
     int prev = k > 0 ? (int)(keys[k - 1] >> 24) : -1;
     for (int x = prev + 1; x <= c; ++x)
@@ -847,6 +851,7 @@ int colour_bodies(AvbdContext *ctx)
     CHECK(reserve(ctx, ctx->colourState, n, false));
     CHECK(reserve(ctx, ctx->colour, n, false));
     CHECK(reserve(ctx, ctx->solveList, n, false));
+    CHECK(reserve(ctx, ctx->solveEntry, n, false));
     CHECK(reserve(ctx, ctx->colKeys, n, false));
     CHECK(reserve(ctx, ctx->colKeysAlt, n, false));
     CHECK(reserve(ctx, ctx->colourStart, 257, false));
@@ -877,7 +882,8 @@ int colour_bodies(AvbdContext *ctx)
     k_colour_count<<<1, 1, 0, ctx->stream>>>(ctx->colourCtl.p, ctx->colourStart.p + 257 - 257, ctx->hColourSummary);
     LAUNCHED();
     k_solve_list_all<<<grid_for(n, 256), 256, 0, ctx->stream>>>(dk.Current(), n, ctx->solveList.p, ctx->colourStart.p,
-                                                                 ctx->colourCtl.p);
+                                                                 ctx->colourCtl.p, ctx->rowStart.p,
+                                                                 ctx->solveEntry.p);
     LAUNCHED();
     CU(cudaMemcpyAsync(ctx->hColourStarts, ctx->colourStart.p, sizeof(int) * 257, cudaMemcpyDeviceToHost,
                        ctx->stream));
@@ -922,7 +928,7 @@ int iterate(AvbdContext *ctx)
             if (count <= 0)
                 continue;
             PhaseScope ps(ctx, AVBD_PHASE_PRIMAL);
-            pv.kernel<<<grid_for(count, GPB), PRIMAL_BLOCK, 0, ctx->stream>>>(B, F, P, ctx->solveList.p, first,
+            pv.kernel<<<grid_for(count, GPB), PRIMAL_BLOCK, 0, ctx->stream>>>(B, F, P, ctx->solveEntry.p, first,
                                                                                count);
             LAUNCHED();
         }
@@ -1333,6 +1339,7 @@ void avbd_destroy(AvbdContext *ctx)
     release(ctx->colourState);
     release(ctx->colour);
     release(ctx->solveList);
+    release(ctx->solveEntry);
     release(ctx->colourStart);
     release(ctx->colourCtl);
     release(ctx->colKeys);
@@ -2096,7 +2103,7 @@ int avbd_autotune(AvbdContext *ctx, int32_t repeats, int32_t *best_variant, floa
             {
                 int first = ctx->hColourStart[c], count = ctx->hColourStart[c + 1] - first;
                 if (count > 0)
-                    pv.kernel<<<grid_for(count, GPB), PRIMAL_BLOCK, 0, ctx->stream>>>(B, F, P, ctx->solveList.p,
+                    pv.kernel<<<grid_for(count, GPB), PRIMAL_BLOCK, 0, ctx->stream>>>(B, F, P, ctx->solveEntry.p,
                                                                                        first, count);
             }
             CU(cudaGetLastError());

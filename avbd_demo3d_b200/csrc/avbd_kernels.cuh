@@ -75,7 +75,7 @@ struct DevForces
     unsigned *adj;
     // the constraint rows each body's primal solve stamps, in force order (rows_listed)
     int *rowStart; // n + 1
-    int2 *rows;    // (force-list entry, row of that force)
+    int2 *rows;    // (force-list entry, (partner body + 1) << 3 | row of that force)
 };
 
 // The reference caps each grid at 2^22 cells (solver.cpp:341-357).
@@ -1754,25 +1754,6 @@ AVBD_DEV ContactEval eval_contact(const Pose &A, const Pose &Bp, const M3 &basis
     return eval_contact(motion_of(A), motion_of(Bp), basis, friction, c, alpha);
 }
 
-AVBD_DEV unsigned contact_term(const DevBodies &B, const DevForces &F, unsigned m, int ci, bool isA, float alpha,
-                               float *t)
-{
-    int2 ab = F.man.ab[m];
-    Motion A = load_motion(B, ab.x), Bp = load_motion(B, ab.y);
-    const float4 *bs = F.man.basis + 3 * (size_t)m;
-    float4 b0 = bs[0];
-    M3 basis = rows(xyz(b0), xyz(bs[1]), xyz(bs[2]));
-    ContactRec c = load_contact(F.man.contact + (size_t)m * 32 + 4 * ci);
-    ContactEval e = eval_contact(A, Bp, basis, b0.w, c, alpha);
-    const M3 &jLin = isA ? e.jALin : e.jBLin;
-    const M3 &jAng = isA ? e.jAAng : e.jBAng;
-    M3 jLinT = trans(jLin), jAngT = trans(jAng);
-    M3 jAngTk = times_diag(jAngT, c.pen);
-    store_terms(t, mm(times_diag(jLinT, c.pen), jLin), mm(jAngTk, jAng), mm(jAngTk, jLin), mv(jLinT, e.F),
-                mv(jAngT, e.F));
-    return KIND_FULL;
-}
-
 AVBD_DEV M3 gs_ball_socket(int k, float3 v)
 {
     float vk = comp(v, k);
@@ -1949,6 +1930,34 @@ __global__ void k_row_starts(const int *adjStart, const int *entryRow, int n, in
         rowStart[b] = entryRow[adjStart[b]];
 }
 
+// The other body of a force-list entry (-1: the world side of an anchored joint).
+AVBD_DEV int entry_partner(const DevForces &F, unsigned e)
+{
+    unsigned i = adj_index(e);
+    bool isA = adj_isA(e) != 0;
+    int2 ab = make_int2(-1, -1);
+    switch (adj_type(e))
+    {
+    case ADJ_MANIFOLD:
+        ab = F.man.ab[i];
+        break;
+    case ADJ_JOINT:
+        ab = F.jointAB[i];
+        break;
+    case ADJ_SPRING:
+        ab = F.springAB[i];
+        break;
+    default:
+        break;
+    }
+    return isA ? ab.y : ab.x;
+}
+
+// Row entries carry the partner body next to the row index (bodies < 2^24, rows < 8), so
+// a contact row's partner pose is fetched together with its contact data.
+AVBD_DEV int row_sub(int2 row) { return row.y & 7; }
+AVBD_DEV int row_partner(int2 row) { return (row.y >> 3) - 1; }
+
 __global__ void k_entry_fill(DevForces F, const int *entryRow, const int *count, int total)
 {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1956,25 +1965,51 @@ __global__ void k_entry_fill(DevForces F, const int *entryRow, const int *count,
         return;
     int out = entryRow[k];
     unsigned e = F.adj[k];
-    for (int sub = 0; sub < count[k]; ++sub)
-        F.rows[out + sub] = make_int2((int)e, sub);
+    int n = count[k];
+    if (n == 0)
+        return;
+    int code = (entry_partner(F, e) + 1) << 3;
+    for (int sub = 0; sub < n; ++sub)
+        F.rows[out + sub] = make_int2((int)e, code | sub);
+}
+
+// Contact row of body `self` against its partner (Manifold::updatePrimal,
+// manifold.cpp:183-228); the partner comes from the row entry.
+AVBD_DEV unsigned contact_term_self(const DevBodies &B, const DevForces &F, unsigned m, int ci, bool isA, int self,
+                                    int partner, float alpha, float *t)
+{
+    const float4 *bs = F.man.basis + 3 * (size_t)m;
+    float4 b0 = bs[0];
+    M3 basis = rows(xyz(b0), xyz(bs[1]), xyz(bs[2]));
+    ContactRec c = load_contact(F.man.contact + (size_t)m * 32 + 4 * ci);
+    Motion A = load_motion(B, isA ? self : partner), Bm = load_motion(B, isA ? partner : self);
+    ContactEval e = eval_contact(A, Bm, basis, b0.w, c, alpha);
+    const M3 &jLin = isA ? e.jALin : e.jBLin;
+    const M3 &jAng = isA ? e.jAAng : e.jBAng;
+    M3 jLinT = trans(jLin), jAngT = trans(jAng);
+    M3 jAngTk = times_diag(jAngT, c.pen);
+    store_terms(t, mm(times_diag(jLinT, c.pen), jLin), mm(jAngTk, jAng), mm(jAngTk, jLin), mv(jLinT, e.F),
+                mv(jAngT, e.F));
+    return KIND_FULL;
 }
 
 // One listed row's contribution (Manifold/Joint/Spring::updatePrimal).
-AVBD_DEV unsigned listed_row_term(const DevBodies &B, const DevForces &F, int2 row, float alpha, float *t)
+AVBD_DEV unsigned listed_row_term(const DevBodies &B, const DevForces &F, int2 row, int self, float alpha,
+                                  float *t)
 {
     unsigned e = (unsigned)row.x;
     unsigned i = adj_index(e);
     bool isA = adj_isA(e) != 0;
+    int sub = row_sub(row);
     switch (adj_type(e))
     {
     case ADJ_MANIFOLD:
-        return contact_term(B, F, i, row.y, isA, alpha, t);
+        return contact_term_self(B, F, i, sub, isA, self, row_partner(row), alpha, t);
     case ADJ_JOINT:
     {
         const float4 *d = F.joint + 8 * (size_t)i;
-        bool on = row.y < 2 ? lensq(xyz(d[4])) > 0 : lensq(xyz(d[5])) > 0;
-        return on ? joint_term(B, F, i, row.y, isA, alpha, t) : KIND_NONE;
+        bool on = sub < 2 ? lensq(xyz(d[4])) > 0 : lensq(xyz(d[5])) > 0;
+        return on ? joint_term(B, F, i, sub, isA, alpha, t) : KIND_NONE;
     }
     case ADJ_SPRING:
         return spring_term(B, F, i, isA, t);
@@ -1998,8 +2033,15 @@ AVBD_DEV void initial_system(const DevBodies &B, int b, float dt, float *t)
     store_terms(t, lhsLin, lhsAng, lhsCross, rhsLin, rhsAng);
 }
 
+// One primal solve per body of a colour (solver.cpp:1186-1233). Rows: G lanes per body.
+// The solve entries carry the body and its row range; every lane of a group builds the
+// initial system M/dt^2 and keeps the entries it owns, then the rows are evaluated G at a
+// time (lane j evaluates row base + j into shared memory) and every lane adds its entries
+// row by row, so each sum keeps the reference's order. Solve: the block's accumulated
+// systems go to shared memory and one thread per body factors its 6x6 system and moves
+// the body, so the factorisation runs with every lane of its warp busy.
 template <int G, int BLOCK, int MINB>
-__global__ void __launch_bounds__(BLOCK, MINB) k_primal(DevBodies B, DevForces F, Params P, const int *list,
+__global__ void __launch_bounds__(BLOCK, MINB) k_primal(DevBodies B, DevForces F, Params P, const int4 *entries,
                                                         int first, int count)
 {
     static_assert(BLOCK % G == 0 && 32 % G == 0, "group size");
@@ -2007,62 +2049,84 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_primal(DevBodies B, DevForces F
     constexpr int OWN = (E_COUNT + G - 1) / G;
     __shared__ float sTerm[GPB][G][E_COUNT];
     __shared__ unsigned sKind[GPB][G];
+    __shared__ float sSys[GPB][E_COUNT]; // odd stride: one system per thread without bank conflicts
+    __shared__ int sBody[GPB];
 
     const int g = threadIdx.x / G;
     const int lane = threadIdx.x % G;
     const int gid = blockIdx.x * GPB + g;
-    if (gid >= count)
-        return;
-    const unsigned gmask = (G == 32) ? 0xFFFFFFFFu : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
-    const int b = list[first + gid];
-
-    if (lane == 0)
-        initial_system(B, b, P.dt, sTerm[g][0]);
-    __syncwarp(gmask);
-    float acc[OWN];
-#pragma unroll
-    for (int k = 0; k < OWN; ++k)
+    if (gid < count)
     {
-        int e = lane + k * G;
-        acc[k] = e < E_COUNT ? sTerm[g][0][e] : 0.0f;
-    }
-    __syncwarp(gmask);
+        const unsigned gmask = (G == 32) ? 0xFFFFFFFFu : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
+        const int4 ent = entries[first + gid];
+        const int b = ent.x, r0 = ent.y, r1 = ent.z;
 
-    // the body's rows in force order, G at a time: lane j evaluates row base + j, then every
-    // lane adds the entries it owns row by row, so each sum keeps the reference's order
-    const int r0 = F.rowStart[b], r1 = F.rowStart[b + 1];
-    for (int base = r0; base < r1; base += G)
-    {
-        int r = base + lane;
-        if (r < r1)
-            sKind[g][lane] = listed_row_term(B, F, F.rows[r], P.alpha, sTerm[g][lane]);
-        __syncwarp(gmask);
-        int nrows = min(G, r1 - base);
-        for (int rr = 0; rr < nrows; ++rr)
+        float acc[OWN];
         {
-            unsigned kind = sKind[g][rr];
+            float t0[E_COUNT];
+            initial_system(B, b, P.dt, t0);
 #pragma unroll
-            for (int kk = 0; kk < OWN; ++kk)
+            for (int k = 0; k < OWN; ++k) // acc[k] = t0[lane + k G], with constant indices only
             {
-                int e = lane + kk * G;
-                if (e < E_COUNT && ((kind >> e) & 1u))
-                    acc[kk] = acc[kk] + sTerm[g][rr][e];
+                float v = 0.0f;
+#pragma unroll
+                for (int j = 0; j < G; ++j)
+                    if (j + k * G < E_COUNT && lane == j)
+                        v = t0[j + k * G];
+                acc[k] = v;
             }
         }
-        __syncwarp(gmask);
-    }
+
+        for (int base = r0; base < r1; base += G)
+        {
+            int r = base + lane;
+            if (r < r1)
+                sKind[g][lane] = listed_row_term(B, F, F.rows[r], b, P.alpha, sTerm[g][lane]);
+            __syncwarp(gmask);
+            int nrows = min(G, r1 - base);
+            for (int rr = 0; rr < nrows; ++rr)
+            {
+                unsigned kind = sKind[g][rr];
+                if (kind == KIND_FULL)
+                {
 #pragma unroll
-    for (int k = 0; k < OWN; ++k)
-    {
-        int e = lane + k * G;
-        if (e < E_COUNT)
-            sTerm[g][0][e] = acc[k];
+                    for (int kk = 0; kk < OWN; ++kk)
+                    {
+                        int e = lane + kk * G;
+                        if (e < E_COUNT)
+                            acc[kk] = acc[kk] + sTerm[g][rr][e];
+                    }
+                }
+                else
+                {
+#pragma unroll
+                    for (int kk = 0; kk < OWN; ++kk)
+                    {
+                        int e = lane + kk * G;
+                        if (e < E_COUNT && ((kind >> e) & 1u))
+                            acc[kk] = acc[kk] + sTerm[g][rr][e];
+                    }
+                }
+            }
+            __syncwarp(gmask);
+        }
+#pragma unroll
+        for (int k = 0; k < OWN; ++k)
+        {
+            int e = lane + k * G;
+            if (e < E_COUNT)
+                sSys[g][e] = acc[k];
+        }
+        if (lane == 0)
+            sBody[g] = b;
     }
-    __syncwarp(gmask);
-    if (lane == 0)
+    __syncthreads();
+    const int t = threadIdx.x;
+    if (t < GPB && blockIdx.x * GPB + t < count)
     {
+        const int b = sBody[t];
         float3 dxl, dxa;
-        ldl_solve27(sTerm[g][0], dxl, dxa);
+        ldl_solve27(sSys[t], dxl, dxa);
         float3 p = add(xyz(B.pos[b]), dxl);
         float4 q = qstep(B.quat[b], dxa);
         B.pos[b] = f4(p, 0.0f);

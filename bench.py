@@ -141,7 +141,11 @@ def run_cuda(args):
     w = World(scene, device=local, stream=stream.cuda_stream)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
     w.step(args.warmup)
-    tuned, variant_us = w.autotune(3)  # pick the primal variant on this scene's colouring
+    if args.primal_variant >= 0:  # fixed variant (profiling captures), no sweep
+        tuned, variant_us = args.primal_variant, []
+        w.set_primal_variant(tuned)
+    else:
+        tuned, variant_us = w.autotune(3)  # pick the primal variant on this scene's colouring
 
     # ---- timed region: device-resident step, L2 flushed before every step
     w.set_profiling(True)
@@ -474,6 +478,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-adjoint-check", action="store_true")
+    ap.add_argument("--primal-variant", type=int, default=-1,
+                    help="use this primal variant (index into World.primal_variants()) instead of autotuning")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

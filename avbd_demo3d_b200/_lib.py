@@ -108,6 +108,8 @@ SIGNATURES = {
     "avbd_num_joints": (ctypes.c_int, [ctypes.c_void_p, c_int_p]),
     "avbd_read_joints": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AvbdJointsOut)]),
     "avbd_next_seq": (ctypes.c_int, [ctypes.c_void_p, c_i64_p]),
+    "avbd_set_iteration_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    "avbd_iteration_mode": (ctypes.c_int, [ctypes.c_void_p, c_int_p]),
     "avbd_add_joints": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AvbdJoints)]),
     "avbd_remove_joints": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, c_i64_p]),
     "avbd_write_joints": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AvbdJoints)]),

@@ -44,6 +44,7 @@ struct ManBuf
 };
 
 constexpr int PRIMAL_BLOCK = 128;
+constexpr int ITER_G = 4, ITER_BLOCK = 1024; // iteration kernel: lanes per body, threads per block (one per SM)
 
 // Primal kernel variants: lanes per body (G) and the occupancy target given to the
 // compiler (resident blocks per SM; 1 = no register cap).
@@ -136,6 +137,10 @@ struct AvbdContext
     DArr<unsigned> colKeys, colKeysAlt;
     DArr<ColourControl> colourCtl;
     int colourBlocks = 148;   // co-resident blocks for the cooperative colouring launch
+    int iterationMode = AVBD_ITERATIONS_PERSISTENT;
+    int iterBlocks = 0;       // co-resident blocks of the iteration kernel (0: not launchable)
+    DArr<IterSync> iterSync;
+    int *hIterError = nullptr; // pinned: barrier expiry of the last iteration kernel
     int colourMode = 0;       // 0 greedy (list-index priority), 1 hashed priority
     int *hColourSummary = nullptr; // pinned: vertices, rounds, max colour, error
     int *hColourStarts = nullptr;  // pinned: 257 colour range starts
@@ -431,7 +436,7 @@ __global__ void k_colour_count(const ColourControl *ctl, int *unused, int *summa
 }
 
 __global__ void k_solve_list_all(const unsigned *keys, int n, int *list, int *colourStart, const ColourControl *ctl,
-                                 const int *rowStart, int4 *entries)
+                                 const int *rowStart, int4 *entries, const int *colour, int2 *rows)
 {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     int count = ctl->vertices;
@@ -441,7 +446,18 @@ __global__ void k_solve_list_all(const unsigned *keys, int n, int *list, int *co
     unsigned key = keys[k];
     int b = (int)(key & 0xFFFFFFu);
     list[k] = b;
-    entries[k] = make_int4(b, rowStart[b], rowStart[b + 1], 0);
+    int r0 = rowStart[b], r1 = rowStart[b + 1];
+    entries[k] = make_int4(b, r0, r1, 0);
+    // the contact rows whose dual update this body owns in a fused pass
+    int cb = colour[b];
+    for (int r = r0; r < r1; ++r)
+    {
+        int2 row = rows[r];
+        int p = row_partner(row);
+        bool own = p < 0 || colour[p] < 0 || cb < colour[p];
+        row.y = own ? (row.y | ROW_OWNS_DUAL) : (row.y & ~ROW_OWNS_DUAL);
+        rows[r] = row;
+    }
     int c = (int)(key >> 24);
     int prev = k > 0 ? (int)(keys[k - 1] >> 24) : -1;
     for (int x = prev + 1; x <= c; ++x)
@@ -883,12 +899,14 @@ int colour_bodies(AvbdContext *ctx)
     LAUNCHED();
     k_solve_list_all<<<grid_for(n, 256), 256, 0, ctx->stream>>>(dk.Current(), n, ctx->solveList.p, ctx->colourStart.p,
                                                                  ctx->colourCtl.p, ctx->rowStart.p,
-                                                                 ctx->solveEntry.p);
+                                                                 ctx->solveEntry.p, ctx->colour.p, ctx->rows.p);
     LAUNCHED();
     CU(cudaMemcpyAsync(ctx->hColourStarts, ctx->colourStart.p, sizeof(int) * 257, cudaMemcpyDeviceToHost,
                        ctx->stream));
     CU(cudaMemcpyAsync(ctx->hCounters, ctx->counters.p, sizeof(StepCounters), cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
+    if (*ctx->hIterError)
+        return fail(ctx, AVBD_ERR_STATE, "iteration kernel barrier wait expired");
     const int *sum = ctx->hColourSummary; // vertices, rounds, maxColour, error
     if (sum[3])
         return fail(ctx, AVBD_ERR_STATE, "colouring did not finish (barrier wait expired or round cap reached)");
@@ -910,8 +928,36 @@ int rec_iteration(AvbdContext *ctx, int it);
 void adjoint_release(AvbdContext *ctx);
 void adjoint_invalidate(AvbdContext *ctx); // the world changed: no backward for the last forward
 
+// Every iteration in one cooperative launch (k_iterations), the contacts' dual updates
+// fused into the next iteration's rows. Recording the differentiable step keeps the
+// per-colour launches, which it hooks between iterations.
+int iterate_persistent(AvbdContext *ctx)
+{
+    DevBodies B = dev_bodies(ctx);
+    DevForces F = dev_forces(ctx);
+    Params P = dev_params(ctx->params);
+    CHECK(reserve(ctx, ctx->iterSync, 1, false));
+    CU(cudaMemsetAsync(ctx->iterSync.p, 0, sizeof(IterSync), ctx->stream));
+    int nColours = ctx->nColours, iterations = ctx->params.iterations;
+    const int4 *entries = ctx->solveEntry.p;
+    const int *colourStart = ctx->colourStart.p;
+    IterSync *sync = ctx->iterSync.p;
+    void *args[] = {&B, &F, &P, &entries, &colourStart, &nColours, &iterations, &sync};
+    {
+        PhaseScope ps(ctx, AVBD_PHASE_PRIMAL);
+        CU(cudaLaunchCooperativeKernel((void *)k_iterations<ITER_G, ITER_BLOCK>, ctx->iterBlocks, ITER_BLOCK, args,
+                                       sizeof(PrimalShared<ITER_G, ITER_BLOCK>), ctx->stream));
+        LAUNCHED();
+    }
+    CU(cudaMemcpyAsync(ctx->hIterError, &ctx->iterSync.p->error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    return AVBD_OK;
+}
+
 int iterate(AvbdContext *ctx)
 {
+    if (ctx->iterationMode == AVBD_ITERATIONS_PERSISTENT && ctx->iterBlocks > 0 && !ctx->recording &&
+        ctx->params.iterations > 0 && ctx->nSolve > 0)
+        return iterate_persistent(ctx);
     DevBodies B = dev_bodies(ctx);
     DevForces F = dev_forces(ctx);
     Params P = dev_params(ctx->params);
@@ -1231,17 +1277,28 @@ int avbd_create(AvbdContext **out, int32_t device_ordinal, void *cuda_stream)
         cudaMallocHost((void **)&ctx->hColourSummary, sizeof(int) * 4) != cudaSuccess ||
         cudaMallocHost((void **)&ctx->hCapped, sizeof(int)) != cudaSuccess ||
         cudaMallocHost((void **)&ctx->hColourStarts, sizeof(int) * 257) != cudaSuccess ||
+        cudaMallocHost((void **)&ctx->hIterError, sizeof(int)) != cudaSuccess ||
         cudaEventCreate(&ctx->evStart) != cudaSuccess || cudaEventCreate(&ctx->evStop) != cudaSuccess)
     {
         avbd_destroy(ctx);
         return AVBD_ERR_CUDA;
     }
     memset(ctx->hCounters, 0, sizeof(StepCounters));
+    *ctx->hIterError = 0;
     {
         int sms = 0, perSm = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_ordinal);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_colour_all, 256, 0);
         ctx->colourBlocks = std::max(1, sms * std::max(1, perSm));
+        // the iteration kernel: one block of ITER_BLOCK threads per SM with its shared batch
+        int iterSm = 0;
+        size_t smem = sizeof(PrimalShared<ITER_G, ITER_BLOCK>);
+        if (cudaFuncSetAttribute((const void *)k_iterations<ITER_G, ITER_BLOCK>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&iterSm, k_iterations<ITER_G, ITER_BLOCK>, ITER_BLOCK,
+                                                          smem) == cudaSuccess)
+            ctx->iterBlocks = sms * iterSm;
+        cudaGetLastError(); // an unsupported configuration only leaves the per-colour launches
     }
     if (reserve(ctx, ctx->counters, 1, false) || reserve(ctx, ctx->bounds, 8, false) ||
         reserve(ctx, ctx->grid, 1, false))
@@ -1360,6 +1417,9 @@ void avbd_destroy(AvbdContext *ctx)
         cudaFreeHost(ctx->hCapped);
     if (ctx->hColourStarts)
         cudaFreeHost(ctx->hColourStarts);
+    if (ctx->hIterError)
+        cudaFreeHost(ctx->hIterError);
+    release(ctx->iterSync);
     if (ctx->stageDone)
         cudaEventDestroy(ctx->stageDone);
     if (ctx->evStart)
@@ -1639,6 +1699,8 @@ int avbd_synchronize(AvbdContext *ctx)
     if (!ctx)
         return AVBD_ERR_ARGUMENT;
     CU(cudaStreamSynchronize(ctx->stream));
+    if (*ctx->hIterError)
+        return fail(ctx, AVBD_ERR_STATE, "iteration kernel barrier wait expired");
     return AVBD_OK;
 }
 
@@ -2135,6 +2197,27 @@ int avbd_autotune(AvbdContext *ctx, int32_t repeats, int32_t *best_variant, floa
     ctx->primalVariant = best;
     if (best_variant)
         *best_variant = best;
+    return AVBD_OK;
+}
+
+int avbd_set_iteration_mode(AvbdContext *ctx, int32_t mode)
+{
+    if (!ctx)
+        return AVBD_ERR_ARGUMENT;
+    if (mode != AVBD_ITERATIONS_PER_COLOUR && mode != AVBD_ITERATIONS_PERSISTENT)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "unknown iteration mode %d", mode);
+    ctx->iterationMode = mode;
+    return AVBD_OK;
+}
+
+int avbd_iteration_mode(AvbdContext *ctx, int32_t *mode)
+{
+    if (!ctx || !mode)
+        return AVBD_ERR_ARGUMENT;
+    // the mode the next step runs in (per-colour launches where the device cannot hold the
+    // persistent kernel's blocks)
+    *mode = ctx->iterationMode == AVBD_ITERATIONS_PERSISTENT && ctx->iterBlocks > 0 ? AVBD_ITERATIONS_PERSISTENT
+                                                                                    : AVBD_ITERATIONS_PER_COLOUR;
     return AVBD_OK;
 }
 

@@ -1163,9 +1163,23 @@ struct ContactRec
     bool stick;
 };
 
+// Loads of state that other blocks of one persistent launch write between its grid
+// barriers (poses, pose differences, contact and joint multipliers and penalties) go to L2
+// (ld.global.cg) there, so no block reads a stale L1 line after a barrier. Kernels that
+// end before the state changes again use plain loads.
+template <bool COH>
+AVBD_DEV float4 ld_state(const float4 *p)
+{
+    if constexpr (COH)
+        return __ldcg(p);
+    else
+        return *p;
+}
+
+template <bool COH = false>
 AVBD_DEV ContactRec load_contact(const float4 *c)
 {
-    float4 k0 = c[0], k1 = c[1], k2 = c[2], k3 = c[3];
+    float4 k0 = c[0], k1 = c[1], k2 = ld_state<COH>(c + 2), k3 = ld_state<COH>(c + 3);
     ContactRec r;
     r.rA = f3(k0.x, k0.y, k0.z);
     r.rB = f3(k0.w, k1.x, k1.y);
@@ -1658,12 +1672,13 @@ AVBD_DEV Motion motion_of(const Pose &s)
     return m;
 }
 
+template <bool COH = false>
 AVBD_DEV Motion load_motion(const DevBodies &B, int b)
 {
     Motion m;
-    m.q = B.quat[b];
-    m.dLin = xyz(B.dqLin[b]);
-    m.dAng = xyz(B.dqAng[b]);
+    m.q = ld_state<COH>(B.quat + b);
+    m.dLin = xyz(ld_state<COH>(B.dqLin + b));
+    m.dAng = xyz(ld_state<COH>(B.dqAng + b));
     return m;
 }
 
@@ -1718,6 +1733,44 @@ struct ContactEval
     float fs, bounds;
 };
 
+// F from C with the contact's penalty and multiplier: normal clamp and friction cone
+// (manifold.cpp:199-212).
+AVBD_DEV void contact_force(ContactEval &e, const ContactRec &c, float friction)
+{
+    M3 K = diag(c.pen.x, c.pen.y, c.pen.z);
+    float3 F = add(mv(K, e.C), c.lam);
+    F.x = rmin(F.x, 0.0f);
+    e.bounds = fabsf(F.x) * friction;
+    e.fs = sqrtf(F.y * F.y + F.z * F.z);
+    if (e.fs > e.bounds && e.fs > 0)
+    {
+        F.y *= e.bounds / e.fs;
+        F.z *= e.bounds / e.fs;
+    }
+    e.F = F;
+}
+
+// Manifold::updateDual for one contact (manifold.cpp:231-280), on the evaluation at the
+// current poses: lambda takes F, the penalties ramp, the stick flag follows.
+AVBD_DEV void contact_dual(ContactRec &c, const ContactEval &e, float betaLin)
+{
+    c.lam = e.F;
+    if (e.F.x < 0)
+        c.pen.x = rmin(c.pen.x + betaLin * fabsf(e.C.x), PENALTY_MAX);
+    if (e.fs <= e.bounds)
+    {
+        c.pen.y = rmin(c.pen.y + betaLin * fabsf(e.C.y), PENALTY_MAX);
+        c.pen.z = rmin(c.pen.z + betaLin * fabsf(e.C.z), PENALTY_MAX);
+        c.stick = sqrtf(e.C.y * e.C.y + e.C.z * e.C.z) < STICK_THRESH;
+    }
+}
+
+AVBD_DEV void store_contact_state(float4 *cp, const ContactRec &c)
+{
+    cp[2] = make_float4(c.C0.z, c.pen.x, c.pen.y, c.pen.z);
+    cp[3] = make_float4(c.lam.x, c.lam.y, c.lam.z, __uint_as_float((unsigned)c.key | (c.stick ? 0x80000000u : 0u)));
+}
+
 AVBD_DEV ContactEval eval_contact(const Motion &A, const Motion &Bp, const M3 &basis, float friction,
                                   const ContactRec &c, float alpha)
 {
@@ -1732,19 +1785,9 @@ AVBD_DEV ContactEval eval_contact(const Motion &A, const Motion &Bp, const M3 &b
     e.jBLin = mneg(basis);
     e.jAAng = rows(cross(rAW, e.jALin.r0), cross(rAW, e.jALin.r1), cross(rAW, e.jALin.r2));
     e.jBAng = rows(cross(rBW, e.jBLin.r0), cross(rBW, e.jBLin.r1), cross(rBW, e.jBLin.r2));
-    M3 K = diag(c.pen.x, c.pen.y, c.pen.z);
     e.C = add(add(add(add(mul(c.C0, 1.0f - alpha), mv(e.jALin, dqALin)), mv(e.jBLin, dqBLin)), mv(e.jAAng, dqAAng)),
               mv(e.jBAng, dqBAng));
-    float3 F = add(mv(K, e.C), c.lam);
-    F.x = rmin(F.x, 0.0f);
-    e.bounds = fabsf(F.x) * friction;
-    e.fs = sqrtf(F.y * F.y + F.z * F.z);
-    if (e.fs > e.bounds && e.fs > 0)
-    {
-        F.y *= e.bounds / e.fs;
-        F.z *= e.bounds / e.fs;
-    }
-    e.F = F;
+    contact_force(e, c, friction);
     return e;
 }
 
@@ -1781,27 +1824,28 @@ AVBD_DEV M3 gs_ball_socket(int k, float3 v)
 
 // Joint rows (joint.cpp:56-123): part 0 = linear stamp, 1 = diagonalised geometric
 // stiffness added to lhsAng, 2 = angular stamp.
+template <bool COH = false>
 AVBD_DEV unsigned joint_term(const DevBodies &B, const DevForces &F, unsigned j, int part, bool isA, float alpha,
                              float *t)
 {
     const float4 *d = F.joint + 8 * (size_t)j;
     int2 ab = F.jointAB[j];
     float4 d0 = d[0], d1 = d[1];
-    float3 pB = xyz(B.pos[ab.y]);
-    float4 qB = B.quat[ab.y];
+    float3 pB = xyz(ld_state<COH>(B.pos + ab.y));
+    float4 qB = ld_state<COH>(B.quat + ab.y);
     const M3 I = rows(f3(1, 0, 0), f3(0, 1, 0), f3(0, 0, 1));
     const M3 NI = rows(f3(-1, 0, 0), f3(0, -1, 0), f3(0, 0, -1));
     if (part < 2)
     {
         float3 rA = xyz(d0), rB = xyz(d1);
-        float3 penLin = xyz(d[4]);
-        float3 rAW = ab.x >= 0 ? rotate(B.quat[ab.x], rA) : f3(0, 0, 0);
+        float3 penLin = xyz(ld_state<COH>(d + 4));
+        float3 rAW = ab.x >= 0 ? rotate(ld_state<COH>(B.quat + ab.x), rA) : f3(0, 0, 0);
         float3 rBW = rotate(qB, rB);
         M3 K = diag(penLin.x, penLin.y, penLin.z);
-        float3 C = sub(ab.x >= 0 ? add(xyz(B.pos[ab.x]), rAW) : rA, add(pB, rBW));
+        float3 C = sub(ab.x >= 0 ? add(xyz(ld_state<COH>(B.pos + ab.x)), rAW) : rA, add(pB, rBW));
         if (isinf(d0.w))
             C = sub(C, mul(xyz(d[2]), alpha));
-        float3 Fv = add(mv(K, C), xyz(d[6]));
+        float3 Fv = add(mv(K, C), xyz(ld_state<COH>(d + 6)));
         if (part == 0)
         {
             M3 jLin = isA ? I : NI;
@@ -1824,14 +1868,14 @@ AVBD_DEV unsigned joint_term(const DevBodies &B, const DevForces &F, unsigned j,
         t[E_LA22] = D.r2.z;
         return KIND_LHSANG;
     }
-    float3 penAng = xyz(d[5]);
+    float3 penAng = xyz(ld_state<COH>(d + 5));
     float torqueArm = d[3].w;
     M3 K = diag(penAng.x, penAng.y, penAng.z);
-    float4 qa = ab.x >= 0 ? B.quat[ab.x] : make_float4(0, 0, 0, 1);
+    float4 qa = ab.x >= 0 ? ld_state<COH>(B.quat + ab.x) : make_float4(0, 0, 0, 1);
     float3 C = mul(qdiff(qa, qB), torqueArm);
     if (isinf(d1.w))
         C = sub(C, mul(xyz(d[3]), alpha));
-    float3 Fv = add(mv(K, C), xyz(d[7]));
+    float3 Fv = add(mv(K, C), xyz(ld_state<COH>(d + 7)));
     M3 jAng = mscale(isA ? I : NI, torqueArm);
     M3 LA = mm(mm(trans(jAng), K), jAng);
     float3 RA = mv(trans(jAng), Fv);
@@ -1848,6 +1892,7 @@ AVBD_DEV unsigned joint_term(const DevBodies &B, const DevForces &F, unsigned j,
 }
 
 // Spring row (spring.cpp:27-69)
+template <bool COH = false>
 AVBD_DEV unsigned spring_term(const DevBodies &B, const DevForces &F, unsigned s, bool isA, float *t)
 {
     const float4 *d = F.spring + 2 * (size_t)s;
@@ -1855,9 +1900,9 @@ AVBD_DEV unsigned spring_term(const DevBodies &B, const DevForces &F, unsigned s
     float4 d0 = d[0], d1 = d[1];
     float3 rA = xyz(d0), rB = xyz(d1);
     float rest = d0.w, stiffness = d1.w;
-    float4 qA = B.quat[ab.x], qB = B.quat[ab.y];
-    float3 pA = xform(xyz(B.pos[ab.x]), qA, rA);
-    float3 pB = xform(xyz(B.pos[ab.y]), qB, rB);
+    float4 qA = ld_state<COH>(B.quat + ab.x), qB = ld_state<COH>(B.quat + ab.y);
+    float3 pA = xform(xyz(ld_state<COH>(B.pos + ab.x)), qA, rA);
+    float3 pB = xform(xyz(ld_state<COH>(B.pos + ab.y)), qB, rB);
     float3 dd = sub(pA, pB);
     float dLen = len(dd);
     if (dLen <= 1.0e-6f)
@@ -1955,8 +2000,11 @@ AVBD_DEV int entry_partner(const DevForces &F, unsigned e)
 
 // Row entries carry the partner body next to the row index (bodies < 2^24, rows < 8), so
 // a contact row's partner pose is fetched together with its contact data.
+// Bit 30 marks the rows whose contact this body updates in a fused dual pass: the body
+// with the lower colour, or the only dynamic one (set after colouring).
+constexpr int ROW_OWNS_DUAL = 1 << 30;
 AVBD_DEV int row_sub(int2 row) { return row.y & 7; }
-AVBD_DEV int row_partner(int2 row) { return (row.y >> 3) - 1; }
+AVBD_DEV int row_partner(int2 row) { return ((row.y & (ROW_OWNS_DUAL - 1)) >> 3) - 1; }
 
 __global__ void k_entry_fill(DevForces F, const int *entryRow, const int *count, int total)
 {
@@ -1975,17 +2023,27 @@ __global__ void k_entry_fill(DevForces F, const int *entryRow, const int *count,
 
 // Contact row of body `self` against its partner (Manifold::updatePrimal,
 // manifold.cpp:183-228); the partner comes from the row entry.
+template <bool COH = false>
 AVBD_DEV unsigned contact_term_self(const DevBodies &B, const DevForces &F, unsigned m, int ci, bool isA, int self,
-                                    int partner, float alpha, float *t)
+                                    int partner, bool dual, const Params &P, float *t)
 {
     const float4 *bs = F.man.basis + 3 * (size_t)m;
     float4 b0 = bs[0];
     M3 basis = rows(xyz(b0), xyz(bs[1]), xyz(bs[2]));
-    ContactRec c = load_contact(F.man.contact + (size_t)m * 32 + 4 * ci);
-    Motion A = load_motion(B, isA ? self : partner), Bm = load_motion(B, isA ? partner : self);
-    ContactEval e = eval_contact(A, Bm, basis, b0.w, c, alpha);
-    const M3 &jLin = isA ? e.jALin : e.jBLin;
-    const M3 &jAng = isA ? e.jAAng : e.jBAng;
+    float4 *cp = F.man.contact + (size_t)m * 32 + 4 * ci;
+    ContactRec c = load_contact<COH>(cp);
+    Motion A = load_motion<COH>(B, isA ? self : partner), Bm = load_motion<COH>(B, isA ? partner : self);
+    ContactEval e = eval_contact(A, Bm, basis, b0.w, c, P.alpha);
+    const M3 jLin = isA ? e.jALin : e.jBLin; // this body's rows, taken before the dual update
+    const M3 jAng = isA ? e.jAAng : e.jBAng;
+    if (dual)
+    {
+        // the previous iteration's dual update of this contact, at the same poses, then
+        // this row's force from the same C with the updated penalty and multiplier
+        contact_dual(c, e, P.betaLin);
+        store_contact_state(cp, c);
+        contact_force(e, c, b0.w);
+    }
     M3 jLinT = trans(jLin), jAngT = trans(jAng);
     M3 jAngTk = times_diag(jAngT, c.pen);
     store_terms(t, mm(times_diag(jLinT, c.pen), jLin), mm(jAngTk, jAng), mm(jAngTk, jLin), mv(jLinT, e.F),
@@ -1994,8 +2052,11 @@ AVBD_DEV unsigned contact_term_self(const DevBodies &B, const DevForces &F, unsi
 }
 
 // One listed row's contribution (Manifold/Joint/Spring::updatePrimal).
-AVBD_DEV unsigned listed_row_term(const DevBodies &B, const DevForces &F, int2 row, int self, float alpha,
-                                  float *t)
+// `fusedDual`: this launch also performs the previous iteration's contact dual updates,
+// each by the row of the body that owns it.
+template <bool COH = false>
+AVBD_DEV unsigned listed_row_term(const DevBodies &B, const DevForces &F, int2 row, int self, bool fusedDual,
+                                  const Params &P, float *t)
 {
     unsigned e = (unsigned)row.x;
     unsigned i = adj_index(e);
@@ -2004,21 +2065,23 @@ AVBD_DEV unsigned listed_row_term(const DevBodies &B, const DevForces &F, int2 r
     switch (adj_type(e))
     {
     case ADJ_MANIFOLD:
-        return contact_term_self(B, F, i, sub, isA, self, row_partner(row), alpha, t);
+        return contact_term_self<COH>(B, F, i, sub, isA, self, row_partner(row),
+                                      fusedDual && (row.y & ROW_OWNS_DUAL) != 0, P, t);
     case ADJ_JOINT:
     {
         const float4 *d = F.joint + 8 * (size_t)i;
-        bool on = sub < 2 ? lensq(xyz(d[4])) > 0 : lensq(xyz(d[5])) > 0;
-        return on ? joint_term(B, F, i, sub, isA, alpha, t) : KIND_NONE;
+        bool on = sub < 2 ? lensq(xyz(ld_state<COH>(d + 4))) > 0 : lensq(xyz(ld_state<COH>(d + 5))) > 0;
+        return on ? joint_term<COH>(B, F, i, sub, isA, P.alpha, t) : KIND_NONE;
     }
     case ADJ_SPRING:
-        return spring_term(B, F, i, isA, t);
+        return spring_term<COH>(B, F, i, isA, t);
     default:
         return KIND_NONE;
     }
 }
 
 // Initial system M/dt^2 (solver.cpp:1189-1198) as 27 entries
+template <bool COH = false>
 AVBD_DEV void initial_system(const DevBodies &B, int b, float dt, float *t)
 {
     float4 mm4 = B.massMoment[b];
@@ -2028,43 +2091,49 @@ AVBD_DEV void initial_system(const DevBodies &B, int b, float dt, float *t)
     M3 lhsLin = mdivs(MLin, dt2);
     M3 lhsAng = mdivs(MAng, dt2);
     M3 lhsCross = diag(0, 0, 0);
-    float3 rhsLin = mv(mdivs(MLin, dt2), sub(xyz(B.pos[b]), xyz(B.inertLin[b])));
-    float3 rhsAng = mv(mdivs(MAng, dt2), qdiff(B.quat[b], B.inertAng[b]));
+    float3 rhsLin = mv(mdivs(MLin, dt2), sub(xyz(ld_state<COH>(B.pos + b)), xyz(B.inertLin[b])));
+    float3 rhsAng = mv(mdivs(MAng, dt2), qdiff(ld_state<COH>(B.quat + b), B.inertAng[b]));
     store_terms(t, lhsLin, lhsAng, lhsCross, rhsLin, rhsAng);
 }
 
-// One primal solve per body of a colour (solver.cpp:1186-1233). Rows: G lanes per body.
-// The solve entries carry the body and its row range; every lane of a group builds the
-// initial system M/dt^2 and keeps the entries it owns, then the rows are evaluated G at a
-// time (lane j evaluates row base + j into shared memory) and every lane adds its entries
-// row by row, so each sum keeps the reference's order. Solve: the block's accumulated
-// systems go to shared memory and one thread per body factors its 6x6 system and moves
-// the body, so the factorisation runs with every lane of its warp busy.
-template <int G, int BLOCK, int MINB>
-__global__ void __launch_bounds__(BLOCK, MINB) k_primal(DevBodies B, DevForces F, Params P, const int4 *entries,
-                                                        int first, int count)
+// Shared memory of one primal batch: GPB bodies, G lanes each.
+template <int G, int BLOCK>
+struct PrimalShared
+{
+    static constexpr int GPB = BLOCK / G;
+    float term[GPB][G][E_COUNT];
+    float sys[GPB][E_COUNT]; // odd stride: one system per thread without bank conflicts
+    unsigned kind[GPB][G];
+    int body[GPB];
+};
+
+// One primal solve per body of a batch of one colour (solver.cpp:1186-1233). Rows: G lanes
+// per body. The solve entries carry the body and its row range; every lane of a group
+// builds the initial system M/dt^2 and keeps the entries it owns, then the rows are
+// evaluated G at a time (lane j evaluates row base + j into shared memory) and every lane
+// adds its entries row by row, so each sum keeps the reference's order. Solve: the batch's
+// accumulated systems go to shared memory and one thread per body factors its 6x6 system
+// and moves the body, so the factorisation runs with every lane of its warp busy. Every
+// thread of the block calls this (it holds a block barrier).
+template <int G, int BLOCK, bool COH>
+AVBD_DEV void primal_batch(const DevBodies &B, const DevForces &F, const Params &P, const int4 *entries, int count,
+                           bool fusedDual, PrimalShared<G, BLOCK> &sh)
 {
     static_assert(BLOCK % G == 0 && 32 % G == 0, "group size");
     constexpr int GPB = BLOCK / G;
     constexpr int OWN = (E_COUNT + G - 1) / G;
-    __shared__ float sTerm[GPB][G][E_COUNT];
-    __shared__ unsigned sKind[GPB][G];
-    __shared__ float sSys[GPB][E_COUNT]; // odd stride: one system per thread without bank conflicts
-    __shared__ int sBody[GPB];
-
     const int g = threadIdx.x / G;
     const int lane = threadIdx.x % G;
-    const int gid = blockIdx.x * GPB + g;
-    if (gid < count)
+    if (g < count)
     {
         const unsigned gmask = (G == 32) ? 0xFFFFFFFFu : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
-        const int4 ent = entries[first + gid];
+        const int4 ent = entries[g];
         const int b = ent.x, r0 = ent.y, r1 = ent.z;
 
         float acc[OWN];
         {
             float t0[E_COUNT];
-            initial_system(B, b, P.dt, t0);
+            initial_system<COH>(B, b, P.dt, t0);
 #pragma unroll
             for (int k = 0; k < OWN; ++k) // acc[k] = t0[lane + k G], with constant indices only
             {
@@ -2081,12 +2150,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_primal(DevBodies B, DevForces F
         {
             int r = base + lane;
             if (r < r1)
-                sKind[g][lane] = listed_row_term(B, F, F.rows[r], b, P.alpha, sTerm[g][lane]);
+                sh.kind[g][lane] = listed_row_term<COH>(B, F, F.rows[r], b, fusedDual, P, sh.term[g][lane]);
             __syncwarp(gmask);
             int nrows = min(G, r1 - base);
             for (int rr = 0; rr < nrows; ++rr)
             {
-                unsigned kind = sKind[g][rr];
+                unsigned kind = sh.kind[g][rr];
                 if (kind == KIND_FULL)
                 {
 #pragma unroll
@@ -2094,7 +2163,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_primal(DevBodies B, DevForces F
                     {
                         int e = lane + kk * G;
                         if (e < E_COUNT)
-                            acc[kk] = acc[kk] + sTerm[g][rr][e];
+                            acc[kk] = acc[kk] + sh.term[g][rr][e];
                     }
                 }
                 else
@@ -2104,7 +2173,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_primal(DevBodies B, DevForces F
                     {
                         int e = lane + kk * G;
                         if (e < E_COUNT && ((kind >> e) & 1u))
-                            acc[kk] = acc[kk] + sTerm[g][rr][e];
+                            acc[kk] = acc[kk] + sh.term[g][rr][e];
                     }
                 }
             }
@@ -2115,77 +2184,88 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_primal(DevBodies B, DevForces F
         {
             int e = lane + k * G;
             if (e < E_COUNT)
-                sSys[g][e] = acc[k];
+                sh.sys[g][e] = acc[k];
         }
         if (lane == 0)
-            sBody[g] = b;
+            sh.body[g] = b;
     }
     __syncthreads();
     const int t = threadIdx.x;
-    if (t < GPB && blockIdx.x * GPB + t < count)
+    if (t < GPB && t < count)
     {
-        const int b = sBody[t];
+        const int b = sh.body[t];
+        const float4 p0 = ld_state<COH>(B.pos + b), q0 = ld_state<COH>(B.quat + b); // in flight during the solve
+        const float4 i0 = B.initLin[b], a0 = B.initAng[b];
         float3 dxl, dxa;
-        ldl_solve27(sSys[t], dxl, dxa);
-        float3 p = add(xyz(B.pos[b]), dxl);
-        float4 q = qstep(B.quat[b], dxa);
+        ldl_solve27(sh.sys[t], dxl, dxa);
+        float3 p = add(xyz(p0), dxl);
+        float4 q = qstep(q0, dxa);
         B.pos[b] = f4(p, 0.0f);
         B.quat[b] = q;
-        B.dqLin[b] = f4(sub(p, xyz(B.initLin[b])), 0.0f);
-        B.dqAng[b] = f4(qdiff(q, B.initAng[b]), 0.0f);
+        B.dqLin[b] = f4(sub(p, xyz(i0)), 0.0f);
+        B.dqAng[b] = f4(qdiff(q, a0), 0.0f);
     }
+}
+
+// One launch per colour: block k takes the colour's bodies [k GPB, (k+1) GPB).
+template <int G, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_primal(DevBodies B, DevForces F, Params P, const int4 *entries,
+                                                        int first, int count)
+{
+    __shared__ PrimalShared<G, BLOCK> sh;
+    constexpr int GPB = BLOCK / G;
+    const int base = blockIdx.x * GPB;
+    primal_batch<G, BLOCK, false>(B, F, P, entries + first + base, min(GPB, count - base), false, sh);
 }
 
 // ---------------------------------------------------------------------------
 // Dual (solver.cpp:1244-1271)
 // ---------------------------------------------------------------------------
 
-// Manifold::updateDual per contact slot (manifold.cpp:231-280)
-__global__ void k_dual_contacts(DevBodies B, DevManifolds M, int nMan, Params P)
+// Manifold::updateDual per contact slot (manifold.cpp:231-280); t = manifold * 8 + slot.
+template <bool COH>
+AVBD_DEV void dual_contact_slot(const DevBodies &B, const DevManifolds &M, long long t, const Params &P)
 {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    int m = t >> 3, ci = t & 7;
-    if (m >= nMan || ci >= M.n[m])
+    int m = (int)(t >> 3), ci = (int)(t & 7);
+    if (ci >= M.n[m])
         return;
     int2 ab = M.ab[m];
-    Motion A = load_motion(B, ab.x), Bp = load_motion(B, ab.y);
+    Motion A = load_motion<COH>(B, ab.x), Bp = load_motion<COH>(B, ab.y);
     const float4 *bs = M.basis + 3 * (size_t)m;
     float4 b0 = bs[0];
     M3 basis = rows(xyz(b0), xyz(bs[1]), xyz(bs[2]));
     float4 *cp = M.contact + (size_t)m * 32 + 4 * ci;
-    ContactRec c = load_contact(cp);
+    ContactRec c = load_contact<COH>(cp);
     ContactEval e = eval_contact(A, Bp, basis, b0.w, c, P.alpha);
-    c.lam = e.F;
-    if (e.F.x < 0)
-        c.pen.x = rmin(c.pen.x + P.betaLin * fabsf(e.C.x), PENALTY_MAX);
-    if (e.fs <= e.bounds)
-    {
-        c.pen.y = rmin(c.pen.y + P.betaLin * fabsf(e.C.y), PENALTY_MAX);
-        c.pen.z = rmin(c.pen.z + P.betaLin * fabsf(e.C.z), PENALTY_MAX);
-        c.stick = sqrtf(e.C.y * e.C.y + e.C.z * e.C.z) < STICK_THRESH;
-    }
-    cp[2] = make_float4(c.C0.z, c.pen.x, c.pen.y, c.pen.z);
-    cp[3] = make_float4(c.lam.x, c.lam.y, c.lam.z, __uint_as_float((unsigned)c.key | (c.stick ? 0x80000000u : 0u)));
+    contact_dual(c, e, P.betaLin);
+    store_contact_state(cp, c);
+}
+
+__global__ void k_dual_contacts(DevBodies B, DevManifolds M, int nMan, Params P)
+{
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < 8ll * nMan)
+        dual_contact_slot<false>(B, M, t, P);
 }
 
 // Joint::updateDual with fracture (joint.cpp:125-182)
-__global__ void k_dual_joints(DevBodies B, DevForces F, Params P)
+template <bool COH>
+AVBD_DEV void dual_joint(const DevBodies &B, const DevForces &F, int j, const Params &P)
 {
-    int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= F.nJoint)
-        return;
     float4 *d = F.joint + 8 * (size_t)j;
     int2 ab = F.jointAB[j];
     float4 d0 = d[0], d1 = d[1];
-    float3 penLin = xyz(d[4]), penAng = xyz(d[5]);
-    float3 lamLin = xyz(d[6]), lamAng = xyz(d[7]);
-    float brokenFlag = d[4].w;
-    float3 pB = xyz(B.pos[ab.y]);
-    float4 qB = B.quat[ab.y];
+    float4 d4 = ld_state<COH>(d + 4);
+    float3 penLin = xyz(d4), penAng = xyz(ld_state<COH>(d + 5));
+    float3 lamLin = xyz(ld_state<COH>(d + 6)), lamAng = xyz(ld_state<COH>(d + 7));
+    float brokenFlag = d4.w;
+    float3 pB = xyz(ld_state<COH>(B.pos + ab.y));
+    float4 qB = ld_state<COH>(B.quat + ab.y);
     if (lensq(penLin) > 0)
     {
         M3 K = diag(penLin.x, penLin.y, penLin.z);
-        float3 pa = ab.x >= 0 ? xform(xyz(B.pos[ab.x]), B.quat[ab.x], xyz(d0)) : xyz(d0);
+        float3 pa = ab.x >= 0 ? xform(xyz(ld_state<COH>(B.pos + ab.x)), ld_state<COH>(B.quat + ab.x), xyz(d0))
+                              : xyz(d0);
         float3 C = sub(pa, xform(pB, qB, xyz(d1)));
         if (isinf(d0.w))
         {
@@ -2197,7 +2277,7 @@ __global__ void k_dual_joints(DevBodies B, DevForces F, Params P)
     if (lensq(penAng) > 0)
     {
         M3 K = diag(penAng.x, penAng.y, penAng.z);
-        float4 qa = ab.x >= 0 ? B.quat[ab.x] : make_float4(0, 0, 0, 1);
+        float4 qa = ab.x >= 0 ? ld_state<COH>(B.quat + ab.x) : make_float4(0, 0, 0, 1);
         float3 C = mul(qdiff(qa, qB), d[3].w);
         if (isinf(d1.w))
         {
@@ -2219,6 +2299,113 @@ __global__ void k_dual_joints(DevBodies B, DevForces F, Params P)
     d[5] = f4(penAng, 0.0f);
     d[6] = f4(lamLin, 0.0f);
     d[7] = f4(lamAng, 0.0f);
+}
+
+__global__ void k_dual_joints(DevBodies B, DevForces F, Params P)
+{
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < F.nJoint)
+        dual_joint<false>(B, F, j, P);
+}
+
+// ---------------------------------------------------------------------------
+// All iterations of a step in one cooperative launch
+// ---------------------------------------------------------------------------
+
+// Bounded grid-wide barrier of the iteration kernel: on expiry the kernel records an
+// error and every block leaves.
+constexpr unsigned ITER_SPIN_LIMIT = 1u << 22;
+
+struct IterSync
+{
+    unsigned arrive;
+    unsigned generation;
+    int error;
+    int pad;
+};
+
+AVBD_DEV bool iter_barrier(IterSync *s)
+{
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        volatile unsigned *gen = &s->generation;
+        unsigned g = *gen;
+        __threadfence();
+        if (atomicAdd(&s->arrive, 1u) == gridDim.x - 1)
+        {
+            s->arrive = 0;
+            __threadfence();
+            atomicAdd(&s->generation, 1u);
+            ok = 1;
+        }
+        else
+        {
+            unsigned spins = 0;
+            while (*gen == g && ++spins < ITER_SPIN_LIMIT)
+                if (spins > 256)
+                    __nanosleep(32);
+            ok = spins < ITER_SPIN_LIMIT;
+            if (!ok)
+                atomicExch(&s->error, 1);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok && ((volatile int *)&s->error)[0] == 0;
+}
+
+// Solver::iteratePrimalDualCpu (solver.cpp:1177-1271) for every iteration of a step, one
+// block per SM, all state read at L2 between barriers. Per iteration: each colour's bodies
+// in batches of GPB (a barrier after each colour), then the joints' dual update. The
+// contacts' dual update of iteration k is done in iteration k + 1 by the row of the body
+// that owns the contact, before that row uses it: the owner is the contact's body with the
+// lower colour (or its only dynamic body), which has not moved yet in iteration k + 1, and
+// neither has the other body, so both poses are those the dual sweep of iteration k reads
+// and every contact's update is the same. The last iteration's contact updates close the
+// launch.
+template <int G, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces F, Params P, const int4 *entries,
+                                                         const int *colourStart, int nColours, int iterations,
+                                                         IterSync *sync)
+{
+    extern __shared__ __align__(16) unsigned char smemRaw[];
+    PrimalShared<G, BLOCK> &sh = *reinterpret_cast<PrimalShared<G, BLOCK> *>(smemRaw);
+    constexpr int GPB = BLOCK / G;
+    const long long stride = (long long)gridDim.x * BLOCK;
+    const long long tid = (long long)blockIdx.x * BLOCK + threadIdx.x;
+    for (int it = 0; it < iterations; ++it)
+    {
+        for (int c = 0; c < nColours; ++c)
+        {
+            const int first = colourStart[c], cnt = colourStart[c + 1] - first;
+            for (int base = blockIdx.x * GPB; base < cnt; base += gridDim.x * GPB)
+            {
+                primal_batch<G, BLOCK, true>(B, F, P, entries + first + base, min(GPB, cnt - base), it > 0, sh);
+                __syncthreads(); // the batch's solve threads are done with the shared systems
+            }
+            if (!iter_barrier(sync))
+                return;
+        }
+        if (F.nJoint > 0)
+        {
+            for (long long j = tid; j < F.nJoint; j += stride)
+                dual_joint<true>(B, F, (int)j, P);
+            if (!iter_barrier(sync))
+                return;
+        }
+    }
+    // Contacts between two static bodies have no owning row: nothing moves them, so their
+    // update of every iteration runs here, one after the other on the same poses.
+    if (iterations > 0)
+        for (long long t = tid; t < 8ll * F.nMan; t += stride)
+        {
+            int2 ab = F.man.ab[t >> 3];
+            bool orphan = B.massMoment[ab.x].x <= 0 && B.massMoment[ab.y].x <= 0;
+            for (int r = orphan ? iterations : 1; r > 0; --r)
+                dual_contact_slot<true>(B, F.man, t, P);
+        }
 }
 
 } // namespace avbd

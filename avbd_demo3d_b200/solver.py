@@ -346,6 +346,16 @@ class World:
                     "avbd_autotune")
         return best.value, us
 
+    def set_iteration_mode(self, mode: int):
+        """0 = one launch per colour and iteration plus the dual sweep, 1 = every iteration in
+        one cooperative launch (default). Both give the same bits."""
+        self._check(self.lib.avbd_set_iteration_mode(self.h, mode), "avbd_set_iteration_mode")
+
+    def iteration_mode(self) -> int:
+        m = ctypes.c_int32()
+        self._check(self.lib.avbd_iteration_mode(self.h, ctypes.byref(m)), "avbd_iteration_mode")
+        return m.value
+
     def set_colouring(self, mode: int):
         """0 = greedy colouring in list order (default), 1 = hashed priorities."""
         self._check(self.lib.avbd_set_colouring(self.h, mode), "avbd_set_colouring")

@@ -49,9 +49,10 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic_per_launch():
-    """dram bytes per primal launch from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", "primal_stacks65k_ncu.md")
+def ncu_traffic_per_launch(kernel: str = "k_primal"):
+    """dram bytes per launch of `kernel` from its committed ncu summary, if present."""
+    name = {"k_primal": "primal_stacks65k_ncu.md", "k_iterations": "iterations_stacks65k_ncu.md"}[kernel]
+    path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -141,6 +142,7 @@ def run_cuda(args):
     w = World(scene, device=local, stream=stream.cuda_stream)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
     w.step(args.warmup)
+    w.set_iteration_mode(args.iteration_mode)
     if args.primal_variant >= 0:  # fixed variant (profiling captures), no sweep
         tuned, variant_us = args.primal_variant, []
         w.set_primal_variant(tuned)
@@ -174,19 +176,27 @@ def run_cuda(args):
     bodies = scene.n_bodies - 1  # the static ground is not counted
     value = world_size * bodies * args.steps / (max_ms / 1e3)
 
-    # ---- roofline of the dominant kernel (the coloured primal sweep)
+    # ---- roofline of the dominant kernel: the iteration kernel (one launch per step) or, in
+    # the per-colour form, the coloured primal sweep
     per_iter, counts = algorithmic_primal_bytes(w)
     iters = scene.params.iterations
+    persistent = w.iteration_mode() == 1
+    if persistent:  # each contact's dual update also writes its multiplier and penalties (32 B)
+        per_iter += 32 * counts["contacts"]
     primal_ms = prof["primal_ms"]
     primal_launches = max(1, prof["primal_spans"])
     achieved = per_iter * iters * prof["steps"] / (primal_ms / 1e3) / 1e9 if primal_ms > 0 else None
     peak, peak_kind = measured_peak()
-    traffic = ncu_traffic_per_launch()
-    roofline = {"kernel": "k_primal (coloured primal sweep)", "bound": "hbm", "achieved": achieved, "peak": peak,
+    traffic = ncu_traffic_per_launch("k_iterations" if persistent else "k_primal")
+    kernel = ("k_iterations (every iteration of a step: coloured primal sweeps, contact dual updates fused into "
+              "the rows, joint dual updates)" if persistent else "k_primal (coloured primal sweep, one launch per "
+              "colour)")
+    roofline = {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                 "algorithmic_bytes_per_launch": per_iter * iters * prof["steps"] / primal_launches,
-                "avg_launch_us": primal_ms * 1e3 / primal_launches, "launches": primal_launches, **counts}
+                "avg_launch_us": primal_ms * 1e3 / primal_launches, "launches": primal_launches,
+                "iteration_mode": "one launch per step" if persistent else "one launch per colour", **counts}
     phases = {k[:-3]: round(v / max(1, prof["steps"]), 4) for k, v in prof.items() if k.endswith("_ms")}
 
     # ---- end to end through the C ABI with host buffers (H2D state, step, D2H state)
@@ -478,6 +488,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-adjoint-check", action="store_true")
+    ap.add_argument("--iteration-mode", type=int, default=1, choices=(0, 1),
+                    help="0 = one launch per colour and iteration plus the dual sweep, 1 = one launch per step")
     ap.add_argument("--primal-variant", type=int, default=-1,
                     help="use this primal variant (index into World.primal_variants()) instead of autotuning")
     args = ap.parse_args()

@@ -42,6 +42,10 @@ extern "C" {
 #define AVBD_BROADPHASE_GRID 1
 #define AVBD_BROADPHASE_SAP 2
 
+/* How a step runs its solver iterations (avbd_set_iteration_mode). */
+#define AVBD_ITERATIONS_PER_COLOUR 0 /* one launch per colour and iteration, then the dual sweep */
+#define AVBD_ITERATIONS_PERSISTENT 1 /* all iterations in one cooperative launch (default) */
+
 #define AVBD_FORCE_MANIFOLD 0
 #define AVBD_FORCE_JOINT 1
 #define AVBD_FORCE_SPRING 2
@@ -250,6 +254,16 @@ int avbd_next_seq(AvbdContext *ctx, int64_t *next_seq);
  * avbd_write_joints overwrites state28 and broken of existing joints, matched by sequence
  * number; body_ab2 must equal the joint's bodies (it is a check, not an edit).
  * Each call drops the recorded forward of the differentiable step. */
+/* Iteration mode: AVBD_ITERATIONS_PERSISTENT (default) runs every iteration of a step in
+ * one cooperative launch with grid-wide barriers between colours and each contact's dual
+ * update fused into the next iteration's primal row of the body that owns it;
+ * AVBD_ITERATIONS_PER_COLOUR launches each colour and the dual sweep separately. Both give
+ * the same bits. avbd_iteration_mode reports the mode the next step runs in (the
+ * per-colour form where the device cannot hold the persistent launch, and while the
+ * differentiable step records). */
+int avbd_set_iteration_mode(AvbdContext *ctx, int32_t mode);
+int avbd_iteration_mode(AvbdContext *ctx, int32_t *mode);
+
 int avbd_add_joints(AvbdContext *ctx, const AvbdJoints *joints);
 int avbd_remove_joints(AvbdContext *ctx, int32_t count, const int64_t *seq);
 int avbd_write_joints(AvbdContext *ctx, const AvbdJoints *joints);

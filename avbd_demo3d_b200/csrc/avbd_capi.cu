@@ -44,7 +44,9 @@ struct ManBuf
 };
 
 constexpr int PRIMAL_BLOCK = 128;
-constexpr int ITER_G = 4, ITER_BLOCK = 1024; // iteration kernel: lanes per body, threads per block (one per SM)
+// iteration kernel: lanes per body, threads per block (one block per SM), threads per
+// independently synchronised unit
+constexpr int ITER_G = 4, ITER_BLOCK = 1024, ITER_SUB = 1024;
 
 // Primal kernel variants: lanes per body (G) and the occupancy target given to the
 // compiler (resident blocks per SM; 1 = no register cap).
@@ -945,7 +947,7 @@ int iterate_persistent(AvbdContext *ctx)
     void *args[] = {&B, &F, &P, &entries, &colourStart, &nColours, &iterations, &sync};
     {
         PhaseScope ps(ctx, AVBD_PHASE_PRIMAL);
-        CU(cudaLaunchCooperativeKernel((void *)k_iterations<ITER_G, ITER_BLOCK>, ctx->iterBlocks, ITER_BLOCK, args,
+        CU(cudaLaunchCooperativeKernel((void *)k_iterations<ITER_G, ITER_BLOCK, ITER_SUB>, ctx->iterBlocks, ITER_BLOCK, args,
                                        sizeof(PrimalShared<ITER_G, ITER_BLOCK>), ctx->stream));
         LAUNCHED();
     }
@@ -1293,9 +1295,9 @@ int avbd_create(AvbdContext **out, int32_t device_ordinal, void *cuda_stream)
         // the iteration kernel: one block of ITER_BLOCK threads per SM with its shared batch
         int iterSm = 0;
         size_t smem = sizeof(PrimalShared<ITER_G, ITER_BLOCK>);
-        if (cudaFuncSetAttribute((const void *)k_iterations<ITER_G, ITER_BLOCK>,
+        if (cudaFuncSetAttribute((const void *)k_iterations<ITER_G, ITER_BLOCK, ITER_SUB>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess &&
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&iterSm, k_iterations<ITER_G, ITER_BLOCK>, ITER_BLOCK,
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&iterSm, k_iterations<ITER_G, ITER_BLOCK, ITER_SUB>, ITER_BLOCK,
                                                           smem) == cudaSuccess)
             ctx->iterBlocks = sms * iterSm;
         cudaGetLastError(); // an unsupported configuration only leaves the per-colour launches

@@ -2107,20 +2107,33 @@ struct PrimalShared
     int body[GPB];
 };
 
+// Barrier of one SUB-thread unit of the block (SUB = BLOCK: the whole block). Units use
+// named barriers 1..BLOCK/SUB, so they never wait for each other.
+template <int SUB, int BLOCK>
+AVBD_DEV void unit_sync()
+{
+    static_assert(BLOCK % SUB == 0 && SUB % 32 == 0 && BLOCK / SUB <= 15, "barrier units");
+    if constexpr (SUB == BLOCK)
+        __syncthreads();
+    else
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + (int)threadIdx.x / SUB), "n"(SUB) : "memory");
+}
+
 // One primal solve per body of a batch of one colour (solver.cpp:1186-1233). Rows: G lanes
 // per body. The solve entries carry the body and its row range; every lane of a group
 // builds the initial system M/dt^2 and keeps the entries it owns, then the rows are
 // evaluated G at a time (lane j evaluates row base + j into shared memory) and every lane
 // adds its entries row by row, so each sum keeps the reference's order. Solve: the batch's
 // accumulated systems go to shared memory and one thread per body factors its 6x6 system
-// and moves the body, so the factorisation runs with every lane of its warp busy. Every
-// thread of the block calls this (it holds a block barrier).
-template <int G, int BLOCK, bool COH>
+// and moves the body, so the factorisation runs with every lane of its warp busy. The
+// block works in independent units of SUB threads (SUB / G bodies, which the unit's first
+// SUB / G threads factorise); every thread of the block calls this (it holds the units'
+// barriers).
+template <int G, int BLOCK, int SUB, bool COH>
 AVBD_DEV void primal_batch(const DevBodies &B, const DevForces &F, const Params &P, const int4 *entries, int count,
                            bool fusedDual, PrimalShared<G, BLOCK> &sh)
 {
     static_assert(BLOCK % G == 0 && 32 % G == 0, "group size");
-    constexpr int GPB = BLOCK / G;
     constexpr int OWN = (E_COUNT + G - 1) / G;
     const int g = threadIdx.x / G;
     const int lane = threadIdx.x % G;
@@ -2189,9 +2202,10 @@ AVBD_DEV void primal_batch(const DevBodies &B, const DevForces &F, const Params 
         if (lane == 0)
             sh.body[g] = b;
     }
-    __syncthreads();
-    const int t = threadIdx.x;
-    if (t < GPB && t < count)
+    unit_sync<SUB, BLOCK>();
+    const int lt = threadIdx.x % SUB;
+    const int t = (threadIdx.x / SUB) * (SUB / G) + lt; // the unit's body this thread factorises
+    if (lt < SUB / G && t < count)
     {
         const int b = sh.body[t];
         const float4 p0 = ld_state<COH>(B.pos + b), q0 = ld_state<COH>(B.quat + b); // in flight during the solve
@@ -2215,7 +2229,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_primal(DevBodies B, DevForces F
     __shared__ PrimalShared<G, BLOCK> sh;
     constexpr int GPB = BLOCK / G;
     const int base = blockIdx.x * GPB;
-    primal_batch<G, BLOCK, false>(B, F, P, entries + first + base, min(GPB, count - base), false, sh);
+    primal_batch<G, BLOCK, BLOCK, false>(B, F, P, entries + first + base, min(GPB, count - base), false, sh);
 }
 
 // ---------------------------------------------------------------------------
@@ -2365,7 +2379,7 @@ AVBD_DEV bool iter_barrier(IterSync *s)
 // neither has the other body, so both poses are those the dual sweep of iteration k reads
 // and every contact's update is the same. The last iteration's contact updates close the
 // launch.
-template <int G, int BLOCK>
+template <int G, int BLOCK, int SUB>
 __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces F, Params P, const int4 *entries,
                                                          const int *colourStart, int nColours, int iterations,
                                                          IterSync *sync)
@@ -2382,8 +2396,9 @@ __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces 
             const int first = colourStart[c], cnt = colourStart[c + 1] - first;
             for (int base = blockIdx.x * GPB; base < cnt; base += gridDim.x * GPB)
             {
-                primal_batch<G, BLOCK, true>(B, F, P, entries + first + base, min(GPB, cnt - base), it > 0, sh);
-                __syncthreads(); // the batch's solve threads are done with the shared systems
+                primal_batch<G, BLOCK, SUB, true>(B, F, P, entries + first + base, min(GPB, cnt - base), it > 0,
+                                                  sh);
+                unit_sync<SUB, BLOCK>(); // the unit's solve threads are done with the shared systems
             }
             if (!iter_barrier(sync))
                 return;

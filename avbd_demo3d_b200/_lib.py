@@ -12,6 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libavbd_cuda.so")
 
 AVBD_OK = 0
+AVBD_ERR_ARGUMENT, AVBD_ERR_CUDA, AVBD_ERR_CAPACITY, AVBD_ERR_STATE, AVBD_ERR_LATCHED = -1, -2, -3, -4, -5
 ERRORS = {-1: "argument", -2: "cuda", -3: "capacity", -4: "state", -5: "latched"}
 
 c_float_p = ctypes.POINTER(ctypes.c_float)
@@ -108,6 +109,10 @@ SIGNATURES = {
     "avbd_num_joints": (ctypes.c_int, [ctypes.c_void_p, c_int_p]),
     "avbd_read_joints": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AvbdJointsOut)]),
     "avbd_next_seq": (ctypes.c_int, [ctypes.c_void_p, c_i64_p]),
+    "avbd_snapshot_binary": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_char_p, c_int_p,
+                                            ctypes.c_void_p, ctypes.c_int64, c_i64_p]),
+    "avbd_snapshot_json": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_char_p, c_int_p,
+                                          ctypes.c_char_p, ctypes.c_int64, c_i64_p]),
     "avbd_set_iteration_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     "avbd_iteration_mode": (ctypes.c_int, [ctypes.c_void_p, c_int_p]),
     "avbd_add_joints": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AvbdJoints)]),

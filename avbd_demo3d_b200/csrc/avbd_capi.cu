@@ -16,6 +16,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <iomanip>
+#include <sstream>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -124,6 +126,9 @@ struct AvbdContext
     DArr<int2> editAB;                // their bodies, packed states (8 float4 each),
     DArr<float4> editData;            // matched joint per edit, then the match count
     DArr<int> editJoint;
+    DArr<unsigned> snapIds, snapIdsAlt; // snapshot records: caller ids sorted with their bodies
+    DArr<int> snapOrder, snapOrderAlt;
+    DArr<uint4> snapRecords;
     DArr<int2> springAB, ignoreAB;
     DArr<unsigned long long> springSeq, ignoreSeq;
     DArr<float4> spring;
@@ -1381,6 +1386,11 @@ void avbd_destroy(AvbdContext *ctx)
         release(ctx->jointAB[k]);
         release(ctx->jointSeq[k]);
     }
+    release(ctx->snapIds);
+    release(ctx->snapIdsAlt);
+    release(ctx->snapOrder);
+    release(ctx->snapOrderAlt);
+    release(ctx->snapRecords);
     release(ctx->editSeq);
     release(ctx->editAB);
     release(ctx->editData);
@@ -2050,6 +2060,179 @@ int avbd_write_joints(AvbdContext *ctx, const AvbdJoints *joints)
                                                                   ctx->joint[ctx->jcur].p, ctx->nJoint);
     LAUNCHED();
     CU(cudaStreamSynchronize(ctx->stream));
+    return AVBD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Snapshots for the viewer bridge (viewer_bridge.cpp:748-842)
+// ---------------------------------------------------------------------------
+
+constexpr uint32_t SNAPSHOT_MAGIC = 0x53425641u; // "AVBS" read as a little-endian u32
+constexpr uint32_t SNAPSHOT_VERSION = 1;
+constexpr size_t SNAPSHOT_HEADER = 24, SNAPSHOT_RECORD = 64;
+
+// One 64-byte record per body, four 16-byte stores: id, shape (0 = box), material
+// (materialIdForBody: 0 static, 1 dynamic box), dynamic, position, rotation (x y z w),
+// full size, bounding radius, half length (0 for boxes). Record k is body order[k] with id
+// ids[k]; without them, the body of creation rank k (list index n - 1 - k) with id k.
+__global__ void k_snapshot_records(DevBodies B, const int *order, const unsigned *ids, int n, uint4 *out)
+{
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int k = (int)(t >> 2), part = (int)(t & 3);
+    if (k >= n)
+        return;
+    int b = order ? order[k] : n - 1 - k;
+    uint4 w;
+    if (part == 0)
+    {
+        unsigned id = ids ? ids[k] : (unsigned)k;
+        unsigned dyn = B.massMoment[b].x > 0.0f ? 1u : 0u;
+        w = make_uint4(id, 0u, dyn, dyn);
+    }
+    else if (part == 1)
+    {
+        float4 p = B.pos[b], q = B.quat[b];
+        w = make_uint4(__float_as_uint(p.x), __float_as_uint(p.y), __float_as_uint(p.z), __float_as_uint(q.x));
+    }
+    else if (part == 2)
+    {
+        float4 q = B.quat[b], sz = B.sizeRad[b];
+        w = make_uint4(__float_as_uint(q.y), __float_as_uint(q.z), __float_as_uint(q.w), __float_as_uint(sz.x));
+    }
+    else
+    {
+        float4 sz = B.sizeRad[b];
+        w = make_uint4(__float_as_uint(sz.y), __float_as_uint(sz.z), __float_as_uint(sz.w), 0u);
+    }
+    out[4 * (size_t)k + part] = w;
+}
+
+// Records of every body into host memory at `dst`, in ascending id order.
+int snapshot_records(AvbdContext *ctx, const int32_t *body_id, unsigned char *dst)
+{
+    int n = ctx->n;
+    if (n == 0)
+        return AVBD_OK;
+    const int *order = nullptr;
+    const unsigned *ids = nullptr;
+    if (body_id)
+    {
+        for (int i = 0; i < n; ++i)
+            if (body_id[i] < 0)
+                return fail(ctx, AVBD_ERR_ARGUMENT, "body %d: negative snapshot id", i);
+        std::vector<int> idx(n);
+        for (int i = 0; i < n; ++i)
+            idx[i] = i;
+        CHECK(upload(ctx, ctx->snapIds, (const unsigned *)body_id, n));
+        CHECK(upload(ctx, ctx->snapOrder, idx.data(), n));
+        CHECK(reserve(ctx, ctx->snapIdsAlt, n, false));
+        CHECK(reserve(ctx, ctx->snapOrderAlt, n, false));
+        cub::DoubleBuffer<unsigned> dk(ctx->snapIds.p, ctx->snapIdsAlt.p);
+        cub::DoubleBuffer<int> dv(ctx->snapOrder.p, ctx->snapOrderAlt.p);
+        size_t bytes = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, bytes, dk, dv, n, 0, 32, ctx->stream);
+        CHECK(ensure_temp(ctx, bytes));
+        CU(cub::DeviceRadixSort::SortPairs(ctx->cubTemp.p, bytes, dk, dv, n, 0, 32, ctx->stream));
+        ids = dk.Current();
+        order = dv.Current();
+    }
+    CHECK(reserve(ctx, ctx->snapRecords, 4 * (size_t)n, false));
+    k_snapshot_records<<<grid_for(4ll * n, 256), 256, 0, ctx->stream>>>(dev_bodies(ctx), order, ids, n,
+                                                                          ctx->snapRecords.p);
+    LAUNCHED();
+    CU(cudaMemcpyAsync(dst, ctx->snapRecords.p, SNAPSHOT_RECORD * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return AVBD_OK;
+}
+
+int avbd_snapshot_binary(AvbdContext *ctx, uint64_t frame, const char *scene_name, const int32_t *body_id,
+                         uint8_t *out, int64_t capacity, int64_t *size)
+{
+    if (!ctx || !size)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
+    if (!ctx->loaded)
+        return fail(ctx, AVBD_ERR_STATE, "no world loaded");
+    CU(cudaSetDevice(ctx->device));
+    size_t sceneBytes = scene_name ? strlen(scene_name) : 0;
+    size_t total = SNAPSHOT_HEADER + sceneBytes + SNAPSHOT_RECORD * (size_t)ctx->n;
+    *size = (int64_t)total;
+    if (!out)
+        return AVBD_OK;
+    if (capacity < (int64_t)total)
+        return fail(ctx, AVBD_ERR_CAPACITY, "snapshot needs %zu bytes, buffer holds %lld", total, (long long)capacity);
+    uint32_t head[2] = {SNAPSHOT_MAGIC, SNAPSHOT_VERSION}, counts[2] = {(uint32_t)sceneBytes, (uint32_t)ctx->n};
+    memcpy(out, head, 8);
+    memcpy(out + 8, &frame, 8);
+    memcpy(out + 16, counts, 8);
+    if (sceneBytes)
+        memcpy(out + SNAPSHOT_HEADER, scene_name, sceneBytes);
+    return snapshot_records(ctx, body_id, out + SNAPSHOT_HEADER + sceneBytes);
+}
+
+// makeSnapshotJson's text (viewer_bridge.cpp:748-777, jsonEscape :495-530) from the same
+// records, with the same stream settings (fixed, 5 decimals).
+int avbd_snapshot_json(AvbdContext *ctx, uint64_t frame, const char *scene_name, const int32_t *body_id, char *out,
+                       int64_t capacity, int64_t *size)
+{
+    if (!ctx || !size)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
+    if (!ctx->loaded)
+        return fail(ctx, AVBD_ERR_STATE, "no world loaded");
+    CU(cudaSetDevice(ctx->device));
+    int n = ctx->n;
+    std::vector<unsigned char> rec(SNAPSHOT_RECORD * (size_t)n);
+    CHECK(snapshot_records(ctx, body_id, rec.data()));
+    std::string scene;
+    for (const char *c = scene_name ? scene_name : ""; *c; ++c)
+    {
+        if (*c == '"' || *c == '\\')
+        {
+            scene.push_back('\\');
+            scene.push_back(*c);
+        }
+        else if (*c == '\n')
+            scene += "\\n";
+        else if (*c == '\r')
+            scene += "\\r";
+        else if (*c == '\t')
+            scene += "\\t";
+        else if ((unsigned char)*c < 0x20)
+        {
+            char escaped[7];
+            snprintf(escaped, sizeof(escaped), "\\u%04x", (unsigned char)*c);
+            scene += escaped;
+        }
+        else
+            scene.push_back(*c);
+    }
+    std::ostringstream os;
+    os << std::fixed << std::setprecision(5);
+    os << "{\"type\":\"snapshot\",\"version\":1,\"frame\":" << frame << ",\"scene\":\"" << scene
+       << "\",\"bodies\":[";
+    for (int k = 0; k < n; ++k)
+    {
+        const unsigned char *r = rec.data() + SNAPSHOT_RECORD * (size_t)k;
+        uint32_t w[4];
+        float f[12];
+        memcpy(w, r, 16);
+        memcpy(f, r + 16, 48);
+        if (k)
+            os << ",";
+        os << "{\"id\":" << w[0] << ",\"shape\":\"box\"" << ",\"position\":[" << f[0] << "," << f[1] << ","
+           << f[2] << "]" << ",\"rotation\":[" << f[3] << "," << f[4] << "," << f[5] << "," << f[6] << "]"
+           << ",\"size\":[" << f[7] << "," << f[8] << "," << f[9] << "]" << ",\"radius\":" << f[10]
+           << ",\"halfLength\":" << f[11] << ",\"dynamic\":" << (w[3] ? "true" : "false")
+           << ",\"material\":" << w[2] << "}";
+    }
+    os << "]}";
+    std::string text = os.str();
+    *size = (int64_t)text.size() + 1;
+    if (!out)
+        return AVBD_OK;
+    if (capacity < *size)
+        return fail(ctx, AVBD_ERR_CAPACITY, "snapshot text needs %lld bytes, buffer holds %lld", (long long)*size,
+                    (long long)capacity);
+    memcpy(out, text.c_str(), text.size() + 1);
     return AVBD_OK;
 }
 

@@ -346,6 +346,28 @@ class World:
                     "avbd_autotune")
         return best.value, us
 
+    # -- viewer-bridge snapshots (viewer_bridge.cpp:748-842)
+    def _snapshot(self, fn, frame, scene, body_id, make):
+        ids = None if body_id is None else _c(body_id, np.int32)
+        idp = None if ids is None else ids.ctypes.data_as(_lib.c_int_p)
+        name = scene.encode()
+        size = ctypes.c_int64()
+        self._check(getattr(self.lib, fn)(self.h, frame, name, idp, None, 0, ctypes.byref(size)), fn)
+        buf = make(size.value)
+        self._check(getattr(self.lib, fn)(self.h, frame, name, idp, buf, size.value, ctypes.byref(size)), fn)
+        return buf
+
+    def snapshot_binary(self, frame: int = 0, scene: str = "", body_id=None) -> bytes:
+        """The AVBS binary snapshot of every body, in ascending id order (ids: the creation rank
+        unless body_id gives each list-order body's id)."""
+        return bytes(self._snapshot("avbd_snapshot_binary", frame, scene, body_id,
+                                    lambda n: (ctypes.c_uint8 * n)()))
+
+    def snapshot_json(self, frame: int = 0, scene: str = "", body_id=None) -> str:
+        """makeSnapshotJson's text for every body."""
+        buf = self._snapshot("avbd_snapshot_json", frame, scene, body_id, ctypes.create_string_buffer)
+        return buf.value.decode()
+
     def set_iteration_mode(self, mode: int):
         """0 = one launch per colour and iteration plus the dual sweep, 1 = every iteration in
         one cooperative launch (default). Both give the same bits."""

@@ -254,6 +254,22 @@ int avbd_next_seq(AvbdContext *ctx, int64_t *next_seq);
  * avbd_write_joints overwrites state28 and broken of existing joints, matched by sequence
  * number; body_ab2 must equal the joint's bodies (it is a check, not an edit).
  * Each call drops the recorded forward of the differentiable step. */
+/* Viewer-bridge snapshots of every body, written from the device state
+ * (makeSnapshotBinary / makeSnapshotJson, viewer_bridge.cpp:748-842; the viewer's decoder
+ * is decodeBinarySnapshot, viewer/src/main.js:986-1050).
+ * Binary ("AVBS"): u32 magic 0x53425641, u32 version 1, u64 frame, u32 scene bytes, u32
+ * body count, the scene name, then per body in ascending id order 64 bytes: u32 id, shape
+ * (0 = box), material (0 static, 1 dynamic box), dynamic; f32 position[3], rotation[4]
+ * (x y z w), size[3] (full widths), radius, half length. JSON: the same fields as text,
+ * numbers with 5 decimals.
+ * body_id: the SimWorld dense id of each body (list order), or NULL for the creation rank
+ * (the dense id of a world built without deletions). *size receives the bytes needed
+ * (the JSON text with its terminating zero); out = NULL only queries it. */
+int avbd_snapshot_binary(AvbdContext *ctx, uint64_t frame, const char *scene_name, const int32_t *body_id,
+                         uint8_t *out, int64_t capacity, int64_t *size);
+int avbd_snapshot_json(AvbdContext *ctx, uint64_t frame, const char *scene_name, const int32_t *body_id, char *out,
+                       int64_t capacity, int64_t *size);
+
 /* Iteration mode: AVBD_ITERATIONS_PERSISTENT (default) runs every iteration of a step in
  * one cooperative launch with grid-wide barriers between colours and each contact's dual
  * update fused into the next iteration's primal row of the body that owns it;

@@ -11,6 +11,7 @@ Only the tests, the smoke check and the benchmark's CPU-baseline leg use this mo
 from __future__ import annotations
 
 import ctypes
+import struct
 import os
 import subprocess
 
@@ -79,6 +80,9 @@ def _lib(kind: str) -> ctypes.CDLL:
     for name in ("prepare", "iterate", "finish", "num_bodies", "num_manifolds", "num_joints", "broadphase_only"):
         getattr(lib, p + name).argtypes = [vp]
         getattr(lib, p + name).restype = ip
+    if p == "ref_":
+        lib.ref_world_bodies.argtypes = [vp] + [ctypes.c_void_p] * 9
+        lib.ref_world_bodies.restype = ip
     getattr(lib, p + "add_joint").argtypes = [vp, ip, ip, fp, fp, ctypes.c_float, ctypes.c_float, ctypes.c_float]
     getattr(lib, p + "add_joint").restype = ctypes.c_int64
     getattr(lib, p + "set_joint_anchor").argtypes = [vp, ctypes.c_int64, fp]
@@ -186,6 +190,17 @@ class World:
 
     def broadphase_only(self):
         self._f("broadphase_only")(self.h)
+
+    # reference only: the dense SimWorld bodies (the snapshot source)
+    def world_bodies(self) -> dict:
+        n = self.lib.ref_world_bodies(self.h, *([None] * 9))
+        out = {"active": np.zeros(n, np.int32), "shape": np.zeros(n, np.int32), "mass": np.zeros(n, np.float32),
+               "pos": np.zeros((n, 3), np.float32), "quat": np.zeros((n, 4), np.float32),
+               "size": np.zeros((n, 3), np.float32), "radius": np.zeros(n, np.float32),
+               "half_length": np.zeros(n, np.float32), "list_index": np.zeros(n, np.int32)}
+        self.lib.ref_world_bodies(self.h, *[_ptr(out[k]) for k in ("active", "shape", "mass", "pos", "quat", "size",
+                                                                   "radius", "half_length", "list_index")])
+        return out
 
     # joint edits between steps (list-order bodies; a = -1 anchors to the world point rA)
     def add_joint(self, a, b, rA, rB, stiff_lin=float("inf"), stiff_ang=0.0, fracture=float("inf")) -> int:
@@ -350,3 +365,92 @@ def collide_boxes(kind: str, pA, qA, sA, pB, qB, sB):
 
 def colour_priority(b: int) -> int:
     return int(_lib("oracle").oracle_colour_priority(b))
+
+
+# ---------------------------------------------------------------------------
+# Viewer-bridge snapshots (test restatement of viewer_bridge.cpp:748-842 and of the
+# viewer's decoder, viewer/src/main.js:986-1050)
+# ---------------------------------------------------------------------------
+
+SNAPSHOT_MAGIC = 0x53425641
+SHAPE_NAMES = {0: "box", 1: "sphere", 2: "capsule", 3: "cylinder"}
+
+
+def material_id(mass, shape):
+    """materialIdForBody (viewer_bridge.cpp:475-493)."""
+    if mass <= 0.0:
+        return 0
+    return {0: 1, 1: 3, 3: 4, 2: 5}.get(int(shape), 1)
+
+
+def snapshot_fields(ids, shape, mass, pos, quat, size, radius, half_length) -> list:
+    """Per-body snapshot fields in ascending id order (one dict each)."""
+    order = np.argsort(np.asarray(ids), kind="stable")
+    return [{"id": int(ids[i]), "shape": int(shape[i]), "material": material_id(float(mass[i]), shape[i]),
+             "dynamic": bool(mass[i] > 0), "pos": np.asarray(pos[i], np.float32),
+             "quat": np.asarray(quat[i], np.float32), "size": np.asarray(size[i], np.float32),
+             "radius": np.float32(radius[i]), "half_length": np.float32(half_length[i])} for i in order]
+
+
+def encode_snapshot(frame: int, scene: str, bodies: list) -> bytes:
+    """makeSnapshotBinary (viewer_bridge.cpp:800-842)."""
+    name = scene.encode()
+    out = [struct.pack("<IIQII", SNAPSHOT_MAGIC, 1, frame, len(name), len(bodies)), name]
+    for b in bodies:
+        out.append(struct.pack("<IIII", b["id"], b["shape"], b["material"], 1 if b["dynamic"] else 0))
+        out.append(np.concatenate([b["pos"], b["quat"], b["size"], [b["radius"], b["half_length"]]]).astype(
+            "<f4").tobytes())
+    return b"".join(out)
+
+
+def decode_snapshot(buf: bytes) -> dict:
+    """decodeBinarySnapshot (viewer/src/main.js:986-1050)."""
+    magic, version, frame, scene_bytes, count = struct.unpack_from("<IIQII", buf, 0)
+    if magic != SNAPSHOT_MAGIC or version != 1:
+        raise ValueError("not an AVBD binary snapshot")
+    off = 24
+    scene = buf[off:off + scene_bytes].decode()
+    off += scene_bytes
+    bodies = []
+    for _ in range(count):
+        i, shape, material, dynamic = struct.unpack_from("<IIII", buf, off)
+        f = np.frombuffer(buf, "<f4", 12, off + 16)
+        bodies.append({"id": i, "shape": shape, "material": material, "dynamic": dynamic != 0, "pos": f[0:3],
+                       "quat": f[3:7], "size": f[7:10], "radius": f[10], "half_length": f[11]})
+        off += 64
+    if off != len(buf):
+        raise ValueError("trailing bytes")
+    return {"frame": frame, "scene": scene, "bodies": bodies}
+
+
+def _json_escape(text: str) -> str:
+    """jsonEscape (viewer_bridge.cpp:495-530)."""
+    out = []
+    for ch in text:
+        if ch in '"\\':
+            out.append("\\" + ch)
+        elif ch == "\n":
+            out.append("\\n")
+        elif ch == "\r":
+            out.append("\\r")
+        elif ch == "\t":
+            out.append("\\t")
+        elif ord(ch) < 0x20:
+            out.append("\\u%04x" % ord(ch))
+        else:
+            out.append(ch)
+    return "".join(out)
+
+
+def snapshot_json(frame: int, scene: str, bodies: list) -> str:
+    """makeSnapshotJson (viewer_bridge.cpp:748-777): fixed notation, 5 decimals."""
+    f = lambda x: "%.5f" % float(x)
+    items = []
+    for b in bodies:
+        items.append('{"id":%d,"shape":"%s","position":[%s],"rotation":[%s],"size":[%s],"radius":%s,'
+                     '"halfLength":%s,"dynamic":%s,"material":%d}' % (
+                         b["id"], SHAPE_NAMES.get(b["shape"], "box"), ",".join(map(f, b["pos"])),
+                         ",".join(map(f, b["quat"])), ",".join(map(f, b["size"])), f(b["radius"]),
+                         f(b["half_length"]), "true" if b["dynamic"] else "false", b["material"]))
+    return ('{"type":"snapshot","version":1,"frame":%d,"scene":"%s","bodies":[' % (frame, _json_escape(scene))
+            + ",".join(items) + "]}")

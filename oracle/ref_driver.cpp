@@ -164,6 +164,42 @@ int ref_remove_joint(void *p, int64_t handle)
     return 0;
 }
 
+/* The dense SimWorld bodies, the source of the viewer bridge's snapshots
+ * (viewer_bridge.cpp:748-842), synced from the objects as finishStep does; listIndex maps a
+ * dense id to its body's list index (-1 for an inactive slot). Returns the slot count. */
+int ref_world_bodies(void *p, int *active, int *shape, float *mass, float *pos3, float *quat4, float *size3,
+                     float *radius, float *halfLength, int *listIndex)
+{
+    RefWorld *w = (RefWorld *)p;
+    w->solver.world.syncFromLegacy(w->solver);
+    const SimWorld &sw = w->solver.world;
+    int n = (int)sw.bodies.size();
+    if (!active)
+        return n;
+    for (int i = 0; i < n; ++i)
+    {
+        const SimBodyData &b = sw.bodies[i];
+        active[i] = b.active ? 1 : 0;
+        shape[i] = (int)b.shape.type;
+        mass[i] = b.mass;
+        pos3[3 * i] = b.positionLin.x;
+        pos3[3 * i + 1] = b.positionLin.y;
+        pos3[3 * i + 2] = b.positionLin.z;
+        quat4[4 * i] = b.positionAng.x;
+        quat4[4 * i + 1] = b.positionAng.y;
+        quat4[4 * i + 2] = b.positionAng.z;
+        quat4[4 * i + 3] = b.positionAng.w;
+        size3[3 * i] = b.shape.size.x;
+        size3[3 * i + 1] = b.shape.size.y;
+        size3[3 * i + 2] = b.shape.size.z;
+        radius[i] = b.shape.radius;
+        halfLength[i] = b.shape.halfLength;
+        auto it = b.source ? w->index.find(b.source) : w->index.end();
+        listIndex[i] = it == w->index.end() ? -1 : it->second;
+    }
+    return n;
+}
+
 int ref_broadphase_only(void *p)
 {
     RefWorld *w = (RefWorld *)p;

@@ -119,6 +119,34 @@ def test_drag_edits_match_reference():
         assert np.array_equal(jo["ab"], jr["ab"]) and np.array_equal(bits(jo["state"]), bits(jr["state"])), so
 
 
+def test_snapshot_fields_match_reference_world():
+    """The viewer-bridge snapshot of the oracle's state (dense id = creation rank, shape box,
+    full size, bounding radius, half length 0) is byte-identical to the one assembled from the
+    reference's own SimWorld, and the viewer's decoder reads it back."""
+    sc = scenes.mixed_drop(900, 6, 8, 0.1, extent=(18, 18, 12), seed=37)
+    o = checkers.World(sc, "oracle", order_mode=0)
+    r = checkers.World(sc, "ref")
+    o.step(25)
+    r.step(25)
+    wb = r.world_bodies()
+    n = sc.n_bodies
+    assert len(wb["active"]) == n and wb["active"].all()
+    assert np.array_equal(wb["list_index"], n - 1 - np.arange(n))  # dense id = creation rank
+    ref = checkers.snapshot_fields(np.arange(n), wb["shape"], wb["mass"], wb["pos"], wb["quat"], wb["size"],
+                                   wb["radius"], wb["half_length"])
+    ob, pr = o.bodies(), o.body_props()
+    mine = checkers.snapshot_fields(n - 1 - np.arange(n), np.zeros(n, np.int32), pr["mass"], ob["pos"], ob["quat"],
+                                    pr["size"], pr["radius"], np.zeros(n, np.float32))
+    blob = checkers.encode_snapshot(1234, "Mixed", ref)
+    assert blob == checkers.encode_snapshot(1234, "Mixed", mine)
+    assert len(blob) == 24 + 5 + 64 * n
+    assert checkers.snapshot_json(1234, "Mixed", ref) == checkers.snapshot_json(1234, "Mixed", mine)
+    dec = checkers.decode_snapshot(blob)
+    assert dec["frame"] == 1234 and dec["scene"] == "Mixed" and [b["id"] for b in dec["bodies"]] == list(range(n))
+    assert all(np.array_equal(b["pos"], f["pos"]) and b["material"] == f["material"]
+               for b, f in zip(dec["bodies"], ref))
+
+
 def test_narrowphase_random_pairs():
     import make_golden
 

@@ -138,6 +138,7 @@ struct AvbdContext
     DArr<int> rowCount, entryRow, rowStart; // rows per force-list entry, their offsets, ranges per body
     DArr<int2> rows;
     DArr<unsigned long long> incKeys, incKeysAlt;
+    int incShift = 1; // sequence bits of the incidence keys of the current adjacency
 
     DArr<int> colourState, colour, solveList, colourStart;
     DArr<int4> solveEntry; // solve list with each body's row range, for the primal
@@ -484,6 +485,9 @@ __global__ void k_u8_to_int(const unsigned char *in, int *out, int n)
 // Per-body force lists (CSR) sorted newest first.
 int build_rows(AvbdContext *ctx, const unsigned long long *sortedKeys, int total);
 
+// Bits needed to write v (0 for v = 0).
+int bit_width(unsigned long long v) { return v ? 64 - __builtin_clzll(v) : 0; }
+
 int build_adjacency(AvbdContext *ctx)
 {
     int n = ctx->n;
@@ -502,17 +506,22 @@ int build_adjacency(AvbdContext *ctx)
     CHECK(reserve(ctx, ctx->incValsAlt, T, false));
     CHECK(reserve(ctx, ctx->adj, T, false));
     DevForces F = dev_forces(ctx);
-    k_incidences<<<grid_for(T, 256), 256, 0, ctx->stream>>>(F, ctx->incKeys.p, ctx->incVals.p);
+    // every sequence number is below nextSeq: the key needs bit_width(nextSeq) + bit_width(n) bits
+    int shift = std::max(1, bit_width((unsigned long long)std::max<long long>(ctx->nextSeq, 1)));
+    int endBit = shift + bit_width((unsigned long long)n);
+    if (shift > KEY_SEQ_BITS || endBit > 64)
+        return fail(ctx, AVBD_ERR_CAPACITY, "sequence numbers (%lld) too large for the incidence keys", ctx->nextSeq);
+    ctx->incShift = shift;
+    k_incidences<<<grid_for(T, 256), 256, 0, ctx->stream>>>(F, shift, n, ctx->incKeys.p, ctx->incVals.p);
     LAUNCHED();
     cub::DoubleBuffer<unsigned long long> dk(ctx->incKeys.p, ctx->incKeysAlt.p);
     cub::DoubleBuffer<unsigned> dv(ctx->incVals.p, ctx->incValsAlt.p);
     size_t bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, bytes, dk, dv, (int)T, 0, 64, ctx->stream);
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, dk, dv, (int)T, 0, endBit, ctx->stream);
     CHECK(ensure_temp(ctx, bytes));
-    CU(cub::DeviceRadixSort::SortPairs(ctx->cubTemp.p, bytes, dk, dv, (int)T, 0, 64, ctx->stream));
+    CU(cub::DeviceRadixSort::SortPairs(ctx->cubTemp.p, bytes, dk, dv, (int)T, 0, endBit, ctx->stream));
     ctx->launches++;
-    k_segment_starts<<<grid_for(T, 256), 256, 0, ctx->stream>>>(dk.Current(), (int)T, KEY_BODY_SHIFT, n,
-                                                                  ctx->adjStart.p);
+    k_segment_starts<<<grid_for(T, 256), 256, 0, ctx->stream>>>(dk.Current(), (int)T, shift, n, ctx->adjStart.p);
     LAUNCHED();
     k_copy_adj<<<grid_for(T, 256), 256, 0, ctx->stream>>>(dv.Current(), ctx->adj.p, (int)T);
     LAUNCHED();
@@ -536,7 +545,7 @@ int build_rows(AvbdContext *ctx, const unsigned long long *sortedKeys, int total
     CHECK(reserve(ctx, ctx->rows, std::max<size_t>(bound, 1), false));
     DevForces F = dev_forces(ctx);
     k_entry_rows<<<grid_for((long long)total + 1, 256), 256, 0, ctx->stream>>>(F, dev_bodies(ctx), sortedKeys, total,
-                                                                               KEY_BODY_SHIFT, ctx->rowCount.p);
+                                                                               ctx->incShift, ctx->rowCount.p);
     LAUNCHED();
     CHECK(scan_counts(ctx, ctx->rowCount.p, ctx->entryRow.p, total + 1, 0));
     ctx->launches++;
@@ -711,9 +720,11 @@ int broadphase(AvbdContext *ctx)
             LAUNCHED();
             dk = cub::DoubleBuffer<unsigned long long>(ctx->bpKeys.p, ctx->bpKeysAlt.p);
             size_t bytes = 0;
-            cub::DeviceRadixSort::SortKeys(nullptr, bytes, dk, nB, 0, 64, ctx->stream);
+            // grid keys: world (below W) | cell (22 bits) | body (24 bits)
+            int gridEnd = 46 + bit_width((unsigned long long)(ctx->W - 1));
+            cub::DeviceRadixSort::SortKeys(nullptr, bytes, dk, nB, 0, gridEnd, ctx->stream);
             CHECK(ensure_temp(ctx, bytes));
-            CU(cub::DeviceRadixSort::SortKeys(ctx->cubTemp.p, bytes, dk, nB, 0, 64, ctx->stream));
+            CU(cub::DeviceRadixSort::SortKeys(ctx->cubTemp.p, bytes, dk, nB, 0, gridEnd, ctx->stream));
             ctx->launches++;
             CU(cudaMemsetAsync(ctx->cellHashKeys.p, 0xFF,
                                sizeof(unsigned long long) * ((size_t)ctx->cellHashMask + 1), ctx->stream));
@@ -1541,6 +1552,20 @@ int avbd_load_batch(AvbdContext *ctx, int32_t num_worlds, const int32_t *world_s
         for (int i = 0; i < count; ++i)
             out[i] = (unsigned long long)s[i];
     };
+    // every sequence number lies in [0, next_seq): new forces continue from next_seq and the
+    // adjacency keys are sized by it
+    auto seqs_below = [&](const int64_t *s, int count) {
+        for (int i = 0; i < count; ++i)
+            if (s[i] < 0 || s[i] >= next_seq)
+                return false;
+        return true;
+    };
+    if (next_seq < 0 || (unsigned long long)next_seq > KEY_SEQ_MASK ||
+        (joints && joints->count > 0 && joints->seq && !seqs_below(joints->seq, joints->count)) ||
+        (springs && springs->count > 0 && springs->seq && !seqs_below(springs->seq, springs->count)) ||
+        (ignores && ignores->count > 0 && ignores->seq && !seqs_below(ignores->seq, ignores->count)) ||
+        (manifolds && manifolds->count > 0 && manifolds->seq && !seqs_below(manifolds->seq, manifolds->count)))
+        return fail(ctx, AVBD_ERR_ARGUMENT, "sequence numbers must lie in [0, next_seq) with next_seq < 2^40");
     std::vector<unsigned long long> sq;
     // joints
     int J = joints ? joints->count : 0;

@@ -1383,18 +1383,23 @@ __global__ void k_joint_write(int edits, const int *editJoint, const float4 *edi
 // Adjacency (per-body force lists, newest first)
 // ---------------------------------------------------------------------------
 
-constexpr int KEY_BODY_SHIFT = 40;
-constexpr unsigned long long KEY_SEQ_MASK = (1ull << KEY_BODY_SHIFT) - 1ull;
-constexpr unsigned long long KEY_NO_BODY = 0xFFFFFFull;
+constexpr int KEY_SEQ_BITS = 40; // sequence numbers stay below 2^40
+constexpr unsigned long long KEY_SEQ_MASK = (1ull << KEY_SEQ_BITS) - 1ull;
+constexpr unsigned long long KEY_NO_BODY = 0xFFFFFFull; // body counts stay below this
 
-AVBD_DEV unsigned long long incidence_key(int body, unsigned long long seq)
+// Incidence key: body, then newest force first. `shift` is the bit width of the sequence
+// counter (every sequence number is below 2^shift), so the key spans shift + bits(n) bits
+// and the sort passes only over those; the world side of an anchored joint takes body n,
+// after every real body.
+AVBD_DEV unsigned long long incidence_key(int body, unsigned long long seq, int shift, int n)
 {
-    unsigned long long b = body >= 0 ? (unsigned long long)body : KEY_NO_BODY;
-    return (b << KEY_BODY_SHIFT) | (KEY_SEQ_MASK - (seq & KEY_SEQ_MASK));
+    unsigned long long b = body >= 0 ? (unsigned long long)body : (unsigned long long)n;
+    unsigned long long cap = (1ull << shift) - 1ull;
+    return (b << shift) | (cap - (seq & cap));
 }
 
 // Two incidences per force: manifolds [0, 2M), joints [2M, 2M+2J), springs, ignores.
-__global__ void k_incidences(DevForces F, unsigned long long *keys, unsigned *vals)
+__global__ void k_incidences(DevForces F, int shift, int n, unsigned long long *keys, unsigned *vals)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     int total = 2 * (F.nMan + F.nJoint + F.nSpring + F.nIgnore);
@@ -1430,7 +1435,7 @@ __global__ void k_incidences(DevForces F, unsigned long long *keys, unsigned *va
         seq = F.ignoreSeq[f];
         type = ADJ_IGNORE;
     }
-    keys[t] = incidence_key(isA ? ab.x : ab.y, seq);
+    keys[t] = incidence_key(isA ? ab.x : ab.y, seq, shift, n);
     vals[t] = make_adj(type, isA, (unsigned)f);
 }
 

@@ -29,7 +29,7 @@ class AvbdParams(ctypes.Structure):
 class AvbdBodies(ctypes.Structure):
     _fields_ = [("count", ctypes.c_int32)] + [(k, ctypes.c_void_p) for k in (
         "position3", "orientation4", "velocity3", "angular3", "prev_velocity3", "size3", "mass", "moment3",
-        "friction", "radius")]
+        "friction", "radius", "shape", "shape_radius", "half_length")]
 
 
 class AvbdBodyState(ctypes.Structure):

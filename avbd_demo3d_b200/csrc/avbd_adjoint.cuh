@@ -1551,6 +1551,9 @@ int avbd_adjoint_forward(AvbdContext *ctx, int32_t nsteps, int32_t checkpoint_ev
     if (ctx->nJoint > 0 || ctx->nSpring > 0)
         return fail(ctx, AVBD_ERR_ARGUMENT,
                     "adjoint_forward: the differentiable step covers contacts; the world has joints or springs");
+    if (ctx->hasShapes)
+        return fail(ctx, AVBD_ERR_ARGUMENT,
+                    "adjoint_forward: the differentiable step covers boxes; the world has round bodies");
     if (ctx->params.iterations < 1)
         return fail(ctx, AVBD_ERR_ARGUMENT, "adjoint_forward: needs at least one solver iteration");
     if (!ctx->adjoint)

@@ -146,6 +146,9 @@ struct AvbdContext
     DArr<ColourControl> colourCtl;
     int colourBlocks = 148;   // co-resident blocks for the cooperative colouring launch
     int iterationMode = AVBD_ITERATIONS_PERSISTENT;
+    DArr<float4> shape;      // (type, radius, half length, 0) per body when any body is round
+    bool hasShapes = false;  // some body is not a box
+    bool hasSpheres = false; // rolling friction pass after the velocity update
     int iterBlocks = 0;       // co-resident blocks of the iteration kernel (0: not launchable)
     DArr<IterSync> iterSync;
     int *hIterError = nullptr; // pinned: barrier expiry of the last iteration kernel
@@ -343,6 +346,7 @@ DevBodies dev_bodies(AvbdContext *ctx)
     B.prevVel = ctx->prevVel.p;
     B.massMoment = ctx->massMoment.p;
     B.sizeRad = ctx->sizeRad.p;
+    B.shape = ctx->hasShapes ? ctx->shape.p : nullptr;
     B.friction = ctx->friction.p;
     return B;
 }
@@ -1051,6 +1055,11 @@ int step_once(AvbdContext *ctx)
         PhaseScope ps(ctx, AVBD_PHASE_VELOCITY);
         k_finish<<<grid_for(ctx->n, 256), 256, 0, ctx->stream>>>(B, P);
         LAUNCHED();
+        if (ctx->hasSpheres)
+        {
+            k_rolling_friction<<<grid_for(ctx->n, 128), 128, 0, ctx->stream>>>(B, dev_forces(ctx), ctx->adjStart.p);
+            LAUNCHED();
+        }
     }
     ctx->stats.body_count = ctx->n;
     ctx->stats.manifold_count = ctx->nMan;
@@ -1147,6 +1156,27 @@ int upload_bodies(AvbdContext *ctx, const AvbdBodies *b, bool props)
             tmp[i] = make_float4(b->size3[3 * i], b->size3[3 * i + 1], b->size3[3 * i + 2], b->radius[i]);
         CHECK(upload(ctx, ctx->sizeRad, tmp.data(), n));
         CHECK(upload(ctx, ctx->friction, b->friction, n));
+        ctx->hasShapes = ctx->hasSpheres = false;
+        if (b->shape)
+        {
+            for (int i = 0; i < n; ++i)
+            {
+                int t = b->shape[i];
+                if (t < AVBD_SHAPE_BOX || t > AVBD_SHAPE_CYLINDER)
+                    return fail(ctx, AVBD_ERR_ARGUMENT, "body %d: unknown shape %d", i, t);
+                if (t != AVBD_SHAPE_BOX && (!b->shape_radius || !b->half_length))
+                    return fail(ctx, AVBD_ERR_ARGUMENT, "round bodies need shape_radius and half_length");
+                ctx->hasShapes |= t != AVBD_SHAPE_BOX;
+                ctx->hasSpheres |= t == AVBD_SHAPE_SPHERE;
+            }
+            if (ctx->hasShapes)
+            {
+                for (int i = 0; i < n; ++i)
+                    tmp[i] = make_float4((float)b->shape[i], b->shape_radius ? b->shape_radius[i] : b->radius[i],
+                                         b->half_length ? b->half_length[i] : 0.0f, 0.0f);
+                CHECK(upload(ctx, ctx->shape, tmp.data(), n));
+            }
+        }
         for (DArr<float4> *a : {&ctx->initLin, &ctx->initAng, &ctx->inertLin, &ctx->inertAng, &ctx->dqLin, &ctx->dqAng})
         {
             CHECK(reserve(ctx, *a, std::max(n, 1), false));
@@ -1397,6 +1427,7 @@ void avbd_destroy(AvbdContext *ctx)
         release(ctx->jointAB[k]);
         release(ctx->jointSeq[k]);
     }
+    release(ctx->shape);
     release(ctx->snapIds);
     release(ctx->snapIdsAlt);
     release(ctx->snapOrder);
@@ -2096,9 +2127,9 @@ constexpr uint32_t SNAPSHOT_MAGIC = 0x53425641u; // "AVBS" read as a little-endi
 constexpr uint32_t SNAPSHOT_VERSION = 1;
 constexpr size_t SNAPSHOT_HEADER = 24, SNAPSHOT_RECORD = 64;
 
-// One 64-byte record per body, four 16-byte stores: id, shape (0 = box), material
-// (materialIdForBody: 0 static, 1 dynamic box), dynamic, position, rotation (x y z w),
-// full size, bounding radius, half length (0 for boxes). Record k is body order[k] with id
+// One 64-byte record per body, four 16-byte stores: id, shape, material
+// (materialIdForBody), dynamic, position, rotation (x y z w), full size, shape radius, half
+// length (0 for boxes and spheres). Record k is body order[k] with id
 // ids[k]; without them, the body of creation rank k (list index n - 1 - k) with id k.
 __global__ void k_snapshot_records(DevBodies B, const int *order, const unsigned *ids, int n, uint4 *out)
 {
@@ -2108,11 +2139,18 @@ __global__ void k_snapshot_records(DevBodies B, const int *order, const unsigned
         return;
     int b = order ? order[k] : n - 1 - k;
     uint4 w;
+    BodyShape sh = body_shape(B, b);
     if (part == 0)
     {
         unsigned id = ids ? ids[k] : (unsigned)k;
         unsigned dyn = B.massMoment[b].x > 0.0f ? 1u : 0u;
-        w = make_uint4(id, 0u, dyn, dyn);
+        // materialIdForBody (viewer_bridge.cpp:475-493)
+        unsigned mat = !dyn                        ? 0u
+                       : sh.type == SHAPE_SPHERE   ? 3u
+                       : sh.type == SHAPE_CYLINDER ? 4u
+                       : sh.type == SHAPE_CAPSULE  ? 5u
+                                                   : 1u;
+        w = make_uint4(id, (unsigned)sh.type, mat, dyn);
     }
     else if (part == 1)
     {
@@ -2127,7 +2165,9 @@ __global__ void k_snapshot_records(DevBodies B, const int *order, const unsigned
     else
     {
         float4 sz = B.sizeRad[b];
-        w = make_uint4(__float_as_uint(sz.y), __float_as_uint(sz.z), __float_as_uint(sz.w), 0u);
+        float radius = B.shape ? sh.radius : sz.w; // a box's shape radius is its bounding radius
+        w = make_uint4(__float_as_uint(sz.y), __float_as_uint(sz.z), __float_as_uint(radius),
+                       __float_as_uint(sh.halfLength));
     }
     out[4 * (size_t)k + part] = w;
 }
@@ -2243,7 +2283,8 @@ int avbd_snapshot_json(AvbdContext *ctx, uint64_t frame, const char *scene_name,
         memcpy(f, r + 16, 48);
         if (k)
             os << ",";
-        os << "{\"id\":" << w[0] << ",\"shape\":\"box\"" << ",\"position\":[" << f[0] << "," << f[1] << ","
+        static const char *names[4] = {"box", "sphere", "capsule", "cylinder"}; // shapeName (:458-473)
+        os << "{\"id\":" << w[0] << ",\"shape\":\"" << names[w[1] & 3] << "\"" << ",\"position\":[" << f[0] << "," << f[1] << ","
            << f[2] << "]" << ",\"rotation\":[" << f[3] << "," << f[4] << "," << f[5] << "," << f[6] << "]"
            << ",\"size\":[" << f[7] << "," << f[8] << "," << f[9] << "]" << ",\"radius\":" << f[10]
            << ",\"halfLength\":" << f[11] << ",\"dynamic\":" << (w[3] ? "true" : "false")

@@ -45,6 +45,7 @@ struct DevBodies
     float4 *dqLin, *dqAng;
     float4 *massMoment, *sizeRad;
     float *friction;
+    float4 *shape; // (type, radius, half length, 0) per body; null when every body is a box
 };
 
 struct DevManifolds
@@ -300,13 +301,17 @@ __global__ void k_bp_large(DevBodies B, const int *large, int nLarge, float dt, 
     float4 q = B.quat[b];
     float4 sr = B.sizeRad[b];
     float slack = len(xyz(B.vel[b])) * dt;
-    float3 e = mul(xyz(sr), 0.5f);
-    float3 cx = rotate(q, f3(1, 0, 0));
-    float3 cy = rotate(q, f3(0, 1, 0));
-    float3 cz = rotate(q, f3(0, 0, 1));
-    float3 h = f3(fabsf(cx.x) * e.x + fabsf(cy.x) * e.y + fabsf(cz.x) * e.z,
-                  fabsf(cx.y) * e.x + fabsf(cy.y) * e.y + fabsf(cz.y) * e.z,
-                  fabsf(cx.z) * e.x + fabsf(cy.z) * e.y + fabsf(cz.z) * e.z);
+    float3 h = f3(sr.w, sr.w, sr.w); // round shapes: the bounding radius (solver.cpp:315-326)
+    if (!B.shape || B.shape[b].x == 0.0f)
+    {
+        float3 e = mul(xyz(sr), 0.5f);
+        float3 cx = rotate(q, f3(1, 0, 0));
+        float3 cy = rotate(q, f3(0, 1, 0));
+        float3 cz = rotate(q, f3(0, 0, 1));
+        h = f3(fabsf(cx.x) * e.x + fabsf(cy.x) * e.y + fabsf(cz.x) * e.z,
+               fabsf(cx.y) * e.x + fabsf(cy.y) * e.y + fabsf(cz.y) * e.z,
+               fabsf(cx.z) * e.x + fabsf(cy.z) * e.y + fabsf(cz.z) * e.z);
+    }
     lo[k] = f4(sub(p, h), slack);
     hi[k] = f4(add(p, h), slack);
     sphere[k] = f4(p, sr.w);
@@ -1202,18 +1207,25 @@ AVBD_DEV void store_contact(float4 *c, const ContactRec &r)
 
 AVBD_DEV M3 load_basis(const float4 *b) { return rows(xyz(b[0]), xyz(b[1]), xyz(b[2])); }
 
-// Manifold::initialize for boxes (manifold.cpp:100-174): collide at q-, keep warm-start data
-// of contacts whose feature key persists, C0, lambda/penalty decay.
+#include "avbd_round.cuh"
+
+// Manifold::initialize (manifold.cpp:100-174): collide at q-, keep warm-start data of
+// contacts whose feature key persists, C0, lambda/penalty decay.
 __global__ void k_manifold_init(DevBodies B, DevManifolds M, int count, Params P, unsigned char *keep)
 {
     int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= count)
         return;
     int2 ab = M.ab[m];
-    float3 pA = xyz(B.pos[ab.x]), pB = xyz(B.pos[ab.y]);
-    float4 qA = B.quat[ab.x], qB = B.quat[ab.y];
-    float3 sA = xyz(B.sizeRad[ab.x]), sB = xyz(B.sizeRad[ab.y]);
+    NpBody A = np_body(B, ab.x), Bb = np_body(B, ab.y);
+    float3 pA = A.p, pB = Bb.p;
+    float4 qA = A.q, qB = Bb.q;
     float friction = sqrtf(B.friction[ab.x] * B.friction[ab.y]);
+    if (A.s.type == SHAPE_SPHERE || Bb.s.type == SHAPE_SPHERE)
+        friction = 0.0f;
+    // round contacts take the new locations every step and restart their tangential rows
+    // (manifold.cpp:120-147; cylinders count as round here)
+    const bool round = A.s.type != SHAPE_BOX || Bb.s.type != SHAPE_BOX;
     NewContact nc[8];
     for (int i = 0; i < 8; ++i)
     {
@@ -1222,7 +1234,8 @@ __global__ void k_manifold_init(DevBodies B, DevManifolds M, int count, Params P
         nc[i].rB = f3(0, 0, 0);
     }
     M3 basis = load_basis(M.basis + 3 * m);
-    int nn = collide_boxes(pA, qA, sA, pB, qB, sB, nc, basis);
+    int nn = round ? collide_shapes(A, Bb, P.dt, nc, basis)
+                   : collide_boxes(pA, qA, A.size, pB, qB, Bb.size, nc, basis);
     int nOld = M.n[m];
     float4 *cbase = M.contact + (size_t)m * 32;
     ContactRec merged[8];
@@ -1242,10 +1255,18 @@ __global__ void k_manifold_init(DevBodies B, DevManifolds M, int count, Params P
             if (o.key == nc[i].key)
             {
                 r = o;
-                if (!o.stick)
+                if (round || !o.stick)
                 {
                     r.rA = nc[i].rA;
                     r.rB = nc[i].rB;
+                }
+                if (round)
+                {
+                    r.lam.y = 0.0f;
+                    r.lam.z = 0.0f;
+                    r.pen.y = PENALTY_MIN;
+                    r.pen.z = PENALTY_MIN;
+                    r.stick = false;
                 }
                 break;
             }
@@ -1255,8 +1276,8 @@ __global__ void k_manifold_init(DevBodies B, DevManifolds M, int count, Params P
     for (int i = 0; i < nn; ++i)
     {
         ContactRec &c = merged[i];
-        float3 xA = add(pA, rotate(qA, c.rA));
-        float3 xB = add(pB, rotate(qB, c.rB));
+        float3 xA = add(pA, contact_offset(A.s, qA, c.rA, basis, true, c.key));
+        float3 xB = add(pB, contact_offset(Bb.s, qB, c.rB, basis, false, c.key));
         c.C0 = add(mv(basis, sub(xA, xB)), f3(COLLISION_MARGIN, 0, 0));
         c.lam = mul(mul(c.lam, P.alpha), P.gamma);
         c.pen = clampv(mul(c.pen, P.gamma), PENALTY_MIN, PENALTY_MAX);
@@ -1264,7 +1285,7 @@ __global__ void k_manifold_init(DevBodies B, DevManifolds M, int count, Params P
     }
     M.n[m] = nn;
     M.basis[3 * m + 0] = f4(basis.r0, friction);
-    M.basis[3 * m + 1] = f4(basis.r1, 0.0f);
+    M.basis[3 * m + 1] = f4(basis.r1, round ? ROUND_FLAG : 0.0f);
     M.basis[3 * m + 2] = f4(basis.r2, 0.0f);
     keep[m] = nn > 0 ? 1 : 0;
 }
@@ -1776,16 +1797,16 @@ AVBD_DEV void store_contact_state(float4 *cp, const ContactRec &c)
     cp[3] = make_float4(c.lam.x, c.lam.y, c.lam.z, __uint_as_float((unsigned)c.key | (c.stick ? 0x80000000u : 0u)));
 }
 
-AVBD_DEV ContactEval eval_contact(const Motion &A, const Motion &Bp, const M3 &basis, float friction,
-                                  const ContactRec &c, float alpha)
+// rAW, rBW: the contact's world offsets from the two bodies' centres (rotate(q, r) for boxes,
+// contactOffsetWorld for round bodies).
+AVBD_DEV ContactEval eval_contact_arms(const Motion &A, const Motion &Bp, const M3 &basis, float friction,
+                                       const ContactRec &c, float alpha, float3 rAW, float3 rBW)
 {
     ContactEval e;
     const float3 &dqALin = A.dLin;
     const float3 &dqAAng = A.dAng;
     const float3 &dqBLin = Bp.dLin;
     const float3 &dqBAng = Bp.dAng;
-    float3 rAW = rotate(A.q, c.rA);
-    float3 rBW = rotate(Bp.q, c.rB);
     e.jALin = basis;
     e.jBLin = mneg(basis);
     e.jAAng = rows(cross(rAW, e.jALin.r0), cross(rAW, e.jALin.r1), cross(rAW, e.jALin.r2));
@@ -1794,6 +1815,12 @@ AVBD_DEV ContactEval eval_contact(const Motion &A, const Motion &Bp, const M3 &b
               mv(e.jBAng, dqBAng));
     contact_force(e, c, friction);
     return e;
+}
+
+AVBD_DEV ContactEval eval_contact(const Motion &A, const Motion &Bp, const M3 &basis, float friction,
+                                  const ContactRec &c, float alpha)
+{
+    return eval_contact_arms(A, Bp, basis, friction, c, alpha, rotate(A.q, c.rA), rotate(Bp.q, c.rB));
 }
 
 AVBD_DEV ContactEval eval_contact(const Pose &A, const Pose &Bp, const M3 &basis, float friction,
@@ -2033,12 +2060,17 @@ AVBD_DEV unsigned contact_term_self(const DevBodies &B, const DevForces &F, unsi
                                     int partner, bool dual, const Params &P, float *t)
 {
     const float4 *bs = F.man.basis + 3 * (size_t)m;
-    float4 b0 = bs[0];
-    M3 basis = rows(xyz(b0), xyz(bs[1]), xyz(bs[2]));
+    float4 b0 = bs[0], b1 = bs[1];
+    M3 basis = rows(xyz(b0), xyz(b1), xyz(bs[2]));
     float4 *cp = F.man.contact + (size_t)m * 32 + 4 * ci;
     ContactRec c = load_contact<COH>(cp);
-    Motion A = load_motion<COH>(B, isA ? self : partner), Bm = load_motion<COH>(B, isA ? partner : self);
-    ContactEval e = eval_contact(A, Bm, basis, b0.w, c, P.alpha);
+    const int ia = isA ? self : partner, ib = isA ? partner : self;
+    Motion A = load_motion<COH>(B, ia), Bm = load_motion<COH>(B, ib);
+    ContactEval e = b1.w == 0.0f
+                        ? eval_contact(A, Bm, basis, b0.w, c, P.alpha)
+                        : eval_contact_arms(A, Bm, basis, b0.w, c, P.alpha,
+                                            contact_offset(body_shape(B, ia), A.q, c.rA, basis, true, c.key),
+                                            contact_offset(body_shape(B, ib), Bm.q, c.rB, basis, false, c.key));
     const M3 jLin = isA ? e.jALin : e.jBLin; // this body's rows, taken before the dual update
     const M3 jAng = isA ? e.jAAng : e.jBAng;
     if (dual)
@@ -2251,11 +2283,15 @@ AVBD_DEV void dual_contact_slot(const DevBodies &B, const DevManifolds &M, long 
     int2 ab = M.ab[m];
     Motion A = load_motion<COH>(B, ab.x), Bp = load_motion<COH>(B, ab.y);
     const float4 *bs = M.basis + 3 * (size_t)m;
-    float4 b0 = bs[0];
-    M3 basis = rows(xyz(b0), xyz(bs[1]), xyz(bs[2]));
+    float4 b0 = bs[0], b1 = bs[1];
+    M3 basis = rows(xyz(b0), xyz(b1), xyz(bs[2]));
     float4 *cp = M.contact + (size_t)m * 32 + 4 * ci;
     ContactRec c = load_contact<COH>(cp);
-    ContactEval e = eval_contact(A, Bp, basis, b0.w, c, P.alpha);
+    ContactEval e = b1.w == 0.0f
+                        ? eval_contact(A, Bp, basis, b0.w, c, P.alpha)
+                        : eval_contact_arms(A, Bp, basis, b0.w, c, P.alpha,
+                                            contact_offset(body_shape(B, ab.x), A.q, c.rA, basis, true, c.key),
+                                            contact_offset(body_shape(B, ab.y), Bp.q, c.rB, basis, false, c.key));
     contact_dual(c, e, P.betaLin);
     store_contact_state(cp, c);
 }

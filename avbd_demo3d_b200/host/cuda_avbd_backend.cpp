@@ -116,9 +116,9 @@ class CudaAvbdBackend : public PhysicsBackend
     bool checkShapes(Solver &solver)
     {
         for (Rigid *b = solver.bodies; b; b = b->next)
-            if (b->shape.type != RIGID_SHAPE_BOX)
+            if (b->shape.type < RIGID_SHAPE_BOX || b->shape.type > RIGID_SHAPE_CYLINDER)
             {
-                std::fprintf(stderr, "CUDA AVBD backend: only box bodies are supported\n");
+                std::fprintf(stderr, "CUDA AVBD backend: unknown body shape %d\n", (int)b->shape.type);
                 failed_ = true;
                 return false;
             }
@@ -264,7 +264,8 @@ class CudaAvbdBackend : public PhysicsBackend
 
     struct BodyArrays
     {
-        std::vector<float> pos, quat, vel, ang, prev, size, mass, moment, friction, radius;
+        std::vector<float> pos, quat, vel, ang, prev, size, mass, moment, friction, radius, shapeRadius, halfLength;
+        std::vector<int32_t> shape;
     };
 
     void gatherBodies(BodyArrays &a) const
@@ -280,6 +281,9 @@ class CudaAvbdBackend : public PhysicsBackend
         a.moment.resize(3 * n);
         a.friction.resize(n);
         a.radius.resize(n);
+        a.shape.resize(n);
+        a.shapeRadius.resize(n);
+        a.halfLength.resize(n);
         for (size_t i = 0; i < n; ++i)
         {
             const Rigid *b = bodies_[i];
@@ -293,14 +297,28 @@ class CudaAvbdBackend : public PhysicsBackend
             std::memcpy(&a.moment[3 * i], &b->moment, 12);
             a.friction[i] = b->friction;
             a.radius[i] = b->radius;
+            a.shape[i] = (int32_t)b->shape.type; // RigidShapeType values are the ABI's AVBD_SHAPE_*
+            a.shapeRadius[i] = b->shape.radius;
+            a.halfLength[i] = b->shape.halfLength;
         }
     }
 
     static AvbdBodies view(int n, const BodyArrays &a)
     {
-        return AvbdBodies{n,         a.pos.data(),    a.quat.data(),   a.vel.data(),      a.ang.data(),
-                          a.prev.data(), a.size.data(), a.mass.data(), a.moment.data(), a.friction.data(),
-                          a.radius.data()};
+        return AvbdBodies{n,
+                          a.pos.data(),
+                          a.quat.data(),
+                          a.vel.data(),
+                          a.ang.data(),
+                          a.prev.data(),
+                          a.size.data(),
+                          a.mass.data(),
+                          a.moment.data(),
+                          a.friction.data(),
+                          a.radius.data(),
+                          a.shape.data(),
+                          a.shapeRadius.data(),
+                          a.halfLength.data()};
     }
 
     bool pushBodyState(Solver &)

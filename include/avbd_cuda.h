@@ -42,6 +42,12 @@ extern "C" {
 #define AVBD_BROADPHASE_GRID 1
 #define AVBD_BROADPHASE_SAP 2
 
+/* Body shapes (RigidShapeType, solver.h:47-53). */
+#define AVBD_SHAPE_BOX 0
+#define AVBD_SHAPE_SPHERE 1
+#define AVBD_SHAPE_CAPSULE 2
+#define AVBD_SHAPE_CYLINDER 3
+
 /* How a step runs its solver iterations (avbd_set_iteration_mode). */
 #define AVBD_ITERATIONS_PER_COLOUR 0 /* one launch per colour and iteration, then the dual sweep */
 #define AVBD_ITERATIONS_PERSISTENT 1 /* all iterations in one cooperative launch (default) */
@@ -69,7 +75,7 @@ typedef struct AvbdParams
 
 /* Rigid state and properties (Rigid, solver.h:197-228), arrays of n entries in list order.
  * position3/velocity3/angular3/prev_velocity3/size3/moment3 hold 3 floats per body,
- * orientation4 holds x, y, z, w. Boxes only (RigidShape::type == RIGID_SHAPE_BOX). */
+ * orientation4 holds x, y, z, w. */
 typedef struct AvbdBodies
 {
     int32_t count;
@@ -83,6 +89,14 @@ typedef struct AvbdBodies
     const float *moment3;
     const float *friction;
     const float *radius;
+    /* Shapes (RigidShape, solver.h:55-61; Rigid::makeSphere / makeCapsule / makeCylinder,
+     * rigid.cpp:44-90), read when the world is loaded; NULL: every body is a box. shape:
+     * AVBD_SHAPE_*; shape_radius: RigidShape::radius (a box's is length(size / 2));
+     * half_length: capsule and cylinder half length (0 otherwise). size3 holds the shape's
+     * bounding widths and radius the body's bounding radius, as on Rigid. */
+    const int32_t *shape;
+    const float *shape_radius;
+    const float *half_length;
 } AvbdBodies;
 
 /* Body state written back after a step. Any pointer may be NULL to skip that field. */
@@ -259,8 +273,9 @@ int avbd_next_seq(AvbdContext *ctx, int64_t *next_seq);
  * is decodeBinarySnapshot, viewer/src/main.js:986-1050).
  * Binary ("AVBS"): u32 magic 0x53425641, u32 version 1, u64 frame, u32 scene bytes, u32
  * body count, the scene name, then per body in ascending id order 64 bytes: u32 id, shape
- * (0 = box), material (0 static, 1 dynamic box), dynamic; f32 position[3], rotation[4]
- * (x y z w), size[3] (full widths), radius, half length. JSON: the same fields as text,
+ * (AVBD_SHAPE_*), material (materialIdForBody: 0 static, 1 box, 3 sphere, 4 cylinder,
+ * 5 capsule), dynamic; f32 position[3], rotation[4] (x y z w), size[3] (full widths), shape
+ * radius, half length. JSON: the same fields as text,
  * numbers with 5 decimals.
  * body_id: the SimWorld dense id of each body (list order), or NULL for the creation rank
  * (the dense id of a world built without deletions). *size receives the bytes needed

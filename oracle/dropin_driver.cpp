@@ -7,7 +7,8 @@
  *     relinked into the sweep order read from the device, iteratePrimalDualCpu,
  *     finishStep): must be bit-identical.
  * With --commands, every host gets the same scripted bridge commands between frames
- * (drag begin / move / end, iterations, broadphase, time step, gravity).
+ * (drag begin / move / end, iterations, broadphase, time step, gravity); --round runs the
+ * reference's scenes with spheres, capsules and cylinders (and the cloth and soft body).
  * Built by oracle/Makefile (target `dropin`) from the reference's sources plus the
  * adapter avbd_demo3d_b200/host/cuda_avbd_backend.cpp; prints one JSON line per scene.
  */
@@ -154,6 +155,17 @@ int main(int argc, char **argv)
             frames = std::atoi(argv[++i]);
         else if (!std::strcmp(argv[i], "--commands"))
             commands = true;
+        else if (!std::strcmp(argv[i], "--round"))
+            names = {"Sphere Stack", "Sphere Ramp", "Capsule Stack", "Capsule Ramp", "Cylinder Stack",
+                     "Cylinder Ramp", "Sphere Pour on Cylinders", "Sphere Pour 5000 on Cylinders",
+                     "Sphere Sphere Contact Probe", "Sphere Cylinder Contact Probe", "Sphere Capsule Contact Probe",
+                     "Sphere Box Contact Probe", "Sphere Rotated Cylinder Contact Probe",
+                     "Sphere Rotated Capsule Contact Probe", "Sphere Rotated Box Contact Probe",
+                     "Sphere Dynamic Rotated Cylinder Contact Probe", "Sphere Dynamic Rotated Capsule Contact Probe",
+                     "Sphere Dynamic Rotated Box Contact Probe", "Capsule Capsule Contact Probe",
+                     "Cylinder Cylinder Contact Probe", "Capsule Cylinder Contact Probe",
+                     "Rotated Capsule Cylinder Contact Probe", "Mixed Primitive Contact Probe",
+                     "Capsule Box Contact Probe", "Cylinder Box Contact Probe", "Cloth", "Soft Body"};
         else
             names.push_back(argv[i]);
     }

@@ -49,7 +49,7 @@ def test_header_constants_match_binding():
 
 def test_struct_sizes_match_header_layout():
     # plain C layouts: int32 count + pointers, all 8-byte aligned on x86-64
-    assert ctypes.sizeof(_lib.AvbdBodies) == 8 + 10 * 8
+    assert ctypes.sizeof(_lib.AvbdBodies) == 8 + 13 * 8
     assert ctypes.sizeof(_lib.AvbdParams) == 32
     assert ctypes.sizeof(_lib.AvbdStats) == 14 * 8 + 8
 

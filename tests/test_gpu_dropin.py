@@ -46,3 +46,19 @@ def test_bridge_commands_through_the_backend_adapter(gpu):
     dragged = [r for r in rows if r["joint_edits"] > 0]
     assert len(dragged) >= 10, rows  # every scene with a dynamic body was dragged
     assert out.returncode == 0, out.stderr
+
+
+def test_round_shape_scenes_through_the_backend_adapter(gpu):
+    """The reference's scenes with spheres, capsules and cylinders (stacks, ramps, the sphere
+    pours on cylinders, every contact probe), the sphere cloth and the soft body: the round
+    narrowphase, contact offsets and sphere rolling friction on the GPU stay bit-exact with
+    the reference's CPU solver in the GPU's colour order."""
+    if not os.path.exists(DROPIN):
+        pytest.skip("drop-in harness not built (needs the reference sources: make -C oracle dropin)")
+    out = subprocess.run([DROPIN, "--frames", "120", "--round"], capture_output=True, text=True, timeout=1200)
+    rows = [json.loads(l) for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(rows) == 27, out.stdout + out.stderr
+    for r in rows:
+        assert r["backend"].startswith("CUDA AVBD"), r
+        assert r["bit_exact_vs_colour_order_reference"], r
+    assert out.returncode == 0, out.stderr

@@ -70,20 +70,37 @@ static int dynamic_body(const SimulationHost &h, int nth)
 
 // A scripted session of the bridge's commands (SimulationHost::applyCommand,
 // simulation_host.cpp:121-226), given before frame f: drag one body along a path,
-// release it, drag another (a new joint, possibly at the freed address), change the
-// iteration count, broadphase, time step and gravity.
-static void apply_commands(SimulationHost &h, int f, float3 &anchor)
+// release it, drag another (a new joint, possibly at the freed address), import a closed
+// cube mesh as a soft lattice (simulation_host.cpp:376-493), change the iteration count,
+// broadphase, time step and gravity. Returns true when the import created bodies.
+static bool apply_commands(SimulationHost &h, int f, float3 &anchor)
 {
+    bool imported = false;
     auto cmd = [&](const char *name) {
         SimulationCommand c;
         c.command = name;
         return c;
     };
+    if (f == 50)
+    {
+        SimulationCommand c = cmd("importMesh");
+        c.meshName = "cube";
+        c.meshMode = "soft";
+        const float v[24] = {-1, -1, -1, 1, -1, -1, 1, 1, -1, -1, 1, -1, -1, -1, 1, 1, -1, 1, 1, 1, 1, -1, 1, 1};
+        const uint32_t t[36] = {0, 2, 1, 0, 3, 2, 4, 5, 6, 4, 6, 7, 0, 1, 5, 0, 5, 4,
+                                1, 2, 6, 1, 6, 5, 2, 3, 7, 2, 7, 6, 3, 0, 4, 3, 4, 7};
+        c.meshVertices.assign(v, v + 24);
+        c.meshTriangles.assign(t, t + 36);
+        c.meshPosition = float3{0.0f, 0.0f, 7.0f};
+        c.hasMeshPosition = true;
+        imported = h.applyCommand(c);
+        h.takeOutboundMessages();
+    }
     if (f == 5 || f == 70)
     {
         int id = dynamic_body(h, f == 5 ? 0 : 1);
         if (id < 0)
-            return;
+            return imported;
         SimulationCommand c = cmd("beginDrag");
         c.bodyId = (uint32_t)id;
         c.hasBodyId = true;
@@ -131,6 +148,7 @@ static void apply_commands(SimulationHost &h, int f, float3 &anchor)
         c.hasNumber = true;
         h.applyCommand(c);
     }
+    return imported;
 }
 
 static double qdist(quat a, quat b)
@@ -165,7 +183,8 @@ int main(int argc, char **argv)
                      "Sphere Dynamic Rotated Box Contact Probe", "Capsule Capsule Contact Probe",
                      "Cylinder Cylinder Contact Probe", "Capsule Cylinder Contact Probe",
                      "Rotated Capsule Cylinder Contact Probe", "Mixed Primitive Contact Probe",
-                     "Capsule Box Contact Probe", "Cylinder Box Contact Probe", "Cloth", "Soft Body"};
+                     "Capsule Box Contact Probe", "Cylinder Box Contact Probe", "Cloth", "Soft Body",
+                     "Soft Body 8x8x8", "Newton's Cradle", "Mesh Torus Soft+Rigid", "Empty"};
         else
             names.push_back(argv[i]);
     }
@@ -190,11 +209,12 @@ int main(int argc, char **argv)
         double maxPos = 0, maxRot = 0, sumSq = 0;
         long count = 0;
         float3 anchors[3] = {};
+        bool imported = false;
         for (int f = 1; f <= frames; ++f)
         {
             if (commands)
             {
-                apply_commands(gpu, f, anchors[0]);
+                imported |= apply_commands(gpu, f, anchors[0]);
                 apply_commands(cpu, f, anchors[1]);
                 apply_commands(colour, f, anchors[2]);
             }
@@ -243,11 +263,12 @@ int main(int argc, char **argv)
         std::printf("{\"scene\": \"%s\", \"commands\": %s, \"backend\": \"%s\", \"frames\": %d, \"bodies\": %d, \"manifolds\": %d, "
                     "\"bit_exact_vs_colour_order_reference\": %s, \"first_mismatch_frame\": %d, "
                     "\"max_position_error_vs_cpu_backend\": %.6g, \"rms_position_error_vs_cpu_backend\": %.6g, "
-                    "\"max_rotation_error_vs_cpu_backend\": %.6g, \"world_uploads\": %d, \"joint_edits\": %d}\n",
+                    "\"max_rotation_error_vs_cpu_backend\": %.6g, \"world_uploads\": %d, \"joint_edits\": %d, "
+                    "\"mesh_imported\": %s}\n",
                     name.c_str(), commands ? "true" : "false", gpu.solver().physicsBackend->name(), frames, (int)list_of(gpu.solver()).size(),
                     gm, exact ? "true" : "false", firstMismatch, maxPos, count ? std::sqrt(sumSq / count) : 0.0,
                     maxRot, cudaAvbdBackendUploads(gpu.solver().physicsBackend.get()),
-                    cudaAvbdBackendJointEdits(gpu.solver().physicsBackend.get()));
+                    cudaAvbdBackendJointEdits(gpu.solver().physicsBackend.get()), imported ? "true" : "false");
         std::fflush(stdout);
     }
     return failures ? 1 : 0;

@@ -31,7 +31,8 @@ def test_reference_scenes_through_the_backend_adapter(gpu):
 
 def test_bridge_commands_through_the_backend_adapter(gpu):
     """The bridge's commands between frames on every scene (drag begin / move / end twice,
-    setIterations, setBroadphase sap, setDt, setGravity): the adapter turns the drag joint's
+    importMesh of a closed cube as a soft sphere lattice, setIterations, setBroadphase sap,
+    setDt, setGravity): the adapter turns the drag joint's
     creation, anchor moves and deletion into device joint edits and stays bit-exact with
     the reference's CPU solver in the GPU's colour order."""
     if not os.path.exists(DROPIN):
@@ -42,23 +43,38 @@ def test_bridge_commands_through_the_backend_adapter(gpu):
     for r in rows:
         assert r["commands"] and r["backend"].startswith("CUDA AVBD"), r
         assert r["bit_exact_vs_colour_order_reference"], r
-        assert r["world_uploads"] == 1, r  # drags are joint edits, not reloads
+        # drags are joint edits, not reloads; the mesh import adds bodies and reloads once
+        assert r["world_uploads"] == 1 + (1 if r["mesh_imported"] else 0), r
     dragged = [r for r in rows if r["joint_edits"] > 0]
     assert len(dragged) >= 10, rows  # every scene with a dynamic body was dragged
+    assert sum(r["mesh_imported"] for r in rows) >= 10, rows  # the cube lattice was built
     assert out.returncode == 0, out.stderr
 
 
 def test_round_shape_scenes_through_the_backend_adapter(gpu):
     """The reference's scenes with spheres, capsules and cylinders (stacks, ramps, the sphere
-    pours on cylinders, every contact probe), the sphere cloth and the soft body: the round
+    pours on cylinders, every contact probe, Newton's cradle, the mesh-lattice torus), the
+    sphere cloth and the soft bodies: the round
     narrowphase, contact offsets and sphere rolling friction on the GPU stay bit-exact with
     the reference's CPU solver in the GPU's colour order."""
     if not os.path.exists(DROPIN):
         pytest.skip("drop-in harness not built (needs the reference sources: make -C oracle dropin)")
     out = subprocess.run([DROPIN, "--frames", "120", "--round"], capture_output=True, text=True, timeout=1200)
     rows = [json.loads(l) for l in out.stdout.splitlines() if l.startswith("{")]
-    assert len(rows) == 27, out.stdout + out.stderr
+    assert len(rows) == 31, out.stdout + out.stderr
     for r in rows:
         assert r["backend"].startswith("CUDA AVBD"), r
         assert r["bit_exact_vs_colour_order_reference"], r
     assert out.returncode == 0, out.stderr
+
+
+def test_sphere_pour_20000(gpu):
+    """The largest reference scene (20,000 spheres poured on cylinders) for its first 20
+    frames, bit-exact in the GPU's colour order."""
+    if not os.path.exists(DROPIN):
+        pytest.skip("drop-in harness not built (needs the reference sources: make -C oracle dropin)")
+    out = subprocess.run([DROPIN, "--frames", "20", "Sphere Pour 20000 on Cylinders"], capture_output=True, text=True,
+                         timeout=1200)
+    rows = [json.loads(l) for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(rows) == 1 and rows[0]["bodies"] > 20000, out.stdout + out.stderr
+    assert rows[0]["bit_exact_vs_colour_order_reference"], rows[0]

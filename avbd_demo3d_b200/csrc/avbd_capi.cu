@@ -66,6 +66,7 @@ const PrimalVariant kPrimalVariants[] = {
     {4, 8, k_primal<4, PRIMAL_BLOCK, 8>},   {2, 8, k_primal<2, PRIMAL_BLOCK, 8>},
 };
 constexpr int kNumPrimalVariants = (int)(sizeof(kPrimalVariants) / sizeof(kPrimalVariants[0]));
+const PrimalVariant kRoundPrimal = {4, 1, k_primal<4, PRIMAL_BLOCK, 1, true>}; // worlds with round bodies
 
 } // namespace
 
@@ -166,6 +167,7 @@ struct AvbdContext
     size_t hGridCap = 0;
     int *hCapped = nullptr;        // pinned: any world over the cell cap
     float4 *hStage = nullptr;      // pinned staging for body state transfers
+    DArr<float> stateStage;        // the same on the device: body state in the callers' packed layout
     size_t hStageCap = 0;
     cudaEvent_t stageDone = nullptr; // staging copies issued before this event are complete
 
@@ -834,7 +836,10 @@ int init_forces(AvbdContext *ctx)
     if (M)
     {
         DevManifolds Md = dev_man(ctx->man[ctx->cur]);
-        k_manifold_init<<<grid_for(M, 128), 128, 0, ctx->stream>>>(B, Md, M, P, ctx->keep.p);
+        if (ctx->hasShapes)
+            k_manifold_init<true><<<grid_for(M, 128), 128, 0, ctx->stream>>>(B, Md, M, P, ctx->keep.p);
+        else
+            k_manifold_init<false><<<grid_for(M, 128), 128, 0, ctx->stream>>>(B, Md, M, P, ctx->keep.p);
         LAUNCHED();
         k_u8_to_int<<<grid_for(M, 256), 256, 0, ctx->stream>>>(ctx->keep.p, cnt32, M);
         LAUNCHED();
@@ -967,7 +972,10 @@ int iterate_persistent(AvbdContext *ctx)
     void *args[] = {&B, &F, &P, &entries, &colourStart, &nColours, &iterations, &sync};
     {
         PhaseScope ps(ctx, AVBD_PHASE_PRIMAL);
-        CU(cudaLaunchCooperativeKernel((void *)k_iterations<ITER_G, ITER_BLOCK, ITER_SUB>, ctx->iterBlocks, ITER_BLOCK, args,
+        // worlds with round bodies run the instance that evaluates their contact offsets
+        void *kernel = ctx->hasShapes ? (void *)k_iterations<ITER_G, ITER_BLOCK, ITER_SUB, true>
+                                      : (void *)k_iterations<ITER_G, ITER_BLOCK, ITER_SUB, false>;
+        CU(cudaLaunchCooperativeKernel(kernel, ctx->iterBlocks, ITER_BLOCK, args,
                                        sizeof(PrimalShared<ITER_G, ITER_BLOCK>), ctx->stream));
         LAUNCHED();
     }
@@ -983,7 +991,8 @@ int iterate(AvbdContext *ctx)
     DevBodies B = dev_bodies(ctx);
     DevForces F = dev_forces(ctx);
     Params P = dev_params(ctx->params);
-    const PrimalVariant &pv = kPrimalVariants[ctx->primalVariant];
+    // worlds with round bodies: the one instance that evaluates their contact offsets
+    const PrimalVariant &pv = ctx->hasShapes ? kRoundPrimal : kPrimalVariants[ctx->primalVariant];
     const int GPB = PRIMAL_BLOCK / pv.group;
     for (int it = 0; it < ctx->params.iterations; ++it)
     {
@@ -1003,7 +1012,10 @@ int iterate(AvbdContext *ctx)
         PhaseScope ps(ctx, AVBD_PHASE_DUAL);
         if (ctx->nMan)
         {
-            k_dual_contacts<<<grid_for(8ll * ctx->nMan, 256), 256, 0, ctx->stream>>>(B, F.man, ctx->nMan, P);
+            if (ctx->hasShapes)
+                k_dual_contacts<true><<<grid_for(8ll * ctx->nMan, 256), 256, 0, ctx->stream>>>(B, F.man, ctx->nMan, P);
+            else
+                k_dual_contacts<false><<<grid_for(8ll * ctx->nMan, 256), 256, 0, ctx->stream>>>(B, F.man, ctx->nMan, P);
             LAUNCHED();
         }
         if (ctx->nJoint)
@@ -1094,42 +1106,101 @@ int stage_reserve(AvbdContext *ctx, size_t count)
     return AVBD_OK;
 }
 
-// Body state from caller arrays (3 or 4 floats per body) into pinned staging, then one
-// asynchronous copy per field.
+// Body state fields in the callers' packed layout: per field n entries of `width` floats
+// (3, or 4 for orientations) at `offset` floats into one buffer (-1: field absent).
+struct PackedField
+{
+    float4 *arr;
+    long long offset;
+    int width;
+    float w; // fourth component written for an absent field
+};
+
+constexpr int MAX_PACKED = 9;
+struct PackedFields
+{
+    PackedField f[MAX_PACKED];
+    int count;
+};
+
+// Packed caller layout -> the device's float4 arrays (absent fields take (0, 0, 0, w)).
+__global__ void k_unpack_state(PackedFields P, const float *in, int n)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+#pragma unroll
+    for (int k = 0; k < MAX_PACKED; ++k)
+    {
+        if (k >= P.count)
+            break;
+        const PackedField f = P.f[k];
+        float4 v = make_float4(0.0f, 0.0f, 0.0f, f.w);
+        if (f.offset >= 0)
+        {
+            const float *s = in + f.offset + (size_t)f.width * i;
+            v = f.width == 4 ? make_float4(s[0], s[1], s[2], s[3]) : make_float4(s[0], s[1], s[2], 0.0f);
+        }
+        f.arr[i] = v;
+    }
+}
+
+// The device's float4 arrays -> the packed caller layout (requested fields only).
+__global__ void k_pack_state(PackedFields P, float *out, int n)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+#pragma unroll
+    for (int k = 0; k < MAX_PACKED; ++k)
+    {
+        if (k >= P.count)
+            break;
+        const PackedField f = P.f[k];
+        if (f.offset < 0)
+            continue;
+        float4 v = f.arr[i];
+        float *d = out + f.offset + (size_t)f.width * i;
+        d[0] = v.x;
+        d[1] = v.y;
+        d[2] = v.z;
+        if (f.width == 4)
+            d[3] = v.w;
+    }
+}
+
+// Body state from caller arrays: one copy of the packed fields into pinned staging, one
+// asynchronous upload, and the conversion to float4 on the device.
 int write_state(AvbdContext *ctx, const AvbdBodies *b)
 {
     int n = b->count;
-    CHECK(stage_reserve(ctx, (size_t)5 * n));
-    struct F
-    {
-        const float *src;
-        int width;
-        DArr<float4> *dst;
-        float w;
-    } fields[] = {{b->position3, 3, &ctx->pos, 0.0f},
-                  {b->orientation4, 4, &ctx->quat, 1.0f},
-                  {b->velocity3, 3, &ctx->vel, 0.0f},
-                  {b->angular3, 3, &ctx->angvel, 0.0f},
-                  {b->prev_velocity3 ? b->prev_velocity3 : b->velocity3, 3, &ctx->prevVel, 0.0f}};
+    const float *src[5] = {b->position3, b->orientation4, b->velocity3, b->angular3,
+                           b->prev_velocity3 ? b->prev_velocity3 : b->velocity3};
+    DArr<float4> *dst[5] = {&ctx->pos, &ctx->quat, &ctx->vel, &ctx->angvel, &ctx->prevVel};
+    const int width[5] = {3, 4, 3, 3, 3};
+    PackedFields P{};
+    P.count = 5;
+    long long floats = 0;
     for (int f = 0; f < 5; ++f)
     {
-        float4 *st = ctx->hStage + (size_t)f * n;
-        const float *src = fields[f].src;
-        int wdt = fields[f].width;
-        for (int i = 0; i < n; ++i)
-        {
-            if (!src)
-                st[i] = wdt == 4 ? make_float4(0, 0, 0, 1) : make_float4(0, 0, 0, 0);
-            else if (wdt == 4)
-                st[i] = make_float4(src[4 * i], src[4 * i + 1], src[4 * i + 2], src[4 * i + 3]);
-            else
-                st[i] = make_float4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.0f);
-        }
-        CHECK(reserve(ctx, *fields[f].dst, std::max(n, 1), false));
-        if (n)
-            CU(cudaMemcpyAsync(fields[f].dst->p, st, sizeof(float4) * n, cudaMemcpyHostToDevice, ctx->stream));
+        CHECK(reserve(ctx, *dst[f], std::max(n, 1), false));
+        P.f[f] = PackedField{dst[f]->p, src[f] ? floats : -1, width[f], f == 1 ? 1.0f : 0.0f};
+        if (src[f])
+            floats += (long long)width[f] * n;
     }
+    if (!n)
+        return AVBD_OK;
+    CHECK(stage_reserve(ctx, (size_t)(floats + 3) / 4));
+    float *st = (float *)ctx->hStage;
+    for (int f = 0; f < 5; ++f)
+        if (src[f])
+            memcpy(st + P.f[f].offset, src[f], sizeof(float) * width[f] * (size_t)n);
+    CHECK(reserve(ctx, ctx->stateStage, (size_t)std::max<long long>(floats, 1), false));
+    if (floats)
+        CU(cudaMemcpyAsync(ctx->stateStage.p, st, sizeof(float) * floats, cudaMemcpyHostToDevice, ctx->stream));
     CU(cudaEventRecord(ctx->stageDone, ctx->stream));
+    k_unpack_state<<<grid_for(n, 256), 256, 0, ctx->stream>>>(P, ctx->stateStage.p, n);
+    LAUNCHED();
     return AVBD_OK;
 }
 
@@ -1341,11 +1412,16 @@ int avbd_create(AvbdContext **out, int32_t device_ordinal, void *cuda_stream)
         // the iteration kernel: one block of ITER_BLOCK threads per SM with its shared batch
         int iterSm = 0;
         size_t smem = sizeof(PrimalShared<ITER_G, ITER_BLOCK>);
-        if (cudaFuncSetAttribute((const void *)k_iterations<ITER_G, ITER_BLOCK, ITER_SUB>,
+        int roundSm = 0;
+        if (cudaFuncSetAttribute((const void *)k_iterations<ITER_G, ITER_BLOCK, ITER_SUB, false>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess &&
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&iterSm, k_iterations<ITER_G, ITER_BLOCK, ITER_SUB>, ITER_BLOCK,
-                                                          smem) == cudaSuccess)
-            ctx->iterBlocks = sms * iterSm;
+            cudaFuncSetAttribute((const void *)k_iterations<ITER_G, ITER_BLOCK, ITER_SUB, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&iterSm, k_iterations<ITER_G, ITER_BLOCK, ITER_SUB, false>,
+                                                          ITER_BLOCK, smem) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&roundSm, k_iterations<ITER_G, ITER_BLOCK, ITER_SUB, true>,
+                                                          ITER_BLOCK, smem) == cudaSuccess)
+            ctx->iterBlocks = sms * std::min(iterSm, roundSm);
         cudaGetLastError(); // an unsupported configuration only leaves the per-colour launches
     }
     if (reserve(ctx, ctx->counters, 1, false) || reserve(ctx, ctx->bounds, 8, false) ||
@@ -1428,6 +1504,7 @@ void avbd_destroy(AvbdContext *ctx)
         release(ctx->jointSeq[k]);
     }
     release(ctx->shape);
+    release(ctx->stateStage);
     release(ctx->snapIds);
     release(ctx->snapIdsAlt);
     release(ctx->snapOrder);
@@ -1777,44 +1854,36 @@ int avbd_read_bodies(AvbdContext *ctx, const AvbdBodyState *out)
     if (!ctx || !out)
         return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
     int n = ctx->n;
-    struct Field
-    {
-        DArr<float4> *src;
-        float *dst;
-        int width;
-    } fields[] = {{&ctx->pos, out->position3, 3},
-                  {&ctx->quat, out->orientation4, 4},
-                  {&ctx->vel, out->velocity3, 3},
-                  {&ctx->angvel, out->angular3, 3},
-                  {&ctx->prevVel, out->prev_velocity3, 3},
-                  {&ctx->initLin, out->initial_position3, 3},
-                  {&ctx->initAng, out->initial_orientation4, 4},
-                  {&ctx->inertLin, out->inertial_position3, 3},
-                  {&ctx->inertAng, out->inertial_orientation4, 4}};
+    DArr<float4> *src[MAX_PACKED] = {&ctx->pos,     &ctx->quat,    &ctx->vel,      &ctx->angvel,  &ctx->prevVel,
+                                     &ctx->initLin, &ctx->initAng, &ctx->inertLin, &ctx->inertAng};
+    float *dst[MAX_PACKED] = {out->position3,         out->orientation4,         out->velocity3,
+                              out->angular3,          out->prev_velocity3,       out->initial_position3,
+                              out->initial_orientation4, out->inertial_position3, out->inertial_orientation4};
+    const int width[MAX_PACKED] = {3, 4, 3, 3, 3, 3, 4, 3, 4};
     if (!n)
         return AVBD_OK;
-    CHECK(stage_reserve(ctx, (size_t)9 * n));
-    for (int f = 0; f < 9; ++f)
-        if (fields[f].dst)
-            CU(cudaMemcpyAsync(ctx->hStage + (size_t)f * n, fields[f].src->p, sizeof(float4) * n,
-                               cudaMemcpyDeviceToHost, ctx->stream));
-    CU(cudaStreamSynchronize(ctx->stream));
-    for (int f = 0; f < 9; ++f)
+    // requested fields packed on the device, one download, one copy per field on the host
+    PackedFields P{};
+    P.count = MAX_PACKED;
+    long long floats = 0;
+    for (int f = 0; f < MAX_PACKED; ++f)
     {
-        float *d = fields[f].dst;
-        if (!d)
-            continue;
-        const float4 *st = ctx->hStage + (size_t)f * n;
-        if (fields[f].width == 4)
-            memcpy(d, st, sizeof(float4) * n);
-        else
-            for (int i = 0; i < n; ++i)
-            {
-                d[3 * i] = st[i].x;
-                d[3 * i + 1] = st[i].y;
-                d[3 * i + 2] = st[i].z;
-            }
+        P.f[f] = PackedField{src[f]->p, dst[f] ? floats : -1, width[f], 0.0f};
+        if (dst[f])
+            floats += (long long)width[f] * n;
     }
+    if (!floats)
+        return AVBD_OK;
+    CHECK(stage_reserve(ctx, (size_t)(floats + 3) / 4));
+    CHECK(reserve(ctx, ctx->stateStage, (size_t)floats, false));
+    k_pack_state<<<grid_for(n, 256), 256, 0, ctx->stream>>>(P, ctx->stateStage.p, n);
+    LAUNCHED();
+    float *st = (float *)ctx->hStage;
+    CU(cudaMemcpyAsync(st, ctx->stateStage.p, sizeof(float) * floats, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    for (int f = 0; f < MAX_PACKED; ++f)
+        if (dst[f])
+            memcpy(dst[f], st + P.f[f].offset, sizeof(float) * width[f] * (size_t)n);
     return AVBD_OK;
 }
 

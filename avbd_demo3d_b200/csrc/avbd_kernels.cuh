@@ -1211,6 +1211,7 @@ AVBD_DEV M3 load_basis(const float4 *b) { return rows(xyz(b[0]), xyz(b[1]), xyz(
 
 // Manifold::initialize (manifold.cpp:100-174): collide at q-, keep warm-start data of
 // contacts whose feature key persists, C0, lambda/penalty decay.
+template <bool ROUND>
 __global__ void k_manifold_init(DevBodies B, DevManifolds M, int count, Params P, unsigned char *keep)
 {
     int m = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1221,11 +1222,11 @@ __global__ void k_manifold_init(DevBodies B, DevManifolds M, int count, Params P
     float3 pA = A.p, pB = Bb.p;
     float4 qA = A.q, qB = Bb.q;
     float friction = sqrtf(B.friction[ab.x] * B.friction[ab.y]);
-    if (A.s.type == SHAPE_SPHERE || Bb.s.type == SHAPE_SPHERE)
+    if (ROUND && (A.s.type == SHAPE_SPHERE || Bb.s.type == SHAPE_SPHERE))
         friction = 0.0f;
     // round contacts take the new locations every step and restart their tangential rows
-    // (manifold.cpp:120-147; cylinders count as round here)
-    const bool round = A.s.type != SHAPE_BOX || Bb.s.type != SHAPE_BOX;
+    // (manifold.cpp:120-147; cylinders count as round here); ROUND: the world has round bodies
+    const bool round = ROUND && (A.s.type != SHAPE_BOX || Bb.s.type != SHAPE_BOX);
     NewContact nc[8];
     for (int i = 0; i < 8; ++i)
     {
@@ -2055,7 +2056,7 @@ __global__ void k_entry_fill(DevForces F, const int *entryRow, const int *count,
 
 // Contact row of body `self` against its partner (Manifold::updatePrimal,
 // manifold.cpp:183-228); the partner comes from the row entry.
-template <bool COH = false>
+template <bool COH = false, bool ROUND = false>
 AVBD_DEV unsigned contact_term_self(const DevBodies &B, const DevForces &F, unsigned m, int ci, bool isA, int self,
                                     int partner, bool dual, const Params &P, float *t)
 {
@@ -2066,11 +2067,12 @@ AVBD_DEV unsigned contact_term_self(const DevBodies &B, const DevForces &F, unsi
     ContactRec c = load_contact<COH>(cp);
     const int ia = isA ? self : partner, ib = isA ? partner : self;
     Motion A = load_motion<COH>(B, ia), Bm = load_motion<COH>(B, ib);
-    ContactEval e = b1.w == 0.0f
-                        ? eval_contact(A, Bm, basis, b0.w, c, P.alpha)
-                        : eval_contact_arms(A, Bm, basis, b0.w, c, P.alpha,
+    // ROUND: the world has round bodies, whose manifolds are flagged in basis row 1
+    ContactEval e = ROUND && b1.w != 0.0f
+                        ? eval_contact_arms(A, Bm, basis, b0.w, c, P.alpha,
                                             contact_offset(body_shape(B, ia), A.q, c.rA, basis, true, c.key),
-                                            contact_offset(body_shape(B, ib), Bm.q, c.rB, basis, false, c.key));
+                                            contact_offset(body_shape(B, ib), Bm.q, c.rB, basis, false, c.key))
+                        : eval_contact(A, Bm, basis, b0.w, c, P.alpha);
     const M3 jLin = isA ? e.jALin : e.jBLin; // this body's rows, taken before the dual update
     const M3 jAng = isA ? e.jAAng : e.jBAng;
     if (dual)
@@ -2091,7 +2093,7 @@ AVBD_DEV unsigned contact_term_self(const DevBodies &B, const DevForces &F, unsi
 // One listed row's contribution (Manifold/Joint/Spring::updatePrimal).
 // `fusedDual`: this launch also performs the previous iteration's contact dual updates,
 // each by the row of the body that owns it.
-template <bool COH = false>
+template <bool COH = false, bool ROUND = false>
 AVBD_DEV unsigned listed_row_term(const DevBodies &B, const DevForces &F, int2 row, int self, bool fusedDual,
                                   const Params &P, float *t)
 {
@@ -2102,7 +2104,7 @@ AVBD_DEV unsigned listed_row_term(const DevBodies &B, const DevForces &F, int2 r
     switch (adj_type(e))
     {
     case ADJ_MANIFOLD:
-        return contact_term_self<COH>(B, F, i, sub, isA, self, row_partner(row),
+        return contact_term_self<COH, ROUND>(B, F, i, sub, isA, self, row_partner(row),
                                       fusedDual && (row.y & ROW_OWNS_DUAL) != 0, P, t);
     case ADJ_JOINT:
     {
@@ -2166,7 +2168,7 @@ AVBD_DEV void unit_sync()
 // block works in independent units of SUB threads (SUB / G bodies, which the unit's first
 // SUB / G threads factorise); every thread of the block calls this (it holds the units'
 // barriers).
-template <int G, int BLOCK, int SUB, bool COH>
+template <int G, int BLOCK, int SUB, bool COH, bool ROUND>
 AVBD_DEV void primal_batch(const DevBodies &B, const DevForces &F, const Params &P, const int4 *entries, int count,
                            bool fusedDual, PrimalShared<G, BLOCK> &sh)
 {
@@ -2200,7 +2202,7 @@ AVBD_DEV void primal_batch(const DevBodies &B, const DevForces &F, const Params 
         {
             int r = base + lane;
             if (r < r1)
-                sh.kind[g][lane] = listed_row_term<COH>(B, F, F.rows[r], b, fusedDual, P, sh.term[g][lane]);
+                sh.kind[g][lane] = listed_row_term<COH, ROUND>(B, F, F.rows[r], b, fusedDual, P, sh.term[g][lane]);
             __syncwarp(gmask);
             int nrows = min(G, r1 - base);
             for (int rr = 0; rr < nrows; ++rr)
@@ -2259,14 +2261,14 @@ AVBD_DEV void primal_batch(const DevBodies &B, const DevForces &F, const Params 
 }
 
 // One launch per colour: block k takes the colour's bodies [k GPB, (k+1) GPB).
-template <int G, int BLOCK, int MINB>
+template <int G, int BLOCK, int MINB, bool ROUND = false>
 __global__ void __launch_bounds__(BLOCK, MINB) k_primal(DevBodies B, DevForces F, Params P, const int4 *entries,
                                                         int first, int count)
 {
     __shared__ PrimalShared<G, BLOCK> sh;
     constexpr int GPB = BLOCK / G;
     const int base = blockIdx.x * GPB;
-    primal_batch<G, BLOCK, BLOCK, false>(B, F, P, entries + first + base, min(GPB, count - base), false, sh);
+    primal_batch<G, BLOCK, BLOCK, false, ROUND>(B, F, P, entries + first + base, min(GPB, count - base), false, sh);
 }
 
 // ---------------------------------------------------------------------------
@@ -2274,7 +2276,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_primal(DevBodies B, DevForces F
 // ---------------------------------------------------------------------------
 
 // Manifold::updateDual per contact slot (manifold.cpp:231-280); t = manifold * 8 + slot.
-template <bool COH>
+template <bool COH, bool ROUND>
 AVBD_DEV void dual_contact_slot(const DevBodies &B, const DevManifolds &M, long long t, const Params &P)
 {
     int m = (int)(t >> 3), ci = (int)(t & 7);
@@ -2287,20 +2289,21 @@ AVBD_DEV void dual_contact_slot(const DevBodies &B, const DevManifolds &M, long 
     M3 basis = rows(xyz(b0), xyz(b1), xyz(bs[2]));
     float4 *cp = M.contact + (size_t)m * 32 + 4 * ci;
     ContactRec c = load_contact<COH>(cp);
-    ContactEval e = b1.w == 0.0f
-                        ? eval_contact(A, Bp, basis, b0.w, c, P.alpha)
-                        : eval_contact_arms(A, Bp, basis, b0.w, c, P.alpha,
+    ContactEval e = ROUND && b1.w != 0.0f
+                        ? eval_contact_arms(A, Bp, basis, b0.w, c, P.alpha,
                                             contact_offset(body_shape(B, ab.x), A.q, c.rA, basis, true, c.key),
-                                            contact_offset(body_shape(B, ab.y), Bp.q, c.rB, basis, false, c.key));
+                                            contact_offset(body_shape(B, ab.y), Bp.q, c.rB, basis, false, c.key))
+                        : eval_contact(A, Bp, basis, b0.w, c, P.alpha);
     contact_dual(c, e, P.betaLin);
     store_contact_state(cp, c);
 }
 
+template <bool ROUND = false>
 __global__ void k_dual_contacts(DevBodies B, DevManifolds M, int nMan, Params P)
 {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t < 8ll * nMan)
-        dual_contact_slot<false>(B, M, t, P);
+        dual_contact_slot<false, ROUND>(B, M, t, P);
 }
 
 // Joint::updateDual with fracture (joint.cpp:125-182)
@@ -2420,7 +2423,7 @@ AVBD_DEV bool iter_barrier(IterSync *s)
 // neither has the other body, so both poses are those the dual sweep of iteration k reads
 // and every contact's update is the same. The last iteration's contact updates close the
 // launch.
-template <int G, int BLOCK, int SUB>
+template <int G, int BLOCK, int SUB, bool ROUND = false>
 __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces F, Params P, const int4 *entries,
                                                          const int *colourStart, int nColours, int iterations,
                                                          IterSync *sync)
@@ -2437,8 +2440,8 @@ __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces 
             const int first = colourStart[c], cnt = colourStart[c + 1] - first;
             for (int base = blockIdx.x * GPB; base < cnt; base += gridDim.x * GPB)
             {
-                primal_batch<G, BLOCK, SUB, true>(B, F, P, entries + first + base, min(GPB, cnt - base), it > 0,
-                                                  sh);
+                primal_batch<G, BLOCK, SUB, true, ROUND>(B, F, P, entries + first + base, min(GPB, cnt - base),
+                                                         it > 0, sh);
                 unit_sync<SUB, BLOCK>(); // the unit's solve threads are done with the shared systems
             }
             if (!iter_barrier(sync))
@@ -2460,7 +2463,7 @@ __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces 
             int2 ab = F.man.ab[t >> 3];
             bool orphan = B.massMoment[ab.x].x <= 0 && B.massMoment[ab.y].x <= 0;
             for (int r = orphan ? iterations : 1; r > 0; --r)
-                dual_contact_slot<true>(B, F.man, t, P);
+                dual_contact_slot<true, ROUND>(B, F.man, t, P);
         }
 }
 

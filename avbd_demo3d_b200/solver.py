@@ -228,8 +228,9 @@ class World:
         return out
 
     def write_bodies(self, pos=None, quat=None, vel=None, angvel=None, prevvel=None):
-        """Overwrite body state (list order) between steps."""
-        cur = self.bodies()
+        """Overwrite body state (list order) between steps; fields not given keep their values."""
+        given = (pos, quat, vel, angvel, prevvel)
+        cur = self.bodies() if any(x is None for x in given) else {}
         arr = dict(position3=_c(cur["pos"] if pos is None else pos, F32),
                    orientation4=_c(cur["quat"] if quat is None else quat, F32),
                    velocity3=_c(cur["vel"] if vel is None else vel, F32),

@@ -1169,6 +1169,21 @@ __global__ void k_pack_state(PackedFields P, float *out, int n)
     }
 }
 
+// Host copies between callers' arrays and the pinned staging. (Splitting them over threads
+// was measured slower: starting the threads costs more than the copies.)
+struct HostCopy
+{
+    void *dst;
+    const void *src;
+    size_t bytes;
+};
+
+void copy_host(const std::vector<HostCopy> &copies)
+{
+    for (const HostCopy &c : copies)
+        memcpy(c.dst, c.src, c.bytes);
+}
+
 // Body state from caller arrays: one copy of the packed fields into pinned staging, one
 // asynchronous upload, and the conversion to float4 on the device.
 int write_state(AvbdContext *ctx, const AvbdBodies *b)
@@ -1192,9 +1207,11 @@ int write_state(AvbdContext *ctx, const AvbdBodies *b)
         return AVBD_OK;
     CHECK(stage_reserve(ctx, (size_t)(floats + 3) / 4));
     float *st = (float *)ctx->hStage;
+    std::vector<HostCopy> copies;
     for (int f = 0; f < 5; ++f)
         if (src[f])
-            memcpy(st + P.f[f].offset, src[f], sizeof(float) * width[f] * (size_t)n);
+            copies.push_back({st + P.f[f].offset, src[f], sizeof(float) * width[f] * (size_t)n});
+    copy_host(copies);
     CHECK(reserve(ctx, ctx->stateStage, (size_t)std::max<long long>(floats, 1), false));
     if (floats)
         CU(cudaMemcpyAsync(ctx->stateStage.p, st, sizeof(float) * floats, cudaMemcpyHostToDevice, ctx->stream));
@@ -1881,9 +1898,11 @@ int avbd_read_bodies(AvbdContext *ctx, const AvbdBodyState *out)
     float *st = (float *)ctx->hStage;
     CU(cudaMemcpyAsync(st, ctx->stateStage.p, sizeof(float) * floats, cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
+    std::vector<HostCopy> copies;
     for (int f = 0; f < MAX_PACKED; ++f)
         if (dst[f])
-            memcpy(dst[f], st + P.f[f].offset, sizeof(float) * width[f] * (size_t)n);
+            copies.push_back({dst[f], st + P.f[f].offset, sizeof(float) * width[f] * (size_t)n});
+    copy_host(copies);
     return AVBD_OK;
 }
 

@@ -110,6 +110,7 @@ struct AvbdContext
     unsigned cellHashMask = 0, largeHashMask = 0;
     DArr<unsigned long long> bpKeys, bpKeysAlt;
     DArr<int> pairCount, pairOffset;
+    DArr<int> pairRecorded; // BP_SLOTS new partners per grid entry from the counting pass
     DArr<int> sapVals, sapValsAlt, sapAxis; // sweep and prune: sorted bodies, axis per world
 
     ManBuf man[2];
@@ -737,9 +738,10 @@ int broadphase(AvbdContext *ctx)
             k_bp_hash_runs<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(dk.Current(), nB, cell_hash(ctx));
             LAUNCHED();
             CHECK(large_cell_lists(ctx, nL));
+            CHECK(reserve(ctx, ctx->pairRecorded, (size_t)nB * BP_SLOTS, false));
             k_bp_pairs<false><<<grid_for(nB, 128), 128, 0, ctx->stream>>>(
                 B, F, G, dk.Current(), nB, cell_hash(ctx), ctx->large.p, ctx->largeLo.p, ctx->largeHi.p,
-                ctx->largeSorted, large_hash(ctx), dt, ctx->pairCount.p, nullptr, 0, 0, cnt);
+                ctx->largeSorted, large_hash(ctx), dt, ctx->pairCount.p, nullptr, 0, 0, cnt, ctx->pairRecorded.p);
             LAUNCHED();
             CHECK(scan_counts(ctx, ctx->pairCount.p, ctx->pairOffset.p, nB, 0));
             ctx->launches++;
@@ -800,12 +802,20 @@ int broadphase(AvbdContext *ctx)
         if (P1 + P2 > 0)
             CHECK(reserve_manifolds(ctx, ctx->man[ctx->cur], (size_t)(M0 + P1 + P2), (size_t)M0));
         F = dev_forces(ctx);
-        if (P1 > 0)
+        if (P1 > 0 && !ctx->hCounters->pairOverflow)
+        {
+            // every entry's new pairs were recorded while counting: write them out
+            k_bp_emit_recorded<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(
+                F, dk.Current(), nB, ctx->pairCount.p, ctx->pairOffset.p, ctx->pairRecorded.p, M0,
+                (unsigned long long)ctx->nextSeq);
+            LAUNCHED();
+        }
+        else if (P1 > 0)
         {
             k_bp_pairs<true><<<grid_for(nB, 128), 128, 0, ctx->stream>>>(
                 B, F, G, dk.Current(), nB, cell_hash(ctx), ctx->large.p, ctx->largeLo.p, ctx->largeHi.p,
                 ctx->largeSorted, large_hash(ctx), dt, nullptr, ctx->pairOffset.p, M0,
-                (unsigned long long)ctx->nextSeq, cnt);
+                (unsigned long long)ctx->nextSeq, cnt, nullptr);
             LAUNCHED();
         }
         if (P2 > 0)
@@ -1498,6 +1508,7 @@ void avbd_destroy(AvbdContext *ctx)
     release(ctx->sapAxis);
     release(ctx->bpKeysAlt);
     release(ctx->pairCount);
+    release(ctx->pairRecorded);
     release(ctx->pairOffset);
     release(ctx->llCount);
     release(ctx->llOffset);

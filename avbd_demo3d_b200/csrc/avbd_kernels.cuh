@@ -103,6 +103,7 @@ struct StepCounters
     int colouredThisRound;
     int maxColour;
     int error;
+    int pairOverflow; // a grid entry found more new pairs than its recorded slots
 };
 
 enum DeviceError
@@ -477,9 +478,12 @@ AVBD_DEV void warp_add(unsigned long long *dst, unsigned v)
         atomicAdd(dst, (unsigned long long)s);
 }
 
+constexpr int BP_SLOTS = 4; // new pairs a grid entry records in the counting pass
+
 // One thread per sorted grid entry i (solver.cpp:405-465). EMIT == false counts new
-// (unconstrained) hits, EMIT == true writes them as fresh manifolds at base + offset[i] in
-// hit order. Large bodies are visited in list order: the entry's cell candidates merged
+// (unconstrained) hits and records the first BP_SLOTS partners of each entry in `recorded`
+// (k_bp_emit_recorded writes them out); EMIT == true, needed only when an entry found more,
+// writes them as fresh manifolds at base + offset[i] in hit order. Large bodies are visited in list order: the entry's cell candidates merged
 // with its world's global list, both sorted by large index.
 template <bool EMIT>
 __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, DevGrid G, const unsigned long long *keys,
@@ -487,7 +491,7 @@ __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, DevG
                                                   const float4 *largeLo, const float4 *largeHi,
                                                   const unsigned long long *largeKeys, HashTable largeCells, float dt,
                                                   int *counts, const int *offsets, int base, unsigned long long seqBase,
-                                                  StepCounters *cnt)
+                                                  StepCounters *cnt, int *recorded)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = i < nBinned;
@@ -520,6 +524,8 @@ __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, DevG
                 F.man.seq[m] = seqBase + (unsigned long long)(m - base);
                 F.man.n[m] = 0;
             }
+            else if (found < BP_SLOTS)
+                recorded[(size_t)i * BP_SLOTS + found] = bIdx;
             found++;
         };
         auto test = [&](int j) {
@@ -591,13 +597,39 @@ __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, DevG
             }
         }
         if (!EMIT)
+        {
             counts[i] = found;
+            if (found > BP_SLOTS)
+                cnt->pairOverflow = 1;
+        }
     }
     if (!EMIT)
     {
         warp_add(&cnt->pairChecks, checks);
         warp_add(&cnt->sphereHits, hits);
         warp_add(&cnt->constrainedHits, cons);
+    }
+}
+
+// The new pairs recorded by the counting pass, as fresh manifolds at base + offset[i] in hit
+// order (every entry found at most BP_SLOTS).
+__global__ void k_bp_emit_recorded(DevForces F, const unsigned long long *keys, int nBinned, const int *counts,
+                                   const int *offsets, const int *recorded, int base, unsigned long long seqBase)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nBinned)
+        return;
+    int c = counts[i];
+    if (c <= 0)
+        return;
+    int a = key_body(keys[i]);
+    int out = base + offsets[i];
+    for (int f = 0; f < c && f < BP_SLOTS; ++f)
+    {
+        int m = out + f;
+        F.man.ab[m] = make_int2(a, recorded[(size_t)i * BP_SLOTS + f]);
+        F.man.seq[m] = seqBase + (unsigned long long)(m - base);
+        F.man.n[m] = 0;
     }
 }
 

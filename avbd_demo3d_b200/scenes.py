@@ -23,6 +23,8 @@ import numpy as np
 
 F32 = np.float32
 
+SHAPE_BOX, SHAPE_SPHERE, SHAPE_CAPSULE, SHAPE_CYLINDER = 0, 1, 2, 3
+
 FORCE_JOINT = 1
 FORCE_SPRING = 2
 FORCE_IGNORE = 3
@@ -108,6 +110,10 @@ class Scene:
     frB: np.ndarray  # (m, 3)
     fparam: np.ndarray  # (m, 3)
     params: Params
+    # round bodies (Rigid::makeSphere / makeCapsule / makeCylinder, rigid.cpp:44-90): shape per
+    # body (SHAPE_*), dims = (radius, half length); None when every body is a box
+    shape: np.ndarray | None = None  # (n,) int32
+    dims: np.ndarray | None = None  # (n, 2)
 
     @property
     def n_bodies(self) -> int:
@@ -122,7 +128,7 @@ class SceneBuilder:
     def __init__(self, name: str, params: Params):
         self.name = name
         self.params = params
-        self.b = {k: [] for k in ("size", "density", "friction", "pos", "vel", "quat")}
+        self.b = {k: [] for k in ("size", "density", "friction", "pos", "vel", "quat", "shape", "dims")}
         self.f = {k: [] for k in ("ftype", "fa", "fb", "frA", "frB", "fparam")}
 
     def body(self, size, density, friction, pos, vel=(0, 0, 0), quat=(0, 0, 0, 1)) -> int:
@@ -132,7 +138,29 @@ class SceneBuilder:
         self.b["pos"].append(np.asarray(pos, dtype=F32).reshape(3))
         self.b["vel"].append(np.asarray(vel, dtype=F32).reshape(3))
         self.b["quat"].append(np.asarray(quat, dtype=F32).reshape(4))
+        self.b["shape"].append(SHAPE_BOX)
+        self.b["dims"].append(np.zeros(2, F32))
         return len(self.b["size"]) - 1
+
+    def round_body(self, shape, radius, half_length, density, friction, pos, vel=(0, 0, 0), quat=(0, 0, 0, 1)) -> int:
+        """Rigid::makeSphere / makeCapsule / makeCylinder (rigid.cpp:44-90); size holds the
+        shape's bounding widths as the constructor gives them."""
+        r, h = F32(radius), F32(half_length)
+        d = F32(r * F32(2.0))
+        height = {SHAPE_SPHERE: d, SHAPE_CAPSULE: F32(F32(h * F32(2.0)) + d), SHAPE_CYLINDER: F32(h * F32(2.0))}[shape]
+        i = self.body((d, d, height), density, friction, pos, vel, quat)
+        self.b["shape"][i] = shape
+        self.b["dims"][i] = np.array([r, h if shape != SHAPE_SPHERE else 0.0], F32)
+        return i
+
+    def sphere(self, radius, density, friction, pos, vel=(0, 0, 0), quat=(0, 0, 0, 1)) -> int:
+        return self.round_body(SHAPE_SPHERE, radius, 0.0, density, friction, pos, vel, quat)
+
+    def capsule(self, radius, half_length, density, friction, pos, vel=(0, 0, 0), quat=(0, 0, 0, 1)) -> int:
+        return self.round_body(SHAPE_CAPSULE, radius, half_length, density, friction, pos, vel, quat)
+
+    def cylinder(self, radius, half_length, density, friction, pos, vel=(0, 0, 0), quat=(0, 0, 0, 1)) -> int:
+        return self.round_body(SHAPE_CYLINDER, radius, half_length, density, friction, pos, vel, quat)
 
     def bodies(self, size, density, friction, pos, vel=None, quat=None) -> np.ndarray:
         n = len(size)
@@ -145,6 +173,8 @@ class SceneBuilder:
         self.b["pos"].extend(np.asarray(pos, dtype=F32))
         self.b["vel"].extend(np.asarray(vel, dtype=F32))
         self.b["quat"].extend(np.asarray(quat, dtype=F32))
+        self.b["shape"].extend([SHAPE_BOX] * n)
+        self.b["dims"].extend(np.zeros((n, 2), F32))
         return np.arange(first, first + n)
 
     def joint(self, a, b, rA, rB, stiffness_lin=math.inf, stiffness_ang=0.0, fracture=math.inf):
@@ -185,6 +215,8 @@ class SceneBuilder:
             frB=arr(self.f["frB"], (m, 3), F32),
             fparam=arr(self.f["fparam"], (m, 3), F32),
             params=self.params,
+            shape=arr(self.b["shape"], (n,), np.int32) if any(self.b["shape"]) else None,
+            dims=arr(self.b["dims"], (n, 2), F32) if any(self.b["shape"]) else None,
         )
 
 
@@ -360,6 +392,60 @@ def mixed_drop(n_boxes: int = 200_000, n_chains: int = 2048, chain_len: int = 48
         for k in range(n_spring_boxes // 2):
             s.spring(int(loose_ids[2 * k]), int(loose_ids[2 * k + 1]), (0, 0, 0), (0, 0, 0), stiff[k], -1.0)
     return s.build()
+
+
+def round_mix(n: int = 600, seed: int = 11, cols: int = 10, params: Params | None = None) -> Scene:
+    """Mixed primitives dropped onto a static ground slab: spheres, capsules, cylinders and
+    boxes in equal shares (shape drawn per body), radii U[0.2, 0.5], half lengths U[0.1, 0.5],
+    box widths U[0.4, 1.0], density U[0.5, 2], friction U[0.3, 0.8], uniform random
+    orientations, placed on a jittered cols x cols x (n / cols^2) lattice of 1.4 m pitch
+    from z = 1.5 with small random velocities; plus four static cylinders lying on the ground
+    and a raised static slab, so every shape pair of the narrowphase meets (round-round,
+    round-box and its static-slab and swept-sphere paths, cylinder-box and cylinder-cylinder)."""
+    rs = Stream(seed)
+    b = SceneBuilder(f"round_mix{n}", params or baseline_params())
+    b.body((100, 100, 1), 0.0, 0.5, (0, 0, -0.5))
+    half = cols * 1.4 / 2.0
+    for k in range(4):  # static cylinders lying on the ground along x
+        b.cylinder(0.3, 2.0, 0.0, 0.6, (-half + 1.0 + k * (2.0 * half - 2.0) / 3.0, 0.0, 0.3),
+                   quat=(0.0, 0.70710677, 0.0, 0.70710677))
+    b.body((4.0, 4.0, 0.2), 0.0, 0.5, (half + 3.0, 0.0, 1.0))  # raised static slab
+    shape = (rs.uniform(n) * 4.0).astype(np.int64).clip(0, 3)
+    radius = rs.uniform(n, 0.2, 0.5)
+    halfl = rs.uniform(n, 0.1, 0.5)
+    width = rs.uniform(3 * n, 0.4, 1.0).reshape(n, 3)
+    density = rs.uniform(n, 0.5, 2.0)
+    friction = rs.uniform(n, 0.3, 0.8)
+    quat = rs.unit_quaternions(n)
+    jitter = rs.uniform(3 * n, -0.1, 0.1).reshape(n, 3)
+    vel = rs.uniform(3 * n, -0.5, 0.5).reshape(n, 3)
+    for i in range(n):
+        cx, cy, cz = i % cols, (i // cols) % cols, i // (cols * cols)
+        pos = (cx * 1.4 - half + 0.7 + jitter[i, 0], cy * 1.4 - half + 0.7 + jitter[i, 1], 1.5 + cz * 1.4 + jitter[i, 2])
+        if shape[i] == SHAPE_BOX:
+            b.body(width[i], density[i], friction[i], pos, vel[i], quat[i])
+        else:
+            b.round_body(int(shape[i]), radius[i], halfl[i], density[i], friction[i], pos, vel[i], quat[i])
+    return b.build()
+
+
+def sphere_pour(n: int = 2000, seed: int = 13, params: Params | None = None) -> Scene:
+    """Spheres (radius U[0.15, 0.3]) streamed in from a seeded column above a row of static
+    standing cylinders on a static ground: many sphere-sphere and sphere-static contacts,
+    rolling friction on the ground and the cylinders."""
+    rs = Stream(seed)
+    b = SceneBuilder(f"sphere_pour{n}", params or baseline_params())
+    b.body((100, 100, 1), 0.0, 0.5, (0, 0, -0.5))
+    for k in range(5):
+        b.cylinder(0.4, 0.6, 0.0, 0.8, (-4.0 + 2.0 * k, 0.0, 0.6))
+    radius = rs.uniform(n, 0.15, 0.3)
+    side = int(math.ceil(n ** (1.0 / 3.0)))
+    jitter = rs.uniform(3 * n, -0.05, 0.05).reshape(n, 3)
+    for i in range(n):
+        x, y, z = i % side, (i // side) % side, i // (side * side)
+        pos = (x * 0.65 - side * 0.325 + jitter[i, 0], y * 0.65 - side * 0.325 + jitter[i, 1], 2.0 + z * 0.65)
+        b.sphere(radius[i], 1.0, 0.45, pos, (1.1, 0.0, -1.5))
+    return b.build()
 
 
 def tower(nx: int = 10, ny: int = 10, height: int = 10, seed: int = 4, params: Params | None = None) -> Scene:

@@ -71,6 +71,46 @@ def box_properties(size: np.ndarray, density: np.ndarray):
     return mass.astype(F32), moment.astype(F32), radius.astype(F32)
 
 
+def round_properties(shape: np.ndarray, dims: np.ndarray, density: np.ndarray, mass, moment, radius):
+    """Mass, moment and bounding radius of spheres, capsules and cylinders, written over the
+    box values in place (Rigid::makeSphere / makeCapsule / makeCylinder, rigid.cpp:44-90, in
+    float32 with the same operation order)."""
+    pi = F32(3.14159265358979323846)
+    r = np.asarray(dims, F32)[:, 0]
+    h = np.asarray(dims, F32)[:, 1]
+    d = np.asarray(density, F32)
+    two5 = F32(2.0) / F32(5.0)
+    sphere_mass = (((F32(4.0) / F32(3.0) * pi) * r) * r) * r * d
+    for t in (1, 2, 3):
+        sel = np.asarray(shape) == t
+        if not sel.any():
+            continue
+        rs, hs, ds, sm = r[sel], h[sel], d[sel], sphere_mass[sel]
+        if t == 1:  # sphere
+            m = sm
+            i = ((two5 * m) * rs) * rs
+            mom = np.stack([i, i, i], axis=1)
+            rad = rs
+        elif t == 2:  # capsule
+            L = hs * F32(2.0)
+            cm = (((pi * rs) * rs) * L) * ds
+            m = cm + sm
+            axial = ((F32(0.5) * cm) * rs) * rs + ((two5 * sm) * rs) * rs
+            trans = ((F32(3.0) * rs) * rs + L * L) / F32(12.0) * cm + ((two5 * sm) * rs) * rs + (sm * hs) * hs
+            mom = np.stack([trans, trans, axial], axis=1)
+            rad = hs + rs
+        else:  # cylinder
+            H = hs * F32(2.0)
+            m = (((pi * rs) * rs) * H) * ds
+            axial = ((F32(0.5) * m) * rs) * rs
+            trans = ((F32(3.0) * rs) * rs + H * H) / F32(12.0) * m
+            mom = np.stack([trans, trans, axial], axis=1)
+            rad = np.sqrt(rs * rs + hs * hs)
+        mass[sel] = m
+        moment[sel] = mom
+        radius[sel] = rad
+
+
 # ---------------------------------------------------------------------------
 # Device world
 # ---------------------------------------------------------------------------
@@ -130,10 +170,19 @@ class World:
         if sc.n_forces and (sc.fb.min() < 0 or sc.fb.max() >= n or sc.fa.max() >= n or sc.fa.min() < -1):
             raise _lib.AvbdError("avbd_load_world failed (argument): force body index out of range")
         mass, moment, radius = box_properties(sc.size, sc.density)
+        shape = np.zeros(n, np.int32)
+        shape_radius, half_length = radius.copy(), np.zeros(n, F32)  # a box's shape radius is its bounding radius
+        if getattr(sc, "shape", None) is not None:
+            round_properties(sc.shape, sc.dims, sc.density, mass, moment, radius)
+            shape = np.asarray(sc.shape, np.int32)
+            rnd = shape != 0
+            shape_radius[rnd] = np.asarray(sc.dims, F32)[rnd, 0]
+            half_length[rnd] = np.asarray(sc.dims, F32)[rnd, 1]
         L = World.list_order
         body = dict(position3=L(sc.pos), orientation4=L(sc.quat), velocity3=L(sc.vel),
                     angular3=np.zeros((n, 3), F32), prev_velocity3=L(sc.vel), size3=L(sc.size), mass=L(mass),
-                    moment3=L(moment), friction=L(sc.friction), radius=L(radius))
+                    moment3=L(moment), friction=L(sc.friction), radius=L(radius), shape=L(shape),
+                    shape_radius=L(shape_radius), half_length=L(half_length))
         local = lambda c: np.where(c >= 0, n - 1 - c, -1).astype(np.int32)
         glob = lambda c: np.where(c >= 0, c + offset, -1).astype(np.int32)
         seq = np.arange(seq0, seq0 + sc.n_forces, dtype=np.int64)
@@ -187,9 +236,11 @@ class World:
                       "radius": self._body_arrays["radius"], "size": self._body_arrays["size3"],
                       "friction": self._body_arrays["friction"]}
         ba, fa_ = self._body_arrays, self._force_arrays
+        has_shapes = bool((ba["shape"] != 0).any())
         bodies_s = _lib.AvbdBodies(self.n, *[_ptr(ba[k]) for k in (
             "position3", "orientation4", "velocity3", "angular3", "prev_velocity3", "size3", "mass", "moment3",
-            "friction", "radius")])
+            "friction", "radius")], *([_ptr(ba[k]) for k in ("shape", "shape_radius", "half_length")]
+                                      if has_shapes else [None, None, None]))
         joints = _lib.AvbdJoints(len(fa_["j_seq"]), _ptr(fa_["j_ab"]), _ptr(fa_["j_seq"]), _ptr(fa_["j_state"]),
                                  _ptr(fa_["j_broken"]))
         springs = _lib.AvbdSprings(len(fa_["s_seq"]), _ptr(fa_["s_ab"]), _ptr(fa_["s_seq"]), _ptr(fa_["s_state"]))

@@ -240,6 +240,9 @@ typedef struct
     V3 moment;
     float friction;
     float radius;
+    int shape;            /* ORACLE_SHAPE_* (RigidShape::type) */
+    float shapeRadius;    /* RigidShape::radius (a box's: length(size / 2)) */
+    float halfLength;     /* RigidShape::halfLength (capsules, cylinders) */
 } Body;
 
 typedef struct
@@ -536,13 +539,18 @@ static void broadphase_grid(OracleWorld *w, PairList *out)
         float slack = vlen(body->vel) * w->p.dt;
         if (body->radius > binnedRadius)
         {
-            V3 e = vmul(body->size, 0.5f);
-            V3 cx = qrotate(body->q, v3(1, 0, 0));
-            V3 cy = qrotate(body->q, v3(0, 1, 0));
-            V3 cz = qrotate(body->q, v3(0, 0, 1));
-            V3 h = v3(fabsf(cx.x) * e.x + fabsf(cy.x) * e.y + fabsf(cz.x) * e.z,
-                      fabsf(cx.y) * e.x + fabsf(cy.y) * e.y + fabsf(cz.y) * e.z,
-                      fabsf(cx.z) * e.x + fabsf(cy.z) * e.y + fabsf(cz.z) * e.z);
+            /* solver.cpp:314-326: boxes by their rotated extents, round shapes by radius */
+            V3 h = v3(body->radius, body->radius, body->radius);
+            if (body->shape == ORACLE_SHAPE_BOX)
+            {
+                V3 e = vmul(body->size, 0.5f);
+                V3 cx = qrotate(body->q, v3(1, 0, 0));
+                V3 cy = qrotate(body->q, v3(0, 1, 0));
+                V3 cz = qrotate(body->q, v3(0, 0, 1));
+                h = v3(fabsf(cx.x) * e.x + fabsf(cy.x) * e.y + fabsf(cz.x) * e.z,
+                       fabsf(cx.y) * e.x + fabsf(cy.y) * e.y + fabsf(cz.y) * e.z,
+                       fabsf(cx.z) * e.x + fabsf(cy.z) * e.y + fabsf(cz.z) * e.z);
+            }
             large[nLarge].body = i;
             large[nLarge].lo = vsub(body->pos, h);
             large[nLarge].hi = vadd(body->pos, h);
@@ -1044,15 +1052,602 @@ static int collide_boxes(V3 pA, Q4 qA, V3 sA, V3 pB, Q4 qB, V3 sB, NewContact *c
 /* Force initialisation                                                      */
 /* ------------------------------------------------------------------------- */
 
+/* ------------------------------------------------------------------------- */
+/* Round shapes: spheres, capsules, cylinders (collide.cpp:435-1176)         */
+/* ------------------------------------------------------------------------- */
+
+#define SAT_EPS 1.0e-6f /* SAT_AXIS_EPSILON (collide.cpp:20) */
+
+static int is_round(const Body *b) { return b->shape == ORACLE_SHAPE_SPHERE || b->shape == ORACLE_SHAPE_CAPSULE; }
+static int is_cyl(const Body *b) { return b->shape == ORACLE_SHAPE_CYLINDER; }
+static V3 vnormalize(V3 v) { return vdiv(v, vlen(v)); }
+
+/* closestPointOnOBB, pointInsideOBB, localToOBBWorld (collide.cpp:435-456) */
+static V3 obb_closest(const Obb *o, V3 p)
+{
+    V3 d = vsub(p, o->center);
+    return vadd(vadd(vadd(o->center, vmul(o->axis[0], rclamp(vdot(d, o->axis[0]), -o->half.x, o->half.x))),
+                     vmul(o->axis[1], rclamp(vdot(d, o->axis[1]), -o->half.y, o->half.y))),
+                vmul(o->axis[2], rclamp(vdot(d, o->axis[2]), -o->half.z, o->half.z)));
+}
+
+static V3 obb_local(const Obb *o, V3 p)
+{
+    V3 d = vsub(p, o->center);
+    return v3(vdot(d, o->axis[0]), vdot(d, o->axis[1]), vdot(d, o->axis[2]));
+}
+
+static V3 obb_world(const Obb *o, V3 l)
+{
+    return vadd(vadd(vadd(o->center, vmul(o->axis[0], l.x)), vmul(o->axis[1], l.y)), vmul(o->axis[2], l.z));
+}
+
+/* capsuleSegment / cylinderSegment (collide.cpp:468-488): a sphere is a point segment */
+static void round_segment(const Body *b, V3 *a, V3 *c)
+{
+    if (b->shape == ORACLE_SHAPE_CAPSULE || b->shape == ORACLE_SHAPE_CYLINDER)
+    {
+        V3 axis = qrotate(b->q, v3(0.0f, 0.0f, 1.0f));
+        *a = vsub(b->pos, vmul(axis, b->halfLength));
+        *c = vadd(b->pos, vmul(axis, b->halfLength));
+    }
+    else
+        *a = *c = b->pos;
+}
+
+/* closestPointOnSegment (collide.cpp:490-498) */
+static V3 segment_closest(V3 a, V3 b, V3 p)
+{
+    V3 ab = vsub(b, a);
+    float denom = vlensq(ab);
+    if (denom < SAT_EPS)
+        return a;
+    float t = rclamp(vdot(vsub(p, a), ab) / denom, 0.0f, 1.0f);
+    return vadd(a, vmul(ab, t));
+}
+
+/* addRoundContact (collide.cpp:500-517) */
+static int round_contact(const Body *A, const Body *B, V3 cA, float rA, V3 cB, float rB, int key, NewContact *cs,
+                         M3 *basis)
+{
+    V3 delta = vsub(cB, cA);
+    float rs = rA + rB;
+    float d2 = vlensq(delta);
+    if (d2 > rs * rs)
+        return 0;
+    V3 n = d2 > SAT_EPS ? vdiv(delta, sqrtf(d2)) : v3(1.0f, 0.0f, 0.0f);
+    V3 xA = vadd(cA, vmul(n, rA));
+    V3 xB = vsub(cB, vmul(n, rB));
+    *basis = orthonormal(vneg(n));
+    int count = 0;
+    V3 mids[8];
+    add_contact(A->pos, A->q, B->pos, B->q, cs, &count, mids, xA, xB, key);
+    return count;
+}
+
+/* thinStaticBoxTopFrame (collide.cpp:957-976): a static slab's thin axis and upward sign */
+static int slab_frame(const Obb *o, const Body *box, int *thin, float *sign)
+{
+    if (box->mass > 0.0f)
+        return 0;
+    int t = 0;
+    if (o->half.y < VEC(o->half, t))
+        t = 1;
+    if (o->half.z < VEC(o->half, t))
+        t = 2;
+    int a = (t + 1) % 3, b = (t + 2) % 3;
+    if (VEC(o->half, t) * 4.0f > rmin(VEC(o->half, a), VEC(o->half, b)))
+        return 0;
+    *thin = t;
+    *sign = vdot(o->axis[t], v3(0.0f, 0.0f, 1.0f)) >= 0.0f ? 1.0f : -1.0f;
+    return 1;
+}
+
+/* sweptSphereBoxContact (collide.cpp:519-587) */
+static int swept_sphere_box(const Obb *o, const Body *sph, const Body *box, float dt, V3 *nBoxToSphere, V3 *xBox)
+{
+    V3 rv = vsub(sph->vel, box->vel);
+    if (dt <= 0.0f || vlensq(rv) < SAT_EPS)
+        return 0;
+    V3 cur = sph->pos;
+    V3 prev = vsub(cur, vmul(rv, dt));
+    V3 l0 = obb_local(o, prev), l1 = obb_local(o, cur);
+    V3 delta = vsub(l1, l0);
+    V3 eh = vadd(o->half, v3(sph->shapeRadius, sph->shapeRadius, sph->shapeRadius));
+    float tEnter = 0.0f, tExit = 1.0f, hitSign = 1.0f;
+    int hitAxis = -1;
+    for (int ax = 0; ax < 3; ++ax)
+    {
+        float d = VEC(delta, ax), s0 = VEC(l0, ax), e = VEC(eh, ax);
+        if (fabsf(d) < SAT_EPS)
+        {
+            if (s0 < -e || s0 > e)
+                return 0;
+            continue;
+        }
+        float inv = 1.0f / d;
+        float t0 = (-e - s0) * inv, t1 = (e - s0) * inv, sg = -1.0f;
+        if (t0 > t1)
+        {
+            float tmp = t0;
+            t0 = t1;
+            t1 = tmp;
+            sg = 1.0f;
+        }
+        if (t0 > tEnter)
+        {
+            tEnter = t0;
+            hitAxis = ax;
+            hitSign = sg;
+        }
+        tExit = rmin(tExit, t1);
+        if (tEnter > tExit)
+            return 0;
+    }
+    if (hitAxis < 0 || tEnter < 0.0f || tEnter > 1.0f)
+        return 0;
+    V3 sl = vadd(l0, vmul(delta, tEnter));
+    VE(sl, hitAxis) = VEC(o->half, hitAxis) * hitSign;
+    for (int ax = 0; ax < 3; ++ax)
+        if (ax != hitAxis)
+            VE(sl, ax) = rclamp(VEC(sl, ax), -VEC(o->half, ax), VEC(o->half, ax));
+    *nBoxToSphere = vmul(o->axis[hitAxis], hitSign);
+    *xBox = obb_world(o, sl);
+    return 1;
+}
+
+/* The slab-top point of a round body's centre (collide.cpp:651-684, 689-708), or 0. */
+static int slab_point(const Obb *o, int thin, float sign, float radius, V3 center, V3 *xBox)
+{
+    V3 l = obb_local(o, center);
+    float sd = VEC(l, thin) * sign - VEC(o->half, thin);
+    if (sd > radius)
+        return 0;
+    for (int ax = 0; ax < 3; ++ax)
+    {
+        if (ax == thin)
+            continue;
+        if (VEC(l, ax) < -VEC(o->half, ax) - radius || VEC(l, ax) > VEC(o->half, ax) + radius)
+            return 0;
+    }
+    VE(l, thin) = VEC(o->half, thin) * sign;
+    for (int ax = 0; ax < 3; ++ax)
+        if (ax != thin)
+            VE(l, ax) = rclamp(VEC(l, ax), -VEC(o->half, ax), VEC(o->half, ax));
+    *xBox = obb_world(o, l);
+    return 1;
+}
+
+/* collideThinStaticBoxTopRound (collide.cpp:717-754): -1 when the box is no static slab */
+static int slab_top_round(const Obb *o, const Body *rb, const Body *box, int roundIsA, NewContact *cs, M3 *basis)
+{
+    int thin;
+    float sign;
+    if (!slab_frame(o, box, &thin, &sign))
+        return -1;
+    V3 n = vmul(o->axis[thin], sign);
+    V3 nAB = roundIsA ? vneg(n) : n;
+    *basis = orthonormal(vneg(nAB));
+    int count = 0;
+    V3 mids[8], ends[2];
+    int keys[2], nEnds;
+    if (rb->shape == ORACLE_SHAPE_CAPSULE)
+    {
+        round_segment(rb, &ends[0], &ends[1]);
+        keys[0] = 0x04000000;
+        keys[1] = 0x04000001;
+        nEnds = 2;
+    }
+    else
+    {
+        ends[0] = rb->pos;
+        keys[0] = 0x02000000;
+        nEnds = 1;
+    }
+    for (int e = 0; e < nEnds; ++e)
+    {
+        V3 xBox;
+        if (!slab_point(o, thin, sign, rb->shapeRadius, ends[e], &xBox))
+            continue;
+        V3 xRound = vsub(ends[e], vmul(n, rb->shapeRadius));
+        if (roundIsA)
+            add_contact(rb->pos, rb->q, box->pos, box->q, cs, &count, mids, xRound, xBox, keys[e]);
+        else
+            add_contact(box->pos, box->q, rb->pos, rb->q, cs, &count, mids, xBox, xRound, keys[e]);
+    }
+    return count > 0 ? count : -1;
+}
+
+/* collideRoundRound (collide.cpp:756-765) */
+static int collide_round_round(const Body *A, const Body *B, NewContact *cs, M3 *basis)
+{
+    V3 a0, a1, b0, b1, cA, cB;
+    round_segment(A, &a0, &a1);
+    round_segment(B, &b0, &b1);
+    closest_segments(a0, a1, b0, b1, &cA, &cB);
+    return round_contact(A, B, cA, A->shapeRadius, cB, B->shapeRadius, 0x03000000, cs, basis);
+}
+
+/* collideRoundBox (collide.cpp:767-896) */
+static int collide_round_box(const Body *rb, const Body *box, int roundIsA, float dt, NewContact *cs, M3 *basis)
+{
+    Obb o = make_obb(box->pos, box->q, box->size);
+    int top = slab_top_round(&o, rb, box, roundIsA, cs, basis);
+    if (top >= 0)
+        return top;
+    V3 rc = rb->pos;
+    if (rb->shape == ORACLE_SHAPE_CAPSULE)
+    {
+        V3 sa, sb;
+        round_segment(rb, &sa, &sb);
+        V3 ca = obb_closest(&o, sa), cb = obb_closest(&o, sb);
+        rc = vlensq(vsub(sa, ca)) <= vlensq(vsub(sb, cb)) ? sa : sb;
+    }
+    float rr = rb->shapeRadius;
+    V3 closest = obb_closest(&o, rc);
+    V3 boxToRound = vsub(rc, closest);
+    float d2 = vlensq(boxToRound);
+    int onTop = 0;
+    {
+        /* thinStaticBoxTopContactRound (collide.cpp:632-685) */
+        int thin;
+        float sign;
+        if (slab_frame(&o, box, &thin, &sign))
+        {
+            V3 n = vmul(o.axis[thin], sign);
+            V3 sa, sb;
+            round_segment(rb, &sa, &sb);
+            float da = vdot(sa, n), db = vdot(sb, n);
+            V3 topCenter;
+            if (rb->shape == ORACLE_SHAPE_CAPSULE && fabsf(da - db) < 1.0e-4f)
+                topCenter = segment_closest(sa, sb, rb->pos);
+            else
+                topCenter = da <= db ? sa : sb;
+            V3 xBox;
+            if (slab_point(&o, thin, sign, rr, topCenter, &xBox))
+            {
+                rc = topCenter;
+                boxToRound = n;
+                closest = xBox;
+                d2 = 1.0f;
+                onTop = 1;
+            }
+        }
+    }
+    V3 local = obb_local(&o, rc);
+    int inside = fabsf(local.x) <= o.half.x && fabsf(local.y) <= o.half.y && fabsf(local.z) <= o.half.z;
+    if (onTop)
+    {
+    }
+    else if (inside)
+    {
+        V3 sn, sp;
+        if (rb->shape == ORACLE_SHAPE_SPHERE && swept_sphere_box(&o, rb, box, dt, &sn, &sp))
+        {
+            boxToRound = sn;
+            closest = sp;
+            d2 = 1.0f;
+        }
+        else
+        {
+            int axis = 0;
+            float sign = local.x >= 0.0f ? 1.0f : -1.0f;
+            float best = o.half.x - fabsf(local.x);
+            V3 rv = vsub(rb->vel, box->vel);
+            if (box->mass <= 0.0f)
+            {
+                axis = 0;
+                if (o.half.y < VEC(o.half, axis))
+                    axis = 1;
+                if (o.half.z < VEC(o.half, axis))
+                    axis = 2;
+                sign = vdot(o.axis[axis], v3(0.0f, 0.0f, 1.0f)) >= 0.0f ? 1.0f : -1.0f;
+            }
+            else if (vlensq(rv) > SAT_EPS)
+            {
+                V3 against = vneg(rv);
+                float bestDot = -FLT_MAX;
+                for (int ca = 0; ca < 3; ++ca)
+                    for (int si = 0; si < 2; ++si)
+                    {
+                        float cs_ = si == 0 ? -1.0f : 1.0f;
+                        float d = vdot(vmul(o.axis[ca], cs_), against);
+                        if (d > bestDot)
+                        {
+                            bestDot = d;
+                            axis = ca;
+                            sign = cs_;
+                        }
+                    }
+            }
+            else
+            {
+                float dy = o.half.y - fabsf(local.y);
+                if (dy < best)
+                {
+                    axis = 1;
+                    sign = local.y >= 0.0f ? 1.0f : -1.0f;
+                    best = dy;
+                }
+                float dz = o.half.z - fabsf(local.z);
+                if (dz < best)
+                {
+                    axis = 2;
+                    sign = local.z >= 0.0f ? 1.0f : -1.0f;
+                }
+            }
+            V3 sl = local;
+            VE(sl, axis) = VEC(o.half, axis) * sign;
+            closest = obb_world(&o, sl);
+            boxToRound = vmul(o.axis[axis], sign);
+            d2 = 1.0f;
+        }
+    }
+    else if (d2 > rr * rr)
+    {
+        V3 sn, sp;
+        if (rb->shape != ORACLE_SHAPE_SPHERE || !swept_sphere_box(&o, rb, box, dt, &sn, &sp))
+            return 0;
+        boxToRound = sn;
+        closest = sp;
+        d2 = 1.0f;
+    }
+    V3 nBR = d2 > SAT_EPS ? vdiv(boxToRound, sqrtf(d2)) : v3(0.0f, 0.0f, 1.0f);
+    V3 nAB = roundIsA ? vneg(nBR) : nBR;
+    V3 xRound = vsub(rc, vmul(nBR, rr));
+    *basis = orthonormal(vneg(nAB));
+    int count = 0;
+    V3 mids[8];
+    int key = rb->shape == ORACLE_SHAPE_CAPSULE ? 0x04000000 : 0x02000000;
+    if (roundIsA)
+        add_contact(rb->pos, rb->q, box->pos, box->q, cs, &count, mids, xRound, closest, key);
+    else
+        add_contact(box->pos, box->q, rb->pos, rb->q, cs, &count, mids, closest, xRound, key);
+    return count;
+}
+
+/* addThinStaticBoxTopCylinderContact (collide.cpp:978-1007) */
+static void slab_cylinder_point(const Obb *o, const Body *cyl, const Body *box, int cylIsA, int thin, float sign, V3 xc,
+                                int key, NewContact *cs, int *count, V3 *mids)
+{
+    V3 l = v3(vdot(vsub(xc, o->center), o->axis[0]), vdot(vsub(xc, o->center), o->axis[1]),
+              vdot(vsub(xc, o->center), o->axis[2]));
+    float sd = VEC(l, thin) * sign - VEC(o->half, thin);
+    if (sd > COLLISION_MARGIN)
+        return;
+    for (int ax = 0; ax < 3; ++ax)
+    {
+        if (ax == thin)
+            continue;
+        if (VEC(l, ax) < -VEC(o->half, ax) - cyl->shapeRadius || VEC(l, ax) > VEC(o->half, ax) + cyl->shapeRadius)
+            return;
+    }
+    VE(l, thin) = (VEC(o->half, thin) + COLLISION_MARGIN) * sign;
+    for (int ax = 0; ax < 3; ++ax)
+        if (ax != thin)
+            VE(l, ax) = rclamp(VEC(l, ax), -VEC(o->half, ax), VEC(o->half, ax));
+    V3 xBox = obb_world(o, l);
+    if (cylIsA)
+        add_contact(cyl->pos, cyl->q, box->pos, box->q, cs, count, mids, xc, xBox, key);
+    else
+        add_contact(box->pos, box->q, cyl->pos, cyl->q, cs, count, mids, xBox, xc, key);
+}
+
+static void across(V3 a, V3 *u, V3 *v)
+{
+    *u = fabsf(a.x) > fabsf(a.z) ? vnormalize(v3(-a.y, a.x, 0.0f)) : vnormalize(v3(0.0f, -a.z, a.y));
+    *v = vnormalize(vcross(a, *u));
+}
+
+/* collideThinStaticBoxTopCylinder (collide.cpp:1009-1053) */
+static int slab_top_cylinder(const Obb *o, const Body *cyl, const Body *box, int cylIsA, NewContact *cs, M3 *basis)
+{
+    int thin;
+    float sign;
+    if (!slab_frame(o, box, &thin, &sign))
+        return -1;
+    V3 n = vmul(o->axis[thin], sign);
+    V3 nAB = cylIsA ? vneg(n) : n;
+    *basis = orthonormal(vneg(nAB));
+    V3 axis = qrotate(cyl->q, v3(0.0f, 0.0f, 1.0f));
+    float ad = vdot(axis, n);
+    int count = 0;
+    V3 mids[8];
+    if (fabsf(ad) > 0.65f)
+    {
+        float as = ad >= 0.0f ? 1.0f : -1.0f;
+        V3 cap = vsub(cyl->pos, vmul(axis, cyl->halfLength * as));
+        V3 u, v;
+        across(axis, &u, &v);
+        V3 offs[4] = {vmul(u, cyl->shapeRadius), vmul(vneg(u), cyl->shapeRadius), vmul(v, cyl->shapeRadius),
+                      vmul(vneg(v), cyl->shapeRadius)};
+        for (int i = 0; i < 4; ++i)
+            slab_cylinder_point(o, cyl, box, cylIsA, thin, sign, vadd(cap, offs[i]), 0x05000000 | i, cs, &count, mids);
+    }
+    else
+    {
+        V3 radial = vsub(n, vmul(axis, ad));
+        if (vlensq(radial) < SAT_EPS)
+            radial = n;
+        radial = vnormalize(radial);
+        V3 a = vsub(cyl->pos, vmul(axis, cyl->halfLength));
+        V3 b = vadd(cyl->pos, vmul(axis, cyl->halfLength));
+        slab_cylinder_point(o, cyl, box, cylIsA, thin, sign, vsub(a, vmul(radial, cyl->shapeRadius)), 0x05000100, cs,
+                            &count, mids);
+        slab_cylinder_point(o, cyl, box, cylIsA, thin, sign, vsub(b, vmul(radial, cyl->shapeRadius)), 0x05000101, cs,
+                            &count, mids);
+    }
+    return count > 0 ? count : -1;
+}
+
+/* addCylinderCapContacts (collide.cpp:1080-1091) */
+static int cylinder_caps(const Body *A, const Body *B, V3 nAB, V3 capA, V3 capB, float radius, NewContact *cs, M3 *basis)
+{
+    *basis = orthonormal(vneg(nAB));
+    int count = 0;
+    V3 mids[8], u, v;
+    across(nAB, &u, &v);
+    V3 offs[4] = {vmul(u, radius), vmul(vneg(u), radius), vmul(v, radius), vmul(vneg(v), radius)};
+    for (int i = 0; i < 4; ++i)
+        add_contact(A->pos, A->q, B->pos, B->q, cs, &count, mids, vadd(capA, offs[i]), vadd(capB, offs[i]),
+                    0x06000000 | i);
+    return count;
+}
+
+/* collideCylinders (collide.cpp:1093-1150) */
+static int collide_cylinders(const Body *A, const Body *B, NewContact *cs, M3 *basis)
+{
+    V3 axA = qrotate(A->q, v3(0.0f, 0.0f, 1.0f));
+    V3 axB = qrotate(B->q, v3(0.0f, 0.0f, 1.0f));
+    float par = vdot(axA, axB);
+    V3 delta = vsub(B->pos, A->pos);
+    if (fabsf(par) > 0.95f)
+    {
+        float axial = vdot(delta, axA);
+        V3 radial = vsub(delta, vmul(axA, axial));
+        float rl2 = vlensq(radial);
+        float rs = A->shapeRadius + B->shapeRadius;
+        if (rl2 > rs * rs)
+            return 0;
+        float overlap = A->halfLength + B->halfLength - fabsf(axial);
+        if (overlap < -COLLISION_MARGIN)
+            return 0;
+        if (fabsf(axial) > (A->halfLength + B->halfLength) * 0.5f)
+        {
+            float side = axial >= 0.0f ? 1.0f : -1.0f;
+            V3 nAB = vmul(axA, side);
+            V3 capA = vadd(A->pos, vmul(nAB, A->halfLength));
+            V3 capB = vsub(B->pos, vmul(nAB, B->halfLength));
+            return cylinder_caps(A, B, nAB, capA, capB, rmin(A->shapeRadius, B->shapeRadius) * 0.85f, cs, basis);
+        }
+        V3 nAB = rl2 > SAT_EPS ? vdiv(radial, sqrtf(rl2)) : orthonormal(axA).r[1];
+        *basis = orthonormal(vneg(nAB));
+        int count = 0;
+        V3 mids[8];
+        float vals[2] = {rmax(-A->halfLength, axial - B->halfLength), rmin(A->halfLength, axial + B->halfLength)};
+        for (int i = 0; i < 2; ++i)
+        {
+            float tA = vals[i], tB = tA - axial;
+            V3 xA = vadd(vadd(A->pos, vmul(axA, tA)), vmul(nAB, A->shapeRadius));
+            V3 xB = vsub(vadd(B->pos, vmul(axA, tB)), vmul(nAB, B->shapeRadius));
+            add_contact(A->pos, A->q, B->pos, B->q, cs, &count, mids, xA, xB, 0x06000100 | i);
+        }
+        return count;
+    }
+    V3 a0, a1, b0, b1, cA, cB;
+    round_segment(A, &a0, &a1);
+    round_segment(B, &b0, &b1);
+    closest_segments(a0, a1, b0, b1, &cA, &cB);
+    return round_contact(A, B, cA, A->shapeRadius, cB, B->shapeRadius, 0x06000200, cs, basis);
+}
+
+/* collideCylinderRound (collide.cpp:1065-1078) */
+static int collide_cylinder_round(const Body *cyl, const Body *rb, int cylIsA, NewContact *cs, M3 *basis)
+{
+    V3 c0, c1, r0, r1, cc, cr;
+    round_segment(cyl, &c0, &c1);
+    round_segment(rb, &r0, &r1);
+    closest_segments(c0, c1, r0, r1, &cc, &cr);
+    if (cylIsA)
+        return round_contact(cyl, rb, cc, cyl->shapeRadius, cr, rb->shapeRadius, 0x07000000, cs, basis);
+    return round_contact(rb, cyl, cr, rb->shapeRadius, cc, cyl->shapeRadius, 0x07000000, cs, basis);
+}
+
+/* Manifold::collide (collide.cpp:1154-1176) */
+static int collide_shapes(const Body *A, const Body *B, float dt, NewContact *cs, M3 *basis)
+{
+    if (is_cyl(A) && is_cyl(B))
+        return collide_cylinders(A, B, cs, basis);
+    if (is_cyl(A) && is_round(B))
+        return collide_cylinder_round(A, B, 1, cs, basis);
+    if (is_round(A) && is_cyl(B))
+        return collide_cylinder_round(B, A, 0, cs, basis);
+    if (is_cyl(A) && B->shape == ORACLE_SHAPE_BOX)
+    {
+        Obb o = make_obb(B->pos, B->q, B->size);
+        int top = slab_top_cylinder(&o, A, B, 1, cs, basis);
+        return top >= 0 ? top : collide_boxes(A->pos, A->q, A->size, B->pos, B->q, B->size, cs, basis);
+    }
+    if (A->shape == ORACLE_SHAPE_BOX && is_cyl(B))
+    {
+        Obb o = make_obb(A->pos, A->q, A->size);
+        int top = slab_top_cylinder(&o, B, A, 0, cs, basis);
+        return top >= 0 ? top : collide_boxes(A->pos, A->q, A->size, B->pos, B->q, B->size, cs, basis);
+    }
+    if (is_round(A) && is_round(B))
+        return collide_round_round(A, B, cs, basis);
+    if (is_round(A) && B->shape == ORACLE_SHAPE_BOX)
+        return collide_round_box(A, B, 1, dt, cs, basis);
+    if (A->shape == ORACLE_SHAPE_BOX && is_round(B))
+        return collide_round_box(B, A, 0, dt, cs, basis);
+    return collide_boxes(A->pos, A->q, A->size, B->pos, B->q, B->size, cs, basis);
+}
+
+/* contactOffsetWorld (manifold.cpp:28-91) */
+static V3 contact_offset(const Body *b, V3 lo, M3 basis, int isA, int key)
+{
+    if (b->shape == ORACLE_SHAPE_SPHERE)
+        return vmul(basis.r[0], isA ? -b->shapeRadius : b->shapeRadius);
+    if (b->shape == ORACLE_SHAPE_CAPSULE)
+    {
+        V3 axis = qrotate(b->q, v3(0.0f, 0.0f, 1.0f));
+        V3 n = basis.r[0];
+        V3 nl = qrotate(qconj(b->q), n);
+        float cz = isA ? lo.z + nl.z * b->shapeRadius : lo.z - nl.z * b->shapeRadius;
+        cz = rclamp(cz, -b->halfLength, b->halfLength);
+        return vadd(vmul(axis, cz), vmul(n, isA ? -b->shapeRadius : b->shapeRadius));
+    }
+    if (b->shape == ORACLE_SHAPE_CYLINDER)
+    {
+        V3 sw = vmul(basis.r[0], isA ? -1.0f : 1.0f);
+        V3 sl = qrotate(qconj(b->q), sw);
+        float stored = sqrtf(lo.x * lo.x + lo.y * lo.y);
+        int cap = (key & 0xFFFFFF00) == 0x05000000 || (key & 0xFFFFFF00) == 0x06000000;
+        if (cap)
+        {
+            V3 l = v3(0.0f, 0.0f, 0.0f);
+            if (stored > 1.0e-6f)
+            {
+                l.x = lo.x / stored * b->shapeRadius;
+                l.y = lo.y / stored * b->shapeRadius;
+            }
+            float capSign = fabsf(lo.z) > 1.0e-6f ? (lo.z >= 0.0f ? 1.0f : -1.0f) : (sl.z >= 0.0f ? 1.0f : -1.0f);
+            l.z = b->halfLength * capSign;
+            return qrotate(b->q, l);
+        }
+        float radialLen = sqrtf(sl.x * sl.x + sl.y * sl.y);
+        float z = fabsf(sl.z) > 0.15f ? (sl.z >= 0.0f ? b->halfLength : -b->halfLength)
+                                      : rclamp(lo.z, -b->halfLength, b->halfLength);
+        V3 l = v3(0.0f, 0.0f, z);
+        if (radialLen > 1.0e-6f)
+        {
+            l.x = sl.x / radialLen * b->shapeRadius;
+            l.y = sl.y / radialLen * b->shapeRadius;
+        }
+        else if (stored > 1.0e-6f)
+        {
+            l.x = lo.x / stored * b->shapeRadius;
+            l.y = lo.y / stored * b->shapeRadius;
+        }
+        return qrotate(b->q, l);
+    }
+    return qrotate(b->q, lo);
+}
+
 /* Manifold::initialize (manifold.cpp:100-174), boxes only */
 static int manifold_init(OracleWorld *w, Manifold *m)
 {
     const Body *A = &w->bodies[m->a], *B = &w->bodies[m->b];
     m->friction = sqrtf(A->friction * B->friction);
+    if (A->shape == ORACLE_SHAPE_SPHERE || B->shape == ORACLE_SHAPE_SPHERE)
+        m->friction = 0.0f;
+    /* manifold.cpp:120-147: round manifolds (cylinders included) refresh their contact
+     * locations and restart the tangential rows every step */
+    int round = A->shape != ORACLE_SHAPE_BOX || B->shape != ORACLE_SHAPE_BOX;
     NewContact nc[8];
     memset(nc, 0, sizeof(nc));
     M3 basis = m->basis;
-    int nn = collide_boxes(A->pos, A->q, A->size, B->pos, B->q, B->size, nc, &basis);
+    int nn = collide_shapes(A, B, w->p.dt, nc, &basis);
     m->basis = basis;
     Contact merged[8];
     memset(merged, 0, sizeof(merged));
@@ -1067,10 +1662,18 @@ static int manifold_init(OracleWorld *w, Manifold *m)
             {
                 merged[i] = m->c[j];
                 m->srcSlot[i] = j;
-                if (!m->c[j].stick)
+                if (round || !m->c[j].stick)
                 {
                     merged[i].rA = nc[i].rA;
                     merged[i].rB = nc[i].rB;
+                }
+                if (round)
+                {
+                    merged[i].lambda.y = 0.0f;
+                    merged[i].lambda.z = 0.0f;
+                    merged[i].penalty.y = PENALTY_MIN;
+                    merged[i].penalty.z = PENALTY_MIN;
+                    merged[i].stick = 0;
                 }
                 break;
             }
@@ -1081,8 +1684,8 @@ static int manifold_init(OracleWorld *w, Manifold *m)
     for (int i = 0; i < nn; ++i)
     {
         Contact *c = &m->c[i];
-        V3 xA = vadd(A->pos, qrotate(A->q, c->rA));
-        V3 xB = vadd(B->pos, qrotate(B->q, c->rB));
+        V3 xA = vadd(A->pos, contact_offset(A, c->rA, m->basis, 1, c->key));
+        V3 xB = vadd(B->pos, contact_offset(B, c->rB, m->basis, 0, c->key));
         c->C0 = vadd(mvmul(m->basis, vsub(xA, xB)), v3(COLLISION_MARGIN, 0, 0));
         c->lambda = vmul(vmul(c->lambda, w->p.alpha), w->p.gamma);
         V3 pg = vmul(c->penalty, w->p.gamma);
@@ -1376,8 +1979,8 @@ static void manifold_primal(const OracleWorld *w, const Manifold *m, int bodyIsA
     for (int i = 0; i < m->n; ++i)
     {
         const Contact *c = &m->c[i];
-        V3 rAW = qrotate(A->q, c->rA);
-        V3 rBW = qrotate(B->q, c->rB);
+        V3 rAW = contact_offset(A, c->rA, m->basis, 1, c->key);
+        V3 rBW = contact_offset(B, c->rB, m->basis, 0, c->key);
         M3 jALin = m->basis;
         M3 jBLin = mneg(m->basis);
         M3 jAAng = m3rows(vcross(rAW, jALin.r[0]), vcross(rAW, jALin.r[1]), vcross(rAW, jALin.r[2]));
@@ -1544,8 +2147,8 @@ static void manifold_dual(OracleWorld *w, Manifold *m, float alpha)
     for (int i = 0; i < m->n; ++i)
     {
         Contact *c = &m->c[i];
-        V3 rAW = qrotate(A->q, c->rA);
-        V3 rBW = qrotate(B->q, c->rB);
+        V3 rAW = contact_offset(A, c->rA, m->basis, 1, c->key);
+        V3 rBW = contact_offset(B, c->rB, m->basis, 0, c->key);
         M3 jALin = m->basis;
         M3 jBLin = mneg(m->basis);
         M3 jAAng = m3rows(vcross(rAW, jALin.r[0]), vcross(rAW, jALin.r[1]), vcross(rAW, jALin.r[2]));
@@ -1661,6 +2264,31 @@ int oracle_finish(OracleWorld *w)
             body->angvel = vdiv(qdiff(body->q, body->initAng), dt);
         }
     }
+    /* applySphereRollingFriction (solver.cpp:628-662) over the manifolds in the solver's
+     * force order (newest first) */
+    for (int k = w->nMan - 1; k >= 0; --k)
+    {
+        const Manifold *m = &w->man[k];
+        Body *A = &w->bodies[m->a], *B = &w->bodies[m->b];
+        Body *sphere = A->shape == ORACLE_SHAPE_SPHERE ? A : (B->shape == ORACLE_SHAPE_SPHERE ? B : NULL);
+        Body *other = sphere == A ? B : A;
+        if (!sphere || sphere->mass <= 0.0f || other->mass > 0.0f || m->n <= 0)
+            continue;
+        float mf = sqrtf(sphere->friction * other->friction);
+        if (mf <= 0.0f)
+            continue;
+        float blend = rclamp(mf * 0.08f, 0.0f, 0.18f);
+        for (int i = 0; i < m->n; ++i)
+        {
+            V3 n = sphere == A ? m->basis.r[0] : vneg(m->basis.r[0]);
+            V3 r = vmul(vneg(n), sphere->shapeRadius);
+            V3 cv = vadd(sphere->vel, vcross(sphere->angvel, r));
+            V3 tv = vsub(cv, vmul(n, vdot(cv, n)));
+            sphere->vel = vsub(sphere->vel, vmul(tv, blend));
+            V3 desired = vdiv(vcross(n, sphere->vel), sphere->shapeRadius);
+            sphere->angvel = vadd(sphere->angvel, vmul(vsub(desired, sphere->angvel), blend));
+        }
+    }
     return 0;
 }
 
@@ -1748,6 +2376,63 @@ OracleWorld *oracle_create(const OracleParams *params, int nBodies, const float 
                            int nForces, const int *ftype, const int *fa, const int *fb, const float *frA3,
                            const float *frB3, const float *fparam3)
 {
+    return oracle_create_shapes(params, nBodies, NULL, NULL, size3, density, friction, pos3, vel3, quat4, nForces,
+                                ftype, fa, fb, frA3, frB3, fparam3);
+}
+
+/* sphereMass (rigid.cpp:18-21); PI as rigid.cpp:16 */
+#define RIGID_PI 3.14159265358979323846f
+static float sphere_mass(float r, float density) { return 4.0f / 3.0f * RIGID_PI * r * r * r * density; }
+
+/* Rigid::makeSphere / makeCapsule / makeCylinder (rigid.cpp:44-90): the shape, the
+ * constructor's size, then mass, moment and bounding radius. */
+static void round_body(Body *b, int shape, float r, float h, float density)
+{
+    float d = r * 2.0f;
+    b->shape = shape;
+    b->shapeRadius = r;
+    if (shape == ORACLE_SHAPE_SPHERE)
+    {
+        b->size = v3(d, d, d);
+        b->halfLength = 0.0f;
+        b->mass = sphere_mass(r, density);
+        float inertia = 2.0f / 5.0f * b->mass * r * r;
+        b->moment = v3(inertia, inertia, inertia);
+        b->radius = r;
+    }
+    else if (shape == ORACLE_SHAPE_CAPSULE)
+    {
+        float cylLen = h * 2.0f;
+        b->size = v3(d, d, cylLen + d);
+        b->halfLength = h;
+        float cylMass = RIGID_PI * r * r * cylLen * density;
+        float capMass = sphere_mass(r, density);
+        b->mass = cylMass + capMass;
+        float axial = 0.5f * cylMass * r * r + 2.0f / 5.0f * capMass * r * r;
+        float trans = (3.0f * r * r + cylLen * cylLen) / 12.0f * cylMass + 2.0f / 5.0f * capMass * r * r +
+                      capMass * h * h;
+        b->moment = v3(trans, trans, axial);
+        b->radius = h + r;
+    }
+    else
+    {
+        float height = h * 2.0f;
+        b->size = v3(d, d, height);
+        b->halfLength = h;
+        b->mass = RIGID_PI * r * r * height * density;
+        float axial = 0.5f * b->mass * r * r;
+        float trans = (3.0f * r * r + height * height) / 12.0f * b->mass;
+        b->moment = v3(trans, trans, axial);
+        b->radius = sqrtf(r * r + h * h);
+    }
+}
+
+OracleWorld *oracle_create_shapes(const OracleParams *params, int nBodies, const int *shape, const float *dim2,
+                                  const float *size3, const float *density, const float *friction,
+                                  const float *pos3, const float *vel3, const float *quat4, int nForces,
+                                  const int *ftype, const int *fa, const int *fb, const float *frA3,
+                                  const float *frB3, const float *fparam3)
+{
     OracleWorld *w = (OracleWorld *)calloc(1, sizeof(OracleWorld));
     w->p = *params;
     w->n = nBodies;
@@ -1772,6 +2457,11 @@ OracleWorld *oracle_create(const OracleParams *params, int nBodies, const float 
                        (size.x * size.x + size.z * size.z) / 12.0f * b->mass,
                        (size.x * size.x + size.y * size.y) / 12.0f * b->mass);
         b->radius = vlen(vmul(size, 0.5f));
+        b->shape = ORACLE_SHAPE_BOX;
+        b->shapeRadius = b->radius;
+        b->halfLength = 0.0f;
+        if (shape && shape[c] != ORACLE_SHAPE_BOX)
+            round_body(b, shape[c], dim2[2 * c], dim2[2 * c + 1], density[c]);
     }
     for (int k = 0; k < nForces; ++k)
     {

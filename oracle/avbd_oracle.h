@@ -56,6 +56,23 @@ OracleWorld *oracle_create(const OracleParams *params, int nBodies, const float 
                            const float *friction, const float *pos3, const float *vel3, const float *quat4,
                            int nForces, const int *ftype, const int *fa, const int *fb, const float *frA3,
                            const float *frB3, const float *fparam3);
+/* Body shapes (RigidShapeType, solver.h:47-53). */
+enum
+{
+    ORACLE_SHAPE_BOX = 0,
+    ORACLE_SHAPE_SPHERE = 1,
+    ORACLE_SHAPE_CAPSULE = 2,
+    ORACLE_SHAPE_CYLINDER = 3
+};
+
+/* As oracle_create, with a shape per body (creation order): boxes take size3; spheres,
+ * capsules and cylinders are built like Rigid::makeSphere / makeCapsule / makeCylinder
+ * (rigid.cpp:44-90) from dim2 = (radius, halfLength). shape NULL: all boxes. */
+OracleWorld *oracle_create_shapes(const OracleParams *params, int nBodies, const int *shape, const float *dim2,
+                                  const float *size3, const float *density, const float *friction,
+                                  const float *pos3, const float *vel3, const float *quat4, int nForces,
+                                  const int *ftype, const int *fa, const int *fb, const float *frA3,
+                                  const float *frB3, const float *fparam3);
 void oracle_destroy(OracleWorld *w);
 void oracle_set_params(OracleWorld *w, const OracleParams *params);
 

@@ -74,6 +74,8 @@ def _lib(kind: str) -> ctypes.CDLL:
     vp, ip, fp = ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p
     getattr(lib, p + "create").restype = vp
     getattr(lib, p + "create").argtypes = [ctypes.POINTER(_Params), ip] + [fp] * 6 + [ip] + [fp] * 6
+    getattr(lib, p + "create_shapes").restype = vp
+    getattr(lib, p + "create_shapes").argtypes = [ctypes.POINTER(_Params), ip, fp, fp] + [fp] * 6 + [ip] + [fp] * 6
     for name in ("destroy",):
         getattr(lib, p + name).argtypes = [vp]
         getattr(lib, p + name).restype = None
@@ -167,8 +169,14 @@ class World:
             scene.ftype, scene.fa, scene.fb, scene.frA, scene.frB, scene.fparam)]
         k = self._keep
         self.params = make_params(scene.params, order_mode)
-        self.h = self._f("create")(ctypes.byref(self.params), scene.n_bodies, *[_ptr(x) for x in k[:6]],
-                                   scene.n_forces, *[_ptr(x) for x in k[6:]])
+        if getattr(scene, "shape", None) is None:
+            self.h = self._f("create")(ctypes.byref(self.params), scene.n_bodies, *[_ptr(x) for x in k[:6]],
+                                       scene.n_forces, *[_ptr(x) for x in k[6:]])
+        else:  # round bodies built by the shape constructors
+            self._keep += [np.ascontiguousarray(scene.shape, np.int32), np.ascontiguousarray(scene.dims, np.float32)]
+            self.h = self._f("create_shapes")(ctypes.byref(self.params), scene.n_bodies, _ptr(self._keep[-2]),
+                                              _ptr(self._keep[-1]), *[_ptr(x) for x in k[:6]], scene.n_forces,
+                                              *[_ptr(x) for x in k[6:12]])
         self.n = scene.n_bodies
 
     def _f(self, name):

@@ -83,19 +83,32 @@ std::vector<T *> forces_of_type(RefWorld *w, SimConstraintType type)
 extern "C"
 {
 
-void *ref_create(const RefParams *params, int nBodies, const float *size3, const float *density,
-                 const float *friction, const float *pos3, const float *vel3, const float *quat4, int nForces,
-                 const int *ftype, const int *fa, const int *fb, const float *frA3, const float *frB3,
-                 const float *fparam3)
+/* shape (creation order, NULL = all boxes): 0 box (size3), 1 sphere, 2 capsule, 3 cylinder,
+ * built with the reference's Rigid::makeSphere / makeCapsule / makeCylinder from
+ * dim2 = (radius, halfLength). */
+void *ref_create_shapes(const RefParams *params, int nBodies, const int *shape, const float *dim2,
+                        const float *size3, const float *density, const float *friction, const float *pos3,
+                        const float *vel3, const float *quat4, int nForces, const int *ftype, const int *fa,
+                        const int *fb, const float *frA3, const float *frB3, const float *fparam3)
 {
     RefWorld *w = new RefWorld();
     apply_params(w->solver, params);
     std::vector<Rigid *> created;
     for (int c = 0; c < nBodies; ++c)
     {
-        Rigid *r = new Rigid(&w->solver, float3{size3[3 * c], size3[3 * c + 1], size3[3 * c + 2]}, density[c],
-                             friction[c], float3{pos3[3 * c], pos3[3 * c + 1], pos3[3 * c + 2]},
-                             float3{vel3[3 * c], vel3[3 * c + 1], vel3[3 * c + 2]});
+        float3 pos = float3{pos3[3 * c], pos3[3 * c + 1], pos3[3 * c + 2]};
+        float3 vel = float3{vel3[3 * c], vel3[3 * c + 1], vel3[3 * c + 2]};
+        int t = shape ? shape[c] : 0;
+        Rigid *r;
+        if (t == 1)
+            r = Rigid::makeSphere(&w->solver, dim2[2 * c], density[c], friction[c], pos, vel);
+        else if (t == 2)
+            r = Rigid::makeCapsule(&w->solver, dim2[2 * c], dim2[2 * c + 1], density[c], friction[c], pos, vel);
+        else if (t == 3)
+            r = Rigid::makeCylinder(&w->solver, dim2[2 * c], dim2[2 * c + 1], density[c], friction[c], pos, vel);
+        else
+            r = new Rigid(&w->solver, float3{size3[3 * c], size3[3 * c + 1], size3[3 * c + 2]}, density[c],
+                          friction[c], pos, vel);
         r->positionAng = quat{quat4[4 * c], quat4[4 * c + 1], quat4[4 * c + 2], quat4[4 * c + 3]};
         created.push_back(r);
     }
@@ -115,6 +128,15 @@ void *ref_create(const RefParams *params, int nBodies, const float *size3, const
     w->solver.world.syncFromLegacy(w->solver);
     rebuild_index(w);
     return w;
+}
+
+void *ref_create(const RefParams *params, int nBodies, const float *size3, const float *density,
+                 const float *friction, const float *pos3, const float *vel3, const float *quat4, int nForces,
+                 const int *ftype, const int *fa, const int *fb, const float *frA3, const float *frB3,
+                 const float *fparam3)
+{
+    return ref_create_shapes(params, nBodies, nullptr, nullptr, size3, density, friction, pos3, vel3, quat4, nForces,
+                             ftype, fa, fb, frA3, frB3, fparam3);
 }
 
 void ref_destroy(void *p) { delete (RefWorld *)p; }

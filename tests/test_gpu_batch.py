@@ -58,3 +58,25 @@ def test_batch_of_identical_worlds_is_identical(gpu):
     for w in range(1, 5):
         assert np.array_equal(bits(b[0]), bits(b[w]))
     g.close()
+
+
+def test_batch_with_round_worlds(gpu):
+    """Box-only and round-shape worlds in one batch: the round kernel instances serve every
+    world, and each world still evolves as the oracle evolves it alone."""
+    worlds = [scenes.round_mix(120, seed=31, cols=4), scenes.stack_grid(3, 3, 5, seed=7),
+              scenes.sphere_pour(200, seed=17), scenes.pyramid(8)]
+    g = World(worlds)
+    oracles = [checkers.World(sc, "oracle", order_mode=1) for sc in worlds]
+    ws = g.world_start
+    for step in range(1, 31):
+        g.step(1)
+        for o in oracles:
+            o.step(1)
+        if step % 10:
+            continue
+        b = g.bodies()
+        for w, o in enumerate(oracles):
+            ob = o.bodies()
+            for k in ("pos", "quat", "vel", "angvel"):
+                assert np.array_equal(bits(per_world(b[k], ws, w)), bits(ob[k])), (step, w, k)
+    g.close()

@@ -65,6 +65,8 @@ SMALL = {
     "cluster": lambda: scenes.box_cluster_probe(),
     "stacks": lambda: scenes.stack_grid(6, 6, 8, seed=3),
     "mixed": lambda: scenes.mixed_drop(3000, 20, 12, 0.05, extent=(30, 30, 20), seed=5),
+    "round_mix": lambda: scenes.round_mix(600, seed=11, cols=8),
+    "sphere_pour": lambda: scenes.sphere_pour(1000),
 }
 
 
@@ -73,7 +75,7 @@ def test_small_scenes_bit_exact_60_steps(gpu, name):
     lockstep(SMALL[name](), 60)
 
 
-@pytest.mark.parametrize("name", ["mixed", "breakable", "stacks", "springs"])
+@pytest.mark.parametrize("name", ["mixed", "breakable", "stacks", "springs", "round_mix"])
 def test_per_colour_launches(gpu, name):
     """The per-colour form (one launch per colour and iteration, then the dual sweep) gives
     the same bits as the oracle, like the default single-launch form."""

@@ -59,3 +59,25 @@ def test_snapshot_buffer_checks(gpu):
     g.lib.avbd_clear_error(g.h)
     g.step(1)
     g.close()
+
+
+def test_round_world_snapshot(gpu):
+    """Spheres, capsules and cylinders in the snapshot: shape code, material id, shape
+    radius and half length from the device's shape table."""
+    sc = scenes.round_mix(180, seed=43, cols=5)
+    n = sc.n_bodies
+    g = World(sc)
+    o = checkers.World(sc, "oracle", order_mode=1)
+    g.step(12)
+    o.step(12)
+    ob, pr = o.bodies(), o.body_props()
+    shape = np.asarray(sc.shape, np.int32)[::-1]
+    dims = np.asarray(sc.dims, np.float32)[::-1]
+    rnd = shape != 0
+    fields = checkers.snapshot_fields(n - 1 - np.arange(n), shape, pr["mass"], ob["pos"], ob["quat"], pr["size"],
+                                      np.where(rnd, dims[:, 0], pr["radius"]).astype(np.float32),
+                                      np.where(rnd, dims[:, 1], 0).astype(np.float32))
+    assert {f["shape"] for f in fields} == {0, 1, 2, 3}
+    assert g.snapshot_binary(3, "Round") == checkers.encode_snapshot(3, "Round", fields)
+    assert g.snapshot_json(3, "Round") == checkers.snapshot_json(3, "Round", fields)
+    g.close()

@@ -46,6 +46,30 @@ def test_mixed_constraints(colour):
     lockstep(scenes.mixed_drop(2000, 12, 10, 0.1, extent=(26, 26, 18), seed=23), 50, colour)
 
 
+@pytest.mark.parametrize("colour", [False, True])
+@pytest.mark.parametrize("scene", ["round_mix", "sphere_pour"])
+def test_round_shapes(scene, colour):
+    """Spheres, capsules and cylinders (rigid.cpp:44-90, collision.cpp round paths) with
+    rolling friction: the same bodies, manifolds and counters as the reference."""
+    sc = scenes.round_mix(300, seed=11, cols=6) if scene == "round_mix" else scenes.sphere_pour(300)
+    lockstep(sc, 60, colour)
+
+
+def test_round_body_properties_match_reference():
+    """Mass and shape fields of round bodies as the reference's SimWorld holds them."""
+    sc = scenes.round_mix(200, seed=19, cols=5)
+    o = checkers.World(sc, "oracle", order_mode=0)
+    r = checkers.World(sc, "ref")
+    wb, pr = r.world_bodies(), o.body_props()
+    n = sc.n_bodies
+    assert np.array_equal(wb["shape"], np.asarray(sc.shape, np.int32))
+    assert np.array_equal(bits(wb["mass"]), bits(pr["mass"][::-1]))
+    rnd = np.asarray(sc.shape) != 0
+    assert np.array_equal(bits(wb["radius"][rnd]), bits(np.asarray(sc.dims, np.float32)[rnd, 0]))
+    assert np.array_equal(bits(wb["half_length"][rnd]), bits(np.asarray(sc.dims, np.float32)[rnd, 1]))
+    assert len(wb["active"]) == n
+
+
 @pytest.mark.parametrize("mode", [scenes.BROADPHASE_ALL_PAIRS, scenes.BROADPHASE_SAP])
 def test_other_broadphase_modes(mode):
     sc = scenes.stack_grid(5, 5, 6, seed=25)
@@ -145,6 +169,31 @@ def test_snapshot_fields_match_reference_world():
     assert dec["frame"] == 1234 and dec["scene"] == "Mixed" and [b["id"] for b in dec["bodies"]] == list(range(n))
     assert all(np.array_equal(b["pos"], f["pos"]) and b["material"] == f["material"]
                for b, f in zip(dec["bodies"], ref))
+
+
+def test_round_snapshot_matches_reference_world():
+    """Snapshot of a world with round bodies: shape codes, sphere/cylinder/capsule materials,
+    shape radius and half length as the reference's SimWorld reports them."""
+    sc = scenes.round_mix(150, seed=41, cols=5)
+    o = checkers.World(sc, "oracle", order_mode=0)
+    r = checkers.World(sc, "ref")
+    o.step(20)
+    r.step(20)
+    wb = r.world_bodies()
+    n = sc.n_bodies
+    ref = checkers.snapshot_fields(np.arange(n), wb["shape"], wb["mass"], wb["pos"], wb["quat"], wb["size"],
+                                   wb["radius"], wb["half_length"])
+    ob, pr = o.bodies(), o.body_props()
+    shape = np.asarray(sc.shape, np.int32)[::-1]
+    dims = np.asarray(sc.dims, np.float32)[::-1]
+    rnd = shape != 0
+    radius = np.where(rnd, dims[:, 0], pr["radius"]).astype(np.float32)
+    half = np.where(rnd, dims[:, 1], 0).astype(np.float32)
+    mine = checkers.snapshot_fields(n - 1 - np.arange(n), shape, pr["mass"], ob["pos"], ob["quat"], pr["size"],
+                                    radius, half)
+    assert {b["shape"] for b in ref} == {0, 1, 2, 3}
+    assert checkers.encode_snapshot(7, "Round", ref) == checkers.encode_snapshot(7, "Round", mine)
+    assert checkers.snapshot_json(7, "Round", ref) == checkers.snapshot_json(7, "Round", mine)
 
 
 def test_narrowphase_random_pairs():

@@ -153,6 +153,7 @@ struct AvbdContext
     bool hasSpheres = false; // rolling friction pass after the velocity update
     int iterBlocks = 0;       // co-resident blocks of the iteration kernel (0: not launchable)
     DArr<IterSync> iterSync;
+    DArr<int> iterDone; // per body: iterations completed in the running iteration launch
     int *hIterError = nullptr; // pinned: barrier expiry of the last iteration kernel
     int colourMode = 0;       // 0 greedy (list-index priority), 1 hashed priority
     int *hColourSummary = nullptr; // pinned: vertices, rounds, max colour, error
@@ -470,7 +471,9 @@ __global__ void k_solve_list_all(const unsigned *keys, int n, int *list, int *co
         int2 row = rows[r];
         int p = row_partner(row);
         bool own = p < 0 || colour[p] < 0 || cb < colour[p];
+        bool later = p >= 0 && colour[p] >= 0 && cb < colour[p];
         row.y = own ? (row.y | ROW_OWNS_DUAL) : (row.y & ~ROW_OWNS_DUAL);
+        row.y = later ? (row.y | ROW_PARTNER_LATER) : (row.y & ~ROW_PARTNER_LATER);
         rows[r] = row;
     }
     int c = (int)(key >> 24);
@@ -979,7 +982,11 @@ int iterate_persistent(AvbdContext *ctx)
     const int4 *entries = ctx->solveEntry.p;
     const int *colourStart = ctx->colourStart.p;
     IterSync *sync = ctx->iterSync.p;
-    void *args[] = {&B, &F, &P, &entries, &colourStart, &nColours, &iterations, &sync};
+    // per-body completed iterations, from zero in every launch
+    CHECK(reserve(ctx, ctx->iterDone, ctx->n, false));
+    CU(cudaMemsetAsync(ctx->iterDone.p, 0, sizeof(int) * (size_t)ctx->n, ctx->stream));
+    int *done = ctx->iterDone.p;
+    void *args[] = {&B, &F, &P, &entries, &colourStart, &nColours, &iterations, &sync, &done};
     {
         PhaseScope ps(ctx, AVBD_PHASE_PRIMAL);
         // worlds with round bodies run the instance that evaluates their contact offsets
@@ -1579,6 +1586,7 @@ void avbd_destroy(AvbdContext *ctx)
     if (ctx->hIterError)
         cudaFreeHost(ctx->hIterError);
     release(ctx->iterSync);
+    release(ctx->iterDone);
     if (ctx->stageDone)
         cudaEventDestroy(ctx->stageDone);
     if (ctx->evStart)

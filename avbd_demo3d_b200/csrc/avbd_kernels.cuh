@@ -2068,6 +2068,9 @@ AVBD_DEV int entry_partner(const DevForces &F, unsigned e)
 // Bit 30 marks the rows whose contact this body updates in a fused dual pass: the body
 // with the lower colour, or the only dynamic one (set after colouring).
 constexpr int ROW_OWNS_DUAL = 1 << 30;
+// Bit 31: the partner is dynamic with a higher colour (so with ROW_OWNS_DUAL clear, the
+// partner is dynamic with a lower colour; with both clear, it is static or absent).
+constexpr int ROW_PARTNER_LATER = (int)0x80000000u;
 AVBD_DEV int row_sub(int2 row) { return row.y & 7; }
 AVBD_DEV int row_partner(int2 row) { return ((row.y & (ROW_OWNS_DUAL - 1)) >> 3) - 1; }
 
@@ -2156,14 +2159,15 @@ template <bool COH = false>
 AVBD_DEV void initial_system(const DevBodies &B, int b, float dt, float *t)
 {
     float4 mm4 = B.massMoment[b];
-    M3 MLin = diag(mm4.x, mm4.x, mm4.x);
-    M3 MAng = diag(mm4.y, mm4.z, mm4.w);
     float dt2 = dt * dt;
-    M3 lhsLin = mdivs(MLin, dt2);
-    M3 lhsAng = mdivs(MAng, dt2);
+    // diag(m) / dt2 entry by entry, as the reference divides the whole matrix: the
+    // diagonal divided, the off-diagonal zeros' quotient 0 / dt2 formed once
+    const float z = zero_over(dt2), ml = fdiv(mm4.x, dt2);
+    M3 lhsLin = rows(f3(ml, z, z), f3(z, ml, z), f3(z, z, ml));
+    M3 lhsAng = rows(f3(fdiv(mm4.y, dt2), z, z), f3(z, fdiv(mm4.z, dt2), z), f3(z, z, fdiv(mm4.w, dt2)));
     M3 lhsCross = diag(0, 0, 0);
-    float3 rhsLin = mv(mdivs(MLin, dt2), sub(xyz(ld_state<COH>(B.pos + b)), xyz(B.inertLin[b])));
-    float3 rhsAng = mv(mdivs(MAng, dt2), qdiff(ld_state<COH>(B.quat + b), B.inertAng[b]));
+    float3 rhsLin = mv(lhsLin, sub(xyz(ld_state<COH>(B.pos + b)), xyz(B.inertLin[b])));
+    float3 rhsAng = mv(lhsAng, qdiff(ld_state<COH>(B.quat + b), B.inertAng[b]));
     store_terms(t, lhsLin, lhsAng, lhsCross, rhsLin, rhsAng);
 }
 
@@ -2174,6 +2178,7 @@ struct PrimalShared
     static constexpr int GPB = BLOCK / G;
     float term[GPB][G][E_COUNT];
     float sys[GPB][E_COUNT]; // odd stride: one system per thread without bank conflicts
+    float4 start[4][GPB];    // the body's pose (position, orientation) and step-start pose
     unsigned kind[GPB][G];
     int body[GPB];
 };
@@ -2200,9 +2205,81 @@ AVBD_DEV void unit_sync()
 // block works in independent units of SUB threads (SUB / G bodies, which the unit's first
 // SUB / G threads factorise); every thread of the block calls this (it holds the units'
 // barriers).
+// Per-body progress of the iteration kernel when it runs without per-colour grid barriers:
+// done[b] = the iterations body b has completed in this launch. `done` null: the
+// barriers order the passes and nothing is waited for.
+struct IterFlow
+{
+    int *done = nullptr;
+    int it = 0;
+    int *error = nullptr;
+};
+
+AVBD_DEV int ld_acquire(const int *p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+AVBD_DEV void st_release(int *p, int v)
+{
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+constexpr unsigned FLOW_SPIN_LIMIT = 1u << 22;
+
+// A row reads its partner's pose (and, for a contact the partner owns, the contact's
+// multipliers) as the colour-ordered sweep leaves them: a partner of an earlier colour
+// must have finished this iteration, one of a later colour the previous iteration (so
+// that it has read this body's previous pose, and made its own contact updates). Static
+// partners never move. On expiry the wait records an error and gives up.
+AVBD_DEV void wait_partner(const IterFlow &flow, int2 row)
+{
+    const int need = (row.y & ROW_OWNS_DUAL) == 0 ? flow.it + 1 : ((row.y & ROW_PARTNER_LATER) ? flow.it : 0);
+    if (need == 0)
+        return;
+    const int *d = flow.done + row_partner(row);
+    unsigned spins = 0;
+    while (ld_acquire(d) < need)
+    {
+        if (++spins >= FLOW_SPIN_LIMIT)
+        {
+            atomicExch(flow.error, 1);
+            return;
+        }
+        if (spins > 64)
+        {
+            if (*(volatile int *)flow.error) // another wait expired: the launch is failing
+                return;
+            __nanosleep(64);
+        }
+    }
+}
+
+// `start`: the body's position, orientation, step-start position and step-start
+// orientation, staged in shared memory by the gathering lanes, so that no register holds
+// them across the factorisation.
+template <bool COH, int GPB>
+AVBD_DEV void solve_and_move(const DevBodies &B, int b, const float *sys, const float4 (*start)[GPB], int t,
+                             const IterFlow &flow)
+{
+    float3 dxl, dxa;
+    ldl_solve27(sys, dxl, dxa);
+    const float4 p0 = start[0][t], q0 = start[1][t], i0 = start[2][t], a0 = start[3][t];
+    float3 p = add(xyz(p0), dxl);
+    float4 q = qstep(q0, dxa);
+    B.pos[b] = f4(p, 0.0f);
+    B.quat[b] = q;
+    B.dqLin[b] = f4(sub(p, xyz(i0)), 0.0f);
+    B.dqAng[b] = f4(qdiff(q, a0), 0.0f);
+    if (flow.done) // a release: the body's pose, and the contact updates its rows made before
+        st_release(flow.done + b, flow.it + 1); // the block's barrier, are visible before the count
+}
+
 template <int G, int BLOCK, int SUB, bool COH, bool ROUND>
 AVBD_DEV void primal_batch(const DevBodies &B, const DevForces &F, const Params &P, const int4 *entries, int count,
-                           bool fusedDual, PrimalShared<G, BLOCK> &sh)
+                           bool fusedDual, PrimalShared<G, BLOCK> &sh, const IterFlow &flow = IterFlow{})
 {
     static_assert(BLOCK % G == 0 && 32 % G == 0, "group size");
     constexpr int OWN = (E_COUNT + G - 1) / G;
@@ -2213,6 +2290,11 @@ AVBD_DEV void primal_batch(const DevBodies &B, const DevForces &F, const Params 
         const unsigned gmask = (G == 32) ? 0xFFFFFFFFu : (((1u << G) - 1u) << ((threadIdx.x & 31) / G * G));
         const int4 ent = entries[g];
         const int b = ent.x, r0 = ent.y, r1 = ent.z;
+        for (int j = lane; j < 4; j += G) // stage the solve's poses while the rows are gathered
+            sh.start[j][g] = j == 0   ? ld_state<COH>(B.pos + b)
+                             : j == 1 ? ld_state<COH>(B.quat + b)
+                             : j == 2 ? B.initLin[b]
+                                      : B.initAng[b];
 
         float acc[OWN];
         {
@@ -2234,7 +2316,12 @@ AVBD_DEV void primal_batch(const DevBodies &B, const DevForces &F, const Params 
         {
             int r = base + lane;
             if (r < r1)
-                sh.kind[g][lane] = listed_row_term<COH, ROUND>(B, F, F.rows[r], b, fusedDual, P, sh.term[g][lane]);
+            {
+                const int2 row = F.rows[r];
+                if (flow.done)
+                    wait_partner(flow, row);
+                sh.kind[g][lane] = listed_row_term<COH, ROUND>(B, F, row, b, fusedDual, P, sh.term[g][lane]);
+            }
             __syncwarp(gmask);
             int nrows = min(G, r1 - base);
             for (int rr = 0; rr < nrows; ++rr)
@@ -2277,19 +2364,7 @@ AVBD_DEV void primal_batch(const DevBodies &B, const DevForces &F, const Params 
     const int lt = threadIdx.x % SUB;
     const int t = (threadIdx.x / SUB) * (SUB / G) + lt; // the unit's body this thread factorises
     if (lt < SUB / G && t < count)
-    {
-        const int b = sh.body[t];
-        const float4 p0 = ld_state<COH>(B.pos + b), q0 = ld_state<COH>(B.quat + b); // in flight during the solve
-        const float4 i0 = B.initLin[b], a0 = B.initAng[b];
-        float3 dxl, dxa;
-        ldl_solve27(sh.sys[t], dxl, dxa);
-        float3 p = add(xyz(p0), dxl);
-        float4 q = qstep(q0, dxa);
-        B.pos[b] = f4(p, 0.0f);
-        B.quat[b] = q;
-        B.dqLin[b] = f4(sub(p, xyz(i0)), 0.0f);
-        B.dqAng[b] = f4(qdiff(q, a0), 0.0f);
-    }
+        solve_and_move<COH, BLOCK / G>(B, sh.body[t], sh.sys[t], sh.start, t, flow);
 }
 
 // One launch per colour: block k takes the colour's bodies [k GPB, (k+1) GPB).
@@ -2408,38 +2483,31 @@ constexpr unsigned ITER_SPIN_LIMIT = 1u << 22;
 
 struct IterSync
 {
-    unsigned arrive;
-    unsigned generation;
+    unsigned arrive; // barrier arrivals so far in this launch
     int error;
-    int pad;
+    int pad[2];
 };
 
-AVBD_DEV bool iter_barrier(IterSync *s)
+// Arrivals count up through the launch (the counter starts at zero): barrier k of the
+// launch releases every block once k x gridDim.x blocks have arrived, so the last block's
+// arrival alone opens it.
+AVBD_DEV bool iter_barrier(IterSync *s, unsigned &target)
 {
     __shared__ int ok;
     __syncthreads();
+    target += gridDim.x;
     if (threadIdx.x == 0)
     {
-        volatile unsigned *gen = &s->generation;
-        unsigned g = *gen;
         __threadfence();
-        if (atomicAdd(&s->arrive, 1u) == gridDim.x - 1)
-        {
-            s->arrive = 0;
-            __threadfence();
-            atomicAdd(&s->generation, 1u);
-            ok = 1;
-        }
-        else
-        {
-            unsigned spins = 0;
-            while (*gen == g && ++spins < ITER_SPIN_LIMIT)
-                if (spins > 256)
-                    __nanosleep(32);
-            ok = spins < ITER_SPIN_LIMIT;
-            if (!ok)
-                atomicExch(&s->error, 1);
-        }
+        atomicAdd(&s->arrive, 1u);
+        volatile unsigned *arrive = &s->arrive;
+        unsigned spins = 0;
+        while (*arrive < target && ++spins < ITER_SPIN_LIMIT)
+            if (spins > 256)
+                __nanosleep(32);
+        ok = spins < ITER_SPIN_LIMIT;
+        if (!ok)
+            atomicExch(&s->error, 1);
         __threadfence();
     }
     __syncthreads();
@@ -2458,35 +2526,51 @@ AVBD_DEV bool iter_barrier(IterSync *s)
 template <int G, int BLOCK, int SUB, bool ROUND = false>
 __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces F, Params P, const int4 *entries,
                                                          const int *colourStart, int nColours, int iterations,
-                                                         IterSync *sync)
+                                                         IterSync *sync, int *done)
 {
     extern __shared__ __align__(16) unsigned char smemRaw[];
     PrimalShared<G, BLOCK> &sh = *reinterpret_cast<PrimalShared<G, BLOCK> *>(smemRaw);
     constexpr int GPB = BLOCK / G;
     const long long stride = (long long)gridDim.x * BLOCK;
     const long long tid = (long long)blockIdx.x * BLOCK + threadIdx.x;
+    unsigned target = 0;
+    // without joints, rows wait for their partners instead of every colour for the grid
+    const bool barriers = F.nJoint > 0 || done == nullptr;
+    IterFlow flow;
+    flow.done = barriers ? nullptr : done;
+    flow.error = &sync->error;
     for (int it = 0; it < iterations; ++it)
     {
+        flow.it = it;
         for (int c = 0; c < nColours; ++c)
         {
+            // the colour's bodies in equal contiguous batches over every block, as few
+            // rounds of at most GPB bodies per block as the colour needs
             const int first = colourStart[c], cnt = colourStart[c + 1] - first;
-            for (int base = blockIdx.x * GPB; base < cnt; base += gridDim.x * GPB)
+            const int rounds = (cnt + gridDim.x * GPB - 1) / (gridDim.x * GPB);
+            const int per = rounds > 0 ? (cnt + gridDim.x * rounds - 1) / (gridDim.x * rounds) : 0;
+            for (int r = 0; r < rounds; ++r)
             {
-                primal_batch<G, BLOCK, SUB, true, ROUND>(B, F, P, entries + first + base, min(GPB, cnt - base),
-                                                         it > 0, sh);
+                const int base = (r * gridDim.x + blockIdx.x) * per;
+                if (base >= cnt)
+                    break;
+                primal_batch<G, BLOCK, SUB, true, ROUND>(B, F, P, entries + first + base, min(per, cnt - base),
+                                                         it > 0, sh, flow);
                 unit_sync<SUB, BLOCK>(); // the unit's solve threads are done with the shared systems
             }
-            if (!iter_barrier(sync))
+            if (barriers && !iter_barrier(sync, target))
                 return;
         }
         if (F.nJoint > 0)
         {
             for (long long j = tid; j < F.nJoint; j += stride)
                 dual_joint<true>(B, F, (int)j, P);
-            if (!iter_barrier(sync))
+            if (!iter_barrier(sync, target))
                 return;
         }
     }
+    if (!barriers && !iter_barrier(sync, target)) // every body has finished every iteration
+        return;
     // Contacts between two static bodies have no owning row: nothing moves them, so their
     // update of every iteration runs here, one after the other on the same poses.
     if (iterations > 0)

@@ -32,7 +32,36 @@ AVBD_DEV float3 add(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + 
 AVBD_DEV float3 sub(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
 AVBD_DEV float3 neg(float3 a) { return f3(-a.x, -a.y, -a.z); }
 AVBD_DEV float3 mul(float3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
-AVBD_DEV float3 divs(float3 a, float s) { return f3(a.x / s, a.y / s, a.z / s); }
+// A value the compiler cannot see through (an empty asm that may rewrite it).
+AVBD_DEV float opaque(float x)
+{
+    asm("" : "+f"(x));
+    return x;
+}
+
+// a / s, IEEE round-to-nearest. A zero dividend over a non-zero, non-NaN divisor gives
+// the signed zero directly (sign of a xor sign of s, as IEEE 754 defines the quotient).
+// Measured on B200: a division whose dividend is zero takes about four times as long as
+// one of two normal numbers, in every lane of the warp, and the solver divides many
+// exact zeros (the off-diagonals of the mass matrices, quaternion components of unrotated
+// bodies, zero couplings of the 6x6 systems). Those lanes divide 1 instead; the dividend
+// goes through `opaque`, or the compiler, seeing the quotient unused for a zero dividend,
+// would divide the zero after all.
+AVBD_DEV float fdiv(float a, float s)
+{
+    const bool zero = a == 0.0f && s != 0.0f && s == s;
+    const float q = opaque(zero ? 1.0f : a) / s;
+    return zero ? __int_as_float((__float_as_int(a) ^ __float_as_int(s)) & (int)0x80000000) : q;
+}
+// 0 / s: the zero with the sign of s for a non-zero, non-NaN s, without dividing (s is
+// the same in every lane where this is used, so the branch does not diverge).
+AVBD_DEV float zero_over(float s)
+{
+    if (s != 0.0f && s == s)
+        return __int_as_float(__float_as_int(s) & (int)0x80000000);
+    return opaque(0.0f) / s;
+}
+AVBD_DEV float3 divs(float3 a, float s) { return f3(fdiv(a.x, s), fdiv(a.y, s), fdiv(a.z, s)); }
 AVBD_DEV float dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 AVBD_DEV float lensq(float3 a) { return dot(a, a); }
 AVBD_DEV float len(float3 a) { return sqrtf(lensq(a)); }
@@ -81,7 +110,7 @@ AVBD_DEV float4 qmul(float4 a, float4 b)
 }
 AVBD_DEV float4 qadd(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
 AVBD_DEV float4 qscale(float4 a, float s) { return make_float4(a.x * s, a.y * s, a.z * s, a.w * s); }
-AVBD_DEV float4 qdivs(float4 a, float s) { return make_float4(a.x / s, a.y / s, a.z / s, a.w / s); }
+AVBD_DEV float4 qdivs(float4 a, float s) { return make_float4(fdiv(a.x, s), fdiv(a.y, s), fdiv(a.z, s), fdiv(a.w, s)); }
 AVBD_DEV float qlensq(float4 q) { return lensq(xyz(q)) + q.w * q.w; }
 AVBD_DEV float4 qnormalize(float4 q) { return qdivs(q, sqrtf(qlensq(q))); }
 AVBD_DEV float4 qconj(float4 q) { return make_float4(-q.x, -q.y, -q.z, q.w); }
@@ -166,7 +195,7 @@ AVBD_DEV void ldl_solve27(const float *s, float3 &xl, float3 &xa)
 #pragma unroll
             for (int k = 0; k < j; ++k)
                 v = v - L[j][k] * L[i][k] * D[k];
-            L[i][j] = v / D[j];
+            L[i][j] = fdiv(v, D[j]);
         }
     }
     float b[6] = {-s[E_RL0], -s[E_RL1], -s[E_RL2], -s[E_RA0], -s[E_RA1], -s[E_RA2]};
@@ -182,7 +211,7 @@ AVBD_DEV void ldl_solve27(const float *s, float3 &xl, float3 &xa)
     }
 #pragma unroll
     for (int i = 0; i < 6; ++i)
-        z[i] = y[i] / D[i];
+        z[i] = fdiv(y[i], D[i]);
 #pragma unroll
     for (int i = 5; i >= 0; --i)
     {

@@ -86,6 +86,7 @@ struct AvbdContext
     int n = 0;
     DArr<float4> pos, quat, initLin, initAng, inertLin, inertAng, vel, angvel, prevVel, massMoment, sizeRad;
     DArr<float4> dqLin, dqAng; // pose - initial pose (linear, qdiff), refreshed wherever the pose is written
+    DArr<float4> initAngInv, inertAngInv; // inverses of the step's initial and inertial orientations
     DArr<float> friction;
 
     // worlds: static per-world classification, per-step grids (one grid per world)
@@ -343,6 +344,8 @@ DevBodies dev_bodies(AvbdContext *ctx)
     B.initAng = ctx->initAng.p;
     B.dqLin = ctx->dqLin.p;
     B.dqAng = ctx->dqAng.p;
+    B.initAngInv = ctx->initAngInv.p;
+    B.inertAngInv = ctx->inertAngInv.p;
     B.inertLin = ctx->inertLin.p;
     B.inertAng = ctx->inertAng.p;
     B.vel = ctx->vel.p;
@@ -1282,7 +1285,8 @@ int upload_bodies(AvbdContext *ctx, const AvbdBodies *b, bool props)
                 CHECK(upload(ctx, ctx->shape, tmp.data(), n));
             }
         }
-        for (DArr<float4> *a : {&ctx->initLin, &ctx->initAng, &ctx->inertLin, &ctx->inertAng, &ctx->dqLin, &ctx->dqAng})
+        for (DArr<float4> *a : {&ctx->initLin, &ctx->initAng, &ctx->inertLin, &ctx->inertAng, &ctx->dqLin, &ctx->dqAng,
+                                &ctx->initAngInv, &ctx->inertAngInv})
         {
             CHECK(reserve(ctx, *a, std::max(n, 1), false));
             CU(cudaMemsetAsync(a->p, 0, sizeof(float4) * std::max(n, 1), ctx->stream));
@@ -1485,7 +1489,7 @@ void avbd_destroy(AvbdContext *ctx)
         cudaStreamSynchronize(ctx->stream);
     adjoint_release(ctx);
     for (DArr<float4> *a : {&ctx->pos, &ctx->quat, &ctx->initLin, &ctx->initAng, &ctx->inertLin, &ctx->inertAng,
-                            &ctx->dqLin, &ctx->dqAng,
+                            &ctx->dqLin, &ctx->dqAng, &ctx->initAngInv, &ctx->inertAngInv,
                             &ctx->vel, &ctx->angvel, &ctx->prevVel, &ctx->massMoment, &ctx->sizeRad, &ctx->largeLo,
                             &ctx->largeHi, &ctx->largeSphere, &ctx->spring, &ctx->joint[0], &ctx->joint[1]})
         release(*a);

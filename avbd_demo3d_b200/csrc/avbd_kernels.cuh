@@ -43,6 +43,9 @@ struct DevBodies
     float4 *pos, *quat, *initLin, *initAng, *inertLin, *inertAng, *vel, *angvel, *prevVel;
     // pose - initial pose: (pos - initLin, qdiff(quat, initAng)), written with the pose
     float4 *dqLin, *dqAng;
+    // inverse(initAng) and inverse(inertAng), formed once per step by the warm start: every
+    // qdiff against them in the iterations multiplies by the same inverse
+    float4 *initAngInv, *inertAngInv;
     float4 *massMoment, *sizeRad;
     float *friction;
     float4 *shape; // (type, radius, half length, 0) per body; null when every body is a box
@@ -1567,6 +1570,8 @@ __global__ void k_warm_start(DevBodies B, const int *adjStart, Params P)
     B.quat[b] = q;
     B.inertLin[b] = f4(inertLin, 0.0f);
     B.inertAng[b] = inertAng;
+    B.initAngInv[b] = qinverse(q0);
+    B.inertAngInv[b] = qinverse(inertAng);
     B.dqLin[b] = f4(sub(pos, pos0), 0.0f);
     B.dqAng[b] = f4(qdiff(q, q0), 0.0f);
 }
@@ -2167,7 +2172,7 @@ AVBD_DEV void initial_system(const DevBodies &B, int b, float dt, float *t)
     M3 lhsAng = rows(f3(fdiv(mm4.y, dt2), z, z), f3(z, fdiv(mm4.z, dt2), z), f3(z, z, fdiv(mm4.w, dt2)));
     M3 lhsCross = diag(0, 0, 0);
     float3 rhsLin = mv(lhsLin, sub(xyz(ld_state<COH>(B.pos + b)), xyz(B.inertLin[b])));
-    float3 rhsAng = mv(lhsAng, qdiff(ld_state<COH>(B.quat + b), B.inertAng[b]));
+    float3 rhsAng = mv(lhsAng, qdiff_inv(ld_state<COH>(B.quat + b), B.inertAngInv[b]));
     store_terms(t, lhsLin, lhsAng, lhsCross, rhsLin, rhsAng);
 }
 
@@ -2257,22 +2262,22 @@ AVBD_DEV void wait_partner(const IterFlow &flow, int2 row)
     }
 }
 
-// `start`: the body's position, orientation, step-start position and step-start
-// orientation, staged in shared memory by the gathering lanes, so that no register holds
-// them across the factorisation.
+// `start`: the body's position, orientation, step-start position and the inverse of the
+// step-start orientation, staged in shared memory by the gathering lanes, so that no
+// register holds them across the factorisation.
 template <bool COH, int GPB>
 AVBD_DEV void solve_and_move(const DevBodies &B, int b, const float *sys, const float4 (*start)[GPB], int t,
                              const IterFlow &flow)
 {
     float3 dxl, dxa;
     ldl_solve27(sys, dxl, dxa);
-    const float4 p0 = start[0][t], q0 = start[1][t], i0 = start[2][t], a0 = start[3][t];
+    const float4 p0 = start[0][t], q0 = start[1][t], i0 = start[2][t], a0inv = start[3][t];
     float3 p = add(xyz(p0), dxl);
     float4 q = qstep(q0, dxa);
     B.pos[b] = f4(p, 0.0f);
     B.quat[b] = q;
     B.dqLin[b] = f4(sub(p, xyz(i0)), 0.0f);
-    B.dqAng[b] = f4(qdiff(q, a0), 0.0f);
+    B.dqAng[b] = f4(qdiff_inv(q, a0inv), 0.0f);
     if (flow.done) // a release: the body's pose, and the contact updates its rows made before
         st_release(flow.done + b, flow.it + 1); // the block's barrier, are visible before the count
 }
@@ -2294,7 +2299,7 @@ AVBD_DEV void primal_batch(const DevBodies &B, const DevForces &F, const Params 
             sh.start[j][g] = j == 0   ? ld_state<COH>(B.pos + b)
                              : j == 1 ? ld_state<COH>(B.quat + b)
                              : j == 2 ? B.initLin[b]
-                                      : B.initAng[b];
+                                      : B.initAngInv[b];
 
         float acc[OWN];
         {

@@ -117,6 +117,8 @@ AVBD_DEV float4 qconj(float4 q) { return make_float4(-q.x, -q.y, -q.z, q.w); }
 AVBD_DEV float4 qinverse(float4 q) { return qdivs(qconj(q), qlensq(q)); }
 // a - b for orientations: 2 vec(a b^-1)
 AVBD_DEV float3 qdiff(float4 a, float4 b) { return mul(xyz(qmul(a, qinverse(b))), 2.0f); }
+// qdiff(a, b) given binv = qinverse(b)
+AVBD_DEV float3 qdiff_inv(float4 a, float4 binv) { return mul(xyz(qmul(a, binv)), 2.0f); }
 // a + w for an orientation and a rotation vector: normalize(a + (w,0) a / 2)
 AVBD_DEV float4 qstep(float4 a, float3 w)
 {
@@ -153,9 +155,8 @@ enum Entry27
 // Unpivoted LDL^T solve of [[aLin, aCross^T],[aCross, aAng]] x = b with the entry
 // order and per-entry operation order of maths.h:481-547. `s` holds the 27 entries;
 // the right-hand side is negated here (solve(..., -rhsLin, -rhsAng, ...), solver.cpp:1233).
-AVBD_DEV void ldl_solve27(const float *s, float3 &xl, float3 &xa)
+AVBD_DEV void load_sys27(const float *s, float (&A)[6][6])
 {
-    float A[6][6];
     A[0][0] = s[E_LL00];
     A[1][0] = s[E_LL10];
     A[1][1] = s[E_LL11];
@@ -173,6 +174,12 @@ AVBD_DEV void ldl_solve27(const float *s, float3 &xl, float3 &xa)
     A[5][3] = s[E_LA20];
     A[5][4] = s[E_LA21];
     A[5][5] = s[E_LA22];
+}
+
+AVBD_DEV void ldl_solve27(const float *s, float3 &xl, float3 &xa)
+{
+    float A[6][6];
+    load_sys27(s, A);
     float L[6][6];
     float D[6];
 #pragma unroll

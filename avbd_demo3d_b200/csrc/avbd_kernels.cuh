@@ -2107,14 +2107,13 @@ AVBD_DEV unsigned contact_term_self(const DevBodies &B, const DevForces &F, unsi
     ContactRec c = load_contact<COH>(cp);
     const int ia = isA ? self : partner, ib = isA ? partner : self;
     Motion A = load_motion<COH>(B, ia), Bm = load_motion<COH>(B, ib);
-    // ROUND: the world has round bodies, whose manifolds are flagged in basis row 1
-    ContactEval e = ROUND && b1.w != 0.0f
-                        ? eval_contact_arms(A, Bm, basis, b0.w, c, P.alpha,
-                                            contact_offset(body_shape(B, ia), A.q, c.rA, basis, true, c.key),
-                                            contact_offset(body_shape(B, ib), Bm.q, c.rB, basis, false, c.key))
-                        : eval_contact(A, Bm, basis, b0.w, c, P.alpha);
-    const M3 jLin = isA ? e.jALin : e.jBLin; // this body's rows, taken before the dual update
-    const M3 jAng = isA ? e.jAAng : e.jBAng;
+    // the contact's world arms (ROUND: the world has round bodies, whose manifolds are
+    // flagged in basis row 1)
+    const bool round = ROUND && b1.w != 0.0f;
+    const float3 rAW = round ? contact_offset(body_shape(B, ia), A.q, c.rA, basis, true, c.key) : rotate(A.q, c.rA);
+    const float3 rBW = round ? contact_offset(body_shape(B, ib), Bm.q, c.rB, basis, false, c.key) : rotate(Bm.q, c.rB);
+    const float3 rW = isA ? rAW : rBW;
+    ContactEval e = eval_contact_arms(A, Bm, basis, b0.w, c, P.alpha, rAW, rBW);
     if (dual)
     {
         // the previous iteration's dual update of this contact, at the same poses, then
@@ -2123,6 +2122,10 @@ AVBD_DEV unsigned contact_term_self(const DevBodies &B, const DevForces &F, unsi
         store_contact_state(cp, c);
         contact_force(e, c, b0.w);
     }
+    // this body's Jacobian rows, formed again from the basis and its arm as
+    // eval_contact_arms forms them (fewer values live across the dual update)
+    const M3 jLin = isA ? basis : mneg(basis);
+    const M3 jAng = rows(cross(rW, jLin.r0), cross(rW, jLin.r1), cross(rW, jLin.r2));
     M3 jLinT = trans(jLin), jAngT = trans(jAng);
     M3 jAngTk = times_diag(jAngT, c.pen);
     store_terms(t, mm(times_diag(jLinT, c.pen), jLin), mm(jAngTk, jAng), mm(jAngTk, jLin), mv(jLinT, e.F),

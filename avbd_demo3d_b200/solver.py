@@ -266,13 +266,25 @@ class World:
         self._check(self.lib.avbd_synchronize(self.h), "avbd_synchronize")
 
     # -- readback
-    def bodies(self, aux: bool = False) -> dict:
+    _BODY_WIDTH = {"pos": 3, "quat": 4, "vel": 3, "angvel": 3, "prevvel": 3, "init_lin": 3, "init_ang": 4,
+                   "inert_lin": 3, "inert_ang": 4}
+
+    def bodies(self, aux: bool = False, out: dict | None = None) -> dict:
+        """Body state in list order. `out`: caller-owned arrays to fill in place (float32,
+        C-contiguous, (n, width)); a simulation loop that reads every step reuses them."""
         n = self.n
-        out = {"pos": np.zeros((n, 3), F32), "quat": np.zeros((n, 4), F32), "vel": np.zeros((n, 3), F32),
-               "angvel": np.zeros((n, 3), F32), "prevvel": np.zeros((n, 3), F32)}
-        if aux:
-            out.update(init_lin=np.zeros((n, 3), F32), init_ang=np.zeros((n, 4), F32),
-                       inert_lin=np.zeros((n, 3), F32), inert_ang=np.zeros((n, 4), F32))
+        if out is not None:
+            for k, v in out.items():
+                if k not in self._BODY_WIDTH or not isinstance(v, np.ndarray) or v.dtype != F32 or \
+                        v.shape != (n, self._BODY_WIDTH[k]) or not v.flags.c_contiguous:
+                    raise ValueError(f"bodies(out=...): {k} must be a C-contiguous float32 array of shape "
+                                     f"({n}, {self._BODY_WIDTH.get(k)})")
+        else:
+            out = {"pos": np.zeros((n, 3), F32), "quat": np.zeros((n, 4), F32), "vel": np.zeros((n, 3), F32),
+                   "angvel": np.zeros((n, 3), F32), "prevvel": np.zeros((n, 3), F32)}
+            if aux:
+                out.update(init_lin=np.zeros((n, 3), F32), init_ang=np.zeros((n, 4), F32),
+                           inert_lin=np.zeros((n, 3), F32), inert_ang=np.zeros((n, 4), F32))
         st = _lib.AvbdBodyState(*[_ptr(out.get(k)) for k in (
             "pos", "quat", "vel", "angvel", "prevvel", "init_lin", "init_ang", "inert_lin", "inert_ang")])
         self._check(self.lib.avbd_read_bodies(self.h, ctypes.byref(st)), "avbd_read_bodies")

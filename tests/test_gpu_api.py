@@ -107,6 +107,28 @@ def test_write_bodies_between_steps(gpu):
     assert np.array_equal(bits(g.bodies()["pos"]), bits(o.bodies()["pos"]))
 
 
+def test_bodies_into_caller_arrays(gpu):
+    """bodies(out=...) fills the caller's arrays in place with what bodies() returns, and
+    refuses arrays of the wrong shape, type or layout."""
+    sc = scenes.stack_grid(3, 3, 4, seed=6)
+    g = World(sc)
+    g.step(4)
+    ref = g.bodies(aux=True)
+    out = {k: np.full_like(v, np.nan) for k, v in ref.items()}
+    same = g.bodies(out=out)
+    assert same is out
+    for k in ref:
+        assert np.array_equal(bits(out[k]), bits(ref[k])), k
+    part = {"quat": np.zeros((g.n, 4), np.float32)}
+    g.bodies(out=part)
+    assert np.array_equal(bits(part["quat"]), bits(ref["quat"]))
+    for bad in ({"pos": np.zeros((g.n, 4), np.float32)}, {"pos": np.zeros((g.n, 3), np.float64)},
+                {"pos": np.zeros((3, g.n), np.float32).T}, {"spin": np.zeros((g.n, 3), np.float32)}):
+        with pytest.raises(ValueError):
+            g.bodies(out=bad)
+    g.close()
+
+
 def test_reference_style_interface(gpu):
     """Scenes built with the mirrored constructors step on the GPU like the oracle."""
     solver = Solver()

@@ -49,3 +49,25 @@ def test_mixed_drop_constraints_and_spacing():
         clash = clash[clash != i]
         # only links of the same chain (12 boxes each, the first 240 bodies) may overlap
         assert all(i < 240 and j < 240 and i // 12 == j // 12 for j in clash), (i, clash)
+
+
+def test_round_scenes_and_mass_properties():
+    """round_mix / sphere_pour carry every shape code, and the mass, moment and bounding
+    radius the device world is loaded with (solver.round_properties, float32 formulas of
+    rigid.cpp:44-90) equal the C oracle's bit for bit."""
+    import checkers
+    from avbd_demo3d_b200.solver import box_properties, round_properties
+
+    for sc in (scenes.round_mix(240, seed=11, cols=6), scenes.sphere_pour(240)):
+        shape = np.asarray(sc.shape)
+        assert sc.dims.shape == (sc.n_bodies, 2) and shape.shape == (sc.n_bodies,)
+        assert set(np.unique(shape)) <= {scenes.SHAPE_BOX, scenes.SHAPE_SPHERE, scenes.SHAPE_CAPSULE,
+                                         scenes.SHAPE_CYLINDER}
+        mass, moment, radius = box_properties(sc.size, sc.density)
+        round_properties(sc.shape, sc.dims, sc.density, mass, moment, radius)
+        o = checkers.World(sc, "oracle")
+        pr = o.body_props()  # list order: creation order reversed
+        for mine, theirs in ((mass, pr["mass"]), (moment, pr["moment"]), (radius, pr["radius"])):
+            assert np.array_equal(np.asarray(mine, np.float32)[::-1].view(np.uint32),
+                                  np.asarray(theirs, np.float32).view(np.uint32))
+    assert {1, 2, 3} <= set(np.unique(scenes.round_mix(240, seed=11, cols=6).shape))

@@ -25,8 +25,8 @@ constexpr unsigned BARRIER_SPIN_LIMIT = 1u << 24;
 
 struct ColourControl
 {
-    unsigned arrive;
-    unsigned generation;
+    unsigned arrive; // barrier arrivals so far in this launch
+    unsigned unused; // keeps the layout that readers of the block index by word
     int error;
     int vertices;
     int rounds;
@@ -34,31 +34,26 @@ struct ColourControl
     int coloured[MAX_COLOUR_ROUNDS];
 };
 
-AVBD_DEV bool grid_barrier(ColourControl *ctl)
+// Arrivals count up through the launch (the control block starts zeroed): barrier k
+// releases every block once k x gridDim.x blocks have arrived, so the last block's arrival
+// alone opens it. `target` is the calling block's count of barriers passed x gridDim.x.
+AVBD_DEV bool grid_barrier(ColourControl *ctl, unsigned &target)
 {
     __syncthreads();
     __shared__ int ok;
+    target += gridDim.x;
     if (threadIdx.x == 0)
     {
-        volatile unsigned *gen = &ctl->generation;
-        unsigned g = *gen;
         __threadfence();
-        if (atomicAdd(&ctl->arrive, 1u) == gridDim.x - 1)
-        {
-            ctl->arrive = 0;
-            __threadfence();
-            atomicAdd(&ctl->generation, 1u);
-            ok = 1;
-        }
-        else
-        {
-            unsigned spins = 0;
-            while (*gen == g && ++spins < BARRIER_SPIN_LIMIT)
+        atomicAdd(&ctl->arrive, 1u);
+        volatile unsigned *arrive = &ctl->arrive;
+        unsigned spins = 0;
+        while (*arrive < target && ++spins < BARRIER_SPIN_LIMIT)
+            if (spins > 256)
                 __nanosleep(64);
-            ok = spins < BARRIER_SPIN_LIMIT;
-            if (!ok)
-                atomicExch(&ctl->error, 1);
-        }
+        ok = spins < BARRIER_SPIN_LIMIT;
+        if (!ok)
+            atomicExch(&ctl->error, 1);
         __threadfence();
     }
     __syncthreads();

@@ -1615,7 +1615,8 @@ __global__ void k_colour_all(DevBodies B, DevForces F, int n, int mode, int *sta
     int bs = block_sum(mine);
     if (threadIdx.x == 0 && bs)
         atomicAdd(&ctl->vertices, bs);
-    if (!grid_barrier(ctl))
+    unsigned target = 0;
+    if (!grid_barrier(ctl, target))
         return;
     const int total = ((volatile int *)&ctl->vertices)[0];
     int done = 0, round = 0;
@@ -1674,7 +1675,7 @@ __global__ void k_colour_all(DevBodies B, DevForces F, int n, int mode, int *sta
         bs = block_sum(mine);
         if (threadIdx.x == 0 && bs)
             atomicAdd(&ctl->coloured[round], bs);
-        if (!grid_barrier(ctl))
+        if (!grid_barrier(ctl, target))
             return;
         done += ((volatile int *)ctl->coloured)[round];
     }

@@ -52,7 +52,8 @@ __global__ void k_colour_csr_noalloc(int n, const int *vertex, const int *adjSta
     int bs = block_sum(mine);
     if (threadIdx.x == 0 && bs)
         atomicAdd(&ctl->vertices, bs);
-    if (!grid_barrier(ctl))
+    unsigned target = 0;
+    if (!grid_barrier(ctl, target))
         return;
     const int total = ((volatile int *)&ctl->vertices)[0];
     int done = 0, round = 0;
@@ -107,7 +108,7 @@ __global__ void k_colour_csr_noalloc(int n, const int *vertex, const int *adjSta
         bs = block_sum(mine);
         if (threadIdx.x == 0 && bs)
             atomicAdd(&ctl->coloured[round], bs);
-        if (!grid_barrier(ctl))
+        if (!grid_barrier(ctl, target))
             return;
         done += ((volatile int *)ctl->coloured)[round];
     }
@@ -175,7 +176,7 @@ extern "C" int avbd_colour_graph_noalloc(int32_t n, const int32_t *vertex, const
     void *args[] = {&n, (void *)&vertex, (void *)&adj_start, (void *)&adj_other, &mode, &scratch, (void *)&colour};
     if (cudaLaunchCooperativeKernel((void *)k_colour_csr_noalloc, blocks, 256, args, 0, stream) != cudaSuccess)
         return AVBD_ERR_CUDA;
-    int summary[6] = {0}; // arrive, generation, error, vertices, rounds, maxColour
+    int summary[6] = {0}; // arrive, unused, error, vertices, rounds, maxColour
     if (cudaMemcpyAsync(summary, scratch, sizeof(summary), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
         cudaStreamSynchronize(stream) != cudaSuccess)
         return AVBD_ERR_CUDA;

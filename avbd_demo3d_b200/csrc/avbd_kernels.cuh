@@ -2524,14 +2524,17 @@ AVBD_DEV bool iter_barrier(IterSync *s, unsigned &target)
 }
 
 // Solver::iteratePrimalDualCpu (solver.cpp:1177-1271) for every iteration of a step, one
-// block per SM, all state read at L2 between barriers. Per iteration: each colour's bodies
-// in batches of GPB (a barrier after each colour), then the joints' dual update. The
-// contacts' dual update of iteration k is done in iteration k + 1 by the row of the body
-// that owns the contact, before that row uses it: the owner is the contact's body with the
-// lower colour (or its only dynamic body), which has not moved yet in iteration k + 1, and
-// neither has the other body, so both poses are those the dual sweep of iteration k reads
-// and every contact's update is the same. The last iteration's contact updates close the
-// launch.
+// block per SM, mutable state read at L2. Per iteration: each colour's bodies in batches of
+// at most GPB per block, spread evenly over the blocks; the block works in independent
+// units of SUB threads. With joints, a grid barrier follows each colour and the joints'
+// dual update each iteration; without, each row waits for its partner's iteration count
+// instead (wait_partner), so blocks and units run ahead of one another. The contacts' dual
+// update of iteration k is done in iteration k + 1 by the row of the body that owns the
+// contact, before that row uses it: the owner is the contact's body with the lower colour
+// (or its only dynamic body), which has not moved yet in iteration k + 1, and neither has
+// the other body, so both poses are those the dual sweep of iteration k reads and every
+// contact's update is the same. After one closing grid barrier, the last iteration's
+// contact updates end the launch.
 template <int G, int BLOCK, int SUB, bool ROUND = false>
 __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces F, Params P, const int4 *entries,
                                                          const int *colourStart, int nColours, int iterations,

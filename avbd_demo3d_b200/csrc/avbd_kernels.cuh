@@ -2187,7 +2187,7 @@ struct PrimalShared
     static constexpr int GPB = BLOCK / G;
     float term[GPB][G][E_COUNT];
     float sys[GPB][E_COUNT]; // odd stride: one system per thread without bank conflicts
-    float4 start[4][GPB];    // the body's pose (position, orientation) and step-start pose
+    float4 start[4][GPB];    // position, orientation, step-start position, inverse step-start orientation
     unsigned kind[GPB][G];
     int body[GPB];
 };
@@ -2204,16 +2204,6 @@ AVBD_DEV void unit_sync()
         asm volatile("bar.sync %0, %1;" ::"r"(1 + (int)threadIdx.x / SUB), "n"(SUB) : "memory");
 }
 
-// One primal solve per body of a batch of one colour (solver.cpp:1186-1233). Rows: G lanes
-// per body. The solve entries carry the body and its row range; every lane of a group
-// builds the initial system M/dt^2 and keeps the entries it owns, then the rows are
-// evaluated G at a time (lane j evaluates row base + j into shared memory) and every lane
-// adds its entries row by row, so each sum keeps the reference's order. Solve: the batch's
-// accumulated systems go to shared memory and one thread per body factors its 6x6 system
-// and moves the body, so the factorisation runs with every lane of its warp busy. The
-// block works in independent units of SUB threads (SUB / G bodies, which the unit's first
-// SUB / G threads factorise); every thread of the block calls this (it holds the units'
-// barriers).
 // Per-body progress of the iteration kernel when it runs without per-colour grid barriers:
 // done[b] = the iterations body b has completed in this launch. `done` null: the
 // barriers order the passes and nothing is waited for.
@@ -2286,6 +2276,16 @@ AVBD_DEV void solve_and_move(const DevBodies &B, int b, const float *sys, const 
         st_release(flow.done + b, flow.it + 1); // the block's barrier, are visible before the count
 }
 
+// One primal solve per body of a batch of one colour (solver.cpp:1186-1233). Rows: G lanes
+// per body. The solve entries carry the body and its row range; every lane of a group
+// builds the initial system M/dt^2 and keeps the entries it owns, then the rows are
+// evaluated G at a time (lane j evaluates row base + j into shared memory) and every lane
+// adds its entries row by row, so each sum keeps the reference's order. Solve: the batch's
+// accumulated systems go to shared memory and one thread per body factors its 6x6 system
+// and moves the body, so the factorisation runs with every lane of its warp busy. The
+// block works in independent units of SUB threads (SUB / G bodies, which the unit's first
+// SUB / G threads factorise); every thread of the block calls this (it holds the units'
+// barriers).
 template <int G, int BLOCK, int SUB, bool COH, bool ROUND>
 AVBD_DEV void primal_batch(const DevBodies &B, const DevForces &F, const Params &P, const int4 *entries, int count,
                            bool fusedDual, PrimalShared<G, BLOCK> &sh, const IterFlow &flow = IterFlow{})

@@ -2588,6 +2588,8 @@ __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces 
     if (iterations > 0)
         for (long long t = tid; t < 8ll * F.nMan; t += stride)
         {
+            if ((int)(t & 7) >= F.man.n[t >> 3]) // an empty slot: nothing to load
+                continue;
             int2 ab = F.man.ab[t >> 3];
             bool orphan = B.massMoment[ab.x].x <= 0 && B.massMoment[ab.y].x <= 0;
             for (int r = orphan ? iterations : 1; r > 0; --r)

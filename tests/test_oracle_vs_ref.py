@@ -55,6 +55,12 @@ def test_round_shapes(scene, colour):
     lockstep(sc, 60, colour)
 
 
+def test_sphere_pour_2000_colour_order():
+    """2,000 spheres poured among static cylinders: many simultaneous sphere-sphere and
+    sphere-cylinder contacts with rolling friction, in the GPU's colour order."""
+    lockstep(scenes.sphere_pour(2000), 120, True)  # the pour lands after about 40 steps
+
+
 def test_round_body_properties_match_reference():
     """Mass and shape fields of round bodies as the reference's SimWorld holds them."""
     sc = scenes.round_mix(200, seed=19, cols=5)

@@ -61,6 +61,12 @@ def test_sphere_pour_2000_colour_order():
     lockstep(scenes.sphere_pour(2000), 120, True)  # the pour lands after about 40 steps
 
 
+def test_round_mix_long_horizon():
+    """Spheres, capsules and cylinders settling on static cylinders and a raised slab for
+    200 steps in list order: the trajectory stays bit-identical well past the impacts."""
+    lockstep(scenes.round_mix(400, seed=17, cols=8), 200, False)
+
+
 def test_round_body_properties_match_reference():
     """Mass and shape fields of round bodies as the reference's SimWorld holds them."""
     sc = scenes.round_mix(200, seed=19, cols=5)

@@ -90,10 +90,13 @@ def test_other_broadphase_modes(mode):
 
 
 @pytest.mark.parametrize("mode", [scenes.BROADPHASE_GRID, scenes.BROADPHASE_SAP, scenes.BROADPHASE_ALL_PAIRS])
-def test_broadphase_only_matches_reference(mode):
+@pytest.mark.parametrize("world", ["boxes", "round"])
+def test_broadphase_only_matches_reference(mode, world):
     """Solver::benchmarkBroadphaseOnly after some steps: same new pairs, same counters, and
-    the next steps (which initialise the new manifolds) stay bit-identical."""
-    sc = scenes.mixed_drop(1500, 8, 10, 0.1, extent=(22, 22, 14), seed=29)
+    the next steps (which initialise the new manifolds) stay bit-identical. Round bodies
+    enter the broadphase with bounds from their shape radius."""
+    sc = (scenes.mixed_drop(1500, 8, 10, 0.1, extent=(22, 22, 14), seed=29) if world == "boxes"
+          else scenes.round_mix(500, seed=23, cols=8))
     sc.params.broadphase = mode
     o = checkers.World(sc, "oracle", order_mode=0)
     r = checkers.World(sc, "ref")

@@ -140,10 +140,12 @@ def _drag_script(w, props, steps=60):
         yield steps + s
 
 
-def test_drag_edits_match_reference():
+@pytest.mark.parametrize("world", ["boxes", "round"])
+def test_drag_edits_match_reference(world):
     """Joint edits between steps (drag begin / move / release, a body-body joint added and
-    deleted) keep the oracle bit-identical to the reference."""
-    sc = scenes.mixed_drop(1200, 8, 10, 0.1, extent=(20, 20, 14), seed=31)
+    deleted) keep the oracle bit-identical to the reference, on boxes and on round bodies."""
+    sc = (scenes.mixed_drop(1200, 8, 10, 0.1, extent=(20, 20, 14), seed=31) if world == "boxes"
+          else scenes.round_mix(400, seed=29, cols=8))
     o = checkers.World(sc, "oracle", order_mode=0)
     r = checkers.World(sc, "ref")
     o.step(20)

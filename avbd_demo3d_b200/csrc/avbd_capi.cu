@@ -954,7 +954,7 @@ int colour_bodies(AvbdContext *ctx)
     CU(cudaMemcpyAsync(ctx->hCounters, ctx->counters.p, sizeof(StepCounters), cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
     if (*ctx->hIterError)
-        return fail(ctx, AVBD_ERR_STATE, "iteration kernel barrier wait expired");
+        return fail(ctx, AVBD_ERR_STATE, "iteration kernel wait expired (a grid barrier or a partner body's iteration count)");
     const int *sum = ctx->hColourSummary; // vertices, rounds, maxColour, error
     if (sum[3])
         return fail(ctx, AVBD_ERR_STATE, "colouring did not finish (barrier wait expired or round cap reached)");
@@ -1890,7 +1890,7 @@ int avbd_synchronize(AvbdContext *ctx)
         return AVBD_ERR_ARGUMENT;
     CU(cudaStreamSynchronize(ctx->stream));
     if (*ctx->hIterError)
-        return fail(ctx, AVBD_ERR_STATE, "iteration kernel barrier wait expired");
+        return fail(ctx, AVBD_ERR_STATE, "iteration kernel wait expired (a grid barrier or a partner body's iteration count)");
     return AVBD_OK;
 }
 

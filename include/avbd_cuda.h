@@ -236,7 +236,10 @@ int avbd_write_bodies(AvbdContext *ctx, const AvbdBodies *bodies);
 
 /* Solver::step() for nsteps steps (solver.cpp:934-937 via stepCpuReference 1036-1041).
  * Asynchronous on the context stream; returns after launch except where the step
- * needs a device count (buffer growth). */
+ * needs a device count (buffer growth). Every wait inside a step's kernels is bounded:
+ * if one expires (a grid barrier, or a row waiting for its partner body's iteration
+ * count), the step reports AVBD_ERR_STATE at its next host check and the context
+ * latches the error. */
 int avbd_step(AvbdContext *ctx, int32_t nsteps);
 /* Wait for the context stream. */
 int avbd_synchronize(AvbdContext *ctx);

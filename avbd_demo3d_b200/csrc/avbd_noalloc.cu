@@ -5,9 +5,12 @@
 // must not allocate after start-up, and hosts that pre-reserve every byte of the GPU.
 // avbd_colour_graph_noalloc gives them the same Jones-Plassmann colouring that avbd_step
 // computes for its primal sweep (k_colour_all), with all scratch memory in a fixed-size
-// array that is part of the loaded library image (a file-scope __device__ array), so the
-// call itself allocates nothing. Every GPU that loads the library holds this array
-// (about 4 MiB) until the process exits.
+// file-scope __device__ array of the library, so the call itself allocates nothing. Every
+// GPU that loads the library holds this array (about 4 MiB) until the process exits.
+// Under CUDA 12's default lazy module loading the driver loads this file's module onto a
+// device, and places the array there, at the first call on that device (its
+// cudaGetSymbolAddress); that first call is the one that needs the memory free, which is
+// why callers make it at start-up. Later calls allocate nothing.
 #include "../../include/avbd_cuda.h"
 #include "avbd_colour.cuh"
 

@@ -363,10 +363,16 @@ int avbd_set_colouring(AvbdContext *ctx, int32_t mode);
  * each vertex and -1 elsewhere. Runs on cuda_stream (NULL = default stream) and waits for
  * it before returning.
  *
- * The first call on a device sets that device up (looks up the scratch array's device
- * address and the co-resident block count); make that first call before any stream
- * capture. All calls share the one scratch array: calls that overlap on the GPU (other
- * streams, other threads) race and must be serialised by the caller.
+ * The first call on a device sets that device up: it looks up the scratch array's device
+ * address and the co-resident block count. Under CUDA 12's default lazy module loading
+ * that first call is also when the driver loads this part of the library onto the device
+ * and places the scratch array there, so it needs about 4 MiB free on the GPU and can
+ * fail with AVBD_ERR_CUDA when the GPU is already full. Make the first call at start-up,
+ * before the GPU is filled and before any stream capture begins (or set
+ * CUDA_MODULE_LOADING=EAGER, which places the array when the library's context is
+ * created); after it, calls allocate nothing. All calls share the one scratch array,
+ * which keeps the last call's contents: calls that overlap on the GPU (other streams,
+ * other threads) race and must be serialised by the caller.
  * Returns AVBD_OK, AVBD_ERR_ARGUMENT (bad arguments), AVBD_ERR_CAPACITY (n above the
  * maximum, or more than 256 colours), AVBD_ERR_STATE (colouring did not finish) or
  * AVBD_ERR_CUDA. */

@@ -20,6 +20,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libavbd_ref.so")
+REF64_LIB = os.path.join(HERE, "_ref", "libavbd_ref64.so")
 
 _libs: dict[str, ctypes.CDLL] = {}
 
@@ -56,6 +57,10 @@ def build_oracle() -> str:
 
 def ref_available() -> bool:
     return os.path.exists(REF_LIB)
+
+
+def ref64_available() -> bool:
+    return os.path.exists(REF64_LIB)
 
 
 def _lib(kind: str) -> ctypes.CDLL:
@@ -352,6 +357,81 @@ class World:
         self.lib.adjref_fd(self.h, _ptr(theta), _ptr(target), int(dirs.shape[0]), _ptr(dirs), float(h),
                            int(threads), _ptr(out))
         return out[:dirs.shape[0]].copy()
+
+
+class Fp64Reference:
+    """The reference solver built in double precision (oracle/make_fp64.py), stepped by its
+    stock CPU backend in its own list order from the scene's single-precision inputs
+    (widened exactly). Box worlds with joints, springs and ignore pairs."""
+
+    def __init__(self, scene):
+        if getattr(scene, "shape", None) is not None:
+            raise ValueError("the FP64 reference driver builds box worlds only")
+        if not ref64_available():
+            raise FileNotFoundError(f"{REF64_LIB} not built (make -C oracle ref64)")
+        lib = _libs.get("ref64")
+        if lib is None:
+            lib = ctypes.CDLL(REF64_LIB)
+            vp, ip, fp = ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p
+            lib.ref64_create.restype = vp
+            lib.ref64_create.argtypes = [ctypes.POINTER(_Params), ip] + [fp] * 6 + [ip] + [fp] * 6
+            lib.ref64_destroy.argtypes = [vp]
+            lib.ref64_destroy.restype = None
+            lib.ref64_step.argtypes = [vp, ip]
+            lib.ref64_step.restype = ip
+            lib.ref64_num_bodies.argtypes = [vp]
+            lib.ref64_num_bodies.restype = ip
+            lib.ref64_get_bodies.argtypes = [vp] + [fp] * 4
+            lib.ref64_get_bodies.restype = None
+            lib.ref64_is_double.argtypes = []
+            lib.ref64_is_double.restype = ip
+            if lib.ref64_is_double() != 1:
+                raise RuntimeError("libavbd_ref64.so was not built in double precision")
+            _libs["ref64"] = lib
+        self.lib = lib
+        self._keep = [np.ascontiguousarray(x) for x in (
+            scene.size, scene.density, scene.friction, scene.pos, scene.vel, scene.quat,
+            scene.ftype, scene.fa, scene.fb, scene.frA, scene.frB, scene.fparam)]
+        self.params = make_params(scene.params, 0)
+        self.h = lib.ref64_create(ctypes.byref(self.params), scene.n_bodies, *[_ptr(x) for x in self._keep[:6]],
+                                  scene.n_forces, *[_ptr(x) for x in self._keep[6:]])
+        self.n = scene.n_bodies
+
+    def step(self, n: int = 1):
+        self.lib.ref64_step(self.h, n)
+
+    def bodies(self) -> dict:
+        n = self.n
+        out = {k: np.zeros((n, d), np.float64) for k, d in (("pos", 3), ("quat", 4), ("vel", 3), ("angvel", 3))}
+        self.lib.ref64_get_bodies(self.h, *[_ptr(out[k]) for k in ("pos", "quat", "vel", "angvel")])
+        return out
+
+    def close(self):
+        if self.h:
+            self.lib.ref64_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def pose_error(a: dict, b: dict) -> tuple[float, float]:
+    """Largest position difference (m) and largest rotation angle between orientations
+    (rad) over all bodies of two body-state dicts, evaluated in double precision."""
+    dp = float(np.abs(np.asarray(a["pos"], np.float64) - np.asarray(b["pos"], np.float64)).max()) \
+        if len(a["pos"]) else 0.0
+    qa = np.asarray(a["quat"], np.float64)
+    qb = np.asarray(b["quat"], np.float64)
+    qa = qa / np.linalg.norm(qa, axis=1, keepdims=True)
+    qb = qb / np.linalg.norm(qb, axis=1, keepdims=True)
+    c = np.clip(np.abs(np.sum(qa * qb, axis=1)), 0.0, 1.0)
+    # 2 asin(|qa x qb| ...) is better conditioned than 2 acos(c) for tiny angles
+    s = np.sqrt(np.maximum(0.0, 1.0 - c * c))
+    ang = 2.0 * np.arctan2(s, c)
+    return dp, float(ang.max()) if len(ang) else 0.0
 
 
 def adjoint_selftest() -> float:

@@ -68,6 +68,48 @@ def test_noalloc_colouring_matches_the_step(gpu):
     w.close()
 
 
+def test_noalloc_calls_leave_free_device_memory_unchanged(gpu):
+    """The point of the entry point: once the first call on the device has placed the
+    library's scratch array, further calls take no device memory. Inputs for graphs of
+    three sizes are allocated up front; the device's free-memory count (cudaMemGetInfo)
+    is read after a warm-up call and again after six more calls, which must colour
+    exactly like the warm-up calls."""
+    import torch
+
+    lib = _lib.load()
+    sc = scenes.mixed_drop(3000, 20, 12, 0.05, extent=(30, 30, 20), seed=5)
+    w = World(sc)
+    w.step(12)
+    vertex, start, other = constraint_graph(w)
+    w.close()
+    cases = []
+    for n in (w.n, w.n // 2, 257):
+        # a prefix of the bodies: neighbours at n or above are skipped by the entry point
+        dv = torch.from_numpy(np.ascontiguousarray(vertex[:n])).cuda()
+        ds = torch.from_numpy(np.ascontiguousarray(start[:n + 1])).cuda()
+        do = torch.from_numpy(other).cuda()
+        out = torch.full((n,), -7, dtype=torch.int32, device="cuda")
+        cases.append((n, dv, ds, do, out))
+    nc = ctypes.c_int32(-1)
+
+    def call(case, mode):
+        n, dv, ds, do, out = case
+        rc = lib.avbd_colour_graph_noalloc(n, dv.data_ptr(), ds.data_ptr(), do.data_ptr(), mode, out.data_ptr(),
+                                           ctypes.byref(nc), None)
+        assert rc == _lib.AVBD_OK, (n, rc)
+        return out.cpu().numpy().copy(), nc.value
+
+    first = [call(c, 0) for c in cases]
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    again = [call(c, m) for m in (0, 1) for c in cases]
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before, (free_before, free_after)
+    for (c0, n0), (c1, n1) in zip(first, again[:3]):
+        assert n0 == n1 and np.array_equal(c0, c1)
+
+
 def test_noalloc_rejects_oversize_and_bad_arguments(gpu):
     lib = _lib.load()
     nc = ctypes.c_int32()

@@ -68,7 +68,7 @@ class AvbdStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_int64) for k in (
         "body_count", "pair_checks", "sphere_hits", "constrained_hits", "manifolds_created", "manifold_count",
         "contact_count", "joint_count", "spring_count", "solved_bodies", "colours", "colour_rounds",
-        "primal_rows", "grid_rescaled")] + [("step_ms", ctypes.c_float)]
+        "primal_rows", "grid_rescaled", "device_steps", "redone_steps")] + [("step_ms", ctypes.c_float)]
 
 
 PHASES = ("broadphase", "force_init", "adjacency", "body_init", "colouring", "primal", "dual", "velocity")
@@ -102,6 +102,9 @@ SIGNATURES = {
     "avbd_write_bodies": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AvbdBodies)]),
     "avbd_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     "avbd_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
+    "avbd_set_step_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    "avbd_set_manifold_headroom": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64]),
+    "avbd_set_wait_limits": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32]),
     "avbd_broadphase_only": (ctypes.c_int, [ctypes.c_void_p]),
     "avbd_read_bodies": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AvbdBodyState)]),
     "avbd_num_manifolds": (ctypes.c_int, [ctypes.c_void_p, c_int_p]),

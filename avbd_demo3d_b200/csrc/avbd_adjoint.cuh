@@ -1545,6 +1545,7 @@ extern "C"
 
 int avbd_adjoint_forward(AvbdContext *ctx, int32_t nsteps, int32_t checkpoint_every)
 {
+    SETTLED();
     CHECK(adjoint_guard(ctx));
     if (nsteps < 1 || checkpoint_every < 1)
         return fail(ctx, AVBD_ERR_ARGUMENT, "adjoint_forward: nsteps and checkpoint_every must be positive");
@@ -1658,6 +1659,7 @@ int avbd_adjoint_forward(AvbdContext *ctx, int32_t nsteps, int32_t checkpoint_ev
 
 int avbd_adjoint_num_pairs(AvbdContext *ctx, int32_t *count)
 {
+    SETTLED();
     CHECK(adjoint_ready(ctx, "adjoint_num_pairs"));
     if (!count)
         return fail(ctx, AVBD_ERR_ARGUMENT, "adjoint_num_pairs: null output");
@@ -1667,6 +1669,7 @@ int avbd_adjoint_num_pairs(AvbdContext *ctx, int32_t *count)
 
 int avbd_adjoint_read_pairs(AvbdContext *ctx, int32_t *lohi2, float *friction)
 {
+    SETTLED();
     CHECK(adjoint_ready(ctx, "adjoint_read_pairs"));
     AdjointState *a = ctx->adjoint;
     std::vector<unsigned long long> keys(std::max(a->P, 1));
@@ -1694,6 +1697,7 @@ int avbd_adjoint_read_pairs(AvbdContext *ctx, int32_t *lohi2, float *friction)
 int avbd_adjoint_replay_state(AvbdContext *ctx, double *position3, double *orientation4, double *velocity3,
                               double *angular_velocity3)
 {
+    SETTLED();
     CHECK(adjoint_ready(ctx, "adjoint_replay_state"));
     AdjointState *a = ctx->adjoint;
     int n = ctx->n;
@@ -1723,6 +1727,7 @@ int avbd_adjoint_replay_state(AvbdContext *ctx, double *position3, double *orien
 int avbd_adjoint_tape_step(AvbdContext *ctx, int32_t step, int32_t *num_manifolds, uint16_t *flags,
                            uint8_t *body_flags, int32_t *link)
 {
+    SETTLED();
     CHECK(adjoint_ready(ctx, "adjoint_tape_step"));
     AdjointState *a = ctx->adjoint;
     if (step < 0 || step >= a->steps)
@@ -1744,6 +1749,7 @@ int avbd_adjoint_tape_step(AvbdContext *ctx, int32_t step, int32_t *num_manifold
 int avbd_adjoint_backward(AvbdContext *ctx, const double *d_position3, const double *d_orientation4,
                           const double *d_velocity3, const double *d_angular_velocity3, const AvbdAdjointGrad *out)
 {
+    SETTLED();
     CHECK(adjoint_ready(ctx, "adjoint_backward"));
     AdjointState *a = ctx->adjoint;
     if (!out)

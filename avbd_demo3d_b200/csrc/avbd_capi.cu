@@ -153,6 +153,10 @@ struct AvbdContext
     DArr<unsigned> colKeys, colKeysAlt;
     DArr<ColourControl> colourCtl;
     int colourBlocks = 148;   // co-resident blocks for the cooperative colouring launch
+    int colourFlowBlocks = 148; // blocks of the greedy colouring's cooperative launch
+    DArr<unsigned long long> colourFlow; // per body: (epoch, round, colour) of the greedy colouring
+    DArr<int> colourBlockCounts;          // 256 colours x blocks
+    unsigned colourEpoch = 0;
     int iterationMode = AVBD_ITERATIONS_PERSISTENT;
     DArr<float4> shape;      // (type, radius, half length, 0) per body when any body is round
     bool hasShapes = false;  // some body is not a box
@@ -197,10 +201,29 @@ struct AvbdContext
     // adjoint: checkpoints, tape and adjoint buffers; `recording` while a step is taped
     AdjointState *adjoint = nullptr;
     bool recording = false;
+
+    // Device-resident steps (grid broadphase, single-launch iterations): the counts live in
+    // a device StepState and a step issues all its launches without waiting for the device.
+    // pendingFast steps have been issued since the host last read that state; until then the
+    // host's nMan / nextSeq / cur are the values at that read (the *AtConfirm fields).
+    DArr<StepState> stepState;
+    StepState *hState = nullptr; // pinned copy of the state, written by every device step
+    DArr<int> stepFlags;          // STEP_SEEN_* bits of the synchronous step's admission check
+    int *hStepFlags = nullptr;    // pinned copy
+    int stepMode = AVBD_STEP_DEVICE;
+    int pendingFast = 0;
+    int doneAtConfirm = 0, flipsAtConfirm = 0, curAtConfirm = 0;
+    bool stateDirty = true;        // the host changed counts: write them to the device state
+    unsigned long long seqBound = 0; // above every sequence number a pending step can create
+    long long manifoldSpare = 0;   // manifold room beyond the live count (0: the default policy)
+    long long deviceSteps = 0, redoneSteps = 0;
+    unsigned waitColour = 0, waitIteration = 0; // poll limits of the bounded waits (0: default)
 };
 
 namespace
 {
+
+int settle(AvbdContext *ctx);
 
 int fail(AvbdContext *ctx, int code, const char *fmt, ...)
 {
@@ -232,6 +255,15 @@ int fail(AvbdContext *ctx, int code, const char *fmt, ...)
         int r_ = (expr);                                                                                           \
         if (r_ != AVBD_OK)                                                                                         \
             return r_;                                                                                             \
+    } while (0)
+
+// Entry points that read or change device state first wait for the device-resident steps
+// issued so far (redoing any that stopped on the device), so calls act in issue order.
+#define SETTLED()                                                                                                  \
+    do                                                                                                             \
+    {                                                                                                              \
+        if (ctx && ctx->pendingFast)                                                                               \
+            CHECK(settle(ctx));                                                                                    \
     } while (0)
 
 #define LAUNCHED()                                                                                                 \
@@ -448,7 +480,6 @@ __global__ void k_total(const int *scan, const int *in, int n, long long *out)
 {
     *out = (long long)scan[n - 1] + (long long)in[n - 1];
 }
-__global__ void k_fill_int(int *p, int v) { *p = v; }
 
 // Colouring summary into pinned host memory: vertices, rounds, max colour, error.
 __global__ void k_colour_count(const ColourControl *ctl, int *unused, int *summary)
@@ -460,11 +491,31 @@ __global__ void k_colour_count(const ColourControl *ctl, int *unused, int *summa
 }
 
 __global__ void k_solve_list_all(const unsigned *keys, int n, int *list, int *colourStart, const ColourControl *ctl,
-                                 const int *rowStart, int4 *entries, const int *colour, int2 *rows)
+                                 const int *rowStart, int4 *entries, const int *colour, int2 *rows,
+                                 StepState *st = nullptr, const StepCounters *cnt = nullptr)
 {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     int count = ctl->vertices;
     int nColours = count > 0 ? ctl->maxColour + 1 : 0;
+    if (st)
+    {
+        if (step_aborted(st))
+            return;
+        if (k == 0)
+        {
+            // a failed colouring stops this step and every later one
+            int err = ctl->error ? STEP_ERR_COLOURING
+                                 : (cnt->error == DERR_TOO_MANY_COLOURS ? STEP_ERR_COLOURS : STEP_ERR_NONE);
+            st->nColours = nColours;
+            st->nSolve = count;
+            st->rounds = ctl->rounds;
+            if (err != STEP_ERR_NONE)
+            {
+                st->error = err;
+                st->abort = ABORT_ERROR;
+            }
+        }
+    }
     if (k >= count)
         return;
     unsigned key = keys[k];
@@ -493,28 +544,96 @@ __global__ void k_solve_list_all(const unsigned *keys, int n, int *list, int *co
             colourStart[x] = count;
 }
 
-__global__ void k_u8_to_int(const unsigned char *in, int *out, int n)
+__global__ void k_u8_to_int(const unsigned char *in, int *out, int n, const StepState *st = nullptr)
 {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < n)
-        out[k] = in[k];
+    if (k >= n)
+        return;
+    // device-resident steps: the launch covers the capacity, the live count is the state's
+    out[k] = (!st || k < st->nManBp) ? in[k] : 0;
+}
+
+// Host counts into the device step state (after a load, an edit or a synchronous step).
+__global__ void k_state_set(StepState *st, int nMan, unsigned long long nextSeq)
+{
+    StepState s = {};
+    s.nMan = nMan;
+    s.nManBp = nMan;
+    s.nextSeq = nextSeq;
+    *st = s;
+}
+
+// After the counting passes of the grid broadphase: the new pairs' total, their place
+// after the live manifolds and their sequence numbers, or a stop when they do not fit or
+// the grid needs the host's cell-count cap.
+__global__ void k_bp_commit(StepState *st, const int *offset, const int *count, int nB, const int *llOffset,
+                            const int *llCount, int nItems, const int *cappedAny, const StepCounters *cnt,
+                            long long capacity)
+{
+    if (st->abort)
+        return;
+    if ((cappedAny && *cappedAny) || cnt->error)
+    {
+        st->abort = ABORT_GRID;
+        return;
+    }
+    long long p1 = nB > 0 ? (long long)offset[nB - 1] + count[nB - 1] : 0;
+    long long p2 = nItems > 0 ? (long long)llOffset[nItems - 1] + llCount[nItems - 1] : 0;
+    if ((long long)st->nMan + p1 + p2 > capacity)
+    {
+        st->abort = ABORT_MANIFOLDS;
+        return;
+    }
+    st->manBase = st->nMan;
+    st->newBinned = (int)p1;
+    st->seqBase = st->nextSeq;
+    st->nManBp = st->nMan + (int)(p1 + p2);
+    st->nextSeq += (unsigned long long)(p1 + p2);
+    st->created = (int)(p1 + p2);
+}
+
+// End of a device-resident step: an expired iteration wait stops every later step.
+__global__ void k_step_end(StepState *st, const IterSync *sync)
+{
+    if (st->abort)
+        return;
+    if (sync->error)
+    {
+        st->error = STEP_ERR_ITERATION;
+        st->abort = ABORT_ERROR;
+        return;
+    }
+    st->stepsDone++;
 }
 
 // Per-body force lists (CSR) sorted newest first.
-int build_rows(AvbdContext *ctx, const unsigned long long *sortedKeys, int total);
+int build_rows(AvbdContext *ctx, const unsigned long long *sortedKeys, int total, size_t manifolds,
+               const StepState *st = nullptr);
 
 // Bits needed to write v (0 for v = 0).
 int bit_width(unsigned long long v) { return v ? 64 - __builtin_clzll(v) : 0; }
 
-int build_adjacency(AvbdContext *ctx)
+// Manifolds both buffers can hold.
+size_t man_capacity(const AvbdContext *ctx)
+{
+    size_t c = ~(size_t)0;
+    for (const ManBuf &b : ctx->man)
+        c = std::min({c, b.ab.cap, b.seq.cap, b.n.cap, b.basis.cap / 3, b.contact.cap / 32});
+    return c == ~(size_t)0 ? 0 : c;
+}
+
+// `deviceCounts`: a device-resident step; the manifold count is the step state's, so the
+// incidences cover the manifold buffers' capacity and the unused slots sort last.
+int build_adjacency(AvbdContext *ctx, bool deviceCounts = false)
 {
     int n = ctx->n;
     CHECK(reserve(ctx, ctx->adjStart, (size_t)n + 1, false));
-    long long T = 2ll * (ctx->nMan + ctx->nJoint + ctx->nSpring + ctx->nIgnore);
+    const size_t mans = deviceCounts ? man_capacity(ctx) : (size_t)ctx->nMan;
+    long long T = 2ll * ((long long)mans + ctx->nJoint + ctx->nSpring + ctx->nIgnore);
     if (T == 0)
     {
         CU(cudaMemsetAsync(ctx->adjStart.p, 0, sizeof(int) * ((size_t)n + 1), ctx->stream));
-        return build_rows(ctx, nullptr, 0);
+        return build_rows(ctx, nullptr, 0, 0);
     }
     if (T > (long long)ADJ_INDEX_MASK)
         return fail(ctx, AVBD_ERR_CAPACITY, "too many force incidences (%lld)", T);
@@ -524,13 +643,16 @@ int build_adjacency(AvbdContext *ctx)
     CHECK(reserve(ctx, ctx->incValsAlt, T, false));
     CHECK(reserve(ctx, ctx->adj, T, false));
     DevForces F = dev_forces(ctx);
-    // every sequence number is below nextSeq: the key needs bit_width(nextSeq) + bit_width(n) bits
-    int shift = std::max(1, bit_width((unsigned long long)std::max<long long>(ctx->nextSeq, 1)));
+    // every sequence number is below nextSeq (below seqBound while steps are pending on the
+    // device): the key needs bit_width(that) + bit_width(n) bits
+    const unsigned long long seqTop = deviceCounts ? ctx->seqBound : (unsigned long long)ctx->nextSeq;
+    int shift = std::max(1, bit_width(std::max<unsigned long long>(seqTop, 1)));
     int endBit = shift + bit_width((unsigned long long)n);
     if (shift > KEY_SEQ_BITS || endBit > 64)
-        return fail(ctx, AVBD_ERR_CAPACITY, "sequence numbers (%lld) too large for the incidence keys", ctx->nextSeq);
+        return fail(ctx, AVBD_ERR_CAPACITY, "sequence numbers (%llu) too large for the incidence keys", seqTop);
     ctx->incShift = shift;
-    k_incidences<<<grid_for(T, 256), 256, 0, ctx->stream>>>(F, shift, n, ctx->incKeys.p, ctx->incVals.p);
+    k_incidences<<<grid_for(T, 256), 256, 0, ctx->stream>>>(F, shift, n, ctx->incKeys.p, ctx->incVals.p,
+                                                            deviceCounts ? ctx->stepState.p : nullptr, (int)T);
     LAUNCHED();
     cub::DoubleBuffer<unsigned long long> dk(ctx->incKeys.p, ctx->incKeysAlt.p);
     cub::DoubleBuffer<unsigned> dv(ctx->incVals.p, ctx->incValsAlt.p);
@@ -539,16 +661,18 @@ int build_adjacency(AvbdContext *ctx)
     CHECK(ensure_temp(ctx, bytes));
     CU(cub::DeviceRadixSort::SortPairs(ctx->cubTemp.p, bytes, dk, dv, (int)T, 0, endBit, ctx->stream));
     ctx->launches++;
-    k_segment_starts<<<grid_for(T, 256), 256, 0, ctx->stream>>>(dk.Current(), (int)T, shift, n, ctx->adjStart.p);
+    const StepState *st = deviceCounts ? ctx->stepState.p : nullptr;
+    k_segment_starts<<<grid_for(T, 256), 256, 0, ctx->stream>>>(dk.Current(), (int)T, shift, n, ctx->adjStart.p, st);
     LAUNCHED();
-    k_copy_adj<<<grid_for(T, 256), 256, 0, ctx->stream>>>(dv.Current(), ctx->adj.p, (int)T);
+    k_copy_adj<<<grid_for(T, 256), 256, 0, ctx->stream>>>(dv.Current(), ctx->adj.p, (int)T, st);
     LAUNCHED();
-    return build_rows(ctx, dk.Current(), (int)T);
+    return build_rows(ctx, dk.Current(), (int)T, mans, st);
 }
 
 // The primal's row list, one (entry, row) pair per constraint row in force order, for the
 // dynamic bodies (no host read: sized by an upper bound, ranges from a device scan).
-int build_rows(AvbdContext *ctx, const unsigned long long *sortedKeys, int total)
+int build_rows(AvbdContext *ctx, const unsigned long long *sortedKeys, int total, size_t manifolds,
+               const StepState *st)
 {
     int n = ctx->n;
     CHECK(reserve(ctx, ctx->rowStart, (size_t)n + 1, false));
@@ -559,19 +683,19 @@ int build_rows(AvbdContext *ctx, const unsigned long long *sortedKeys, int total
     }
     CHECK(reserve(ctx, ctx->rowCount, (size_t)total + 1, false));
     CHECK(reserve(ctx, ctx->entryRow, (size_t)total + 1, false));
-    size_t bound = 16 * (size_t)ctx->nMan + 6 * (size_t)ctx->nJoint + 2 * (size_t)ctx->nSpring;
+    size_t bound = 16 * manifolds + 6 * (size_t)ctx->nJoint + 2 * (size_t)ctx->nSpring;
     CHECK(reserve(ctx, ctx->rows, std::max<size_t>(bound, 1), false));
     DevForces F = dev_forces(ctx);
     k_entry_rows<<<grid_for((long long)total + 1, 256), 256, 0, ctx->stream>>>(F, dev_bodies(ctx), sortedKeys, total,
-                                                                               ctx->incShift, ctx->rowCount.p);
+                                                                               ctx->incShift, ctx->rowCount.p, st);
     LAUNCHED();
     CHECK(scan_counts(ctx, ctx->rowCount.p, ctx->entryRow.p, total + 1, 0));
     ctx->launches++;
     k_row_starts<<<grid_for((long long)n + 1, 256), 256, 0, ctx->stream>>>(ctx->adjStart.p, ctx->entryRow.p, n,
-                                                                           ctx->rowStart.p);
+                                                                           ctx->rowStart.p, st);
     LAUNCHED();
     F = dev_forces(ctx);
-    k_entry_fill<<<grid_for(total, 256), 256, 0, ctx->stream>>>(F, ctx->entryRow.p, ctx->rowCount.p, total);
+    k_entry_fill<<<grid_for(total, 256), 256, 0, ctx->stream>>>(F, ctx->entryRow.p, ctx->rowCount.p, total, st);
     LAUNCHED();
     return AVBD_OK;
 }
@@ -618,9 +742,13 @@ int large_cell_lists(AvbdContext *ctx, int nL)
     LAUNCHED();
     cub::DoubleBuffer<unsigned long long> lk(ctx->largeKeys.p, ctx->largeKeysAlt.p);
     size_t bytes = 0;
-    cub::DeviceRadixSort::SortKeys(nullptr, bytes, lk, total, 0, 64, ctx->stream);
+    // keys: world | global (1) | cell (22) | large index (24), written large body by large
+    // body: the stable sort orders (world, global, cell) only and keeps each run in large-index
+    // order. Unused slots (all ones) still sort last.
+    const int largeEnd = 47 + std::max(1, bit_width((unsigned long long)(ctx->W - 1)));
+    cub::DeviceRadixSort::SortKeys(nullptr, bytes, lk, total, 24, largeEnd, ctx->stream);
     CHECK(ensure_temp(ctx, bytes));
-    CU(cub::DeviceRadixSort::SortKeys(ctx->cubTemp.p, bytes, lk, total, 0, 64, ctx->stream));
+    CU(cub::DeviceRadixSort::SortKeys(ctx->cubTemp.p, bytes, lk, total, 24, largeEnd, ctx->stream));
     ctx->launches++;
     ctx->largeSorted = lk.Current();
     // sentinel after the sorted keys: candidate walks stop at it
@@ -632,10 +760,20 @@ int large_cell_lists(AvbdContext *ctx, int nL)
     return AVBD_OK;
 }
 
-// Broadphase of every world: appends new manifolds after the existing ones.
-int broadphase(AvbdContext *ctx)
+// Broadphase of every world: appends new manifolds after the existing ones. `deviceCounts`
+// (grid mode only): no host read; k_bp_commit places the new pairs from the device counts
+// and the emitting passes take their base from the step state.
+int broadphase(AvbdContext *ctx, bool deviceCounts = false)
 {
     int n = ctx->n;
+    if (deviceCounts && n < 2)
+    {
+        // still commit (no new pairs), so the step state carries this step's counts
+        k_bp_commit<<<1, 1, 0, ctx->stream>>>(ctx->stepState.p, nullptr, nullptr, 0, nullptr, nullptr, 0,
+                                              nullptr, ctx->counters.p, (long long)man_capacity(ctx));
+        LAUNCHED();
+        return AVBD_OK;
+    }
     if (n < 2)
         return AVBD_OK;
     DevBodies B = dev_bodies(ctx);
@@ -738,11 +876,14 @@ int broadphase(AvbdContext *ctx)
             LAUNCHED();
             dk = cub::DoubleBuffer<unsigned long long>(ctx->bpKeys.p, ctx->bpKeysAlt.p);
             size_t bytes = 0;
-            // grid keys: world (below W) | cell (22 bits) | body (24 bits)
+            // grid keys: world (below W) | cell (22 bits) | body (24 bits). The keys are
+            // written in the binned list's order (world by world, ascending body index) and the
+            // radix sort is stable, so ordering the (world, cell) bits alone leaves every cell's
+            // entries in body order: 3 passes for one world instead of 6.
             int gridEnd = 46 + bit_width((unsigned long long)(ctx->W - 1));
-            cub::DeviceRadixSort::SortKeys(nullptr, bytes, dk, nB, 0, gridEnd, ctx->stream);
+            cub::DeviceRadixSort::SortKeys(nullptr, bytes, dk, nB, 24, gridEnd, ctx->stream);
             CHECK(ensure_temp(ctx, bytes));
-            CU(cub::DeviceRadixSort::SortKeys(ctx->cubTemp.p, bytes, dk, nB, 0, gridEnd, ctx->stream));
+            CU(cub::DeviceRadixSort::SortKeys(ctx->cubTemp.p, bytes, dk, nB, 24, gridEnd, ctx->stream));
             ctx->launches++;
             CU(cudaMemsetAsync(ctx->cellHashKeys.p, 0xFF,
                                sizeof(unsigned long long) * ((size_t)ctx->cellHashMask + 1), ctx->stream));
@@ -750,14 +891,17 @@ int broadphase(AvbdContext *ctx)
             LAUNCHED();
             CHECK(large_cell_lists(ctx, nL));
             CHECK(reserve(ctx, ctx->pairRecorded, (size_t)nB * BP_SLOTS, false));
-            k_bp_pairs<false><<<grid_for(nB, 128), 128, 0, ctx->stream>>>(
+            k_bp_pairs<BP_COUNT><<<grid_for(nB, 128), 128, 0, ctx->stream>>>(
                 B, F, G, dk.Current(), nB, cell_hash(ctx), ctx->large.p, ctx->largeLo.p, ctx->largeHi.p,
                 ctx->largeSorted, large_hash(ctx), dt, ctx->pairCount.p, nullptr, 0, 0, cnt, ctx->pairRecorded.p);
             LAUNCHED();
             CHECK(scan_counts(ctx, ctx->pairCount.p, ctx->pairOffset.p, nB, 0));
             ctx->launches++;
-            k_total<<<1, 1, 0, ctx->stream>>>(ctx->pairOffset.p, ctx->pairCount.p, nB, ctx->hScalars);
-            LAUNCHED();
+            if (!deviceCounts)
+            {
+                k_total<<<1, 1, 0, ctx->stream>>>(ctx->pairOffset.p, ctx->pairCount.p, nB, ctx->hScalars);
+                LAUNCHED();
+            }
             return AVBD_OK;
         };
         auto large_large_count = [&]() -> int {
@@ -768,8 +912,11 @@ int broadphase(AvbdContext *ctx)
                 LAUNCHED();
                 CHECK(scan_counts(ctx, ctx->llCount.p, ctx->llOffset.p, nItems, 0));
                 ctx->launches++;
-                k_total<<<1, 1, 0, ctx->stream>>>(ctx->llOffset.p, ctx->llCount.p, nItems, ctx->hScalars + 1);
-                LAUNCHED();
+                if (!deviceCounts)
+                {
+                    k_total<<<1, 1, 0, ctx->stream>>>(ctx->llOffset.p, ctx->llCount.p, nItems, ctx->hScalars + 1);
+                    LAUNCHED();
+                }
             }
             return AVBD_OK;
         };
@@ -785,6 +932,31 @@ int broadphase(AvbdContext *ctx)
             CHECK(counting_pass());
         }
         CHECK(large_large_count());
+        if (deviceCounts)
+        {
+            StepState *st = ctx->stepState.p;
+            k_bp_commit<<<1, 1, 0, ctx->stream>>>(st, ctx->pairOffset.p, ctx->pairCount.p, nB, ctx->llOffset.p,
+                                                  ctx->llCount.p, nItems, ctx->cappedAny.p, cnt,
+                                                  (long long)man_capacity(ctx));
+            LAUNCHED();
+            F = dev_forces(ctx);
+            if (nB)
+            {
+                k_bp_pairs<BP_EMIT_RECORDED><<<grid_for(nB, 128), 128, 0, ctx->stream>>>(
+                    B, F, G, dk.Current(), nB, cell_hash(ctx), ctx->large.p, ctx->largeLo.p, ctx->largeHi.p,
+                    ctx->largeSorted, large_hash(ctx), dt, ctx->pairCount.p, ctx->pairOffset.p, 0, 0, cnt,
+                    ctx->pairRecorded.p, st);
+                LAUNCHED();
+            }
+            if (nItems > 0)
+            {
+                k_bp_large_large<true><<<grid_for(nItems, 128), 128, 0, ctx->stream>>>(
+                    F, ctx->large.p, ctx->largeSphere.p, ctx->llItems.p, nItems, nullptr, ctx->llOffset.p, 0, 0, cnt,
+                    st);
+                LAUNCHED();
+            }
+            return AVBD_OK;
+        }
         CU(cudaMemcpyAsync(ctx->hCapped, ctx->cappedAny.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaMemcpyAsync(ctx->hCounters, cnt, sizeof(StepCounters), cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaStreamSynchronize(ctx->stream));
@@ -813,20 +985,13 @@ int broadphase(AvbdContext *ctx)
         if (P1 + P2 > 0)
             CHECK(reserve_manifolds(ctx, ctx->man[ctx->cur], (size_t)(M0 + P1 + P2), (size_t)M0));
         F = dev_forces(ctx);
-        if (P1 > 0 && !ctx->hCounters->pairOverflow)
+        if (P1 > 0)
         {
-            // every entry's new pairs were recorded while counting: write them out
-            k_bp_emit_recorded<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(
-                F, dk.Current(), nB, ctx->pairCount.p, ctx->pairOffset.p, ctx->pairRecorded.p, M0,
-                (unsigned long long)ctx->nextSeq);
-            LAUNCHED();
-        }
-        else if (P1 > 0)
-        {
-            k_bp_pairs<true><<<grid_for(nB, 128), 128, 0, ctx->stream>>>(
+            // the pairs each entry recorded while counting; entries that found more search again
+            k_bp_pairs<BP_EMIT_RECORDED><<<grid_for(nB, 128), 128, 0, ctx->stream>>>(
                 B, F, G, dk.Current(), nB, cell_hash(ctx), ctx->large.p, ctx->largeLo.p, ctx->largeHi.p,
-                ctx->largeSorted, large_hash(ctx), dt, nullptr, ctx->pairOffset.p, M0,
-                (unsigned long long)ctx->nextSeq, cnt, nullptr);
+                ctx->largeSorted, large_hash(ctx), dt, ctx->pairCount.p, ctx->pairOffset.p, M0,
+                (unsigned long long)ctx->nextSeq, cnt, ctx->pairRecorded.p);
             LAUNCHED();
         }
         if (P2 > 0)
@@ -840,6 +1005,47 @@ int broadphase(AvbdContext *ctx)
     ctx->stats.manifolds_created = P1 + P2;
     ctx->nMan = (int)(M0 + P1 + P2);
     ctx->nextSeq += P1 + P2;
+    return AVBD_OK;
+}
+
+// Force initialisation of a device-resident step: the launches cover the manifold
+// capacity, the live count comes from the step state, and the compaction records the
+// surviving count there. Joints need no compaction here: a step starts only when none is
+// broken (k_step_begin), and a joint breaks only in the iterations.
+int init_forces_device(AvbdContext *ctx)
+{
+    DevBodies B = dev_bodies(ctx);
+    Params P = dev_params(ctx->params);
+    StepState *st = ctx->stepState.p;
+    const int M = (int)man_capacity(ctx), J = ctx->nJoint;
+    const int need = std::max(std::max(M, J), 1);
+    CHECK(reserve(ctx, ctx->keep, (size_t)need, false));
+    CHECK(reserve(ctx, ctx->keepIdx, (size_t)need * 2, false));
+    int *idx = ctx->keepIdx.p;
+    int *cnt32 = ctx->keepIdx.p + need;
+    if (M)
+    {
+        DevManifolds Md = dev_man(ctx->man[ctx->cur]);
+        if (ctx->hasShapes)
+            k_manifold_init<true><<<grid_for(M, 128), 128, 0, ctx->stream>>>(B, Md, M, P, ctx->keep.p, st);
+        else
+            k_manifold_init<false><<<grid_for(M, 128), 128, 0, ctx->stream>>>(B, Md, M, P, ctx->keep.p, st);
+        LAUNCHED();
+        k_u8_to_int<<<grid_for(M, 256), 256, 0, ctx->stream>>>(ctx->keep.p, cnt32, M, st);
+        LAUNCHED();
+        CHECK(scan_counts(ctx, cnt32, idx, M, 0));
+        ctx->launches++;
+        k_manifold_compact<<<grid_for(M, 128), 128, 0, ctx->stream>>>(Md, dev_man(ctx->man[ctx->cur ^ 1]), M,
+                                                                      ctx->keep.p, idx, st);
+        LAUNCHED();
+        ctx->cur ^= 1;
+    }
+    if (J)
+    {
+        DevForces F = dev_forces(ctx);
+        k_joint_init<<<grid_for(J, 128), 128, 0, ctx->stream>>>(B, F, P, ctx->keep.p, st);
+        LAUNCHED();
+    }
     return AVBD_OK;
 }
 
@@ -907,7 +1113,13 @@ int init_forces(AvbdContext *ctx)
     return AVBD_OK;
 }
 
-int colour_bodies(AvbdContext *ctx)
+int colour_readback(AvbdContext *ctx);
+
+// `deviceCounts`: the colouring summary and colour ranges stay on the device (the
+// single-launch iteration kernel reads them there); errors go to the step state. Greedy
+// mode (the default) colours in one dataflow launch (k_colour_greedy); hashed priorities
+// run Jones-Plassmann rounds (k_colour_all) and sort (colour, body) keys.
+int colour_bodies(AvbdContext *ctx, bool deviceCounts = false)
 {
     int n = ctx->n;
     DevBodies B = dev_bodies(ctx);
@@ -920,16 +1132,43 @@ int colour_bodies(AvbdContext *ctx)
     CHECK(reserve(ctx, ctx->colKeysAlt, n, false));
     CHECK(reserve(ctx, ctx->colourStart, 257, false));
     CHECK(reserve(ctx, ctx->colourCtl, 1, false));
-    if (n == 0)
+    if (n == 0 && !deviceCounts)
     {
         ctx->nColours = ctx->nSolve = 0;
         ctx->hColourStart.assign(1, 0);
         return AVBD_OK;
     }
     CU(cudaMemsetAsync(ctx->colourCtl.p, 0, sizeof(ColourControl), ctx->stream));
-    int blocks = std::min(grid_for(n, 256), ctx->colourBlocks);
+    int blocks = std::min(grid_for(std::max(n, 1), 256), ctx->colourBlocks);
     int mode = ctx->colourMode;
-    void *args[] = {&B, &F, &n, &mode, &ctx->colourState.p, &ctx->colourCtl.p, &ctx->counters.p};
+    unsigned spinLimit = ctx->waitColour ? ctx->waitColour : BARRIER_SPIN_LIMIT;
+    StepState *st = deviceCounts ? ctx->stepState.p : nullptr;
+    if (mode == AVBD_COLOUR_GREEDY)
+    {
+        // one cooperative launch: colours, ranges, solve list and entries, row bits
+        const unsigned long long *oldFlow = ctx->colourFlow.p;
+        CHECK(reserve(ctx, ctx->colourFlow, std::max(n, 1), false));
+        if (ctx->colourFlow.p != oldFlow) // fresh memory: no epoch may match by accident
+            CU(cudaMemsetAsync(ctx->colourFlow.p, 0, sizeof(unsigned long long) * ctx->colourFlow.cap, ctx->stream));
+        int fb = std::min(grid_for(std::max(n, 1), COLOUR_FLOW_BLOCK), ctx->colourFlowBlocks);
+        CHECK(reserve(ctx, ctx->colourBlockCounts, (size_t)256 * fb, false));
+        unsigned epoch = ++ctx->colourEpoch;
+        if (epoch == 0) // wrapped: clear every stored epoch and start again
+        {
+            CU(cudaMemsetAsync(ctx->colourFlow.p, 0, sizeof(unsigned long long) * ctx->colourFlow.cap, ctx->stream));
+            epoch = ctx->colourEpoch = 1;
+        }
+        DevForces Fr = dev_forces(ctx);
+        void *fargs[] = {&B, &Fr, &n, &ctx->colourFlow.p, &epoch, &ctx->colour.p, &ctx->colourCtl.p,
+                         &ctx->counters.p, &spinLimit, &ctx->colourBlockCounts.p, &ctx->colourStart.p,
+                         &ctx->solveList.p, &ctx->solveEntry.p, &ctx->rowStart.p, &st};
+        CU(cudaLaunchCooperativeKernel((void *)k_colour_greedy, fb, COLOUR_FLOW_BLOCK, fargs, 0, ctx->stream));
+        LAUNCHED();
+        if (deviceCounts)
+            return AVBD_OK;
+        return colour_readback(ctx);
+    }
+    void *args[] = {&B, &F, &n, &mode, &ctx->colourState.p, &ctx->colourCtl.p, &ctx->counters.p, &spinLimit, &st};
     CU(cudaLaunchCooperativeKernel((void *)k_colour_all, blocks, 256, args, 0, ctx->stream));
     LAUNCHED();
     k_colour_keys<<<grid_for(n, 256), 256, 0, ctx->stream>>>(ctx->colourState.p, n, ctx->colour.p, ctx->colKeys.p);
@@ -943,11 +1182,25 @@ int colour_bodies(AvbdContext *ctx)
     // colour ranges for up to 256 colours are written from the sorted keys; the host reads
     // them together with the colouring summary in one copy
     CU(cudaMemsetAsync(ctx->colourStart.p, 0, sizeof(int) * 257, ctx->stream));
-    k_colour_count<<<1, 1, 0, ctx->stream>>>(ctx->colourCtl.p, ctx->colourStart.p + 257 - 257, ctx->hColourSummary);
-    LAUNCHED();
+    if (deviceCounts)
+    {
+        k_solve_list_all<<<grid_for(std::max(n, 1), 256), 256, 0, ctx->stream>>>(
+            dk.Current(), n, ctx->solveList.p, ctx->colourStart.p, ctx->colourCtl.p, ctx->rowStart.p,
+            ctx->solveEntry.p, ctx->colour.p, ctx->rows.p, st, ctx->counters.p);
+        LAUNCHED();
+        return AVBD_OK;
+    }
     k_solve_list_all<<<grid_for(n, 256), 256, 0, ctx->stream>>>(dk.Current(), n, ctx->solveList.p, ctx->colourStart.p,
                                                                  ctx->colourCtl.p, ctx->rowStart.p,
                                                                  ctx->solveEntry.p, ctx->colour.p, ctx->rows.p);
+    LAUNCHED();
+    return colour_readback(ctx);
+}
+
+// The synchronous step reads the colouring's summary and colour ranges on the host.
+int colour_readback(AvbdContext *ctx)
+{
+    k_colour_count<<<1, 1, 0, ctx->stream>>>(ctx->colourCtl.p, nullptr, ctx->hColourSummary);
     LAUNCHED();
     CU(cudaMemcpyAsync(ctx->hColourStarts, ctx->colourStart.p, sizeof(int) * 257, cudaMemcpyDeviceToHost,
                        ctx->stream));
@@ -979,7 +1232,7 @@ void adjoint_invalidate(AvbdContext *ctx); // the world changed: no backward for
 // Every iteration in one cooperative launch (k_iterations), the contacts' dual updates
 // fused into the next iteration's rows. Recording the differentiable step keeps the
 // per-colour launches, which it hooks between iterations.
-int iterate_persistent(AvbdContext *ctx)
+int iterate_persistent(AvbdContext *ctx, bool deviceCounts = false)
 {
     DevBodies B = dev_bodies(ctx);
     DevForces F = dev_forces(ctx);
@@ -991,10 +1244,12 @@ int iterate_persistent(AvbdContext *ctx)
     const int *colourStart = ctx->colourStart.p;
     IterSync *sync = ctx->iterSync.p;
     // per-body completed iterations, from zero in every launch
-    CHECK(reserve(ctx, ctx->iterDone, ctx->n, false));
+    CHECK(reserve(ctx, ctx->iterDone, std::max(ctx->n, 1), false));
     CU(cudaMemsetAsync(ctx->iterDone.p, 0, sizeof(int) * (size_t)ctx->n, ctx->stream));
     int *done = ctx->iterDone.p;
-    void *args[] = {&B, &F, &P, &entries, &colourStart, &nColours, &iterations, &sync, &done};
+    unsigned spinLimit = ctx->waitIteration ? ctx->waitIteration : ITER_SPIN_LIMIT;
+    const StepState *st = deviceCounts ? ctx->stepState.p : nullptr;
+    void *args[] = {&B, &F, &P, &entries, &colourStart, &nColours, &iterations, &sync, &done, &spinLimit, &st};
     {
         PhaseScope ps(ctx, AVBD_PHASE_PRIMAL);
         // worlds with round bodies run the instance that evaluates their contact offsets
@@ -1004,7 +1259,9 @@ int iterate_persistent(AvbdContext *ctx)
                                        sizeof(PrimalShared<ITER_G, ITER_BLOCK>), ctx->stream));
         LAUNCHED();
     }
-    CU(cudaMemcpyAsync(ctx->hIterError, &ctx->iterSync.p->error, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    if (!deviceCounts) // device-resident steps hand the error to the step state (k_step_end)
+        CU(cudaMemcpyAsync(ctx->hIterError, &ctx->iterSync.p->error, sizeof(int), cudaMemcpyDeviceToHost,
+                           ctx->stream));
     return AVBD_OK;
 }
 
@@ -1056,6 +1313,16 @@ int iterate(AvbdContext *ctx)
 
 int step_once(AvbdContext *ctx)
 {
+    // refuse non-finite body state before anything changes, like a device-resident step
+    CU(cudaMemsetAsync(ctx->stepFlags.p, 0, sizeof(int), ctx->stream));
+    k_step_begin<<<grid_for(std::max(ctx->n, 1), 256), 256, 0, ctx->stream>>>(dev_bodies(ctx), nullptr, 0, nullptr,
+                                                                               ctx->stepFlags.p);
+    LAUNCHED();
+    CU(cudaMemcpyAsync(ctx->hStepFlags, ctx->stepFlags.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    if (*ctx->hStepFlags & STEP_SEEN_NONFINITE)
+        return fail(ctx, AVBD_ERR_STATE,
+                    "non-finite body position, orientation or velocity at the start of a step (the step was not run)");
     if (ctx->recording)
         CHECK(rec_step_begin(ctx));
     CU(cudaMemsetAsync(ctx->counters.p, 0, sizeof(StepCounters), ctx->stream));
@@ -1109,6 +1376,179 @@ int step_once(AvbdContext *ctx)
     ctx->stats.constrained_hits = (int64_t)ctx->hCounters->constrainedHits;
     if (ctx->profiling)
         ctx->stepsProfiled++;
+    return AVBD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Device-resident steps
+// ---------------------------------------------------------------------------
+
+// The host's counts become the device state's (no step is pending).
+int push_state(AvbdContext *ctx)
+{
+    k_state_set<<<1, 1, 0, ctx->stream>>>(ctx->stepState.p, ctx->nMan, (unsigned long long)ctx->nextSeq);
+    LAUNCHED();
+    ctx->doneAtConfirm = 0;
+    ctx->flipsAtConfirm = 0;
+    ctx->curAtConfirm = ctx->cur;
+    ctx->seqBound = (unsigned long long)ctx->nextSeq;
+    ctx->stateDirty = false;
+    return AVBD_OK;
+}
+
+// Steps that can keep their counts on the device: the grid broadphase, the single-launch
+// iterations, not while the differentiable step records.
+bool device_step_ok(const AvbdContext *ctx)
+{
+    return ctx->stepMode == AVBD_STEP_DEVICE && ctx->params.broadphase == AVBD_BROADPHASE_GRID &&
+           ctx->iterationMode == AVBD_ITERATIONS_PERSISTENT && ctx->iterBlocks > 0 && !ctx->recording &&
+           ctx->params.iterations > 0;
+}
+
+// Both manifold buffers with room for the live manifolds and a step's new pairs (grown
+// only while no step is pending, when the live count is known).
+int device_reserve(AvbdContext *ctx)
+{
+    size_t live = (size_t)ctx->nMan;
+    size_t want = ctx->manifoldSpare > 0 ? live + (size_t)ctx->manifoldSpare
+                                         : std::max(2 * live, live + (size_t)ctx->n / 2) + 1024;
+    if (ctx->pendingFast == 0 && man_capacity(ctx) < want)
+    {
+        CHECK(reserve_manifolds(ctx, ctx->man[ctx->cur], want, live));
+        CHECK(reserve_manifolds(ctx, ctx->man[ctx->cur ^ 1], want, 0));
+    }
+    return AVBD_OK;
+}
+
+// One Solver::step with every count on the device: the same kernels as step_once, sized by
+// capacity, with k_step_begin / k_bp_commit deciding on the device whether the step can run.
+int step_device(AvbdContext *ctx)
+{
+    // with no step pending the host's counts are current (a settle, a synchronous step, a
+    // load or an edit came last): they become the device state's
+    if (ctx->stateDirty || ctx->pendingFast == 0)
+        CHECK(push_state(ctx));
+    CHECK(device_reserve(ctx));
+    // this step's new manifolds take sequence numbers below nextSeq + capacity: the bound the
+    // incidence keys of this step (and of later pending steps) are sized by
+    ctx->seqBound += (unsigned long long)man_capacity(ctx);
+    StepState *st = ctx->stepState.p;
+    CU(cudaMemsetAsync(ctx->counters.p, 0, sizeof(StepCounters), ctx->stream));
+    ctx->stats.grid_rescaled = 0;
+    DevBodies B = dev_bodies(ctx);
+    Params P = dev_params(ctx->params);
+    {
+        PhaseScope ps(ctx, AVBD_PHASE_BROADPHASE);
+        const int J = ctx->nJoint;
+        k_step_begin<<<grid_for(std::max(std::max(ctx->n, J), 1), 256), 256, 0, ctx->stream>>>(
+            B, ctx->joint[ctx->jcur].p, J, st, nullptr);
+        LAUNCHED();
+        CHECK(broadphase(ctx, true));
+    }
+    {
+        PhaseScope ps(ctx, AVBD_PHASE_FORCE_INIT);
+        CHECK(init_forces_device(ctx));
+    }
+    {
+        PhaseScope ps(ctx, AVBD_PHASE_ADJACENCY);
+        CHECK(build_adjacency(ctx, true));
+    }
+    if (ctx->n)
+    {
+        PhaseScope ps(ctx, AVBD_PHASE_BODY_INIT);
+        k_warm_start<<<grid_for(ctx->n, 256), 256, 0, ctx->stream>>>(B, ctx->adjStart.p, P, st);
+        LAUNCHED();
+    }
+    {
+        PhaseScope ps(ctx, AVBD_PHASE_COLOURING);
+        CHECK(colour_bodies(ctx, true));
+    }
+    CHECK(iterate_persistent(ctx, true));
+    if (ctx->n)
+    {
+        PhaseScope ps(ctx, AVBD_PHASE_VELOCITY);
+        k_finish<<<grid_for(ctx->n, 256), 256, 0, ctx->stream>>>(B, P, st);
+        LAUNCHED();
+        if (ctx->hasSpheres)
+        {
+            k_rolling_friction<<<grid_for(ctx->n, 128), 128, 0, ctx->stream>>>(B, dev_forces(ctx), ctx->adjStart.p,
+                                                                               st);
+            LAUNCHED();
+        }
+    }
+    k_step_end<<<1, 1, 0, ctx->stream>>>(st, ctx->iterSync.p);
+    LAUNCHED();
+    CU(cudaMemcpyAsync(ctx->hState, st, sizeof(StepState), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaMemcpyAsync(ctx->hCounters, ctx->counters.p, sizeof(StepCounters), cudaMemcpyDeviceToHost, ctx->stream));
+    ctx->pendingFast++;
+    ctx->deviceSteps++;
+    if (ctx->profiling)
+        ctx->stepsProfiled++;
+    return AVBD_OK;
+}
+
+// Wait for the device-resident steps issued so far and take their counts. Steps that
+// stopped on the device before changing anything (ABORT_JOINTS / GRID / MANIFOLDS, and
+// every step issued after one) are redone synchronously by step_once, which compacts the
+// broken joints, rescales the grid with the host's cbrtf or grows the buffers; errors
+// latch. Afterwards the host's counts are current again.
+int settle(AvbdContext *ctx)
+{
+    if (ctx->pendingFast == 0)
+        return AVBD_OK;
+    const int pending = ctx->pendingFast;
+    ctx->pendingFast = 0;
+    CU(cudaStreamSynchronize(ctx->stream));
+    const StepState s = *ctx->hState;
+    const int done = s.stepsDone - ctx->doneAtConfirm;
+    const int flips = s.flips - ctx->flipsAtConfirm;
+    ctx->cur = ctx->curAtConfirm ^ (flips & 1);
+    ctx->nMan = s.nMan;
+    ctx->nextSeq = (long long)s.nextSeq;
+    ctx->nColours = s.nColours;
+    ctx->nSolve = s.nSolve;
+    ctx->doneAtConfirm = s.stepsDone;
+    ctx->flipsAtConfirm = s.flips;
+    ctx->curAtConfirm = ctx->cur;
+    ctx->seqBound = s.nextSeq;
+    if (done > 0)
+    {
+        ctx->stats.body_count = ctx->n;
+        ctx->stats.manifold_count = ctx->nMan;
+        ctx->stats.joint_count = ctx->nJoint;
+        ctx->stats.spring_count = ctx->nSpring;
+        ctx->stats.solved_bodies = ctx->nSolve;
+        ctx->stats.colours = ctx->nColours;
+        ctx->stats.colour_rounds = s.rounds;
+        ctx->stats.manifolds_created = s.created;
+        ctx->stats.pair_checks = (int64_t)ctx->hCounters->pairChecks;
+        ctx->stats.sphere_hits = (int64_t)ctx->hCounters->sphereHits;
+        ctx->stats.constrained_hits = (int64_t)ctx->hCounters->constrainedHits;
+    }
+    if (s.abort == ABORT_NONE)
+        return AVBD_OK;
+    ctx->stateDirty = true; // the device's stop word is cleared before the next device step
+    // The stopped steps still rebuilt the per-body force lists (from buffers the host had
+    // swapped for them); the next broadphase reads those lists, so rebuild them from the
+    // confirmed state.
+    CHECK(build_adjacency(ctx));
+    if (s.abort == ABORT_ERROR)
+    {
+        if (s.error == STEP_ERR_ITERATION)
+            return fail(ctx, AVBD_ERR_STATE,
+                        "iteration kernel wait expired (a grid barrier or a partner body's iteration count)");
+        if (s.error == STEP_ERR_COLOURS)
+            return fail(ctx, AVBD_ERR_CAPACITY, "constraint graph needs more than 256 colours");
+        return fail(ctx, AVBD_ERR_STATE, "colouring did not finish (barrier wait expired or round cap reached)");
+    }
+    if (s.abort == ABORT_NONFINITE)
+        return fail(ctx, AVBD_ERR_STATE,
+                    "non-finite body position, orientation or velocity at the start of a step (the step was not run)");
+    for (int r = done; r < pending; ++r)
+    {
+        CHECK(step_once(ctx));
+        ctx->redoneSteps++;
+    }
     return AVBD_OK;
 }
 
@@ -1440,18 +1880,26 @@ int avbd_create(AvbdContext **out, int32_t device_ordinal, void *cuda_stream)
         cudaMallocHost((void **)&ctx->hCapped, sizeof(int)) != cudaSuccess ||
         cudaMallocHost((void **)&ctx->hColourStarts, sizeof(int) * 257) != cudaSuccess ||
         cudaMallocHost((void **)&ctx->hIterError, sizeof(int)) != cudaSuccess ||
+        cudaMallocHost((void **)&ctx->hState, sizeof(StepState)) != cudaSuccess ||
+        cudaMallocHost((void **)&ctx->hStepFlags, sizeof(int)) != cudaSuccess ||
         cudaEventCreate(&ctx->evStart) != cudaSuccess || cudaEventCreate(&ctx->evStop) != cudaSuccess)
     {
         avbd_destroy(ctx);
         return AVBD_ERR_CUDA;
     }
     memset(ctx->hCounters, 0, sizeof(StepCounters));
+    memset(ctx->hState, 0, sizeof(StepState));
     *ctx->hIterError = 0;
     {
         int sms = 0, perSm = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_ordinal);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_colour_all, 256, 0);
         ctx->colourBlocks = std::max(1, sms * std::max(1, perSm));
+        // the greedy colouring: co-resident, and at most two blocks per SM (every block
+        // reads all blocks' colour counts once)
+        int flowSm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&flowSm, k_colour_greedy, COLOUR_FLOW_BLOCK, 0);
+        ctx->colourFlowBlocks = std::max(1, sms * std::min(2, std::max(1, flowSm)));
         // the iteration kernel: one block of ITER_BLOCK threads per SM with its shared batch
         int iterSm = 0;
         size_t smem = sizeof(PrimalShared<ITER_G, ITER_BLOCK>);
@@ -1468,7 +1916,8 @@ int avbd_create(AvbdContext **out, int32_t device_ordinal, void *cuda_stream)
         cudaGetLastError(); // an unsupported configuration only leaves the per-colour launches
     }
     if (reserve(ctx, ctx->counters, 1, false) || reserve(ctx, ctx->bounds, 8, false) ||
-        reserve(ctx, ctx->grid, 1, false))
+        reserve(ctx, ctx->grid, 1, false) || reserve(ctx, ctx->stepState, 1, false) ||
+        reserve(ctx, ctx->stepFlags, 1, false))
     {
         avbd_destroy(ctx);
         return AVBD_ERR_CUDA;
@@ -1578,6 +2027,10 @@ void avbd_destroy(AvbdContext *ctx)
     release(ctx->colKeysAlt);
     release(ctx->cubTemp);
     release(ctx->counters);
+    release(ctx->stepState);
+    release(ctx->colourFlow);
+    release(ctx->colourBlockCounts);
+    release(ctx->stepFlags);
     if (ctx->hCounters)
         cudaFreeHost(ctx->hCounters);
     if (ctx->hScalars)
@@ -1594,6 +2047,10 @@ void avbd_destroy(AvbdContext *ctx)
         cudaFreeHost(ctx->hColourStarts);
     if (ctx->hIterError)
         cudaFreeHost(ctx->hIterError);
+    if (ctx->hState)
+        cudaFreeHost(ctx->hState);
+    if (ctx->hStepFlags)
+        cudaFreeHost(ctx->hStepFlags);
     release(ctx->iterSync);
     release(ctx->iterDone);
     if (ctx->stageDone)
@@ -1617,6 +2074,9 @@ void avbd_clear_error(AvbdContext *ctx)
     {
         ctx->err.clear();
         ctx->errCode = 0;
+        ctx->stateDirty = true; // clears the device steps' stop word before the next one
+        if (ctx->hIterError)
+            *ctx->hIterError = 0; // the failed iteration launch's flag was read already
     }
 }
 
@@ -1629,6 +2089,9 @@ int avbd_set_params(AvbdContext *ctx, const AvbdParams *params)
     if (params->broadphase != AVBD_BROADPHASE_GRID && params->broadphase != AVBD_BROADPHASE_ALL_PAIRS &&
         params->broadphase != AVBD_BROADPHASE_SAP)
         return fail(ctx, AVBD_ERR_ARGUMENT, "broadphase mode %d is not available on the GPU", params->broadphase);
+    // pending device-resident steps run (or are redone) with the parameters they were issued with
+    if (memcmp(&ctx->params, params, sizeof(AvbdParams)) != 0)
+        SETTLED();
     ctx->params = *params;
     return AVBD_OK;
 }
@@ -1665,6 +2128,7 @@ int avbd_load_batch(AvbdContext *ctx, int32_t num_worlds, const int32_t *world_s
     if (ctx->errCode)
         return AVBD_ERR_LATCHED;
     adjoint_invalidate(ctx);
+    ctx->pendingFast = 0; // steps of the old world still in flight no longer matter (stream order)
     int n = bodies->count;
     if (n < 0 || n >= (int)KEY_NO_BODY)
         return fail(ctx, AVBD_ERR_ARGUMENT, "body count %d out of range", n);
@@ -1818,11 +2282,14 @@ int avbd_load_batch(AvbdContext *ctx, int32_t num_worlds, const int32_t *world_s
     ctx->nColours = 0;
     ctx->nSolve = 0;
     ctx->loaded = true;
+    ctx->stateDirty = true;
+    ctx->deviceSteps = ctx->redoneSteps = 0;
     return AVBD_OK;
 }
 
 int avbd_write_bodies(AvbdContext *ctx, const AvbdBodies *bodies)
 {
+    SETTLED();
     if (!ctx || !bodies)
         return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
     if (!ctx->loaded || bodies->count != ctx->n)
@@ -1844,12 +2311,50 @@ int avbd_step(AvbdContext *ctx, int32_t nsteps)
     adjoint_invalidate(ctx);
     CU(cudaSetDevice(ctx->device));
     for (int s = 0; s < nsteps; ++s)
-        CHECK(step_once(ctx));
+    {
+        if (device_step_ok(ctx))
+            CHECK(step_device(ctx));
+        else
+        {
+            SETTLED();
+            CHECK(step_once(ctx));
+            ctx->stateDirty = true;
+        }
+    }
+    return AVBD_OK;
+}
+
+int avbd_set_step_mode(AvbdContext *ctx, int32_t mode)
+{
+    if (!ctx || (mode != AVBD_STEP_DEVICE && mode != AVBD_STEP_HOST))
+        return fail(ctx, AVBD_ERR_ARGUMENT, "step mode must be AVBD_STEP_DEVICE or AVBD_STEP_HOST");
+    SETTLED();
+    ctx->stepMode = mode;
+    return AVBD_OK;
+}
+
+int avbd_set_manifold_headroom(AvbdContext *ctx, int64_t spare)
+{
+    if (!ctx || spare < 0)
+        return fail(ctx, AVBD_ERR_ARGUMENT, "manifold headroom must be zero or positive");
+    SETTLED();
+    ctx->manifoldSpare = spare;
+    return AVBD_OK;
+}
+
+int avbd_set_wait_limits(AvbdContext *ctx, uint32_t colouring_polls, uint32_t iteration_polls)
+{
+    if (!ctx)
+        return AVBD_ERR_ARGUMENT;
+    SETTLED();
+    ctx->waitColour = colouring_polls;
+    ctx->waitIteration = iteration_polls;
     return AVBD_OK;
 }
 
 int avbd_broadphase_only(AvbdContext *ctx)
 {
+    SETTLED();
     if (!ctx)
         return AVBD_ERR_ARGUMENT;
     if (ctx->errCode)
@@ -1888,6 +2393,9 @@ int avbd_synchronize(AvbdContext *ctx)
 {
     if (!ctx)
         return AVBD_ERR_ARGUMENT;
+    if (ctx->errCode)
+        return AVBD_ERR_LATCHED;
+    SETTLED();
     CU(cudaStreamSynchronize(ctx->stream));
     if (*ctx->hIterError)
         return fail(ctx, AVBD_ERR_STATE, "iteration kernel wait expired (a grid barrier or a partner body's iteration count)");
@@ -1896,6 +2404,7 @@ int avbd_synchronize(AvbdContext *ctx)
 
 int avbd_read_bodies(AvbdContext *ctx, const AvbdBodyState *out)
 {
+    SETTLED();
     if (!ctx || !out)
         return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
     int n = ctx->n;
@@ -1936,6 +2445,7 @@ int avbd_read_bodies(AvbdContext *ctx, const AvbdBodyState *out)
 
 int avbd_num_manifolds(AvbdContext *ctx, int32_t *count)
 {
+    SETTLED();
     if (!ctx || !count)
         return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
     *count = ctx->nMan;
@@ -1944,6 +2454,7 @@ int avbd_num_manifolds(AvbdContext *ctx, int32_t *count)
 
 int avbd_read_manifolds(AvbdContext *ctx, const AvbdManifoldsOut *out)
 {
+    SETTLED();
     if (!ctx || !out)
         return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
     int M = ctx->nMan;
@@ -2005,6 +2516,7 @@ int avbd_read_manifolds(AvbdContext *ctx, const AvbdManifoldsOut *out)
 
 int avbd_num_joints(AvbdContext *ctx, int32_t *count)
 {
+    SETTLED();
     if (!ctx || !count)
         return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
     *count = ctx->nJoint;
@@ -2013,6 +2525,7 @@ int avbd_num_joints(AvbdContext *ctx, int32_t *count)
 
 int avbd_read_joints(AvbdContext *ctx, const AvbdJointsOut *out)
 {
+    SETTLED();
     if (!ctx || !out)
         return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
     int J = ctx->nJoint;
@@ -2058,6 +2571,7 @@ int avbd_read_joints(AvbdContext *ctx, const AvbdJointsOut *out)
 
 int avbd_next_seq(AvbdContext *ctx, int64_t *next_seq)
 {
+    SETTLED();
     if (!ctx || !next_seq)
         return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
     *next_seq = ctx->nextSeq;
@@ -2118,6 +2632,7 @@ int match_joints(AvbdContext *ctx, const std::vector<unsigned long long> &seq, c
 
 int avbd_add_joints(AvbdContext *ctx, const AvbdJoints *joints)
 {
+    SETTLED();
     CHECK(edit_begin(ctx));
     if (!joints || joints->count < 0)
         return fail(ctx, AVBD_ERR_ARGUMENT, "null or negative joint list");
@@ -2163,6 +2678,7 @@ int avbd_add_joints(AvbdContext *ctx, const AvbdJoints *joints)
 
 int avbd_remove_joints(AvbdContext *ctx, int32_t count, const int64_t *seq)
 {
+    SETTLED();
     CHECK(edit_begin(ctx));
     if (count < 0 || (count && !seq))
         return fail(ctx, AVBD_ERR_ARGUMENT, "null or negative sequence list");
@@ -2198,6 +2714,7 @@ int avbd_remove_joints(AvbdContext *ctx, int32_t count, const int64_t *seq)
 
 int avbd_write_joints(AvbdContext *ctx, const AvbdJoints *joints)
 {
+    SETTLED();
     CHECK(edit_begin(ctx));
     if (!joints || joints->count < 0)
         return fail(ctx, AVBD_ERR_ARGUMENT, "null or negative joint list");
@@ -2329,6 +2846,7 @@ int snapshot_records(AvbdContext *ctx, const int32_t *body_id, unsigned char *ds
 int avbd_snapshot_binary(AvbdContext *ctx, uint64_t frame, const char *scene_name, const int32_t *body_id,
                          uint8_t *out, int64_t capacity, int64_t *size)
 {
+    SETTLED();
     if (!ctx || !size)
         return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
     if (!ctx->loaded)
@@ -2355,6 +2873,7 @@ int avbd_snapshot_binary(AvbdContext *ctx, uint64_t frame, const char *scene_nam
 int avbd_snapshot_json(AvbdContext *ctx, uint64_t frame, const char *scene_name, const int32_t *body_id, char *out,
                        int64_t capacity, int64_t *size)
 {
+    SETTLED();
     if (!ctx || !size)
         return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
     if (!ctx->loaded)
@@ -2420,6 +2939,7 @@ int avbd_snapshot_json(AvbdContext *ctx, uint64_t frame, const char *scene_name,
 
 int avbd_read_colours(AvbdContext *ctx, int32_t *colour, int32_t *num_colours)
 {
+    SETTLED();
     if (!ctx)
         return AVBD_ERR_ARGUMENT;
     if (num_colours)
@@ -2440,6 +2960,7 @@ int avbd_read_colours(AvbdContext *ctx, int32_t *colour, int32_t *num_colours)
 
 int avbd_read_solve_order(AvbdContext *ctx, int32_t *order, int32_t *count)
 {
+    SETTLED();
     if (!ctx)
         return AVBD_ERR_ARGUMENT;
     if (count)
@@ -2454,6 +2975,12 @@ int avbd_read_solve_order(AvbdContext *ctx, int32_t *order, int32_t *count)
 
 int avbd_get_stats(AvbdContext *ctx, AvbdStats *stats)
 {
+    SETTLED();
+    if (ctx)
+    {
+        ctx->stats.device_steps = ctx->deviceSteps;
+        ctx->stats.redone_steps = ctx->redoneSteps;
+    }
     if (!ctx || !stats)
         return AVBD_ERR_ARGUMENT;
     *stats = ctx->stats;
@@ -2462,6 +2989,7 @@ int avbd_get_stats(AvbdContext *ctx, AvbdStats *stats)
 
 int avbd_device_pose(AvbdContext *ctx, void **position4, void **orientation4)
 {
+    SETTLED();
     if (!ctx)
         return AVBD_ERR_ARGUMENT;
     if (position4)
@@ -2487,6 +3015,7 @@ int avbd_num_primal_variants(int32_t *count, int32_t *group4, int32_t *min_block
 
 int avbd_set_primal_variant(AvbdContext *ctx, int32_t variant)
 {
+    SETTLED();
     if (!ctx)
         return AVBD_ERR_ARGUMENT;
     if (variant < 0 || variant >= kNumPrimalVariants)
@@ -2497,6 +3026,7 @@ int avbd_set_primal_variant(AvbdContext *ctx, int32_t variant)
 
 int avbd_autotune(AvbdContext *ctx, int32_t repeats, int32_t *best_variant, float *variant_us)
 {
+    SETTLED();
     if (!ctx)
         return AVBD_ERR_ARGUMENT;
     if (ctx->errCode)
@@ -2569,6 +3099,7 @@ int avbd_autotune(AvbdContext *ctx, int32_t repeats, int32_t *best_variant, floa
 
 int avbd_set_iteration_mode(AvbdContext *ctx, int32_t mode)
 {
+    SETTLED();
     if (!ctx)
         return AVBD_ERR_ARGUMENT;
     if (mode != AVBD_ITERATIONS_PER_COLOUR && mode != AVBD_ITERATIONS_PERSISTENT)
@@ -2590,6 +3121,7 @@ int avbd_iteration_mode(AvbdContext *ctx, int32_t *mode)
 
 int avbd_set_colouring(AvbdContext *ctx, int32_t mode)
 {
+    SETTLED();
     if (!ctx)
         return AVBD_ERR_ARGUMENT;
     if (mode != AVBD_COLOUR_GREEDY && mode != AVBD_COLOUR_HASHED)
@@ -2600,6 +3132,7 @@ int avbd_set_colouring(AvbdContext *ctx, int32_t mode)
 
 int avbd_set_profiling(AvbdContext *ctx, int32_t enable)
 {
+    SETTLED();
     if (!ctx)
         return AVBD_ERR_ARGUMENT;
     ctx->profiling = enable != 0;
@@ -2608,6 +3141,7 @@ int avbd_set_profiling(AvbdContext *ctx, int32_t enable)
 
 int avbd_read_profile(AvbdContext *ctx, AvbdProfile *out)
 {
+    SETTLED();
     if (!ctx || !out)
         return AVBD_ERR_ARGUMENT;
     CHECK(prof_collect(ctx));
@@ -2623,6 +3157,7 @@ int avbd_read_profile(AvbdContext *ctx, AvbdProfile *out)
 
 int avbd_reset_profile(AvbdContext *ctx)
 {
+    SETTLED();
     if (!ctx)
         return AVBD_ERR_ARGUMENT;
     CHECK(prof_collect(ctx));

@@ -18,8 +18,9 @@ AVBD_DEV unsigned colour_priority(unsigned b)
     return h;
 }
 
-// Bounded grid-wide barrier for cooperative launches. Every wait has an iteration limit;
-// on expiry the kernel records an error and all blocks leave (the caller checks `error`).
+// Bounded grid-wide barrier for cooperative launches. Every wait has an iteration limit
+// (BARRIER_SPIN_LIMIT unless the caller passes one); on expiry the kernel records an error
+// and all blocks leave (the caller checks `error`).
 constexpr int MAX_COLOUR_ROUNDS = 4096;
 constexpr unsigned BARRIER_SPIN_LIMIT = 1u << 24;
 
@@ -37,7 +38,7 @@ struct ColourControl
 // Arrivals count up through the launch (the control block starts zeroed): barrier k
 // releases every block once k x gridDim.x blocks have arrived, so the last block's arrival
 // alone opens it. `target` is the calling block's count of barriers passed x gridDim.x.
-AVBD_DEV bool grid_barrier(ColourControl *ctl, unsigned &target)
+AVBD_DEV bool grid_barrier(ColourControl *ctl, unsigned &target, unsigned spinLimit = BARRIER_SPIN_LIMIT)
 {
     __syncthreads();
     __shared__ int ok;
@@ -48,10 +49,10 @@ AVBD_DEV bool grid_barrier(ColourControl *ctl, unsigned &target)
         atomicAdd(&ctl->arrive, 1u);
         volatile unsigned *arrive = &ctl->arrive;
         unsigned spins = 0;
-        while (*arrive < target && ++spins < BARRIER_SPIN_LIMIT)
+        while (*arrive < target && ++spins < spinLimit)
             if (spins > 256)
                 __nanosleep(64);
-        ok = spins < BARRIER_SPIN_LIMIT;
+        ok = spins < spinLimit;
         if (!ok)
             atomicExch(&ctl->error, 1);
         __threadfence();

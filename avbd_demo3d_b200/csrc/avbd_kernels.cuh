@@ -116,6 +116,49 @@ enum DeviceError
     DERR_TOO_MANY_CELLS = 2
 };
 
+// Counts of a step that the device keeps for itself, so that a step runs without reading
+// anything back to the host. Every kernel that changes the world checks `abort` first.
+// The reasons a step stops before changing anything (the host redoes it with the
+// synchronous path, which handles each case) come first; an error stops the step where it
+// happens, latches, and every later step does nothing until the host reloads or clears.
+enum StepAbort
+{
+    ABORT_NONE = 0,
+    ABORT_JOINTS = 1,    // a joint broke in an earlier step: the joint list is compacted first
+    ABORT_GRID = 2,      // the grid needs the reference's cell-count cap (host cbrtf)
+    ABORT_MANIFOLDS = 3, // the new pairs do not fit the manifold buffers
+    ABORT_NONFINITE = 4, // a body's position, orientation or velocity is not finite
+    ABORT_ERROR = 5      // the colouring or an iteration wait failed (see `error`)
+};
+
+enum StepError
+{
+    STEP_ERR_NONE = 0,
+    STEP_ERR_COLOURING = 1,     // the colouring's barrier wait expired or it ran out of rounds
+    STEP_ERR_COLOURS = 2,       // the constraint graph needs more than 256 colours
+    STEP_ERR_ITERATION = 3      // a grid barrier or partner wait of the iteration kernel expired
+};
+
+struct StepState
+{
+    int nMan;                    // live manifolds after the last compaction
+    int nManBp;                  // live manifolds plus this step's new pairs
+    int manBase;                 // first new manifold of this step
+    int newBinned;               // new pairs from grid entries (the large-large pairs follow)
+    unsigned long long nextSeq;  // sequence counter after this step's new pairs
+    unsigned long long seqBase;  // sequence number of the step's first new manifold
+    int abort;                   // StepAbort, sticky until the host clears it
+    int error;                   // StepError of the failure that set ABORT_ERROR
+    int stepsDone;               // steps that ran to the end
+    int flips;                   // manifold compactions (each swaps the manifold buffers)
+    int nColours, nSolve, rounds;
+    int created;                 // new manifolds of the last step
+};
+
+AVBD_DEV bool step_aborted(const StepState *st) { return st && ((volatile const int *)&st->abort)[0] != 0; }
+
+AVBD_DEV void step_abort(StepState *st, int reason) { atomicCAS(&st->abort, 0, reason); }
+
 AVBD_DEV unsigned adj_type(unsigned e) { return e >> 30; }
 AVBD_DEV unsigned adj_isA(unsigned e) { return (e >> 29) & 1u; }
 AVBD_DEV unsigned adj_index(unsigned e) { return e & ADJ_INDEX_MASK; }
@@ -483,21 +526,52 @@ AVBD_DEV void warp_add(unsigned long long *dst, unsigned v)
 
 constexpr int BP_SLOTS = 4; // new pairs a grid entry records in the counting pass
 
-// One thread per sorted grid entry i (solver.cpp:405-465). EMIT == false counts new
-// (unconstrained) hits and records the first BP_SLOTS partners of each entry in `recorded`
-// (k_bp_emit_recorded writes them out); EMIT == true, needed only when an entry found more,
-// writes them as fresh manifolds at base + offset[i] in hit order. Large bodies are visited in list order: the entry's cell candidates merged
-// with its world's global list, both sorted by large index.
-template <bool EMIT>
+// Modes of the grid-entry pass: count (and record), emit every entry's pairs by searching
+// again, or emit what the counting pass recorded and search again only for the entries
+// that found more than BP_SLOTS.
+constexpr int BP_COUNT = 0, BP_EMIT = 1, BP_EMIT_RECORDED = 2;
+
+// One thread per sorted grid entry i (solver.cpp:405-465). BP_COUNT counts new
+// (unconstrained) hits and records the first BP_SLOTS partners of each entry in `recorded`;
+// the emitting modes write them as fresh manifolds at base + offset[i] in hit order. Large
+// bodies are visited in list order: the entry's cell candidates merged with its world's
+// global list, both sorted by large index. With a device step state the emitting modes take
+// base and seqBase from it.
+template <int MODE>
 __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, DevGrid G, const unsigned long long *keys,
                                                   int nBinned, HashTable cells, const int *large,
                                                   const float4 *largeLo, const float4 *largeHi,
                                                   const unsigned long long *largeKeys, HashTable largeCells, float dt,
                                                   int *counts, const int *offsets, int base, unsigned long long seqBase,
-                                                  StepCounters *cnt, int *recorded)
+                                                  StepCounters *cnt, int *recorded, const StepState *st = nullptr)
 {
+    constexpr bool EMIT = MODE != BP_COUNT;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool active = i < nBinned;
+    bool active = i < nBinned;
+    if (EMIT && st)
+    {
+        if (step_aborted(st))
+            return;
+        base = st->manBase;
+        seqBase = st->seqBase;
+    }
+    if (MODE == BP_EMIT_RECORDED && active)
+    {
+        const int c = counts[i];
+        if (c <= BP_SLOTS)
+        {
+            const int a = key_body(keys[i]);
+            const int out = base + offsets[i];
+            for (int f = 0; f < c; ++f)
+            {
+                const int m = out + f;
+                F.man.ab[m] = make_int2(a, recorded[(size_t)i * BP_SLOTS + f]);
+                F.man.seq[m] = seqBase + (unsigned long long)(m - base);
+                F.man.n[m] = 0;
+            }
+            active = false;
+        }
+    }
     unsigned checks = 0, hits = 0, cons = 0;
     if (active)
     {
@@ -614,37 +688,22 @@ __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, DevG
     }
 }
 
-// The new pairs recorded by the counting pass, as fresh manifolds at base + offset[i] in hit
-// order (every entry found at most BP_SLOTS).
-__global__ void k_bp_emit_recorded(DevForces F, const unsigned long long *keys, int nBinned, const int *counts,
-                                   const int *offsets, const int *recorded, int base, unsigned long long seqBase)
-{
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nBinned)
-        return;
-    int c = counts[i];
-    if (c <= 0)
-        return;
-    int a = key_body(keys[i]);
-    int out = base + offsets[i];
-    for (int f = 0; f < c && f < BP_SLOTS; ++f)
-    {
-        int m = out + f;
-        F.man.ab[m] = make_int2(a, recorded[(size_t)i * BP_SLOTS + f]);
-        F.man.seq[m] = seqBase + (unsigned long long)(m - base);
-        F.man.n[m] = 0;
-    }
-}
-
 // Large-vs-large pairs of each world (solver.cpp:476-479), tested by the reference serially
 // after all grid pairs. Work item = (world's large base, world's large count, i, chunk); the
 // items are ordered by world, i, chunk, which reproduces each world's serial i < j order.
 template <bool EMIT>
 __global__ void k_bp_large_large(DevForces F, const int *large, const float4 *largeSphere, const int4 *items,
                                  int nItems, int *counts, const int *offsets, int base, unsigned long long seqBase,
-                                 StepCounters *cnt)
+                                 StepCounters *cnt, const StepState *st = nullptr)
 {
     const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (EMIT && st)
+    {
+        if (step_aborted(st))
+            return;
+        base = st->manBase + st->newBinned;
+        seqBase = st->seqBase + (unsigned long long)st->newBinned;
+    }
     const bool active = w < nItems;
     unsigned checks = 0, hits = 0, cons = 0;
     if (active)
@@ -1247,9 +1306,16 @@ AVBD_DEV M3 load_basis(const float4 *b) { return rows(xyz(b[0]), xyz(b[1]), xyz(
 // Manifold::initialize (manifold.cpp:100-174): collide at q-, keep warm-start data of
 // contacts whose feature key persists, C0, lambda/penalty decay.
 template <bool ROUND>
-__global__ void k_manifold_init(DevBodies B, DevManifolds M, int count, Params P, unsigned char *keep)
+__global__ void k_manifold_init(DevBodies B, DevManifolds M, int count, Params P, unsigned char *keep,
+                                const StepState *st = nullptr)
 {
     int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (st)
+    {
+        if (step_aborted(st))
+            return;
+        count = st->nManBp;
+    }
     if (m >= count)
         return;
     int2 ab = M.ab[m];
@@ -1327,10 +1393,10 @@ __global__ void k_manifold_init(DevBodies B, DevManifolds M, int count, Params P
 }
 
 // Joint::initialize (joint.cpp:35-54)
-__global__ void k_joint_init(DevBodies B, DevForces F, Params P, unsigned char *keep)
+__global__ void k_joint_init(DevBodies B, DevForces F, Params P, unsigned char *keep, const StepState *st = nullptr)
 {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= F.nJoint)
+    if (j >= F.nJoint || step_aborted(st))
         return;
     float4 *d = F.joint + 8 * (size_t)j;
     int2 ab = F.jointAB[j];
@@ -1358,11 +1424,23 @@ __global__ void k_joint_init(DevBodies B, DevForces F, Params P, unsigned char *
     keep[j] = d4.w != 0.0f ? 0 : 1;
 }
 
-// Stable compaction of manifolds into the other buffer.
+// Stable compaction of manifolds into the other buffer. With a device step state the count
+// is the state's, and the kernel records the surviving count and the buffer swap there.
 __global__ void k_manifold_compact(DevManifolds src, DevManifolds dst, int count, const unsigned char *keep,
-                                   const int *newIndex)
+                                   const int *newIndex, StepState *st = nullptr)
 {
     int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (st)
+    {
+        if (step_aborted(st))
+            return;
+        count = st->nManBp;
+        if (m == 0)
+        {
+            st->nMan = count > 0 ? newIndex[count - 1] + (keep[count - 1] ? 1 : 0) : 0;
+            st->flips++;
+        }
+    }
     if (m >= count || !keep[m])
         return;
     int d = newIndex[m];
@@ -1455,11 +1533,26 @@ AVBD_DEV unsigned long long incidence_key(int body, unsigned long long seq, int 
     return (b << shift) | (cap - (seq & cap));
 }
 
-// Two incidences per force: manifolds [0, 2M), joints [2M, 2M+2J), springs, ignores.
-__global__ void k_incidences(DevForces F, int shift, int n, unsigned long long *keys, unsigned *vals)
+// Two incidences per force: manifolds [0, 2M), joints [2M, 2M+2J), springs, ignores. With a
+// device step state M is the state's and the launch covers the buffers' capacity: slots
+// past the live incidences get keys of all ones, which sort after every body.
+__global__ void k_incidences(DevForces F, int shift, int n, unsigned long long *keys, unsigned *vals,
+                             const StepState *st = nullptr, int capacity = 0)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
+    // A stopped step writes nothing from here on: the host has already swapped the manifold
+    // buffers for it, so the counts it would read there are not the live ones.
+    if (step_aborted(st))
+        return;
+    if (st)
+        F.nMan = st->nMan;
     int total = 2 * (F.nMan + F.nJoint + F.nSpring + F.nIgnore);
+    if (st && t >= total && t < capacity)
+    {
+        keys[t] = ~0ull;
+        vals[t] = ADJ_NONE;
+        return;
+    }
     if (t >= total)
         return;
     int f = t >> 1;
@@ -1498,10 +1591,11 @@ __global__ void k_incidences(DevForces F, int shift, int n, unsigned long long *
 
 // Segment starts of a sorted key array whose top bits are the segment id (0..n-1, or
 // larger for "no segment"); start[s] for s in [0, n] with gaps filled.
-__global__ void k_segment_starts(const unsigned long long *keys, int total, int shift, int n, int *start)
+__global__ void k_segment_starts(const unsigned long long *keys, int total, int shift, int n, int *start,
+                                 const StepState *st = nullptr)
 {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= total)
+    if (k >= total || step_aborted(st))
         return;
     long long cur = (long long)(keys[k] >> shift);
     if (cur > n)
@@ -1520,21 +1614,62 @@ __global__ void k_segment_starts(const unsigned long long *keys, int total, int 
             start[s] = total;
 }
 
-__global__ void k_copy_adj(const unsigned *vals, unsigned *adj, int total)
+__global__ void k_copy_adj(const unsigned *vals, unsigned *adj, int total, const StepState *st = nullptr)
 {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < total)
+    if (k < total && !step_aborted(st))
         adj[k] = vals[k];
+}
+
+// ---------------------------------------------------------------------------
+// Step admission (device-resident steps): nothing of the world has changed yet, so a step
+// that cannot run as issued stops here and the host redoes it.
+// ---------------------------------------------------------------------------
+
+AVBD_DEV bool finite4(float4 v) { return isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && isfinite(v.w); }
+
+// Every body's pose and velocities must be finite (the reference propagates NaN silently;
+// this step refuses it before touching anything); a joint broken in an earlier step must
+// first leave the joint list (Joint::initialize returns false, solver.cpp:1085-1132), which
+// the host's compaction does. With a step state the kernel stops the step; `seen` (either
+// path) collects STEP_SEEN_* bits for the host.
+constexpr int STEP_SEEN_NONFINITE = 1, STEP_SEEN_BROKEN_JOINT = 2;
+
+__global__ void k_step_begin(DevBodies B, const float4 *joint, int nJoint, StepState *st, int *seen)
+{
+    if (step_aborted(st))
+        return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    bool bad = false, broke = false;
+    if (t < B.n)
+        bad = !finite4(B.pos[t]) || !finite4(B.quat[t]) || !finite4(B.vel[t]) || !finite4(B.angvel[t]);
+    if (t < nJoint)
+        broke = joint[8 * (size_t)t + 4].w != 0.0f;
+    const bool lead = (threadIdx.x & 31) == 0;
+    if (__any_sync(0xFFFFFFFFu, bad) && lead)
+    {
+        if (st)
+            step_abort(st, ABORT_NONFINITE);
+        if (seen)
+            atomicOr(seen, STEP_SEEN_NONFINITE);
+    }
+    if (__any_sync(0xFFFFFFFFu, broke) && lead)
+    {
+        if (st)
+            step_abort(st, ABORT_JOINTS);
+        if (seen)
+            atomicOr(seen, STEP_SEEN_BROKEN_JOINT);
+    }
 }
 
 // ---------------------------------------------------------------------------
 // Body warm start (solver.cpp:1134-1169)
 // ---------------------------------------------------------------------------
 
-__global__ void k_warm_start(DevBodies B, const int *adjStart, Params P)
+__global__ void k_warm_start(DevBodies B, const int *adjStart, Params P, const StepState *st = nullptr)
 {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= B.n)
+    if (b >= B.n || step_aborted(st))
         return;
     float dt = P.dt, g = P.gravity;
     float3 pos = xyz(B.pos[b]);
@@ -1577,10 +1712,10 @@ __global__ void k_warm_start(DevBodies B, const int *adjStart, Params P)
 }
 
 // finishStep velocities (solver.cpp:1275-1287); rolling friction is sphere-only
-__global__ void k_finish(DevBodies B, Params P)
+__global__ void k_finish(DevBodies B, Params P, const StepState *st = nullptr)
 {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= B.n)
+    if (b >= B.n || step_aborted(st))
         return;
     float4 v = B.vel[b];
     B.prevVel[b] = v;
@@ -1602,8 +1737,10 @@ __global__ void k_finish(DevBodies B, Params P)
 // All Jones-Plassmann rounds in one cooperative launch. Priority mode 0: lower list index
 // first, which reproduces the sequential greedy colouring in list order; mode 1: hashed.
 __global__ void k_colour_all(DevBodies B, DevForces F, int n, int mode, int *state, ColourControl *ctl,
-                             StepCounters *cnt)
+                             StepCounters *cnt, unsigned spinLimit, const StepState *st)
 {
+    if (step_aborted(st)) // uniform: every block leaves before the first barrier
+        return;
     const int stride = gridDim.x * blockDim.x;
     int mine = 0;
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += stride)
@@ -1616,7 +1753,7 @@ __global__ void k_colour_all(DevBodies B, DevForces F, int n, int mode, int *sta
     if (threadIdx.x == 0 && bs)
         atomicAdd(&ctl->vertices, bs);
     unsigned target = 0;
-    if (!grid_barrier(ctl, target))
+    if (!grid_barrier(ctl, target, spinLimit))
         return;
     const int total = ((volatile int *)&ctl->vertices)[0];
     int done = 0, round = 0;
@@ -1675,7 +1812,7 @@ __global__ void k_colour_all(DevBodies B, DevForces F, int n, int mode, int *sta
         bs = block_sum(mine);
         if (threadIdx.x == 0 && bs)
             atomicAdd(&ctl->coloured[round], bs);
-        if (!grid_barrier(ctl, target))
+        if (!grid_barrier(ctl, target, spinLimit))
             return;
         done += ((volatile int *)ctl->coloured)[round];
     }
@@ -2024,10 +2161,10 @@ AVBD_DEV int rows_listed(const DevForces &F, unsigned e)
 // Incidences without a body (the world side of an anchored joint) sort after the last body
 // and contribute none.
 __global__ void k_entry_rows(DevForces F, DevBodies B, const unsigned long long *sortedKeys, int total, int shift,
-                             int *count)
+                             int *count, const StepState *st = nullptr)
 {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k > total)
+    if (k > total || step_aborted(st))
         return;
     int r = 0;
     if (k < total)
@@ -2039,10 +2176,11 @@ __global__ void k_entry_rows(DevForces F, DevBodies B, const unsigned long long 
     count[k] = r; // count[total] = 0, so the exclusive scan ends with the row total
 }
 
-__global__ void k_row_starts(const int *adjStart, const int *entryRow, int n, int *rowStart)
+__global__ void k_row_starts(const int *adjStart, const int *entryRow, int n, int *rowStart,
+                             const StepState *st = nullptr)
 {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b <= n)
+    if (b <= n && !step_aborted(st))
         rowStart[b] = entryRow[adjStart[b]];
 }
 
@@ -2080,10 +2218,11 @@ constexpr int ROW_PARTNER_LATER = (int)0x80000000u;
 AVBD_DEV int row_sub(int2 row) { return row.y & 7; }
 AVBD_DEV int row_partner(int2 row) { return ((row.y & (ROW_OWNS_DUAL - 1)) >> 3) - 1; }
 
-__global__ void k_entry_fill(DevForces F, const int *entryRow, const int *count, int total)
+__global__ void k_entry_fill(DevForces F, const int *entryRow, const int *count, int total,
+                             const StepState *st = nullptr)
 {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= total)
+    if (k >= total || step_aborted(st))
         return;
     int out = entryRow[k];
     unsigned e = F.adj[k];
@@ -2212,6 +2351,7 @@ struct IterFlow
     int *done = nullptr;
     int it = 0;
     int *error = nullptr;
+    unsigned spinLimit = 1u << 22; // polls before a partner wait gives up
 };
 
 AVBD_DEV int ld_acquire(const int *p)
@@ -2226,7 +2366,7 @@ AVBD_DEV void st_release(int *p, int v)
     asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-constexpr unsigned FLOW_SPIN_LIMIT = 1u << 22;
+constexpr unsigned FLOW_SPIN_LIMIT = 1u << 22; // default poll limit of a partner wait
 
 // A row reads its partner's pose (and, for a contact the partner owns, the contact's
 // multipliers) as the colour-ordered sweep leaves them: a partner of an earlier colour
@@ -2242,7 +2382,7 @@ AVBD_DEV void wait_partner(const IterFlow &flow, int2 row)
     unsigned spins = 0;
     while (ld_acquire(d) < need)
     {
-        if (++spins >= FLOW_SPIN_LIMIT)
+        if (++spins >= flow.spinLimit)
         {
             atomicExch(flow.error, 1);
             return;
@@ -2500,7 +2640,7 @@ struct IterSync
 // Arrivals count up through the launch (the counter starts at zero): barrier k of the
 // launch releases every block once k x gridDim.x blocks have arrived, so the last block's
 // arrival alone opens it.
-AVBD_DEV bool iter_barrier(IterSync *s, unsigned &target)
+AVBD_DEV bool iter_barrier(IterSync *s, unsigned &target, unsigned spinLimit = ITER_SPIN_LIMIT)
 {
     __shared__ int ok;
     __syncthreads();
@@ -2511,10 +2651,10 @@ AVBD_DEV bool iter_barrier(IterSync *s, unsigned &target)
         atomicAdd(&s->arrive, 1u);
         volatile unsigned *arrive = &s->arrive;
         unsigned spins = 0;
-        while (*arrive < target && ++spins < ITER_SPIN_LIMIT)
+        while (*arrive < target && ++spins < spinLimit)
             if (spins > 256)
                 __nanosleep(32);
-        ok = spins < ITER_SPIN_LIMIT;
+        ok = spins < spinLimit;
         if (!ok)
             atomicExch(&s->error, 1);
         __threadfence();
@@ -2538,8 +2678,16 @@ AVBD_DEV bool iter_barrier(IterSync *s, unsigned &target)
 template <int G, int BLOCK, int SUB, bool ROUND = false>
 __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces F, Params P, const int4 *entries,
                                                          const int *colourStart, int nColours, int iterations,
-                                                         IterSync *sync, int *done)
+                                                         IterSync *sync, int *done, unsigned spinLimit,
+                                                         const StepState *st)
 {
+    if (st)
+    {
+        if (step_aborted(st)) // uniform: every block leaves before the first barrier
+            return;
+        nColours = st->nColours;
+        F.nMan = st->nMan;
+    }
     extern __shared__ __align__(16) unsigned char smemRaw[];
     PrimalShared<G, BLOCK> &sh = *reinterpret_cast<PrimalShared<G, BLOCK> *>(smemRaw);
     constexpr int GPB = BLOCK / G;
@@ -2551,6 +2699,7 @@ __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces 
     IterFlow flow;
     flow.done = barriers ? nullptr : done;
     flow.error = &sync->error;
+    flow.spinLimit = spinLimit;
     for (int it = 0; it < iterations; ++it)
     {
         flow.it = it;
@@ -2570,18 +2719,18 @@ __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces 
                                                          it > 0, sh, flow);
                 unit_sync<SUB, BLOCK>(); // the unit's solve threads are done with the shared systems
             }
-            if (barriers && !iter_barrier(sync, target))
+            if (barriers && !iter_barrier(sync, target, spinLimit))
                 return;
         }
         if (F.nJoint > 0)
         {
             for (long long j = tid; j < F.nJoint; j += stride)
                 dual_joint<true>(B, F, (int)j, P);
-            if (!iter_barrier(sync, target))
+            if (!iter_barrier(sync, target, spinLimit))
                 return;
         }
     }
-    if (!barriers && !iter_barrier(sync, target)) // every body has finished every iteration
+    if (!barriers && !iter_barrier(sync, target, spinLimit)) // every body has finished every iteration
         return;
     // Contacts between two static bodies have no owning row: nothing moves them, so their
     // update of every iteration runs here, one after the other on the same poses.
@@ -2595,6 +2744,251 @@ __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces 
             for (int r = orphan ? iterations : 1; r > 0; --r)
                 dual_contact_slot<true, ROUND>(B, F.man, t, P);
         }
+}
+
+// ---------------------------------------------------------------------------
+// Greedy colouring in list order as one dataflow pass (the default colouring mode)
+// ---------------------------------------------------------------------------
+
+AVBD_DEV unsigned long long ld_acquire_u64(const unsigned long long *p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+AVBD_DEV void st_release_u64(unsigned long long *p, unsigned long long v)
+{
+    asm volatile("st.release.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// With list-index priority the Jones-Plassmann rounds colour a vertex once every
+// lower-index neighbour has its colour, with the smallest colour none of them uses (the
+// sequential greedy colouring in list order, which the oracle restates); its round is one
+// more than the largest round among those neighbours. So each vertex simply waits for its
+// lower-index neighbours: the smallest uncoloured vertex can always proceed (its thread has
+// finished every smaller vertex of its grid-stride sequence and all blocks are resident),
+// so the waits cannot cycle; each is bounded and on expiry records ctl->error and gives up.
+// `state` holds (epoch << 32 | round << 16 | colour) of the vertices coloured in the launch
+// with that epoch, so nothing needs clearing between launches.
+//
+// The same cooperative launch then places the vertices in colour order, ascending body
+// index inside each colour (what sorting (colour, body) keys gives): block b counts the
+// colours of its contiguous share of the bodies, and after a grid barrier every block
+// derives its colours' write positions from all blocks' counts and writes the solve list,
+// the solve entries (body, row range) and each row's dual-owner / later-partner bits.
+constexpr int COLOUR_FLOW_BLOCK = 256;
+
+__global__ void __launch_bounds__(COLOUR_FLOW_BLOCK) k_colour_greedy(
+    DevBodies B, DevForces F, int n, unsigned long long *state, unsigned epoch, int *colour, ColourControl *ctl,
+    StepCounters *cnt, unsigned spinLimit, int *blockCounts, int *colourStart, int *solveList, int4 *entries,
+    const int *rowStart, StepState *st)
+{
+    if (step_aborted(st)) // uniform: every block leaves before the first barrier
+        return;
+    __shared__ int hist[256];
+    __shared__ int running[256];
+    __shared__ int shTotal[256];
+    __shared__ int shC, shVertices;
+    const int stride = gridDim.x * blockDim.x;
+    const int G = gridDim.x;
+    int mine = 0, maxC = -1, maxR = -1;
+    bool failed = false;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n && !failed; v += stride)
+    {
+        const bool vertex = B.massMoment[v].x > 0 && F.adjStart[v + 1] > F.adjStart[v];
+        if (!vertex)
+        {
+            __stcg(&colour[v], -1);
+            continue;
+        }
+        unsigned long long used[4] = {0ull, 0ull, 0ull, 0ull};
+        int round = 0;
+        for (int k = F.adjStart[v]; k < F.adjStart[v + 1] && !failed; ++k)
+        {
+            unsigned e = F.adj[k];
+            if (adj_type(e) == ADJ_IGNORE)
+                continue;
+            int2 ab = force_bodies(F, e);
+            int u = ab.x == v ? ab.y : ab.x;
+            if (u < 0 || u >= v || B.massMoment[u].x <= 0) // static bodies are not vertices
+                continue;
+            // u shares this force, so it is a vertex: wait for its colour of this launch
+            unsigned long long su;
+            unsigned spins = 0;
+            while (((su = ld_acquire_u64(&state[u])) >> 32) != (unsigned long long)epoch)
+            {
+                if (++spins >= spinLimit)
+                {
+                    atomicExch(&ctl->error, 1);
+                    failed = true;
+                    break;
+                }
+                if (spins > 64)
+                {
+                    if (((volatile int *)&ctl->error)[0])
+                    {
+                        failed = true;
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+            }
+            if (failed)
+                break;
+            int cu = (int)(su & 0xFFFFu), ru = (int)((su >> 16) & 0xFFFFu);
+            if (cu < 256)
+                used[cu >> 6] |= 1ull << (cu & 63);
+            round = max(round, ru + 1);
+        }
+        if (failed)
+            break;
+        int c = 0;
+        while (c < 256 && ((used[c >> 6] >> (c & 63)) & 1ull))
+            c++;
+        if (c >= 256)
+        {
+            cnt->error = DERR_TOO_MANY_COLOURS;
+            c = 255;
+        }
+        st_release_u64(&state[v], ((unsigned long long)epoch << 32) | ((unsigned long long)min(round, 0xFFFF) << 16) |
+                                      (unsigned long long)c);
+        __stcg(&colour[v], c);
+        mine++;
+        maxC = max(maxC, c);
+        maxR = max(maxR, round);
+    }
+    // vertices, largest colour and round of the launch
+    {
+        int s = block_sum(mine);
+        if (threadIdx.x == 0 && s)
+            atomicAdd(&ctl->vertices, s);
+        int wc = __reduce_max_sync(0xFFFFFFFFu, maxC + 1) - 1;
+        int wr = __reduce_max_sync(0xFFFFFFFFu, maxR + 1) - 1;
+        if ((threadIdx.x & 31) == 0 && wc >= 0)
+        {
+            atomicMax(&ctl->maxColour, wc);
+            atomicMax(&ctl->rounds, wr + 1);
+        }
+    }
+    unsigned target = 0;
+    auto failing = [&]() {
+        if (blockIdx.x == 0 && threadIdx.x == 0 && st)
+        {
+            st->error = STEP_ERR_COLOURING;
+            st->abort = ABORT_ERROR;
+        }
+    };
+    if (!grid_barrier(ctl, target, spinLimit))
+        return failing();
+    // counts per colour of this block's share of the bodies
+    const int chunk = (n + G - 1) / G;
+    const int b0 = min(n, blockIdx.x * chunk), b1 = min(n, b0 + chunk);
+    if (threadIdx.x == 0)
+    {
+        shVertices = ((volatile int *)&ctl->vertices)[0];
+        shC = shVertices > 0 ? ((volatile int *)&ctl->maxColour)[0] + 1 : 0;
+    }
+    for (int c = threadIdx.x; c < 256; c += blockDim.x)
+        hist[c] = 0;
+    __syncthreads();
+    const int C = shC;
+    for (int v = b0 + threadIdx.x; v < b1; v += blockDim.x)
+    {
+        int c = __ldcg(&colour[v]);
+        if (c >= 0)
+            atomicAdd(&hist[c], 1);
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < C; c += blockDim.x)
+        __stcg(&blockCounts[(size_t)c * G + blockIdx.x], hist[c]);
+    if (!grid_barrier(ctl, target, spinLimit))
+        return failing();
+    // each colour's total and this block's first position inside the colour
+    for (int c = threadIdx.x; c < C; c += blockDim.x)
+    {
+        int before = 0, total = 0;
+        for (int b = 0; b < G; ++b)
+        {
+            int k = __ldcg(&blockCounts[(size_t)c * G + b]);
+            total += k;
+            before += b < (int)blockIdx.x ? k : 0;
+        }
+        shTotal[c] = total;
+        running[c] = before;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        int acc = 0;
+        for (int c = 0; c < C; ++c)
+        {
+            int t = shTotal[c];
+            shTotal[c] = acc; // now the colour's start
+            acc += t;
+        }
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < C; c += blockDim.x)
+        running[c] += shTotal[c];
+    if (blockIdx.x == 0)
+    {
+        for (int c = threadIdx.x; c < C; c += blockDim.x)
+            colourStart[c] = shTotal[c];
+        if (threadIdx.x == 0)
+            colourStart[C] = shVertices;
+    }
+    __syncthreads();
+    // stable placement: tiles of the block's share, warps in order inside a tile
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int base = b0; base < b1; base += blockDim.x)
+    {
+        const int v = base + threadIdx.x;
+        const int c = v < b1 ? __ldcg(&colour[v]) : -1;
+        const unsigned same = __match_any_sync(0xFFFFFFFFu, c);
+        const int rank = __popc(same & lt);
+        const bool leader = (same & lt) == 0;
+        for (int w = 0; w < COLOUR_FLOW_BLOCK / 32; ++w)
+        {
+            if (warp == w && c >= 0)
+            {
+                const int pos = running[c] + rank;
+                __syncwarp(same);
+                if (leader)
+                    running[c] += __popc(same);
+                solveList[pos] = v;
+                const int r0 = rowStart[v], r1 = rowStart[v + 1];
+                entries[pos] = make_int4(v, r0, r1, 0);
+                // the contact rows whose dual update this body owns in the fused pass
+                for (int r = r0; r < r1; ++r)
+                {
+                    int2 row = F.rows[r];
+                    const int p = row_partner(row);
+                    const int cp = p >= 0 ? __ldcg(&colour[p]) : -1;
+                    const bool own = p < 0 || cp < 0 || c < cp;
+                    const bool later = p >= 0 && cp >= 0 && c < cp;
+                    row.y = own ? (row.y | ROW_OWNS_DUAL) : (row.y & ~ROW_OWNS_DUAL);
+                    row.y = later ? (row.y | ROW_PARTNER_LATER) : (row.y & ~ROW_PARTNER_LATER);
+                    F.rows[r] = row;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && st)
+    {
+        int err = ctl->error ? STEP_ERR_COLOURING
+                             : (cnt->error == DERR_TOO_MANY_COLOURS ? STEP_ERR_COLOURS : STEP_ERR_NONE);
+        st->nColours = C;
+        st->nSolve = shVertices;
+        st->rounds = ctl->rounds;
+        if (err != STEP_ERR_NONE)
+        {
+            st->error = err;
+            st->abort = ABORT_ERROR;
+        }
+    }
 }
 
 } // namespace avbd

@@ -663,10 +663,10 @@ AVBD_DEV float3 contact_offset(const BodyShape &s, float4 q, float3 lo, const M3
 
 // applySphereRollingFriction (solver.cpp:628-662) for every manifold of a dynamic sphere, in
 // the solver's force order (the body's list, newest first), after the velocity update.
-__global__ void k_rolling_friction(DevBodies B, DevForces F, const int *adjStart)
+__global__ void k_rolling_friction(DevBodies B, DevForces F, const int *adjStart, const StepState *st = nullptr)
 {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= B.n || !B.shape)
+    if (b >= B.n || !B.shape || step_aborted(st))
         return;
     BodyShape s = body_shape(B, b);
     if (s.type != SHAPE_SPHERE || B.massMoment[b].x <= 0.0f)

@@ -446,6 +446,32 @@ class World:
         """0 = greedy colouring in list order (default), 1 = hashed priorities."""
         self._check(self.lib.avbd_set_colouring(self.h, mode), "avbd_set_colouring")
 
+    STEP_DEVICE, STEP_HOST = 0, 1
+
+    def set_step_mode(self, mode: int):
+        """STEP_DEVICE (default): a step keeps its counts on the device and never waits for
+        it; STEP_HOST: the host reads the counts each step needs. Both give the same bits."""
+        self._check(self.lib.avbd_set_step_mode(self.h, mode), "avbd_set_step_mode")
+
+    def set_manifold_headroom(self, spare: int):
+        """Manifold room beyond the live count for device-resident steps (0 = default)."""
+        self._check(self.lib.avbd_set_manifold_headroom(self.h, int(spare)), "avbd_set_manifold_headroom")
+
+    def set_wait_limits(self, colouring_polls: int = 0, iteration_polls: int = 0):
+        """Poll limits of the bounded waits (0 = defaults)."""
+        self._check(self.lib.avbd_set_wait_limits(self.h, colouring_polls, iteration_polls),
+                    "avbd_set_wait_limits")
+
+    def clear_error(self):
+        self.lib.avbd_clear_error(self.h)
+
+    def last_error(self) -> str:
+        return self.lib.avbd_last_error(self.h).decode(errors="replace")
+
+    def reload(self):
+        """Load the world's scenes again (a fresh start in the same context)."""
+        self._load(self.scenes)
+
     # -- differentiable step
     def adjoint_forward(self, steps: int, checkpoint_every: int = 10, sync: bool = True):
         """Step like step(steps), keeping a state snapshot every checkpoint_every steps for

@@ -52,6 +52,10 @@ extern "C" {
 #define AVBD_ITERATIONS_PER_COLOUR 0 /* one launch per colour and iteration, then the dual sweep */
 #define AVBD_ITERATIONS_PERSISTENT 1 /* all iterations in one cooperative launch (default) */
 
+/* How a step is issued (avbd_set_step_mode). */
+#define AVBD_STEP_DEVICE 0 /* counts stay on the device; no host wait inside a step (default) */
+#define AVBD_STEP_HOST 1   /* the host reads the counts it needs at three points of each step */
+
 #define AVBD_FORCE_MANIFOLD 0
 #define AVBD_FORCE_JOINT 1
 #define AVBD_FORCE_SPRING 2
@@ -196,6 +200,8 @@ typedef struct AvbdStats
     int64_t colour_rounds;
     int64_t primal_rows;
     int64_t grid_rescaled; /* 1 if the grid hit the reference's 2^22-cell cap this step */
+    int64_t device_steps;  /* steps issued without a host wait (since the world was loaded) */
+    int64_t redone_steps;  /* of those, steps the host redid synchronously (see avbd_step) */
     float step_ms;
 } AvbdStats;
 
@@ -235,14 +241,37 @@ int avbd_load_batch(AvbdContext *ctx, int32_t num_worlds, const int32_t *world_s
 int avbd_write_bodies(AvbdContext *ctx, const AvbdBodies *bodies);
 
 /* Solver::step() for nsteps steps (solver.cpp:934-937 via stepCpuReference 1036-1041).
- * Asynchronous on the context stream; returns after launch except where the step
- * needs a device count (buffer growth). Every wait inside a step's kernels is bounded:
- * if one expires (a grid barrier, or a row waiting for its partner body's iteration
- * count), the step reports AVBD_ERR_STATE at its next host check and the context
- * latches the error. */
+ * Asynchronous on the context stream. In AVBD_STEP_DEVICE mode (the default, for the grid
+ * broadphase with the single-launch iterations) a step keeps every count it needs on the
+ * device and returns as soon as its launches are issued. A step that cannot run as issued
+ * stops on the device before it changes anything, and so does every step issued after
+ * it: new pairs that do not fit the manifold buffers, a grid that needs the reference's
+ * cell-count cap (rescaled with the host's cbrtf), a joint broken in an earlier step (its
+ * removal is compacted on the host). The next call that waits for the device (a read,
+ * avbd_synchronize, avbd_get_stats, an edit) redoes those steps synchronously, so results
+ * are always the same bits. In AVBD_STEP_HOST mode every step reads its counts on the host.
+ * Errors of a step surface at the next call that waits for the device and latch:
+ * AVBD_ERR_STATE when a bounded wait expires (a grid barrier, a row waiting for its
+ * partner body's iteration count, the colouring's barrier) and when a body's position,
+ * orientation or velocity is not finite at the start of a step (the step refuses it and
+ * leaves the world as it was). */
 int avbd_step(AvbdContext *ctx, int32_t nsteps);
-/* Wait for the context stream. */
+/* Wait for the context stream (and redo or report any device-resident step, as above). */
 int avbd_synchronize(AvbdContext *ctx);
+
+/* AVBD_STEP_DEVICE (default) or AVBD_STEP_HOST, for later steps; both give the same bits.
+ * No counterpart in the reference (its CPU step has no device). */
+int avbd_set_step_mode(AvbdContext *ctx, int32_t mode);
+/* Manifold room kept beyond the live count for device-resident steps: spare = 0 restores
+ * the default (twice the live count, and at least half the body count more); a small spare
+ * makes steps that create many pairs stop on the device and be redone on the host. */
+int avbd_set_manifold_headroom(AvbdContext *ctx, int64_t spare);
+/* Poll limits of the bounded waits: the colouring's grid barrier and the iteration
+ * kernel's grid barriers and partner waits (0 = the defaults, 2^24 and 2^22 polls). A wait
+ * that reaches its limit makes the step fail with AVBD_ERR_STATE, as described at
+ * avbd_step; the context stays usable after avbd_clear_error and a reload. No counterpart
+ * in the reference (its CPU solver never waits). */
+int avbd_set_wait_limits(AvbdContext *ctx, uint32_t colouring_polls, uint32_t iteration_polls);
 
 /* Solver::benchmarkBroadphaseOnly (solver.cpp:989-1034), the reference's collision-only
  * benchmark step (headless_server.cpp:664-690): every manifold is deleted and the selected

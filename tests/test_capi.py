@@ -51,7 +51,7 @@ def test_struct_sizes_match_header_layout():
     # plain C layouts: int32 count + pointers, all 8-byte aligned on x86-64
     assert ctypes.sizeof(_lib.AvbdBodies) == 8 + 13 * 8
     assert ctypes.sizeof(_lib.AvbdParams) == 32
-    assert ctypes.sizeof(_lib.AvbdStats) == 14 * 8 + 8
+    assert ctypes.sizeof(_lib.AvbdStats) == 16 * 8 + 8
 
 
 def test_host_derived_properties_match_oracle():

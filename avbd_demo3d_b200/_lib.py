@@ -64,6 +64,11 @@ class AvbdJointsOut(ctypes.Structure):
     _fields_ = [(k, ctypes.c_void_p) for k in ("body_ab2", "seq", "state28", "broken")]
 
 
+class AvbdExternalContacts(ctypes.Structure):
+    _fields_ = [("count", ctypes.c_int32)] + [(k, ctypes.c_void_p) for k in (
+        "body_ab2", "num_contacts", "basis9", "keys8", "contact15x8", "stick8", "creates")]
+
+
 class AvbdStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_int64) for k in (
         "body_count", "pair_checks", "sphere_hits", "constrained_hits", "manifolds_created", "manifold_count",
@@ -103,6 +108,8 @@ SIGNATURES = {
     "avbd_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     "avbd_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "avbd_set_step_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    "avbd_step_external": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, c_int_p,
+                                          ctypes.POINTER(AvbdExternalContacts)]),
     "avbd_set_manifold_headroom": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64]),
     "avbd_set_wait_limits": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32]),
     "avbd_broadphase_only": (ctypes.c_int, [ctypes.c_void_p]),

@@ -218,6 +218,17 @@ struct AvbdContext
     long long manifoldSpare = 0;   // manifold room beyond the live count (0: the default policy)
     long long deviceSteps = 0, redoneSteps = 0;
     unsigned waitColour = 0, waitIteration = 0; // poll limits of the bounded waits (0: default)
+
+    // One step with caller-given pairs (and contacts) in place of the broadphase
+    // (stepCpuReferenceWithExternalBroadphase): set by avbd_step_external for that step only.
+    bool external = false;
+    std::vector<int2> hExtPairs, hExtEntryPairs; // valid pairs; contact entries that may create
+    DArr<int2> extPairs;
+    DArr<unsigned char> extFlags;
+    DArr<unsigned long long> extKeys;
+    DArr<int> extEntry, extNum;
+    DArr<float4> extBasis, extContact;
+    int extKeyCount = 0;
 };
 
 namespace
@@ -1049,6 +1060,98 @@ int init_forces_device(AvbdContext *ctx)
     return AVBD_OK;
 }
 
+ExternalContacts external_contacts(AvbdContext *ctx)
+{
+    ExternalContacts E;
+    if (ctx->external && ctx->extKeyCount > 0)
+    {
+        E.count = ctx->extKeyCount;
+        E.keys = ctx->extKeys.p;
+        E.entry = ctx->extEntry.p;
+        E.num = ctx->extNum.p;
+        E.basis = ctx->extBasis.p;
+        E.contact = ctx->extContact.p;
+    }
+    return E;
+}
+
+// broadphaseExternalPairs (solver.cpp:579-626) for the step avbd_step_external issues: the
+// device tests each given pair's bounding spheres and existing forces; the host walks the
+// pairs, then the contact entries, in the caller's order (a pair made earlier in the list
+// constrains a later duplicate) and the kept ones become new manifolds in that order.
+int external_broadphase(AvbdContext *ctx)
+{
+    const int np = (int)ctx->hExtPairs.size(), ne = (int)ctx->hExtEntryPairs.size();
+    const int total = np + ne;
+    StepCounters c{};
+    std::vector<int2> made;
+    if (total > 0)
+    {
+        std::vector<int2> all(ctx->hExtPairs);
+        all.insert(all.end(), ctx->hExtEntryPairs.begin(), ctx->hExtEntryPairs.end());
+        CHECK(reserve(ctx, ctx->extPairs, (size_t)total, false));
+        CHECK(reserve(ctx, ctx->extFlags, (size_t)total, false));
+        CU(cudaMemcpyAsync(ctx->extPairs.p, all.data(), sizeof(int2) * total, cudaMemcpyHostToDevice, ctx->stream));
+        DevBodies B = dev_bodies(ctx);
+        DevForces F = dev_forces(ctx);
+        if (np)
+        {
+            k_external_classify<<<grid_for(np, 128), 128, 0, ctx->stream>>>(B, F, ctx->extPairs.p, np, 1,
+                                                                             ctx->extFlags.p);
+            LAUNCHED();
+        }
+        if (ne)
+        {
+            k_external_classify<<<grid_for(ne, 128), 128, 0, ctx->stream>>>(B, F, ctx->extPairs.p + np, ne, 0,
+                                                                             ctx->extFlags.p + np);
+            LAUNCHED();
+        }
+        std::vector<unsigned char> flags((size_t)total);
+        CU(cudaMemcpyAsync(flags.data(), ctx->extFlags.p, (size_t)total, cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+        std::vector<unsigned long long> linked; // unordered pairs given a manifold in this pass
+        auto key = [](int2 p) {
+            unsigned lo = (unsigned)std::min(p.x, p.y), hi = (unsigned)std::max(p.x, p.y);
+            return ((unsigned long long)lo << 32) | hi;
+        };
+        auto made_already = [&](unsigned long long k) {
+            return std::find(linked.begin(), linked.end(), k) != linked.end();
+        };
+        for (int k = 0; k < total; ++k)
+        {
+            c.pairChecks++;
+            if (!(flags[k] & 1))
+                continue;
+            c.sphereHits++;
+            unsigned long long pk = key(all[k]);
+            if ((flags[k] & 2) || made_already(pk))
+            {
+                c.constrainedHits++;
+                continue;
+            }
+            made.push_back(all[k]);
+            linked.push_back(pk);
+        }
+    }
+    const int M0 = ctx->nMan, P = (int)made.size();
+    if (P)
+    {
+        CHECK(reserve_manifolds(ctx, ctx->man[ctx->cur], (size_t)(M0 + P), (size_t)M0));
+        CHECK(reserve(ctx, ctx->extPairs, (size_t)P, false));
+        CU(cudaMemcpyAsync(ctx->extPairs.p, made.data(), sizeof(int2) * P, cudaMemcpyHostToDevice, ctx->stream));
+        k_external_emit<<<grid_for(P, 128), 128, 0, ctx->stream>>>(dev_man(ctx->man[ctx->cur]), ctx->extPairs.p, P, M0,
+                                                                   (unsigned long long)ctx->nextSeq);
+        LAUNCHED();
+    }
+    // the step's counters, where the synchronous step reads them
+    CU(cudaMemcpyAsync(ctx->counters.p, &c, sizeof(StepCounters), cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream)); // c and made live on this stack frame
+    ctx->stats.manifolds_created = P;
+    ctx->nMan = M0 + P;
+    ctx->nextSeq += P;
+    return AVBD_OK;
+}
+
 int init_forces(AvbdContext *ctx)
 {
     DevBodies B = dev_bodies(ctx);
@@ -1063,10 +1166,11 @@ int init_forces(AvbdContext *ctx)
     if (M)
     {
         DevManifolds Md = dev_man(ctx->man[ctx->cur]);
+        const ExternalContacts E = external_contacts(ctx);
         if (ctx->hasShapes)
-            k_manifold_init<true><<<grid_for(M, 128), 128, 0, ctx->stream>>>(B, Md, M, P, ctx->keep.p);
+            k_manifold_init<true><<<grid_for(M, 128), 128, 0, ctx->stream>>>(B, Md, M, P, ctx->keep.p, nullptr, E);
         else
-            k_manifold_init<false><<<grid_for(M, 128), 128, 0, ctx->stream>>>(B, Md, M, P, ctx->keep.p);
+            k_manifold_init<false><<<grid_for(M, 128), 128, 0, ctx->stream>>>(B, Md, M, P, ctx->keep.p, nullptr, E);
         LAUNCHED();
         k_u8_to_int<<<grid_for(M, 256), 256, 0, ctx->stream>>>(ctx->keep.p, cnt32, M);
         LAUNCHED();
@@ -1329,7 +1433,7 @@ int step_once(AvbdContext *ctx)
     ctx->stats.grid_rescaled = 0;
     {
         PhaseScope ps(ctx, AVBD_PHASE_BROADPHASE);
-        CHECK(broadphase(ctx));
+        CHECK(ctx->external ? external_broadphase(ctx) : broadphase(ctx));
     }
     {
         PhaseScope ps(ctx, AVBD_PHASE_FORCE_INIT);
@@ -2322,6 +2426,103 @@ int avbd_step(AvbdContext *ctx, int32_t nsteps)
         }
     }
     return AVBD_OK;
+}
+
+int avbd_step_external(AvbdContext *ctx, int32_t num_pairs, const int32_t *pairs_ab2,
+                       const AvbdExternalContacts *contacts)
+{
+    if (!ctx)
+        return AVBD_ERR_ARGUMENT;
+    if (ctx->errCode)
+        return AVBD_ERR_LATCHED;
+    if (!ctx->loaded)
+        return fail(ctx, AVBD_ERR_STATE, "no world loaded");
+    if (num_pairs < 0 || (num_pairs > 0 && !pairs_ab2))
+        return fail(ctx, AVBD_ERR_ARGUMENT, "pairs: negative count or null array");
+    const int ne = contacts ? contacts->count : 0;
+    if (ne < 0 || (ne > 0 && (!contacts->body_ab2 || !contacts->num_contacts || !contacts->basis9 ||
+                              !contacts->keys8 || !contacts->contact15x8 || !contacts->stick8)))
+        return fail(ctx, AVBD_ERR_ARGUMENT, "external contacts: negative count or null array");
+    SETTLED();
+    adjoint_invalidate(ctx);
+    CU(cudaSetDevice(ctx->device));
+    const int n = ctx->n;
+    auto world = [&](int b) {
+        return (int)(std::upper_bound(ctx->hWorldStart.begin(), ctx->hWorldStart.end(), b) - ctx->hWorldStart.begin());
+    };
+    auto valid = [&](int a, int b) { return a >= 0 && b >= 0 && a < n && b < n && a != b && world(a) == world(b); };
+    // pairs naming a body twice, no body or bodies of two worlds are skipped, as the reference
+    // skips invalid ids (solver.cpp:584-593)
+    ctx->hExtPairs.clear();
+    for (int k = 0; k < num_pairs; ++k)
+        if (valid(pairs_ab2[2 * k], pairs_ab2[2 * k + 1]))
+            ctx->hExtPairs.push_back(make_int2(pairs_ab2[2 * k], pairs_ab2[2 * k + 1]));
+    // contact entries: every valid one replaces the narrowphase of its pair (the last entry
+    // for an ordered pair wins); each may also create its pair's manifold (solver.cpp:597-622)
+    ctx->hExtEntryPairs.clear();
+    std::vector<std::pair<unsigned long long, int>> keyed;
+    std::vector<int> num;
+    std::vector<float4> basis, rec;
+    for (int e = 0; e < ne; ++e)
+    {
+        int a = contacts->body_ab2[2 * e], b = contacts->body_ab2[2 * e + 1];
+        if (!valid(a, b))
+            continue;
+        const int slot = (int)num.size();
+        if (!contacts->creates || contacts->creates[e])
+            ctx->hExtEntryPairs.push_back(make_int2(a, b));
+        keyed.push_back({((unsigned long long)(unsigned)a << 32) | (unsigned)b, slot});
+        int nc = std::min(std::max(contacts->num_contacts[e], 0), 8);
+        num.push_back(nc);
+        const float *bs = contacts->basis9 + 9 * (size_t)e;
+        for (int r = 0; r < 3; ++r)
+            basis.push_back(make_float4(bs[3 * r], bs[3 * r + 1], bs[3 * r + 2], 0.0f));
+        for (int i = 0; i < 8; ++i)
+        {
+            const float *c = contacts->contact15x8 + (8 * (size_t)e + i) * 15; // rA rB C0 penalty lambda
+            unsigned key = (unsigned)contacts->keys8[8 * (size_t)e + i];
+            unsigned stick = contacts->stick8[8 * (size_t)e + i] ? 0x80000000u : 0u;
+            rec.push_back(make_float4(c[0], c[1], c[2], c[3]));
+            rec.push_back(make_float4(c[4], c[5], c[6], c[7]));
+            rec.push_back(make_float4(c[8], c[9], c[10], c[11]));
+            unsigned word = (key & 0x7FFFFFFFu) | stick;
+            float last;
+            memcpy(&last, &word, sizeof(last));
+            rec.push_back(make_float4(c[12], c[13], c[14], last));
+        }
+    }
+    // ordered keys, ascending; for a repeated key the later entry is kept
+    std::stable_sort(keyed.begin(), keyed.end(),
+                     [](const std::pair<unsigned long long, int> &x, const std::pair<unsigned long long, int> &y) {
+                         return x.first < y.first;
+                     });
+    std::vector<unsigned long long> keys;
+    std::vector<int> entry;
+    for (size_t k = 0; k < keyed.size(); ++k)
+    {
+        if (k + 1 < keyed.size() && keyed[k + 1].first == keyed[k].first)
+            continue;
+        keys.push_back(keyed[k].first);
+        entry.push_back(keyed[k].second);
+    }
+    ctx->extKeyCount = (int)keys.size();
+    if (ctx->extKeyCount)
+    {
+        CHECK(upload(ctx, ctx->extKeys, keys.data(), keys.size()));
+        CHECK(upload(ctx, ctx->extEntry, entry.data(), entry.size()));
+        CHECK(upload(ctx, ctx->extNum, num.data(), num.size()));
+        CHECK(upload(ctx, ctx->extBasis, basis.data(), basis.size()));
+        CHECK(upload(ctx, ctx->extContact, rec.data(), rec.size()));
+    }
+    ctx->external = true;
+    int rc = step_once(ctx);
+    ctx->external = false;
+    ctx->extKeyCount = 0;
+    ctx->stateDirty = true;
+    if (rc == AVBD_OK)
+        rc = (cudaStreamSynchronize(ctx->stream) == cudaSuccess) ? AVBD_OK
+                                                                  : fail(ctx, AVBD_ERR_CUDA, "external step failed");
+    return rc;
 }
 
 int avbd_set_step_mode(AvbdContext *ctx, int32_t mode)

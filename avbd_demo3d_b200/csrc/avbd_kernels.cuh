@@ -750,6 +750,40 @@ __global__ void k_bp_large_large(DevForces F, const int *large, const float4 *la
     }
 }
 
+// Pairs a caller injects in place of the broadphase (broadphaseExternalPairs,
+// solver.cpp:579-626), classified against the forces that exist before the step: bit 0 the
+// bounding spheres overlap (generatePair's test, solver.cpp:165-174; contact entries skip
+// it), bit 1 an existing force already links the bodies (Rigid::constrainedTo). The host
+// then applies them in list order, where an earlier pair of the list also constrains a
+// later one.
+__global__ void k_external_classify(DevBodies B, DevForces F, const int2 *pairs, int count, int sphereTest,
+                                    unsigned char *flags)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count)
+        return;
+    int2 p = pairs[k];
+    bool hit = true;
+    if (sphereTest)
+    {
+        float3 dp = sub(xyz(B.pos[p.x]), xyz(B.pos[p.y]));
+        float r = B.sizeRad[p.x].w + B.sizeRad[p.y].w;
+        hit = dot(dp, dp) <= r * r;
+    }
+    flags[k] = (hit ? 1 : 0) | ((hit && constrained(F, p.x, p.y)) ? 2 : 0);
+}
+
+// New manifolds for the injected pairs that the host kept, in its order.
+__global__ void k_external_emit(DevManifolds M, const int2 *pairs, int count, int base, unsigned long long seqBase)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count)
+        return;
+    M.ab[base + k] = pairs[k];
+    M.seq[base + k] = seqBase + (unsigned long long)k;
+    M.n[base + k] = 0;
+}
+
 // All-pairs broadphase (solver.cpp:176-185): thread per body a, pairs (a, b > a) of its world.
 // ---------------------------------------------------------------------------
 // Sweep and prune (broadphaseSweepAndPrune, solver.cpp:488-577), one sweep per world.
@@ -1303,11 +1337,47 @@ AVBD_DEV M3 load_basis(const float4 *b) { return rows(xyz(b[0]), xyz(b[1]), xyz(
 
 #include "avbd_round.cuh"
 
-// Manifold::initialize (manifold.cpp:100-174): collide at q-, keep warm-start data of
-// contacts whose feature key persists, C0, lambda/penalty decay.
+// Contacts a caller injects for one step (ExternalManifoldContact, solver.h:336-344): ordered
+// body-pair keys (a << 32 | b, ascending; the last entry given for a key wins, as the
+// reference's map assignment does) with each entry's contacts in the manifold layout.
+struct ExternalContacts
+{
+    int count = 0;
+    const unsigned long long *keys = nullptr;
+    const int *entry = nullptr;
+    const int *num = nullptr;       // per entry, at most 8 used
+    const float4 *basis = nullptr;  // 3 per entry
+    const float4 *contact = nullptr; // 32 per entry
+};
+
+AVBD_DEV int ext_find(const ExternalContacts &E, unsigned long long key)
+{
+    int lo = 0, hi = E.count;
+    while (lo < hi)
+    {
+        int mid = (lo + hi) >> 1;
+        if (E.keys[mid] < key)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo < E.count && E.keys[lo] == key ? E.entry[lo] : -1;
+}
+
+// Solver::findExternalManifoldContact (solver.cpp:975-985): (A, B) first, then (B, A).
+AVBD_DEV int ext_lookup(const ExternalContacts &E, int a, int b)
+{
+    int e = ext_find(E, ((unsigned long long)(unsigned)a << 32) | (unsigned)b);
+    return e >= 0 ? e : ext_find(E, ((unsigned long long)(unsigned)b << 32) | (unsigned)a);
+}
+
+// Manifold::initialize (manifold.cpp:100-174): collide at q- (or take the contacts injected
+// for the pair, manifold.cpp:110-117, whole records: their penalty, multipliers and stick
+// state seed the new contacts), keep warm-start data of contacts whose feature key
+// persists, C0, lambda/penalty decay.
 template <bool ROUND>
 __global__ void k_manifold_init(DevBodies B, DevManifolds M, int count, Params P, unsigned char *keep,
-                                const StepState *st = nullptr)
+                                const StepState *st = nullptr, ExternalContacts E = ExternalContacts())
 {
     int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (st)
@@ -1336,21 +1406,38 @@ __global__ void k_manifold_init(DevBodies B, DevManifolds M, int count, Params P
         nc[i].rB = f3(0, 0, 0);
     }
     M3 basis = load_basis(M.basis + 3 * m);
-    int nn = round ? collide_shapes(A, Bb, P.dt, nc, basis)
-                   : collide_boxes(pA, qA, A.size, pB, qB, Bb.size, nc, basis);
+    const int ext = E.count ? ext_lookup(E, ab.x, ab.y) : -1;
+    int nn;
+    if (ext >= 0)
+    {
+        basis = load_basis(E.basis + 3 * (size_t)ext);
+        nn = min(max(E.num[ext], 0), 8);
+    }
+    else
+        nn = round ? collide_shapes(A, Bb, P.dt, nc, basis) : collide_boxes(pA, qA, A.size, pB, qB, Bb.size, nc, basis);
     int nOld = M.n[m];
     float4 *cbase = M.contact + (size_t)m * 32;
     ContactRec merged[8];
     for (int i = 0; i < nn; ++i)
     {
         ContactRec r;
-        r.key = nc[i].key;
-        r.rA = nc[i].rA;
-        r.rB = nc[i].rB;
-        r.C0 = f3(0, 0, 0);
-        r.pen = f3(0, 0, 0);
-        r.lam = f3(0, 0, 0);
-        r.stick = false;
+        if (ext >= 0)
+        {
+            r = load_contact(E.contact + 32 * (size_t)ext + 4 * i);
+            nc[i].key = r.key;
+            nc[i].rA = r.rA;
+            nc[i].rB = r.rB;
+        }
+        else
+        {
+            r.key = nc[i].key;
+            r.rA = nc[i].rA;
+            r.rB = nc[i].rB;
+            r.C0 = f3(0, 0, 0);
+            r.pen = f3(0, 0, 0);
+            r.lam = f3(0, 0, 0);
+            r.stick = false;
+        }
         for (int j = 0; j < nOld; ++j)
         {
             ContactRec o = load_contact(cbase + 4 * j);

@@ -258,6 +258,25 @@ class World:
         if sync:
             self.synchronize()
 
+    def step_external(self, pairs, contacts: dict | None = None):
+        """One step with the broadphase replaced by `pairs` ((k, 2) list indices) and, for the
+        pairs of `contacts` (dict of ab (e, 2), n (e,), basis (e, 9), keys (e, 8),
+        contact (e, 8, 15), stick (e, 8), optional creates (e,)), the narrowphase replaced by
+        the given contacts (Solver::stepCpuReferenceWithExternalBroadphase)."""
+        pairs = _c(np.asarray(pairs, np.int32).reshape(-1, 2), np.int32)
+        ext = None
+        if contacts is not None:
+            arr = {k: _c(contacts[k], dt) for k, dt in (("ab", np.int32), ("n", np.int32), ("basis", F32),
+                                                        ("keys", np.int32), ("contact", F32), ("stick", np.int32))}
+            cr = contacts.get("creates")
+            arr["creates"] = None if cr is None else _c(cr, np.int32)
+            self._ext_keep = arr
+            ext = _lib.AvbdExternalContacts(len(arr["n"]), *[_ptr(arr[k]) for k in (
+                "ab", "n", "basis", "keys", "contact", "stick", "creates")])
+        rc = self.lib.avbd_step_external(self.h, len(pairs), pairs.ctypes.data_as(_lib.c_int_p),
+                                         ctypes.byref(ext) if ext is not None else None)
+        self._check(rc, "avbd_step_external")
+
     def broadphase_only(self):
         """The reference's collision-only step: drop every manifold, run the broadphase alone."""
         self._check(self.lib.avbd_broadphase_only(self.h), "avbd_broadphase_only")

@@ -49,17 +49,38 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic_per_launch(kernel: str = "k_primal"):
-    """dram bytes per launch of `kernel` from its committed ncu summary, if present."""
-    name = {"k_primal": "primal_stacks65k_ncu.md", "k_iterations": "iterations_stacks65k_ncu.md"}[kernel]
-    path = os.path.join(ROOT, "profiles", name)
-    try:
-        for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
-                return float(line.split(":", 1)[1])
-    except OSError:
-        pass
-    return None
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one ncu capture
+# of the kernel on this workload, with the capture's summary file and date and a digest of
+# the kernel's source files at capture time: when the sources have changed since, the
+# figure no longer describes the kernel and the line reports no traffic.
+NCU_TRAFFIC = {
+    "k_iterations": {"bytes_per_launch": 31094528, "summary": "profiles/iterations_stacks65k_ncu.txt",
+                     "captured": "2026-12-04", "sources_sha": ""},
+    "k_primal": {"bytes_per_launch": None, "summary": "profiles/primal_stacks65k_ncu.txt",
+                 "captured": "2026-12-04", "sources_sha": ""},
+}
+KERNEL_SOURCES = ("avbd_demo3d_b200/csrc/avbd_kernels.cuh", "avbd_demo3d_b200/csrc/avbd_math.cuh",
+                  "avbd_demo3d_b200/csrc/avbd_round.cuh", "avbd_demo3d_b200/csrc/avbd_colour.cuh")
+
+
+def kernel_sources_sha() -> str:
+    import hashlib
+
+    h = hashlib.sha256()
+    for f in KERNEL_SOURCES:
+        with open(os.path.join(ROOT, f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
+def ncu_traffic(kernel: str):
+    """(bytes per launch or None, provenance) of the kernel's recorded ncu capture."""
+    rec = NCU_TRAFFIC.get(kernel)
+    if not rec:
+        return None, None
+    current = rec["sources_sha"] == kernel_sources_sha()
+    prov = {"summary": rec["summary"], "captured": rec["captured"], "matches_current_source": current}
+    return (rec["bytes_per_launch"] if current else None), prov
 
 
 class ClockSampler:
@@ -187,17 +208,27 @@ def run_cuda(args):
     primal_launches = max(1, prof["primal_spans"])
     achieved = per_iter * iters * prof["steps"] / (primal_ms / 1e3) / 1e9 if primal_ms > 0 else None
     peak, peak_kind = measured_peak()
-    traffic = ncu_traffic_per_launch("k_iterations" if persistent else "k_primal")
+    traffic, traffic_source = ncu_traffic("k_iterations" if persistent else "k_primal")
     kernel = ("k_iterations (every iteration of a step: coloured primal sweeps, contact dual updates fused into "
               "the rows, joint dual updates)" if persistent else "k_primal (coloured primal sweep, one launch per "
               "colour)")
     roofline = {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "traffic_source": traffic_source,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                 "algorithmic_bytes_per_launch": per_iter * iters * prof["steps"] / primal_launches,
                 "avg_launch_us": primal_ms * 1e3 / primal_launches, "launches": primal_launches,
                 "iteration_mode": "one launch per step" if persistent else "one launch per colour", **counts}
     phases = {k[:-3]: round(v / max(1, prof["steps"]), 4) for k, v in prof.items() if k.endswith("_ms")}
+    # the whole step against the same peak: the iterations' bytes plus the setup phases'
+    # (broadphase N (40 + 16 x 3 sort passes), narrowphase and force warm start 120 per
+    # manifold + 216 per contact, body warm start and velocities 176 per body)
+    setup_bytes = bodies * (40 + 16 * 3) + 120 * counts["manifolds"] + 216 * counts["contacts"] + 176 * bodies
+    step_bytes = per_iter * iters + setup_bytes
+    step_gbs = step_bytes / (max_ms / args.steps / 1e3) / 1e9
+    roofline["whole_step"] = {"algorithmic_bytes": step_bytes, "setup_bytes": setup_bytes,
+                              "ms": max_ms / args.steps, "achieved": step_gbs, "frac": step_gbs / peak}
+    st_now = w.stats()
 
     # ---- end to end through the C ABI with host buffers (H2D state, step, D2H state)
     st = w.bodies()
@@ -222,13 +253,19 @@ def run_cuda(args):
                    "caller's arrays (allocated once, reused every step), host timer"}
 
     collision = collision_only(w, scene, rank, world_size, local, reference=not args.no_cpu_baseline)
+    w.close()
 
-    cpu = None
+    cpu, fp64 = None, None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(scene)
+        if not args.no_fp64:  # after the timed CPU baseline, so as not to share its cores
+            fp64 = CpuFp64Reference()
     batched = batched_line(args, rank, world_size, local, stream) if not args.no_batched else None
     adjoint = adjoint_line(args, local, stream) if (rank == 0 and not args.no_adjoint) else None
-    w.close()
+    mixed = mixed_line(args, local, stream, reference=cpu is not None) \
+        if (rank == 0 and not args.no_mixed) else None
+    if fp64 is not None:
+        cpu["err_vs_fp64"] = fp64.result(local, stream)
     if world_size > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -241,10 +278,13 @@ def run_cuda(args):
                            "timing": "CUDA events on the solver stream, summed per step, max over ranks"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(),
                 "gpu_launches": prof["launches"], "phases_ms_per_step": phases, "batched": batched,
-                "adjoint": adjoint, "collision_only": collision,
+                "adjoint": adjoint, "collision_only": collision, "mixed200k": mixed,
                 "autotune": {"primal_variant": World.primal_variants()[tuned],
                              "sweep_us": [round(float(x), 1) for x in variant_us]},
-                "step_ms_min_max": [min(step_ms), max(step_ms)]}
+                "step_ms_min_max": [min(step_ms), max(step_ms)],
+                "device_steps": {"issued": int(st_now["device_steps"]), "redone_on_host": int(st_now["redone_steps"]),
+                                 "note": "steps run with every count on the device; a step that stops on the "
+                                         "device is redone synchronously and counted here"}}
         print(json.dumps(line), flush=True)
 
 
@@ -425,6 +465,214 @@ def adjoint_line(args, local, stream):
     return out
 
 
+def _rot_apply(q, v):
+    """Rotate vectors v by unit quaternions q = (x, y, z, w), in double precision."""
+    q = np.asarray(q, np.float64)
+    v = np.asarray(v, np.float64)
+    u, w = q[:, :3], q[:, 3:4]
+    t = 2.0 * np.cross(u, v)
+    return v + w * t + np.cross(u, t)
+
+
+def scene_checks(scene, bodies) -> dict:
+    """The reference's long-run checks on one state (bodies in list order), in double
+    precision: the largest ground penetration of a dynamic box (the ground top is the
+    highest static box top, clearance = z - the box's vertical extent - ground top, values
+    within 1e-5 count as 0; headless_server.cpp:395-490) and the largest ball-joint
+    position error |x_A + R_A r_A - (x_B + R_B r_B)| (the linear constraint C of
+    Joint::updatePrimal, joint.cpp:61-64)."""
+    from avbd_demo3d_b200.solver import box_properties
+
+    n = scene.n_bodies
+    mass = box_properties(scene.size, scene.density)[0][::-1]
+    size = np.asarray(scene.size, np.float64)[::-1]
+    pos = np.asarray(bodies["pos"], np.float64)
+    q = np.asarray(bodies["quat"], np.float64)
+    static = mass <= 0
+    ground_top = float((pos[static, 2] + 0.5 * size[static, 2]).max()) if static.any() else 0.0
+    dyn = ~static
+    ez = (np.abs(2 * (q[:, 0] * q[:, 2] - q[:, 3] * q[:, 1])) * 0.5 * size[:, 0] +
+          np.abs(2 * (q[:, 1] * q[:, 2] + q[:, 3] * q[:, 0])) * 0.5 * size[:, 1] +
+          np.abs(1 - 2 * (q[:, 0] ** 2 + q[:, 1] ** 2)) * 0.5 * size[:, 2])
+    clear = pos[:, 2] - ez - ground_top
+    clear[np.abs(clear) < 1e-5] = 0.0
+    pen = np.where(dyn & (clear < -1e-5), -clear, 0.0)
+    jm = scene.ftype == 1
+    jerr = 0.0
+    if jm.any():
+        fa, fb = scene.fa[jm], scene.fb[jm]
+        a = np.where(fa >= 0, n - 1 - fa, 0)
+        b = n - 1 - fb
+        xa = np.where((fa >= 0)[:, None], pos[a] + _rot_apply(q[a], scene.frA[jm]), scene.frA[jm])
+        xb = pos[b] + _rot_apply(q[b], scene.frB[jm])
+        jerr = float(np.linalg.norm(xa - xb, axis=1).max())
+    return {"max_penetration_m": float(pen.max()) if n else 0.0, "below_ground": int((pen > 0).sum()),
+            "max_joint_error_m": jerr}
+
+
+def mixed_line(args, local, stream, reference: bool, steps: int = 600, chunk: int = 10, ref_steps: int = 5):
+    """The mixed-constraint scene: 200,000 boxes (2,048 jointed chains of 48 boxes, springs
+    between 5% of the rest) dropped from a 200 x 200 x 100 m volume onto the ground, 600
+    steps at 10 iterations. Body-steps/s from CUDA events around chunks of 10 device-resident
+    steps (state read back between chunks, outside the events), the iteration kernel's
+    roofline, and the reference's long-run checks: the largest ground penetration and joint
+    error over the run (sampled every chunk, every step for the first ref_steps), and the
+    resting drift (the largest displacement between steps 500 and 600 of the boxes slower
+    than 0.05 m/s at step 500). The reference's CPU solver (its own list order) gives the same
+    checks for its first ref_steps steps, beside the GPU's over the same steps."""
+    import torch
+
+    from avbd_demo3d_b200 import World, scenes
+
+    scene = scenes.mixed_drop()
+    w = World(scene, device=local, stream=stream.cuda_stream)
+    bodies = scene.n_bodies - 1
+    w.set_profiling(True)
+    w.reset_profile()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * (steps // chunk + ref_steps))]
+    spans, k, done = [], 0, 0
+    worst = {"max_penetration_m": 0.0, "below_ground": 0, "max_joint_error_m": 0.0}
+    early, settled, x500 = [], None, None
+    torch.cuda.synchronize()
+    while done < steps:
+        m = 1 if done < ref_steps else min(chunk, steps - done)
+        with torch.cuda.stream(stream):
+            ev[k].record(stream)
+        w.step(m, sync=False)
+        with torch.cuda.stream(stream):
+            ev[k + 1].record(stream)
+        spans.append((ev[k], ev[k + 1], m))
+        k += 2
+        done += m
+        b = w.bodies()
+        c = scene_checks(scene, b)
+        for key in worst:
+            worst[key] = max(worst[key], c[key])
+        if done <= ref_steps:
+            early.append(c)
+        if done == 500:
+            speed = np.linalg.norm(b["vel"], axis=1)
+            settled = speed < 0.05
+            x500 = b["pos"].astype(np.float64)
+    torch.cuda.synchronize()
+    total_s = sum(a.elapsed_time(e) for a, e, _ in spans) / 1e3
+    b600 = w.bodies()
+    drift = float(np.linalg.norm(b600["pos"].astype(np.float64)[settled] - x500[settled], axis=1).max()) \
+        if settled is not None and settled.any() else None
+    prof = w.profile()
+    w.set_profiling(False)
+    st = w.stats()
+    per_iter, counts = algorithmic_primal_bytes(w)
+    per_iter += 32 * counts["contacts"]
+    peak, _ = measured_peak()
+    it_ms = prof["primal_ms"]
+    achieved = per_iter * scene.params.iterations / (it_ms / max(1, prof["steps"]) / 1e3) / 1e9 if it_ms else None
+    out = {"workload": "200,000 boxes + ground (mixed_drop, seed 2): 2,048 chains of 48 boxes on ball joints "
+                       "(96,256 joints), springs between 5% of the other boxes; 600 steps, dt 1/60, 10 iterations",
+           "value": bodies * steps / total_s, "unit": UNIT, "ms_per_step": total_s * 1e3 / steps, "steps": steps,
+           "final": {"manifolds": int(st["manifold_count"]), "colours": int(st["colours"]),
+                     "joints": int(st["joint_count"]), "springs": int(st["spring_count"])},
+           "checks_600_steps": {**worst, "resting_drift_m": drift,
+                                "resting_bodies": int(settled.sum()) if settled is not None else None,
+                                "sampling": f"every step for the first {ref_steps}, then every {chunk}"},
+           "roofline": {"kernel": "k_iterations", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak if achieved else None,
+                        "algorithmic_bytes_per_launch": per_iter * scene.params.iterations,
+                        "avg_launch_us": it_ms * 1e3 / max(1, prof["primal_spans"]), **counts,
+                        "note": "counts at step 600"},
+           "phases_ms_per_step": {kk[:-3]: round(v / max(1, prof["steps"]), 4) for kk, v in prof.items()
+                                  if kk.endswith("_ms")},
+           "device_steps": int(st["device_steps"]), "redone_steps": int(st["redone_steps"])}
+    w.close()
+    gpu_early = {key: max(c[key] for c in early) for key in ("max_penetration_m", "max_joint_error_m")}
+    out["checks_first_steps"] = {"steps": ref_steps, "gpu": gpu_early}
+    if reference:
+        ref, kind = reference_world(scene)
+        ref_checks = []
+        t0 = time.perf_counter()
+        for _ in range(ref_steps):
+            ref.step(1)
+            ref_checks.append(scene_checks(scene, ref.bodies()))
+        ref_s = time.perf_counter() - t0
+        ref.close()
+        out["checks_first_steps"]["reference"] = {key: max(c[key] for c in ref_checks)
+                                                  for key in ("max_penetration_m", "max_joint_error_m")}
+        out["checks_first_steps"]["reference_kind"] = kind
+        out["cpu_reference"] = {"value": bodies * ref_steps / ref_s, "unit": UNIT, "kind": kind,
+                                "cores": cpu_cores(kind), "sample": f"the first {ref_steps} steps of the same scene"}
+    return out
+
+
+class CpuFp64Reference:
+    """CPU checker leg: the reference's double-precision build (oracle/_ref/libavbd_ref64.so,
+    made by oracle/make_fp64.py from the reference's own sources) stepped in its own list
+    order on a background thread (the stepping call releases the GIL), for the 65,536-box
+    stack field to steps 10 and 60 and the 210-box pyramid to steps 10, 60 and 600. The GPU's
+    state at the same steps comes from fresh GPU runs (the step is deterministic), and the
+    line states the largest position and rotation differences from FP64."""
+
+    MARKS = {"stacks65k": (10, 60), "pyramid20": (10, 60, 600)}
+
+    def __init__(self):
+        import threading
+
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import checkers
+
+        self.checkers = checkers
+        self.available = checkers.ref64_available()
+        self.states, self.error = {}, None
+        self.thread = threading.Thread(target=self._run, daemon=True) if self.available else None
+        if self.thread:
+            self.thread.start()
+
+    @staticmethod
+    def scenes():
+        from avbd_demo3d_b200 import scenes
+
+        return {"stacks65k": scenes.stack_grid(*GRID, seed=SEED), "pyramid20": scenes.pyramid(20)}
+
+    def _run(self):
+        try:
+            for name, sc in self.scenes().items():
+                r = self.checkers.Fp64Reference(sc)
+                done, got = 0, {}
+                for m in self.MARKS[name]:
+                    r.step(m - done)
+                    done = m
+                    got[m] = r.bodies()
+                r.close()
+                self.states[name] = got
+        except Exception as e:  # reported in the line
+            self.error = repr(e)
+
+    def result(self, local, stream):
+        from avbd_demo3d_b200 import World
+
+        if not self.available:
+            return {"unavailable": "oracle/_ref/libavbd_ref64.so not built"}
+        gpu = {}
+        for name, sc in self.scenes().items():
+            w = World(sc, device=local, stream=stream.cuda_stream)
+            done, got = 0, {}
+            for m in self.MARKS[name]:
+                w.step(m - done)
+                done = m
+                got[m] = w.bodies()
+            w.close()
+            gpu[name] = got
+        self.thread.join()
+        if self.error:
+            return {"unavailable": self.error}
+        out = {"reference": "the reference's double-precision build, its own list order (same inputs)"}
+        for name, marks in self.MARKS.items():
+            out[name] = {}
+            for m in marks:
+                dp, dq = self.checkers.pose_error(gpu[name][m], self.states[name][m])
+                out[name][str(m)] = {"max_pos_m": dp, "max_rot_rad": dq}
+        return out
+
+
 def reference_world(scene):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import checkers
@@ -489,6 +737,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-adjoint-check", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the 200,000-box mixed-constraint section")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the error against the FP64 reference build")
     ap.add_argument("--iteration-mode", type=int, default=1, choices=(0, 1),
                     help="0 = one launch per colour and iteration plus the dual sweep, 1 = one launch per step")
     ap.add_argument("--primal-variant", type=int, default=-1,

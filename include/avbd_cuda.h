@@ -259,6 +259,43 @@ int avbd_step(AvbdContext *ctx, int32_t nsteps);
 /* Wait for the context stream (and redo or report any device-resident step, as above). */
 int avbd_synchronize(AvbdContext *ctx);
 
+/* Contacts injected for one step (ExternalManifoldContact, solver.h:336-344): per entry the
+ * bodies (list indices a, b), up to 8 contacts and the contact basis (rows: normal pointing
+ * from B to A, two tangents), in the layout avbd_read_manifolds writes: keys8 feature keys,
+ * contact15x8 per contact rA(3) rB(3) C0(3, recomputed) penalty(3) lambda(3), stick8. */
+typedef struct AvbdExternalContacts
+{
+    int32_t count;
+    const int32_t *body_ab2;
+    const int32_t *num_contacts;
+    const float *basis9;
+    const int32_t *keys8;
+    const float *contact15x8;
+    const int32_t *stick8;
+    const int32_t *creates; /* per entry: nonzero = may make its pair's manifold (NULL: all) */
+} AvbdExternalContacts;
+
+/* One Solver::step with the broadphase replaced by the caller's pairs and, optionally, the
+ * narrowphase replaced by the caller's contacts: Solver::stepCpuReferenceWithExternalBroadphase
+ * (pairs[, contacts]) (solver.cpp:939-957, solver.h:403-404), whose pair handling is
+ * broadphaseExternalPairs (solver.cpp:579-626) and whose contact lookup is
+ * Manifold::initialize's (manifold.cpp:110-117). Bodies are list indices; the reference's
+ * dense BodyIds map to them through the caller's body list.
+ *  - pairs_ab2[2k], [2k+1]: pair k. Pairs naming no body, one body twice or bodies of two
+ *    worlds are skipped. The others, in order: a bounding-sphere test, then a new manifold
+ *    (bodies in the given order) unless a force already links the two bodies, counting an
+ *    earlier pair of this call.
+ *  - contacts (NULL: none): after the pairs, every valid entry with creates[e] != 0 in order
+ *    makes its pair's manifold the same way, without the sphere test. The reference makes
+ *    one only for entries whose dense ids increase (bodyA < bodyB): the caller sets creates
+ *    from that. During this step every manifold whose bodies match an entry, as (a, b) or
+ *    else as (b, a), takes that entry's basis and contacts instead of the narrowphase (the
+ *    later of two entries with the same (a, b) wins); its penalty, multipliers and stick
+ *    flags seed contacts that do not persist from the previous step.
+ * Synchronous (returns when the step is done); counters land in avbd_get_stats. */
+int avbd_step_external(AvbdContext *ctx, int32_t num_pairs, const int32_t *pairs_ab2,
+                       const AvbdExternalContacts *contacts);
+
 /* AVBD_STEP_DEVICE (default) or AVBD_STEP_HOST, for later steps; both give the same bits.
  * No counterpart in the reference (its CPU step has no device). */
 int avbd_set_step_mode(AvbdContext *ctx, int32_t mode);

@@ -149,6 +149,8 @@ def _lib(kind: str) -> ctypes.CDLL:
     else:
         lib.ref_iterate_ordered.argtypes = [vp, fp, ip]
         lib.ref_iterate_ordered.restype = ip
+        lib.ref_prepare_external.argtypes = [vp, ip, fp, ip] + [fp] * 6
+        lib.ref_prepare_external.restype = ip
     _libs[kind] = lib
     return lib
 
@@ -238,6 +240,18 @@ class World:
 
     def iterate(self):
         self._f("iterate")(self.h)
+
+    def prepare_external(self, pairs, contacts: dict | None = None):
+        """Reference only: prepareStep with the caller's pairs (and contacts) in place of the
+        broadphase (and narrowphase), as stepCpuReferenceWithExternalBroadphase sets up."""
+        pairs = np.ascontiguousarray(np.asarray(pairs, np.int32).reshape(-1, 2))
+        c = contacts or {"ab": np.zeros((0, 2), np.int32), "n": np.zeros(0, np.int32),
+                         "basis": np.zeros((0, 9), np.float32), "keys": np.zeros((0, 8), np.int32),
+                         "contact": np.zeros((0, 8, 15), np.float32), "stick": np.zeros((0, 8), np.int32)}
+        arr = [np.ascontiguousarray(c[k], dt) for k, dt in (("ab", np.int32), ("n", np.int32), ("basis", np.float32),
+                                                            ("keys", np.int32), ("contact", np.float32),
+                                                            ("stick", np.int32))]
+        self.lib.ref_prepare_external(self.h, len(pairs), _ptr(pairs), len(arr[1]), *[_ptr(a) for a in arr])
 
     def iterate_ordered(self, order: np.ndarray):
         order = np.ascontiguousarray(order, dtype=np.int32)

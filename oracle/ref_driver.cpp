@@ -235,6 +235,55 @@ int ref_prepare(void *p)
     return 0;
 }
 
+/* prepareStep with the broadphase replaced by the given pairs and the narrowphase of the
+ * given entries' pairs by their contacts, exactly as stepCpuReferenceWithExternalBroadphase
+ * (solver.cpp:949-957) sets them up around stepCpuReference; the external state is only read
+ * by prepareStep (broadphaseExternalPairs, Manifold::initialize), so it is cleared right after.
+ * Bodies are list indices (mapped to the reference's dense ids here); contacts use the
+ * ref_get_manifolds layout. */
+int ref_prepare_external(void *p, int nPairs, const int *ab2, int nEntries, const int *eab2, const int *num,
+                         const float *basis9, const int *keys8, const float *contact15x8, const int *stick8)
+{
+    RefWorld *w = (RefWorld *)p;
+    Solver &s = w->solver;
+    auto dense = [&](int i) -> BodyId {
+        return (i >= 0 && i < (int)w->list.size()) ? w->list[i]->denseId : INVALID_BODY_ID;
+    };
+    std::vector<BroadphasePair> pairs;
+    for (int k = 0; k < nPairs; ++k)
+        pairs.push_back(BroadphasePair{dense(ab2[2 * k]), dense(ab2[2 * k + 1])});
+    std::vector<ExternalManifoldContact> contacts((size_t)nEntries);
+    for (int e = 0; e < nEntries; ++e)
+    {
+        ExternalManifoldContact &c = contacts[e];
+        c = ExternalManifoldContact{};
+        c.bodyA = dense(eab2[2 * e]);
+        c.bodyB = dense(eab2[2 * e + 1]);
+        c.numContacts = num[e];
+        std::memcpy(&c.basis, basis9 + 9 * e, 36);
+        for (int i = 0; i < 8; ++i)
+        {
+            Manifold::Contact &m = c.contacts[i];
+            const float *v = contact15x8 + (8 * e + i) * 15;
+            m.feature.key = keys8[8 * e + i];
+            std::memcpy(&m.rA, v, 12);
+            std::memcpy(&m.rB, v + 3, 12);
+            std::memcpy(&m.C0, v + 6, 12);
+            std::memcpy(&m.penalty, v + 9, 12);
+            std::memcpy(&m.lambda, v + 12, 12);
+            m.stick = stick8[8 * e + i] != 0;
+        }
+    }
+    s.setExternalManifoldContacts(contacts);
+    s.externalBroadphasePairs = pairs;
+    s.useExternalBroadphasePairs = true;
+    s.prepareStep();
+    s.useExternalBroadphasePairs = false;
+    s.externalBroadphasePairs.clear();
+    s.clearExternalManifoldContacts();
+    return 0;
+}
+
 int ref_iterate(void *p)
 {
     ((RefWorld *)p)->solver.iteratePrimalDualCpu();

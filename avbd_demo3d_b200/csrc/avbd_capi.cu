@@ -106,6 +106,8 @@ struct AvbdContext
     DArr<int> binned, large;
     DArr<float4> largeLo, largeHi, largeSphere;
     DArr<int> llCount, llOffset;
+    DArr<float4> llChunkLo, llChunkHi; // bounds of each large-list chunk's spheres
+    DArr<int> llRecorded;               // LL_SLOTS partners per large-large work item
     DArr<unsigned long long> largeKeys, largeKeysAlt;
     const unsigned long long *largeSorted = nullptr;
     DArr<unsigned> bounds;  // 8 words per world
@@ -147,6 +149,8 @@ struct AvbdContext
     DArr<int2> rows;
     DArr<unsigned long long> incKeys, incKeysAlt;
     int incShift = 1; // sequence bits of the incidence keys of the current adjacency
+    bool seqRanked = false; // force lists in ascending, distinct sequence order (incidences by rank)
+    DArr<unsigned> incKeys32, incKeys32Alt; // body keys of the ranked incidences
 
     DArr<int> colourState, colour, solveList, colourStart;
     DArr<int4> solveEntry; // solve list with each body's row range, for the primal
@@ -618,8 +622,8 @@ __global__ void k_step_end(StepState *st, const IterSync *sync)
 }
 
 // Per-body force lists (CSR) sorted newest first.
-int build_rows(AvbdContext *ctx, const unsigned long long *sortedKeys, int total, size_t manifolds,
-               const StepState *st = nullptr);
+template <class Key>
+int build_rows(AvbdContext *ctx, const Key *sortedKeys, int total, size_t manifolds, const StepState *st = nullptr);
 
 // Bits needed to write v (0 for v = 0).
 int bit_width(unsigned long long v) { return v ? 64 - __builtin_clzll(v) : 0; }
@@ -644,16 +648,41 @@ int build_adjacency(AvbdContext *ctx, bool deviceCounts = false)
     if (T == 0)
     {
         CU(cudaMemsetAsync(ctx->adjStart.p, 0, sizeof(int) * ((size_t)n + 1), ctx->stream));
-        return build_rows(ctx, nullptr, 0, 0);
+        return build_rows<unsigned>(ctx, nullptr, 0, 0);
     }
     if (T > (long long)ADJ_INDEX_MASK)
         return fail(ctx, AVBD_ERR_CAPACITY, "too many force incidences (%lld)", T);
-    CHECK(reserve(ctx, ctx->incKeys, T, false));
-    CHECK(reserve(ctx, ctx->incKeysAlt, T, false));
     CHECK(reserve(ctx, ctx->incVals, T, false));
     CHECK(reserve(ctx, ctx->incValsAlt, T, false));
     CHECK(reserve(ctx, ctx->adj, T, false));
     DevForces F = dev_forces(ctx);
+    const StepState *st = deviceCounts ? ctx->stepState.p : nullptr;
+    if (ctx->seqRanked)
+    {
+        // incidences in newest-first order of their forces, then a stable sort by body
+        CHECK(reserve(ctx, ctx->incKeys32, T, false));
+        CHECK(reserve(ctx, ctx->incKeys32Alt, T, false));
+        const int forces = (int)(T / 2);
+        k_incidences_ranked<<<grid_for(forces, 256), 256, 0, ctx->stream>>>(F, n, ctx->incKeys32.p, ctx->incVals.p,
+                                                                            st, forces);
+        LAUNCHED();
+        cub::DoubleBuffer<unsigned> dk(ctx->incKeys32.p, ctx->incKeys32Alt.p);
+        cub::DoubleBuffer<unsigned> dv(ctx->incVals.p, ctx->incValsAlt.p);
+        const int endBit = std::max(1, bit_width((unsigned long long)n));
+        size_t bytes = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, bytes, dk, dv, (int)T, 0, endBit, ctx->stream);
+        CHECK(ensure_temp(ctx, bytes));
+        CU(cub::DeviceRadixSort::SortPairs(ctx->cubTemp.p, bytes, dk, dv, (int)T, 0, endBit, ctx->stream));
+        ctx->launches++;
+        ctx->incShift = 0;
+        k_segment_starts<<<grid_for(T, 256), 256, 0, ctx->stream>>>(dk.Current(), (int)T, 0, n, ctx->adjStart.p, st);
+        LAUNCHED();
+        k_copy_adj<<<grid_for(T, 256), 256, 0, ctx->stream>>>(dv.Current(), ctx->adj.p, (int)T, st);
+        LAUNCHED();
+        return build_rows(ctx, dk.Current(), (int)T, mans, st);
+    }
+    CHECK(reserve(ctx, ctx->incKeys, T, false));
+    CHECK(reserve(ctx, ctx->incKeysAlt, T, false));
     // every sequence number is below nextSeq (below seqBound while steps are pending on the
     // device): the key needs bit_width(that) + bit_width(n) bits
     const unsigned long long seqTop = deviceCounts ? ctx->seqBound : (unsigned long long)ctx->nextSeq;
@@ -672,7 +701,6 @@ int build_adjacency(AvbdContext *ctx, bool deviceCounts = false)
     CHECK(ensure_temp(ctx, bytes));
     CU(cub::DeviceRadixSort::SortPairs(ctx->cubTemp.p, bytes, dk, dv, (int)T, 0, endBit, ctx->stream));
     ctx->launches++;
-    const StepState *st = deviceCounts ? ctx->stepState.p : nullptr;
     k_segment_starts<<<grid_for(T, 256), 256, 0, ctx->stream>>>(dk.Current(), (int)T, shift, n, ctx->adjStart.p, st);
     LAUNCHED();
     k_copy_adj<<<grid_for(T, 256), 256, 0, ctx->stream>>>(dv.Current(), ctx->adj.p, (int)T, st);
@@ -682,8 +710,8 @@ int build_adjacency(AvbdContext *ctx, bool deviceCounts = false)
 
 // The primal's row list, one (entry, row) pair per constraint row in force order, for the
 // dynamic bodies (no host read: sized by an upper bound, ranges from a device scan).
-int build_rows(AvbdContext *ctx, const unsigned long long *sortedKeys, int total, size_t manifolds,
-               const StepState *st)
+template <class Key>
+int build_rows(AvbdContext *ctx, const Key *sortedKeys, int total, size_t manifolds, const StepState *st)
 {
     int n = ctx->n;
     CHECK(reserve(ctx, ctx->rowStart, (size_t)n + 1, false));
@@ -918,8 +946,15 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
         auto large_large_count = [&]() -> int {
             if (nItems > 0)
             {
-                k_bp_large_large<false><<<grid_for(nItems, 128), 128, 0, ctx->stream>>>(
-                    F, ctx->large.p, ctx->largeSphere.p, ctx->llItems.p, nItems, ctx->llCount.p, nullptr, 0, 0, cnt);
+                CHECK(reserve(ctx, ctx->llChunkLo, (size_t)nL, false));
+                CHECK(reserve(ctx, ctx->llChunkHi, (size_t)nL, false));
+                CHECK(reserve(ctx, ctx->llRecorded, (size_t)nItems * LL_SLOTS, false));
+                k_ll_chunk_bounds<<<grid_for(nL, 128), 128, 0, ctx->stream>>>(G, ctx->large.p, ctx->largeSphere.p, nL,
+                                                                               ctx->llChunkLo.p, ctx->llChunkHi.p);
+                LAUNCHED();
+                k_bp_large_large<BP_COUNT><<<grid_for(nItems, 128), 128, 0, ctx->stream>>>(
+                    F, ctx->large.p, ctx->largeSphere.p, ctx->llItems.p, nItems, ctx->llCount.p, nullptr, 0, 0, cnt,
+                    nullptr, ctx->llChunkLo.p, ctx->llChunkHi.p, ctx->llRecorded.p);
                 LAUNCHED();
                 CHECK(scan_counts(ctx, ctx->llCount.p, ctx->llOffset.p, nItems, 0));
                 ctx->launches++;
@@ -961,9 +996,9 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
             }
             if (nItems > 0)
             {
-                k_bp_large_large<true><<<grid_for(nItems, 128), 128, 0, ctx->stream>>>(
-                    F, ctx->large.p, ctx->largeSphere.p, ctx->llItems.p, nItems, nullptr, ctx->llOffset.p, 0, 0, cnt,
-                    st);
+                k_bp_large_large<BP_EMIT_RECORDED><<<grid_for(nItems, 128), 128, 0, ctx->stream>>>(
+                    F, ctx->large.p, ctx->largeSphere.p, ctx->llItems.p, nItems, ctx->llCount.p, ctx->llOffset.p, 0, 0,
+                    cnt, st, ctx->llChunkLo.p, ctx->llChunkHi.p, ctx->llRecorded.p);
                 LAUNCHED();
             }
             return AVBD_OK;
@@ -1007,9 +1042,10 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
         }
         if (P2 > 0)
         {
-            k_bp_large_large<true><<<grid_for(nItems, 128), 128, 0, ctx->stream>>>(
-                F, ctx->large.p, ctx->largeSphere.p, ctx->llItems.p, nItems, nullptr, ctx->llOffset.p, (int)(M0 + P1),
-                (unsigned long long)(ctx->nextSeq + P1), cnt);
+            k_bp_large_large<BP_EMIT_RECORDED><<<grid_for(nItems, 128), 128, 0, ctx->stream>>>(
+                F, ctx->large.p, ctx->largeSphere.p, ctx->llItems.p, nItems, ctx->llCount.p, ctx->llOffset.p,
+                (int)(M0 + P1), (unsigned long long)(ctx->nextSeq + P1), cnt, nullptr, ctx->llChunkLo.p,
+                ctx->llChunkHi.p, ctx->llRecorded.p);
             LAUNCHED();
         }
     }
@@ -1515,7 +1551,7 @@ int device_reserve(AvbdContext *ctx)
 {
     size_t live = (size_t)ctx->nMan;
     size_t want = ctx->manifoldSpare > 0 ? live + (size_t)ctx->manifoldSpare
-                                         : std::max(2 * live, live + (size_t)ctx->n / 2) + 1024;
+                                         : std::max(2 * live, live + (size_t)ctx->n) + 1024;
     if (ctx->pendingFast == 0 && man_capacity(ctx) < want)
     {
         CHECK(reserve_manifolds(ctx, ctx->man[ctx->cur], want, live));
@@ -2121,6 +2157,8 @@ void avbd_destroy(AvbdContext *ctx)
     release(ctx->incValsAlt);
     release(ctx->incKeys);
     release(ctx->incKeysAlt);
+    release(ctx->incKeys32);
+    release(ctx->incKeys32Alt);
     release(ctx->colourState);
     release(ctx->colour);
     release(ctx->solveList);
@@ -2132,6 +2170,9 @@ void avbd_destroy(AvbdContext *ctx)
     release(ctx->cubTemp);
     release(ctx->counters);
     release(ctx->stepState);
+    release(ctx->llChunkLo);
+    release(ctx->llChunkHi);
+    release(ctx->llRecorded);
     release(ctx->colourFlow);
     release(ctx->colourBlockCounts);
     release(ctx->stepFlags);
@@ -2381,6 +2422,29 @@ int avbd_load_batch(AvbdContext *ctx, int32_t num_worlds, const int32_t *world_s
     }
     ctx->nMan = M;
     ctx->nextSeq = next_seq;
+    {
+        // the force lists' sequence numbers: each list ascending and no number in two lists
+        // lets the adjacency place incidences by rank (later forces always get larger numbers)
+        std::vector<unsigned long long> all;
+        bool ascending = true;
+        auto take = [&](const int64_t *sq, int count) {
+            for (int i = 0; i < count; ++i)
+            {
+                ascending = ascending && (i == 0 || sq[i] > sq[i - 1]);
+                all.push_back((unsigned long long)sq[i]);
+            }
+        };
+        if (J)
+            take(joints->seq, J);
+        if (S)
+            take(springs->seq, S);
+        if (I)
+            take(ignores->seq, I);
+        if (M)
+            take(manifolds->seq, M);
+        std::sort(all.begin(), all.end());
+        ctx->seqRanked = ascending && std::adjacent_find(all.begin(), all.end()) == all.end();
+    }
     CHECK(build_adjacency(ctx));
     CU(cudaStreamSynchronize(ctx->stream));
     ctx->nColours = 0;

@@ -691,11 +691,47 @@ __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, DevG
 // Large-vs-large pairs of each world (solver.cpp:476-479), tested by the reference serially
 // after all grid pairs. Work item = (world's large base, world's large count, i, chunk); the
 // items are ordered by world, i, chunk, which reproduces each world's serial i < j order.
-template <bool EMIT>
+// Modes as k_bp_pairs: BP_COUNT counts and records the first LL_SLOTS partners of each
+// item, BP_EMIT_RECORDED writes them (searching again only for items that found more).
+// A chunk whose bounding box (of every sphere in it, with a relative margin far above FP32
+// rounding) is out of reach of body i's sphere holds no hit: its pairs are counted as
+// checked, as the reference checks them, without loading them.
+constexpr int LL_SLOTS = 4;
+
+// Bounding box of the spheres of each LL_CHUNK-body chunk of every world's large list, at
+// the chunk's first global large index.
+__global__ void k_ll_chunk_bounds(DevGrid G, const int *large, const float4 *largeSphere, int nLarge, float4 *lo,
+                                  float4 *hi)
+{
+    int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= nLarge)
+        return;
+    const int w = G.bodyWorld[large[l]];
+    const int l0 = G.worldLargeStart[w], l1 = G.worldLargeStart[w + 1];
+    if ((l - l0) % LL_CHUNK != 0)
+        return;
+    float3 mn = f3(INFINITY, INFINITY, INFINITY), mx = f3(-INFINITY, -INFINITY, -INFINITY);
+    bool finite = true;
+    for (int k = l; k < min(l1, l + LL_CHUNK); ++k)
+    {
+        float4 sp = largeSphere[k];
+        float r = sp.w * 1.001f + 1.0e-4f;
+        finite = finite && isfinite(sp.x) && isfinite(sp.y) && isfinite(sp.z) && isfinite(r);
+        mn = f3(fminf(mn.x, sp.x - r), fminf(mn.y, sp.y - r), fminf(mn.z, sp.z - r));
+        mx = f3(fmaxf(mx.x, sp.x + r), fmaxf(mx.y, sp.y + r), fmaxf(mx.z, sp.z + r));
+    }
+    // a non-finite sphere disables the cull for its chunk (w = 1: test every pair)
+    lo[l] = f4(mn, finite ? 0.0f : 1.0f);
+    hi[l] = f4(mx, 0.0f);
+}
+
+template <int MODE>
 __global__ void k_bp_large_large(DevForces F, const int *large, const float4 *largeSphere, const int4 *items,
                                  int nItems, int *counts, const int *offsets, int base, unsigned long long seqBase,
-                                 StepCounters *cnt, const StepState *st = nullptr)
+                                 StepCounters *cnt, const StepState *st, const float4 *chunkLo,
+                                 const float4 *chunkHi, int *recorded)
 {
+    constexpr bool EMIT = MODE != BP_COUNT;
     const int w = blockIdx.x * blockDim.x + threadIdx.x;
     if (EMIT && st)
     {
@@ -704,7 +740,27 @@ __global__ void k_bp_large_large(DevForces F, const int *large, const float4 *la
         base = st->manBase + st->newBinned;
         seqBase = st->seqBase + (unsigned long long)st->newBinned;
     }
-    const bool active = w < nItems;
+    bool active = w < nItems;
+    if (MODE == BP_EMIT_RECORDED && active)
+    {
+        const int c = counts[w];
+        if (c <= LL_SLOTS)
+        {
+            if (c > 0)
+            {
+                const int a = large[items[w].x + items[w].z];
+                const int out = base + offsets[w];
+                for (int f = 0; f < c; ++f)
+                {
+                    const int m = out + f;
+                    F.man.ab[m] = make_int2(a, recorded[(size_t)w * LL_SLOTS + f]);
+                    F.man.seq[m] = seqBase + (unsigned long long)(m - base);
+                    F.man.n[m] = 0;
+                }
+            }
+            active = false;
+        }
+    }
     unsigned checks = 0, hits = 0, cons = 0;
     if (active)
     {
@@ -712,10 +768,23 @@ __global__ void k_bp_large_large(DevForces F, const int *large, const float4 *la
         int lbase = it.x, nL = it.y, i = it.z, c = it.w;
         int jBeg = max(i + 1, c * LL_CHUNK), jEnd = min(nL, (c + 1) * LL_CHUNK);
         float4 si = largeSphere[lbase + i];
+        bool reach = true;
+        if (chunkLo && jBeg < jEnd)
+        {
+            const float4 lo = chunkLo[lbase + c * LL_CHUNK], hi = chunkHi[lbase + c * LL_CHUNK];
+            const float r = si.w * 1.001f + 1.0e-4f;
+            const float3 q = f3(fminf(fmaxf(si.x, lo.x), hi.x), fminf(fmaxf(si.y, lo.y), hi.y),
+                                fminf(fmaxf(si.z, lo.z), hi.z));
+            const float3 d = sub(xyz(si), q);
+            reach = lo.w != 0.0f || !isfinite(si.x) || !isfinite(si.y) || !isfinite(si.z) || !isfinite(r) ||
+                    dot(d, d) <= r * r;
+        }
         int a = large[lbase + i];
         int found = 0;
         int out = EMIT ? base + offsets[w] : 0;
-        for (int j = jBeg; j < jEnd; ++j)
+        if (!reach)
+            checks += (unsigned)max(0, jEnd - jBeg);
+        for (int j = reach ? jBeg : jEnd; j < jEnd; ++j)
         {
             checks++;
             float4 sj = largeSphere[lbase + j];
@@ -737,6 +806,8 @@ __global__ void k_bp_large_large(DevForces F, const int *large, const float4 *la
                 F.man.seq[m] = seqBase + (unsigned long long)(m - base);
                 F.man.n[m] = 0;
             }
+            else if (found < LL_SLOTS && recorded)
+                recorded[(size_t)w * LL_SLOTS + found] = b;
             found++;
         }
         if (!EMIT)
@@ -1676,9 +1747,93 @@ __global__ void k_incidences(DevForces F, int shift, int n, unsigned long long *
     vals[t] = make_adj(type, isA, (unsigned)f);
 }
 
+// Number of entries of an ascending sequence list above s.
+AVBD_DEV int count_above(const unsigned long long *seq, int count, unsigned long long s)
+{
+    int lo = 0, hi = count;
+    while (lo < hi)
+    {
+        int mid = (lo + hi) >> 1;
+        if (seq[mid] <= s)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return count - lo;
+}
+
+// Incidences written in the global newest-first order of their forces, when each force
+// list (manifolds, joints, springs, ignore pairs) is stored in ascending sequence order: a
+// force's place is the number of forces with a larger sequence number, found by binary
+// search in the other lists. A stable sort by body alone then gives every body's force list
+// newest first. Keys are the body (n for the world side of an anchored joint); with a device
+// step state the launch covers the capacity and unused slots get keys of all ones.
+__global__ void k_incidences_ranked(DevForces F, int n, unsigned *keys, unsigned *vals, const StepState *st = nullptr,
+                                    int capacityForces = 0)
+{
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (step_aborted(st))
+        return;
+    if (st)
+        F.nMan = st->nMan;
+    const int total = F.nMan + F.nJoint + F.nSpring + F.nIgnore;
+    if (f >= total)
+    {
+        if (st && f < capacityForces)
+        {
+            keys[2 * f] = keys[2 * f + 1] = 0xFFFFFFFFu;
+            vals[2 * f] = vals[2 * f + 1] = ADJ_NONE;
+        }
+        return;
+    }
+    int2 ab;
+    unsigned type;
+    int idx = f;
+    unsigned long long s;
+    int rank;
+    if (idx < F.nMan)
+    {
+        ab = F.man.ab[idx];
+        s = F.man.seq[idx];
+        type = ADJ_MANIFOLD;
+        rank = F.nMan - 1 - idx + count_above(F.jointSeq, F.nJoint, s) + count_above(F.springSeq, F.nSpring, s) +
+               count_above(F.ignoreSeq, F.nIgnore, s);
+    }
+    else if ((idx -= F.nMan) < F.nJoint)
+    {
+        ab = F.jointAB[idx];
+        s = F.jointSeq[idx];
+        type = ADJ_JOINT;
+        rank = F.nJoint - 1 - idx + count_above(F.man.seq, F.nMan, s) + count_above(F.springSeq, F.nSpring, s) +
+               count_above(F.ignoreSeq, F.nIgnore, s);
+    }
+    else if ((idx -= F.nJoint) < F.nSpring)
+    {
+        ab = F.springAB[idx];
+        s = F.springSeq[idx];
+        type = ADJ_SPRING;
+        rank = F.nSpring - 1 - idx + count_above(F.man.seq, F.nMan, s) + count_above(F.jointSeq, F.nJoint, s) +
+               count_above(F.ignoreSeq, F.nIgnore, s);
+    }
+    else
+    {
+        idx -= F.nSpring;
+        ab = F.ignoreAB[idx];
+        s = F.ignoreSeq[idx];
+        type = ADJ_IGNORE;
+        rank = F.nIgnore - 1 - idx + count_above(F.man.seq, F.nMan, s) + count_above(F.jointSeq, F.nJoint, s) +
+               count_above(F.springSeq, F.nSpring, s);
+    }
+    keys[2 * rank] = ab.x >= 0 ? (unsigned)ab.x : (unsigned)n;
+    vals[2 * rank] = make_adj(type, 1u, (unsigned)idx);
+    keys[2 * rank + 1] = (unsigned)ab.y;
+    vals[2 * rank + 1] = make_adj(type, 0u, (unsigned)idx);
+}
+
 // Segment starts of a sorted key array whose top bits are the segment id (0..n-1, or
 // larger for "no segment"); start[s] for s in [0, n] with gaps filled.
-__global__ void k_segment_starts(const unsigned long long *keys, int total, int shift, int n, int *start,
+template <class Key>
+__global__ void k_segment_starts(const Key *keys, int total, int shift, int n, int *start,
                                  const StepState *st = nullptr)
 {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2247,7 +2402,8 @@ AVBD_DEV int rows_listed(const DevForces &F, unsigned e)
 // body): entry k contributes rows_listed rows unless its body is static (never solved).
 // Incidences without a body (the world side of an anchored joint) sort after the last body
 // and contribute none.
-__global__ void k_entry_rows(DevForces F, DevBodies B, const unsigned long long *sortedKeys, int total, int shift,
+template <class Key>
+__global__ void k_entry_rows(DevForces F, DevBodies B, const Key *sortedKeys, int total, int shift,
                              int *count, const StepState *st = nullptr)
 {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2879,71 +3035,143 @@ __global__ void __launch_bounds__(COLOUR_FLOW_BLOCK) k_colour_greedy(
     __shared__ int shC, shVertices;
     const int stride = gridDim.x * blockDim.x;
     const int G = gridDim.x;
+    const int lane = threadIdx.x & 31;
     int mine = 0, maxC = -1, maxR = -1;
     bool failed = false;
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n && !failed; v += stride)
+    // Warps take 32 consecutive bodies at a time and colour them in rounds: each round every
+    // waiting lane polls (without blocking) the neighbours it has not seen coloured yet, and
+    // a lane whose lower-index neighbours are all coloured takes its colour. A chain of
+    // neighbours inside the warp advances one link per round; a warp that makes no progress
+    // in a round backs off, and after spinLimit such rounds the wait has expired.
+    constexpr int NB = 8; // lower-index neighbours kept in registers (more: rescanned per round)
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n && !failed; base += stride)
     {
-        const bool vertex = B.massMoment[v].x > 0 && F.adjStart[v + 1] > F.adjStart[v];
-        if (!vertex)
-        {
-            __stcg(&colour[v], -1);
-            continue;
-        }
+        const int v = base + lane;
+        bool pending = false, many = false;
+        int nb[NB];
+        int nnb = 0;
+        unsigned seen = 0; // bit k: nb[k]'s colour is in `used`
         unsigned long long used[4] = {0ull, 0ull, 0ull, 0ull};
         int round = 0;
-        for (int k = F.adjStart[v]; k < F.adjStart[v + 1] && !failed; ++k)
+        if (v < n)
         {
-            unsigned e = F.adj[k];
-            if (adj_type(e) == ADJ_IGNORE)
-                continue;
-            int2 ab = force_bodies(F, e);
-            int u = ab.x == v ? ab.y : ab.x;
-            if (u < 0 || u >= v || B.massMoment[u].x <= 0) // static bodies are not vertices
-                continue;
-            // u shares this force, so it is a vertex: wait for its colour of this launch
-            unsigned long long su;
-            unsigned spins = 0;
-            while (((su = ld_acquire_u64(&state[u])) >> 32) != (unsigned long long)epoch)
-            {
-                if (++spins >= spinLimit)
+            pending = B.massMoment[v].x > 0 && F.adjStart[v + 1] > F.adjStart[v];
+            if (!pending)
+                __stcg(&colour[v], -1);
+            else
+                for (int k = F.adjStart[v]; k < F.adjStart[v + 1]; ++k)
                 {
+                    unsigned e = F.adj[k];
+                    if (adj_type(e) == ADJ_IGNORE)
+                        continue;
+                    int2 ab = force_bodies(F, e);
+                    int u = ab.x == v ? ab.y : ab.x;
+                    // static bodies are not vertices; a dynamic neighbour shares this force
+                    if (u < 0 || u >= v || B.massMoment[u].x <= 0)
+                        continue;
+                    if (nnb < NB)
+                        nb[nnb++] = u;
+                    else
+                        many = true;
+                }
+        }
+        unsigned idle = 0;
+        while (__any_sync(0xFFFFFFFFu, pending))
+        {
+            bool progressed = false;
+            if (pending)
+            {
+                bool ready = true;
+                if (!many)
+                {
+#pragma unroll
+                    for (int k = 0; k < NB; ++k)
+                    {
+                        if (k >= nnb || ((seen >> k) & 1u))
+                            continue;
+                        const unsigned long long su = ld_acquire_u64(&state[nb[k]]);
+                        if ((su >> 32) != (unsigned long long)epoch)
+                        {
+                            ready = false;
+                            continue;
+                        }
+                        const int cu = (int)(su & 0xFFFFu), ru = (int)((su >> 16) & 0xFFFFu);
+                        if (cu < 256)
+                            used[cu >> 6] |= 1ull << (cu & 63);
+                        round = max(round, ru + 1);
+                        seen |= 1u << k;
+                    }
+                }
+                else
+                {
+                    // more than NB lower neighbours: look at all of them again each round
+                    used[0] = used[1] = used[2] = used[3] = 0ull;
+                    round = 0;
+                    for (int k = F.adjStart[v]; k < F.adjStart[v + 1] && ready; ++k)
+                    {
+                        unsigned e = F.adj[k];
+                        if (adj_type(e) == ADJ_IGNORE)
+                            continue;
+                        int2 ab = force_bodies(F, e);
+                        int u = ab.x == v ? ab.y : ab.x;
+                        if (u < 0 || u >= v || B.massMoment[u].x <= 0)
+                            continue;
+                        const unsigned long long su = ld_acquire_u64(&state[u]);
+                        if ((su >> 32) != (unsigned long long)epoch)
+                        {
+                            ready = false;
+                            break;
+                        }
+                        const int cu = (int)(su & 0xFFFFu), ru = (int)((su >> 16) & 0xFFFFu);
+                        if (cu < 256)
+                            used[cu >> 6] |= 1ull << (cu & 63);
+                        round = max(round, ru + 1);
+                    }
+                }
+                if (ready)
+                {
+                    int c = 0;
+                    while (c < 256 && ((used[c >> 6] >> (c & 63)) & 1ull))
+                        c++;
+                    if (c >= 256)
+                    {
+                        cnt->error = DERR_TOO_MANY_COLOURS;
+                        c = 255;
+                    }
+                    st_release_u64(&state[v], ((unsigned long long)epoch << 32) |
+                                                  ((unsigned long long)min(round, 0xFFFF) << 16) |
+                                                  (unsigned long long)c);
+                    __stcg(&colour[v], c);
+                    mine++;
+                    maxC = max(maxC, c);
+                    maxR = max(maxR, round);
+                    pending = false;
+                    progressed = true;
+                }
+            }
+            if (__any_sync(0xFFFFFFFFu, progressed))
+            {
+                idle = 0;
+                continue;
+            }
+            // no lane of the warp could move: its neighbours belong to other warps
+            if (++idle >= spinLimit)
+            {
+                if (lane == 0)
                     atomicExch(&ctl->error, 1);
+                failed = true;
+                break;
+            }
+            if (idle > 16)
+            {
+                if (((volatile int *)&ctl->error)[0])
+                {
                     failed = true;
                     break;
                 }
-                if (spins > 64)
-                {
-                    if (((volatile int *)&ctl->error)[0])
-                    {
-                        failed = true;
-                        break;
-                    }
-                    __nanosleep(32);
-                }
+                __nanosleep(32);
             }
-            if (failed)
-                break;
-            int cu = (int)(su & 0xFFFFu), ru = (int)((su >> 16) & 0xFFFFu);
-            if (cu < 256)
-                used[cu >> 6] |= 1ull << (cu & 63);
-            round = max(round, ru + 1);
         }
-        if (failed)
-            break;
-        int c = 0;
-        while (c < 256 && ((used[c >> 6] >> (c & 63)) & 1ull))
-            c++;
-        if (c >= 256)
-        {
-            cnt->error = DERR_TOO_MANY_COLOURS;
-            c = 255;
-        }
-        st_release_u64(&state[v], ((unsigned long long)epoch << 32) | ((unsigned long long)min(round, 0xFFFF) << 16) |
-                                      (unsigned long long)c);
-        __stcg(&colour[v], c);
-        mine++;
-        maxC = max(maxC, c);
-        maxR = max(maxR, round);
     }
     // vertices, largest colour and round of the launch
     {
@@ -3027,7 +3255,7 @@ __global__ void __launch_bounds__(COLOUR_FLOW_BLOCK) k_colour_greedy(
     }
     __syncthreads();
     // stable placement: tiles of the block's share, warps in order inside a tile
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     for (int base = b0; base < b1; base += blockDim.x)
     {

@@ -106,8 +106,9 @@ struct AvbdContext
     DArr<int> binned, large;
     DArr<float4> largeLo, largeHi, largeSphere;
     DArr<int> llCount, llOffset;
-    DArr<float4> llChunkLo, llChunkHi; // bounds of each large-list chunk's spheres
+    DArr<uint4> llChunkLo, llChunkHi; // bounds of each large-list chunk's spheres (ordered ints)
     DArr<int> llRecorded;               // LL_SLOTS partners per large-large work item
+    DArr<unsigned long long> pairSetKeys; // body pairs linked by a force, for the broadphase
     DArr<unsigned long long> largeKeys, largeKeysAlt;
     const unsigned long long *largeSorted = nullptr;
     DArr<unsigned> bounds;  // 8 words per world
@@ -899,6 +900,22 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
             return fail(ctx, AVBD_ERR_ARGUMENT, "broadphase mode %d is not implemented on the GPU", mode);
         const int nB = (int)ctx->hBinned.size(), nL = (int)ctx->hLarge.size();
         const int nItems = (int)ctx->hLLItems.size();
+        // the body pairs the existing forces link (constrainedTo by one hash probe run)
+        PairSet S;
+        {
+            const long long forces = (long long)(deviceCounts ? man_capacity(ctx) : (size_t)ctx->nMan) +
+                                     ctx->nJoint + ctx->nSpring + ctx->nIgnore;
+            unsigned long long slots = 1024;
+            while (slots < 2ull * (unsigned long long)forces)
+                slots <<= 1;
+            CHECK(reserve(ctx, ctx->pairSetKeys, (size_t)slots, false));
+            CU(cudaMemsetAsync(ctx->pairSetKeys.p, 0xFF, sizeof(unsigned long long) * slots, ctx->stream));
+            S.keys = ctx->pairSetKeys.p;
+            S.mask = (unsigned)(slots - 1);
+            k_pair_set<<<grid_for(std::max(forces, 1ll), 256), 256, 0, ctx->stream>>>(
+                dev_forces(ctx), S, deviceCounts ? ctx->stepState.p : nullptr);
+            LAUNCHED();
+        }
         if (nL)
         {
             k_bp_large<<<grid_for(nL, 64), 64, 0, ctx->stream>>>(B, ctx->large.p, nL, dt, ctx->largeLo.p,
@@ -932,7 +949,8 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
             CHECK(reserve(ctx, ctx->pairRecorded, (size_t)nB * BP_SLOTS, false));
             k_bp_pairs<BP_COUNT><<<grid_for(nB, 128), 128, 0, ctx->stream>>>(
                 B, F, G, dk.Current(), nB, cell_hash(ctx), ctx->large.p, ctx->largeLo.p, ctx->largeHi.p,
-                ctx->largeSorted, large_hash(ctx), dt, ctx->pairCount.p, nullptr, 0, 0, cnt, ctx->pairRecorded.p);
+                ctx->largeSorted, large_hash(ctx), dt, ctx->pairCount.p, nullptr, 0, 0, cnt, ctx->pairRecorded.p,
+                nullptr, S);
             LAUNCHED();
             CHECK(scan_counts(ctx, ctx->pairCount.p, ctx->pairOffset.p, nB, 0));
             ctx->launches++;
@@ -949,12 +967,14 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
                 CHECK(reserve(ctx, ctx->llChunkLo, (size_t)nL, false));
                 CHECK(reserve(ctx, ctx->llChunkHi, (size_t)nL, false));
                 CHECK(reserve(ctx, ctx->llRecorded, (size_t)nItems * LL_SLOTS, false));
+                k_ll_chunk_init<<<grid_for(nL, 256), 256, 0, ctx->stream>>>(ctx->llChunkLo.p, ctx->llChunkHi.p, nL);
+                LAUNCHED();
                 k_ll_chunk_bounds<<<grid_for(nL, 128), 128, 0, ctx->stream>>>(G, ctx->large.p, ctx->largeSphere.p, nL,
                                                                                ctx->llChunkLo.p, ctx->llChunkHi.p);
                 LAUNCHED();
                 k_bp_large_large<BP_COUNT><<<grid_for(nItems, 128), 128, 0, ctx->stream>>>(
                     F, ctx->large.p, ctx->largeSphere.p, ctx->llItems.p, nItems, ctx->llCount.p, nullptr, 0, 0, cnt,
-                    nullptr, ctx->llChunkLo.p, ctx->llChunkHi.p, ctx->llRecorded.p);
+                    nullptr, ctx->llChunkLo.p, ctx->llChunkHi.p, ctx->llRecorded.p, S);
                 LAUNCHED();
                 CHECK(scan_counts(ctx, ctx->llCount.p, ctx->llOffset.p, nItems, 0));
                 ctx->launches++;
@@ -991,14 +1011,14 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
                 k_bp_pairs<BP_EMIT_RECORDED><<<grid_for(nB, 128), 128, 0, ctx->stream>>>(
                     B, F, G, dk.Current(), nB, cell_hash(ctx), ctx->large.p, ctx->largeLo.p, ctx->largeHi.p,
                     ctx->largeSorted, large_hash(ctx), dt, ctx->pairCount.p, ctx->pairOffset.p, 0, 0, cnt,
-                    ctx->pairRecorded.p, st);
+                    ctx->pairRecorded.p, st, S);
                 LAUNCHED();
             }
             if (nItems > 0)
             {
                 k_bp_large_large<BP_EMIT_RECORDED><<<grid_for(nItems, 128), 128, 0, ctx->stream>>>(
                     F, ctx->large.p, ctx->largeSphere.p, ctx->llItems.p, nItems, ctx->llCount.p, ctx->llOffset.p, 0, 0,
-                    cnt, st, ctx->llChunkLo.p, ctx->llChunkHi.p, ctx->llRecorded.p);
+                    cnt, st, ctx->llChunkLo.p, ctx->llChunkHi.p, ctx->llRecorded.p, S);
                 LAUNCHED();
             }
             return AVBD_OK;
@@ -1037,7 +1057,7 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
             k_bp_pairs<BP_EMIT_RECORDED><<<grid_for(nB, 128), 128, 0, ctx->stream>>>(
                 B, F, G, dk.Current(), nB, cell_hash(ctx), ctx->large.p, ctx->largeLo.p, ctx->largeHi.p,
                 ctx->largeSorted, large_hash(ctx), dt, ctx->pairCount.p, ctx->pairOffset.p, M0,
-                (unsigned long long)ctx->nextSeq, cnt, ctx->pairRecorded.p);
+                (unsigned long long)ctx->nextSeq, cnt, ctx->pairRecorded.p, nullptr, S);
             LAUNCHED();
         }
         if (P2 > 0)
@@ -1045,7 +1065,7 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
             k_bp_large_large<BP_EMIT_RECORDED><<<grid_for(nItems, 128), 128, 0, ctx->stream>>>(
                 F, ctx->large.p, ctx->largeSphere.p, ctx->llItems.p, nItems, ctx->llCount.p, ctx->llOffset.p,
                 (int)(M0 + P1), (unsigned long long)(ctx->nextSeq + P1), cnt, nullptr, ctx->llChunkLo.p,
-                ctx->llChunkHi.p, ctx->llRecorded.p);
+                ctx->llChunkHi.p, ctx->llRecorded.p, S);
             LAUNCHED();
         }
     }
@@ -1551,7 +1571,7 @@ int device_reserve(AvbdContext *ctx)
 {
     size_t live = (size_t)ctx->nMan;
     size_t want = ctx->manifoldSpare > 0 ? live + (size_t)ctx->manifoldSpare
-                                         : std::max(2 * live, live + (size_t)ctx->n) + 1024;
+                                         : std::max(2 * live, live + 2 * (size_t)ctx->n) + 1024;
     if (ctx->pendingFast == 0 && man_capacity(ctx) < want)
     {
         CHECK(reserve_manifolds(ctx, ctx->man[ctx->cur], want, live));
@@ -1620,6 +1640,9 @@ int step_device(AvbdContext *ctx)
     LAUNCHED();
     CU(cudaMemcpyAsync(ctx->hState, st, sizeof(StepState), cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaMemcpyAsync(ctx->hCounters, ctx->counters.p, sizeof(StepCounters), cudaMemcpyDeviceToHost, ctx->stream));
+    // the colour ranges, for host-side users of the last colouring (per-colour launches)
+    CU(cudaMemcpyAsync(ctx->hColourStarts, ctx->colourStart.p, sizeof(int) * 257, cudaMemcpyDeviceToHost,
+                       ctx->stream));
     ctx->pendingFast++;
     ctx->deviceSteps++;
     if (ctx->profiling)
@@ -1653,6 +1676,7 @@ int settle(AvbdContext *ctx)
     ctx->seqBound = s.nextSeq;
     if (done > 0)
     {
+        ctx->hColourStart.assign(ctx->hColourStarts, ctx->hColourStarts + std::min(std::max(ctx->nColours, 0), 256) + 1);
         ctx->stats.body_count = ctx->n;
         ctx->stats.manifold_count = ctx->nMan;
         ctx->stats.joint_count = ctx->nJoint;
@@ -1666,7 +1690,7 @@ int settle(AvbdContext *ctx)
         ctx->stats.constrained_hits = (int64_t)ctx->hCounters->constrainedHits;
     }
     if (s.abort == ABORT_NONE)
-        return AVBD_OK;
+        return device_step_ok(ctx) ? device_reserve(ctx) : AVBD_OK; // room for the next steps, now
     ctx->stateDirty = true; // the device's stop word is cleared before the next device step
     // The stopped steps still rebuilt the per-body force lists (from buffers the host had
     // swapped for them); the next broadphase reads those lists, so rebuild them from the
@@ -1689,7 +1713,7 @@ int settle(AvbdContext *ctx)
         CHECK(step_once(ctx));
         ctx->redoneSteps++;
     }
-    return AVBD_OK;
+    return device_step_ok(ctx) ? device_reserve(ctx) : AVBD_OK;
 }
 
 int stage_reserve(AvbdContext *ctx, size_t count)
@@ -2173,6 +2197,7 @@ void avbd_destroy(AvbdContext *ctx)
     release(ctx->llChunkLo);
     release(ctx->llChunkHi);
     release(ctx->llRecorded);
+    release(ctx->pairSetKeys);
     release(ctx->colourFlow);
     release(ctx->colourBlockCounts);
     release(ctx->stepFlags);
@@ -2489,6 +2514,9 @@ int avbd_step(AvbdContext *ctx, int32_t nsteps)
             ctx->stateDirty = true;
         }
     }
+    // a synchronous step knows its counts: make room for device-resident steps right away
+    if (ctx->pendingFast == 0 && device_step_ok(ctx))
+        CHECK(device_reserve(ctx));
     return AVBD_OK;
 }
 
@@ -3296,7 +3324,7 @@ int avbd_autotune(AvbdContext *ctx, int32_t repeats, int32_t *best_variant, floa
         return AVBD_ERR_ARGUMENT;
     if (ctx->errCode)
         return AVBD_ERR_LATCHED;
-    if (!ctx->loaded || ctx->nSolve == 0)
+    if (!ctx->loaded || ctx->nSolve == 0 || (int)ctx->hColourStart.size() < ctx->nColours + 1)
         return fail(ctx, AVBD_ERR_STATE, "autotune needs a stepped world (run avbd_step first)");
     CU(cudaSetDevice(ctx->device));
     int n = ctx->n;

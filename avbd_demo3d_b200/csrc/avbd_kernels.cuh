@@ -196,6 +196,82 @@ AVBD_DEV bool constrained(const DevForces &F, int a, int b)
     return false;
 }
 
+// The set of body pairs some force links, as open-addressing keys (min << 32 | max), built
+// from the force lists at the start of a step's broadphase: membership is exactly
+// Rigid::constrainedTo (some force of either body joins the two), answered with one probe
+// run instead of walking a force list. World-anchored joints never match a pair.
+struct PairSet
+{
+    unsigned long long *keys = nullptr;
+    unsigned mask = 0;
+};
+
+AVBD_DEV unsigned long long pair_key(int a, int b)
+{
+    unsigned lo = (unsigned)min(a, b), hi = (unsigned)max(a, b);
+    return ((unsigned long long)lo << 32) | hi;
+}
+
+AVBD_DEV unsigned pair_slot(unsigned long long k, unsigned mask)
+{
+    k ^= k >> 31;
+    k *= 0x9E3779B97F4A7C15ull;
+    k ^= k >> 29;
+    return (unsigned)k & mask;
+}
+
+AVBD_DEV bool pair_linked(const PairSet &S, int a, int b)
+{
+    const unsigned long long key = pair_key(a, b);
+    unsigned h = pair_slot(key, S.mask);
+    for (unsigned p = 0; p <= S.mask; ++p)
+    {
+        unsigned long long k = S.keys[h];
+        if (k == key)
+            return true;
+        if (k == ~0ull)
+            return false;
+        h = (h + 1) & S.mask;
+    }
+    return false;
+}
+
+// constrainedTo through the pair set when there is one, else by walking the force lists.
+AVBD_DEV bool linked(const DevForces &F, const PairSet &S, int a, int b)
+{
+    return S.keys ? pair_linked(S, a, b) : constrained(F, a, b);
+}
+
+// One thread per force (manifolds, joints, springs, ignore pairs): insert its body pair.
+__global__ void k_pair_set(DevForces F, PairSet S, const StepState *st = nullptr)
+{
+    if (st)
+        F.nMan = st->nMan;
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    int2 ab;
+    if (f < F.nMan)
+        ab = F.man.ab[f];
+    else if ((f -= F.nMan) < F.nJoint)
+        ab = F.jointAB[f];
+    else if ((f -= F.nJoint) < F.nSpring)
+        ab = F.springAB[f];
+    else if ((f -= F.nSpring) < F.nIgnore)
+        ab = F.ignoreAB[f];
+    else
+        return;
+    if (ab.x < 0 || ab.y < 0)
+        return;
+    const unsigned long long key = pair_key(ab.x, ab.y);
+    unsigned h = pair_slot(key, S.mask);
+    for (unsigned p = 0; p <= S.mask; ++p)
+    {
+        unsigned long long prev = atomicCAS(&S.keys[h], ~0ull, key);
+        if (prev == ~0ull || prev == key)
+            return;
+        h = (h + 1) & S.mask;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Broadphase: the reference's uniform grid (solver.cpp:284-486), one grid per world.
 // W independent worlds are stepped together (W = 1 for one solver); each keeps its own
@@ -524,7 +600,7 @@ AVBD_DEV void warp_add(unsigned long long *dst, unsigned v)
         atomicAdd(dst, (unsigned long long)s);
 }
 
-constexpr int BP_SLOTS = 4; // new pairs a grid entry records in the counting pass
+constexpr int BP_SLOTS = 8; // new pairs a grid entry records in the counting pass
 
 // Modes of the grid-entry pass: count (and record), emit every entry's pairs by searching
 // again, or emit what the counting pass recorded and search again only for the entries
@@ -543,7 +619,8 @@ __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, DevG
                                                   const float4 *largeLo, const float4 *largeHi,
                                                   const unsigned long long *largeKeys, HashTable largeCells, float dt,
                                                   int *counts, const int *offsets, int base, unsigned long long seqBase,
-                                                  StepCounters *cnt, int *recorded, const StepState *st = nullptr)
+                                                  StepCounters *cnt, int *recorded, const StepState *st = nullptr,
+                                                  PairSet S = PairSet())
 {
     constexpr bool EMIT = MODE != BP_COUNT;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -589,7 +666,7 @@ __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, DevG
 
         auto hit = [&](int bIdx) {
             hits++;
-            if (constrained(F, a, bIdx))
+            if (linked(F, S, a, bIdx))
             {
                 cons++;
                 return;
@@ -624,22 +701,49 @@ __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, DevG
             hit(large[l]);
         };
 
-        for (int j = i + 1; j < nBinned && (keys[j] >> 24) == arun; ++j)
-            test(j);
         int ix = (int)(akey % (unsigned)g.nx);
         unsigned t = akey / (unsigned)g.nx;
         int iy = (int)(t % (unsigned)g.ny);
         int iz = (int)(t / (unsigned)g.ny);
+        // The 13 forward cells' run starts: every cell's first hash probe is issued before any
+        // is used (independent loads instead of 13 dependent lookups); a probe that meets
+        // another key continues the usual linear probe.
+        unsigned long long nrun[13], probe[13];
+        unsigned slot[13];
+#pragma unroll
         for (int d = 0; d < 13; ++d)
         {
             int cx = ix + c_forward[d][0], cy = iy + c_forward[d][1], cz = iz + c_forward[d][2];
-            if (cx < 0 || cx >= g.nx || cy < 0 || cy >= g.ny || cz < 0 || cz >= g.nz)
+            bool inside = !(cx < 0 || cx >= g.nx || cy < 0 || cy >= g.ny || cz < 0 || cz >= g.nz);
+            nrun[d] = inside ? (((unsigned long long)w << 22) | (unsigned)(cx + g.nx * (cy + g.ny * cz))) : HASH_EMPTY;
+            slot[d] = hash_slot(nrun[d], cells.mask);
+            probe[d] = inside ? cells.keys[slot[d]] : HASH_EMPTY;
+        }
+        for (int j = i + 1; j < nBinned && (keys[j] >> 24) == arun; ++j)
+            test(j);
+#pragma unroll
+        for (int d = 0; d < 13; ++d)
+        {
+            if (nrun[d] == HASH_EMPTY)
                 continue;
-            unsigned long long nrun = ((unsigned long long)w << 22) | (unsigned)(cx + g.nx * (cy + g.ny * cz));
-            unsigned s = hash_find(cells, nrun);
+            unsigned s = HASH_NONE;
+            unsigned h = slot[d];
+            unsigned long long k = probe[d];
+            for (unsigned p = 0; p <= cells.mask; ++p)
+            {
+                if (k == nrun[d])
+                {
+                    s = cells.vals[h];
+                    break;
+                }
+                if (k == HASH_EMPTY)
+                    break;
+                h = (h + 1) & cells.mask;
+                k = cells.keys[h];
+            }
             if (s == HASH_NONE)
                 continue;
-            for (int j = (int)s; j < nBinned && (keys[j] >> 24) == nrun; ++j)
+            for (int j = (int)s; j < nBinned && (keys[j] >> 24) == nrun[d]; ++j)
                 test(j);
         }
         const int nLargeW = G.worldLargeStart[w + 1] - G.worldLargeStart[w];
@@ -696,40 +800,52 @@ __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, DevG
 // A chunk whose bounding box (of every sphere in it, with a relative margin far above FP32
 // rounding) is out of reach of body i's sphere holds no hit: its pairs are counted as
 // checked, as the reference checks them, without loading them.
-constexpr int LL_SLOTS = 4;
+constexpr int LL_SLOTS = 8;
 
 // Bounding box of the spheres of each LL_CHUNK-body chunk of every world's large list, at
-// the chunk's first global large index.
-__global__ void k_ll_chunk_bounds(DevGrid G, const int *large, const float4 *largeSphere, int nLarge, float4 *lo,
-                                  float4 *hi)
+// the chunk's first global large index, as order-preserving integers (float_order): every
+// large body folds its sphere into its chunk's box with atomic min / max. The boxes start at
+// (all ones, 0) for the minima and 0 for the maxima; w of the minimum marks a non-finite
+// sphere in the chunk (no culling there).
+__global__ void k_ll_chunk_init(uint4 *lo, uint4 *hi, int nLarge)
+{
+    int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l < nLarge)
+    {
+        lo[l] = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u);
+        hi[l] = make_uint4(0u, 0u, 0u, 0u);
+    }
+}
+
+__global__ void k_ll_chunk_bounds(DevGrid G, const int *large, const float4 *largeSphere, int nLarge, uint4 *lo,
+                                  uint4 *hi)
 {
     int l = blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= nLarge)
         return;
     const int w = G.bodyWorld[large[l]];
-    const int l0 = G.worldLargeStart[w], l1 = G.worldLargeStart[w + 1];
-    if ((l - l0) % LL_CHUNK != 0)
-        return;
-    float3 mn = f3(INFINITY, INFINITY, INFINITY), mx = f3(-INFINITY, -INFINITY, -INFINITY);
-    bool finite = true;
-    for (int k = l; k < min(l1, l + LL_CHUNK); ++k)
+    const int l0 = G.worldLargeStart[w];
+    const int c = l0 + (l - l0) / LL_CHUNK * LL_CHUNK;
+    const float4 sp = largeSphere[l];
+    const float r = sp.w * 1.001f + 1.0e-4f;
+    if (!(isfinite(sp.x) && isfinite(sp.y) && isfinite(sp.z) && isfinite(r)))
     {
-        float4 sp = largeSphere[k];
-        float r = sp.w * 1.001f + 1.0e-4f;
-        finite = finite && isfinite(sp.x) && isfinite(sp.y) && isfinite(sp.z) && isfinite(r);
-        mn = f3(fminf(mn.x, sp.x - r), fminf(mn.y, sp.y - r), fminf(mn.z, sp.z - r));
-        mx = f3(fmaxf(mx.x, sp.x + r), fmaxf(mx.y, sp.y + r), fmaxf(mx.z, sp.z + r));
+        atomicOr(&lo[c].w, 1u);
+        return;
     }
-    // a non-finite sphere disables the cull for its chunk (w = 1: test every pair)
-    lo[l] = f4(mn, finite ? 0.0f : 1.0f);
-    hi[l] = f4(mx, 0.0f);
+    atomicMin(&lo[c].x, float_order(sp.x - r));
+    atomicMin(&lo[c].y, float_order(sp.y - r));
+    atomicMin(&lo[c].z, float_order(sp.z - r));
+    atomicMax(&hi[c].x, float_order(sp.x + r));
+    atomicMax(&hi[c].y, float_order(sp.y + r));
+    atomicMax(&hi[c].z, float_order(sp.z + r));
 }
 
 template <int MODE>
 __global__ void k_bp_large_large(DevForces F, const int *large, const float4 *largeSphere, const int4 *items,
                                  int nItems, int *counts, const int *offsets, int base, unsigned long long seqBase,
-                                 StepCounters *cnt, const StepState *st, const float4 *chunkLo,
-                                 const float4 *chunkHi, int *recorded)
+                                 StepCounters *cnt, const StepState *st, const uint4 *chunkLo,
+                                 const uint4 *chunkHi, int *recorded, PairSet S = PairSet())
 {
     constexpr bool EMIT = MODE != BP_COUNT;
     const int w = blockIdx.x * blockDim.x + threadIdx.x;
@@ -771,12 +887,14 @@ __global__ void k_bp_large_large(DevForces F, const int *large, const float4 *la
         bool reach = true;
         if (chunkLo && jBeg < jEnd)
         {
-            const float4 lo = chunkLo[lbase + c * LL_CHUNK], hi = chunkHi[lbase + c * LL_CHUNK];
+            const uint4 lo = chunkLo[lbase + c * LL_CHUNK], hi = chunkHi[lbase + c * LL_CHUNK];
             const float r = si.w * 1.001f + 1.0e-4f;
-            const float3 q = f3(fminf(fmaxf(si.x, lo.x), hi.x), fminf(fmaxf(si.y, lo.y), hi.y),
-                                fminf(fmaxf(si.z, lo.z), hi.z));
+            const float3 mn = f3(float_unorder(lo.x), float_unorder(lo.y), float_unorder(lo.z));
+            const float3 mx = f3(float_unorder(hi.x), float_unorder(hi.y), float_unorder(hi.z));
+            const float3 q = f3(fminf(fmaxf(si.x, mn.x), mx.x), fminf(fmaxf(si.y, mn.y), mx.y),
+                                fminf(fmaxf(si.z, mn.z), mx.z));
             const float3 d = sub(xyz(si), q);
-            reach = lo.w != 0.0f || !isfinite(si.x) || !isfinite(si.y) || !isfinite(si.z) || !isfinite(r) ||
+            reach = lo.w != 0u || !isfinite(si.x) || !isfinite(si.y) || !isfinite(si.z) || !isfinite(r) ||
                     dot(d, d) <= r * r;
         }
         int a = large[lbase + i];
@@ -794,7 +912,7 @@ __global__ void k_bp_large_large(DevForces F, const int *large, const float4 *la
                 continue;
             hits++;
             int b = large[lbase + j];
-            if (constrained(F, a, b))
+            if (linked(F, S, a, b))
             {
                 cons++;
                 continue;
@@ -2659,6 +2777,9 @@ AVBD_DEV void solve_and_move(const DevBodies &B, int b, const float *sys, const 
         st_release(flow.done + b, flow.it + 1); // the block's barrier, are visible before the count
 }
 
+template <bool COH>
+AVBD_DEV void dual_joint(const DevBodies &B, const DevForces &F, int j, const Params &P);
+
 // One primal solve per body of a batch of one colour (solver.cpp:1186-1233). Rows: G lanes
 // per body. The solve entries carry the body and its row range; every lane of a group
 // builds the initial system M/dt^2 and keeps the entries it owns, then the rows are
@@ -2688,6 +2809,26 @@ AVBD_DEV void primal_batch(const DevBodies &B, const DevForces &F, const Params 
                              : j == 2 ? B.initLin[b]
                                       : B.initAngInv[b];
 
+        // Joints' dual updates of the previous iteration (Joint::updateDual, fracture
+        // included), made by the body that owns them before any of its rows reads them, as
+        // the contact rows do for their contacts: the lower colour (or the only dynamic body)
+        // owns the joint, its partner has finished the previous iteration and neither has
+        // moved in this one, so the poses are the ones the reference's dual sweep reads.
+        if (fusedDual && F.nJoint > 0)
+        {
+            for (int r = r0 + lane; r < r1; r += G)
+            {
+                const int2 row = F.rows[r];
+                const unsigned e = (unsigned)row.x;
+                if (adj_type(e) == ADJ_JOINT && row_sub(row) == 0 && (row.y & ROW_OWNS_DUAL) != 0)
+                {
+                    if (flow.done)
+                        wait_partner(flow, row);
+                    dual_joint<COH>(B, F, (int)adj_index(e), P);
+                }
+            }
+            __syncwarp(gmask);
+        }
         float acc[OWN];
         {
             float t0[E_COUNT];
@@ -2937,8 +3078,9 @@ __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces 
     const long long stride = (long long)gridDim.x * BLOCK;
     const long long tid = (long long)blockIdx.x * BLOCK + threadIdx.x;
     unsigned target = 0;
-    // without joints, rows wait for their partners instead of every colour for the grid
-    const bool barriers = F.nJoint > 0 || done == nullptr;
+    // rows wait for their partners instead of every colour for the grid; joints' dual
+    // updates are fused into their owners' rows like the contacts'
+    const bool barriers = done == nullptr;
     IterFlow flow;
     flow.done = barriers ? nullptr : done;
     flow.error = &sync->error;
@@ -2965,7 +3107,7 @@ __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces 
             if (barriers && !iter_barrier(sync, target, spinLimit))
                 return;
         }
-        if (F.nJoint > 0)
+        if (barriers && F.nJoint > 0)
         {
             for (long long j = tid; j < F.nJoint; j += stride)
                 dual_joint<true>(B, F, (int)j, P);
@@ -2986,6 +3128,15 @@ __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces 
             bool orphan = B.massMoment[ab.x].x <= 0 && B.massMoment[ab.y].x <= 0;
             for (int r = orphan ? iterations : 1; r > 0; --r)
                 dual_contact_slot<true, ROUND>(B, F.man, t, P);
+        }
+    // the joints' last dual updates likewise (joints without a dynamic body: all of them)
+    if (iterations > 0 && !barriers)
+        for (long long j = tid; j < F.nJoint; j += stride)
+        {
+            int2 ab = F.jointAB[j];
+            bool orphan = (ab.x < 0 || B.massMoment[ab.x].x <= 0) && B.massMoment[ab.y].x <= 0;
+            for (int r = orphan ? iterations : 1; r > 0; --r)
+                dual_joint<true>(B, F, (int)j, P);
         }
 }
 
@@ -3219,18 +3370,24 @@ __global__ void __launch_bounds__(COLOUR_FLOW_BLOCK) k_colour_greedy(
         __stcg(&blockCounts[(size_t)c * G + blockIdx.x], hist[c]);
     if (!grid_barrier(ctl, target, spinLimit))
         return failing();
-    // each colour's total and this block's first position inside the colour
-    for (int c = threadIdx.x; c < C; c += blockDim.x)
+    // each colour's total and this block's first position inside the colour: the block
+    // sums all blocks' counts of the colour together (G <= blockDim x a few)
+    for (int c = 0; c < C; ++c)
     {
         int before = 0, total = 0;
-        for (int b = 0; b < G; ++b)
+        for (int b = threadIdx.x; b < G; b += blockDim.x)
         {
             int k = __ldcg(&blockCounts[(size_t)c * G + b]);
             total += k;
             before += b < (int)blockIdx.x ? k : 0;
         }
-        shTotal[c] = total;
-        running[c] = before;
+        total = block_sum(total);
+        before = block_sum(before);
+        if (threadIdx.x == 0)
+        {
+            shTotal[c] = total;
+            running[c] = before;
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0)

@@ -337,6 +337,8 @@ def batched_line(args, rank, world_size, local, stream):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if world_size > 1:
         dist.barrier()
+    w.set_profiling(True)
+    w.reset_profile()
     torch.cuda.synchronize()
     with torch.cuda.stream(stream):
         ev0.record(stream)
@@ -346,6 +348,20 @@ def batched_line(args, rank, world_size, local, stream):
     torch.cuda.synchronize()
     batched_s = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, device=f"cuda:{local}")
     n_bodies = int(sum(sc.n_bodies - 1 for sc in all_worlds))
+    # the iteration kernel of the whole batch, against the same peak (counts at the end)
+    prof = w.profile()
+    w.set_profiling(False)
+    per_iter, counts = algorithmic_primal_bytes(w)
+    per_iter += 32 * counts["contacts"]
+    iters = worlds[0].params.iterations
+    it_s = prof["primal_ms"] / max(1, prof["steps"]) / 1e3
+    peak, _ = measured_peak()
+    achieved = per_iter * iters / it_s / 1e9 if it_s > 0 else None
+    batched_roofline = {"kernel": "k_iterations (all worlds in one launch)", "bound": "hbm", "achieved": achieved,
+                        "peak": peak, "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                        "algorithmic_bytes_per_launch": per_iter * iters, "avg_launch_us": it_s * 1e6, **counts,
+                        "phases_ms_per_step": {k[:-3]: round(v / max(1, prof["steps"]), 4) for k, v in prof.items()
+                                               if k.endswith("_ms")}}
     w.close()
     # loop baseline: the plain step looped over a sample of this rank's worlds, each resident
     sample = worlds[:: max(1, len(worlds) // 128)][:128]
@@ -373,7 +389,7 @@ def batched_line(args, rank, world_size, local, stream):
             "body_steps_per_s": n_bodies * steps / batched_s,
             "sharding": f"{world_size} rank(s), size-balanced; {len(worlds)} worlds on rank {rank}",
             "loop_plain_step": {"value": loop_rate, "sample_worlds": len(sample), "steps": loop_steps},
-            "speedup_vs_loop": batched_rate / loop_rate,
+            "speedup_vs_loop": batched_rate / loop_rate, "roofline": batched_roofline,
             "workload": "4,096 worlds, box counts log-uniform in [8, 2048] (seed 3): stack fields, jointed "
                         "chains and drop piles, one ground each; same solver parameters"}
 
@@ -431,12 +447,30 @@ def adjoint_line(args, local, stream):
         grad = np.concatenate([(g["vel"] + g["prevvel"]).ravel(), g["angvel"].ravel(), g["mass"] + dmass,
                                g["pair_friction"]])
     f_s, a_s, b_s = (statistics.median(x) for x in (fwd, afwd, bwd))
+    # roofline of the forward + backward pair against the same peak. Bytes per step: the
+    # FP32 forward's iteration bytes; the backward replays each iteration in FP64 (twice the
+    # FP32 bytes), reads the stored per-iteration snapshots and factors (64 B per solved
+    # body and per contact slot, 224 B of factors per solved body) and reads and writes the
+    # FP64 adjoints of the same rows (twice the FP32 bytes again).
+    wr = World(scene, device=local, stream=stream.cuda_stream)
+    wr.step(T // 2)
+    per_iter, counts = algorithmic_primal_bytes(wr)
+    wr.close()
+    per_iter += 32 * counts["contacts"]
+    iters = scene.params.iterations
+    fwd_bytes = per_iter * iters * T
+    bwd_bytes = iters * T * (4 * per_iter + (64 + 224) * counts["solved_bodies"] + 64 * 8 * counts["manifolds"])
+    peak, _ = measured_peak()
+    ach = (fwd_bytes + bwd_bytes) / (a_s + b_s) / 1e9
+    adjoint_roofline = {"form": "taping forward + backward", "bound": "hbm", "achieved": ach, "peak": peak,
+                        "unit": "GB/s", "frac": ach / peak, "algorithmic_bytes": fwd_bytes + bwd_bytes,
+                        "counts_at_step": T // 2, **counts}
     out = {"workload": "tower 10x10x10 = 1,000 boxes + ground (seed 4), 120 steps, 10 iterations, checkpoint "
                        "every 10 steps; loss |COM(x_120) - target|^2, target = COM_0 + U[-1,1]^3 (seed 7)",
            "forward_ms": f_s * 1e3, "adjoint_forward_ms": a_s * 1e3, "backward_ms": b_s * 1e3,
            "bwd_over_fwd": b_s / f_s, "fwd_plus_bwd_over_fwd": (a_s + b_s) / f_s,
            "timing": "host timer around the C-ABI calls (the step itself reads a few counts per step), "
-                     "median of 3 after one warm-up", "params": int(grad.size)}
+                     "median of 3 after one warm-up", "params": int(grad.size), "roofline": adjoint_roofline}
     if not args.no_adjoint_check:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import checkers

@@ -300,7 +300,8 @@ int avbd_step_external(AvbdContext *ctx, int32_t num_pairs, const int32_t *pairs
  * No counterpart in the reference (its CPU step has no device). */
 int avbd_set_step_mode(AvbdContext *ctx, int32_t mode);
 /* Manifold room kept beyond the live count for device-resident steps: spare = 0 restores
- * the default (twice the live count, and at least the body count more); a small spare
+ * the default (twice the live count, and at least twice the body count more: bodies whose
+ * bounding spheres overlap without touching get a manifold that lasts one step); a small spare
  * makes steps that create many pairs stop on the device and be redone on the host. */
 int avbd_set_manifold_headroom(AvbdContext *ctx, int64_t spare);
 /* Poll limits of the bounded waits: the colouring's grid barrier and the iteration

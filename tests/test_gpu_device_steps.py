@@ -95,3 +95,23 @@ def test_batch_device_steps_equal_host_steps(gpu):
             same_world(host, dev, f"batch step {s}")
     host.close()
     dev.close()
+
+
+def test_autotune_after_device_steps(gpu):
+    """The autotuner times the per-colour primal on the last colouring, whose ranges a
+    device-resident step hands to the host when it is confirmed; the world is unchanged by
+    the trials and keeps stepping bit-exactly."""
+    sc = scenes.stack_grid(6, 6, 8, seed=3)
+    g = World(sc)
+    o = checkers.World(sc, "oracle", order_mode=1)
+    g.step(4)
+    o.step(4)
+    assert g.stats()["redone_steps"] == 0 and g.stats()["device_steps"] == 4
+    best, us = g.autotune(2)
+    assert len(us) == len(World.primal_variants()) and all(x > 0 for x in us)
+    assert_same_state(g, o, "after autotune")
+    for s in range(1, 6):
+        g.step(1)
+        o.step(1)
+        assert_same_state(g, o, f"after autotune, step {s}")
+    g.close()

@@ -119,7 +119,8 @@ struct AvbdContext
     unsigned cellHashMask = 0, largeHashMask = 0;
     DArr<unsigned long long> bpKeys, bpKeysAlt;
     DArr<int> pairCount, pairOffset;
-    DArr<int> pairRecorded; // BP_SLOTS new partners per grid entry from the counting pass
+    DArr<int> pairRecorded; // BP_SLOTS new partners per grid entry lane from the counting pass
+    DArr<int> pairLaneCount; // new partners per grid entry lane
     DArr<int> sapVals, sapValsAlt, sapAxis; // sweep and prune: sorted bodies, axis per world
 
     ManBuf man[2];
@@ -946,11 +947,12 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
             k_bp_hash_runs<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(dk.Current(), nB, cell_hash(ctx));
             LAUNCHED();
             CHECK(large_cell_lists(ctx, nL));
-            CHECK(reserve(ctx, ctx->pairRecorded, (size_t)nB * BP_SLOTS, false));
-            k_bp_pairs<BP_COUNT><<<grid_for(nB, 128), 128, 0, ctx->stream>>>(
+            CHECK(reserve(ctx, ctx->pairRecorded, (size_t)nB * BP_LANES * BP_SLOTS, false));
+            CHECK(reserve(ctx, ctx->pairLaneCount, (size_t)nB * BP_LANES, false));
+            k_bp_pairs<BP_COUNT><<<grid_for((long long)nB * BP_LANES, 128), 128, 0, ctx->stream>>>(
                 B, F, G, dk.Current(), nB, cell_hash(ctx), ctx->large.p, ctx->largeLo.p, ctx->largeHi.p,
                 ctx->largeSorted, large_hash(ctx), dt, ctx->pairCount.p, nullptr, 0, 0, cnt, ctx->pairRecorded.p,
-                nullptr, S);
+                ctx->pairLaneCount.p, nullptr, S);
             LAUNCHED();
             CHECK(scan_counts(ctx, ctx->pairCount.p, ctx->pairOffset.p, nB, 0));
             ctx->launches++;
@@ -1008,10 +1010,10 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
             F = dev_forces(ctx);
             if (nB)
             {
-                k_bp_pairs<BP_EMIT_RECORDED><<<grid_for(nB, 128), 128, 0, ctx->stream>>>(
+                k_bp_pairs<BP_EMIT_RECORDED><<<grid_for((long long)nB * BP_LANES, 128), 128, 0, ctx->stream>>>(
                     B, F, G, dk.Current(), nB, cell_hash(ctx), ctx->large.p, ctx->largeLo.p, ctx->largeHi.p,
                     ctx->largeSorted, large_hash(ctx), dt, ctx->pairCount.p, ctx->pairOffset.p, 0, 0, cnt,
-                    ctx->pairRecorded.p, st, S);
+                    ctx->pairRecorded.p, ctx->pairLaneCount.p, st, S);
                 LAUNCHED();
             }
             if (nItems > 0)
@@ -1054,10 +1056,10 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
         if (P1 > 0)
         {
             // the pairs each entry recorded while counting; entries that found more search again
-            k_bp_pairs<BP_EMIT_RECORDED><<<grid_for(nB, 128), 128, 0, ctx->stream>>>(
+            k_bp_pairs<BP_EMIT_RECORDED><<<grid_for((long long)nB * BP_LANES, 128), 128, 0, ctx->stream>>>(
                 B, F, G, dk.Current(), nB, cell_hash(ctx), ctx->large.p, ctx->largeLo.p, ctx->largeHi.p,
                 ctx->largeSorted, large_hash(ctx), dt, ctx->pairCount.p, ctx->pairOffset.p, M0,
-                (unsigned long long)ctx->nextSeq, cnt, ctx->pairRecorded.p, nullptr, S);
+                (unsigned long long)ctx->nextSeq, cnt, ctx->pairRecorded.p, ctx->pairLaneCount.p, nullptr, S);
             LAUNCHED();
         }
         if (P2 > 0)
@@ -1102,7 +1104,7 @@ int init_forces_device(AvbdContext *ctx)
         LAUNCHED();
         CHECK(scan_counts(ctx, cnt32, idx, M, 0));
         ctx->launches++;
-        k_manifold_compact<<<grid_for(M, 128), 128, 0, ctx->stream>>>(Md, dev_man(ctx->man[ctx->cur ^ 1]), M,
+        k_manifold_compact<<<grid_for((long long)M * COMPACT_LANES, 128), 128, 0, ctx->stream>>>(Md, dev_man(ctx->man[ctx->cur ^ 1]), M,
                                                                       ctx->keep.p, idx, st);
         LAUNCHED();
         ctx->cur ^= 1;
@@ -1238,7 +1240,7 @@ int init_forces(AvbdContext *ctx)
         newM = ctx->hScalars[0];
         ManBuf &dst = ctx->man[ctx->cur ^ 1];
         CHECK(reserve_manifolds(ctx, dst, (size_t)std::max<long long>(newM, 1), 0));
-        k_manifold_compact<<<grid_for(M, 128), 128, 0, ctx->stream>>>(Md, dev_man(dst), M, ctx->keep.p, idx);
+        k_manifold_compact<<<grid_for((long long)M * COMPACT_LANES, 128), 128, 0, ctx->stream>>>(Md, dev_man(dst), M, ctx->keep.p, idx);
         LAUNCHED();
         ctx->cur ^= 1;
         ctx->nMan = (int)newM;
@@ -2198,6 +2200,7 @@ void avbd_destroy(AvbdContext *ctx)
     release(ctx->llChunkHi);
     release(ctx->llRecorded);
     release(ctx->pairSetKeys);
+    release(ctx->pairLaneCount);
     release(ctx->colourFlow);
     release(ctx->colourBlockCounts);
     release(ctx->stepFlags);

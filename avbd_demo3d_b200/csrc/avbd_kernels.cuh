@@ -600,31 +600,38 @@ AVBD_DEV void warp_add(unsigned long long *dst, unsigned v)
         atomicAdd(dst, (unsigned long long)s);
 }
 
-constexpr int BP_SLOTS = 8; // new pairs a grid entry records in the counting pass
-
 // Modes of the grid-entry pass: count (and record), emit every entry's pairs by searching
-// again, or emit what the counting pass recorded and search again only for the entries
-// that found more than BP_SLOTS.
+// again, or emit what the counting pass recorded and search again only for the parts of an
+// entry that found more than BP_SLOTS.
 constexpr int BP_COUNT = 0, BP_EMIT = 1, BP_EMIT_RECORDED = 2;
 
-// One thread per sorted grid entry i (solver.cpp:405-465). BP_COUNT counts new
-// (unconstrained) hits and records the first BP_SLOTS partners of each entry in `recorded`;
-// the emitting modes write them as fresh manifolds at base + offset[i] in hit order. Large
-// bodies are visited in list order: the entry's cell candidates merged with its world's
-// global list, both sorted by large index. With a device step state the emitting modes take
-// base and seqBase from it.
+// Each sorted grid entry i (solver.cpp:405-465) is worked on by BP_LANES lanes, one per part
+// of its search, in the reference's visiting order: lane 0 the rest of its own cell, lanes 1
+// to 13 the 13 forward cells, lane 14 the large bodies (visited in list order: the entry's
+// cell candidates merged with its world's global list, both sorted by large index); lane 15
+// idles. A lane's new (unconstrained) hits form a consecutive run of the entry's pairs, placed
+// after the runs of the lanes before it, so the entry's hit order is the reference's.
+// BP_COUNT counts each lane's hits (laneCounts), records its first BP_SLOTS partners and
+// writes the entry's total (counts); the emitting modes write them as fresh manifolds at
+// base + offset[i] + the lane's place; with a device step state they take base and seqBase
+// from it.
+constexpr int BP_SLOTS = 8;  // new pairs each lane records in the counting pass
+constexpr int BP_LANES = 16; // lanes per grid entry (15 parts)
+
 template <int MODE>
 __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, DevGrid G, const unsigned long long *keys,
                                                   int nBinned, HashTable cells, const int *large,
                                                   const float4 *largeLo, const float4 *largeHi,
                                                   const unsigned long long *largeKeys, HashTable largeCells, float dt,
                                                   int *counts, const int *offsets, int base, unsigned long long seqBase,
-                                                  StepCounters *cnt, int *recorded, const StepState *st = nullptr,
-                                                  PairSet S = PairSet())
+                                                  StepCounters *cnt, int *recorded, int *laneCounts,
+                                                  const StepState *st = nullptr, PairSet S = PairSet())
 {
     constexpr bool EMIT = MODE != BP_COUNT;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    bool active = i < nBinned;
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)(tid / BP_LANES);
+    const int part = (int)(tid % BP_LANES);
+    const bool entry = i < nBinned;
     if (EMIT && st)
     {
         if (step_aborted(st))
@@ -632,37 +639,52 @@ __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, DevG
         base = st->manBase;
         seqBase = st->seqBase;
     }
-    if (MODE == BP_EMIT_RECORDED && active)
+    const size_t slot0 = ((size_t)i * BP_LANES + part) * BP_SLOTS;
+    // the lane's place among the entry's new pairs: the runs of the lanes before it
+    int place = 0, mine = 0;
+    if (EMIT)
     {
-        const int c = counts[i];
-        if (c <= BP_SLOTS)
+        mine = entry ? laneCounts[(size_t)i * BP_LANES + part] : 0;
+        int incl = mine;
+#pragma unroll
+        for (int d = 1; d < BP_LANES; d <<= 1)
+        {
+            int v = __shfl_up_sync(0xFFFFFFFFu, incl, d, BP_LANES);
+            if (part >= d)
+                incl += v;
+        }
+        place = incl - mine;
+    }
+    bool active = entry && part < 15;
+    if (MODE == BP_EMIT_RECORDED && active && mine <= BP_SLOTS)
+    {
+        if (mine > 0)
         {
             const int a = key_body(keys[i]);
-            const int out = base + offsets[i];
-            for (int f = 0; f < c; ++f)
+            const int out = base + offsets[i] + place;
+            for (int f = 0; f < mine; ++f)
             {
                 const int m = out + f;
-                F.man.ab[m] = make_int2(a, recorded[(size_t)i * BP_SLOTS + f]);
+                F.man.ab[m] = make_int2(a, recorded[slot0 + f]);
                 F.man.seq[m] = seqBase + (unsigned long long)(m - base);
                 F.man.n[m] = 0;
             }
-            active = false;
         }
+        active = false;
     }
+    if (MODE == BP_EMIT_RECORDED && active && mine == 0)
+        active = false;
     unsigned checks = 0, hits = 0, cons = 0;
+    int found = 0;
     if (active)
     {
         unsigned long long ki = keys[i];
         const int w = key_world(ki);
         const unsigned akey = key_cell(ki);
-        const unsigned long long arun = ki >> 24;
         const int a = key_body(ki);
-        GridParams g = G.grid[w];
         float3 ac = xyz(B.pos[a]);
         float ar = B.sizeRad[a].w;
-        float aslack = len(xyz(B.vel[a])) * dt;
-        int found = 0;
-        int out = EMIT ? base + offsets[i] : 0;
+        int out = EMIT ? base + offsets[i] + place : 0;
 
         auto hit = [&](int bIdx) {
             hits++;
@@ -679,7 +701,7 @@ __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, DevG
                 F.man.n[m] = 0;
             }
             else if (found < BP_SLOTS)
-                recorded[(size_t)i * BP_SLOTS + found] = bIdx;
+                recorded[slot0 + found] = bIdx;
             found++;
         };
         auto test = [&](int j) {
@@ -690,102 +712,89 @@ __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, DevG
             if (!(dot(dp, dp) > r * r))
                 hit(bIdx);
         };
-        const float margin4 = 4.0f * COLLISION_MARGIN;
-        auto test_large = [&](int l) {
-            float4 lo = largeLo[l], hi = largeHi[l];
-            float3 q = f3(rclamp(ac.x, lo.x, hi.x), rclamp(ac.y, lo.y, hi.y), rclamp(ac.z, lo.z, hi.z));
-            float3 dp = sub(ac, q);
-            float reach = ar + aslack + lo.w + margin4;
-            if (dot(dp, dp) > reach * reach)
-                return;
-            hit(large[l]);
-        };
-
-        int ix = (int)(akey % (unsigned)g.nx);
-        unsigned t = akey / (unsigned)g.nx;
-        int iy = (int)(t % (unsigned)g.ny);
-        int iz = (int)(t / (unsigned)g.ny);
-        // The 13 forward cells' run starts: every cell's first hash probe is issued before any
-        // is used (independent loads instead of 13 dependent lookups); a probe that meets
-        // another key continues the usual linear probe.
-        unsigned long long nrun[13], probe[13];
-        unsigned slot[13];
-#pragma unroll
-        for (int d = 0; d < 13; ++d)
+        if (part == 0)
         {
-            int cx = ix + c_forward[d][0], cy = iy + c_forward[d][1], cz = iz + c_forward[d][2];
-            bool inside = !(cx < 0 || cx >= g.nx || cy < 0 || cy >= g.ny || cz < 0 || cz >= g.nz);
-            nrun[d] = inside ? (((unsigned long long)w << 22) | (unsigned)(cx + g.nx * (cy + g.ny * cz))) : HASH_EMPTY;
-            slot[d] = hash_slot(nrun[d], cells.mask);
-            probe[d] = inside ? cells.keys[slot[d]] : HASH_EMPTY;
-        }
-        for (int j = i + 1; j < nBinned && (keys[j] >> 24) == arun; ++j)
-            test(j);
-#pragma unroll
-        for (int d = 0; d < 13; ++d)
-        {
-            if (nrun[d] == HASH_EMPTY)
-                continue;
-            unsigned s = HASH_NONE;
-            unsigned h = slot[d];
-            unsigned long long k = probe[d];
-            for (unsigned p = 0; p <= cells.mask; ++p)
-            {
-                if (k == nrun[d])
-                {
-                    s = cells.vals[h];
-                    break;
-                }
-                if (k == HASH_EMPTY)
-                    break;
-                h = (h + 1) & cells.mask;
-                k = cells.keys[h];
-            }
-            if (s == HASH_NONE)
-                continue;
-            for (int j = (int)s; j < nBinned && (keys[j] >> 24) == nrun[d]; ++j)
+            const unsigned long long arun = ki >> 24;
+            for (int j = i + 1; j < nBinned && (keys[j] >> 24) == arun; ++j)
                 test(j);
         }
-        const int nLargeW = G.worldLargeStart[w + 1] - G.worldLargeStart[w];
-        if (nLargeW > 0)
+        else if (part <= 13)
         {
-            // the reference tests every large body of the world; all that can pass are here
-            checks += (unsigned)nLargeW;
-            const unsigned long long crun = large_run(w, 0, akey), grun = large_run(w, 1, 0u);
-            unsigned cs = hash_find(largeCells, crun);
-            unsigned gs = hash_find(largeCells, grun);
-            int jc = cs == HASH_NONE ? -1 : (int)cs;
-            int jg = gs == HASH_NONE ? -1 : (int)gs;
-            auto next = [&](int j, unsigned long long run) -> unsigned {
-                if (j < 0)
-                    return 0xFFFFFFFFu;
-                unsigned long long v = largeKeys[j];
-                return (v != HASH_EMPTY && (v >> 24) == run) ? (unsigned)(v & 0xFFFFFFull) : 0xFFFFFFFFu;
-            };
-            unsigned lc = next(jc, crun), lg = next(jg, grun);
-            while (lc != 0xFFFFFFFFu || lg != 0xFFFFFFFFu)
+            const GridParams g = G.grid[w];
+            const int d = part - 1;
+            int ix = (int)(akey % (unsigned)g.nx);
+            unsigned t = akey / (unsigned)g.nx;
+            int iy = (int)(t % (unsigned)g.ny);
+            int iz = (int)(t / (unsigned)g.ny);
+            int cx = ix + c_forward[d][0], cy = iy + c_forward[d][1], cz = iz + c_forward[d][2];
+            if (!(cx < 0 || cx >= g.nx || cy < 0 || cy >= g.ny || cz < 0 || cz >= g.nz))
             {
-                if (lc < lg)
-                {
-                    test_large((int)lc);
-                    lc = next(++jc, crun);
-                }
-                else
-                {
-                    test_large((int)lg);
-                    lg = next(++jg, grun);
-                }
+                unsigned long long nrun = ((unsigned long long)w << 22) | (unsigned)(cx + g.nx * (cy + g.ny * cz));
+                unsigned s = hash_find(cells, nrun);
+                if (s != HASH_NONE)
+                    for (int j = (int)s; j < nBinned && (keys[j] >> 24) == nrun; ++j)
+                        test(j);
             }
         }
-        if (!EMIT)
+        else
         {
-            counts[i] = found;
-            if (found > BP_SLOTS)
-                cnt->pairOverflow = 1;
+            const int nLargeW = G.worldLargeStart[w + 1] - G.worldLargeStart[w];
+            if (nLargeW > 0)
+            {
+                // the reference tests every large body of the world; all that can pass are here
+                checks += (unsigned)nLargeW;
+                const float aslack = len(xyz(B.vel[a])) * dt;
+                const float margin4 = 4.0f * COLLISION_MARGIN;
+                auto test_large = [&](int l) {
+                    float4 lo = largeLo[l], hi = largeHi[l];
+                    float3 q = f3(rclamp(ac.x, lo.x, hi.x), rclamp(ac.y, lo.y, hi.y), rclamp(ac.z, lo.z, hi.z));
+                    float3 dp = sub(ac, q);
+                    float reach = ar + aslack + lo.w + margin4;
+                    if (dot(dp, dp) > reach * reach)
+                        return;
+                    hit(large[l]);
+                };
+                const unsigned long long crun = large_run(w, 0, akey), grun = large_run(w, 1, 0u);
+                unsigned cs = hash_find(largeCells, crun);
+                unsigned gs = hash_find(largeCells, grun);
+                int jc = cs == HASH_NONE ? -1 : (int)cs;
+                int jg = gs == HASH_NONE ? -1 : (int)gs;
+                auto next = [&](int j, unsigned long long run) -> unsigned {
+                    if (j < 0)
+                        return 0xFFFFFFFFu;
+                    unsigned long long v = largeKeys[j];
+                    return (v != HASH_EMPTY && (v >> 24) == run) ? (unsigned)(v & 0xFFFFFFull) : 0xFFFFFFFFu;
+                };
+                unsigned lc = next(jc, crun), lg = next(jg, grun);
+                while (lc != 0xFFFFFFFFu || lg != 0xFFFFFFFFu)
+                {
+                    if (lc < lg)
+                    {
+                        test_large((int)lc);
+                        lc = next(++jc, crun);
+                    }
+                    else
+                    {
+                        test_large((int)lg);
+                        lg = next(++jg, grun);
+                    }
+                }
+            }
         }
     }
     if (!EMIT)
     {
+        if (entry)
+            laneCounts[(size_t)i * BP_LANES + part] = found;
+        if (found > BP_SLOTS)
+            cnt->pairOverflow = 1;
+        // the entry's total
+        int total = found;
+#pragma unroll
+        for (int d = BP_LANES / 2; d > 0; d >>= 1)
+            total += __shfl_down_sync(0xFFFFFFFFu, total, d, BP_LANES);
+        if (entry && part == 0)
+            counts[i] = total;
         warp_add(&cnt->pairChecks, checks);
         warp_add(&cnt->sphereHits, hits);
         warp_add(&cnt->constrainedHits, cons);
@@ -1702,16 +1711,21 @@ __global__ void k_joint_init(DevBodies B, DevForces F, Params P, unsigned char *
 
 // Stable compaction of manifolds into the other buffer. With a device step state the count
 // is the state's, and the kernel records the surviving count and the buffer swap there.
+// COMPACT_LANES threads per manifold: the first copies the header and basis, all of them
+// the live contacts' float4s.
+constexpr int COMPACT_LANES = 8;
+
 __global__ void k_manifold_compact(DevManifolds src, DevManifolds dst, int count, const unsigned char *keep,
                                    const int *newIndex, StepState *st = nullptr)
 {
-    int m = blockIdx.x * blockDim.x + threadIdx.x;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = (int)(t / COMPACT_LANES), lane = (int)(t % COMPACT_LANES);
     if (st)
     {
         if (step_aborted(st))
             return;
         count = st->nManBp;
-        if (m == 0)
+        if (t == 0)
         {
             st->nMan = count > 0 ? newIndex[count - 1] + (keep[count - 1] ? 1 : 0) : 0;
             st->flips++;
@@ -1719,18 +1733,20 @@ __global__ void k_manifold_compact(DevManifolds src, DevManifolds dst, int count
     }
     if (m >= count || !keep[m])
         return;
-    int d = newIndex[m];
-    dst.ab[d] = src.ab[m];
-    dst.seq[d] = src.seq[m];
-    int n = src.n[m];
-    dst.n[d] = n;
-    dst.basis[3 * d + 0] = src.basis[3 * m + 0];
-    dst.basis[3 * d + 1] = src.basis[3 * m + 1];
-    dst.basis[3 * d + 2] = src.basis[3 * m + 2];
+    const int d = newIndex[m];
+    const int n = src.n[m];
+    if (lane == 0)
+    {
+        dst.ab[d] = src.ab[m];
+        dst.seq[d] = src.seq[m];
+        dst.n[d] = n;
+    }
+    if (lane < 3)
+        dst.basis[3 * d + lane] = src.basis[3 * m + lane];
     const float4 *s = src.contact + (size_t)m * 32;
-    float4 *t = dst.contact + (size_t)d * 32;
-    for (int k = 0; k < 4 * n; ++k)
-        t[k] = s[k];
+    float4 *o = dst.contact + (size_t)d * 32;
+    for (int k = lane; k < 4 * n; k += COMPACT_LANES)
+        o[k] = s[k];
 }
 
 __global__ void k_joint_compact(int count, const unsigned char *keep, const int *newIndex, const int2 *abS,
@@ -3421,31 +3437,36 @@ __global__ void __launch_bounds__(COLOUR_FLOW_BLOCK) k_colour_greedy(
         const unsigned same = __match_any_sync(0xFFFFFFFFu, c);
         const int rank = __popc(same & lt);
         const bool leader = (same & lt) == 0;
+        // only the positions need the warps in turn; the writes follow in parallel
+        int pos = -1;
         for (int w = 0; w < COLOUR_FLOW_BLOCK / 32; ++w)
         {
             if (warp == w && c >= 0)
             {
-                const int pos = running[c] + rank;
+                pos = running[c] + rank;
                 __syncwarp(same);
                 if (leader)
                     running[c] += __popc(same);
-                solveList[pos] = v;
-                const int r0 = rowStart[v], r1 = rowStart[v + 1];
-                entries[pos] = make_int4(v, r0, r1, 0);
-                // the contact rows whose dual update this body owns in the fused pass
-                for (int r = r0; r < r1; ++r)
-                {
-                    int2 row = F.rows[r];
-                    const int p = row_partner(row);
-                    const int cp = p >= 0 ? __ldcg(&colour[p]) : -1;
-                    const bool own = p < 0 || cp < 0 || c < cp;
-                    const bool later = p >= 0 && cp >= 0 && c < cp;
-                    row.y = own ? (row.y | ROW_OWNS_DUAL) : (row.y & ~ROW_OWNS_DUAL);
-                    row.y = later ? (row.y | ROW_PARTNER_LATER) : (row.y & ~ROW_PARTNER_LATER);
-                    F.rows[r] = row;
-                }
             }
             __syncthreads();
+        }
+        if (pos >= 0)
+        {
+            solveList[pos] = v;
+            const int r0 = rowStart[v], r1 = rowStart[v + 1];
+            entries[pos] = make_int4(v, r0, r1, 0);
+            // the rows whose contact or joint dual update this body owns in the fused pass
+            for (int r = r0; r < r1; ++r)
+            {
+                int2 row = F.rows[r];
+                const int p = row_partner(row);
+                const int cp = p >= 0 ? __ldcg(&colour[p]) : -1;
+                const bool own = p < 0 || cp < 0 || c < cp;
+                const bool later = p >= 0 && cp >= 0 && c < cp;
+                row.y = own ? (row.y | ROW_OWNS_DUAL) : (row.y & ~ROW_OWNS_DUAL);
+                row.y = later ? (row.y | ROW_PARTNER_LATER) : (row.y & ~ROW_PARTNER_LATER);
+                F.rows[r] = row;
+            }
         }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && st)

@@ -121,6 +121,11 @@ struct AvbdContext
     DArr<int> pairCount, pairOffset;
     DArr<int> pairRecorded; // BP_SLOTS new partners per grid entry lane from the counting pass
     DArr<int> pairLaneCount; // new partners per grid entry lane
+    // LBVH broadphase mode: Morton-sorted binned bodies, tree nodes, grid position per body
+    DArr<unsigned long long> lbvhCodes, lbvhCodesAlt;
+    DArr<int> lbvhBodies, lbvhBodiesAlt, lbvhChild, lbvhParent, entryOf, worldBinnedStart;
+    DArr<float4> lbvhLo, lbvhHi;
+    DArr<unsigned> lbvhArrivals;
     DArr<int> sapVals, sapValsAlt, sapAxis; // sweep and prune: sorted bodies, axis per world
 
     ManBuf man[2];
@@ -801,6 +806,60 @@ int large_cell_lists(AvbdContext *ctx, int nL)
     return AVBD_OK;
 }
 
+// The LBVH part of the grid's counting pass: each world's tree over its binned bodies, then
+// every grid entry's binned partners through it (k_lbvh_count writes the entry totals).
+int lbvh_count(AvbdContext *ctx, const unsigned long long *gridKeys, int nB, const PairSet &S)
+{
+    const int W = ctx->W;
+    CHECK(reserve(ctx, ctx->lbvhCodes, (size_t)nB, false));
+    CHECK(reserve(ctx, ctx->lbvhCodesAlt, (size_t)nB, false));
+    CHECK(reserve(ctx, ctx->lbvhBodies, (size_t)nB, false));
+    CHECK(reserve(ctx, ctx->lbvhBodiesAlt, (size_t)nB, false));
+    CHECK(reserve(ctx, ctx->lbvhChild, 2 * (size_t)nB, false));
+    CHECK(reserve(ctx, ctx->lbvhParent, 2 * (size_t)nB, false));
+    CHECK(reserve(ctx, ctx->lbvhLo, 2 * (size_t)nB, false));
+    CHECK(reserve(ctx, ctx->lbvhHi, 2 * (size_t)nB, false));
+    CHECK(reserve(ctx, ctx->lbvhArrivals, (size_t)nB, false));
+    CHECK(reserve(ctx, ctx->entryOf, (size_t)ctx->n, false));
+    DevBodies B = dev_bodies(ctx);
+    DevGrid G = dev_grid(ctx);
+    k_grid_entry_of<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(gridKeys, nB, ctx->entryOf.p);
+    LAUNCHED();
+    k_lbvh_codes<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(B, G, ctx->binned.p, nB, ctx->lbvhCodes.p,
+                                                             ctx->lbvhBodies.p);
+    LAUNCHED();
+    cub::DoubleBuffer<unsigned long long> dk(ctx->lbvhCodes.p, ctx->lbvhCodesAlt.p);
+    cub::DoubleBuffer<int> dv(ctx->lbvhBodies.p, ctx->lbvhBodiesAlt.p);
+    const int endBit = 32 + bit_width((unsigned long long)(W - 1));
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, dk, dv, nB, 0, endBit, ctx->stream);
+    CHECK(ensure_temp(ctx, bytes));
+    CU(cub::DeviceRadixSort::SortPairs(ctx->cubTemp.p, bytes, dk, dv, nB, 0, endBit, ctx->stream));
+    ctx->launches++;
+    CU(cudaMemsetAsync(ctx->lbvhParent.p, 0xFF, sizeof(int) * 2 * (size_t)nB, ctx->stream));
+    CU(cudaMemsetAsync(ctx->lbvhArrivals.p, 0, sizeof(unsigned) * (size_t)nB, ctx->stream));
+    Lbvh T;
+    T.codes = dk.Current();
+    T.bodies = dv.Current();
+    T.segStart = ctx->worldBinnedStart.p;
+    T.W = W;
+    T.n = nB;
+    T.child = ctx->lbvhChild.p;
+    T.parent = ctx->lbvhParent.p;
+    T.lo = ctx->lbvhLo.p;
+    T.hi = ctx->lbvhHi.p;
+    T.arrivals = ctx->lbvhArrivals.p;
+    k_lbvh_build<<<grid_for(nB, 128), 128, 0, ctx->stream>>>(T);
+    LAUNCHED();
+    k_lbvh_refit<<<grid_for(nB, 128), 128, 0, ctx->stream>>>(T, B);
+    LAUNCHED();
+    k_lbvh_count<<<grid_for(nB, 128), 128, 0, ctx->stream>>>(B, dev_forces(ctx), G, T, gridKeys, nB, ctx->entryOf.p,
+                                                             ctx->pairCount.p, ctx->pairLaneCount.p,
+                                                             ctx->pairRecorded.p, ctx->counters.p, S);
+    LAUNCHED();
+    return AVBD_OK;
+}
+
 // Broadphase of every world: appends new manifolds after the existing ones. `deviceCounts`
 // (grid mode only): no host read; k_bp_commit places the new pairs from the device counts
 // and the emitting passes take their base from the step state.
@@ -897,8 +956,9 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
     }
     else
     {
-        if (mode != AVBD_BROADPHASE_GRID)
+        if (mode != AVBD_BROADPHASE_GRID && mode != AVBD_BROADPHASE_LBVH)
             return fail(ctx, AVBD_ERR_ARGUMENT, "broadphase mode %d is not implemented on the GPU", mode);
+        const bool lbvh = mode == AVBD_BROADPHASE_LBVH;
         const int nB = (int)ctx->hBinned.size(), nL = (int)ctx->hLarge.size();
         const int nItems = (int)ctx->hLLItems.size();
         // the body pairs the existing forces link (constrainedTo by one hash probe run)
@@ -949,11 +1009,14 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
             CHECK(large_cell_lists(ctx, nL));
             CHECK(reserve(ctx, ctx->pairRecorded, (size_t)nB * BP_LANES * BP_SLOTS, false));
             CHECK(reserve(ctx, ctx->pairLaneCount, (size_t)nB * BP_LANES, false));
+            // LBVH mode: the grid pass counts the large-body part only; the tree finds the rest
             k_bp_pairs<BP_COUNT><<<grid_for((long long)nB * BP_LANES, 128), 128, 0, ctx->stream>>>(
                 B, F, G, dk.Current(), nB, cell_hash(ctx), ctx->large.p, ctx->largeLo.p, ctx->largeHi.p,
                 ctx->largeSorted, large_hash(ctx), dt, ctx->pairCount.p, nullptr, 0, 0, cnt, ctx->pairRecorded.p,
-                ctx->pairLaneCount.p, nullptr, S);
+                ctx->pairLaneCount.p, nullptr, S, lbvh ? (1u << 14) : 0x7FFFu);
             LAUNCHED();
+            if (lbvh)
+                CHECK(lbvh_count(ctx, dk.Current(), nB, S));
             CHECK(scan_counts(ctx, ctx->pairCount.p, ctx->pairOffset.p, nB, 0));
             ctx->launches++;
             if (!deviceCounts)
@@ -1562,7 +1625,8 @@ int push_state(AvbdContext *ctx)
 // iterations, not while the differentiable step records.
 bool device_step_ok(const AvbdContext *ctx)
 {
-    return ctx->stepMode == AVBD_STEP_DEVICE && ctx->params.broadphase == AVBD_BROADPHASE_GRID &&
+    return ctx->stepMode == AVBD_STEP_DEVICE &&
+           (ctx->params.broadphase == AVBD_BROADPHASE_GRID || ctx->params.broadphase == AVBD_BROADPHASE_LBVH) &&
            ctx->iterationMode == AVBD_ITERATIONS_PERSISTENT && ctx->iterBlocks > 0 && !ctx->recording &&
            ctx->params.iterations > 0;
 }
@@ -1955,6 +2019,12 @@ int classify_bodies(AvbdContext *ctx, const float *radius)
     CHECK(upload(ctx, ctx->worldStart, ctx->hWorldStart.data(), (size_t)W + 1));
     CHECK(upload(ctx, ctx->worldLargeStart, ctx->hWorldLargeStart.data(), (size_t)W + 1));
     CHECK(upload(ctx, ctx->worldBinned, worldBinned.data(), W));
+    {
+        std::vector<int> start(W + 1, 0);
+        for (int w = 0; w < W; ++w)
+            start[w + 1] = start[w] + worldBinned[w];
+        CHECK(upload(ctx, ctx->worldBinnedStart, start.data(), start.size()));
+    }
     CHECK(upload(ctx, ctx->binnedRadiusW, binnedR.data(), W));
     CHECK(upload(ctx, ctx->binned, ctx->hBinned.data(), nB));
     CHECK(upload(ctx, ctx->large, ctx->hLarge.data(), nL));
@@ -2201,6 +2271,14 @@ void avbd_destroy(AvbdContext *ctx)
     release(ctx->llRecorded);
     release(ctx->pairSetKeys);
     release(ctx->pairLaneCount);
+    for (DArr<int> *a : {&ctx->lbvhBodies, &ctx->lbvhBodiesAlt, &ctx->lbvhChild, &ctx->lbvhParent, &ctx->entryOf,
+                         &ctx->worldBinnedStart})
+        release(*a);
+    release(ctx->lbvhCodes);
+    release(ctx->lbvhCodesAlt);
+    release(ctx->lbvhLo);
+    release(ctx->lbvhHi);
+    release(ctx->lbvhArrivals);
     release(ctx->colourFlow);
     release(ctx->colourBlockCounts);
     release(ctx->stepFlags);
@@ -2260,7 +2338,7 @@ int avbd_set_params(AvbdContext *ctx, const AvbdParams *params)
     if (!(params->dt > 0.0f) || params->iterations < 0)
         return fail(ctx, AVBD_ERR_ARGUMENT, "invalid dt or iteration count");
     if (params->broadphase != AVBD_BROADPHASE_GRID && params->broadphase != AVBD_BROADPHASE_ALL_PAIRS &&
-        params->broadphase != AVBD_BROADPHASE_SAP)
+        params->broadphase != AVBD_BROADPHASE_SAP && params->broadphase != AVBD_BROADPHASE_LBVH)
         return fail(ctx, AVBD_ERR_ARGUMENT, "broadphase mode %d is not available on the GPU", params->broadphase);
     // pending device-resident steps run (or are redone) with the parameters they were issued with
     if (memcmp(&ctx->params, params, sizeof(AvbdParams)) != 0)

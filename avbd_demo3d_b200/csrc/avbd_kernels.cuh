@@ -616,6 +616,7 @@ constexpr int BP_COUNT = 0, BP_EMIT = 1, BP_EMIT_RECORDED = 2;
 // base + offset[i] + the lane's place; with a device step state they take base and seqBase
 // from it.
 constexpr int BP_SLOTS = 8;  // new pairs each lane records in the counting pass
+constexpr unsigned BP_UNRECORDED = 1u << 30; // lane count flag: its partners were not recorded
 constexpr int BP_LANES = 16; // lanes per grid entry (15 parts)
 
 template <int MODE>
@@ -625,7 +626,8 @@ __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, DevG
                                                   const unsigned long long *largeKeys, HashTable largeCells, float dt,
                                                   int *counts, const int *offsets, int base, unsigned long long seqBase,
                                                   StepCounters *cnt, int *recorded, int *laneCounts,
-                                                  const StepState *st = nullptr, PairSet S = PairSet())
+                                                  const StepState *st = nullptr, PairSet S = PairSet(),
+                                                  unsigned partMask = 0x7FFFu)
 {
     constexpr bool EMIT = MODE != BP_COUNT;
     const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -642,9 +644,12 @@ __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, DevG
     const size_t slot0 = ((size_t)i * BP_LANES + part) * BP_SLOTS;
     // the lane's place among the entry's new pairs: the runs of the lanes before it
     int place = 0, mine = 0;
+    bool recordedOk = true;
     if (EMIT)
     {
-        mine = entry ? laneCounts[(size_t)i * BP_LANES + part] : 0;
+        const int raw = entry ? laneCounts[(size_t)i * BP_LANES + part] : 0;
+        mine = raw & ~(int)BP_UNRECORDED;
+        recordedOk = (raw & (int)BP_UNRECORDED) == 0;
         int incl = mine;
 #pragma unroll
         for (int d = 1; d < BP_LANES; d <<= 1)
@@ -655,8 +660,8 @@ __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, DevG
         }
         place = incl - mine;
     }
-    bool active = entry && part < 15;
-    if (MODE == BP_EMIT_RECORDED && active && mine <= BP_SLOTS)
+    bool active = entry && part < 15 && ((partMask >> part) & 1u);
+    if (MODE == BP_EMIT_RECORDED && active && mine <= BP_SLOTS && recordedOk)
     {
         if (mine > 0)
         {
@@ -799,6 +804,315 @@ __global__ void __launch_bounds__(128) k_bp_pairs(DevBodies B, DevForces F, DevG
         warp_add(&cnt->sphereHits, hits);
         warp_add(&cnt->constrainedHits, cons);
     }
+}
+
+// ---------------------------------------------------------------------------
+// Sorted-Morton LBVH broadphase mode: a bounding volume hierarchy over each world's binned
+// bodies (Morton codes of the centres, radix-sorted; Karras's radix-tree construction;
+// bottom-up refit of the spheres' boxes) finds each grid entry's binned partners. It is only
+// the candidate generator: every candidate keeps the grid's own order and test (the entry
+// owns a pair when the partner lies later in its own cell or in one of its 13 forward
+// cells, solver.cpp:405-447; the reference's exact FP32 sphere predicate decides), so the
+// pair set and creation order are the grid's.
+// ---------------------------------------------------------------------------
+
+AVBD_DEV unsigned morton_spread10(unsigned v)
+{
+    v &= 0x3FFu;
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+AVBD_DEV unsigned morton_axis(float x, float bmin, float extent)
+{
+    float f = extent > 0.0f ? (x - bmin) / extent : 0.0f;
+    f = fminf(fmaxf(f, 0.0f), 1.0f); // also maps NaN to 0
+    return (unsigned)(f * 1023.0f);
+}
+
+// Morton code of every binned centre inside its world's bounds, keyed by world.
+__global__ void k_lbvh_codes(DevBodies B, DevGrid G, const int *binned, int nB, unsigned long long *keys, int *bodies)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nB)
+        return;
+    int b = binned[k];
+    int w = G.bodyWorld[b];
+    GridParams g = G.grid[w];
+    float4 c = B.pos[b];
+    unsigned code = (morton_spread10(morton_axis(c.x, g.bminx, g.extx)) << 2) |
+                    (morton_spread10(morton_axis(c.y, g.bminy, g.exty)) << 1) |
+                    morton_spread10(morton_axis(c.z, g.bminz, g.extz));
+    keys[k] = ((unsigned long long)w << 32) | code;
+    bodies[k] = b;
+}
+
+// A radius padded far above the FP32 rounding of boxes and distances at this position
+// (relative 1e-5 of the radius, 4e-7 of the coordinates, 1e-4 m).
+AVBD_DEV float lbvh_pad(float r, float4 c)
+{
+    return r * 1.00001f + 1.0e-4f + 4.0e-7f * (fabsf(c.x) + fabsf(c.y) + fabsf(c.z));
+}
+
+struct Lbvh
+{
+    const unsigned long long *codes; // sorted (world, Morton) keys
+    const int *bodies;               // body of each sorted leaf
+    const int *segStart;             // W + 1 leaf ranges, one tree per world
+    int W, n;                        // worlds, leaves
+    int *child;                      // 2 per internal node; a leaf child is encoded as -1 - leaf
+    int *parent;                     // internal nodes [0, n), leaves [n, 2n); -1 at a root
+    float4 *lo, *hi;                 // boxes: internal nodes [0, n), leaves [n, 2n)
+    unsigned *arrivals;              // per internal node, for the refit
+};
+
+AVBD_DEV int lbvh_world(const Lbvh &T, int k)
+{
+    int lo = 0, hi = T.W; // last w with segStart[w] <= k
+    while (hi - lo > 1)
+    {
+        int mid = (lo + hi) >> 1;
+        if (T.segStart[mid] <= k)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// Common-prefix length of leaves i and j of a segment (the index breaks ties of equal codes).
+AVBD_DEV int lbvh_delta(const Lbvh &T, int s, int m, int i, int j)
+{
+    if (j < 0 || j >= m)
+        return -1;
+    unsigned a = (unsigned)T.codes[s + i], b = (unsigned)T.codes[s + j];
+    return a == b ? 32 + __clz((unsigned)(i ^ j)) : __clz(a ^ b);
+}
+
+// Internal node i of its world's tree (Karras, "Maximizing parallelism in the construction
+// of BVHs, octrees and k-d trees", 2012): the range it covers and the split inside it. A
+// world of m leaves has m - 1 internal nodes, stored from the world's first leaf slot on.
+__global__ void k_lbvh_build(Lbvh T)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= T.n)
+        return;
+    const int w = lbvh_world(T, k);
+    const int s = T.segStart[w], m = T.segStart[w + 1] - s, i = k - s;
+    if (i >= m - 1)
+        return;
+    const int d = lbvh_delta(T, s, m, i, i + 1) > lbvh_delta(T, s, m, i, i - 1) ? 1 : -1;
+    const int dmin = lbvh_delta(T, s, m, i, i - d);
+    int lmax = 2;
+    while (lbvh_delta(T, s, m, i, i + lmax * d) > dmin)
+        lmax *= 2;
+    int l = 0;
+    for (int t = lmax / 2; t >= 1; t /= 2)
+        if (lbvh_delta(T, s, m, i, i + (l + t) * d) > dmin)
+            l += t;
+    const int j = i + l * d;
+    const int dnode = lbvh_delta(T, s, m, i, j);
+    int split = 0;
+    for (int div = 2;; div *= 2)
+    {
+        int t = (l + div - 1) / div;
+        if (lbvh_delta(T, s, m, i, i + (split + t) * d) > dnode)
+            split += t;
+        if (t <= 1)
+            break;
+    }
+    const int gamma = i + split * d + min(d, 0);
+    const int left = min(i, j) == gamma ? -1 - (s + gamma) : s + gamma;
+    const int right = max(i, j) == gamma + 1 ? -1 - (s + gamma + 1) : s + gamma + 1;
+    T.child[2 * k] = left;
+    T.child[2 * k + 1] = right;
+    T.parent[left < 0 ? T.n + (-1 - left) : left] = k;
+    T.parent[right < 0 ? T.n + (-1 - right) : right] = k;
+}
+
+// Leaf boxes (the sphere, padded far above FP32 rounding) and, bottom-up, every internal
+// node's box: the second child to arrive at a node combines both.
+__global__ void k_lbvh_refit(Lbvh T, DevBodies B)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= T.n)
+        return;
+    const int b = T.bodies[k];
+    const float4 c = B.pos[b];
+    const float r = lbvh_pad(B.sizeRad[b].w, c);
+    float4 lo = make_float4(c.x - r, c.y - r, c.z - r, 0.0f), hi = make_float4(c.x + r, c.y + r, c.z + r, 0.0f);
+    __stcg(&T.lo[T.n + k], lo);
+    __stcg(&T.hi[T.n + k], hi);
+    int node = T.parent[T.n + k];
+    while (node >= 0)
+    {
+        __threadfence();
+        if (atomicAdd(&T.arrivals[node], 1u) == 0u)
+            return; // the other child finishes this node
+        const int cl = T.child[2 * node], cr = T.child[2 * node + 1];
+        const int il = cl < 0 ? T.n + (-1 - cl) : cl, ir = cr < 0 ? T.n + (-1 - cr) : cr;
+        const float4 al = __ldcg(&T.lo[il]), ah = __ldcg(&T.hi[il]), bl = __ldcg(&T.lo[ir]), bh = __ldcg(&T.hi[ir]);
+        lo = make_float4(fminf(al.x, bl.x), fminf(al.y, bl.y), fminf(al.z, bl.z), 0.0f);
+        hi = make_float4(fmaxf(ah.x, bh.x), fmaxf(ah.y, bh.y), fmaxf(ah.z, bh.z), 0.0f);
+        __stcg(&T.lo[node], lo);
+        __stcg(&T.hi[node], hi);
+        node = T.parent[node];
+    }
+}
+
+// Sorted grid position of every binned body.
+__global__ void k_grid_entry_of(const unsigned long long *keys, int nB, int *entryOf)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nB)
+        entryOf[key_body(keys[k])] = k;
+}
+
+// Forward-stencil slot (0..12) of a neighbour cell offset, -1 when it is not forward.
+AVBD_DEV int forward_slot(int dx, int dy, int dz)
+{
+    if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1)
+        return -1;
+    const int code = (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1); // 13 = (0, 0, 0)
+    return code > 13 ? code - 14 : -1;
+}
+
+constexpr int LBVH_TUPLES = 32;              // owned hits an entry keeps for recording
+constexpr int LBVH_STACK = 128; // tree depth is at most 64 (32 code + 32 index bits)
+
+// The binned parts (lanes 0..13 of k_bp_pairs) of grid entry i, found by traversing its
+// world's tree with its bounding sphere: each owned candidate is tested with the grid's
+// predicate; hits that no force links are counted per part and recorded in the part's
+// order (ascending grid position); the large-body part was counted by k_bp_pairs already
+// (laneCounts lane 14), so the entry's total is written here.
+__global__ void k_lbvh_count(DevBodies B, DevForces F, DevGrid G, Lbvh T, const unsigned long long *keys, int nB,
+                             const int *entryOf, int *counts, int *laneCounts, int *recorded, StepCounters *cnt,
+                             PairSet S)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned checks = 0, hits = 0, cons = 0;
+    if (i < nB)
+    {
+        const unsigned long long ki = keys[i];
+        const int a = key_body(ki), w = key_world(ki);
+        const unsigned ca = key_cell(ki);
+        const GridParams g = G.grid[w];
+        const int ax = (int)(ca % (unsigned)g.nx);
+        const unsigned t0 = ca / (unsigned)g.nx;
+        const int ay = (int)(t0 % (unsigned)g.ny), az = (int)(t0 / (unsigned)g.ny);
+        const float4 pa = B.pos[a];
+        const float3 ac = xyz(pa);
+        const float ar = B.sizeRad[a].w, reach = lbvh_pad(ar, pa);
+        int partCount[14];
+#pragma unroll
+        for (int q = 0; q < 14; ++q)
+            partCount[q] = 0;
+        unsigned tupleKey[LBVH_TUPLES];
+        int tupleBody[LBVH_TUPLES];
+        int tuples = 0;
+        bool complete = true;
+        const int s0 = T.segStart[w], m = T.segStart[w + 1] - s0;
+        int stack[LBVH_STACK];
+        int top = 0;
+        if (m >= 2)
+            stack[top++] = s0;
+        while (top > 0)
+        {
+            const int node = stack[--top];
+            const int cl = T.child[2 * node], cr = T.child[2 * node + 1];
+#pragma unroll
+            for (int side = 0; side < 2; ++side)
+            {
+                const int c = side == 0 ? cl : cr;
+                const int box = c < 0 ? T.n + (-1 - c) : c;
+                const float4 lo = T.lo[box], hi = T.hi[box];
+                const float3 q = f3(fminf(fmaxf(ac.x, lo.x), hi.x), fminf(fmaxf(ac.y, lo.y), hi.y),
+                                    fminf(fmaxf(ac.z, lo.z), hi.z));
+                const float3 dq = sub(ac, q);
+                if (!(dot(dq, dq) <= reach * reach) && isfinite(ac.x + ac.y + ac.z))
+                    continue;
+                if (c >= 0)
+                {
+                    if (top < LBVH_STACK)
+                        stack[top++] = c;
+                    else
+                        cnt->error = DERR_TOO_MANY_CELLS; // the step fails rather than miss a pair
+                    continue;
+                }
+                const int b = T.bodies[-1 - c];
+                if (b == a)
+                    continue;
+                const int j = entryOf[b];
+                const unsigned cb = key_cell(keys[j]);
+                int part;
+                if (cb == ca)
+                    part = j > i ? 0 : -1;
+                else
+                {
+                    const int bx = (int)(cb % (unsigned)g.nx);
+                    const unsigned t1 = cb / (unsigned)g.nx;
+                    const int by = (int)(t1 % (unsigned)g.ny), bz = (int)(t1 / (unsigned)g.ny);
+                    const int d = forward_slot(bx - ax, by - ay, bz - az);
+                    part = d < 0 ? -1 : d + 1;
+                }
+                if (part < 0)
+                    continue;
+                checks++;
+                const float3 dp = sub(ac, xyz(B.pos[b]));
+                const float r = ar + B.sizeRad[b].w;
+                if (dot(dp, dp) > r * r)
+                    continue;
+                hits++;
+                if (linked(F, S, a, b))
+                {
+                    cons++;
+                    continue;
+                }
+                partCount[part]++;
+                if (tuples < LBVH_TUPLES)
+                {
+                    tupleKey[tuples] = ((unsigned)part << 24) | (unsigned)j;
+                    tupleBody[tuples] = b;
+                    tuples++;
+                }
+                else
+                    complete = false;
+            }
+        }
+        // the recorded hits in the grid's order: by part, then by grid position
+        for (int x = 1; x < tuples; ++x)
+        {
+            unsigned kx = tupleKey[x];
+            int bx = tupleBody[x], y = x - 1;
+            while (y >= 0 && tupleKey[y] > kx)
+            {
+                tupleKey[y + 1] = tupleKey[y];
+                tupleBody[y + 1] = tupleBody[y];
+                --y;
+            }
+            tupleKey[y + 1] = kx;
+            tupleBody[y + 1] = bx;
+        }
+        int total = laneCounts[(size_t)i * BP_LANES + 14];
+        int x = 0;
+        for (int part = 0; part < 14; ++part)
+        {
+            const int c = partCount[part];
+            total += c;
+            const bool keep = complete && c <= BP_SLOTS;
+            laneCounts[(size_t)i * BP_LANES + part] = c | (keep ? 0 : (int)BP_UNRECORDED);
+            for (int f = 0; f < c && x < tuples; ++f, ++x)
+                if (keep)
+                    recorded[((size_t)i * BP_LANES + part) * BP_SLOTS + f] = tupleBody[x];
+        }
+        counts[i] = total;
+    }
+    warp_add(&cnt->pairChecks, checks);
+    warp_add(&cnt->sphereHits, hits);
+    warp_add(&cnt->constrainedHits, cons);
 }
 
 // Large-vs-large pairs of each world (solver.cpp:476-479), tested by the reference serially

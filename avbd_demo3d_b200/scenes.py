@@ -32,6 +32,7 @@ FORCE_IGNORE = 3
 BROADPHASE_ALL_PAIRS = 0
 BROADPHASE_GRID = 1
 BROADPHASE_SAP = 2
+BROADPHASE_LBVH = 3  # the grid's pairs, candidates from a sorted-Morton LBVH (GPU only)
 
 _GOLDEN = np.uint64(0x9E3779B97F4A7C15)
 _MIX1 = np.uint64(0xBF58476D1CE4E5B9)

@@ -41,6 +41,10 @@ extern "C" {
 #define AVBD_BROADPHASE_ALL_PAIRS 0
 #define AVBD_BROADPHASE_GRID 1
 #define AVBD_BROADPHASE_SAP 2
+/* No counterpart in the reference: the uniform grid's pair set and creation order (mode
+ * AVBD_BROADPHASE_GRID, solver.cpp:284-486) with the binned candidates found by a
+ * sorted-Morton LBVH over each world's binned bodies instead of the grid's cell table. */
+#define AVBD_BROADPHASE_LBVH 3
 
 /* Body shapes (RigidShapeType, solver.h:47-53). */
 #define AVBD_SHAPE_BOX 0

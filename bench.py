@@ -254,6 +254,7 @@ def run_cuda(args):
 
     collision = collision_only(w, scene, rank, world_size, local, reference=not args.no_cpu_baseline)
     w.close()
+    lbvh = lbvh_line(args, local, stream) if (rank == 0 and not args.no_lbvh) else None
 
     cpu, fp64 = None, None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
@@ -278,7 +279,7 @@ def run_cuda(args):
                            "timing": "CUDA events on the solver stream, summed per step, max over ranks"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(),
                 "gpu_launches": prof["launches"], "phases_ms_per_step": phases, "batched": batched,
-                "adjoint": adjoint, "collision_only": collision, "mixed200k": mixed,
+                "adjoint": adjoint, "collision_only": collision, "mixed200k": mixed, "lbvh_mode": lbvh,
                 "autotune": {"primal_variant": World.primal_variants()[tuned],
                              "sweep_us": [round(float(x), 1) for x in variant_us]},
                 "step_ms_min_max": [min(step_ms), max(step_ms)],
@@ -286,6 +287,51 @@ def run_cuda(args):
                                  "note": "steps run with every count on the device; a step that stops on the "
                                          "device is redone synchronously and counted here"}}
         print(json.dumps(line), flush=True)
+
+
+def lbvh_line(args, local, stream, steps: int = 10):
+    """The same 65,536-box scene with the sorted-Morton LBVH broadphase mode (the grid's pair
+    set and creation order, binned candidates from the tree): ms per step and per phase
+    (CUDA events on the solver stream, L2 flushed before each step), and whether the state
+    after the steps equals the grid mode's bit for bit."""
+    import copy
+
+    import torch
+
+    from avbd_demo3d_b200 import World, scenes
+
+    scene = scenes.stack_grid(*GRID, seed=SEED)
+    out = {}
+    states = {}
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
+    for mode, name in ((scenes.BROADPHASE_LBVH, "lbvh"), (scenes.BROADPHASE_GRID, "grid")):
+        w = World(scene, device=local, stream=stream.cuda_stream)
+        p = copy.copy(scene.params)
+        p.broadphase = mode
+        w.set_params(p)
+        w.step(max(3, args.warmup))
+        w.set_profiling(True)
+        w.reset_profile()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        torch.cuda.synchronize()
+        for a, b in ev:
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                a.record(stream)
+            w.step(1, sync=False)
+            with torch.cuda.stream(stream):
+                b.record(stream)
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in ev) / steps
+        prof = w.profile()
+        w.set_profiling(False)
+        states[name] = w.bodies()
+        out[name] = {"ms_per_step": ms, "broadphase_ms": prof["broadphase_ms"] / max(1, prof["steps"])}
+        w.close()
+    out["same_bits_as_grid"] = all(np.array_equal(states["lbvh"][k].view(np.uint32), states["grid"][k].view(np.uint32))
+                                   for k in states["grid"])
+    out["steps"] = steps
+    return out
 
 
 def collision_only(w, scene, rank, world_size, local, reference: bool, frames: int = 10):
@@ -773,6 +819,7 @@ def main():
     ap.add_argument("--no-adjoint-check", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the 200,000-box mixed-constraint section")
     ap.add_argument("--no-fp64", action="store_true", help="skip the error against the FP64 reference build")
+    ap.add_argument("--no-lbvh", action="store_true", help="skip the LBVH broadphase mode section")
     ap.add_argument("--iteration-mode", type=int, default=1, choices=(0, 1),
                     help="0 = one launch per colour and iteration plus the dual sweep, 1 = one launch per step")
     ap.add_argument("--primal-variant", type=int, default=-1,

@@ -1159,9 +1159,13 @@ int init_forces_device(AvbdContext *ctx)
     {
         DevManifolds Md = dev_man(ctx->man[ctx->cur]);
         if (ctx->hasShapes)
-            k_manifold_init<true><<<grid_for(M, 128), 128, 0, ctx->stream>>>(B, Md, M, P, ctx->keep.p, st);
+            k_manifold_init<true><<<grid_for(M, 128), 128, 0, ctx->stream>>>(B, Md, M, P, ctx->keep.p, st,
+                                                                            ExternalContacts(),
+                                                                            &ctx->counters.p->orphans);
         else
-            k_manifold_init<false><<<grid_for(M, 128), 128, 0, ctx->stream>>>(B, Md, M, P, ctx->keep.p, st);
+            k_manifold_init<false><<<grid_for(M, 128), 128, 0, ctx->stream>>>(B, Md, M, P, ctx->keep.p, st,
+                                                                             ExternalContacts(),
+                                                                             &ctx->counters.p->orphans);
         LAUNCHED();
         k_u8_to_int<<<grid_for(M, 256), 256, 0, ctx->stream>>>(ctx->keep.p, cnt32, M, st);
         LAUNCHED();
@@ -1175,7 +1179,7 @@ int init_forces_device(AvbdContext *ctx)
     if (J)
     {
         DevForces F = dev_forces(ctx);
-        k_joint_init<<<grid_for(J, 128), 128, 0, ctx->stream>>>(B, F, P, ctx->keep.p, st);
+        k_joint_init<<<grid_for(J, 128), 128, 0, ctx->stream>>>(B, F, P, ctx->keep.p, st, &ctx->counters.p->orphans);
         LAUNCHED();
     }
     return AVBD_OK;
@@ -1289,9 +1293,11 @@ int init_forces(AvbdContext *ctx)
         DevManifolds Md = dev_man(ctx->man[ctx->cur]);
         const ExternalContacts E = external_contacts(ctx);
         if (ctx->hasShapes)
-            k_manifold_init<true><<<grid_for(M, 128), 128, 0, ctx->stream>>>(B, Md, M, P, ctx->keep.p, nullptr, E);
+            k_manifold_init<true><<<grid_for(M, 128), 128, 0, ctx->stream>>>(B, Md, M, P, ctx->keep.p, nullptr, E,
+                                                                            &ctx->counters.p->orphans);
         else
-            k_manifold_init<false><<<grid_for(M, 128), 128, 0, ctx->stream>>>(B, Md, M, P, ctx->keep.p, nullptr, E);
+            k_manifold_init<false><<<grid_for(M, 128), 128, 0, ctx->stream>>>(B, Md, M, P, ctx->keep.p, nullptr, E,
+                                                                             &ctx->counters.p->orphans);
         LAUNCHED();
         k_u8_to_int<<<grid_for(M, 256), 256, 0, ctx->stream>>>(ctx->keep.p, cnt32, M);
         LAUNCHED();
@@ -1311,7 +1317,8 @@ int init_forces(AvbdContext *ctx)
     if (J)
     {
         DevForces F = dev_forces(ctx);
-        k_joint_init<<<grid_for(J, 128), 128, 0, ctx->stream>>>(B, F, P, ctx->keep.p);
+        k_joint_init<<<grid_for(J, 128), 128, 0, ctx->stream>>>(B, F, P, ctx->keep.p, nullptr,
+                                                                 &ctx->counters.p->orphans);
         LAUNCHED();
         k_u8_to_int<<<grid_for(J, 256), 256, 0, ctx->stream>>>(ctx->keep.p, cnt32, J);
         LAUNCHED();
@@ -1474,7 +1481,9 @@ int iterate_persistent(AvbdContext *ctx, bool deviceCounts = false)
     int *done = ctx->iterDone.p;
     unsigned spinLimit = ctx->waitIteration ? ctx->waitIteration : ITER_SPIN_LIMIT;
     const StepState *st = deviceCounts ? ctx->stepState.p : nullptr;
-    void *args[] = {&B, &F, &P, &entries, &colourStart, &nColours, &iterations, &sync, &done, &spinLimit, &st};
+    const int *orphans = &ctx->counters.p->orphans;
+    void *args[] = {&B, &F, &P, &entries, &colourStart, &nColours, &iterations, &sync, &done, &spinLimit, &st,
+                    &orphans};
     {
         PhaseScope ps(ctx, AVBD_PHASE_PRIMAL);
         // worlds with round bodies run the instance that evaluates their contact offsets

@@ -107,6 +107,7 @@ struct StepCounters
     int maxColour;
     int error;
     int pairOverflow; // a grid entry found more new pairs than its recorded slots
+    int orphans;      // live contacts or joints without a dynamic body (no row owns them)
 };
 
 enum DeviceError
@@ -1889,7 +1890,8 @@ AVBD_DEV int ext_lookup(const ExternalContacts &E, int a, int b)
 // persists, C0, lambda/penalty decay.
 template <bool ROUND>
 __global__ void k_manifold_init(DevBodies B, DevManifolds M, int count, Params P, unsigned char *keep,
-                                const StepState *st = nullptr, ExternalContacts E = ExternalContacts())
+                                const StepState *st = nullptr, ExternalContacts E = ExternalContacts(),
+                                int *orphanFlag = nullptr)
 {
     int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (st)
@@ -1989,10 +1991,13 @@ __global__ void k_manifold_init(DevBodies B, DevManifolds M, int count, Params P
     M.basis[3 * m + 1] = f4(basis.r1, round ? ROUND_FLAG : 0.0f);
     M.basis[3 * m + 2] = f4(basis.r2, 0.0f);
     keep[m] = nn > 0 ? 1 : 0;
+    if (nn > 0 && orphanFlag && B.massMoment[ab.x].x <= 0 && B.massMoment[ab.y].x <= 0)
+        *orphanFlag = 1;
 }
 
 // Joint::initialize (joint.cpp:35-54)
-__global__ void k_joint_init(DevBodies B, DevForces F, Params P, unsigned char *keep, const StepState *st = nullptr)
+__global__ void k_joint_init(DevBodies B, DevForces F, Params P, unsigned char *keep, const StepState *st = nullptr,
+                             int *orphanFlag = nullptr)
 {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= F.nJoint || step_aborted(st))
@@ -2021,6 +2026,8 @@ __global__ void k_joint_init(DevBodies B, DevForces F, Params P, unsigned char *
     d[6] = f4(lamLin, 0.0f);
     d[7] = f4(lamAng, 0.0f);
     keep[j] = d4.w != 0.0f ? 0 : 1;
+    if (orphanFlag && (ab.x < 0 || B.massMoment[ab.x].x <= 0) && B.massMoment[ab.y].x <= 0)
+        *orphanFlag = 1;
 }
 
 // Stable compaction of manifolds into the other buffer. With a device step state the count
@@ -3109,6 +3116,8 @@ AVBD_DEV void solve_and_move(const DevBodies &B, int b, const float *sys, const 
 
 template <bool COH>
 AVBD_DEV void dual_joint(const DevBodies &B, const DevForces &F, int j, const Params &P);
+template <bool COH, bool ROUND>
+AVBD_DEV void dual_contact_slot(const DevBodies &B, const DevManifolds &M, long long t, const Params &P);
 
 // One primal solve per body of a batch of one colour (solver.cpp:1186-1233). Rows: G lanes
 // per body. The solve entries carry the body and its row range; every lane of a group
@@ -3122,7 +3131,8 @@ AVBD_DEV void dual_joint(const DevBodies &B, const DevForces &F, int j, const Pa
 // barriers).
 template <int G, int BLOCK, int SUB, bool COH, bool ROUND>
 AVBD_DEV void primal_batch(const DevBodies &B, const DevForces &F, const Params &P, const int4 *entries, int count,
-                           bool fusedDual, PrimalShared<G, BLOCK> &sh, const IterFlow &flow = IterFlow{})
+                           bool fusedDual, PrimalShared<G, BLOCK> &sh, const IterFlow &flow = IterFlow{},
+                           bool lastDual = false)
 {
     static_assert(BLOCK % G == 0 && 32 % G == 0, "group size");
     constexpr int OWN = (E_COUNT + G - 1) / G;
@@ -3228,6 +3238,29 @@ AVBD_DEV void primal_batch(const DevBodies &B, const DevForces &F, const Params 
     const int t = (threadIdx.x / SUB) * (SUB / G) + lt; // the unit's body this thread factorises
     if (lt < SUB / G && t < count)
         solve_and_move<COH, BLOCK / G>(B, sh.body[t], sh.sys[t], sh.start, t, flow);
+    if (lastDual)
+    {
+        // Last iteration: the body that moves last in each of its contacts and joints (the
+        // later colour, or the only dynamic body) makes that force's final dual update right
+        // after its solve, on both bodies' final poses (its earlier partners finished before
+        // its rows were read), which the closing pass would otherwise do.
+        unit_sync<SUB, BLOCK>();
+        if (g < count)
+        {
+            const int4 ent = entries[g];
+            for (int r = ent.y + lane; r < ent.z; r += G)
+            {
+                const int2 row = F.rows[r];
+                if (row.y & ROW_PARTNER_LATER)
+                    continue;
+                const unsigned e = (unsigned)row.x;
+                if (adj_type(e) == ADJ_MANIFOLD)
+                    dual_contact_slot<COH, ROUND>(B, F.man, 8ll * adj_index(e) + row_sub(row), P);
+                else if (adj_type(e) == ADJ_JOINT && row_sub(row) == 0)
+                    dual_joint<COH>(B, F, (int)adj_index(e), P);
+            }
+        }
+    }
 }
 
 // One launch per colour: block k takes the colour's bodies [k GPB, (k+1) GPB).
@@ -3393,7 +3426,7 @@ template <int G, int BLOCK, int SUB, bool ROUND = false>
 __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces F, Params P, const int4 *entries,
                                                          const int *colourStart, int nColours, int iterations,
                                                          IterSync *sync, int *done, unsigned spinLimit,
-                                                         const StepState *st)
+                                                         const StepState *st, const int *orphanFlag)
 {
     if (st)
     {
@@ -3409,8 +3442,11 @@ __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces 
     const long long tid = (long long)blockIdx.x * BLOCK + threadIdx.x;
     unsigned target = 0;
     // rows wait for their partners instead of every colour for the grid; joints' dual
-    // updates are fused into their owners' rows like the contacts'
+    // updates are fused into their owners' rows like the contacts'; the last iteration's
+    // dual updates follow each force's last solve, so only forces without a dynamic body
+    // (flagged by the initialisation) need the closing pass
     const bool barriers = done == nullptr;
+    const bool orphans = barriers || (orphanFlag && *orphanFlag != 0);
     IterFlow flow;
     flow.done = barriers ? nullptr : done;
     flow.error = &sync->error;
@@ -3418,6 +3454,7 @@ __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces 
     for (int it = 0; it < iterations; ++it)
     {
         flow.it = it;
+        const bool last = !barriers && it == iterations - 1;
         for (int c = 0; c < nColours; ++c)
         {
             // the colour's bodies in equal contiguous batches over every block, as few
@@ -3431,7 +3468,7 @@ __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces 
                 if (base >= cnt)
                     break;
                 primal_batch<G, BLOCK, SUB, true, ROUND>(B, F, P, entries + first + base, min(per, cnt - base),
-                                                         it > 0, sh, flow);
+                                                         it > 0, sh, flow, last);
                 unit_sync<SUB, BLOCK>(); // the unit's solve threads are done with the shared systems
             }
             if (barriers && !iter_barrier(sync, target, spinLimit))
@@ -3445,27 +3482,31 @@ __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces 
                 return;
         }
     }
+    if (iterations <= 0 || !orphans)
+        return;
     if (!barriers && !iter_barrier(sync, target, spinLimit)) // every body has finished every iteration
         return;
     // Contacts between two static bodies have no owning row: nothing moves them, so their
-    // update of every iteration runs here, one after the other on the same poses.
-    if (iterations > 0)
-        for (long long t = tid; t < 8ll * F.nMan; t += stride)
-        {
-            if ((int)(t & 7) >= F.man.n[t >> 3]) // an empty slot: nothing to load
-                continue;
-            int2 ab = F.man.ab[t >> 3];
-            bool orphan = B.massMoment[ab.x].x <= 0 && B.massMoment[ab.y].x <= 0;
-            for (int r = orphan ? iterations : 1; r > 0; --r)
-                dual_contact_slot<true, ROUND>(B, F.man, t, P);
-        }
-    // the joints' last dual updates likewise (joints without a dynamic body: all of them)
-    if (iterations > 0 && !barriers)
+    // update of every iteration runs here, one after the other on the same poses. (With
+    // barriers, every contact's last update runs here.)
+    for (long long t = tid; t < 8ll * F.nMan; t += stride)
+    {
+        if ((int)(t & 7) >= F.man.n[t >> 3]) // an empty slot: nothing to load
+            continue;
+        int2 ab = F.man.ab[t >> 3];
+        bool orphan = B.massMoment[ab.x].x <= 0 && B.massMoment[ab.y].x <= 0;
+        if (!orphan && !barriers)
+            continue;
+        for (int r = orphan ? iterations : 1; r > 0; --r)
+            dual_contact_slot<true, ROUND>(B, F.man, t, P);
+    }
+    // joints without a dynamic body likewise
+    if (!barriers)
         for (long long j = tid; j < F.nJoint; j += stride)
         {
             int2 ab = F.jointAB[j];
             bool orphan = (ab.x < 0 || B.massMoment[ab.x].x <= 0) && B.massMoment[ab.y].x <= 0;
-            for (int r = orphan ? iterations : 1; r > 0; --r)
+            for (int r = orphan ? iterations : 0; r > 0; --r)
                 dual_joint<true>(B, F, (int)j, P);
         }
 }

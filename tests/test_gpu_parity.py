@@ -313,3 +313,29 @@ def test_list_order_drift_within_reference_gates(gpu):
             worst = max(worst, float(np.abs(g.bodies()["pos"] - r.bodies()["pos"]).max()))
         assert worst < 0.05, (sc.name, worst)
         g.close()
+
+
+def static_pairs_scene():
+    """A small pyramid beside static bodies that touch each other and are jointed together
+    (contacts and joints with no dynamic body: every iteration's dual updates of those run at
+    the end of the iteration launch), plus a dynamic chain hanging from a static anchor."""
+    s = scenes.SceneBuilder("static_pairs", scenes.baseline_params())
+    g = s.body((40, 40, 1), 0.0, 0.5, (0, 0, -0.5))
+    post = s.body((1, 1, 3), 0.0, 0.5, (8.0, 0.0, 1.0))   # static, sunk into the ground
+    beam = s.body((4, 1, 1), 0.0, 0.5, (8.0, 0.0, 2.9))   # static, resting on the post
+    far = s.body((1, 1, 1), 0.0, 0.5, (-12.0, 0.0, 6.0))   # static, touching nothing
+    s.joint(far, beam, (0.0, 0.0, -0.5), (-2.0, 0.0, 0.0))  # static to static, apart
+    for r in range(5):
+        for i in range(5 - r):
+            s.body((1, 1, 1), 1.0, 0.5, (i * 1.01 + r * 0.5 - 2.5, 0.0, r + 0.5))
+    prev = beam
+    for k in range(6):
+        b = s.body((0.4, 0.4, 0.4), 1.0, 0.5, (9.5, 0.0, 2.4 - 0.45 * k))
+        s.joint(prev, b, (1.5, 0.0, -0.5) if k == 0 else (0.0, 0.0, -0.225), (0.0, 0.0, 0.225))
+        prev = b
+    # the post, sunk into the ground, and the beam on it touch each other and the ground
+    return s.build()
+
+
+def test_contacts_and_joints_without_a_dynamic_body(gpu):
+    lockstep(static_pairs_scene(), 60)

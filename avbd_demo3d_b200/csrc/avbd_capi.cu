@@ -1888,6 +1888,19 @@ void copy_host(const std::vector<HostCopy> &copies)
         memcpy(c.dst, c.src, c.bytes);
 }
 
+// A caller array in page-locked host memory (cudaHostAlloc, cudaHostRegister, a pinned
+// torch tensor) is copied to or from the device directly, without the staging copy.
+bool host_pinned(const void *p)
+{
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
 // Body state from caller arrays: one copy of the packed fields into pinned staging, one
 // asynchronous upload, and the conversion to float4 on the device.
 int write_state(AvbdContext *ctx, const AvbdBodies *b)
@@ -1910,15 +1923,31 @@ int write_state(AvbdContext *ctx, const AvbdBodies *b)
     if (!n)
         return AVBD_OK;
     CHECK(stage_reserve(ctx, (size_t)(floats + 3) / 4));
+    CHECK(reserve(ctx, ctx->stateStage, (size_t)std::max<long long>(floats, 1), false));
     float *st = (float *)ctx->hStage;
     std::vector<HostCopy> copies;
+    bool staged = false;
     for (int f = 0; f < 5; ++f)
-        if (src[f])
-            copies.push_back({st + P.f[f].offset, src[f], sizeof(float) * width[f] * (size_t)n});
-    copy_host(copies);
-    CHECK(reserve(ctx, ctx->stateStage, (size_t)std::max<long long>(floats, 1), false));
-    if (floats)
-        CU(cudaMemcpyAsync(ctx->stateStage.p, st, sizeof(float) * floats, cudaMemcpyHostToDevice, ctx->stream));
+    {
+        if (!src[f])
+            continue;
+        const size_t bytes = sizeof(float) * width[f] * (size_t)n;
+        if (host_pinned(src[f])) // straight from the caller's page-locked array
+            CU(cudaMemcpyAsync(ctx->stateStage.p + P.f[f].offset, src[f], bytes, cudaMemcpyHostToDevice,
+                               ctx->stream));
+        else
+        {
+            copies.push_back({st + P.f[f].offset, src[f], bytes});
+            staged = true;
+        }
+    }
+    if (staged)
+    {
+        copy_host(copies);
+        for (const HostCopy &c : copies)
+            CU(cudaMemcpyAsync(ctx->stateStage.p + ((const float *)c.dst - st), c.dst, c.bytes,
+                               cudaMemcpyHostToDevice, ctx->stream));
+    }
     CU(cudaEventRecord(ctx->stageDone, ctx->stream));
     k_unpack_state<<<grid_for(n, 256), 256, 0, ctx->stream>>>(P, ctx->stateStage.p, n);
     LAUNCHED();
@@ -2816,12 +2845,23 @@ int avbd_read_bodies(AvbdContext *ctx, const AvbdBodyState *out)
     k_pack_state<<<grid_for(n, 256), 256, 0, ctx->stream>>>(P, ctx->stateStage.p, n);
     LAUNCHED();
     float *st = (float *)ctx->hStage;
-    CU(cudaMemcpyAsync(st, ctx->stateStage.p, sizeof(float) * floats, cudaMemcpyDeviceToHost, ctx->stream));
-    CU(cudaStreamSynchronize(ctx->stream));
     std::vector<HostCopy> copies;
     for (int f = 0; f < MAX_PACKED; ++f)
-        if (dst[f])
-            copies.push_back({dst[f], st + P.f[f].offset, sizeof(float) * width[f] * (size_t)n});
+    {
+        if (!dst[f])
+            continue;
+        const size_t bytes = sizeof(float) * width[f] * (size_t)n;
+        if (host_pinned(dst[f])) // straight into the caller's page-locked array
+            CU(cudaMemcpyAsync(dst[f], ctx->stateStage.p + P.f[f].offset, bytes, cudaMemcpyDeviceToHost,
+                               ctx->stream));
+        else
+        {
+            CU(cudaMemcpyAsync(st + P.f[f].offset, ctx->stateStage.p + P.f[f].offset, bytes, cudaMemcpyDeviceToHost,
+                               ctx->stream));
+            copies.push_back({dst[f], st + P.f[f].offset, bytes});
+        }
+    }
+    CU(cudaStreamSynchronize(ctx->stream));
     copy_host(copies);
     return AVBD_OK;
 }

@@ -1056,7 +1056,7 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
         {
             k_bp_bounds_init<<<grid_for(8ll * ctx->W, 256), 256, 0, ctx->stream>>>(ctx->bounds.p, ctx->W);
             LAUNCHED();
-            k_bp_bounds<<<std::min(grid_for(nB, 256), 148 * 8), 256, 0, ctx->stream>>>(B, G, ctx->binned.p, nB, dt);
+            k_bp_bounds<<<std::min(grid_for(nB, 256), 148 * 2), 256, 0, ctx->stream>>>(B, G, ctx->binned.p, nB, dt);
             LAUNCHED();
             k_bp_params<<<grid_for(ctx->W, 128), 128, 0, ctx->stream>>>(G, ctx->worldBinned.p);
             LAUNCHED();

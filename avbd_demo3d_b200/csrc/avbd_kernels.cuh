@@ -371,46 +371,98 @@ __global__ void k_bp_bounds_init(unsigned *bounds, int W)
 }
 
 // Bounds of each world's binned centres and its largest binned travel slack
-// (solver.cpp:306-333); warps inside one world reduce before their atomics.
-__global__ void k_bp_bounds(DevBodies B, DevGrid G, const int *binned, int nBinned, float dt)
+// (solver.cpp:306-333). Each thread folds its grid-stride items while they stay in one world
+// (bodies of a world are contiguous in the binned list), then warps and the block combine
+// the folds of one world before their atomics: a single world costs one set of atomics per
+// block.
+AVBD_DEV void bounds_reset(unsigned v[7])
 {
-    for (int k0 = blockIdx.x * blockDim.x; k0 < nBinned; k0 += gridDim.x * blockDim.x)
+#pragma unroll
+    for (int d = 0; d < 7; ++d)
+        v[d] = d < 3 ? 0xFFFFFFFFu : 0u;
+}
+AVBD_DEV void bounds_flush(const DevGrid &G, int w, const unsigned v[7])
+{
+    unsigned *bw = G.bounds + 8 * w;
+    for (int d = 0; d < 3; ++d)
+        atomicMin(&bw[d], v[d]);
+    for (int d = 3; d < 7; ++d)
+        atomicMax(&bw[d], v[d]);
+}
+// Warp combine of (world, fold): when every lane with a fold shares one world, the warp's
+// fold ends in every lane and the world is returned; otherwise each lane flushes its own
+// fold and -1 is returned.
+AVBD_DEV int bounds_warp_combine(const DevGrid &G, int w, unsigned v[7])
+{
+    int wref = __reduce_max_sync(0xFFFFFFFFu, w);
+    if (!__all_sync(0xFFFFFFFFu, w == wref || w < 0))
     {
-        int k = k0 + threadIdx.x;
-        bool active = k < nBinned;
-        int b = active ? binned[k] : 0;
-        int w = active ? G.bodyWorld[b] : -1;
-        unsigned v[7] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u, 0u};
-        if (active)
-        {
-            float4 p = B.pos[b];
-            v[0] = v[3] = float_order(p.x);
-            v[1] = v[4] = float_order(p.y);
-            v[2] = v[5] = float_order(p.z);
-            v[6] = __float_as_uint(len(xyz(B.vel[b])) * dt);
-        }
-        int w0 = __shfl_sync(0xFFFFFFFFu, w, 0);
-        bool uniform = __all_sync(0xFFFFFFFFu, w == w0 || w < 0);
-        if (uniform)
-        {
-#pragma unroll
-            for (int d = 0; d < 3; ++d)
-                v[d] = __reduce_min_sync(0xFFFFFFFFu, v[d]);
-#pragma unroll
-            for (int d = 3; d < 7; ++d)
-                v[d] = __reduce_max_sync(0xFFFFFFFFu, v[d]);
-            if ((threadIdx.x & 31) != 0 || w0 < 0)
-                continue;
-            w = w0;
-        }
-        else if (!active)
-            continue;
-        unsigned *bw = G.bounds + 8 * w;
-        for (int d = 0; d < 3; ++d)
-            atomicMin(&bw[d], v[d]);
-        for (int d = 3; d < 7; ++d)
-            atomicMax(&bw[d], v[d]);
+        if (w >= 0)
+            bounds_flush(G, w, v);
+        bounds_reset(v);
+        return -1;
     }
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+        v[d] = __reduce_min_sync(0xFFFFFFFFu, v[d]);
+#pragma unroll
+    for (int d = 3; d < 7; ++d)
+        v[d] = __reduce_max_sync(0xFFFFFFFFu, v[d]);
+    return wref;
+}
+__global__ void __launch_bounds__(256) k_bp_bounds(DevBodies B, DevGrid G, const int *binned, int nBinned, float dt)
+{
+    __shared__ unsigned sv[8][7];
+    __shared__ int sw[8];
+    unsigned v[7];
+    bounds_reset(v);
+    int cw = -1;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nBinned; k += gridDim.x * blockDim.x)
+    {
+        int b = binned[k];
+        int w = G.bodyWorld[b];
+        if (w != cw)
+        {
+            if (cw >= 0)
+                bounds_flush(G, cw, v);
+            bounds_reset(v);
+            cw = w;
+        }
+        float4 p = B.pos[b];
+        unsigned x = float_order(p.x), y = float_order(p.y), z = float_order(p.z);
+        v[0] = min(v[0], x);
+        v[1] = min(v[1], y);
+        v[2] = min(v[2], z);
+        v[3] = max(v[3], x);
+        v[4] = max(v[4], y);
+        v[5] = max(v[5], z);
+        v[6] = max(v[6], __float_as_uint(len(xyz(B.vel[b])) * dt));
+    }
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int ww = bounds_warp_combine(G, cw, v);
+    if (lane == 0)
+    {
+        sw[warp] = ww;
+#pragma unroll
+        for (int d = 0; d < 7; ++d)
+            sv[warp][d] = v[d];
+    }
+    __syncthreads();
+    if (warp != 0)
+        return;
+    int bw = -1;
+    if (lane < (int)(blockDim.x >> 5))
+    {
+        bw = sw[lane];
+#pragma unroll
+        for (int d = 0; d < 7; ++d)
+            v[d] = sv[lane][d];
+    }
+    else
+        bounds_reset(v);
+    bw = bounds_warp_combine(G, bw, v);
+    if (lane == 0 && bw >= 0)
+        bounds_flush(G, bw, v);
 }
 
 // World AABB plus travel slack of the bodies too large for the grid (solver.cpp:311-327)

@@ -1811,65 +1811,103 @@ int stage_reserve(AvbdContext *ctx, size_t count)
 }
 
 // Body state fields in the callers' packed layout: per field n entries of `width` floats
-// (3, or 4 for orientations) at `offset` floats into one buffer (-1: field absent).
+// (3, or 4 for orientations), in a device-usable buffer (the device staging buffer, or the
+// caller's page-locked array through its mapped address; null: field absent).
 struct PackedField
 {
     float4 *arr;
-    long long offset;
+    float *buf;
     int width;
-    float w; // fourth component written for an absent field
+    int aligned; // buf is 16-byte aligned: whole float4 accesses
+    float w;     // fourth component written for an absent field
 };
 
 constexpr int MAX_PACKED = 9;
+constexpr int PACK_BLOCK = 256;
 struct PackedFields
 {
     PackedField f[MAX_PACKED];
     int count;
 };
 
-// Packed caller layout -> the device's float4 arrays (absent fields take (0, 0, 0, w)).
-__global__ void k_unpack_state(PackedFields P, const float *in, int n)
+// Each block moves its bodies' contiguous stretch of a field (PACK_BLOCK entries of `width`
+// floats) between the packed buffer and shared memory in whole, consecutive accesses,
+// float4 when the buffer is aligned, so that a caller's page-locked array crosses the bus
+// in full lines. A block's stretch starts at a multiple of 3,072 or 4,096 bytes.
+AVBD_DEV void packed_load(const PackedField &f, int i0, int cnt, float *s)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
-#pragma unroll
-    for (int k = 0; k < MAX_PACKED; ++k)
+    const float *src = f.buf + (size_t)f.width * i0;
+    const int total = cnt * f.width;
+    if (f.aligned && (total & 3) == 0)
+        for (int t = threadIdx.x; t < total / 4; t += blockDim.x)
+            reinterpret_cast<float4 *>(s)[t] = reinterpret_cast<const float4 *>(src)[t];
+    else
+        for (int t = threadIdx.x; t < total; t += blockDim.x)
+            s[t] = src[t];
+}
+
+AVBD_DEV void packed_store(const PackedField &f, int i0, int cnt, const float *s)
+{
+    float *dst = f.buf + (size_t)f.width * i0;
+    const int total = cnt * f.width;
+    if (f.aligned && (total & 3) == 0)
+        for (int t = threadIdx.x; t < total / 4; t += blockDim.x)
+            reinterpret_cast<float4 *>(dst)[t] = reinterpret_cast<const float4 *>(s)[t];
+    else
+        for (int t = threadIdx.x; t < total; t += blockDim.x)
+            dst[t] = s[t];
+}
+
+// Packed caller layout -> the device's float4 arrays (absent fields take (0, 0, 0, w)).
+__global__ void __launch_bounds__(PACK_BLOCK) k_unpack_state(PackedFields P, int n)
+{
+    __shared__ __align__(16) float s[PACK_BLOCK * 4];
+    const int i0 = blockIdx.x * PACK_BLOCK;
+    const int cnt = min(PACK_BLOCK, n - i0);
+    const int t = threadIdx.x;
+    for (int k = 0; k < P.count; ++k)
     {
-        if (k >= P.count)
-            break;
         const PackedField f = P.f[k];
         float4 v = make_float4(0.0f, 0.0f, 0.0f, f.w);
-        if (f.offset >= 0)
+        if (f.buf) // uniform over the block
         {
-            const float *s = in + f.offset + (size_t)f.width * i;
-            v = f.width == 4 ? make_float4(s[0], s[1], s[2], s[3]) : make_float4(s[0], s[1], s[2], 0.0f);
+            packed_load(f, i0, cnt, s);
+            __syncthreads();
+            if (t < cnt)
+                v = f.width == 4 ? make_float4(s[4 * t], s[4 * t + 1], s[4 * t + 2], s[4 * t + 3])
+                                 : make_float4(s[3 * t], s[3 * t + 1], s[3 * t + 2], 0.0f);
+            __syncthreads();
         }
-        f.arr[i] = v;
+        if (t < cnt)
+            f.arr[i0 + t] = v;
     }
 }
 
 // The device's float4 arrays -> the packed caller layout (requested fields only).
-__global__ void k_pack_state(PackedFields P, float *out, int n)
+__global__ void __launch_bounds__(PACK_BLOCK) k_pack_state(PackedFields P, int n)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
-#pragma unroll
-    for (int k = 0; k < MAX_PACKED; ++k)
+    __shared__ __align__(16) float s[PACK_BLOCK * 4];
+    const int i0 = blockIdx.x * PACK_BLOCK;
+    const int cnt = min(PACK_BLOCK, n - i0);
+    const int t = threadIdx.x;
+    for (int k = 0; k < P.count; ++k)
     {
-        if (k >= P.count)
-            break;
         const PackedField f = P.f[k];
-        if (f.offset < 0)
+        if (!f.buf)
             continue;
-        float4 v = f.arr[i];
-        float *d = out + f.offset + (size_t)f.width * i;
-        d[0] = v.x;
-        d[1] = v.y;
-        d[2] = v.z;
-        if (f.width == 4)
-            d[3] = v.w;
+        if (t < cnt)
+        {
+            const float4 v = f.arr[i0 + t];
+            float *d = s + f.width * t;
+            d[0] = v.x;
+            d[1] = v.y;
+            d[2] = v.z;
+            if (f.width == 4)
+                d[3] = v.w;
+        }
+        __syncthreads();
+        packed_store(f, i0, cnt, s);
+        __syncthreads();
     }
 }
 
@@ -1889,20 +1927,23 @@ void copy_host(const std::vector<HostCopy> &copies)
 }
 
 // A caller array in page-locked host memory (cudaHostAlloc, cudaHostRegister, a pinned
-// torch tensor) is copied to or from the device directly, without the staging copy.
-bool host_pinned(const void *p)
+// torch tensor) that the device can address: the packing kernels read or write it in place,
+// over the bus, with no copy call. Null for any other array.
+float *host_mapped(const void *p)
 {
     cudaPointerAttributes a{};
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess)
     {
         cudaGetLastError();
-        return false;
+        return nullptr;
     }
-    return a.type == cudaMemoryTypeHost;
+    return a.type == cudaMemoryTypeHost ? (float *)a.devicePointer : nullptr;
 }
 
-// Body state from caller arrays: one copy of the packed fields into pinned staging, one
-// asynchronous upload, and the conversion to float4 on the device.
+bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+
+// Body state from caller arrays: page-locked arrays are read in place by the unpacking
+// kernel; any other array is copied into pinned staging and uploaded first.
 int write_state(AvbdContext *ctx, const AvbdBodies *b)
 {
     int n = b->count;
@@ -1913,11 +1954,12 @@ int write_state(AvbdContext *ctx, const AvbdBodies *b)
     PackedFields P{};
     P.count = 5;
     long long floats = 0;
+    float *mapped[5] = {};
     for (int f = 0; f < 5; ++f)
     {
         CHECK(reserve(ctx, *dst[f], std::max(n, 1), false));
-        P.f[f] = PackedField{dst[f]->p, src[f] ? floats : -1, width[f], f == 1 ? 1.0f : 0.0f};
-        if (src[f])
+        mapped[f] = src[f] && n ? host_mapped(src[f]) : nullptr;
+        if (src[f] && !mapped[f])
             floats += (long long)width[f] * n;
     }
     if (!n)
@@ -1926,22 +1968,21 @@ int write_state(AvbdContext *ctx, const AvbdBodies *b)
     CHECK(reserve(ctx, ctx->stateStage, (size_t)std::max<long long>(floats, 1), false));
     float *st = (float *)ctx->hStage;
     std::vector<HostCopy> copies;
-    bool staged = false;
+    long long off = 0;
     for (int f = 0; f < 5; ++f)
     {
-        if (!src[f])
-            continue;
-        const size_t bytes = sizeof(float) * width[f] * (size_t)n;
-        if (host_pinned(src[f])) // straight from the caller's page-locked array
-            CU(cudaMemcpyAsync(ctx->stateStage.p + P.f[f].offset, src[f], bytes, cudaMemcpyHostToDevice,
-                               ctx->stream));
-        else
+        float *buf = nullptr;
+        if (mapped[f])
+            buf = mapped[f];
+        else if (src[f])
         {
-            copies.push_back({st + P.f[f].offset, src[f], bytes});
-            staged = true;
+            copies.push_back({st + off, src[f], sizeof(float) * width[f] * (size_t)n});
+            buf = ctx->stateStage.p + off;
+            off += (long long)width[f] * n;
         }
+        P.f[f] = PackedField{dst[f]->p, buf, width[f], buf ? (int)aligned16(buf) : 0, f == 1 ? 1.0f : 0.0f};
     }
-    if (staged)
+    if (!copies.empty())
     {
         copy_host(copies);
         for (const HostCopy &c : copies)
@@ -1949,7 +1990,7 @@ int write_state(AvbdContext *ctx, const AvbdBodies *b)
                                cudaMemcpyHostToDevice, ctx->stream));
     }
     CU(cudaEventRecord(ctx->stageDone, ctx->stream));
-    k_unpack_state<<<grid_for(n, 256), 256, 0, ctx->stream>>>(P, ctx->stateStage.p, n);
+    k_unpack_state<<<grid_for(n, PACK_BLOCK), PACK_BLOCK, 0, ctx->stream>>>(P, n);
     LAUNCHED();
     return AVBD_OK;
 }
@@ -2828,39 +2869,43 @@ int avbd_read_bodies(AvbdContext *ctx, const AvbdBodyState *out)
     const int width[MAX_PACKED] = {3, 4, 3, 3, 3, 3, 4, 3, 4};
     if (!n)
         return AVBD_OK;
-    // requested fields packed on the device, one download, one copy per field on the host
+    // requested fields packed on the device: written in place into page-locked caller arrays,
+    // the rest downloaded through the staging buffer and copied on the host
     PackedFields P{};
     P.count = MAX_PACKED;
     long long floats = 0;
+    float *mapped[MAX_PACKED] = {};
+    if (std::none_of(dst, dst + MAX_PACKED, [](const float *d) { return d != nullptr; }))
+        return AVBD_OK;
     for (int f = 0; f < MAX_PACKED; ++f)
     {
-        P.f[f] = PackedField{src[f]->p, dst[f] ? floats : -1, width[f], 0.0f};
-        if (dst[f])
+        mapped[f] = dst[f] ? host_mapped(dst[f]) : nullptr;
+        if (dst[f] && !mapped[f])
             floats += (long long)width[f] * n;
     }
-    if (!floats)
-        return AVBD_OK;
     CHECK(stage_reserve(ctx, (size_t)(floats + 3) / 4));
-    CHECK(reserve(ctx, ctx->stateStage, (size_t)floats, false));
-    k_pack_state<<<grid_for(n, 256), 256, 0, ctx->stream>>>(P, ctx->stateStage.p, n);
-    LAUNCHED();
+    CHECK(reserve(ctx, ctx->stateStage, (size_t)std::max<long long>(floats, 1), false));
     float *st = (float *)ctx->hStage;
     std::vector<HostCopy> copies;
+    long long off = 0;
     for (int f = 0; f < MAX_PACKED; ++f)
     {
-        if (!dst[f])
-            continue;
-        const size_t bytes = sizeof(float) * width[f] * (size_t)n;
-        if (host_pinned(dst[f])) // straight into the caller's page-locked array
-            CU(cudaMemcpyAsync(dst[f], ctx->stateStage.p + P.f[f].offset, bytes, cudaMemcpyDeviceToHost,
-                               ctx->stream));
-        else
+        float *buf = nullptr;
+        if (mapped[f])
+            buf = mapped[f];
+        else if (dst[f])
         {
-            CU(cudaMemcpyAsync(st + P.f[f].offset, ctx->stateStage.p + P.f[f].offset, bytes, cudaMemcpyDeviceToHost,
-                               ctx->stream));
-            copies.push_back({dst[f], st + P.f[f].offset, bytes});
+            buf = ctx->stateStage.p + off;
+            copies.push_back({dst[f], st + off, sizeof(float) * width[f] * (size_t)n});
+            off += (long long)width[f] * n;
         }
+        P.f[f] = PackedField{src[f]->p, buf, width[f], buf ? (int)aligned16(buf) : 0, 0.0f};
     }
+    k_pack_state<<<grid_for(n, PACK_BLOCK), PACK_BLOCK, 0, ctx->stream>>>(P, n);
+    LAUNCHED();
+    for (const HostCopy &c : copies)
+        CU(cudaMemcpyAsync((void *)c.src, ctx->stateStage.p + ((const float *)c.src - st), c.bytes,
+                           cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
     copy_host(copies);
     return AVBD_OK;

@@ -3612,11 +3612,11 @@ __global__ void __launch_bounds__(COLOUR_FLOW_BLOCK) k_colour_greedy(
     const int lane = threadIdx.x & 31;
     int mine = 0, maxC = -1, maxR = -1;
     bool failed = false;
-    // Warps take 32 consecutive bodies at a time and colour them in rounds: each round every
-    // waiting lane polls (without blocking) the neighbours it has not seen coloured yet, and
-    // a lane whose lower-index neighbours are all coloured takes its colour. A chain of
-    // neighbours inside the warp advances one link per round; a warp that makes no progress
-    // in a round backs off, and after spinLimit such rounds the wait has expired.
+    // Warps take 32 consecutive bodies at a time and colour them in rounds. A lower-index
+    // neighbour inside the warp is read from its lane by shuffles, so a chain of neighbours
+    // inside the warp advances one link per shuffle pass, all in registers; a neighbour in
+    // another warp is polled (without blocking) in memory once per round. A warp that makes
+    // no progress in a round backs off, and after spinLimit such rounds the wait has expired.
     constexpr int NB = 8; // lower-index neighbours kept in registers (more: rescanned per round)
     for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n && !failed; base += stride)
     {
@@ -3624,9 +3624,12 @@ __global__ void __launch_bounds__(COLOUR_FLOW_BLOCK) k_colour_greedy(
         bool pending = false, many = false;
         int nb[NB];
         int nnb = 0;
-        unsigned seen = 0; // bit k: nb[k]'s colour is in `used`
+        unsigned seen = 0;  // bit k: nb[k]'s colour is in `used`
+        unsigned intra = 0; // bit k: nb[k] is a lane of this warp
         unsigned long long used[4] = {0ull, 0ull, 0ull, 0ull};
         int round = 0;
+        unsigned mine_cr = ~0u; // round << 16 | colour once taken (read by the warp's shuffles)
+        bool publish = false;  // taken in this round, not yet in `state`
         if (v < n)
         {
             pending = B.massMoment[v].x > 0 && F.adjStart[v + 1] > F.adjStart[v];
@@ -3644,84 +3647,124 @@ __global__ void __launch_bounds__(COLOUR_FLOW_BLOCK) k_colour_greedy(
                     if (u < 0 || u >= v || B.massMoment[u].x <= 0)
                         continue;
                     if (nnb < NB)
+                    {
+                        if (u >= base)
+                            intra |= 1u << nnb;
                         nb[nnb++] = u;
+                    }
                     else
                         many = true;
                 }
         }
+        const unsigned all = (1u << nnb) - 1u;
+        // shuffle passes look at the first kIntra neighbours (the warp's largest in-warp one)
+        const int kIntra = __reduce_max_sync(0xFFFFFFFFu, 32 - __clz((int)intra));
+        // takes the smallest colour no lower neighbour uses; `state` is written at the end of
+        // the round, by all lanes that took one together (one release for the warp)
+        auto take = [&]() {
+            int c = 0;
+            while (c < 256 && ((used[c >> 6] >> (c & 63)) & 1ull))
+                c++;
+            if (c >= 256)
+            {
+                cnt->error = DERR_TOO_MANY_COLOURS;
+                c = 255;
+            }
+            __stcg(&colour[v], c);
+            mine++;
+            maxC = max(maxC, c);
+            maxR = max(maxR, round);
+            mine_cr = ((unsigned)min(round, 0xFFFF) << 16) | (unsigned)c;
+            publish = true;
+            pending = false;
+        };
         unsigned idle = 0;
         while (__any_sync(0xFFFFFFFFu, pending))
         {
             bool progressed = false;
-            if (pending)
+            if (pending && !many)
             {
-                bool ready = true;
-                if (!many)
-                {
+                // neighbours in other warps
 #pragma unroll
-                    for (int k = 0; k < NB; ++k)
-                    {
-                        if (k >= nnb || ((seen >> k) & 1u))
-                            continue;
-                        const unsigned long long su = ld_acquire_u64(&state[nb[k]]);
-                        if ((su >> 32) != (unsigned long long)epoch)
-                        {
-                            ready = false;
-                            continue;
-                        }
-                        const int cu = (int)(su & 0xFFFFu), ru = (int)((su >> 16) & 0xFFFFu);
-                        if (cu < 256)
-                            used[cu >> 6] |= 1ull << (cu & 63);
-                        round = max(round, ru + 1);
-                        seen |= 1u << k;
-                    }
-                }
-                else
+                for (int k = 0; k < NB; ++k)
                 {
-                    // more than NB lower neighbours: look at all of them again each round
-                    used[0] = used[1] = used[2] = used[3] = 0ull;
-                    round = 0;
-                    for (int k = F.adjStart[v]; k < F.adjStart[v + 1] && ready; ++k)
+                    if (k >= nnb || (((seen | intra) >> k) & 1u))
+                        continue;
+                    const unsigned long long su = ld_acquire_u64(&state[nb[k]]);
+                    if ((su >> 32) != (unsigned long long)epoch)
+                        continue;
+                    const int cu = (int)(su & 0xFFFFu), ru = (int)((su >> 16) & 0xFFFFu);
+                    if (cu < 256)
+                        used[cu >> 6] |= 1ull << (cu & 63);
+                    round = max(round, ru + 1);
+                    seen |= 1u << k;
+                }
+            }
+            else if (pending)
+            {
+                // more than NB lower neighbours: look at all of them again each round
+                bool ready = true;
+                used[0] = used[1] = used[2] = used[3] = 0ull;
+                round = 0;
+                for (int k = F.adjStart[v]; k < F.adjStart[v + 1] && ready; ++k)
+                {
+                    unsigned e = F.adj[k];
+                    if (adj_type(e) == ADJ_IGNORE)
+                        continue;
+                    int2 ab = force_bodies(F, e);
+                    int u = ab.x == v ? ab.y : ab.x;
+                    if (u < 0 || u >= v || B.massMoment[u].x <= 0)
+                        continue;
+                    const unsigned long long su = ld_acquire_u64(&state[u]);
+                    if ((su >> 32) != (unsigned long long)epoch)
                     {
-                        unsigned e = F.adj[k];
-                        if (adj_type(e) == ADJ_IGNORE)
-                            continue;
-                        int2 ab = force_bodies(F, e);
-                        int u = ab.x == v ? ab.y : ab.x;
-                        if (u < 0 || u >= v || B.massMoment[u].x <= 0)
-                            continue;
-                        const unsigned long long su = ld_acquire_u64(&state[u]);
-                        if ((su >> 32) != (unsigned long long)epoch)
-                        {
-                            ready = false;
-                            break;
-                        }
-                        const int cu = (int)(su & 0xFFFFu), ru = (int)((su >> 16) & 0xFFFFu);
-                        if (cu < 256)
-                            used[cu >> 6] |= 1ull << (cu & 63);
-                        round = max(round, ru + 1);
+                        ready = false;
+                        break;
                     }
+                    const int cu = (int)(su & 0xFFFFu), ru = (int)((su >> 16) & 0xFFFFu);
+                    if (cu < 256)
+                        used[cu >> 6] |= 1ull << (cu & 63);
+                    round = max(round, ru + 1);
                 }
                 if (ready)
                 {
-                    int c = 0;
-                    while (c < 256 && ((used[c >> 6] >> (c & 63)) & 1ull))
-                        c++;
-                    if (c >= 256)
-                    {
-                        cnt->error = DERR_TOO_MANY_COLOURS;
-                        c = 255;
-                    }
-                    st_release_u64(&state[v], ((unsigned long long)epoch << 32) |
-                                                  ((unsigned long long)min(round, 0xFFFF) << 16) |
-                                                  (unsigned long long)c);
-                    __stcg(&colour[v], c);
-                    mine++;
-                    maxC = max(maxC, c);
-                    maxR = max(maxR, round);
-                    pending = false;
+                    take();
                     progressed = true;
                 }
+            }
+            // neighbours inside the warp: shuffle passes while any lane takes a colour
+            for (;;)
+            {
+                bool took = false;
+#pragma unroll
+                for (int k = 0; k < NB; ++k)
+                {
+                    if (k >= kIntra) // warp-uniform
+                        break;
+                    const bool in = (intra >> k) & 1u;
+                    const int src = in ? nb[k] - base : lane;
+                    const unsigned cr = __shfl_sync(0xFFFFFFFFu, mine_cr, src);
+                    if (pending && !many && in && !((seen >> k) & 1u) && cr != ~0u)
+                    {
+                        const int cu = (int)(cr & 0xFFFFu);
+                        used[cu >> 6] |= 1ull << (cu & 63);
+                        round = max(round, (int)(cr >> 16) + 1);
+                        seen |= 1u << k;
+                    }
+                }
+                if (pending && !many && seen == all)
+                {
+                    take();
+                    took = true;
+                    progressed = true;
+                }
+                if (!__any_sync(0xFFFFFFFFu, took))
+                    break;
+            }
+            if (publish)
+            {
+                st_release_u64(&state[v], ((unsigned long long)epoch << 32) | (unsigned long long)mine_cr);
+                publish = false;
             }
             if (__any_sync(0xFFFFFFFFu, progressed))
             {

@@ -54,8 +54,8 @@ def measured_peak():
 # the kernel's source files at capture time: when the sources have changed since, the
 # figure no longer describes the kernel and the line reports no traffic.
 NCU_TRAFFIC = {
-    "k_iterations": {"bytes_per_launch": 31094528, "summary": "profiles/iterations_stacks65k_ncu.txt",
-                     "captured": "2026-12-04", "sources_sha": ""},
+    "k_iterations": {"bytes_per_launch": 31351296, "summary": "profiles/iterations_stacks65k_ncu.txt",
+                     "captured": "2026-12-04", "sources_sha": "3fe84d6fc1737e2b"},
     "k_primal": {"bytes_per_launch": None, "summary": "profiles/primal_stacks65k_ncu.txt",
                  "captured": "2026-12-04", "sources_sha": ""},
 }
@@ -254,9 +254,9 @@ def run_cuda(args):
     e2e_max = max_over_ranks(e2e_s, device=f"cuda:{local}")
     e2e = {"value": world_size * bodies * e2e_steps / e2e_max, "unit": UNIT, "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h, "steps": e2e_steps,
-           "path": "avbd_write_bodies (H2D straight from the caller's page-locked arrays) + avbd_step + "
-                   "avbd_read_bodies (D2H straight into them); arrays allocated once, reused every step; host "
-                   "timer"}
+           "path": "avbd_write_bodies (a kernel reads the caller's page-locked arrays in place over the bus) + "
+                   "avbd_step + avbd_read_bodies (a kernel writes them in place); arrays allocated once, reused "
+                   "every step; host timer"}
 
     # the end of the configuration's 300 steps, timed the same way (the stacks have settled)
     late = None

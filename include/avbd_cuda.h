@@ -242,10 +242,11 @@ int avbd_load_batch(AvbdContext *ctx, int32_t num_worlds, const int32_t *world_s
 
 /* Overwrite body state only (positions/orientations/velocities edited between steps,
  * e.g. scenes.h:45). Same layout and order as avbd_load_world's bodies. Arrays in
- * page-locked host memory are uploaded directly and asynchronously: keep them unchanged
- * until the next call that waits for the device (a read, avbd_synchronize); other arrays
- * are copied before the call returns. avbd_read_bodies likewise writes page-locked arrays
- * directly. */
+ * page-locked host memory that the device can address (cudaHostAlloc, cudaHostRegister, a
+ * pinned torch tensor) are read in place by a kernel on the context stream, asynchronously:
+ * keep them unchanged until the next call that waits for the device (a read,
+ * avbd_synchronize); other arrays are copied before the call returns. avbd_read_bodies
+ * likewise has its kernel write page-locked arrays in place before it returns. */
 int avbd_write_bodies(AvbdContext *ctx, const AvbdBodies *bodies);
 
 /* Solver::step() for nsteps steps (solver.cpp:934-937 via stepCpuReference 1036-1041).

@@ -183,6 +183,13 @@ struct AvbdContext
     int nColours = 0, nSolve = 0;
 
     DArr<char> cubTemp;
+    // Broadphase side streams: side[0] builds the pair set, the large bodies' boxes and the
+    // large-large pass, side[1] the large bodies' cell lists, while the context stream bins
+    // and sorts the grid entries; events fork and join them (sideEv) and each side stream
+    // has its own cub scratch.
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t sideEv[6] = {};
+    DArr<char> cubTempSide[2];
     DArr<StepCounters> counters;
     StepCounters *hCounters = nullptr;
     long long *hScalars = nullptr; // pinned scratch for small readbacks
@@ -777,31 +784,43 @@ void host_grid_cap(GridParams &g)
 // Large bodies binned into the grid cells of their world that their inflated AABB touches:
 // sorted (world, cell, index) keys and a hash table of run starts, including each world's
 // global run for bodies spanning too many cells.
-int large_cell_lists(AvbdContext *ctx, int nL)
+// keys: world | global (1) | cell (22) | large index (24), written large body by large body:
+// the stable sort orders (world, global, cell) only and keeps each run in large-index order.
+// Unused slots (all ones) still sort last.
+int large_sort_end(const AvbdContext *ctx) { return 47 + std::max(1, bit_width((unsigned long long)(ctx->W - 1))); }
+
+// cub scratch the large bodies' cell-list sort needs (reserved before the lists are built
+// on a side stream)
+size_t large_sort_bytes(AvbdContext *ctx, int nL)
+{
+    if (!nL)
+        return 0;
+    cub::DoubleBuffer<unsigned long long> lk(ctx->largeKeys.p, ctx->largeKeysAlt.p);
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortKeys(nullptr, bytes, lk, nL * LARGE_MAX_CELLS, 24, large_sort_end(ctx));
+    return bytes;
+}
+
+// The large bodies' cell lists on stream s, with scratch `temp` already reserved for
+// large_sort_bytes (no allocation here: s may be a side stream).
+int large_cell_lists(AvbdContext *ctx, int nL, cudaStream_t s, DArr<char> &temp)
 {
     ctx->largeSorted = ctx->largeKeys.p;
     if (!nL)
         return AVBD_OK;
     int total = nL * LARGE_MAX_CELLS;
-    k_bp_large_cells<<<grid_for(nL, 128), 128, 0, ctx->stream>>>(dev_grid(ctx), ctx->large.p, ctx->largeLo.p,
-                                                                   ctx->largeHi.p, nL, ctx->largeKeys.p);
+    k_bp_large_cells<<<grid_for(nL, 128), 128, 0, s>>>(dev_grid(ctx), ctx->large.p, ctx->largeLo.p, ctx->largeHi.p,
+                                                       nL, ctx->largeKeys.p);
     LAUNCHED();
     cub::DoubleBuffer<unsigned long long> lk(ctx->largeKeys.p, ctx->largeKeysAlt.p);
-    size_t bytes = 0;
-    // keys: world | global (1) | cell (22) | large index (24), written large body by large
-    // body: the stable sort orders (world, global, cell) only and keeps each run in large-index
-    // order. Unused slots (all ones) still sort last.
-    const int largeEnd = 47 + std::max(1, bit_width((unsigned long long)(ctx->W - 1)));
-    cub::DeviceRadixSort::SortKeys(nullptr, bytes, lk, total, 24, largeEnd, ctx->stream);
-    CHECK(ensure_temp(ctx, bytes));
-    CU(cub::DeviceRadixSort::SortKeys(ctx->cubTemp.p, bytes, lk, total, 24, largeEnd, ctx->stream));
+    size_t bytes = temp.cap;
+    CU(cub::DeviceRadixSort::SortKeys(temp.p, bytes, lk, total, 24, large_sort_end(ctx), s));
     ctx->launches++;
     ctx->largeSorted = lk.Current();
     // sentinel after the sorted keys: candidate walks stop at it
-    CU(cudaMemsetAsync(lk.Current() + total, 0xFF, sizeof(unsigned long long), ctx->stream));
-    CU(cudaMemsetAsync(ctx->largeHashKeys.p, 0xFF, sizeof(unsigned long long) * ((size_t)ctx->largeHashMask + 1),
-                       ctx->stream));
-    k_bp_hash_large_runs<<<grid_for(total, 256), 256, 0, ctx->stream>>>(lk.Current(), total, large_hash(ctx));
+    CU(cudaMemsetAsync(lk.Current() + total, 0xFF, sizeof(unsigned long long), s));
+    CU(cudaMemsetAsync(ctx->largeHashKeys.p, 0xFF, sizeof(unsigned long long) * ((size_t)ctx->largeHashMask + 1), s));
+    k_bp_hash_large_runs<<<grid_for(total, 256), 256, 0, s>>>(lk.Current(), total, large_hash(ctx));
     LAUNCHED();
     return AVBD_OK;
 }
@@ -961,35 +980,69 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
         const bool lbvh = mode == AVBD_BROADPHASE_LBVH;
         const int nB = (int)ctx->hBinned.size(), nL = (int)ctx->hLarge.size();
         const int nItems = (int)ctx->hLLItems.size();
+        // Three streams: the context stream bins and sorts the grid entries and counts their
+        // pairs; side[0] builds the pair set, the large bodies' boxes and the large-large
+        // pass; side[1] the large bodies' cell lists (after the grid parameters and the
+        // boxes). Every buffer the side streams touch is reserved before they fork, since
+        // growth is ordered on the context stream.
+        cudaStream_t M = ctx->stream, S1 = ctx->side[0], S2 = ctx->side[1];
+        cudaEvent_t evFork = ctx->sideEv[0], evPairSet = ctx->sideEv[1], evLarge = ctx->sideEv[2],
+                    evParams = ctx->sideEv[3], evLists = ctx->sideEv[4], evLL = ctx->sideEv[5];
+        StepState *stp = deviceCounts ? ctx->stepState.p : nullptr;
         // the body pairs the existing forces link (constrainedTo by one hash probe run)
         PairSet S;
+        const long long forces = (long long)(deviceCounts ? man_capacity(ctx) : (size_t)ctx->nMan) + ctx->nJoint +
+                                 ctx->nSpring + ctx->nIgnore;
+        unsigned long long slots = 1024;
+        while (slots < 2ull * (unsigned long long)forces)
+            slots <<= 1;
+        CHECK(reserve(ctx, ctx->pairSetKeys, (size_t)slots, false));
+        S.keys = ctx->pairSetKeys.p;
+        S.mask = (unsigned)(slots - 1);
+        if (nItems > 0)
         {
-            const long long forces = (long long)(deviceCounts ? man_capacity(ctx) : (size_t)ctx->nMan) +
-                                     ctx->nJoint + ctx->nSpring + ctx->nIgnore;
-            unsigned long long slots = 1024;
-            while (slots < 2ull * (unsigned long long)forces)
-                slots <<= 1;
-            CHECK(reserve(ctx, ctx->pairSetKeys, (size_t)slots, false));
-            CU(cudaMemsetAsync(ctx->pairSetKeys.p, 0xFF, sizeof(unsigned long long) * slots, ctx->stream));
-            S.keys = ctx->pairSetKeys.p;
-            S.mask = (unsigned)(slots - 1);
-            k_pair_set<<<grid_for(std::max(forces, 1ll), 256), 256, 0, ctx->stream>>>(
-                dev_forces(ctx), S, deviceCounts ? ctx->stepState.p : nullptr);
-            LAUNCHED();
+            CHECK(reserve(ctx, ctx->llChunkLo, (size_t)nL, false));
+            CHECK(reserve(ctx, ctx->llChunkHi, (size_t)nL, false));
+            CHECK(reserve(ctx, ctx->llRecorded, (size_t)nItems * LL_SLOTS, false));
+            size_t bytes = 0;
+            cub::DeviceScan::ExclusiveSum(nullptr, bytes, ctx->llCount.p, ctx->llOffset.p, nItems);
+            CHECK(reserve(ctx, ctx->cubTempSide[0], std::max<size_t>(bytes, 16), false));
         }
-        if (nL)
-        {
-            k_bp_large<<<grid_for(nL, 64), 64, 0, ctx->stream>>>(B, ctx->large.p, nL, dt, ctx->largeLo.p,
-                                                                  ctx->largeHi.p, ctx->largeSphere.p);
-            LAUNCHED();
-        }
+        if (nB && nL)
+            CHECK(reserve(ctx, ctx->cubTempSide[1], std::max<size_t>(large_sort_bytes(ctx, nL), 16), false));
         cub::DoubleBuffer<unsigned long long> dk(ctx->bpKeys.p, ctx->bpKeysAlt.p);
         ctx->hScalars[0] = 0;
         ctx->hScalars[1] = 0;
         DevForces F = dev_forces(ctx);
-        // keys -> sorted entries -> cell runs -> large-body lists -> counted new pairs
-        auto counting_pass = [&]() -> int {
-            k_bp_keys<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(B, G, ctx->binned.p, nB, ctx->bpKeys.p);
+        // the large-large pass on stream s: chunk bounds, counts (and records), offsets
+        auto large_large_count = [&](cudaStream_t s) -> int {
+            if (nItems > 0)
+            {
+                k_ll_chunk_init<<<grid_for(nL, 256), 256, 0, s>>>(ctx->llChunkLo.p, ctx->llChunkHi.p, nL);
+                LAUNCHED();
+                k_ll_chunk_bounds<<<grid_for(nL, 128), 128, 0, s>>>(G, ctx->large.p, ctx->largeSphere.p, nL,
+                                                                    ctx->llChunkLo.p, ctx->llChunkHi.p);
+                LAUNCHED();
+                k_bp_large_large<BP_COUNT><<<grid_for(nItems, 128), 128, 0, s>>>(
+                    F, ctx->large.p, ctx->largeSphere.p, ctx->llItems.p, nItems, ctx->llCount.p, nullptr, 0, 0, cnt,
+                    nullptr, ctx->llChunkLo.p, ctx->llChunkHi.p, ctx->llRecorded.p, S);
+                LAUNCHED();
+                size_t bytes = ctx->cubTempSide[0].cap;
+                CU(cub::DeviceScan::ExclusiveSum(ctx->cubTempSide[0].p, bytes, ctx->llCount.p, ctx->llOffset.p, nItems,
+                                                 s));
+                ctx->launches++;
+                if (!deviceCounts)
+                {
+                    k_total<<<1, 1, 0, s>>>(ctx->llOffset.p, ctx->llCount.p, nItems, ctx->hScalars + 1);
+                    LAUNCHED();
+                }
+            }
+            return AVBD_OK;
+        };
+        // keys -> sorted entries -> cell runs -> counted new pairs, on the context stream;
+        // the pair set and (waitLists) the large bodies' cell lists are waited for first
+        auto counting_pass = [&](bool waitLists) -> int {
+            k_bp_keys<<<grid_for(nB, 256), 256, 0, M>>>(B, G, ctx->binned.p, nB, ctx->bpKeys.p);
             LAUNCHED();
             dk = cub::DoubleBuffer<unsigned long long>(ctx->bpKeys.p, ctx->bpKeysAlt.p);
             size_t bytes = 0;
@@ -998,19 +1051,21 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
             // radix sort is stable, so ordering the (world, cell) bits alone leaves every cell's
             // entries in body order: 3 passes for one world instead of 6.
             int gridEnd = 46 + bit_width((unsigned long long)(ctx->W - 1));
-            cub::DeviceRadixSort::SortKeys(nullptr, bytes, dk, nB, 24, gridEnd, ctx->stream);
+            cub::DeviceRadixSort::SortKeys(nullptr, bytes, dk, nB, 24, gridEnd, M);
             CHECK(ensure_temp(ctx, bytes));
-            CU(cub::DeviceRadixSort::SortKeys(ctx->cubTemp.p, bytes, dk, nB, 24, gridEnd, ctx->stream));
+            CU(cub::DeviceRadixSort::SortKeys(ctx->cubTemp.p, bytes, dk, nB, 24, gridEnd, M));
             ctx->launches++;
             CU(cudaMemsetAsync(ctx->cellHashKeys.p, 0xFF,
-                               sizeof(unsigned long long) * ((size_t)ctx->cellHashMask + 1), ctx->stream));
-            k_bp_hash_runs<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(dk.Current(), nB, cell_hash(ctx));
+                               sizeof(unsigned long long) * ((size_t)ctx->cellHashMask + 1), M));
+            k_bp_hash_runs<<<grid_for(nB, 256), 256, 0, M>>>(dk.Current(), nB, cell_hash(ctx));
             LAUNCHED();
-            CHECK(large_cell_lists(ctx, nL));
             CHECK(reserve(ctx, ctx->pairRecorded, (size_t)nB * BP_LANES * BP_SLOTS, false));
             CHECK(reserve(ctx, ctx->pairLaneCount, (size_t)nB * BP_LANES, false));
+            if (waitLists)
+                CU(cudaStreamWaitEvent(M, evLists, 0));
+            CU(cudaStreamWaitEvent(M, evPairSet, 0));
             // LBVH mode: the grid pass counts the large-body part only; the tree finds the rest
-            k_bp_pairs<BP_COUNT><<<grid_for((long long)nB * BP_LANES, 128), 128, 0, ctx->stream>>>(
+            k_bp_pairs<BP_COUNT><<<grid_for((long long)nB * BP_LANES, 128), 128, 0, M>>>(
                 B, F, G, dk.Current(), nB, cell_hash(ctx), ctx->large.p, ctx->largeLo.p, ctx->largeHi.p,
                 ctx->largeSorted, large_hash(ctx), dt, ctx->pairCount.p, nullptr, 0, 0, cnt, ctx->pairRecorded.p,
                 ctx->pairLaneCount.p, nullptr, S, lbvh ? (1u << 14) : 0x7FFFu);
@@ -1021,48 +1076,50 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
             ctx->launches++;
             if (!deviceCounts)
             {
-                k_total<<<1, 1, 0, ctx->stream>>>(ctx->pairOffset.p, ctx->pairCount.p, nB, ctx->hScalars);
+                k_total<<<1, 1, 0, M>>>(ctx->pairOffset.p, ctx->pairCount.p, nB, ctx->hScalars);
                 LAUNCHED();
             }
             return AVBD_OK;
         };
-        auto large_large_count = [&]() -> int {
-            if (nItems > 0)
-            {
-                CHECK(reserve(ctx, ctx->llChunkLo, (size_t)nL, false));
-                CHECK(reserve(ctx, ctx->llChunkHi, (size_t)nL, false));
-                CHECK(reserve(ctx, ctx->llRecorded, (size_t)nItems * LL_SLOTS, false));
-                k_ll_chunk_init<<<grid_for(nL, 256), 256, 0, ctx->stream>>>(ctx->llChunkLo.p, ctx->llChunkHi.p, nL);
-                LAUNCHED();
-                k_ll_chunk_bounds<<<grid_for(nL, 128), 128, 0, ctx->stream>>>(G, ctx->large.p, ctx->largeSphere.p, nL,
-                                                                               ctx->llChunkLo.p, ctx->llChunkHi.p);
-                LAUNCHED();
-                k_bp_large_large<BP_COUNT><<<grid_for(nItems, 128), 128, 0, ctx->stream>>>(
-                    F, ctx->large.p, ctx->largeSphere.p, ctx->llItems.p, nItems, ctx->llCount.p, nullptr, 0, 0, cnt,
-                    nullptr, ctx->llChunkLo.p, ctx->llChunkHi.p, ctx->llRecorded.p, S);
-                LAUNCHED();
-                CHECK(scan_counts(ctx, ctx->llCount.p, ctx->llOffset.p, nItems, 0));
-                ctx->launches++;
-                if (!deviceCounts)
-                {
-                    k_total<<<1, 1, 0, ctx->stream>>>(ctx->llOffset.p, ctx->llCount.p, nItems, ctx->hScalars + 1);
-                    LAUNCHED();
-                }
-            }
-            return AVBD_OK;
-        };
-        CU(cudaMemsetAsync(ctx->cappedAny.p, 0, sizeof(int), ctx->stream));
+        // side[0]: pair set, large boxes, large-large pass
+        CU(cudaEventRecord(evFork, M));
+        CU(cudaStreamWaitEvent(S1, evFork, 0));
+        CU(cudaMemsetAsync(ctx->pairSetKeys.p, 0xFF, sizeof(unsigned long long) * slots, S1));
+        k_pair_set<<<grid_for(std::max(forces, 1ll), 256), 256, 0, S1>>>(dev_forces(ctx), S, stp);
+        LAUNCHED();
+        CU(cudaEventRecord(evPairSet, S1));
+        if (nL)
+        {
+            k_bp_large<<<grid_for(nL, 64), 64, 0, S1>>>(B, ctx->large.p, nL, dt, ctx->largeLo.p, ctx->largeHi.p,
+                                                        ctx->largeSphere.p);
+            LAUNCHED();
+        }
+        CU(cudaEventRecord(evLarge, S1));
+        CHECK(large_large_count(S1));
+        CU(cudaEventRecord(evLL, S1));
+        // context stream: bounds and grid parameters, then (side[1]) the large cell lists
+        // beside the grid entries' sort
+        CU(cudaMemsetAsync(ctx->cappedAny.p, 0, sizeof(int), M));
+        ctx->largeSorted = ctx->largeKeys.p;
         if (nB)
         {
-            k_bp_bounds_init<<<grid_for(8ll * ctx->W, 256), 256, 0, ctx->stream>>>(ctx->bounds.p, ctx->W);
+            k_bp_bounds_init<<<grid_for(8ll * ctx->W, 256), 256, 0, M>>>(ctx->bounds.p, ctx->W);
             LAUNCHED();
-            k_bp_bounds<<<std::min(grid_for(nB, 256), 148 * 2), 256, 0, ctx->stream>>>(B, G, ctx->binned.p, nB, dt);
+            k_bp_bounds<<<std::min(grid_for(nB, 256), 148 * 2), 256, 0, M>>>(B, G, ctx->binned.p, nB, dt);
             LAUNCHED();
-            k_bp_params<<<grid_for(ctx->W, 128), 128, 0, ctx->stream>>>(G, ctx->worldBinned.p);
+            k_bp_params<<<grid_for(ctx->W, 128), 128, 0, M>>>(G, ctx->worldBinned.p);
             LAUNCHED();
-            CHECK(counting_pass());
+            if (nL)
+            {
+                CU(cudaEventRecord(evParams, M));
+                CU(cudaStreamWaitEvent(S2, evParams, 0));
+                CU(cudaStreamWaitEvent(S2, evLarge, 0));
+                CHECK(large_cell_lists(ctx, nL, S2, ctx->cubTempSide[1]));
+                CU(cudaEventRecord(evLists, S2));
+            }
+            CHECK(counting_pass(nL > 0));
         }
-        CHECK(large_large_count());
+        CU(cudaStreamWaitEvent(M, evLL, 0)); // join: everything side[0] made
         if (deviceCounts)
         {
             StepState *st = ctx->stepState.p;
@@ -1103,8 +1160,11 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
             CU(cudaMemcpyAsync(ctx->grid.p, ctx->hGrid, sizeof(GridParams) * ctx->W, cudaMemcpyHostToDevice,
                                ctx->stream));
             CU(cudaMemsetAsync(cnt, 0, sizeof(StepCounters), ctx->stream));
-            CHECK(counting_pass());
-            CHECK(large_large_count());
+            // the recount runs on the context stream alone (every side stream has joined)
+            if (nL)
+                CHECK(large_cell_lists(ctx, nL, M, ctx->cubTempSide[1]));
+            CHECK(counting_pass(false));
+            CHECK(large_large_count(M));
             CU(cudaMemcpyAsync(ctx->hCounters, cnt, sizeof(StepCounters), cudaMemcpyDeviceToHost, ctx->stream));
             CU(cudaStreamSynchronize(ctx->stream));
             ctx->stats.grid_rescaled = 1;
@@ -2202,6 +2262,20 @@ int avbd_create(AvbdContext **out, int32_t device_ordinal, void *cuda_stream)
         avbd_destroy(ctx);
         return AVBD_ERR_CUDA;
     }
+    for (cudaStream_t &sd : ctx->side)
+        if (cudaStreamCreateWithFlags(&sd, cudaStreamNonBlocking) != cudaSuccess)
+        {
+            sd = nullptr;
+            avbd_destroy(ctx);
+            return AVBD_ERR_CUDA;
+        }
+    for (cudaEvent_t &e : ctx->sideEv)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+        {
+            e = nullptr;
+            avbd_destroy(ctx);
+            return AVBD_ERR_CUDA;
+        }
     memset(ctx->hCounters, 0, sizeof(StepCounters));
     memset(ctx->hState, 0, sizeof(StepState));
     *ctx->hIterError = 0;
@@ -2256,6 +2330,9 @@ void avbd_destroy(AvbdContext *ctx)
     cudaSetDevice(ctx->device);
     if (ctx->stream)
         cudaStreamSynchronize(ctx->stream);
+    for (cudaStream_t sd : ctx->side)
+        if (sd)
+            cudaStreamSynchronize(sd);
     adjoint_release(ctx);
     for (DArr<float4> *a : {&ctx->pos, &ctx->quat, &ctx->initLin, &ctx->initAng, &ctx->inertLin, &ctx->inertAng,
                             &ctx->dqLin, &ctx->dqAng, &ctx->initAngInv, &ctx->inertAngInv,
@@ -2343,6 +2420,8 @@ void avbd_destroy(AvbdContext *ctx)
     release(ctx->colKeys);
     release(ctx->colKeysAlt);
     release(ctx->cubTemp);
+    release(ctx->cubTempSide[0]);
+    release(ctx->cubTempSide[1]);
     release(ctx->counters);
     release(ctx->stepState);
     release(ctx->llChunkLo);
@@ -2389,6 +2468,12 @@ void avbd_destroy(AvbdContext *ctx)
         cudaEventDestroy(ctx->evStart);
     if (ctx->evStop)
         cudaEventDestroy(ctx->evStop);
+    for (cudaEvent_t e : ctx->sideEv)
+        if (e)
+            cudaEventDestroy(e);
+    for (cudaStream_t sd : ctx->side)
+        if (sd)
+            cudaStreamDestroy(sd);
     if (ctx->pool)
         cudaMemPoolDestroy(ctx->pool);
     if (ctx->ownStream && ctx->stream)

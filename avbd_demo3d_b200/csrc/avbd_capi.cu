@@ -183,12 +183,13 @@ struct AvbdContext
     int nColours = 0, nSolve = 0;
 
     DArr<char> cubTemp;
-    // Broadphase side streams: side[0] builds the pair set, the large bodies' boxes and the
-    // large-large pass, side[1] the large bodies' cell lists, while the context stream bins
-    // and sorts the grid entries; events fork and join them (sideEv) and each side stream
-    // has its own cub scratch.
-    cudaStream_t side[2] = {nullptr, nullptr};
-    cudaEvent_t sideEv[6] = {};
+    // Side streams of a device step: side[0] builds the pair set, the large bodies' boxes and
+    // the large-large pass, side[1] the large bodies' cell lists, while the context stream
+    // bins and sorts the grid entries; side[2] initialises the manifolds that existed before
+    // the step meanwhile. Events fork and join them (sideEv; 6 and 7 for side[2]) and the
+    // broadphase's side streams have their own cub scratch.
+    cudaStream_t side[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t sideEv[8] = {};
     DArr<char> cubTempSide[2];
     DArr<StepCounters> counters;
     StepCounters *hCounters = nullptr;
@@ -1204,6 +1205,37 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
 // capacity, the live count comes from the step state, and the compaction records the
 // surviving count there. Joints need no compaction here: a step starts only when none is
 // broken (k_step_begin), and a joint breaks only in the iterations.
+// Manifold::initialize of the manifolds that existed before a device step needs nothing
+// from the step's broadphase: it runs on side[2] beside it, reading the live buffer and
+// writing the updated records into the other one, so a step that stops at its commit leaves
+// the live buffer as it was. init_forces_device joins it, initialises the new pairs the same
+// way and compacts the kept manifolds back into the live buffer.
+int init_old_manifolds(AvbdContext *ctx)
+{
+    const int M = (int)man_capacity(ctx), J = ctx->nJoint;
+    const int need = std::max(std::max(M, J), 1);
+    CHECK(reserve(ctx, ctx->keep, (size_t)need, false));
+    CHECK(reserve(ctx, ctx->keepIdx, (size_t)need * 2, false));
+    if (!M)
+        return AVBD_OK;
+    cudaStream_t s = ctx->side[2];
+    CU(cudaEventRecord(ctx->sideEv[6], ctx->stream));
+    CU(cudaStreamWaitEvent(s, ctx->sideEv[6], 0));
+    DevBodies B = dev_bodies(ctx);
+    Params P = dev_params(ctx->params);
+    DevManifolds Md = dev_man(ctx->man[ctx->cur]), Mo = dev_man(ctx->man[ctx->cur ^ 1]);
+    int *orphans = &ctx->counters.p->orphans;
+    if (ctx->hasShapes)
+        k_manifold_init<true><<<grid_for(M, 128), 128, 0, s>>>(B, Md, M, P, ctx->keep.p, ctx->stepState.p,
+                                                               ExternalContacts(), orphans, Mo, INIT_OLD);
+    else
+        k_manifold_init<false><<<grid_for(M, 128), 128, 0, s>>>(B, Md, M, P, ctx->keep.p, ctx->stepState.p,
+                                                                ExternalContacts(), orphans, Mo, INIT_OLD);
+    LAUNCHED();
+    CU(cudaEventRecord(ctx->sideEv[7], s));
+    return AVBD_OK;
+}
+
 int init_forces_device(AvbdContext *ctx)
 {
     DevBodies B = dev_bodies(ctx);
@@ -1211,30 +1243,28 @@ int init_forces_device(AvbdContext *ctx)
     StepState *st = ctx->stepState.p;
     const int M = (int)man_capacity(ctx), J = ctx->nJoint;
     const int need = std::max(std::max(M, J), 1);
-    CHECK(reserve(ctx, ctx->keep, (size_t)need, false));
-    CHECK(reserve(ctx, ctx->keepIdx, (size_t)need * 2, false));
     int *idx = ctx->keepIdx.p;
     int *cnt32 = ctx->keepIdx.p + need;
     if (M)
     {
-        DevManifolds Md = dev_man(ctx->man[ctx->cur]);
+        DevManifolds Md = dev_man(ctx->man[ctx->cur]), Mo = dev_man(ctx->man[ctx->cur ^ 1]);
+        int *orphans = &ctx->counters.p->orphans;
+        CU(cudaStreamWaitEvent(ctx->stream, ctx->sideEv[7], 0)); // the manifolds from before the step
         if (ctx->hasShapes)
-            k_manifold_init<true><<<grid_for(M, 128), 128, 0, ctx->stream>>>(B, Md, M, P, ctx->keep.p, st,
-                                                                            ExternalContacts(),
-                                                                            &ctx->counters.p->orphans);
+            k_manifold_init<true><<<grid_for(M, 128), 128, 0, ctx->stream>>>(
+                B, Md, M, P, ctx->keep.p, st, ExternalContacts(), orphans, Mo, INIT_NEW);
         else
-            k_manifold_init<false><<<grid_for(M, 128), 128, 0, ctx->stream>>>(B, Md, M, P, ctx->keep.p, st,
-                                                                             ExternalContacts(),
-                                                                             &ctx->counters.p->orphans);
+            k_manifold_init<false><<<grid_for(M, 128), 128, 0, ctx->stream>>>(
+                B, Md, M, P, ctx->keep.p, st, ExternalContacts(), orphans, Mo, INIT_NEW);
         LAUNCHED();
         k_u8_to_int<<<grid_for(M, 256), 256, 0, ctx->stream>>>(ctx->keep.p, cnt32, M, st);
         LAUNCHED();
         CHECK(scan_counts(ctx, cnt32, idx, M, 0));
         ctx->launches++;
-        k_manifold_compact<<<grid_for((long long)M * COMPACT_LANES, 128), 128, 0, ctx->stream>>>(Md, dev_man(ctx->man[ctx->cur ^ 1]), M,
-                                                                      ctx->keep.p, idx, st);
+        // back into the live buffer: no swap
+        k_manifold_compact<<<grid_for((long long)M * COMPACT_LANES, 128), 128, 0, ctx->stream>>>(
+            Mo, Md, M, ctx->keep.p, idx, st, false);
         LAUNCHED();
-        ctx->cur ^= 1;
     }
     if (J)
     {
@@ -1738,6 +1768,7 @@ int step_device(AvbdContext *ctx)
         k_step_begin<<<grid_for(std::max(std::max(ctx->n, J), 1), 256), 256, 0, ctx->stream>>>(
             B, ctx->joint[ctx->jcur].p, J, st, nullptr);
         LAUNCHED();
+        CHECK(init_old_manifolds(ctx));
         CHECK(broadphase(ctx, true));
     }
     {

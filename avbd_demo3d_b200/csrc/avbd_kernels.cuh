@@ -1940,21 +1940,43 @@ AVBD_DEV int ext_lookup(const ExternalContacts &E, int a, int b)
 // for the pair, manifold.cpp:110-117, whole records: their penalty, multipliers and stick
 // state seed the new contacts), keep warm-start data of contacts whose feature key
 // persists, C0, lambda/penalty decay.
+// Ranges with a device step state: INIT_ALL the step's manifolds [0, nManBp); INIT_OLD the
+// ones that existed before the step [0, nMan), which need nothing from this step's
+// broadphase; INIT_NEW its new pairs [nMan, nManBp). With an output buffer O other than M
+// the whole updated record (bodies and sequence number included) goes to O and M is only
+// read, so that a step stopped later leaves M as it was.
+enum ManifoldInitRange
+{
+    INIT_ALL = 0,
+    INIT_OLD = 1,
+    INIT_NEW = 2
+};
+
 template <bool ROUND>
 __global__ void k_manifold_init(DevBodies B, DevManifolds M, int count, Params P, unsigned char *keep,
                                 const StepState *st = nullptr, ExternalContacts E = ExternalContacts(),
-                                int *orphanFlag = nullptr)
+                                int *orphanFlag = nullptr, DevManifolds O = DevManifolds(), int range = INIT_ALL)
 {
     int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (st)
     {
         if (step_aborted(st))
             return;
-        count = st->nManBp;
+        count = range == INIT_OLD ? st->nMan : st->nManBp;
+        if (range == INIT_NEW)
+            m += st->nMan;
     }
     if (m >= count)
         return;
+    const bool moved = O.ab != nullptr && O.ab != M.ab;
+    if (!moved)
+        O = M;
     int2 ab = M.ab[m];
+    if (moved)
+    {
+        O.ab[m] = ab;
+        O.seq[m] = M.seq[m];
+    }
     NpBody A = np_body(B, ab.x), Bb = np_body(B, ab.y);
     float3 pA = A.p, pB = Bb.p;
     float4 qA = A.q, qB = Bb.q;
@@ -1982,7 +2004,8 @@ __global__ void k_manifold_init(DevBodies B, DevManifolds M, int count, Params P
     else
         nn = round ? collide_shapes(A, Bb, P.dt, nc, basis) : collide_boxes(pA, qA, A.size, pB, qB, Bb.size, nc, basis);
     int nOld = M.n[m];
-    float4 *cbase = M.contact + (size_t)m * 32;
+    const float4 *cbase = M.contact + (size_t)m * 32;
+    float4 *obase = O.contact + (size_t)m * 32;
     ContactRec merged[8];
     for (int i = 0; i < nn; ++i)
     {
@@ -2036,12 +2059,12 @@ __global__ void k_manifold_init(DevBodies B, DevManifolds M, int count, Params P
         c.C0 = add(mv(basis, sub(xA, xB)), f3(COLLISION_MARGIN, 0, 0));
         c.lam = mul(mul(c.lam, P.alpha), P.gamma);
         c.pen = clampv(mul(c.pen, P.gamma), PENALTY_MIN, PENALTY_MAX);
-        store_contact(cbase + 4 * i, c);
+        store_contact(obase + 4 * i, c);
     }
-    M.n[m] = nn;
-    M.basis[3 * m + 0] = f4(basis.r0, friction);
-    M.basis[3 * m + 1] = f4(basis.r1, round ? ROUND_FLAG : 0.0f);
-    M.basis[3 * m + 2] = f4(basis.r2, 0.0f);
+    O.n[m] = nn;
+    O.basis[3 * m + 0] = f4(basis.r0, friction);
+    O.basis[3 * m + 1] = f4(basis.r1, round ? ROUND_FLAG : 0.0f);
+    O.basis[3 * m + 2] = f4(basis.r2, 0.0f);
     keep[m] = nn > 0 ? 1 : 0;
     if (nn > 0 && orphanFlag && B.massMoment[ab.x].x <= 0 && B.massMoment[ab.y].x <= 0)
         *orphanFlag = 1;
@@ -2088,8 +2111,10 @@ __global__ void k_joint_init(DevBodies B, DevForces F, Params P, unsigned char *
 // the live contacts' float4s.
 constexpr int COMPACT_LANES = 8;
 
+// `flip`: dst becomes the live buffer (the state counts the swap); otherwise dst is the
+// buffer the step started from and stays the live one.
 __global__ void k_manifold_compact(DevManifolds src, DevManifolds dst, int count, const unsigned char *keep,
-                                   const int *newIndex, StepState *st = nullptr)
+                                   const int *newIndex, StepState *st = nullptr, bool flip = true)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int m = (int)(t / COMPACT_LANES), lane = (int)(t % COMPACT_LANES);
@@ -2101,7 +2126,8 @@ __global__ void k_manifold_compact(DevManifolds src, DevManifolds dst, int count
         if (t == 0)
         {
             st->nMan = count > 0 ? newIndex[count - 1] + (keep[count - 1] ? 1 : 0) : 0;
-            st->flips++;
+            if (flip)
+                st->flips++;
         }
     }
     if (m >= count || !keep[m])

@@ -2973,9 +2973,11 @@ int avbd_synchronize(AvbdContext *ctx)
 
 int avbd_read_bodies(AvbdContext *ctx, const AvbdBodyState *out)
 {
-    SETTLED();
     if (!ctx || !out)
+    {
+        SETTLED();
         return fail(ctx, AVBD_ERR_ARGUMENT, "null argument");
+    }
     int n = ctx->n;
     DArr<float4> *src[MAX_PACKED] = {&ctx->pos,     &ctx->quat,    &ctx->vel,      &ctx->angvel,  &ctx->prevVel,
                                      &ctx->initLin, &ctx->initAng, &ctx->inertLin, &ctx->inertAng};
@@ -2983,45 +2985,60 @@ int avbd_read_bodies(AvbdContext *ctx, const AvbdBodyState *out)
                               out->angular3,          out->prev_velocity3,       out->initial_position3,
                               out->initial_orientation4, out->inertial_position3, out->inertial_orientation4};
     const int width[MAX_PACKED] = {3, 4, 3, 3, 3, 3, 4, 3, 4};
-    if (!n)
+    if (!n || std::none_of(dst, dst + MAX_PACKED, [](const float *d) { return d != nullptr; }))
+    {
+        SETTLED();
         return AVBD_OK;
+    }
     // requested fields packed on the device: written in place into page-locked caller arrays,
-    // the rest downloaded through the staging buffer and copied on the host
-    PackedFields P{};
-    P.count = MAX_PACKED;
-    long long floats = 0;
-    float *mapped[MAX_PACKED] = {};
-    if (std::none_of(dst, dst + MAX_PACKED, [](const float *d) { return d != nullptr; }))
-        return AVBD_OK;
-    for (int f = 0; f < MAX_PACKED; ++f)
-    {
-        mapped[f] = dst[f] ? host_mapped(dst[f]) : nullptr;
-        if (dst[f] && !mapped[f])
-            floats += (long long)width[f] * n;
-    }
-    CHECK(stage_reserve(ctx, (size_t)(floats + 3) / 4));
-    CHECK(reserve(ctx, ctx->stateStage, (size_t)std::max<long long>(floats, 1), false));
-    float *st = (float *)ctx->hStage;
+    // the rest downloaded through the staging buffer (and copied on the host after the wait)
     std::vector<HostCopy> copies;
-    long long off = 0;
-    for (int f = 0; f < MAX_PACKED; ++f)
-    {
-        float *buf = nullptr;
-        if (mapped[f])
-            buf = mapped[f];
-        else if (dst[f])
+    auto issue = [&]() -> int {
+        PackedFields P{};
+        P.count = MAX_PACKED;
+        long long floats = 0;
+        float *mapped[MAX_PACKED] = {};
+        for (int f = 0; f < MAX_PACKED; ++f)
         {
-            buf = ctx->stateStage.p + off;
-            copies.push_back({dst[f], st + off, sizeof(float) * width[f] * (size_t)n});
-            off += (long long)width[f] * n;
+            mapped[f] = dst[f] ? host_mapped(dst[f]) : nullptr;
+            if (dst[f] && !mapped[f])
+                floats += (long long)width[f] * n;
         }
-        P.f[f] = PackedField{src[f]->p, buf, width[f], buf ? (int)aligned16(buf) : 0, 0.0f};
-    }
-    k_pack_state<<<grid_for(n, PACK_BLOCK), PACK_BLOCK, 0, ctx->stream>>>(P, n);
-    LAUNCHED();
-    for (const HostCopy &c : copies)
-        CU(cudaMemcpyAsync((void *)c.src, ctx->stateStage.p + ((const float *)c.src - st), c.bytes,
-                           cudaMemcpyDeviceToHost, ctx->stream));
+        CHECK(stage_reserve(ctx, (size_t)(floats + 3) / 4));
+        CHECK(reserve(ctx, ctx->stateStage, (size_t)std::max<long long>(floats, 1), false));
+        float *st = (float *)ctx->hStage;
+        copies.clear();
+        long long off = 0;
+        for (int f = 0; f < MAX_PACKED; ++f)
+        {
+            float *buf = nullptr;
+            if (mapped[f])
+                buf = mapped[f];
+            else if (dst[f])
+            {
+                buf = ctx->stateStage.p + off;
+                copies.push_back({dst[f], st + off, sizeof(float) * width[f] * (size_t)n});
+                off += (long long)width[f] * n;
+            }
+            P.f[f] = PackedField{src[f]->p, buf, width[f], buf ? (int)aligned16(buf) : 0, 0.0f};
+        }
+        k_pack_state<<<grid_for(n, PACK_BLOCK), PACK_BLOCK, 0, ctx->stream>>>(P, n);
+        LAUNCHED();
+        for (const HostCopy &c : copies)
+            CU(cudaMemcpyAsync((void *)c.src, ctx->stateStage.p + ((const float *)c.src - st), c.bytes,
+                               cudaMemcpyDeviceToHost, ctx->stream));
+        return AVBD_OK;
+    };
+    // With device steps pending, the packing is queued behind them before the wait for them,
+    // so that one wait serves both; if a step stopped on the device and was redone, the
+    // fields are packed again after the redo.
+    const bool early = ctx->pendingFast > 0 && ctx->errCode == 0;
+    if (early)
+        CHECK(issue());
+    const long long redone = ctx->redoneSteps;
+    SETTLED();
+    if (!early || ctx->redoneSteps != redone)
+        CHECK(issue());
     CU(cudaStreamSynchronize(ctx->stream));
     copy_host(copies);
     return AVBD_OK;

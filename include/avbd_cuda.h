@@ -326,7 +326,10 @@ int avbd_set_wait_limits(AvbdContext *ctx, uint32_t colouring_polls, uint32_t it
  * Bodies do not move. Counters land in avbd_get_stats. */
 int avbd_broadphase_only(AvbdContext *ctx);
 
-/* Post-step readback (the contract of readbackAndApply, avbd_gpu_solver.cpp:1970-2022). */
+/* Post-step readback (the contract of readbackAndApply, avbd_gpu_solver.cpp:1970-2022).
+ * Waits for the pending steps; the packing is queued behind them first, so one wait serves
+ * both. On an error return (a pending step failed) the output arrays may have been written
+ * and hold no defined state. */
 int avbd_read_bodies(AvbdContext *ctx, const AvbdBodyState *out);
 int avbd_num_manifolds(AvbdContext *ctx, int32_t *count);
 int avbd_read_manifolds(AvbdContext *ctx, const AvbdManifoldsOut *out);

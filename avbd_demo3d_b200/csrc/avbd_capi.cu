@@ -1949,57 +1949,60 @@ AVBD_DEV void packed_store(const PackedField &f, int i0, int cnt, const float *s
             dst[t] = s[t];
 }
 
-// Packed caller layout -> the device's float4 arrays (absent fields take (0, 0, 0, w)).
+// Packed caller layout -> the device's float4 arrays (absent fields take (0, 0, 0, w)). Every
+// field's stretch is requested before any is used (one shared buffer holds them all), so a
+// block keeps all its reads across the bus in flight at once.
 __global__ void __launch_bounds__(PACK_BLOCK) k_unpack_state(PackedFields P, int n)
 {
-    __shared__ __align__(16) float s[PACK_BLOCK * 4];
+    __shared__ __align__(16) float s[MAX_PACKED][PACK_BLOCK * 4];
     const int i0 = blockIdx.x * PACK_BLOCK;
     const int cnt = min(PACK_BLOCK, n - i0);
     const int t = threadIdx.x;
+    for (int k = 0; k < P.count; ++k)
+        if (P.f[k].buf)
+            packed_load(P.f[k], i0, cnt, s[k]);
+    __syncthreads();
+    if (t >= cnt)
+        return;
     for (int k = 0; k < P.count; ++k)
     {
         const PackedField f = P.f[k];
         float4 v = make_float4(0.0f, 0.0f, 0.0f, f.w);
-        if (f.buf) // uniform over the block
+        if (f.buf)
         {
-            packed_load(f, i0, cnt, s);
-            __syncthreads();
-            if (t < cnt)
-                v = f.width == 4 ? make_float4(s[4 * t], s[4 * t + 1], s[4 * t + 2], s[4 * t + 3])
-                                 : make_float4(s[3 * t], s[3 * t + 1], s[3 * t + 2], 0.0f);
-            __syncthreads();
+            const float *e = s[k] + f.width * t;
+            v = f.width == 4 ? make_float4(e[0], e[1], e[2], e[3]) : make_float4(e[0], e[1], e[2], 0.0f);
         }
-        if (t < cnt)
-            f.arr[i0 + t] = v;
+        f.arr[i0 + t] = v;
     }
 }
 
-// The device's float4 arrays -> the packed caller layout (requested fields only).
+// The device's float4 arrays -> the packed caller layout (requested fields only); all
+// fields are staged first, then stored together.
 __global__ void __launch_bounds__(PACK_BLOCK) k_pack_state(PackedFields P, int n)
 {
-    __shared__ __align__(16) float s[PACK_BLOCK * 4];
+    __shared__ __align__(16) float s[MAX_PACKED][PACK_BLOCK * 4];
     const int i0 = blockIdx.x * PACK_BLOCK;
     const int cnt = min(PACK_BLOCK, n - i0);
     const int t = threadIdx.x;
-    for (int k = 0; k < P.count; ++k)
-    {
-        const PackedField f = P.f[k];
-        if (!f.buf)
-            continue;
-        if (t < cnt)
+    if (t < cnt)
+        for (int k = 0; k < P.count; ++k)
         {
+            const PackedField f = P.f[k];
+            if (!f.buf)
+                continue;
             const float4 v = f.arr[i0 + t];
-            float *d = s + f.width * t;
+            float *d = s[k] + f.width * t;
             d[0] = v.x;
             d[1] = v.y;
             d[2] = v.z;
             if (f.width == 4)
                 d[3] = v.w;
         }
-        __syncthreads();
-        packed_store(f, i0, cnt, s);
-        __syncthreads();
-    }
+    __syncthreads();
+    for (int k = 0; k < P.count; ++k)
+        if (P.f[k].buf)
+            packed_store(P.f[k], i0, cnt, s[k]);
 }
 
 // Host copies between callers' arrays and the pinned staging. (Splitting them over threads

@@ -270,6 +270,35 @@ __global__ void k_rec_iteration(const float4 *pos, const float4 *quat, int n, co
     }
 }
 
+// A taped step run by the single-launch iteration kernel: every slice of the per-iteration
+// records starts as the state before the first iteration, and the kernel overwrites what each
+// iteration changes (the solved bodies' poses, the live slots' multipliers and penalties), so
+// the records equal those k_rec_iteration takes between per-colour iterations.
+__global__ void k_rec_fill(const float4 *pos, const float4 *quat, int n, const float4 *contact, int nMan,
+                           float4 *pose, float4 *lp, int slices)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+    {
+        const float4 p = pos[i], q = quat[i];
+        for (int k = 0; k < slices; ++k)
+        {
+            pose[(size_t)k * 2 * n + i] = p;
+            pose[(size_t)k * 2 * n + n + i] = q;
+        }
+    }
+    if (i < 8ll * nMan)
+    {
+        const float4 *c = contact + (size_t)(i >> 3) * 32 + 4 * (i & 7);
+        const float4 c2 = c[2], c3 = c[3];
+        for (int k = 0; k < slices; ++k)
+        {
+            lp[(size_t)k * 16 * nMan + 2 * i] = c2;
+            lp[(size_t)k * 16 * nMan + 2 * i + 1] = c3;
+        }
+    }
+}
+
 // body-local anchors of every slot
 __global__ void k_tape_geo(const float4 *contact, int nMan, float4 *geo)
 {
@@ -1218,6 +1247,21 @@ int rec_iteration(AvbdContext *ctx, int it)
         ctx->pos.p, ctx->quat.p, n, ctx->man[ctx->cur].contact.p, M, a->pose32.p + (size_t)it * 2 * n,
         a->lp32.p + (size_t)it * 16 * M);
     LAUNCHED();
+    return AVBD_OK;
+}
+
+// the records of a step whose iterations run in one launch (k_iterations writes into them)
+int rec_tape(AvbdContext *ctx, IterTape *tape)
+{
+    AdjointState *a = ctx->adjoint;
+    int n = ctx->n, M = ctx->nMan, slices = ctx->params.iterations + 1;
+    k_rec_fill<<<grid_for(std::max<long long>(n, 8ll * M), 256), 256, 0, ctx->stream>>>(
+        ctx->pos.p, ctx->quat.p, n, ctx->man[ctx->cur].contact.p, M, a->pose32.p, a->lp32.p, slices);
+    LAUNCHED();
+    tape->pose = a->pose32.p;
+    tape->lp = a->lp32.p;
+    tape->n = n;
+    tape->nMan = M;
     return AVBD_OK;
 }
 

@@ -1548,13 +1548,15 @@ int colour_readback(AvbdContext *ctx)
 int rec_step_begin(AvbdContext *ctx);
 int rec_prepared(AvbdContext *ctx);
 int rec_iteration(AvbdContext *ctx, int it);
+int rec_tape(AvbdContext *ctx, IterTape *tape);
 void adjoint_release(AvbdContext *ctx);
 void adjoint_invalidate(AvbdContext *ctx); // the world changed: no backward for the last forward
 
 // Every iteration in one cooperative launch (k_iterations), the contacts' dual updates
-// fused into the next iteration's rows. Recording the differentiable step keeps the
-// per-colour launches, which it hooks between iterations.
-int iterate_persistent(AvbdContext *ctx, bool deviceCounts = false)
+// fused into the next iteration's rows. A taped step (the adjoint's forward) passes its
+// per-iteration records, which the kernel fills as each body and contact finishes an
+// iteration.
+int iterate_persistent(AvbdContext *ctx, bool deviceCounts = false, IterTape tape = IterTape())
 {
     DevBodies B = dev_bodies(ctx);
     DevForces F = dev_forces(ctx);
@@ -1573,11 +1575,13 @@ int iterate_persistent(AvbdContext *ctx, bool deviceCounts = false)
     const StepState *st = deviceCounts ? ctx->stepState.p : nullptr;
     const int *orphans = &ctx->counters.p->orphans;
     void *args[] = {&B, &F, &P, &entries, &colourStart, &nColours, &iterations, &sync, &done, &spinLimit, &st,
-                    &orphans};
+                    &orphans, &tape};
     {
         PhaseScope ps(ctx, AVBD_PHASE_PRIMAL);
         // worlds with round bodies run the instance that evaluates their contact offsets
+        // (a taped step, boxes only, runs the instance that fills its records)
         void *kernel = ctx->hasShapes ? (void *)k_iterations<ITER_G, ITER_BLOCK, ITER_SUB, true>
+                       : tape.pose    ? (void *)k_iterations<ITER_G, ITER_BLOCK, ITER_SUB, false, true>
                                       : (void *)k_iterations<ITER_G, ITER_BLOCK, ITER_SUB, false>;
         CU(cudaLaunchCooperativeKernel(kernel, ctx->iterBlocks, ITER_BLOCK, args,
                                        sizeof(PrimalShared<ITER_G, ITER_BLOCK>), ctx->stream));
@@ -1591,9 +1595,14 @@ int iterate_persistent(AvbdContext *ctx, bool deviceCounts = false)
 
 int iterate(AvbdContext *ctx)
 {
-    if (ctx->iterationMode == AVBD_ITERATIONS_PERSISTENT && ctx->iterBlocks > 0 && !ctx->recording &&
-        ctx->params.iterations > 0 && ctx->nSolve > 0)
-        return iterate_persistent(ctx);
+    if (ctx->iterationMode == AVBD_ITERATIONS_PERSISTENT && ctx->iterBlocks > 0 && ctx->params.iterations > 0 &&
+        ctx->nSolve > 0)
+    {
+        IterTape tape;
+        if (ctx->recording)
+            CHECK(rec_tape(ctx, &tape));
+        return iterate_persistent(ctx, false, tape);
+    }
     DevBodies B = dev_bodies(ctx);
     DevForces F = dev_forces(ctx);
     Params P = dev_params(ctx->params);
@@ -2326,16 +2335,20 @@ int avbd_create(AvbdContext **out, int32_t device_ordinal, void *cuda_stream)
         // the iteration kernel: one block of ITER_BLOCK threads per SM with its shared batch
         int iterSm = 0;
         size_t smem = sizeof(PrimalShared<ITER_G, ITER_BLOCK>);
-        int roundSm = 0;
+        int roundSm = 0, tapeSm = 0;
         if (cudaFuncSetAttribute((const void *)k_iterations<ITER_G, ITER_BLOCK, ITER_SUB, false>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess &&
             cudaFuncSetAttribute((const void *)k_iterations<ITER_G, ITER_BLOCK, ITER_SUB, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess &&
+            cudaFuncSetAttribute((const void *)k_iterations<ITER_G, ITER_BLOCK, ITER_SUB, false, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tapeSm, k_iterations<ITER_G, ITER_BLOCK, ITER_SUB, false, true>,
+                                                          ITER_BLOCK, smem) == cudaSuccess &&
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&iterSm, k_iterations<ITER_G, ITER_BLOCK, ITER_SUB, false>,
                                                           ITER_BLOCK, smem) == cudaSuccess &&
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&roundSm, k_iterations<ITER_G, ITER_BLOCK, ITER_SUB, true>,
                                                           ITER_BLOCK, smem) == cudaSuccess)
-            ctx->iterBlocks = sms * std::min(iterSm, roundSm);
+            ctx->iterBlocks = sms * std::min({iterSm, roundSm, tapeSm});
         cudaGetLastError(); // an unsupported configuration only leaves the per-colour launches
     }
     if (reserve(ctx, ctx->counters, 1, false) || reserve(ctx, ctx->bounds, 8, false) ||

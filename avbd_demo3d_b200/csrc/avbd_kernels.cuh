@@ -2748,6 +2748,17 @@ AVBD_DEV void store_contact_state(float4 *cp, const ContactRec &c)
     cp[3] = make_float4(c.lam.x, c.lam.y, c.lam.z, __uint_as_float((unsigned)c.key | (c.stick ? 0x80000000u : 0u)));
 }
 
+// The same two words into a taped step's record of contact slot `slot` (lp: one iteration's
+// slice of the adjoint's multiplier and penalty tape, two float4s per slot; null: no tape).
+AVBD_DEV void tape_contact_state(float4 *lp, long long slot, const ContactRec &c)
+{
+    if (!lp)
+        return;
+    lp[2 * slot] = make_float4(c.C0.z, c.pen.x, c.pen.y, c.pen.z);
+    lp[2 * slot + 1] =
+        make_float4(c.lam.x, c.lam.y, c.lam.z, __uint_as_float((unsigned)c.key | (c.stick ? 0x80000000u : 0u)));
+}
+
 // rAW, rBW: the contact's world offsets from the two bodies' centres (rotate(q, r) for boxes,
 // contactOffsetWorld for round bodies).
 AVBD_DEV ContactEval eval_contact_arms(const Motion &A, const Motion &Bp, const M3 &basis, float friction,
@@ -3014,7 +3025,7 @@ __global__ void k_entry_fill(DevForces F, const int *entryRow, const int *count,
 // manifold.cpp:183-228); the partner comes from the row entry.
 template <bool COH = false, bool ROUND = false>
 AVBD_DEV unsigned contact_term_self(const DevBodies &B, const DevForces &F, unsigned m, int ci, bool isA, int self,
-                                    int partner, bool dual, const Params &P, float *t)
+                                    int partner, bool dual, const Params &P, float *t, float4 *lpTape = nullptr)
 {
     const float4 *bs = F.man.basis + 3 * (size_t)m;
     float4 b0 = bs[0], b1 = bs[1];
@@ -3036,6 +3047,7 @@ AVBD_DEV unsigned contact_term_self(const DevBodies &B, const DevForces &F, unsi
         // this row's force from the same C with the updated penalty and multiplier
         contact_dual(c, e, P.betaLin);
         store_contact_state(cp, c);
+        tape_contact_state(lpTape, 8ll * m + ci, c);
         contact_force(e, c, b0.w);
     }
     // this body's Jacobian rows, formed again from the basis and its arm as
@@ -3054,7 +3066,7 @@ AVBD_DEV unsigned contact_term_self(const DevBodies &B, const DevForces &F, unsi
 // each by the row of the body that owns it.
 template <bool COH = false, bool ROUND = false>
 AVBD_DEV unsigned listed_row_term(const DevBodies &B, const DevForces &F, int2 row, int self, bool fusedDual,
-                                  const Params &P, float *t)
+                                  const Params &P, float *t, float4 *lpTape = nullptr)
 {
     unsigned e = (unsigned)row.x;
     unsigned i = adj_index(e);
@@ -3064,7 +3076,7 @@ AVBD_DEV unsigned listed_row_term(const DevBodies &B, const DevForces &F, int2 r
     {
     case ADJ_MANIFOLD:
         return contact_term_self<COH, ROUND>(B, F, i, sub, isA, self, row_partner(row),
-                                      fusedDual && (row.y & ROW_OWNS_DUAL) != 0, P, t);
+                                      fusedDual && (row.y & ROW_OWNS_DUAL) != 0, P, t, lpTape);
     case ADJ_JOINT:
     {
         const float4 *d = F.joint + 8 * (size_t)i;
@@ -3128,6 +3140,12 @@ struct IterFlow
     int it = 0;
     int *error = nullptr;
     unsigned spinLimit = 1u << 22; // polls before a partner wait gives up
+    // a taped step (the adjoint's forward): slice k of each tape holds the state after
+    // iteration k - 1 (slice 0 the state before the first); null: no tape
+    float4 *poseTape = nullptr; // per slice: n positions, then n orientations
+    float4 *lpTape = nullptr;   // per slice: two float4s per contact slot (8 per manifold)
+    int tapeN = 0, tapeM = 0;
+    AVBD_DEV float4 *lp_slice(int k) const { return lpTape ? lpTape + (size_t)k * 16 * tapeM : nullptr; }
 };
 
 AVBD_DEV int ld_acquire(const int *p)
@@ -3188,6 +3206,12 @@ AVBD_DEV void solve_and_move(const DevBodies &B, int b, const float *sys, const 
     B.quat[b] = q;
     B.dqLin[b] = f4(sub(p, xyz(i0)), 0.0f);
     B.dqAng[b] = f4(qdiff_inv(q, a0inv), 0.0f);
+    if (flow.poseTape)
+    {
+        float4 *pt = flow.poseTape + (size_t)(flow.it + 1) * 2 * flow.tapeN;
+        pt[b] = f4(p, 0.0f);
+        pt[flow.tapeN + b] = q;
+    }
     if (flow.done) // a release: the body's pose, and the contact updates its rows made before
         st_release(flow.done + b, flow.it + 1); // the block's barrier, are visible before the count
 }
@@ -3195,7 +3219,8 @@ AVBD_DEV void solve_and_move(const DevBodies &B, int b, const float *sys, const 
 template <bool COH>
 AVBD_DEV void dual_joint(const DevBodies &B, const DevForces &F, int j, const Params &P);
 template <bool COH, bool ROUND>
-AVBD_DEV void dual_contact_slot(const DevBodies &B, const DevManifolds &M, long long t, const Params &P);
+AVBD_DEV void dual_contact_slot(const DevBodies &B, const DevManifolds &M, long long t, const Params &P,
+                                float4 *lpTape = nullptr);
 
 // One primal solve per body of a batch of one colour (solver.cpp:1186-1233). Rows: G lanes
 // per body. The solve entries carry the body and its row range; every lane of a group
@@ -3271,7 +3296,8 @@ AVBD_DEV void primal_batch(const DevBodies &B, const DevForces &F, const Params 
                 const int2 row = F.rows[r];
                 if (flow.done)
                     wait_partner(flow, row);
-                sh.kind[g][lane] = listed_row_term<COH, ROUND>(B, F, row, b, fusedDual, P, sh.term[g][lane]);
+                sh.kind[g][lane] =
+                    listed_row_term<COH, ROUND>(B, F, row, b, fusedDual, P, sh.term[g][lane], flow.lp_slice(flow.it));
             }
             __syncwarp(gmask);
             int nrows = min(G, r1 - base);
@@ -3333,7 +3359,8 @@ AVBD_DEV void primal_batch(const DevBodies &B, const DevForces &F, const Params 
                     continue;
                 const unsigned e = (unsigned)row.x;
                 if (adj_type(e) == ADJ_MANIFOLD)
-                    dual_contact_slot<COH, ROUND>(B, F.man, 8ll * adj_index(e) + row_sub(row), P);
+                    dual_contact_slot<COH, ROUND>(B, F.man, 8ll * adj_index(e) + row_sub(row), P,
+                                                  flow.lp_slice(flow.it + 1));
                 else if (adj_type(e) == ADJ_JOINT && row_sub(row) == 0)
                     dual_joint<COH>(B, F, (int)adj_index(e), P);
             }
@@ -3358,7 +3385,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_primal(DevBodies B, DevForces F
 
 // Manifold::updateDual per contact slot (manifold.cpp:231-280); t = manifold * 8 + slot.
 template <bool COH, bool ROUND>
-AVBD_DEV void dual_contact_slot(const DevBodies &B, const DevManifolds &M, long long t, const Params &P)
+AVBD_DEV void dual_contact_slot(const DevBodies &B, const DevManifolds &M, long long t, const Params &P,
+                                float4 *lpTape)
 {
     int m = (int)(t >> 3), ci = (int)(t & 7);
     if (ci >= M.n[m])
@@ -3377,6 +3405,7 @@ AVBD_DEV void dual_contact_slot(const DevBodies &B, const DevManifolds &M, long 
                         : eval_contact(A, Bp, basis, b0.w, c, P.alpha);
     contact_dual(c, e, P.betaLin);
     store_contact_state(cp, c);
+    tape_contact_state(lpTape, t, c);
 }
 
 template <bool ROUND = false>
@@ -3500,11 +3529,21 @@ AVBD_DEV bool iter_barrier(IterSync *s, unsigned &target, unsigned spinLimit = I
 // the other body, so both poses are those the dual sweep of iteration k reads and every
 // contact's update is the same. After one closing grid barrier, the last iteration's
 // contact updates end the launch.
-template <int G, int BLOCK, int SUB, bool ROUND = false>
+// The adjoint's per-iteration record of a taped step (IterFlow's tape fields).
+struct IterTape
+{
+    float4 *pose = nullptr;
+    float4 *lp = nullptr;
+    int n = 0, nMan = 0;
+};
+
+// TAPE: the instance that fills a taped step's records (the others compile without them).
+template <int G, int BLOCK, int SUB, bool ROUND = false, bool TAPE = false>
 __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces F, Params P, const int4 *entries,
                                                          const int *colourStart, int nColours, int iterations,
                                                          IterSync *sync, int *done, unsigned spinLimit,
-                                                         const StepState *st, const int *orphanFlag)
+                                                         const StepState *st, const int *orphanFlag,
+                                                         IterTape tape)
 {
     if (st)
     {
@@ -3529,6 +3568,13 @@ __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces 
     flow.done = barriers ? nullptr : done;
     flow.error = &sync->error;
     flow.spinLimit = spinLimit;
+    if constexpr (TAPE)
+    {
+        flow.poseTape = tape.pose;
+        flow.lpTape = tape.lp;
+        flow.tapeN = tape.n;
+        flow.tapeM = tape.nMan;
+    }
     for (int it = 0; it < iterations; ++it)
     {
         flow.it = it;
@@ -3575,8 +3621,8 @@ __global__ void __launch_bounds__(BLOCK, 1) k_iterations(DevBodies B, DevForces 
         bool orphan = B.massMoment[ab.x].x <= 0 && B.massMoment[ab.y].x <= 0;
         if (!orphan && !barriers)
             continue;
-        for (int r = orphan ? iterations : 1; r > 0; --r)
-            dual_contact_slot<true, ROUND>(B, F.man, t, P);
+        for (int r = orphan ? iterations : 1; r > 0; --r) // update r from the end: iteration iterations - r
+            dual_contact_slot<true, ROUND>(B, F.man, t, P, flow.lp_slice(iterations - r + 1));
     }
     // joints without a dynamic body likewise
     if (!barriers)

@@ -2327,11 +2327,12 @@ int avbd_create(AvbdContext **out, int32_t device_ordinal, void *cuda_stream)
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_ordinal);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_colour_all, 256, 0);
         ctx->colourBlocks = std::max(1, sms * std::max(1, perSm));
-        // the greedy colouring: co-resident, and at most two blocks per SM (every block
-        // reads all blocks' colour counts once)
+        // the greedy colouring: co-resident, and at most four blocks per SM (every block
+        // reads all blocks' colour counts once; more resident warps mean fewer grid-stride
+        // batches per warp, which a chain of neighbours crosses one after another)
         int flowSm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&flowSm, k_colour_greedy, COLOUR_FLOW_BLOCK, 0);
-        ctx->colourFlowBlocks = std::max(1, sms * std::min(2, std::max(1, flowSm)));
+        ctx->colourFlowBlocks = std::max(1, sms * std::min(4, std::max(1, flowSm)));
         // the iteration kernel: one block of ITER_BLOCK threads per SM with its shared batch
         int iterSm = 0;
         size_t smem = sizeof(PrimalShared<ITER_G, ITER_BLOCK>);

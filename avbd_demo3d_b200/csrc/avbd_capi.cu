@@ -189,6 +189,9 @@ struct AvbdContext
     // the step meanwhile. Events fork and join them (sideEv; 6 and 7 for side[2]) and the
     // broadphase's side streams have their own cub scratch.
     cudaStream_t side[3] = {nullptr, nullptr, nullptr};
+    // a synchronous step's non-finite check (k_step_begin's flags, copied to hStepFlags) waits
+    // to be read at the broadphase's first wait for the device, before anything changes
+    bool flagsPending = false;
     cudaEvent_t sideEv[8] = {};
     DArr<char> cubTempSide[2];
     DArr<StepCounters> counters;
@@ -883,6 +886,19 @@ int lbvh_count(AvbdContext *ctx, const unsigned long long *gridKeys, int nB, con
 // Broadphase of every world: appends new manifolds after the existing ones. `deviceCounts`
 // (grid mode only): no host read; k_bp_commit places the new pairs from the device counts
 // and the emitting passes take their base from the step state.
+// The non-finite check of a synchronous step, read after the first wait of its broadphase
+// (which has changed nothing yet): the step is refused before its new pairs are written.
+int nonfinite_checked(AvbdContext *ctx)
+{
+    if (!ctx->flagsPending)
+        return AVBD_OK;
+    ctx->flagsPending = false;
+    if (*ctx->hStepFlags & STEP_SEEN_NONFINITE)
+        return fail(ctx, AVBD_ERR_STATE,
+                    "non-finite body position, orientation or velocity at the start of a step (the step was not run)");
+    return AVBD_OK;
+}
+
 int broadphase(AvbdContext *ctx, bool deviceCounts = false)
 {
     int n = ctx->n;
@@ -916,6 +932,7 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
         k_total<<<1, 1, 0, ctx->stream>>>(ctx->pairOffset.p, ctx->pairCount.p, n, ctx->hScalars);
         LAUNCHED();
         CU(cudaStreamSynchronize(ctx->stream));
+        CHECK(nonfinite_checked(ctx));
         P1 = ctx->hScalars[0];
         if (P1 > 0)
         {
@@ -962,6 +979,7 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
         k_total<<<1, 1, 0, ctx->stream>>>(ctx->pairOffset.p, ctx->pairCount.p, n, ctx->hScalars);
         LAUNCHED();
         CU(cudaStreamSynchronize(ctx->stream));
+        CHECK(nonfinite_checked(ctx));
         P1 = ctx->hScalars[0];
         if (P1 > 0)
         {
@@ -1149,6 +1167,7 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
         CU(cudaMemcpyAsync(ctx->hCapped, ctx->cappedAny.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaMemcpyAsync(ctx->hCounters, cnt, sizeof(StepCounters), cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaStreamSynchronize(ctx->stream));
+        CHECK(nonfinite_checked(ctx));
         if (nB && *ctx->hCapped)
         {
             // rare path: rescale the capped worlds' cells exactly as the reference does, recount
@@ -1324,6 +1343,7 @@ int external_broadphase(AvbdContext *ctx)
         std::vector<unsigned char> flags((size_t)total);
         CU(cudaMemcpyAsync(flags.data(), ctx->extFlags.p, (size_t)total, cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaStreamSynchronize(ctx->stream));
+        CHECK(nonfinite_checked(ctx));
         std::vector<unsigned long long> linked; // unordered pairs given a manifold in this pass
         auto key = [](int2 p) {
             unsigned lo = (unsigned)std::min(p.x, p.y), hi = (unsigned)std::max(p.x, p.y);
@@ -1652,17 +1672,28 @@ int step_once(AvbdContext *ctx)
                                                                                ctx->stepFlags.p);
     LAUNCHED();
     CU(cudaMemcpyAsync(ctx->hStepFlags, ctx->stepFlags.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    CU(cudaStreamSynchronize(ctx->stream));
-    if (*ctx->hStepFlags & STEP_SEEN_NONFINITE)
-        return fail(ctx, AVBD_ERR_STATE,
-                    "non-finite body position, orientation or velocity at the start of a step (the step was not run)");
+    ctx->flagsPending = true; // read by the broadphase at its wait for the pair counts
     if (ctx->recording)
-        CHECK(rec_step_begin(ctx));
+    {
+        int rc = rec_step_begin(ctx);
+        if (rc != AVBD_OK)
+        {
+            ctx->flagsPending = false;
+            return rc;
+        }
+    }
     CU(cudaMemsetAsync(ctx->counters.p, 0, sizeof(StepCounters), ctx->stream));
     ctx->stats.grid_rescaled = 0;
     {
         PhaseScope ps(ctx, AVBD_PHASE_BROADPHASE);
-        CHECK(ctx->external ? external_broadphase(ctx) : broadphase(ctx));
+        int rc = ctx->external ? external_broadphase(ctx) : broadphase(ctx);
+        if (rc == AVBD_OK && ctx->flagsPending) // a broadphase that never waited (fewer than two bodies)
+        {
+            CU(cudaStreamSynchronize(ctx->stream));
+            rc = nonfinite_checked(ctx);
+        }
+        ctx->flagsPending = false;
+        CHECK(rc);
     }
     {
         PhaseScope ps(ctx, AVBD_PHASE_FORCE_INIT);

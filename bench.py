@@ -19,6 +19,7 @@ import os
 import statistics
 import subprocess
 import sys
+import threading
 import time
 
 import numpy as np
@@ -377,12 +378,14 @@ def collision_only(w, scene, rank, world_size, local, reference: bool, frames: i
     out = {"ms_per_frame": dt * 1e3, "bodies_per_s": world_size * (scene.n_bodies - 1) / dt,
            "new_pairs": int(st["manifold_count"]), "pair_checks": int(st["pair_checks"]), "frames": frames}
     if reference and rank == 0:
-        ref, kind = reference_world(scene)
-        ref.step(1)
-        t0 = time.perf_counter()
-        for _ in range(2):
-            ref.broadphase_only()
-        out["cpu_reference"] = {"ms_per_frame": (time.perf_counter() - t0) / 2 * 1e3, "kind": kind,
+        with REFERENCE_LOCK:
+            ref, kind = reference_world(scene)
+            ref.step(1)
+            t0 = time.perf_counter()
+            for _ in range(2):
+                ref.broadphase_only()
+            ref_ms = (time.perf_counter() - t0) / 2 * 1e3
+        out["cpu_reference"] = {"ms_per_frame": ref_ms, "kind": kind,
                                 "cores": cpu_cores(kind),
                                 "state": "the scene after one step (the GPU frames ran on the state after the "
                                          "timed steps; the pair count is of the same order)"}
@@ -711,14 +714,15 @@ def mixed_line(args, local, stream, reference: bool, steps: int = 600, chunk: in
     gpu_early = {key: max(c[key] for c in early) for key in ("max_penetration_m", "max_joint_error_m")}
     out["checks_first_steps"] = {"steps": ref_steps, "gpu": gpu_early}
     if reference:
-        ref, kind = reference_world(scene)
-        ref_checks = []
-        t0 = time.perf_counter()
-        for _ in range(ref_steps):
-            ref.step(1)
-            ref_checks.append(scene_checks(scene, ref.bodies()))
-        ref_s = time.perf_counter() - t0
-        ref.close()
+        with REFERENCE_LOCK:  # waits for the FP64 checker's thread if it still runs
+            ref, kind = reference_world(scene)
+            ref_checks = []
+            t0 = time.perf_counter()
+            for _ in range(ref_steps):
+                ref.step(1)
+                ref_checks.append(scene_checks(scene, ref.bodies()))
+            ref_s = time.perf_counter() - t0
+            ref.close()
         out["checks_first_steps"]["reference"] = {key: max(c[key] for c in ref_checks)
                                                   for key in ("max_penetration_m", "max_joint_error_m")}
         out["checks_first_steps"]["reference_kind"] = kind
@@ -738,8 +742,6 @@ class CpuFp64Reference:
     MARKS = {"stacks65k": (10, 60), "pyramid20": (10, 60, 600)}
 
     def __init__(self):
-        import threading
-
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import checkers
 
@@ -758,15 +760,16 @@ class CpuFp64Reference:
 
     def _run(self):
         try:
-            for name, sc in self.scenes().items():
-                r = self.checkers.Fp64Reference(sc)
-                done, got = 0, {}
-                for m in self.MARKS[name]:
-                    r.step(m - done)
-                    done = m
-                    got[m] = r.bodies()
-                r.close()
-                self.states[name] = got
+            with REFERENCE_LOCK:
+                for name, sc in self.scenes().items():
+                    r = self.checkers.Fp64Reference(sc)
+                    done, got = 0, {}
+                    for m in self.MARKS[name]:
+                        r.step(m - done)
+                        done = m
+                        got[m] = r.bodies()
+                    r.close()
+                    self.states[name] = got
         except Exception as e:  # reported in the line
             self.error = repr(e)
 
@@ -797,6 +800,12 @@ class CpuFp64Reference:
         return out
 
 
+# The reference's CPU solvers (its own build and its double-precision build) share one
+# process-wide worker pool, which serves one caller at a time: every use of them in this
+# process, the FP64 checker's background thread included, holds this lock.
+REFERENCE_LOCK = threading.Lock()
+
+
 def reference_world(scene):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import checkers
@@ -812,11 +821,12 @@ def cpu_cores(kind: str) -> int:
 
 
 def cpu_baseline(scene, warm: int = 1, timed: int = 5):
-    w, kind = reference_world(scene)
-    w.step(warm)
-    t0 = time.perf_counter()
-    w.step(timed)
-    dt = time.perf_counter() - t0
+    with REFERENCE_LOCK:
+        w, kind = reference_world(scene)
+        w.step(warm)
+        t0 = time.perf_counter()
+        w.step(timed)
+        dt = time.perf_counter() - t0
     bodies = scene.n_bodies - 1
     return {"value": bodies * timed / dt, "unit": UNIT, "cores": cpu_cores(kind), "kind": kind,
             "sample": f"the same 65,536-box scene, steps {warm + 1}-{warm + timed} after {warm} untimed step(s), "

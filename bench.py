@@ -57,6 +57,8 @@ def measured_peak():
 NCU_TRAFFIC = {
     "k_iterations": {"bytes_per_launch": 30868224, "summary": "profiles/iterations_stacks65k_ncu.txt",
                      "captured": "2026-12-04", "sources_sha": "cfa5c895c2524f2c"},
+    "k_iterations_batched": {"bytes_per_launch": 9873686000, "summary": "profiles/iterations_batched4096_ncu.txt",
+                             "captured": "2026-12-04", "sources_sha": "cfa5c895c2524f2c"},
     "k_primal": {"bytes_per_launch": None, "summary": "profiles/primal_stacks65k_ncu.txt",
                  "captured": "2026-12-04", "sources_sha": ""},
 }
@@ -432,8 +434,10 @@ def batched_line(args, rank, world_size, local, stream):
     it_s = prof["primal_ms"] / max(1, prof["steps"]) / 1e3
     peak, _ = measured_peak()
     achieved = per_iter * iters / it_s / 1e9 if it_s > 0 else None
+    traffic, traffic_source = ncu_traffic("k_iterations_batched")
     batched_roofline = {"kernel": "k_iterations (all worlds in one launch)", "bound": "hbm", "achieved": achieved,
                         "peak": peak, "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                        "traffic": traffic, "traffic_source": traffic_source,
                         "algorithmic_bytes_per_launch": per_iter * iters, "avg_launch_us": it_s * 1e6, **counts,
                         "phases_ms_per_step": {k[:-3]: round(v / max(1, prof["steps"]), 4) for k, v in prof.items()
                                                if k.endswith("_ms")}}

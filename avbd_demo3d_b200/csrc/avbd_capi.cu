@@ -184,16 +184,18 @@ struct AvbdContext
 
     DArr<char> cubTemp;
     // Side streams of a device step: side[0] builds the pair set, the large bodies' boxes and
-    // the large-large pass, side[1] the large bodies' cell lists, while the context stream
-    // bins and sorts the grid entries; side[2] initialises the manifolds that existed before
-    // the step meanwhile. Events fork and join them (sideEv; 6 and 7 for side[2]) and the
-    // broadphase's side streams have their own cub scratch.
-    cudaStream_t side[3] = {nullptr, nullptr, nullptr};
+    // the large-large pass, side[1] the large bodies' cell lists, side[3] the LBVH mode's tree,
+    // while the context stream bins and sorts the grid entries; side[2] initialises the
+    // manifolds that existed before the step meanwhile. Events fork and join them (sideEv; 6
+    // and 7 for side[2], 8 for the tree) and the broadphase's side streams have their own cub
+    // scratch.
+    cudaStream_t side[4] = {nullptr, nullptr, nullptr, nullptr};
     // a synchronous step's non-finite check (k_step_begin's flags, copied to hStepFlags) waits
     // to be read at the broadphase's first wait for the device, before anything changes
     bool flagsPending = false;
-    cudaEvent_t sideEv[8] = {};
-    DArr<char> cubTempSide[2];
+    cudaEvent_t sideEv[9] = {};
+    DArr<char> cubTempSide[3];
+    Lbvh lbvhTree{}; // the LBVH mode's tree of this step (built on side[3])
     DArr<StepCounters> counters;
     StepCounters *hCounters = nullptr;
     long long *hScalars = nullptr; // pinned scratch for small readbacks
@@ -829,11 +831,12 @@ int large_cell_lists(AvbdContext *ctx, int nL, cudaStream_t s, DArr<char> &temp)
     return AVBD_OK;
 }
 
-// The LBVH part of the grid's counting pass: each world's tree over its binned bodies, then
-// every grid entry's binned partners through it (k_lbvh_count writes the entry totals).
-int lbvh_count(AvbdContext *ctx, const unsigned long long *gridKeys, int nB, const PairSet &S)
+// The LBVH part of the grid's counting pass: each world's tree over its binned bodies
+// (lbvh_build, which needs only the grid parameters and the bodies, so it runs beside the
+// grid entries' sort), then every grid entry's binned partners through it (lbvh_count, which
+// writes the entry totals). lbvh_reserve sizes every buffer first, on the context stream.
+int lbvh_reserve(AvbdContext *ctx, int nB)
 {
-    const int W = ctx->W;
     CHECK(reserve(ctx, ctx->lbvhCodes, (size_t)nB, false));
     CHECK(reserve(ctx, ctx->lbvhCodesAlt, (size_t)nB, false));
     CHECK(reserve(ctx, ctx->lbvhBodies, (size_t)nB, false));
@@ -844,24 +847,30 @@ int lbvh_count(AvbdContext *ctx, const unsigned long long *gridKeys, int nB, con
     CHECK(reserve(ctx, ctx->lbvhHi, 2 * (size_t)nB, false));
     CHECK(reserve(ctx, ctx->lbvhArrivals, (size_t)nB, false));
     CHECK(reserve(ctx, ctx->entryOf, (size_t)ctx->n, false));
+    cub::DoubleBuffer<unsigned long long> dk(ctx->lbvhCodes.p, ctx->lbvhCodesAlt.p);
+    cub::DoubleBuffer<int> dv(ctx->lbvhBodies.p, ctx->lbvhBodiesAlt.p);
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, dk, dv, nB, 0, 32 + bit_width((unsigned long long)(ctx->W - 1)));
+    return reserve(ctx, ctx->cubTempSide[2], std::max<size_t>(bytes, 16), false);
+}
+
+// Morton codes, their sort, the Karras build and the bottom-up refit, on stream s.
+int lbvh_build(AvbdContext *ctx, int nB, cudaStream_t s)
+{
+    const int W = ctx->W;
     DevBodies B = dev_bodies(ctx);
     DevGrid G = dev_grid(ctx);
-    k_grid_entry_of<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(gridKeys, nB, ctx->entryOf.p);
-    LAUNCHED();
-    k_lbvh_codes<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(B, G, ctx->binned.p, nB, ctx->lbvhCodes.p,
-                                                             ctx->lbvhBodies.p);
+    k_lbvh_codes<<<grid_for(nB, 256), 256, 0, s>>>(B, G, ctx->binned.p, nB, ctx->lbvhCodes.p, ctx->lbvhBodies.p);
     LAUNCHED();
     cub::DoubleBuffer<unsigned long long> dk(ctx->lbvhCodes.p, ctx->lbvhCodesAlt.p);
     cub::DoubleBuffer<int> dv(ctx->lbvhBodies.p, ctx->lbvhBodiesAlt.p);
     const int endBit = 32 + bit_width((unsigned long long)(W - 1));
-    size_t bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, bytes, dk, dv, nB, 0, endBit, ctx->stream);
-    CHECK(ensure_temp(ctx, bytes));
-    CU(cub::DeviceRadixSort::SortPairs(ctx->cubTemp.p, bytes, dk, dv, nB, 0, endBit, ctx->stream));
+    size_t bytes = ctx->cubTempSide[2].cap;
+    CU(cub::DeviceRadixSort::SortPairs(ctx->cubTempSide[2].p, bytes, dk, dv, nB, 0, endBit, s));
     ctx->launches++;
-    CU(cudaMemsetAsync(ctx->lbvhParent.p, 0xFF, sizeof(int) * 2 * (size_t)nB, ctx->stream));
-    CU(cudaMemsetAsync(ctx->lbvhArrivals.p, 0, sizeof(unsigned) * (size_t)nB, ctx->stream));
-    Lbvh T;
+    CU(cudaMemsetAsync(ctx->lbvhParent.p, 0xFF, sizeof(int) * 2 * (size_t)nB, s));
+    CU(cudaMemsetAsync(ctx->lbvhArrivals.p, 0, sizeof(unsigned) * (size_t)nB, s));
+    Lbvh &T = ctx->lbvhTree;
     T.codes = dk.Current();
     T.bodies = dv.Current();
     T.segStart = ctx->worldBinnedStart.p;
@@ -872,11 +881,20 @@ int lbvh_count(AvbdContext *ctx, const unsigned long long *gridKeys, int nB, con
     T.lo = ctx->lbvhLo.p;
     T.hi = ctx->lbvhHi.p;
     T.arrivals = ctx->lbvhArrivals.p;
-    k_lbvh_build<<<grid_for(nB, 128), 128, 0, ctx->stream>>>(T);
+    k_lbvh_build<<<grid_for(nB, 128), 128, 0, s>>>(T);
     LAUNCHED();
-    k_lbvh_refit<<<grid_for(nB, 128), 128, 0, ctx->stream>>>(T, B);
+    k_lbvh_refit<<<grid_for(nB, 128), 128, 0, s>>>(T, B);
     LAUNCHED();
-    k_lbvh_count<<<grid_for(nB, 128), 128, 0, ctx->stream>>>(B, dev_forces(ctx), G, T, gridKeys, nB, ctx->entryOf.p,
+    return AVBD_OK;
+}
+
+// The grid entries' partners through the tree, on the context stream (after the build).
+int lbvh_count(AvbdContext *ctx, const unsigned long long *gridKeys, int nB, const PairSet &S)
+{
+    k_grid_entry_of<<<grid_for(nB, 256), 256, 0, ctx->stream>>>(gridKeys, nB, ctx->entryOf.p);
+    LAUNCHED();
+    k_lbvh_count<<<grid_for(nB, 128), 128, 0, ctx->stream>>>(dev_bodies(ctx), dev_forces(ctx), dev_grid(ctx),
+                                                             ctx->lbvhTree, gridKeys, nB, ctx->entryOf.p,
                                                              ctx->pairCount.p, ctx->pairLaneCount.p,
                                                              ctx->pairRecorded.p, ctx->counters.p, S);
     LAUNCHED();
@@ -1029,6 +1047,10 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
         }
         if (nB && nL)
             CHECK(reserve(ctx, ctx->cubTempSide[1], std::max<size_t>(large_sort_bytes(ctx, nL), 16), false));
+        if (nB && lbvh)
+            CHECK(lbvh_reserve(ctx, nB));
+        cudaStream_t S3 = ctx->side[3];
+        cudaEvent_t evTree = ctx->sideEv[8];
         cub::DoubleBuffer<unsigned long long> dk(ctx->bpKeys.p, ctx->bpKeysAlt.p);
         ctx->hScalars[0] = 0;
         ctx->hScalars[1] = 0;
@@ -1090,7 +1112,10 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
                 ctx->pairLaneCount.p, nullptr, S, lbvh ? (1u << 14) : 0x7FFFu);
             LAUNCHED();
             if (lbvh)
+            {
+                CU(cudaStreamWaitEvent(M, evTree, 0)); // the tree, built on side[3]
                 CHECK(lbvh_count(ctx, dk.Current(), nB, S));
+            }
             CHECK(scan_counts(ctx, ctx->pairCount.p, ctx->pairOffset.p, nB, 0));
             ctx->launches++;
             if (!deviceCounts)
@@ -1128,13 +1153,20 @@ int broadphase(AvbdContext *ctx, bool deviceCounts = false)
             LAUNCHED();
             k_bp_params<<<grid_for(ctx->W, 128), 128, 0, M>>>(G, ctx->worldBinned.p);
             LAUNCHED();
+            if (nL || lbvh)
+                CU(cudaEventRecord(evParams, M));
             if (nL)
             {
-                CU(cudaEventRecord(evParams, M));
                 CU(cudaStreamWaitEvent(S2, evParams, 0));
                 CU(cudaStreamWaitEvent(S2, evLarge, 0));
                 CHECK(large_cell_lists(ctx, nL, S2, ctx->cubTempSide[1]));
                 CU(cudaEventRecord(evLists, S2));
+            }
+            if (lbvh) // the tree needs only the grid parameters and the bodies
+            {
+                CU(cudaStreamWaitEvent(S3, evParams, 0));
+                CHECK(lbvh_build(ctx, nB, S3));
+                CU(cudaEventRecord(evTree, S3));
             }
             CHECK(counting_pass(nL > 0));
         }
@@ -2501,6 +2533,7 @@ void avbd_destroy(AvbdContext *ctx)
     release(ctx->cubTemp);
     release(ctx->cubTempSide[0]);
     release(ctx->cubTempSide[1]);
+    release(ctx->cubTempSide[2]);
     release(ctx->counters);
     release(ctx->stepState);
     release(ctx->llChunkLo);

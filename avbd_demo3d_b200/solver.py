@@ -298,6 +298,11 @@ class World:
                         v.shape != (n, self._BODY_WIDTH[k]) or not v.flags.c_contiguous:
                     raise ValueError(f"bodies(out=...): {k} must be a C-contiguous float32 array of shape "
                                      f"({n}, {self._BODY_WIDTH.get(k)})")
+            # the checked arrays' addresses directly (out holds them for the call)
+            st = _lib.AvbdBodyState(*[out[k].ctypes.data if k in out else None for k in (
+                "pos", "quat", "vel", "angvel", "prevvel", "init_lin", "init_ang", "inert_lin", "inert_ang")])
+            self._check(self.lib.avbd_read_bodies(self.h, ctypes.byref(st)), "avbd_read_bodies")
+            return out
         else:
             out = {"pos": np.zeros((n, 3), F32), "quat": np.zeros((n, 4), F32), "vel": np.zeros((n, 3), F32),
                    "angvel": np.zeros((n, 3), F32), "prevvel": np.zeros((n, 3), F32)}
@@ -312,6 +317,13 @@ class World:
     def write_bodies(self, pos=None, quat=None, vel=None, angvel=None, prevvel=None):
         """Overwrite body state (list order) between steps; fields not given keep their values."""
         given = (pos, quat, vel, angvel, prevvel)
+        n = self.n
+        if all(isinstance(x, np.ndarray) and x.dtype == F32 and x.flags.c_contiguous and x.shape == (n, w)
+               for x, w in zip(given, (3, 4, 3, 3, 3))):
+            # every field already float32 and packed: their addresses directly (held by the caller)
+            b = _lib.AvbdBodies(n, *[x.ctypes.data for x in given], None, None, None, None, None)
+            self._check(self.lib.avbd_write_bodies(self.h, ctypes.byref(b)), "avbd_write_bodies")
+            return
         cur = self.bodies() if any(x is None for x in given) else {}
         arr = dict(position3=_c(cur["pos"] if pos is None else pos, F32),
                    orientation4=_c(cur["quat"] if quat is None else quat, F32),

@@ -211,7 +211,10 @@ typedef struct AvbdStats
 
 /* Context lifetime. Replaces constructing a backend for Solver::physicsBackend
  * (makeCpuReferencePhysicsBackend, solver.cpp:676-680). stream may be NULL (the
- * context creates its own). */
+ * context creates its own). The context also creates four non-blocking side streams on the
+ * device, onto which a step forks independent parts of its work (the pair set, large bodies,
+ * the LBVH tree, the initialisation of existing manifolds) and which it joins back with
+ * events: every call's work is still ordered on `stream` as a whole. */
 int avbd_create(AvbdContext **out, int32_t device_ordinal, void *cuda_stream);
 void avbd_destroy(AvbdContext *ctx);
 const char *avbd_last_error(const AvbdContext *ctx);

@@ -1930,9 +1930,9 @@ int settle(AvbdContext *ctx)
     if (s.abort == ABORT_NONE)
         return device_step_ok(ctx) ? device_reserve(ctx) : AVBD_OK; // room for the next steps, now
     ctx->stateDirty = true; // the device's stop word is cleared before the next device step
-    // The stopped steps still rebuilt the per-body force lists (from buffers the host had
-    // swapped for them); the next broadphase reads those lists, so rebuild them from the
-    // confirmed state.
+    // A step that stopped after building the per-body force lists (at the colouring or the
+    // iterations) left them built for its own manifolds; the next broadphase reads those
+    // lists, so rebuild them from the confirmed state.
     CHECK(build_adjacency(ctx));
     if (s.abort == ABORT_ERROR)
     {

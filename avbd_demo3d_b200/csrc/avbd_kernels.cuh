@@ -151,7 +151,7 @@ struct StepState
     int abort;                   // StepAbort, sticky until the host clears it
     int error;                   // StepError of the failure that set ABORT_ERROR
     int stepsDone;               // steps that ran to the end
-    int flips;                   // manifold compactions (each swaps the manifold buffers)
+    int flips;                   // compactions that swapped the manifold buffers (a device step's compacts back without one)
     int nColours, nSolve, rounds;
     int created;                 // new manifolds of the last step
 };
@@ -2106,7 +2106,7 @@ __global__ void k_joint_init(DevBodies B, DevForces F, Params P, unsigned char *
 }
 
 // Stable compaction of manifolds into the other buffer. With a device step state the count
-// is the state's, and the kernel records the surviving count and the buffer swap there.
+// is the state's, and the kernel records the surviving count there (and a swap, with `flip`).
 // COMPACT_LANES threads per manifold: the first copies the header and basis, all of them
 // the live contacts' float4s.
 constexpr int COMPACT_LANES = 8;
@@ -2231,8 +2231,8 @@ __global__ void k_incidences(DevForces F, int shift, int n, unsigned long long *
                              const StepState *st = nullptr, int capacity = 0)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
-    // A stopped step writes nothing from here on: the host has already swapped the manifold
-    // buffers for it, so the counts it would read there are not the live ones.
+    // A stopped step writes nothing from here on: the counts it would read are not the live
+    // ones (its new manifolds were never committed).
     if (step_aborted(st))
         return;
     if (st)

@@ -51,14 +51,15 @@ def measured_peak():
 
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one ncu capture
-# of the kernel on this workload, with the capture's summary file and date and a digest of
-# the kernel's source files at capture time: when the sources have changed since, the
-# figure no longer describes the kernel and the line reports no traffic.
+# of the kernel on this workload, with the capture's summary file and date, the commit the
+# capture ran on and a digest of the kernel sources' code at capture time
+# (kernel_sources_sha, comments left out): when the code has changed since, the figure no
+# longer describes the kernel and the line reports no traffic.
 NCU_TRAFFIC = {
     "k_iterations": {"bytes_per_launch": 30868224, "summary": "profiles/iterations_stacks65k_ncu.txt",
-                     "captured": "2026-12-04", "sources_sha": "cfa5c895c2524f2c"},
+                     "captured": "2026-12-04", "commit": "9466f58", "sources_sha": "6b8145f7b8c71b4a"},
     "k_iterations_batched": {"bytes_per_launch": 9873686000, "summary": "profiles/iterations_batched4096_ncu.txt",
-                             "captured": "2026-12-04", "sources_sha": "cfa5c895c2524f2c"},
+                             "captured": "2026-12-04", "commit": "64ded38", "sources_sha": "6b8145f7b8c71b4a"},
     "k_primal": {"bytes_per_launch": None, "summary": "profiles/primal_stacks65k_ncu.txt",
                  "captured": "2026-12-04", "sources_sha": ""},
 }
@@ -66,13 +67,41 @@ KERNEL_SOURCES = ("avbd_demo3d_b200/csrc/avbd_kernels.cuh", "avbd_demo3d_b200/cs
                   "avbd_demo3d_b200/csrc/avbd_round.cuh", "avbd_demo3d_b200/csrc/avbd_colour.cuh")
 
 
-def kernel_sources_sha() -> str:
+def code_only(text: str) -> str:
+    """C/C++/CUDA source with its comments removed (string and character literals kept) and
+    trailing whitespace and blank lines dropped: what the compiler sees, so that a capture
+    stays matched across comment edits."""
+    out, i, n = [], 0, len(text)
+    while i < n:
+        c = text[i]
+        if c in "\"'":
+            j = i + 1
+            while j < n and text[j] != c:
+                j += 2 if text[j] == "\\" else 1
+            out.append(text[i:j + 1])
+            i = j + 1
+        elif text.startswith("//", i):
+            j = text.find("\n", i)
+            i = n if j < 0 else j
+        elif text.startswith("/*", i):
+            j = text.find("*/", i + 2)
+            i = n if j < 0 else j + 2
+        else:
+            out.append(c)
+            i += 1
+    lines = (line.rstrip() for line in "".join(out).split("\n"))
+    return "\n".join(line for line in lines if line)
+
+
+def kernel_sources_sha(read=None) -> str:
+    """Hash of the kernel sources' code (comments and blank lines left out); `read(path)`
+    gives a file's text (default: the working tree)."""
     import hashlib
 
+    read = read or (lambda f: open(os.path.join(ROOT, f), encoding="utf-8").read())
     h = hashlib.sha256()
     for f in KERNEL_SOURCES:
-        with open(os.path.join(ROOT, f), "rb") as fh:
-            h.update(fh.read())
+        h.update(code_only(read(f)).encode())
     return h.hexdigest()[:16]
 
 
@@ -82,7 +111,8 @@ def ncu_traffic(kernel: str):
     if not rec:
         return None, None
     current = rec["sources_sha"] == kernel_sources_sha()
-    prov = {"summary": rec["summary"], "captured": rec["captured"], "matches_current_source": current}
+    prov = {"summary": rec["summary"], "captured": rec["captured"], "commit": rec.get("commit"),
+            "matches_current_source": current}
     return (rec["bytes_per_launch"] if current else None), prov
 
 
